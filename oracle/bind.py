@@ -1,0 +1,225 @@
+"""ctypes binding of the oracle (oracle/_build/libgi_oracle.so).  Test infrastructure only: imported by tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline leg, never by the product path.
+
+``build()`` compiles the oracle with its Makefile when the library is missing or older than its sources.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libgi_oracle.so")
+SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "orc_par.c", "gi_oracle.h", "orc_math.h", "orc_par.h", "Makefile"]
+
+
+def build(force: bool = False) -> str:
+    newest = max(os.path.getmtime(os.path.join(HERE, s)) for s in SOURCES)
+    if force or not os.path.exists(LIB_PATH) or os.path.getmtime(LIB_PATH) < newest:
+        subprocess.run(["make", "-C", HERE, "-s"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB_PATH)
+        _lib.orc_vox_build.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_rc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_rc_merge_gather.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_rc_merge_gather_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_raster_gbuffer.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_pack4x8unorm.argtypes = [C.c_void_p]
+        _lib.orc_pack4x8unorm.restype = C.c_uint32
+        _lib.orc_pack2x16snorm.argtypes = [C.c_float, C.c_float]
+        _lib.orc_pack2x16snorm.restype = C.c_uint32
+        _lib.orc_f32_to_f16.argtypes = [C.c_float]
+        _lib.orc_f32_to_f16.restype = C.c_uint16
+        _lib.orc_f16_to_f32.argtypes = [C.c_uint16]
+        _lib.orc_f16_to_f32.restype = C.c_float
+        _lib.orc_f32_to_bf16.argtypes = [C.c_float]
+        _lib.orc_f32_to_bf16.restype = C.c_uint16
+        _lib.orc_tri_box.argtypes = [C.c_void_p] * 5
+        _lib.orc_tri_box.restype = C.c_int
+        _lib.orc_round_log2.argtypes = [C.c_float]
+        _lib.orc_round_log2.restype = C.c_uint32
+    return _lib
+
+
+def _p(a: np.ndarray) -> int:
+    assert a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data
+
+
+class OrcScene(C.Structure):
+    _fields_ = [("pos", C.c_void_p), ("nrm", C.c_void_p), ("nverts", C.c_uint32), ("tri", C.c_void_p),
+                ("ntris", C.c_uint32), ("mats", C.c_void_p), ("nmats", C.c_uint32)]
+
+
+class OrcVox(C.Structure):
+    _fields_ = [("v0", C.c_float), ("levels", C.c_uint32), ("G", C.c_uint32), ("max_bricks", C.c_uint32),
+                ("max_voxels", C.c_uint32), ("big_cap", C.c_uint32), ("coarse_from_triangles", C.c_uint32),
+                ("origin", (C.c_int32 * 4) * 8),
+                ("hdr", C.c_void_p), ("ptr", C.c_void_p), ("occ", C.c_void_p), ("base", C.c_void_p),
+                ("code", C.c_void_p), ("rep", C.c_void_p), ("big", C.c_void_p), ("attr", C.c_void_p),
+                ("plane", C.c_void_p), ("sunvis", C.c_void_p)]
+
+
+class OrcCasc(C.Structure):
+    _fields_ = [("probe_off", C.c_uint32), ("cap", C.c_uint32), ("rad_off", C.c_uint32), ("res", C.c_uint32),
+                ("tile_size", C.c_uint32), ("tiles_x", C.c_uint32), ("tiles_y", C.c_uint32), ("pad", C.c_uint32),
+                ("b0", C.c_float), ("b1", C.c_float), ("pad2", C.c_float * 2)]
+
+
+class OrcLayout(C.Structure):
+    _fields_ = [("cascades", C.c_uint32), ("c", OrcCasc * 8), ("vox_scale", C.c_float), ("vox_offset", C.c_float),
+                ("level_map", C.c_float), ("vox_skip", C.c_float), ("dda_cap", C.c_uint32), ("stats", C.c_uint32),
+                ("atlas", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class OrcGbuf(C.Structure):
+    _fields_ = [("frame", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32), ("depth", C.c_void_p),
+                ("normal", C.c_void_p)]
+
+
+class OrcRcOut(C.Structure):
+    _fields_ = [("probes", C.c_void_p), ("rad", C.c_void_p), ("sh", C.c_void_p), ("irr", C.c_void_p),
+                ("counts", C.c_void_p), ("hit", C.c_void_p)]
+
+
+PROBE_DTYPE = np.dtype([("pos", "<f4", (4,)), ("nrm", "<f4", (4,)), ("grid", "<i4", (4,))])
+
+
+def _scene_struct(scene):
+    pos = np.ascontiguousarray(scene.positions, dtype=np.float32)
+    nrm = np.ascontiguousarray(scene.normals, dtype=np.float32)
+    tri = np.ascontiguousarray(scene.tri, dtype=np.uint32)
+    mats = scene.material_array()
+    s = OrcScene(_p(pos), _p(nrm), pos.shape[0], _p(tri), tri.shape[0], _p(mats), len(mats))
+    return s, (pos, nrm, tri, mats)
+
+
+def vox_origins(v0: float, levels: int, G: int, eye) -> np.ndarray:
+    """writeUniform's per-level window origins (voxel.ts:872-876), host f64 math."""
+    import math
+    o = np.zeros((8, 4), dtype=np.int32)
+    for L in range(levels):
+        bs = v0 * 2 ** L * 8
+        for a in range(3):
+            o[L, a] = math.floor(eye[a] / bs) - G // 2
+    return o
+
+
+def vox_build(scene, v0: float, levels: int, G: int, max_bricks: int, max_voxels: int, eye,
+              coarse_from_triangles: bool = False, big_cap: int = 1 << 18) -> dict:
+    s, keep = _scene_struct(scene)
+    per = G ** 3
+    st = {
+        "hdr": np.zeros(64, np.uint32), "ptr": np.zeros(levels * per, np.uint32),
+        "occ": np.zeros(max_bricks * 16, np.uint32), "base": np.zeros(max_bricks, np.uint32),
+        "code": np.zeros(max_bricks, np.uint32), "rep": np.zeros(max_bricks * 512, np.uint32),
+        "big": np.zeros(16 * big_cap, np.uint32), "attr": np.zeros(max_voxels * 4, np.uint32),
+        "plane": np.zeros(max_voxels, np.float32), "sunvis": np.zeros(max_voxels, np.float32),
+    }
+    vx = OrcVox()
+    vx.v0 = np.float32(v0)
+    vx.levels, vx.G, vx.max_bricks, vx.max_voxels, vx.big_cap = levels, G, max_bricks, max_voxels, big_cap
+    vx.coarse_from_triangles = 1 if coarse_from_triangles else 0
+    org = vox_origins(float(np.float32(v0)), levels, G, eye)
+    for L in range(8):
+        for a in range(4):
+            vx.origin[L][a] = int(org[L, a])
+    for k in ("hdr", "ptr", "occ", "base", "code", "rep", "big", "attr", "plane", "sunvis"):
+        setattr(vx, k, _p(st[k]))
+    lib().orc_vox_build(C.byref(s), C.byref(vx))
+    del st["big"]
+    st.update(v0=float(np.float32(v0)), levels=levels, G=G, max_bricks=max_bricks, max_voxels=max_voxels, origin=org)
+    return st
+
+
+def _vox_struct(st: dict) -> OrcVox:
+    vx = OrcVox()
+    vx.v0 = st["v0"]
+    vx.levels, vx.G, vx.max_bricks, vx.max_voxels = st["levels"], st["G"], st["max_bricks"], st["max_voxels"]
+    vx.big_cap = 0
+    for L in range(8):
+        for a in range(4):
+            vx.origin[L][a] = int(st["origin"][L, a])
+    for k in ("hdr", "ptr", "occ", "base", "code", "rep", "attr", "plane", "sunvis"):
+        setattr(vx, k, _p(st[k]))
+    vx.big = None
+    return vx
+
+
+def layout_struct(lay: dict) -> OrcLayout:
+    ly = OrcLayout()
+    ly.cascades = lay["cascades"]
+    for i, c in enumerate(lay["casc"]):
+        ly.c[i].probe_off, ly.c[i].cap, ly.c[i].rad_off, ly.c[i].res = c["probe_off"], c["cap"], c["rad_off"], c["res"]
+        ly.c[i].tile_size, ly.c[i].tiles_x, ly.c[i].tiles_y = c["tile_size"], c["tiles_x"], c["tiles_y"]
+        ly.c[i].b0, ly.c[i].b1 = c["b0"], c["b1"]
+    ly.vox_scale, ly.vox_offset, ly.level_map, ly.vox_skip = lay["vox_scale"], lay["vox_offset"], lay["level_map"], lay["vox_skip"]
+    ly.dda_cap, ly.stats, ly.atlas = lay["dda_cap"], lay["stats"], lay["atlas"]
+    return ly
+
+
+def rc_solve(vox: dict, lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np.ndarray, want_hit: bool = False,
+             merge: bool = True) -> dict:
+    """setupScreen + trace, then (merge=True) mergeScreen + projectSH + gatherScreen.  Returns numpy outputs; 'rad_traced'
+    is the atlas right after the trace."""
+    H, W = depth.shape
+    ly = layout_struct(lay)
+    probes_total = sum(c["cap"] for c in lay["casc"])
+    rad_total = sum(c["cap"] * c["res"] ** 2 for c in lay["casc"])
+    out = {"probes": np.zeros(probes_total, PROBE_DTYPE), "rad": np.zeros((rad_total, 4), np.float32),
+           "sh": np.zeros((lay["casc"][0]["cap"], 32), np.float32), "irr": np.zeros((H, W, 4), np.float32),
+           "counts": np.zeros(80, np.uint32)}
+    if want_hit:
+        out["hit"] = np.zeros((rad_total, 4), np.uint32)
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    normal = np.ascontiguousarray(normal, dtype=np.float32)
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    o = OrcRcOut(_p(out["probes"]), _p(out["rad"]), _p(out["sh"]), _p(out["irr"]), _p(out["counts"]),
+                 _p(out["hit"]) if want_hit else None)
+    vx = _vox_struct(vox)
+    lib().orc_rc_trace(C.byref(vx), C.byref(ly), C.byref(g), C.byref(o))
+    out["rad_traced"] = out["rad"].copy()
+    if merge:
+        lib().orc_rc_merge_gather(C.byref(ly), C.byref(g), C.byref(o))
+    return out
+
+
+def merge_gather_f64(lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np.ndarray, probes: np.ndarray,
+                     rad_traced: np.ndarray) -> np.ndarray:
+    H, W = depth.shape
+    ly = layout_struct(lay)
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    normal = np.ascontiguousarray(normal, dtype=np.float32)
+    probes = np.ascontiguousarray(probes)
+    rad = np.ascontiguousarray(rad_traced, dtype=np.float32)
+    irr = np.zeros((H, W, 4), np.float64)
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    lib().orc_rc_merge_gather_f64(C.byref(ly), C.byref(g), _p(probes), _p(rad), _p(irr))
+    return irr
+
+
+def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int):
+    s, keep = _scene_struct(scene)
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    depth = np.zeros((H, W), np.float32)
+    normal = np.zeros((H, W, 4), np.float32)
+    tri = np.zeros((H, W), np.uint32)
+    r = lib().orc_raster_gbuffer(C.byref(s), _p(frame), W, H, _p(depth), _p(normal), _p(tri))
+    if r != 0:
+        raise MemoryError("oracle raster: out of memory")
+    return depth, normal, tri

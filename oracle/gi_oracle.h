@@ -1,0 +1,149 @@
+/*
+ * gi_oracle — CPU restatement of the real-time-gi-lab GI hot path, used ONLY as test infrastructure.
+ *
+ * This library is the checker for the CUDA path: tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline leg are the only callers.  It is never linked into, or called by, the product library.
+ *
+ * It restates, sequentially and in plain C, the WGSL of the reference renderer (owoDra/real-time-gi-lab):
+ *   - the voxel clipmap rebuild            src/core/voxel.ts:205-620 (build WGSL), :868-892 (writeUniform)
+ *   - the two-level voxel DDA              src/core/voxel.ts:75-203  (voxRank, voxAt, voxLevelFor, traceVox)
+ *   - hit shading                          src/core/rc.ts:95-141, src/core/style.ts:16-26
+ *   - screen probes, trace, merge, SH,     src/core/rc.ts:210-310, :572-622, :679-774, :819-829, :929-954
+ *     gather
+ *   - the headless G-buffer raster         src/core/gbuffer.ts:82-103 (conventions only; the reference draws it
+ *                                          with a graphics pipeline, restated here as a scanline raster)
+ *
+ * Arithmetic follows the WGSL expression order exactly (left-associative, no contraction: build with
+ * -ffp-contract=off).  Where the WGSL leaves a builtin implementation-defined, the choice made here is stated
+ * at the function (normalize = v / sqrt(dot), round(log2(x)) exact, pack* = the WGSL spec formulas, f16 = RNE).
+ *
+ * Pinning: the reference cannot run here (WGSL through Dawn/Vulkan on Node).  The voxel build is pinned against
+ * the brick/voxel counters the reference recorded for its procedural leak rooms
+ * (docs/reference/measurements/s2-voxel-stratabrick/leak-<t>/world-32-voxel.summary.json, static.vox); the
+ * tracer, merge and gather have no recorded reference output for a reproducible scene: parity unpinned there.
+ */
+#ifndef GI_ORACLE_H
+#define GI_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ORC_HDR 64
+#define ORC_EMPTY 0xffffffffu
+#define ORC_DROP 0xfffffffeu
+#define ORC_MARK 0xfffffffdu
+
+/* Material: baseColorFactor, flags (1 alpha mask, 2 double-sided, 4 toon, 8 object; scene_gpu.ts:95-104),
+ * alpha cutoff, and the emissive radiance this build adds (the reference has no emission). 48 bytes. */
+typedef struct {
+  float base_color[4];
+  uint32_t flags;
+  float alpha_cutoff;
+  float emissive[3];
+  uint32_t reserved[3];
+} orc_material;
+
+typedef struct {
+  const float *pos;        /* xyz per vertex */
+  const float *nrm;        /* xyz per vertex */
+  uint32_t nverts;
+  const uint32_t *tri;     /* (i0, i1, i2, material) per triangle: triangleTable, voxel.ts:730 */
+  uint32_t ntris;
+  const orc_material *mats;
+  uint32_t nmats;
+} orc_scene;
+
+/* Voxel world state, laid out exactly as the CUDA path lays it out in device memory (struct of arrays). */
+typedef struct {
+  /* parameters (VoxParams, voxel.ts:31) */
+  float v0;
+  uint32_t levels, G, max_bricks, max_voxels;
+  uint32_t big_cap;                /* entries per big-triangle segment (BIG_CAP, voxel.ts:224) */
+  uint32_t coarse_from_triangles;  /* 1: every level voxelised from the triangles (the pre-phase-21 build); pin runs only */
+  int32_t origin[8][4];            /* per level: first brick of the window (world brick coordinates) */
+  /* buffers (caller-allocated) */
+  uint32_t *hdr;                   /* ORC_HDR counter words (voxel.ts:11) */
+  uint32_t *ptr;                   /* levels * G^3 brick pointers */
+  uint32_t *occ;                   /* max_bricks * 16 occupancy words */
+  uint32_t *base;                  /* max_bricks: first attribute */
+  uint32_t *code;                  /* max_bricks: level << 27 | bx << 18 | by << 9 | bz */
+  uint32_t *rep;                   /* max_bricks * 512: representative triangle + 1 */
+  uint32_t *big;                   /* 16 * big_cap: segments 0-7 voxBits per level, 8-15 markBricks per level */
+  uint32_t *attr;                  /* max_voxels * 4: albedo, normal, emissive rg (f16x2), emissive b (f16) */
+  float *plane;                    /* max_voxels: representative plane offset from the voxel centre */
+  float *sunvis;                   /* max_voxels: sun visibility of the voxel (1 when no visibility pass runs) */
+} orc_vox;
+
+/* Host writeUniform (voxel.ts:868-876): per level origin = floor(eye / bs) - G/2, bs = v0 * 2^L * 8 (f64 host math). */
+void orc_vox_origins(float v0, uint32_t levels, uint32_t G, const double eye[3], int32_t origin_out[8][4]);
+/* The whole rebuild (VOX_STAGES minus sun): clear .. resolveAttr.  Returns 0. */
+int orc_vox_build(const orc_scene *s, orc_vox *vx);
+
+/* Cascade layout (rc.ts:1024-1035) for the screen method. */
+typedef struct {
+  uint32_t probe_off, cap, rad_off, res, tile_size, tiles_x, tiles_y, pad;
+  float b0, b1, pad2[2];
+} orc_casc;
+
+typedef struct {
+  uint32_t cascades;
+  orc_casc c[8];
+  /* wp: voxScale, voxOffset, levelMap, voxSkip */
+  float vox_scale, vox_offset, level_map, vox_skip;
+  uint32_t dda_cap;       /* DDA step cap (the reference hard-codes 1024, voxel.ts:142) */
+  uint32_t stats;         /* 0 off, 1 DDA step counters (rc.ts:232-235) */
+  uint32_t atlas;         /* 0: f32 storage, 1: f16 (the reference's rgba16 packing), 2: bf16 */
+  uint32_t pad;
+} orc_layout;
+
+/* One probe (rc.ts:157): pos.xyz + s0, nrm.xyz + view depth, grid. 48 bytes. */
+typedef struct { float pos[4]; float nrm[4]; int32_t grid[4]; } orc_probe;
+
+typedef struct {
+  const float *frame;       /* 160 words (packFrame, frame.ts:76) */
+  uint32_t width, height;
+  const float *depth;       /* W*H reversed-Z depth (0 = background) */
+  const float *normal;      /* W*H*4, the G-buffer normal as read from its rgba16float texture */
+} orc_gbuf;
+
+typedef struct {
+  orc_probe *probes;        /* sum of caps */
+  float *rad;               /* sum over cascades of cap * res^2 * 4 (values after the atlas rounding) */
+  float *sh;                /* cap0 * 32 (27 used), after the atlas rounding */
+  float *irr;               /* W*H*4 (rgb + alpha), after the output rounding (f16 unless atlas = f32) */
+  uint32_t *counts;         /* 80 words (rc.ts:173-175) */
+  /* optional debug (may be NULL): per traced ray of every cascade, the hit: level, brick pointer, bit, tIn bits */
+  uint32_t *hit;            /* 4 words per ray, rad order */
+} orc_rc_out;
+
+/* setupScreen (all cascades) + trace (all cascades).  rad holds the traced (unmerged) intervals. */
+int orc_rc_trace(const orc_vox *vx, const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o);
+/* mergeScreen (N-1 .. 0) + projectSH + gatherScreen on o->rad (in place). */
+int orc_rc_merge_gather(const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o);
+/* The same in float64 throughout (no intermediate rounding): the FP64 accuracy oracle of the merge and gather.
+ * rad_in: traced intervals (f32, unmerged).  irr_out: W*H*4 doubles. */
+int orc_rc_merge_gather_f64(const orc_layout *ly, const orc_gbuf *g, const orc_probe *probes, const float *rad_in,
+                            double *irr_out);
+
+/* Headless G-buffer: depth (reversed Z, infinite far) and the shading normal (interpolated vertex normal,
+ * flipped to the viewer for back faces), one sample at each pixel centre.  normal_out is rgba, w = 0.
+ * tri_out (optional) receives the winning triangle per pixel (0xffffffff: none). */
+int orc_raster_gbuffer(const orc_scene *s, const float *frame, uint32_t width, uint32_t height, float *depth_out,
+                       float *normal_out, uint32_t *tri_out);
+
+/* WGSL builtins as the oracle defines them (exported for the known-answer tests). */
+uint32_t orc_pack4x8unorm(const float v[4]);
+uint32_t orc_pack2x16snorm(float a, float b);
+uint16_t orc_f32_to_f16(float x);
+float orc_f16_to_f32(uint16_t h);
+uint16_t orc_f32_to_bf16(float x);
+float orc_bf16_to_f32(uint16_t h);
+int orc_tri_box(const float c[3], const float h[3], const float a[3], const float b[3], const float cc[3]);
+uint32_t orc_round_log2(float x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,61 @@
+/* Scalar/vector helpers of the oracle.  Every operation is one IEEE f32 operation in WGSL's evaluation order
+ * (left to right, no fused multiply-add: the oracle is built with -ffp-contract=off). */
+#ifndef ORC_MATH_H
+#define ORC_MATH_H
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+
+typedef struct { float x, y, z; } v3;
+typedef struct { int32_t x, y, z; } i3;
+
+static inline v3 V(float x, float y, float z) { v3 r = {x, y, z}; return r; }
+static inline i3 I(int32_t x, int32_t y, int32_t z) { i3 r = {x, y, z}; return r; }
+static inline v3 add(v3 a, v3 b) { return V(a.x + b.x, a.y + b.y, a.z + b.z); }
+static inline v3 sub(v3 a, v3 b) { return V(a.x - b.x, a.y - b.y, a.z - b.z); }
+static inline v3 mul(v3 a, v3 b) { return V(a.x * b.x, a.y * b.y, a.z * b.z); }
+static inline v3 divv(v3 a, v3 b) { return V(a.x / b.x, a.y / b.y, a.z / b.z); }
+static inline v3 muls(v3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
+static inline v3 divs(v3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
+static inline v3 adds(v3 a, float s) { return V(a.x + s, a.y + s, a.z + s); }
+static inline v3 neg(v3 a) { return V(-a.x, -a.y, -a.z); }
+static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline v3 cross(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+static inline float fminf_(float a, float b) { return a < b ? a : b; }
+static inline float fmaxf_(float a, float b) { return a > b ? a : b; }
+static inline v3 vmin(v3 a, v3 b) { return V(fminf_(a.x, b.x), fminf_(a.y, b.y), fminf_(a.z, b.z)); }
+static inline v3 vmax(v3 a, v3 b) { return V(fmaxf_(a.x, b.x), fmaxf_(a.y, b.y), fmaxf_(a.z, b.z)); }
+static inline v3 vabs(v3 a) { return V(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+static inline v3 vfloor(v3 a) { return V(floorf(a.x), floorf(a.y), floorf(a.z)); }
+/* normalize(v) = v / sqrt(dot(v, v)) (IEEE sqrt and division). */
+static inline float length3(v3 a) { return sqrtf(dot(a, a)); }
+static inline v3 normalize3(v3 a) { float l = length3(a); return V(a.x / l, a.y / l, a.z / l); }
+static inline v3 fromf(const float *p) { return V(p[0], p[1], p[2]); }
+static inline float comp(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
+
+/* f32 -> i32, truncating, saturating (WGSL's conversion of an out-of-range float). */
+static inline int32_t f2i(float f) {
+  if (f != f) return 0;
+  if (f >= 2147483520.0f) return 2147483647;
+  if (f <= -2147483648.0f) return (-2147483647 - 1);
+  return (int32_t)f;
+}
+static inline i3 vf2i(v3 a) { return I(f2i(a.x), f2i(a.y), f2i(a.z)); }
+static inline v3 vi2f(i3 a) { return V((float)a.x, (float)a.y, (float)a.z); }
+static inline int32_t imin(int32_t a, int32_t b) { return a < b ? a : b; }
+static inline int32_t imax(int32_t a, int32_t b) { return a > b ? a : b; }
+static inline int32_t iclamp(int32_t x, int32_t lo, int32_t hi) { return imin(imax(x, lo), hi); }
+static inline i3 iclamp3(i3 a, i3 lo, i3 hi) { return I(iclamp(a.x, lo.x, hi.x), iclamp(a.y, lo.y, hi.y), iclamp(a.z, lo.z, hi.z)); }
+static inline float fclampf(float x, float lo, float hi) { return fminf_(fmaxf_(x, lo), hi); }
+static inline float fbits(uint32_t u) { float f; memcpy(&f, &u, 4); return f; }
+static inline uint32_t ubits(float f) { uint32_t u; memcpy(&u, &f, 4); return u; }
+static inline uint32_t popc(uint32_t x) { return (uint32_t)__builtin_popcount(x); }
+
+/* v0 * 2^L, exact. */
+static inline float scale2(float x, int L) { return ldexpf(x, L); }
+/* exp2(x): exact for integral x (the only values the configs produce), libm otherwise. */
+static inline float exp2_(float x) {
+  if (x == floorf(x) && fabsf(x) < 126.0f) return ldexpf(1.0f, (int)x);
+  return exp2f(x);
+}
+#endif

@@ -1,0 +1,486 @@
+/* Sequential restatement of the screen-probe radiance cascades over the voxel tracer (src/core/rc.ts, method
+ * 'screen', world tracer 'voxel', depthCascades 0: the config token 'voxel').  Test infrastructure only.
+ *
+ * Follows rc.ts:95-141 (shading), :210-245 (traceWorld), :291-311 (octahedral maps, packing), :572-590
+ * (setupScreen), :600-622 (trace), :681-743 (upperAvg, mergeScreen), :745-774 (shBasis, projectSH),
+ * :819-829 (evalSH), :929-954 (gatherScreen), and voxel.ts:81-202 (voxRank, voxAt, voxLevelFor, traceVox).
+ * Multi-bounce (BN_ON), the dynamic layer (dyn[0] = 0) and the triangle comparator are off, as in the
+ * configurations this build measures.  The hit radiance adds the voxel's emissive radiance (the reference has no
+ * emission). */
+#include <stdlib.h>
+#include "gi_oracle.h"
+#include "orc_math.h"
+#include "orc_par.h"
+
+#define PI_F 3.14159265f
+
+/* Frame word offsets (frame.ts:4-21, packFrame :76-93). */
+enum { F_VP = 0, F_IVP = 16, F_EYE = 80, F_FWD = 84, F_SUN = 88, F_SUNE = 92, F_SKY = 96, F_SIZE = 100, F_RC = 104,
+       F_RC2 = 108, F_RU = 112, F_RU2 = 116, F_OMEGA = 120, F_STYLE = 136 };
+
+typedef struct {
+  const orc_vox *vx;
+  const float *F;
+  float sky[3];
+} ctx_t;
+
+static inline float vox_size(const orc_vox *vx, uint32_t L) { return scale2(vx->v0, (int)L); }
+static inline i3 org(const orc_vox *vx, uint32_t L) { return I(vx->origin[L][0], vx->origin[L][1], vx->origin[L][2]); }
+static inline uint32_t ptr_index(const orc_vox *vx, uint32_t L, i3 b) {
+  uint32_t G = vx->G;
+  return L * G * G * G + ((uint32_t)b.z * G + (uint32_t)b.y) * G + (uint32_t)b.x;
+}
+
+/* worldAt (frame.ts:22-26); mat4 * vec4 summed in column order. */
+static v3 world_at(const float *F, int32_t px, int32_t py, float d) {
+  float nx = ((float)px + 0.5f) * F[F_SIZE + 2] * 2.0f - 1.0f;
+  float ny = 1.0f - ((float)py + 0.5f) * F[F_SIZE + 3] * 2.0f;
+  const float *m = F + F_IVP;
+  float h[4];
+  for (int i = 0; i < 4; i++) h[i] = m[i] * nx + m[4 + i] * ny + m[8 + i] * d + m[12 + i] * 1.0f;
+  return V(h[0] / h[3], h[1] / h[3], h[2] / h[3]);
+}
+static float view_z(const float *F, v3 p) { return dot(sub(p, fromf(F + F_EYE)), fromf(F + F_FWD)); }
+
+/* octDecode / dirOf (rc.ts:291-308) */
+static v3 oct_decode(float u, float v) {
+  float fx = u * 2.0f - 1.0f, fy = v * 2.0f - 1.0f;
+  v3 n = V(fx, fy, 1.0f - fabsf(fx) - fabsf(fy));
+  float t = fmaxf_(-n.z, 0.0f);
+  n.x += n.x >= 0.0f ? -t : t;
+  n.y += n.y >= 0.0f ? -t : t;
+  return normalize3(n);
+}
+static v3 dir_of(uint32_t di, uint32_t res) {
+  return oct_decode(((float)(di % res) + 0.5f) / (float)res, ((float)(di / res) + 0.5f) / (float)res);
+}
+
+static float round_store(float x, uint32_t atlas) {
+  if (atlas == 1) return orc_f16_to_f32(orc_f32_to_f16(x));
+  if (atlas == 2) return orc_bf16_to_f32(orc_f32_to_bf16(x));
+  return x;
+}
+
+/* voxRank (voxel.ts:81-87) */
+static uint32_t vox_rank(const orc_vox *vx, uint32_t brick, uint32_t bit) {
+  uint32_t w = bit >> 5;
+  uint32_t r = popc(vx->occ[brick * 16u + w] & ((1u << (bit & 31u)) - 1u));
+  for (uint32_t i = 0; i < w; i++) r += popc(vx->occ[brick * 16u + i]);
+  return vx->base[brick] + r;
+}
+/* voxAt (voxel.ts:90-107): (brick, bit, level) or brick ORC_EMPTY */
+static void vox_at(const orc_vox *vx, uint32_t L, i3 c, uint32_t out[3]) {
+  uint32_t l = L;
+  i3 cc = c;
+  int32_t n8 = (int32_t)vx->G * 8;
+  for (;;) {
+    uint32_t ptr = vx->ptr[ptr_index(vx, l, I(cc.x >> 3, cc.y >> 3, cc.z >> 3))];
+    if (ptr != ORC_DROP) {
+      if (ptr >= ORC_MARK) { out[0] = ORC_EMPTY; out[1] = 0; out[2] = l; return; }
+      uint32_t bit = (uint32_t)((cc.x & 7) + 8 * (cc.y & 7) + 64 * (cc.z & 7));
+      if ((vx->occ[ptr * 16u + (bit >> 5)] & (1u << (bit & 31u))) == 0u) { out[0] = ORC_EMPTY; out[1] = 0; out[2] = l; return; }
+      out[0] = ptr; out[1] = bit; out[2] = l;
+      return;
+    }
+    if (l + 1u >= vx->levels) { out[0] = ORC_EMPTY; out[1] = 0; out[2] = l; return; }
+    i3 o = org(vx, l);
+    i3 w = I((o.x * 8 + cc.x) >> 1, (o.y * 8 + cc.y) >> 1, (o.z * 8 + cc.z) >> 1);
+    l++;
+    i3 o1 = org(vx, l);
+    cc = I(w.x - o1.x * 8, w.y - o1.y * 8, w.z - o1.z * 8);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= n8 || cc.y >= n8 || cc.z >= n8) { out[0] = ORC_EMPTY; out[1] = 0; out[2] = l; return; }
+  }
+}
+/* voxInside / voxLevelFor (voxel.ts:108-119) */
+static int vox_inside(const orc_vox *vx, uint32_t L, v3 p) {
+  float bs = vox_size(vx, L) * 8.0f;
+  v3 lo = muls(vi2f(org(vx, L)), bs);
+  float ext = (float)vx->G * bs;
+  v3 hi = adds(lo, ext);
+  return p.x > lo.x && p.y > lo.y && p.z > lo.z && p.x < hi.x && p.y < hi.y && p.z < hi.z;
+}
+static uint32_t vox_level_for(const orc_vox *vx, uint32_t L, v3 e) {
+  uint32_t l = L;
+  while (l + 1u < vx->levels && !vox_inside(vx, l, e)) l++;
+  return l;
+}
+
+/* style.ts:18-25 */
+static v3 toon_albedo(v3 a) {
+  float l = dot(a, V(0.2126f, 0.7152f, 0.0722f));
+  v3 r = add(V(l, l, l), muls(sub(a, V(l, l, l)), 1.6f));
+  return V(fclampf(r.x, 0.0f, 1.0f), fclampf(r.y, 0.0f, 1.0f), fclampf(r.z, 0.0f, 1.0f));
+}
+static float toon_ramp(float x) { return x > 0.3f ? 1.0f : (x > 0.05f ? 0.5f : 0.0f); }
+
+/* shadeHitV (rc.ts:108-116) with e = 0 (no multi-bounce) */
+static v3 shade_hit_v(const float *F, v3 n0, const float alb[4], v3 d, v3 e, float vis) {
+  v3 n = dot(n0, n0) > 0.01f ? n0 : neg(d);
+  if (dot(n, d) > 0.0f) n = neg(n);
+  v3 a = V(alb[0], alb[1], alb[2]);
+  v3 b = mul(divs(a, PI_F), e);
+  float ndl = fmaxf_(dot(n, fromf(F + F_SUN)), 0.0f);
+  if (ndl <= 0.0f) return b;
+  v3 sunE = fromf(F + F_SUNE);
+  if (alb[3] > 0.5f && F[F_STYLE] > 0.5f) {
+    v3 ts = muls(mul(divs(toon_albedo(a), 3.14159265f), sunE), toon_ramp(ndl * vis));
+    return add(b, ts);
+  }
+  return add(b, muls(muls(mul(divs(a, PI_F), sunE), ndl), vis));
+}
+
+typedef struct { float r, g, b, T; uint32_t lvl, ptr, bit, tin; uint32_t steps; } trace_t;
+
+/* The hit: attributes of voxel (brick, bit), shaded (voxShade, rc.ts:136-140) plus the emissive radiance. */
+static void shade_voxel(const ctx_t *cx, uint32_t brick, uint32_t bit, v3 d, trace_t *out) {
+  const orc_vox *vx = cx->vx;
+  uint32_t w[4] = {0, 0, 0, 0};
+  float vis = 0.0f;
+  if (vx->base[brick] != ORC_EMPTY) {
+    uint32_t ai = vox_rank(vx, brick, bit);
+    for (int k = 0; k < 4; k++) w[k] = vx->attr[ai * 4u + k];
+    vis = vx->sunvis[ai];
+  }
+  float alb[4];
+  for (int k = 0; k < 4; k++) alb[k] = (float)((w[0] >> (8 * k)) & 0xffu) / 255.0f;
+  float nx = fmaxf_((float)(int16_t)(w[1] & 0xffffu) / 32767.0f, -1.0f);
+  float ny = fmaxf_((float)(int16_t)(w[1] >> 16) / 32767.0f, -1.0f);
+  v3 n = V(nx, ny, 1.0f - fabsf(nx) - fabsf(ny));
+  float q = fmaxf_(-n.z, 0.0f);
+  n.x += n.x >= 0.0f ? -q : q;
+  n.y += n.y >= 0.0f ? -q : q;
+  v3 r = shade_hit_v(cx->F, n, alb, d, V(0.0f, 0.0f, 0.0f), vis);
+  v3 em = V(orc_f16_to_f32((uint16_t)(w[2] & 0xffffu)), orc_f16_to_f32((uint16_t)(w[2] >> 16)), orc_f16_to_f32((uint16_t)(w[3] & 0xffffu)));
+  r = add(r, em);
+  out->r = r.x; out->g = r.y; out->b = r.z; out->T = 0.0f;
+}
+
+/* traceVox (voxel.ts:121-202) with a configurable step cap. */
+static void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tskip, uint32_t L, uint32_t cap, trace_t *out) {
+  const orc_vox *vx = cx->vx;
+  out->r = out->g = out->b = 0.0f; out->T = 1.0f; out->lvl = ORC_EMPTY; out->ptr = ORC_EMPTY; out->bit = 0; out->tin = 0;
+  out->steps = 0;
+  float v = vox_size(vx, L);
+  int32_t G = (int32_t)vx->G;
+  v3 lo = muls(muls(vi2f(org(vx, L)), v), 8.0f);
+  v3 hi = adds(lo, (float)G * v * 8.0f);
+  v3 dd = V(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
+  v3 inv = V(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+  v3 ta = mul(sub(lo, o), inv), tb = mul(sub(hi, o), inv);
+  v3 tn = vmin(ta, tb), tf = vmax(ta, tb);
+  float t = fmaxf_(fmaxf_(fmaxf_(tn.x, tn.y), tn.z), t0);
+  float tEnd = fminf_(fminf_(fminf_(tf.x, tf.y), tf.z), t1);
+  if (t >= tEnd) return;
+  i3 st = I(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
+  v3 sp = V(st.x > 0 ? 1.0f : 0.0f, st.y > 0 ? 1.0f : 0.0f, st.z > 0 ? 1.0f : 0.0f);
+  int32_t nVox = G * 8;
+  i3 c = iclamp3(vf2i(vfloor(divs(sub(add(o, muls(d, t)), lo), v))), I(0, 0, 0), I(nVox - 1, nVox - 1, nVox - 1));
+  v3 tMax = mul(sub(add(muls(add(vi2f(c), sp), v), lo), o), inv);
+  v3 tDelta = vabs(muls(inv, v));
+  float tIn = t;
+  for (uint32_t it = 0; it < cap; it++) {
+    out->steps++;
+    i3 b = I(c.x >> 3, c.y >> 3, c.z >> 3);
+    uint32_t ptr = vx->ptr[ptr_index(vx, L, b)];
+    if (ptr == ORC_DROP) {
+      uint32_t r[3];
+      vox_at(vx, L, c, r);
+      if (r[0] != ORC_EMPTY && tIn >= tskip) {
+        shade_voxel(cx, r[0], r[1], d, out);
+        out->lvl = r[2]; out->ptr = r[0]; out->bit = r[1]; out->tin = ubits(tIn);
+        return;
+      }
+      float tx = fminf_(fminf_(tMax.x, tMax.y), tMax.z);
+      if (tx >= tEnd) break;
+      tIn = tx;
+      if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
+      else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
+      else { c.z += st.z; tMax.z += tDelta.z; }
+      if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
+      continue;
+    }
+    if (ptr >= ORC_MARK) {
+      v3 bt = mul(sub(add(muls(add(vi2f(I(b.x * 8, b.y * 8, b.z * 8)), muls(sp, 8.0f)), v), lo), o), inv);
+      float te = fminf_(fminf_(bt.x, bt.y), bt.z);
+      if (te >= tEnd) break;
+      i3 nb = b;
+      if (bt.x <= bt.y && bt.x <= bt.z) nb.x += st.x; else if (bt.y <= bt.z) nb.y += st.y; else nb.z += st.z;
+      if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) break;
+      t = te; tIn = te;
+      c = iclamp3(vf2i(vfloor(divs(sub(add(o, muls(d, t)), lo), v))), I(nb.x * 8, nb.y * 8, nb.z * 8),
+                  I(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
+      tMax = mul(sub(add(muls(add(vi2f(c), sp), v), lo), o), inv);
+      continue;
+    }
+    uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
+    uint32_t occ = vx->occ[ptr * 16u + (bit >> 5)];
+    float tExit = fminf_(fminf_(tMax.x, tMax.y), tMax.z);
+    if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
+      shade_voxel(cx, ptr, bit, d, out);
+      out->lvl = L; out->ptr = ptr; out->bit = bit; out->tin = ubits(tIn);
+      return;
+    }
+    if (tExit >= tEnd) break;
+    tIn = tExit;
+    if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
+    else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
+    else { c.z += st.z; tMax.z += tDelta.z; }
+    if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
+  }
+}
+
+/* voxLevel (rc.ts:210-213): round(log2(v / v0)) taken exactly, clamped to the levels. */
+static uint32_t vox_level(const orc_vox *vx, const orc_layout *ly, float s0, uint32_t c) {
+  float v = ly->vox_scale * s0 * exp2_(ly->level_map * (float)c);
+  int32_t r = (int32_t)orc_round_log2(v / vx->v0);
+  int32_t top = (int32_t)vx->levels - 1;
+  return (uint32_t)(r < 0 ? 0 : (r > top ? top : r));
+}
+
+typedef struct {
+  const ctx_t *cx; const orc_layout *ly; orc_rc_out *o; uint32_t c;
+  uint32_t n_traces, n_steps, n_cap;
+} trace_job;
+
+static void trace_range(void *p, uint64_t b, uint64_t e) {
+  trace_job *j = (trace_job *)p;
+  const orc_vox *vx = j->cx->vx;
+  const orc_layout *ly = j->ly;
+  orc_rc_out *o = j->o;
+  const orc_casc *L = &ly->c[j->c];
+  uint32_t dirs = L->res * L->res;
+  uint32_t n_traces = 0, n_steps = 0, n_cap = 0;
+  for (uint32_t t = (uint32_t)b; t < (uint32_t)e; t++) {
+    uint32_t pi = t / dirs, di = t % dirs;
+    const orc_probe *pr = &o->probes[L->probe_off + pi];
+    trace_t tr;
+    memset(&tr, 0, sizeof tr);
+    tr.T = 1.0f; tr.lvl = ORC_EMPTY; tr.ptr = ORC_EMPTY;
+    if (pr->pos[3] > 0.0f) {
+      v3 dir = dir_of(di, L->res);
+      float s0 = pr->pos[3];
+      float t0 = L->b0 * s0, t1 = L->b1 * s0;
+      v3 po = V(pr->pos[0], pr->pos[1], pr->pos[2]);
+      v3 pn = V(pr->nrm[0], pr->nrm[1], pr->nrm[2]);
+      uint32_t Lv = vox_level_for(vx, vox_level(vx, ly, s0, j->c), add(po, muls(dir, t1)));
+      float v = vox_size(vx, Lv);
+      trace_vox(j->cx, add(po, muls(pn, ly->vox_offset * v)), dir, t0, t1, ly->vox_skip * v, Lv, ly->dda_cap, &tr);
+      n_traces += 1;
+      n_steps += tr.steps;
+      n_cap += tr.steps >= ly->dda_cap ? 1u : 0u;
+    }
+    float *r = o->rad + 4u * ((size_t)L->rad_off + t);
+    r[0] = round_store(tr.r, ly->atlas); r[1] = round_store(tr.g, ly->atlas);
+    r[2] = round_store(tr.b, ly->atlas); r[3] = round_store(tr.T, ly->atlas);
+    if (o->hit) {
+      uint32_t *h = o->hit + 4u * ((size_t)L->rad_off + t);
+      h[0] = tr.lvl; h[1] = tr.ptr; h[2] = tr.bit; h[3] = tr.tin;
+    }
+  }
+  __atomic_fetch_add(&j->n_traces, n_traces, __ATOMIC_RELAXED);
+  __atomic_fetch_add(&j->n_steps, n_steps, __ATOMIC_RELAXED);
+  __atomic_fetch_add(&j->n_cap, n_cap, __ATOMIC_RELAXED);
+}
+
+int orc_rc_trace(const orc_vox *vx, const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o) {
+  ctx_t cx = {vx, g->frame, {g->frame[F_SKY], g->frame[F_SKY + 1], g->frame[F_SKY + 2]}};
+  const float *F = g->frame;
+  int32_t W = (int32_t)g->width, H = (int32_t)g->height;
+  memset(o->counts, 0, 80 * 4);
+  /* setupScreen (rc.ts:572-590) */
+  for (uint32_t c = 0; c < ly->cascades; c++) {
+    const orc_casc *L = &ly->c[c];
+    uint32_t n = L->tiles_x * L->tiles_y;
+    o->counts[c] = n;
+    for (uint32_t t = 0; t < n; t++) {
+      uint32_t tx = t % L->tiles_x, ty = t / L->tiles_x;
+      int32_t px = imin((int32_t)(tx * L->tile_size + L->tile_size / 2u), W - 1);
+      int32_t py = imin((int32_t)(ty * L->tile_size + L->tile_size / 2u), H - 1);
+      float d = g->depth[(size_t)py * (size_t)W + (size_t)px];
+      orc_probe pr;
+      memset(&pr, 0, sizeof pr);
+      pr.grid[0] = (int32_t)tx; pr.grid[1] = (int32_t)ty;
+      if (d > 0.0f) {
+        v3 x = world_at(F, px, py, d);
+        const float *nn = g->normal + 4u * ((size_t)py * (size_t)W + (size_t)px);
+        v3 nrm = V(nn[0], nn[1], nn[2]);
+        float s0 = length3(sub(x, fromf(F + F_EYE))) * F[F_RC + 1] * F[F_RC + 2];
+        float e2 = exp2_((float)c);
+        v3 p = add(x, muls(muls(muls(nrm, F[F_RC2]), s0), e2));
+        pr.pos[0] = p.x; pr.pos[1] = p.y; pr.pos[2] = p.z; pr.pos[3] = s0;
+        pr.nrm[0] = nrm.x; pr.nrm[1] = nrm.y; pr.nrm[2] = nrm.z; pr.nrm[3] = view_z(F, x);
+      }
+      o->probes[L->probe_off + t] = pr;
+    }
+  }
+  /* trace (rc.ts:600-622) -> traceWorld (:216-245) -> traceVox */
+  for (uint32_t c = 0; c < ly->cascades; c++) {
+    const orc_casc *L = &ly->c[c];
+    uint32_t dirs = L->res * L->res, np = L->tiles_x * L->tiles_y;
+    trace_job j = {&cx, ly, o, c, 0, 0, 0};
+    orc_parallel((uint64_t)np * dirs, 512, trace_range, &j);
+    if (ly->stats > 0) { o->counts[24 + c] = j.n_traces; o->counts[32 + c] = j.n_steps; o->counts[64 + c] = j.n_cap; }
+  }
+  return 0;
+}
+
+/* upperAvg (rc.ts:681-686) */
+static v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_t q, uint32_t u, uint32_t v, uint32_t lr) {
+  const orc_casc *U = &ly->c[cu];
+  if (U->res == lr) {
+    const float *p = rad + 4u * ((size_t)U->rad_off + q * U->res * U->res + v * U->res + u);
+    return V(p[0], p[1], p[2]);
+  }
+  size_t base = (size_t)U->rad_off + q * U->res * U->res + v * 2u * U->res + u * 2u;
+  const float *a = rad + 4u * base, *b = rad + 4u * (base + 1u), *c = rad + 4u * (base + U->res), *d = rad + 4u * (base + U->res + 1u);
+  return muls(add(add(add(V(a[0], a[1], a[2]), V(b[0], b[1], b[2])), V(c[0], c[1], c[2])), V(d[0], d[1], d[2])), 0.25f);
+}
+
+static void sh_basis(v3 n, float y[9]) {
+  y[0] = 0.282095f; y[1] = 0.488603f * n.y; y[2] = 0.488603f * n.z; y[3] = 0.488603f * n.x;
+  y[4] = 1.092548f * n.x * n.y; y[5] = 1.092548f * n.y * n.z; y[6] = 0.315392f * (3.0f * n.z * n.z - 1.0f);
+  y[7] = 1.092548f * n.x * n.z; y[8] = 0.546274f * (n.x * n.x - n.y * n.y);
+}
+
+typedef struct { const orc_layout *ly; const orc_gbuf *g; orc_rc_out *o; uint32_t c; } mg_job;
+
+/* mergeScreen (rc.ts:710-743), cascade j->c, in place */
+static void merge_range(void *p, uint64_t b, uint64_t e) {
+  mg_job *j = (mg_job *)p;
+  const orc_layout *ly = j->ly;
+  orc_rc_out *o = j->o;
+  const float *F = j->g->frame;
+  uint32_t c = j->c, N = ly->cascades;
+  const orc_casc *L = &ly->c[c];
+  uint32_t dirs = L->res * L->res;
+  v3 sky = fromf(F + F_SKY);
+  for (uint32_t t = (uint32_t)b; t < (uint32_t)e; t++) {
+    uint32_t pi = t / dirs, di = t % dirs;
+    float *rv = o->rad + 4u * ((size_t)L->rad_off + t);
+    v3 up = sky;
+    if (c + 1u < N && rv[3] > 0.0f) {
+      up = V(0.0f, 0.0f, 0.0f);
+      const orc_probe *pr = &o->probes[L->probe_off + pi];
+      if (pr->pos[3] > 0.0f) {
+        const orc_casc *U = &ly->c[c + 1u];
+        float cx = ((float)(pi % L->tiles_x) + 0.5f) * (float)L->tile_size;
+        float cy = ((float)(pi / L->tiles_x) + 0.5f) * (float)L->tile_size;
+        float ux = cx / (float)U->tile_size - 0.5f, uy = cy / (float)U->tile_size - 0.5f;
+        int32_t bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+        float fx = ux - (float)bx, fy = uy - (float)by;
+        uint32_t u0 = di % L->res, v0 = di / L->res;
+        v3 acc = V(0.0f, 0.0f, 0.0f);
+        float ws = 0.0f;
+        for (uint32_t k = 0; k < 4; k++) {
+          int32_t ox = (int32_t)(k & 1u), oy = (int32_t)(k >> 1);
+          int32_t qx = iclamp(bx + ox, 0, (int32_t)U->tiles_x - 1), qy = iclamp(by + oy, 0, (int32_t)U->tiles_y - 1);
+          uint32_t qi = (uint32_t)qy * U->tiles_x + (uint32_t)qx;
+          const orc_probe *qp = &o->probes[U->probe_off + qi];
+          if (qp->pos[3] <= 0.0f) continue;
+          float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
+          float rel = fabsf(qp->nrm[3] - pr->nrm[3]) / pr->nrm[3];
+          float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f);
+          acc = add(acc, muls(upper_avg(ly, o->rad, c + 1u, qi, u0, v0, L->res), w));
+          ws += w;
+        }
+        if (ws > 0.0f) up = divs(acc, ws);
+      }
+    }
+    v3 m = add(V(rv[0], rv[1], rv[2]), muls(up, rv[3]));
+    rv[0] = round_store(m.x, ly->atlas); rv[1] = round_store(m.y, ly->atlas); rv[2] = round_store(m.z, ly->atlas);
+    rv[3] = round_store(1.0f, ly->atlas);
+  }
+}
+
+/* projectSH (rc.ts:752-774) */
+static void sh_range(void *p, uint64_t b, uint64_t e) {
+  mg_job *j = (mg_job *)p;
+  const orc_layout *ly = j->ly;
+  orc_rc_out *o = j->o;
+  const float *F = j->g->frame;
+  const orc_casc *L0 = &ly->c[0];
+  float a_k[3] = {PI_F, 2.0f * PI_F / 3.0f, PI_F / 4.0f};
+  for (uint32_t pi = (uint32_t)b; pi < (uint32_t)e; pi++) {
+    v3 cf[9];
+    for (int k = 0; k < 9; k++) cf[k] = V(0.0f, 0.0f, 0.0f);
+    for (uint32_t d = 0; d < 16; d++) {
+      const float *rp = o->rad + 4u * ((size_t)L0->rad_off + pi * 16u + d);
+      v3 r = muls(V(rp[0], rp[1], rp[2]), F[F_OMEGA + d]);
+      float y[9];
+      sh_basis(dir_of(d, 4u), y);
+      for (int k = 0; k < 9; k++) cf[k] = add(cf[k], muls(r, y[k]));
+    }
+    float *sh = o->sh + 32u * pi;
+    for (int k = 0; k < 32; k++) sh[k] = 0.0f;
+    for (int k = 0; k < 9; k++) {
+      float a = k == 0 ? a_k[0] : (k < 4 ? a_k[1] : a_k[2]);
+      sh[k * 3 + 0] = round_store(cf[k].x * a, ly->atlas);
+      sh[k * 3 + 1] = round_store(cf[k].y * a, ly->atlas);
+      sh[k * 3 + 2] = round_store(cf[k].z * a, ly->atlas);
+    }
+  }
+}
+
+/* gatherScreen (rc.ts:929-954), rows [b, e) */
+static void gather_range(void *p, uint64_t b, uint64_t e) {
+  mg_job *j = (mg_job *)p;
+  const orc_layout *ly = j->ly;
+  const orc_gbuf *g = j->g;
+  orc_rc_out *o = j->o;
+  const float *F = g->frame;
+  const orc_casc *L0 = &ly->c[0];
+  int32_t W = (int32_t)g->width;
+  uint32_t out_fmt = ly->atlas == 0 ? 0u : 1u;
+  for (int32_t py = (int32_t)b; py < (int32_t)e; py++)
+    for (int32_t px = 0; px < W; px++) {
+      size_t q = (size_t)py * (size_t)W + (size_t)px;
+      float *out = o->irr + 4u * q;
+      float d = g->depth[q];
+      if (!(d > 0.0f)) { out[0] = out[1] = out[2] = out[3] = 0.0f; continue; }
+      v3 x = world_at(F, px, py, d);
+      v3 n = V(g->normal[4 * q], g->normal[4 * q + 1], g->normal[4 * q + 2]);
+      float z = view_z(F, x);
+      float ux = ((float)px + 0.5f) / (float)L0->tile_size - 0.5f, uy = ((float)py + 0.5f) / (float)L0->tile_size - 0.5f;
+      int32_t bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+      float fx = ux - (float)bx, fy = uy - (float)by;
+      v3 acc = V(0.0f, 0.0f, 0.0f);
+      float ws = 0.0f;
+      float y[9];
+      sh_basis(n, y);
+      for (uint32_t k = 0; k < 4; k++) {
+        int32_t ox = (int32_t)(k & 1u), oy = (int32_t)(k >> 1);
+        int32_t qx = iclamp(bx + ox, 0, (int32_t)L0->tiles_x - 1), qy = iclamp(by + oy, 0, (int32_t)L0->tiles_y - 1);
+        uint32_t qi = (uint32_t)qy * L0->tiles_x + (uint32_t)qx;
+        const orc_probe *pr = &o->probes[L0->probe_off + qi];
+        if (pr->pos[3] <= 0.0f) continue;
+        float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
+        float rel = fabsf(pr->nrm[3] - z) / z;
+        float nd = fmaxf_(dot(n, V(pr->nrm[0], pr->nrm[1], pr->nrm[2])), 0.0f);
+        float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
+        /* evalSH (rc.ts:819-829) */
+        const float *sh = o->sh + 32u * qi;
+        v3 es = V(0.0f, 0.0f, 0.0f);
+        for (int k2 = 0; k2 < 9; k2++) es = add(es, muls(V(sh[3 * k2], sh[3 * k2 + 1], sh[3 * k2 + 2]), y[k2]));
+        es = vmax(es, V(0.0f, 0.0f, 0.0f));
+        acc = add(acc, muls(es, w));
+        ws += w;
+      }
+      v3 r = ws > 0.0f ? divs(acc, ws) : V(0.0f, 0.0f, 0.0f);
+      out[0] = out_fmt ? round_store(r.x, 1) : r.x;
+      out[1] = out_fmt ? round_store(r.y, 1) : r.y;
+      out[2] = out_fmt ? round_store(r.z, 1) : r.z;
+      out[3] = 1.0f;
+    }
+}
+
+int orc_rc_merge_gather(const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o) {
+  mg_job j = {ly, g, o, 0};
+  for (int32_t ci = (int32_t)ly->cascades - 1; ci >= 0; ci--) {
+    j.c = (uint32_t)ci;
+    const orc_casc *L = &ly->c[j.c];
+    orc_parallel((uint64_t)L->tiles_x * L->tiles_y * L->res * L->res, 4096, merge_range, &j);
+  }
+  orc_parallel((uint64_t)ly->c[0].tiles_x * ly->c[0].tiles_y, 256, sh_range, &j);
+  orc_parallel(g->height, 4, gather_range, &j);
+  return 0;
+}

@@ -1,0 +1,353 @@
+/* Sequential restatement of the voxel clipmap rebuild (src/core/voxel.ts:205-620).  Test infrastructure only.
+ *
+ * The GPU build is a set of passes whose results do not depend on scheduling (bits are ORed, representatives are the
+ * maximum triangle index + 1); this file runs the same passes one after another.  Two allocations depend on the
+ * order of an atomic counter in the reference (bricks when the pool holds them all, voxel attribute bases); both
+ * are restated here in the fixed order the reference uses when the brick pool overflows (coarse levels first, then
+ * pointer index; attribute bases in brick order), which is one of the orders the reference can produce and the one
+ * the CUDA path uses. */
+#include <stdlib.h>
+#include "gi_oracle.h"
+#include "orc_math.h"
+
+#define BIG 8u
+
+typedef struct { v3 a, b, c; const uint32_t *idx; } tri_t;
+typedef struct { i3 lo, n; } range_t;
+
+static inline float vox_size(const orc_vox *vx, uint32_t L) { return scale2(vx->v0, (int)L); }
+static inline uint32_t ptr_index(const orc_vox *vx, uint32_t L, i3 b) {
+  uint32_t G = vx->G;
+  return L * G * G * G + ((uint32_t)b.z * G + (uint32_t)b.y) * G + (uint32_t)b.x;
+}
+static inline i3 org(const orc_vox *vx, uint32_t L) { return I(vx->origin[L][0], vx->origin[L][1], vx->origin[L][2]); }
+/* regionLo (voxel.ts:289): vec3f(origin) * voxSize(L) * 8 */
+static inline v3 region_lo(const orc_vox *vx, uint32_t L) { return muls(muls(vi2f(org(vx, L)), vox_size(vx, L)), 8.0f); }
+static inline i3 ishr(i3 a, int s) { return I(a.x >> s, a.y >> s, a.z >> s); }
+
+static tri_t load_tri(const orc_scene *s, uint32_t t) {
+  tri_t T;
+  const uint32_t *i = s->tri + 4u * t;
+  T.a = fromf(s->pos + 3u * i[0]); T.b = fromf(s->pos + 3u * i[1]); T.c = fromf(s->pos + 3u * i[2]);
+  T.idx = i;
+  return T;
+}
+
+/* voxRange (voxel.ts:293-300) */
+static range_t vox_range(const orc_vox *vx, const tri_t *T, uint32_t L, float cell) {
+  v3 lo = region_lo(vx, L);
+  v3 mn = vmin(vmin(T->a, T->b), T->c), mx = vmax(vmax(T->a, T->b), T->c);
+  int32_t lim = f2i((float)vx->G * vox_size(vx, L) * 8.0f / cell);
+  i3 a = vf2i(vfloor(divs(sub(mn, lo), cell)));
+  i3 b = vf2i(vfloor(divs(sub(mx, lo), cell)));
+  a = iclamp3(a, I(0, 0, 0), I(lim, lim, lim));
+  b = iclamp3(I(b.x + 1, b.y + 1, b.z + 1), I(0, 0, 0), I(lim, lim, lim));
+  range_t r;
+  r.lo = a;
+  r.n = I(imax(b.x - a.x, 0), imax(b.y - a.y, 0), imax(b.z - a.z, 0));
+  return r;
+}
+
+/* finerHolds / finerHoldsRange / finerBuilt / finerBuiltRange (voxel.ts:303-320) */
+static int finer_holds(const orc_vox *vx, uint32_t L, i3 c) {
+  if (L == 0) return 0;
+  i3 o = org(vx, L), of = org(vx, L - 1);
+  int32_t n = (int32_t)vx->G * 8;
+  i3 f = I((o.x * 8 + c.x) * 2 - of.x * 8, (o.y * 8 + c.y) * 2 - of.y * 8, (o.z * 8 + c.z) * 2 - of.z * 8);
+  return f.x >= 0 && f.y >= 0 && f.z >= 0 && f.x < n && f.y < n && f.z < n;
+}
+static int finer_holds_range(const orc_vox *vx, uint32_t L, range_t r, int32_t s) {
+  return finer_holds(vx, L, I(r.lo.x * s, r.lo.y * s, r.lo.z * s))
+      && finer_holds(vx, L, I((r.lo.x + r.n.x) * s - 1, (r.lo.y + r.n.y) * s - 1, (r.lo.z + r.n.z) * s - 1));
+}
+static int finer_built(const orc_vox *vx, uint32_t L, i3 c) {
+  if (!finer_holds(vx, L, c)) return 0;
+  if (vx->hdr[2] == 0) return 1;
+  i3 o = org(vx, L), of = org(vx, L - 1);
+  i3 f = I((o.x * 8 + c.x) * 2 - of.x * 8, (o.y * 8 + c.y) * 2 - of.y * 8, (o.z * 8 + c.z) * 2 - of.z * 8);
+  return vx->ptr[ptr_index(vx, L - 1, ishr(f, 3))] != ORC_DROP;
+}
+static int finer_built_range(const orc_vox *vx, uint32_t L, range_t r) {
+  return vx->hdr[2] == 0 && finer_holds_range(vx, L, r, 1);
+}
+
+static int tri_box_v(v3 c, v3 h, const tri_t *T) {
+  float cf[3] = {c.x, c.y, c.z}, hf[3] = {h.x, h.y, h.z};
+  float af[3] = {T->a.x, T->a.y, T->a.z}, bf[3] = {T->b.x, T->b.y, T->b.z}, cc[3] = {T->c.x, T->c.y, T->c.z};
+  return orc_tri_box(cf, hf, af, bf, cc);
+}
+
+/* closestBary (voxel.ts:250-267), Ericson 5.1.5 */
+static v3 closest_bary(v3 p, v3 a, v3 b, v3 c) {
+  v3 ab = sub(b, a), ac = sub(c, a), ap = sub(p, a);
+  float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) return V(1.0f, 0.0f, 0.0f);
+  v3 bp = sub(p, b);
+  float d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) return V(0.0f, 1.0f, 0.0f);
+  float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) { float w = d1 / (d1 - d3); return V(1.0f - w, w, 0.0f); }
+  v3 cp = sub(p, c);
+  float d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) return V(0.0f, 0.0f, 1.0f);
+  float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) { float w = d2 / (d2 - d6); return V(1.0f - w, 0.0f, w); }
+  float va = d3 * d6 - d5 * d4;
+  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    return V(0.0f, 1.0f - w, w);
+  }
+  float dn = 1.0f / (va + vb + vc);
+  float v = vb * dn, w = vc * dn;
+  return V(1.0f - v - w, v, w);
+}
+
+typedef struct { int ok; float albedo[3]; v3 n; float toon; v3 q; } surf_t;
+/* surfaceAt (voxel.ts:325-336) for untextured materials: the base colour texture's default layer is white, so the
+ * sampled colour is the material's baseColorFactor exactly. */
+static surf_t surface_at(const orc_scene *s, const tri_t *T, v3 p, int want_attr) {
+  surf_t r;
+  memset(&r, 0, sizeof r);
+  const orc_material *m = &s->mats[T->idx[3]];
+  int masked = (m->flags & 1u) != 0 && !want_attr;
+  r.q = p;
+  if (!masked && !want_attr) { r.ok = 1; return r; }
+  v3 w = closest_bary(p, T->a, T->b, T->c);
+  if (masked && m->base_color[3] < m->alpha_cutoff) { r.ok = 0; return r; }
+  v3 n0 = fromf(s->nrm + 3u * T->idx[0]), n1 = fromf(s->nrm + 3u * T->idx[1]), n2 = fromf(s->nrm + 3u * T->idx[2]);
+  v3 n = add(add(muls(n0, w.x), muls(n1, w.y)), muls(n2, w.z));
+  if (!(dot(n, n) > 1e-12f)) n = cross(sub(T->b, T->a), sub(T->c, T->a));
+  r.ok = 1;
+  r.albedo[0] = m->base_color[0]; r.albedo[1] = m->base_color[1]; r.albedo[2] = m->base_color[2];
+  r.n = normalize3(n);
+  r.toon = (m->flags & 4u) ? 1.0f : 0.0f;
+  r.q = add(add(muls(T->a, w.x), muls(T->b, w.y)), muls(T->c, w.z));
+  return r;
+}
+
+static void mark_brick(orc_vox *vx, uint32_t i) { if (vx->ptr[i] == ORC_EMPTY) vx->ptr[i] = ORC_MARK; }
+
+/* markRange (voxel.ts:348-358), all of the range's bricks */
+static void mark_range(orc_vox *vx, const tri_t *T, uint32_t L, range_t r) {
+  float bs = vox_size(vx, L) * 8.0f;
+  v3 lo = region_lo(vx, L);
+  uint32_t n = (uint32_t)(r.n.x * r.n.y * r.n.z);
+  for (uint32_t j = 0; j < n; j++) {
+    int32_t q = (int32_t)j;
+    i3 b = I(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y));
+    if (!vx->coarse_from_triangles && finer_holds(vx, L, I(b.x * 8, b.y * 8, b.z * 8))
+        && finer_holds(vx, L, I(b.x * 8 + 7, b.y * 8 + 7, b.z * 8 + 7))) continue;
+    v3 c = add(lo, muls(adds(vi2f(b), 0.5f), bs));
+    float hh = 0.5f * bs * 1.0001f;
+    if (n == 1u || tri_box_v(c, V(hh, hh, hh), T)) mark_brick(vx, ptr_index(vx, L, b));
+  }
+}
+
+/* voxelizeOne (voxel.ts:476-490) */
+static void voxelize_one(const orc_scene *s, orc_vox *vx, const tri_t *T, uint32_t t, uint32_t L, i3 c, int single) {
+  if (!vx->coarse_from_triangles && finer_built(vx, L, c)) return;
+  float v = vox_size(vx, L);
+  v3 p = add(region_lo(vx, L), muls(adds(vi2f(c), 0.5f), v));
+  float hh = 0.5f * v * 1.0001f;
+  if (!single && !tri_box_v(p, V(hh, hh, hh), T)) return;
+  uint32_t ptr = vx->ptr[ptr_index(vx, L, ishr(c, 3))];
+  if (ptr >= ORC_MARK) return;
+  i3 l = I(c.x & 7, c.y & 7, c.z & 7);
+  uint32_t bit = (uint32_t)(l.x + 8 * l.y + 64 * l.z);
+  if (!surface_at(s, T, p, 0).ok) return;
+  vx->occ[ptr * 16u + (bit >> 5)] |= 1u << (bit & 31u);
+  uint32_t *rp = &vx->rep[ptr * 512u + bit];
+  if (*rp < t + 1u) *rp = t + 1u;
+}
+
+void orc_vox_origins(float v0, uint32_t levels, uint32_t G, const double eye[3], int32_t origin_out[8][4]) {
+  for (uint32_t L = 0; L < 8; L++) for (int a = 0; a < 4; a++) origin_out[L][a] = 0;
+  for (uint32_t L = 0; L < levels; L++) {
+    double bs = (double)v0 * ldexp(1.0, (int)L) * 8.0;   /* v0 * 2 ** L * 8 in the host's f64 */
+    for (int a = 0; a < 3; a++) origin_out[L][a] = (int32_t)floor(eye[a] / bs) - (int32_t)(G / 2);
+  }
+}
+
+int orc_vox_build(const orc_scene *s, orc_vox *vx) {
+  const uint32_t NL = vx->levels, G = vx->G, per = G * G * G, cap = vx->big_cap;
+  /* clear (voxel.ts:338) */
+  memset(vx->hdr, 0, ORC_HDR * 4);
+  for (uint32_t i = 0; i < NL * per; i++) vx->ptr[i] = ORC_EMPTY;
+
+  /* markBricks + markBricksBig (voxel.ts:359-387) */
+  for (uint32_t t = 0; t < s->ntris; t++) {
+    tri_t T = load_tri(s, t);
+    for (uint32_t L = 0; L < NL; L++) {
+      range_t r = vox_range(vx, &T, L, vox_size(vx, L) * 8.0f);
+      int32_t n = r.n.x * r.n.y * r.n.z;
+      if (n == 0 || (!vx->coarse_from_triangles && finer_holds_range(vx, L, r, 8))) continue;
+      if (n > 8) {
+        uint32_t k = vx->hdr[24 + L]++;
+        if (k < cap) vx->big[(8u + L) * cap + k] = t; else vx->hdr[3]++;
+        continue;
+      }
+      mark_range(vx, &T, L, r);
+    }
+  }
+  for (uint32_t L = 0; L < NL; L++) {
+    uint32_t n = vx->hdr[24 + L] < cap ? vx->hdr[24 + L] : cap;
+    for (uint32_t k = 0; k < n; k++) {
+      tri_t T = load_tri(s, vx->big[(8u + L) * cap + k]);
+      mark_range(vx, &T, L, vox_range(vx, &T, L, vox_size(vx, L) * 8.0f));
+    }
+  }
+  /* markParents (voxel.ts:390-403) */
+  for (uint32_t i = 0; i < (NL - 1) * per; i++) {
+    if (vx->ptr[i] != ORC_MARK) continue;
+    uint32_t L = i / per, r = i % per;
+    i3 o = org(vx, L);
+    i3 w = I(o.x + (int32_t)(r % G), o.y + (int32_t)((r / G) % G), o.z + (int32_t)(r / (G * G)));
+    for (L++; L < NL; L++) {
+      w = ishr(w, 1);
+      i3 ol = org(vx, L);
+      i3 b = I(w.x - ol.x, w.y - ol.y, w.z - ol.z);
+      if (b.x < 0 || b.y < 0 || b.z < 0 || b.x >= (int32_t)G || b.y >= (int32_t)G || b.z >= (int32_t)G) break;
+      mark_brick(vx, ptr_index(vx, L, b));
+    }
+  }
+  /* countMarks / scanMarks / allocBricks (voxel.ts:411-470), in the ordered form: coarse levels first, then pointer
+   * index; a brick past the pool is dropped. */
+  uint32_t marked = 0;
+  for (uint32_t i = 0; i < NL * per; i++) marked += vx->ptr[i] == ORC_MARK;
+  vx->hdr[5] = marked;
+  vx->hdr[0] = marked;
+  uint32_t idx = 0;
+  for (uint32_t o = 0; o < NL * per; o++) {
+    uint32_t L = NL - 1u - o / per, i = L * per + o % per;
+    if (vx->ptr[i] != ORC_MARK) continue;
+    uint32_t k = idx++;
+    if (k >= vx->max_bricks) { vx->ptr[i] = ORC_DROP; vx->hdr[2]++; continue; }
+    vx->hdr[8 + L]++;
+    vx->ptr[i] = k;
+    for (uint32_t w = 0; w < 16; w++) vx->occ[k * 16u + w] = 0;
+    vx->base[k] = 0;
+    uint32_t r = i % per;
+    vx->code[k] = (L << 27) | ((r % G) << 18) | (((r / G) % G) << 9) | (r / (G * G));
+  }
+  uint32_t nb = marked < vx->max_bricks ? marked : vx->max_bricks;
+  /* clearKeys */
+  memset(vx->rep, 0, (size_t)nb * 512u * 4u);
+
+  /* voxBits + voxBitsBig (voxel.ts:492-534) */
+  for (uint32_t t = 0; t < s->ntris; t++) {
+    tri_t T = load_tri(s, t);
+    for (uint32_t L = 0; L < NL; L++) {
+      range_t r = vox_range(vx, &T, L, vox_size(vx, L));
+      int32_t n = r.n.x * r.n.y * r.n.z;
+      if (n == 0 || (!vx->coarse_from_triangles && finer_built_range(vx, L, r))) continue;
+      if ((uint32_t)n > BIG) {
+        uint32_t k = vx->hdr[16 + L]++;
+        if (k < cap) vx->big[L * cap + k] = t; else vx->hdr[3]++;
+        continue;
+      }
+      for (int32_t k = 0; k < n; k++)
+        voxelize_one(s, vx, &T, t, L, I(r.lo.x + k % r.n.x, r.lo.y + (k / r.n.x) % r.n.y, r.lo.z + k / (r.n.x * r.n.y)), n == 1);
+    }
+  }
+  for (uint32_t L = 0; L < NL; L++) {
+    uint32_t nbig = vx->hdr[16 + L] < cap ? vx->hdr[16 + L] : cap;
+    for (uint32_t k = 0; k < nbig; k++) {
+      uint32_t t = vx->big[L * cap + k];
+      tri_t T = load_tri(s, t);
+      range_t r = vox_range(vx, &T, L, vox_size(vx, L));
+      int32_t n = r.n.x * r.n.y * r.n.z;
+      for (int32_t q = 0; q < n; q++)
+        voxelize_one(s, vx, &T, t, L, I(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y)), 0);
+    }
+  }
+
+  /* reduce, levels 1 .. NL-1 (voxel.ts:540-577) */
+  if (!vx->coarse_from_triangles) {
+    for (uint32_t L = 1; L < NL; L++) {
+      for (uint32_t ptr = 0; ptr < nb; ptr++) {
+        uint32_t code = vx->code[ptr];
+        uint32_t Lc = code >> 27;
+        if (Lc + 1u != L) continue;
+        for (uint32_t w = 0; w < 16; w++) {
+          uint32_t word = vx->occ[ptr * 16u + w];
+          if (word == 0u) continue;
+          i3 b = I((int32_t)((code >> 18) & 511u), (int32_t)((code >> 9) & 511u), (int32_t)(code & 511u));
+          i3 c0 = I(b.x * 8, b.y * 8 + (int32_t)((w & 1u) * 4u), b.z * 8 + (int32_t)(w >> 1));
+          i3 oc = org(vx, Lc), ol = org(vx, L);
+          i3 pc0 = I(((oc.x * 8 + c0.x) >> 1) - ol.x * 8, ((oc.y * 8 + c0.y) >> 1) - ol.y * 8, ((oc.z * 8 + c0.z) >> 1) - ol.z * 8);
+          uint32_t pptr = vx->ptr[ptr_index(vx, L, ishr(pc0, 3))];
+          if (pptr >= ORC_MARK) continue;
+          i3 l0 = I(pc0.x & 7, pc0.y & 7, pc0.z & 7);
+          uint32_t pbit0 = (uint32_t)(l0.x + 8 * l0.y + 64 * l0.z);
+          uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+          while (word != 0u) {
+            uint32_t k = (uint32_t)__builtin_ctz(word);
+            word &= word - 1u;
+            uint32_t px = (k & 7u) >> 1, py = k >> 4;
+            mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
+            uint32_t rv = vx->rep[ptr * 512u + w * 32u + k];
+            if (py == 0u) { if (rv > lo[px]) lo[px] = rv; } else { if (rv > hi[px]) hi[px] = rv; }
+          }
+          vx->occ[pptr * 16u + (pbit0 >> 5)] |= mask;
+          for (uint32_t px = 0; px < 4; px++)
+            for (uint32_t py = 0; py < 2; py++) {
+              uint32_t rv = py == 0 ? lo[px] : hi[px];
+              if (rv == 0u) continue;
+              uint32_t *rp = &vx->rep[pptr * 512u + pbit0 + px + 8u * py];
+              if (*rp < rv) *rp = rv;
+            }
+        }
+      }
+    }
+  }
+
+  /* allocVoxels (voxel.ts:579-588), bases in brick order */
+  uint32_t total = 0;
+  for (uint32_t b = 0; b < nb; b++) {
+    uint32_t n = 0;
+    for (uint32_t w = 0; w < 16; w++) n += popc(vx->occ[b * 16u + w]);
+    uint32_t first = total;
+    total += n;
+    if (first + n > vx->max_voxels) { vx->base[b] = ORC_EMPTY; vx->hdr[4]++; continue; }
+    vx->base[b] = first;
+  }
+  vx->hdr[1] = total;
+
+  /* resolveAttr (voxel.ts:596-620) */
+  for (uint32_t ptr = 0; ptr < nb; ptr++) {
+    uint32_t first = vx->base[ptr];
+    if (first == ORC_EMPTY) continue;
+    uint32_t code = vx->code[ptr];
+    uint32_t L = code >> 27;
+    i3 b = I((int32_t)((code >> 18) & 511u), (int32_t)((code >> 9) & 511u), (int32_t)(code & 511u));
+    uint32_t r = 0;
+    for (uint32_t bit = 0; bit < 512u; bit++) {
+      uint32_t word = vx->occ[ptr * 16u + (bit >> 5)];
+      if ((word & (1u << (bit & 31u))) == 0u) continue;
+      uint32_t ai = first + r++;
+      i3 c = I(b.x * 8 + (int32_t)(bit & 7u), b.y * 8 + (int32_t)((bit >> 3) & 7u), b.z * 8 + (int32_t)(bit >> 6));
+      v3 p = add(region_lo(vx, L), muls(adds(vi2f(c), 0.5f), vox_size(vx, L)));
+      uint32_t t = vx->rep[ptr * 512u + bit] - 1u;
+      tri_t T = load_tri(s, t);
+      surf_t sf = surface_at(s, &T, p, 1);
+      float alb[4] = {sf.albedo[0], sf.albedo[1], sf.albedo[2], sf.toon};
+      /* octEnc (voxel.ts:590-594) */
+      v3 n = sf.n;
+      float sa = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
+      float px = n.x / sa, py = n.y / sa;
+      if (n.z < 0.0f) {
+        float ox = px, oy = py;
+        px = (1.0f - fabsf(oy)) * (ox >= 0.0f ? 1.0f : -1.0f);
+        py = (1.0f - fabsf(ox)) * (oy >= 0.0f ? 1.0f : -1.0f);
+      }
+      const orc_material *m = &s->mats[T.idx[3]];
+      vx->attr[ai * 4u + 0] = orc_pack4x8unorm(alb);
+      vx->attr[ai * 4u + 1] = orc_pack2x16snorm(px, py);
+      vx->attr[ai * 4u + 2] = (uint32_t)orc_f32_to_f16(m->emissive[0]) | ((uint32_t)orc_f32_to_f16(m->emissive[1]) << 16);
+      vx->attr[ai * 4u + 3] = (uint32_t)orc_f32_to_f16(m->emissive[2]);
+      vx->plane[ai] = dot(sf.n, sub(sf.q, p));
+      vx->sunvis[ai] = 1.0f;
+    }
+  }
+  return 0;
+}

@@ -1,0 +1,266 @@
+"""Scene data for the GI path (src/core/gltf.ts SceneData, src/core/scenes.ts Builder and leakRoom) and the seeded
+procedural scenes the benchmarks run on.
+
+A ``Scene`` holds what the voxel build and the G-buffer read: f32 positions and normals, the triangle table
+(absolute vertex indices + material, voxel.ts:730-739 triangleTable) in the reference's order (the triangles of
+material 0 first, as Builder.scene() emits one primitive per material), and the materials.  The reference's
+materials carry no emission; ``Material.emissive`` is this build's addition (radiance added at a voxel hit).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import List, Optional, Sequence
+
+import numpy as np
+
+from . import mathx
+from .frame import Camera
+
+MATERIAL_DTYPE = np.dtype([("base_color", "<f4", (4,)), ("flags", "<u4"), ("alpha_cutoff", "<f4"),
+                           ("emissive", "<f4", (3,)), ("reserved", "<u4", (3,))])
+assert MATERIAL_DTYPE.itemsize == 48
+
+FLAG_ALPHA_MASK, FLAG_DOUBLE_SIDED, FLAG_TOON, FLAG_OBJECT = 1, 2, 4, 8
+
+
+@dataclass
+class Material:
+    name: str
+    base_color: tuple = (0.7, 0.7, 0.7, 1.0)
+    flags: int = 0
+    alpha_cutoff: float = 0.5
+    emissive: tuple = (0.0, 0.0, 0.0)
+
+
+GREY = Material("grey", (0.7, 0.7, 0.7, 1.0))   # scenes.ts:173
+
+
+@dataclass
+class Scene:
+    name: str
+    positions: np.ndarray          # (V, 3) f32
+    normals: np.ndarray            # (V, 3) f32
+    tri: np.ndarray                # (T, 4) u32: i0, i1, i2, material
+    materials: List[Material]
+    camera: Camera
+    sun_dir: tuple = (0.0, 1.0, 0.0)
+    sun_e: tuple = (0.0, 0.0, 0.0)
+    sky: tuple = (0.0, 0.0, 0.0)
+
+    @property
+    def triangle_count(self) -> int:
+        return int(self.tri.shape[0])
+
+    def material_array(self) -> np.ndarray:
+        a = np.zeros(len(self.materials), dtype=MATERIAL_DTYPE)
+        for i, m in enumerate(self.materials):
+            a[i]["base_color"] = m.base_color
+            a[i]["flags"] = m.flags
+            a[i]["alpha_cutoff"] = m.alpha_cutoff
+            a[i]["emissive"] = m.emissive
+        return a
+
+
+class Builder:
+    """Builder (scenes.ts:176-211): quads of 4 new vertices with the face normal, boxes with outward faces."""
+
+    def __init__(self, materials: Optional[List[Material]] = None):
+        self.materials = list(materials) if materials else [GREY]
+        self.pos: List[float] = []
+        self.nrm: List[float] = []
+        self.idx: List[List[int]] = [[] for _ in self.materials]
+        self.mat = 0
+        self.offset = [0.0, 0.0, 0.0]
+        self._extra_pos: List[np.ndarray] = []
+
+    def quad(self, a, b, c, d):
+        e1 = [b[0] - a[0], b[1] - a[1], b[2] - a[2]]
+        e2 = [c[0] - a[0], c[1] - a[1], c[2] - a[2]]
+        n = mathx.normalize([e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]])
+        base = len(self.pos) // 3
+        for p in (a, b, c, d):
+            self.pos += [p[0] + self.offset[0], p[1] + self.offset[1], p[2] + self.offset[2]]
+            self.nrm += n
+        self.idx[self.mat] += [base, base + 1, base + 2, base, base + 2, base + 3]
+
+    def quad_facing(self, a, b, c, d, want):
+        """quad() with the corner order flipped when its face normal points away from ``want``."""
+        e1 = [b[i] - a[i] for i in range(3)]
+        e2 = [c[i] - a[i] for i in range(3)]
+        n = [e1[1] * e2[2] - e1[2] * e2[1], e1[2] * e2[0] - e1[0] * e2[2], e1[0] * e2[1] - e1[1] * e2[0]]
+        if n[0] * want[0] + n[1] * want[1] + n[2] * want[2] < 0:
+            a, b, c, d = a, d, c, b
+        self.quad(a, b, c, d)
+
+    def box(self, c, h):
+        x0, y0, z0 = c[0] - h[0], c[1] - h[1], c[2] - h[2]
+        x1, y1, z1 = c[0] + h[0], c[1] + h[1], c[2] + h[2]
+        self.quad([x0, y0, z1], [x1, y0, z1], [x1, y1, z1], [x0, y1, z1])
+        self.quad([x1, y0, z0], [x0, y0, z0], [x0, y1, z0], [x1, y1, z0])
+        self.quad([x0, y0, z0], [x0, y0, z1], [x0, y1, z1], [x0, y1, z0])
+        self.quad([x1, y0, z1], [x1, y0, z0], [x1, y1, z0], [x1, y1, z1])
+        self.quad([x0, y1, z1], [x1, y1, z1], [x1, y1, z0], [x0, y1, z0])
+        self.quad([x0, y0, z0], [x1, y0, z0], [x1, y0, z1], [x0, y0, z1])
+
+    def mesh(self, pos: np.ndarray, nrm: np.ndarray, tris: np.ndarray):
+        """Appends an indexed mesh (f64 positions/normals, local triangle indices) to the current material."""
+        base = len(self.pos) // 3
+        self.pos += (pos + np.asarray(self.offset)).reshape(-1).tolist()
+        self.nrm += nrm.reshape(-1).tolist()
+        self.idx[self.mat] += (tris.reshape(-1) + base).tolist()
+
+    def scene(self, name: str, camera: Camera, **kw) -> Scene:
+        positions = np.asarray(self.pos, dtype=np.float64).astype(np.float32).reshape(-1, 3)
+        normals = np.asarray(self.nrm, dtype=np.float64).astype(np.float32).reshape(-1, 3)
+        rows = []
+        for m, l in enumerate(self.idx):
+            if not l:
+                continue
+            a = np.asarray(l, dtype=np.uint32).reshape(-1, 3)
+            rows.append(np.concatenate([a, np.full((a.shape[0], 1), m, dtype=np.uint32)], axis=1))
+        tri = np.concatenate(rows, axis=0) if rows else np.zeros((0, 4), dtype=np.uint32)
+        return Scene(name, positions, normals, np.ascontiguousarray(tri), list(self.materials), camera, **kw)
+
+
+def leak_room(t: float) -> Scene:
+    """leakRoom (scenes.ts:261-278): a closed room on a floor of 24 x 24 cells, walls and roof t thick."""
+    b = Builder()
+    cells, size = 24, 8
+    step = size / cells
+    for z in range(cells):
+        for x in range(cells):
+            x0, z0 = -size / 2 + 1.5 + x * step, -size / 2 + z * step
+            b.quad([x0, 0, z0 + step], [x0 + step, 0, z0 + step], [x0 + step, 0, z0], [x0, 0, z0])
+    W, H, D = 3, 2.7, 2.25
+    b.box([-t / 2, H / 2, 0], [t / 2, H / 2, D + t])
+    b.box([W + t / 2, H / 2, 0], [t / 2, H / 2, D + t])
+    b.box([W / 2, H / 2, -D - t / 2], [W / 2, H / 2, t / 2])
+    b.box([W / 2, H / 2, D + t / 2], [W / 2, H / 2, t / 2])
+    b.box([W / 2, H + t / 2, 0], [W / 2 + t, t / 2, D + t])
+    return b.scene(f"leak-{t:g}", Camera((2.6, 1.6, 1.8), (0.2, 1.0, -1.4), 75, 0.05), sun_dir=(-1, 1.1, 0.35))
+
+
+class PCG32:
+    """PCG32 (O'Neill 2014, pcg32_srandom / pcg32_random): the seeded stream of the procedural scenes."""
+    MULT = 6364136223846793005
+    MASK = (1 << 64) - 1
+
+    def __init__(self, seed: int, stream: int = 54):
+        self.state = 0
+        self.inc = ((stream << 1) | 1) & self.MASK
+        self.next_u32()
+        self.state = (self.state + seed) & self.MASK
+        self.next_u32()
+
+    def next_u32(self) -> int:
+        old = self.state
+        self.state = (old * self.MULT + self.inc) & self.MASK
+        xs = (((old >> 18) ^ old) >> 27) & 0xFFFFFFFF
+        rot = old >> 59
+        return ((xs >> rot) | (xs << ((-rot) & 31))) & 0xFFFFFFFF
+
+    def uniform(self, lo: float = 0.0, hi: float = 1.0) -> float:
+        return lo + (hi - lo) * ((self.next_u32() >> 8) * (1.0 / 16777216.0))
+
+
+def room_scene(seed: int = 0, n_boxes: int = 200) -> Scene:
+    """Small procedural scene: a 10 x 10 x 4 m room (12 inward triangles), axis-aligned boxes with centres uniform in
+    the room, sides uniform 0.2-1.5 m, albedo uniform 0.1-0.9 per channel, and one 1 x 1 m emissive quad of radiance 10
+    under the ceiling.  The camera stands in the room; boxes that would hold it are drawn again."""
+    rng = PCG32(seed)
+    eye = (5.5, 1.7, 5.5)
+    mats = [Material("room", (0.75, 0.75, 0.75, 1.0)), Material("lamp", (0.9, 0.9, 0.9, 1.0), emissive=(10.0, 10.0, 10.0))]
+    boxes = []
+    while len(boxes) < n_boxes:
+        c = [rng.uniform(0, 10), rng.uniform(0, 4), rng.uniform(0, 10)]
+        h = [rng.uniform(0.2, 1.5) / 2, rng.uniform(0.2, 1.5) / 2, rng.uniform(0.2, 1.5) / 2]
+        alb = (rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), 1.0)
+        if all(abs(eye[a] - c[a]) < h[a] + 0.3 for a in range(3)):
+            continue
+        boxes.append((c, h, alb))
+    for i, (_, _, alb) in enumerate(boxes):
+        mats.append(Material(f"box{i}", alb))
+    b = Builder(mats)
+    b.mat = 0   # the room, faces inward
+    X, Y, Z = 10.0, 4.0, 10.0
+    b.quad_facing([0, 0, 0], [X, 0, 0], [X, 0, Z], [0, 0, Z], (0, 1, 0))      # floor
+    b.quad_facing([0, Y, Z], [X, Y, Z], [X, Y, 0], [0, Y, 0], (0, -1, 0))     # ceiling
+    b.quad_facing([0, 0, 0], [0, Y, 0], [X, Y, 0], [X, 0, 0], (0, 0, 1))      # z = 0 wall
+    b.quad_facing([X, 0, Z], [X, Y, Z], [0, Y, Z], [0, 0, Z], (0, 0, -1))     # z = Z wall
+    b.quad_facing([0, 0, Z], [0, Y, Z], [0, Y, 0], [0, 0, 0], (1, 0, 0))      # x = 0 wall
+    b.quad_facing([X, 0, 0], [X, Y, 0], [X, Y, Z], [X, 0, Z], (-1, 0, 0))     # x = X wall
+    b.mat = 1
+    b.quad_facing([4.5, 3.95, 5.5], [5.5, 3.95, 5.5], [5.5, 3.95, 4.5], [4.5, 3.95, 4.5], (0, -1, 0))   # lamp
+    for i, (c, h, _) in enumerate(boxes):
+        b.mat = 2 + i
+        b.box(c, h)
+    return b.scene(f"room-{seed}", Camera(eye, (1.0, 1.0, 1.5), 60, 0.05), sun_dir=(0.3, 1.0, 0.2))
+
+
+def _cylinder(cx: float, cz: float, r: float, h: float, seg: int, rings: int):
+    """Smooth cylinder side about the y axis: (seg + 1) x (rings + 1) vertices with radial normals, 2 seg rings
+    triangles wound counter-clockwise seen from outside."""
+    u = np.arange(seg + 1) / seg * 2 * math.pi
+    v = np.arange(rings + 1) / rings * h
+    cu, su = np.cos(u), np.sin(u)
+    pos = np.stack([np.broadcast_to(cx + r * cu, (rings + 1, seg + 1)), np.broadcast_to(v[:, None], (rings + 1, seg + 1)),
+                    np.broadcast_to(cz + r * su, (rings + 1, seg + 1))], axis=-1).reshape(-1, 3)
+    nrm = np.stack([np.broadcast_to(cu, (rings + 1, seg + 1)), np.zeros((rings + 1, seg + 1)),
+                    np.broadcast_to(su, (rings + 1, seg + 1))], axis=-1).reshape(-1, 3)
+    j, i = np.meshgrid(np.arange(rings), np.arange(seg), indexing="ij")
+    a = (j * (seg + 1) + i).reshape(-1)
+    b_ = a + 1
+    c = a + (seg + 1)
+    d = c + 1
+    # outward: (a, c, d) and (a, d, b) are counter-clockwise seen from outside for u increasing towards +z
+    tris = np.concatenate([np.stack([a, c, d], 1), np.stack([a, d, b_], 1)], axis=0)
+    return pos, nrm, tris
+
+
+def colonnade_scene(seed: int = 0, nx: int = 40, nz: int = 16, rings: int = 8, seg: int = 24) -> Scene:
+    """Large procedural scene (~260k triangles): an nx x nz grid of columns 2.5 m apart (seg-segment cylinders of
+    radius 0.3 m and height 8 m, rings bands high), box beams joining neighbouring column heads, a tiled floor, four
+    perimeter walls, four 2 x 2 m emissive panels (radiance ~10) under the beams, and a directional sun."""
+    rng = PCG32(seed, stream=7)
+    mats = [Material("floor", (0.6, 0.55, 0.5, 1.0)), Material("stone", (0.8, 0.78, 0.72, 1.0)),
+            Material("beam", (0.7, 0.5, 0.35, 1.0)), Material("wall", (0.5, 0.55, 0.6, 1.0))]
+    lamp_cols = [(10.0, 9.5, 8.5), (8.5, 9.5, 10.0), (10.0, 8.0, 7.0), (9.0, 10.0, 9.0)]
+    for k, e in enumerate(lamp_cols):
+        mats.append(Material(f"lamp{k}", (0.9, 0.9, 0.9, 1.0), emissive=e))
+    b = Builder(mats)
+    sp = 2.5
+    x0, z0 = -(nx - 1) * sp / 2, -(nz - 1) * sp / 2
+    xs = [x0 + i * sp for i in range(nx)]
+    zs = [z0 + j * sp for j in range(nz)]
+    b.mat = 0
+    for j in range(nz):
+        for i in range(nx):
+            ax, az = xs[i] - sp / 2, zs[j] - sp / 2
+            b.quad([ax, 0, az + sp], [ax + sp, 0, az + sp], [ax + sp, 0, az], [ax, 0, az])
+    b.mat = 1
+    for j in range(nz):
+        for i in range(nx):
+            pos, nrm, tris = _cylinder(xs[i], zs[j], 0.3, 8.0, seg, rings)
+            b.mesh(pos, nrm, tris)
+    b.mat = 2
+    for j in range(nz):
+        for i in range(nx - 1):
+            b.box([xs[i] + sp / 2, 8.25, zs[j]], [sp / 2, 0.25, 0.3])
+    for j in range(nz - 1):
+        for i in range(nx):
+            b.box([xs[i], 8.25, zs[j] + sp / 2], [0.3, 0.25, sp / 2])
+    b.mat = 3
+    hx, hz = nx * sp / 2, nz * sp / 2
+    b.box([0, 5, -hz - 0.15], [hx + 0.3, 5, 0.15])
+    b.box([0, 5, hz + 0.15], [hx + 0.3, 5, 0.15])
+    b.box([-hx - 0.15, 5, 0], [0.15, 5, hz])
+    b.box([hx + 0.15, 5, 0], [0.15, 5, hz])
+    for k in range(4):
+        b.mat = 4 + k
+        cx = xs[int(rng.uniform(2, nx - 3))] + sp / 2
+        cz = zs[int(rng.uniform(2, nz - 3))] + sp / 2
+        b.quad_facing([cx - 1, 7.5, cz + 1], [cx + 1, 7.5, cz + 1], [cx + 1, 7.5, cz - 1], [cx - 1, 7.5, cz - 1], (0, -1, 0))
+    cam = Camera((1.25 + 0.0, 1.7, 1.25), (21.25, 1.3, -3.75), 60, 0.05)
+    from .frame import SUN_E, SKY
+    return b.scene(f"colonnade-{seed}", cam, sun_dir=(-0.4, 1.0, 0.3), sun_e=SUN_E, sky=SKY)
