@@ -1,0 +1,172 @@
+/*
+ * gi.h — C-ABI of the B200 GI hot path: the voxel clipmap rebuild, the voxel DDA radiance cascades, and the cascade
+ * merge plus irradiance gather of the real-time-gi-lab renderer, as sm_100a CUDA kernels.
+ *
+ * The entry points replace the WebGPU dispatch of the reference's `vox` and `giBuild/giTrace/giMerge/giGather`
+ * passes (src/core/rcrun.ts:18, :283-298).  They mirror the reference's two host objects:
+ *   VoxWorld  src/core/voxel.ts:710-727   -> gi_vox_*   (createVoxWorld voxel.ts:746)
+ *   Rc        src/core/rc.ts:980-992      -> gi_rc_*    (createRc rc.ts:1019)
+ * plus the scene upload (src/core/scene_gpu.ts:56 uploadScene) and the frame uniform (src/core/frame.ts:76 packFrame).
+ *
+ * Conventions.  Every function returns a gi_status (0 = GI_OK, negative = error); gi_last_error() returns the
+ * message of the calling thread's last error (the reference throws `new Error(msg)`, e.g. voxel.ts:749).  Pool
+ * overflows are counters, not errors (voxel.ts:463, :586).  Handles own their device memory and free it in
+ * gi_*_destroy (voxel.ts:923, rc.ts:1234).  Host pointers are borrowed for the duration of the call.  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream); work is stream-ordered and asynchronous except where a function
+ * says it synchronises.  A handle may be used by one host thread at a time.
+ */
+#ifndef GI_H
+#define GI_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GI_ABI_VERSION 1
+
+typedef enum {
+  GI_OK = 0,
+  GI_ERR_INVALID = -1,   /* bad argument or unsupported parameter combination */
+  GI_ERR_OOM = -2,       /* device or pinned host allocation failed */
+  GI_ERR_CUDA = -3,      /* a CUDA runtime error (message in gi_last_error) */
+  GI_ERR_TIMEOUT = -4,   /* a bounded device wait gave up */
+  GI_ERR_OVERFLOW = -5,  /* a fixed-capacity structure of the call itself overflowed */
+  GI_ERR_STATE = -6      /* call out of order (e.g. solve before a frame was set) */
+} gi_status;
+
+/* Cascade atlas storage.  F16 is the reference's own packing (pack2x16float, rc.ts:309-310, SH rc.ts:768-771,
+ * rgba16float irradiance rc.ts:1073); F32 keeps every intermediate in f32; BF16 stores the atlases as bfloat16.
+ * Accumulation is f32 in every mode. */
+typedef enum { GI_ATLAS_F32 = 0, GI_ATLAS_F16 = 1, GI_ATLAS_BF16 = 2 } gi_atlas;
+
+typedef struct gi_ctx gi_ctx;
+typedef struct gi_scene gi_scene;
+typedef struct gi_vox gi_vox;
+typedef struct gi_rc gi_rc;
+
+/* Material (scene_gpu.ts:95-106 `struct Material`): base colour factor, flags (1 alpha mask, 2 double-sided,
+ * 4 toon, 8 object), alpha cutoff.  emissive: radiance added at a voxel hit (no counterpart in the reference,
+ * whose materials do not emit).  Textures are not supported: the base colour is the factor (the reference's
+ * untextured materials sample a white default layer).  48 bytes. */
+typedef struct {
+  float base_color[4];
+  uint32_t flags;
+  float alpha_cutoff;
+  float emissive[3];
+  uint32_t reserved[3];
+} gi_material;
+
+/* VoxParams (voxel.ts:31-38).  levels <= 8; G a multiple of 4, <= 256 (brick coordinates are packed in 9 bits). */
+typedef struct {
+  double v0;             /* finest voxel size (m); the window origins use it in f64 like the reference's numbers,
+                            the kernels in f32 like its uniform */
+  uint32_t levels;
+  uint32_t G;
+  uint32_t max_bricks;
+  uint32_t max_voxels;
+  uint32_t dyn_bricks;   /* accepted for parity with VoxParams; the dynamic layer is not part of this library */
+  uint32_t reserved;
+} gi_vox_params;
+
+/* The RcParams fields the screen-probe / voxel-tracer path reads (rc.ts:42-84; parseConfig runner/configs.ts:47). */
+typedef struct {
+  uint32_t cascades;     /* <= 8 */
+  uint32_t P;            /* pixels between c0 probes (tile size of cascade 0) */
+  float k_interval;      /* c0 interval length in units of s0 */
+  float vox_scale;       /* c0 voxel size relative to the c0 probe spacing */
+  float vox_offset;      /* voxel traces start vox_offset voxels along the probe normal */
+  float vox_skip;        /* occupied voxels entered within vox_skip voxels are ignored */
+  float level_map;       /* voxel level grows by level_map per cascade */
+  uint32_t res_cap;      /* directions stop growing above this cascade */
+  uint32_t dda_cap;      /* DDA step cap (the reference hard-codes 1024, voxel.ts:142) */
+  uint32_t stats;        /* 0 off, 1 DDA step counters (rc.ts:232-235) */
+  uint32_t atlas;        /* gi_atlas */
+  uint32_t reserved[5];
+} gi_rc_params;
+
+int gi_version(void);
+const char *gi_status_string(int status);
+/* Message of the calling thread's last failed call ("" when none). */
+const char *gi_last_error(void);
+
+/* ---- context --------------------------------------------------------------------------------------------------- */
+/* Binds CUDA device `device` (env.ts createNativeDevice is the reference's counterpart). */
+int gi_ctx_create(int device, gi_ctx **out);
+int gi_ctx_destroy(gi_ctx *ctx);
+
+/* ---- scene (scene_gpu.ts:56 uploadScene, voxel.ts:730 triangleTable) --------------------------------------------- */
+/* pos, nrm: nverts x 3 floats.  tri4: ntris x (i0, i1, i2, material), absolute vertex indices. */
+int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nverts, const uint32_t *tri4,
+                    uint32_t ntris, const gi_material *mats, uint32_t nmats, gi_scene **out);
+/* Replaces vertices [first, first + count) (the per-frame pose of moving objects, rcrun.ts:206-214). */
+int gi_scene_update_vertices(gi_scene *scene, uint32_t first, uint32_t count, const float *pos, const float *nrm,
+                             void *stream);
+int gi_scene_destroy(gi_scene *scene);
+
+/* ---- voxel world (voxel.ts VoxWorld) ------------------------------------------------------------------------------ */
+int gi_vox_create(gi_scene *scene, const gi_vox_params *params, gi_vox **out);
+/* update(eye) (voxel.ts:868-892 writeUniform): the per-level windows around eye (f64, as the reference's numbers). */
+int gi_vox_update(gi_vox *vox, const double eye[3]);
+/* encode(pass) (voxel.ts:897-899): the whole rebuild, clear .. resolveAttr, stream-ordered. */
+int gi_vox_build(gi_vox *vox, void *stream);
+/* readCounters (voxel.ts:908-918): the 64 header words (0 bricks marked, 1 voxels, 2-4 brick/big/voxel overflow,
+ * 8-15 bricks per level, 16-23 voxBits big triangles per level, 24-31 markBricks big triangles per level).
+ * Synchronises the stream. */
+int gi_vox_read_counters(gi_vox *vox, uint32_t hdr[64], void *stream);
+/* usedBytes (voxel.ts:919-922) of the last counters read: persistent and build-temporary bytes. */
+int gi_vox_used_bytes(gi_vox *vox, uint64_t *persistent, uint64_t *build_temp);
+/* Copies the voxel world's buffers to the host (any pointer may be NULL).  Sizes: ptr levels*G^3, occ
+ * max_bricks*16, base/code max_bricks, rep max_bricks*512, attr max_voxels*4, plane/sunvis max_voxels words.
+ * Synchronises the stream. */
+int gi_vox_read_state(gi_vox *vox, uint32_t *ptr, uint32_t *occ, uint32_t *base, uint32_t *code, uint32_t *rep,
+                      uint32_t *attr, float *plane, float *sunvis, void *stream);
+int gi_vox_destroy(gi_vox *vox);
+
+/* ---- radiance cascades (rc.ts Rc), screen probes traced in the voxel world --------------------------------------- */
+int gi_rc_create(gi_ctx *ctx, const gi_rc_params *params, uint32_t width, uint32_t height, gi_rc **out);
+/* The 640-byte Frame uniform exactly as packFrame (frame.ts:76-94) writes it. */
+int gi_rc_set_frame(gi_rc *rc, const void *frame640, void *stream);
+/* G-buffer from host memory: depth (W*H f32, reversed Z, 0 = background) and the shading normal, either as
+ * rgba f32 (normal4) or in the reference's rgba16float texture format (normal_rgba16f, 4 halves per pixel). */
+int gi_rc_set_gbuffer(gi_rc *rc, const float *depth, const float *normal4, void *stream);
+int gi_rc_set_gbuffer_f16(gi_rc *rc, const float *depth, const uint16_t *normal_rgba16f, void *stream);
+/* G-buffer drawn on the device from the scene and the frame (one primary-ray sample per pixel centre). */
+int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
+/* encode(enc) (rc.ts:1169-1222): giBuild (setupScreen), giTrace, giMerge (mergeScreen N-1..0, projectSH),
+ * giGather (gatherScreen) over the voxel world's current state. */
+int gi_rc_solve(gi_rc *rc, gi_vox *vox, void *stream);
+/* One frame of the GI path: gi_vox_build then gi_rc_solve. */
+int gi_solve(gi_rc *rc, gi_vox *vox, void *stream);
+/* readIrradiance (rcrun.ts:131-149): W*H rgba f32 (rgb irradiance, a = 1 valid / 0 background). Synchronises. */
+int gi_rc_read_irradiance(gi_rc *rc, float *rgba, void *stream);
+/* The irradiance as stored: rgba16float (atlas F16/BF16) or rgba f32 (atlas F32).  Synchronises. */
+int gi_rc_read_irradiance_raw(gi_rc *rc, void *out, size_t bytes, void *stream);
+/* readCounts (rc.ts:1223-1232): the 80 counter words (rc.ts:173-175).  Synchronises. */
+int gi_rc_read_counts(gi_rc *rc, uint32_t counts[80], void *stream);
+/* setStats (rc.ts:1233): 0 off, 1 DDA step counters. */
+int gi_rc_set_stats(gi_rc *rc, uint32_t level);
+/* Bytes of device memory the handle holds (rc.ts `bytes`). */
+int gi_rc_bytes(gi_rc *rc, uint64_t *bytes);
+
+/* Debug readback of an internal buffer (synchronises).  what: */
+enum {
+  GI_RC_PROBES = 0,     /* 48 bytes per probe (pos.xyz, s0; nrm.xyz, view depth; grid), all cascades */
+  GI_RC_RAD = 1,        /* the cascade atlas as stored (4 components per ray) */
+  GI_RC_SH = 2,         /* 32 components per c0 probe as stored (27 used) */
+  GI_RC_DEPTH = 3,      /* W*H f32 */
+  GI_RC_NORMAL = 4,     /* W*H*4 halves */
+  GI_RC_HITS = 5,       /* per ray: level, brick, bit, tIn bits (only after gi_rc_set_debug_hits(rc, 1)) */
+  GI_RC_RAD_TRACED = 6  /* the atlas right after the trace, before the merge (only with debug hits on) */
+};
+int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
+int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);
+int gi_rc_set_debug_hits(gi_rc *rc, int on);
+int gi_rc_destroy(gi_rc *rc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GI_H */

@@ -36,7 +36,7 @@ static inline float comp(v3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.
 /* f32 -> i32, truncating, saturating (WGSL's conversion of an out-of-range float). */
 static inline int32_t f2i(float f) {
   if (f != f) return 0;
-  if (f >= 2147483520.0f) return 2147483647;
+  if (f >= 2147483648.0f) return 2147483647;
   if (f <= -2147483648.0f) return (-2147483647 - 1);
   return (int32_t)f;
 }

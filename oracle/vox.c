@@ -327,8 +327,13 @@ int orc_vox_build(const orc_scene *s, orc_vox *vx) {
       uint32_t ai = first + r++;
       i3 c = I(b.x * 8 + (int32_t)(bit & 7u), b.y * 8 + (int32_t)((bit >> 3) & 7u), b.z * 8 + (int32_t)(bit >> 6));
       v3 p = add(region_lo(vx, L), muls(adds(vi2f(c), 0.5f), vox_size(vx, L)));
-      uint32_t t = vx->rep[ptr * 512u + bit] - 1u;
-      tri_t T = load_tri(s, t);
+      uint32_t rv = vx->rep[ptr * 512u + bit];
+      if (rv == 0u || rv > s->ntris) {   /* no representative (cannot happen for a set bit): no attributes */
+        for (int k = 0; k < 4; k++) vx->attr[ai * 4u + k] = 0u;
+        vx->plane[ai] = 0.0f; vx->sunvis[ai] = 1.0f;
+        continue;
+      }
+      tri_t T = load_tri(s, rv - 1u);
       surf_t sf = surface_at(s, &T, p, 1);
       float alb[4] = {sf.albedo[0], sf.albedo[1], sf.albedo[2], sf.toon};
       /* octEnc (voxel.ts:590-594) */

@@ -1,0 +1,570 @@
+// C-ABI of the GI path (include/gi.h): handle lifetimes, device memory, argument checks and the launch sequences.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <new>
+#include <string>
+
+#include "gi_dev.cuh"
+#include "gi_internal.h"
+
+using namespace gi;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char *what) {
+  if (e == cudaErrorMemoryAllocation) return fail(GI_ERR_OOM, "%s: out of device memory", what);
+  return fail(GI_ERR_CUDA, "%s: %s (%s)", what, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define CK(expr, what)                         \
+  do {                                         \
+    cudaError_t e_ = (expr);                   \
+    if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+  } while (0)
+
+template <class T>
+cudaError_t dalloc(T **p, size_t count) {
+  *p = nullptr;
+  if (count == 0) count = 1;
+  return cudaMalloc((void **)p, count * sizeof(T));
+}
+
+inline cudaStream_t S(void *stream) { return (cudaStream_t)stream; }
+
+}  // namespace
+
+struct gi_ctx {
+  int device;
+  uint32_t sm_count;
+};
+
+struct gi_scene {
+  gi_ctx *ctx;
+  float4 *pos = nullptr, *nrm = nullptr;
+  uint4 *tri = nullptr;
+  gi_material *mats = nullptr;
+  uint32_t nverts = 0, ntris = 0, nmats = 0;
+  uint32_t *raster_big = nullptr, *raster_counter = nullptr;
+  float4 *stage = nullptr;   // vertex staging for updates (nverts * 2)
+  SceneDev dev() const {
+    SceneDev s;
+    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+    return s;
+  }
+};
+
+struct gi_vox {
+  gi_scene *scene;
+  gi_vox_params p;
+  VoxDev dev;
+  bool updated = false;
+  uint32_t hdr[64];
+  uint64_t bytes = 0;
+};
+
+struct gi_rc {
+  gi_ctx *ctx;
+  gi_rc_params p;
+  uint32_t W, H;
+  RcDev dev;
+  float *frame = nullptr;
+  float *depth = nullptr;
+  uint2 *normal = nullptr;
+  unsigned long long *keys = nullptr;
+  float4 *stage = nullptr;
+  uint4 *hits = nullptr;
+  void *rad_traced = nullptr;
+  size_t rad_elem_bytes = 0, sh_elems = 0;
+  bool frame_set = false, gbuf_set = false, debug_hits = false;
+  uint64_t bytes = 0;
+};
+
+static void free_scene(gi_scene *s) {
+  cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
+  cudaFree(s->raster_big); cudaFree(s->raster_counter); cudaFree(s->stage);
+}
+static void free_vox(gi_vox *v) {
+  VoxDev &d = v->dev;
+  cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
+  cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
+}
+static void free_rc(gi_rc *r) {
+  cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->keys); cudaFree(r->stage);
+  cudaFree(r->hits); cudaFree(r->rad_traced);
+  cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
+}
+
+extern "C" {
+
+int gi_version(void) { return GI_ABI_VERSION; }
+
+const char *gi_status_string(int status) {
+  switch (status) {
+    case GI_OK: return "ok";
+    case GI_ERR_INVALID: return "invalid argument";
+    case GI_ERR_OOM: return "out of memory";
+    case GI_ERR_CUDA: return "CUDA error";
+    case GI_ERR_TIMEOUT: return "timeout";
+    case GI_ERR_OVERFLOW: return "overflow";
+    case GI_ERR_STATE: return "call out of order";
+  }
+  return "unknown status";
+}
+
+const char *gi_last_error(void) { return g_err.c_str(); }
+
+int gi_ctx_create(int device, gi_ctx **out) {
+  if (!out) return fail(GI_ERR_INVALID, "gi_ctx_create: out is NULL");
+  *out = nullptr;
+  int n = 0;
+  CK(cudaGetDeviceCount(&n), "gi_ctx_create: cudaGetDeviceCount");
+  if (device < 0 || device >= n) return fail(GI_ERR_INVALID, "gi_ctx_create: device %d of %d", device, n);
+  CK(cudaSetDevice(device), "gi_ctx_create: cudaSetDevice");
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device), "gi_ctx_create: cudaGetDeviceProperties");
+  if (prop.major < 10) return fail(GI_ERR_INVALID, "gi_ctx_create: device %d is sm_%d%d; this library is built for sm_100a", device, prop.major, prop.minor);
+  gi_ctx *c = new (std::nothrow) gi_ctx;
+  if (!c) return fail(GI_ERR_OOM, "gi_ctx_create: host allocation");
+  c->device = device;
+  c->sm_count = (uint32_t)prop.multiProcessorCount;
+  *out = c;
+  return GI_OK;
+}
+
+int gi_ctx_destroy(gi_ctx *ctx) {
+  delete ctx;
+  return GI_OK;
+}
+
+// ---- scene ----------------------------------------------------------------------------------------------------------
+int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nverts, const uint32_t *tri4,
+                    uint32_t ntris, const gi_material *mats, uint32_t nmats, gi_scene **out) {
+  if (!ctx || !out) return fail(GI_ERR_INVALID, "gi_scene_upload: NULL handle");
+  *out = nullptr;
+  if ((nverts && (!pos || !nrm)) || (ntris && !tri4) || (nmats && !mats))
+    return fail(GI_ERR_INVALID, "gi_scene_upload: NULL array with a non-zero count");
+  if (ntris && nmats == 0) return fail(GI_ERR_INVALID, "gi_scene_upload: triangles without materials");
+  for (uint32_t t = 0; t < ntris; t++) {
+    const uint32_t *r = tri4 + 4u * t;
+    if (r[0] >= nverts || r[1] >= nverts || r[2] >= nverts)
+      return fail(GI_ERR_INVALID, "gi_scene_upload: triangle %u indexes vertex %u of %u", t, r[0] >= nverts ? r[0] : (r[1] >= nverts ? r[1] : r[2]), nverts);
+    if (r[3] >= nmats) return fail(GI_ERR_INVALID, "gi_scene_upload: triangle %u uses material %u of %u", t, r[3], nmats);
+  }
+  CK(cudaSetDevice(ctx->device), "gi_scene_upload: cudaSetDevice");
+  gi_scene *s = new (std::nothrow) gi_scene;
+  if (!s) return fail(GI_ERR_OOM, "gi_scene_upload: host allocation");
+  s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats;
+  cudaError_t e = cudaSuccess;
+  float4 *h4 = nullptr;
+  do {
+    if ((e = dalloc(&s->pos, nverts)) || (e = dalloc(&s->nrm, nverts)) || (e = dalloc(&s->tri, ntris)) ||
+        (e = dalloc(&s->mats, nmats)) || (e = dalloc(&s->raster_big, ntris)) || (e = dalloc(&s->raster_counter, 1)) ||
+        (e = dalloc(&s->stage, (size_t)nverts * 2u)))
+      break;
+    h4 = new (std::nothrow) float4[nverts ? nverts : 1];
+    if (!h4) { delete s; return fail(GI_ERR_OOM, "gi_scene_upload: host staging"); }
+    for (uint32_t i = 0; i < nverts; i++) h4[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 0.0f);
+    if ((e = cudaMemcpy(s->pos, h4, nverts * sizeof(float4), cudaMemcpyHostToDevice))) break;
+    for (uint32_t i = 0; i < nverts; i++) h4[i] = make_float4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.0f);
+    if ((e = cudaMemcpy(s->nrm, h4, nverts * sizeof(float4), cudaMemcpyHostToDevice))) break;
+    if (ntris && (e = cudaMemcpy(s->tri, tri4, ntris * sizeof(uint4), cudaMemcpyHostToDevice))) break;
+    if (nmats && (e = cudaMemcpy(s->mats, mats, nmats * sizeof(gi_material), cudaMemcpyHostToDevice))) break;
+  } while (0);
+  delete[] h4;
+  if (e) { free_scene(s); delete s; return cuda_fail(e, "gi_scene_upload"); }
+  *out = s;
+  return GI_OK;
+}
+
+__global__ void k_pack_vertices(const float *src, float4 *dst, uint32_t n) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
+}
+
+int gi_scene_update_vertices(gi_scene *s, uint32_t first, uint32_t count, const float *pos, const float *nrm, void *stream) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_update_vertices: NULL scene");
+  if ((uint64_t)first + count > s->nverts) return fail(GI_ERR_INVALID, "gi_scene_update_vertices: [%u, %u) past %u vertices", first, first + count, s->nverts);
+  if (count == 0) return GI_OK;
+  if (!pos || !nrm) return fail(GI_ERR_INVALID, "gi_scene_update_vertices: NULL array");
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_update_vertices: cudaSetDevice");
+  // the staging area holds the packed xyz triples (3 floats per vertex fit in the float4 slots)
+  float *st = reinterpret_cast<float *>(s->stage);
+  CK(cudaMemcpyAsync(st, pos, (size_t)count * 12u, cudaMemcpyHostToDevice, S(stream)), "gi_scene_update_vertices: positions");
+  k_pack_vertices<<<(count + 255u) / 256u, 256, 0, S(stream)>>>(st, s->pos + first, count);
+  CK(cudaMemcpyAsync(st + (size_t)count * 4u, nrm, (size_t)count * 12u, cudaMemcpyHostToDevice, S(stream)), "gi_scene_update_vertices: normals");
+  k_pack_vertices<<<(count + 255u) / 256u, 256, 0, S(stream)>>>(st + (size_t)count * 4u, s->nrm + first, count);
+  CK(cudaGetLastError(), "gi_scene_update_vertices: launch");
+  return GI_OK;
+}
+
+int gi_scene_destroy(gi_scene *s) {
+  if (!s) return GI_OK;
+  cudaSetDevice(s->ctx->device);
+  free_scene(s);
+  delete s;
+  return GI_OK;
+}
+
+// ---- voxel world ------------------------------------------------------------------------------------------------------
+int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
+  if (!scene || !p || !out) return fail(GI_ERR_INVALID, "gi_vox_create: NULL argument");
+  *out = nullptr;
+  if (p->levels < 1 || p->levels > 8) return fail(GI_ERR_INVALID, "gi_vox_create: levels %u (1..8)", p->levels);
+  if (p->G < 4 || p->G > 256 || p->G % 4) return fail(GI_ERR_INVALID, "gi_vox_create: G %u (a multiple of 4, 4..256)", p->G);
+  if (!(p->v0 > 0.0)) return fail(GI_ERR_INVALID, "gi_vox_create: v0 must be > 0");
+  if (p->max_bricks < 1 || p->max_voxels < 1) return fail(GI_ERR_INVALID, "gi_vox_create: empty pools");
+  if ((uint64_t)p->max_bricks * 512u >= (1ull << 32) || (uint64_t)p->max_voxels >= (1ull << 31))
+    return fail(GI_ERR_INVALID, "gi_vox_create: pools past 32-bit indexing");
+  CK(cudaSetDevice(scene->ctx->device), "gi_vox_create: cudaSetDevice");
+  gi_vox *v = new (std::nothrow) gi_vox;
+  if (!v) return fail(GI_ERR_OOM, "gi_vox_create: host allocation");
+  memset(&v->dev, 0, sizeof v->dev);
+  v->scene = scene;
+  v->p = *p;
+  VoxDev &d = v->dev;
+  d.v0 = (float)p->v0;
+  d.levels = p->levels; d.G = p->G; d.max_bricks = p->max_bricks; d.max_voxels = p->max_voxels;
+  d.big_cap = 1u << 18;   // BIG_CAP (voxel.ts:224)
+  uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
+  uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
+  uint32_t vscan = (p->max_bricks + 255u) / 256u;
+  if (vscan > scan_words) scan_words = vscan;
+  cudaError_t e;
+  if ((e = dalloc(&d.hdr, GI_HDR)) || (e = dalloc(&d.ptr, nptr)) || (e = dalloc(&d.occ, (size_t)p->max_bricks * 16u)) ||
+      (e = dalloc(&d.base, p->max_bricks)) || (e = dalloc(&d.code, p->max_bricks)) ||
+      (e = dalloc(&d.rep, (size_t)p->max_bricks * 512u)) || (e = dalloc(&d.big, (size_t)16u * d.big_cap)) ||
+      (e = dalloc(&d.attr, p->max_voxels)) || (e = dalloc(&d.plane, p->max_voxels)) ||
+      (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words))) {
+    free_vox(v);
+    delete v;
+    return cuda_fail(e, "gi_vox_create");
+  }
+  v->bytes = (GI_HDR + nptr + (uint64_t)p->max_bricks * (16u + 2u + 512u) + (uint64_t)16u * d.big_cap +
+              (uint64_t)p->max_voxels * 6u + scan_words) * 4u;
+  memset(v->hdr, 0, sizeof v->hdr);
+  *out = v;
+  return GI_OK;
+}
+
+int gi_vox_update(gi_vox *v, const double eye[3]) {
+  if (!v || !eye) return fail(GI_ERR_INVALID, "gi_vox_update: NULL argument");
+  for (int a = 0; a < 3; a++)
+    if (!isfinite(eye[a])) return fail(GI_ERR_INVALID, "gi_vox_update: eye is not finite");
+  memset(v->dev.origin, 0, sizeof v->dev.origin);
+  for (uint32_t L = 0; L < v->p.levels; L++) {
+    double bs = v->p.v0 * ldexp(1.0, (int)L) * 8.0;   // v0 * 2 ** L * 8 (voxel.ts:873)
+    for (int a = 0; a < 3; a++) {
+      double o = floor(eye[a] / bs) - (double)(v->p.G / 2);
+      if (fabs(o) > (double)(1 << 22)) return fail(GI_ERR_INVALID, "gi_vox_update: eye too far from the origin");
+      v->dev.origin[L][a] = (int32_t)o;
+    }
+  }
+  v->updated = true;
+  return GI_OK;
+}
+
+int gi_vox_build(gi_vox *v, void *stream) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_build: NULL vox");
+  if (!v->updated) return fail(GI_ERR_STATE, "gi_vox_build: gi_vox_update was not called");
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_build: cudaSetDevice");
+  CK(gi_launch_vox_build(v->dev, v->scene->dev(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
+  return GI_OK;
+}
+
+int gi_vox_read_counters(gi_vox *v, uint32_t hdr[64], void *stream) {
+  if (!v || !hdr) return fail(GI_ERR_INVALID, "gi_vox_read_counters: NULL argument");
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_read_counters: cudaSetDevice");
+  CK(cudaMemcpyAsync(v->hdr, v->dev.hdr, sizeof v->hdr, cudaMemcpyDeviceToHost, S(stream)), "gi_vox_read_counters: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_vox_read_counters: sync");
+  memcpy(hdr, v->hdr, sizeof v->hdr);
+  return GI_OK;
+}
+
+int gi_vox_used_bytes(gi_vox *v, uint64_t *persistent, uint64_t *build_temp) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_used_bytes: NULL vox");
+  uint64_t nb = v->hdr[0] < v->p.max_bricks ? v->hdr[0] : v->p.max_bricks;
+  uint64_t nv = v->hdr[1] < v->p.max_voxels ? v->hdr[1] : v->p.max_voxels;
+  uint64_t nptr = (uint64_t)v->p.levels * v->p.G * v->p.G * v->p.G;
+  // voxel.ts:919-922, with this layout's per-voxel record (16 B attribute + plane + sun visibility)
+  if (persistent) *persistent = (GI_HDR + nptr + nb * 18u) * 4u + nv * 24u;
+  if (build_temp) *build_temp = nb * 512u * 4u;
+  return GI_OK;
+}
+
+int gi_vox_read_state(gi_vox *v, uint32_t *ptr, uint32_t *occ, uint32_t *base, uint32_t *code, uint32_t *rep,
+                      uint32_t *attr, float *plane, float *sunvis, void *stream) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_read_state: NULL vox");
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_read_state: cudaSetDevice");
+  const VoxDev &d = v->dev;
+  size_t nptr = (size_t)v->p.levels * v->p.G * v->p.G * v->p.G, mb = v->p.max_bricks, mv = v->p.max_voxels;
+  cudaStream_t st = S(stream);
+  if (ptr) CK(cudaMemcpyAsync(ptr, d.ptr, nptr * 4u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: ptr");
+  if (occ) CK(cudaMemcpyAsync(occ, d.occ, mb * 64u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: occ");
+  if (base) CK(cudaMemcpyAsync(base, d.base, mb * 4u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: base");
+  if (code) CK(cudaMemcpyAsync(code, d.code, mb * 4u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: code");
+  if (rep) CK(cudaMemcpyAsync(rep, d.rep, mb * 2048u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: rep");
+  if (attr) CK(cudaMemcpyAsync(attr, d.attr, mv * 16u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: attr");
+  if (plane) CK(cudaMemcpyAsync(plane, d.plane, mv * 4u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: plane");
+  if (sunvis) CK(cudaMemcpyAsync(sunvis, d.sunvis, mv * 4u, cudaMemcpyDeviceToHost, st), "gi_vox_read_state: sunvis");
+  CK(cudaStreamSynchronize(st), "gi_vox_read_state: sync");
+  return GI_OK;
+}
+
+int gi_vox_destroy(gi_vox *v) {
+  if (!v) return GI_OK;
+  cudaSetDevice(v->scene->ctx->device);
+  free_vox(v);
+  delete v;
+  return GI_OK;
+}
+
+// ---- radiance cascades --------------------------------------------------------------------------------------------------
+static size_t atlas_elem_bytes(uint32_t atlas) { return atlas == GI_ATLAS_F32 ? 16u : 8u; }
+
+int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_rc **out) {
+  if (!ctx || !p || !out) return fail(GI_ERR_INVALID, "gi_rc_create: NULL argument");
+  *out = nullptr;
+  if (p->cascades < 1 || p->cascades > 8) return fail(GI_ERR_INVALID, "gi_rc_create: at most 8 cascades (rc.ts:1022), got %u", p->cascades);
+  if (W < 1 || H < 1 || W > 16384 || H > 16384) return fail(GI_ERR_INVALID, "gi_rc_create: size %ux%u", W, H);
+  if (p->P < 1 || p->P > 1024) return fail(GI_ERR_INVALID, "gi_rc_create: P %u", p->P);
+  if (p->atlas > GI_ATLAS_BF16) return fail(GI_ERR_INVALID, "gi_rc_create: atlas %u", p->atlas);
+  if (p->dda_cap < 1) return fail(GI_ERR_INVALID, "gi_rc_create: dda_cap must be >= 1");
+  if (!(p->k_interval > 0.0f)) return fail(GI_ERR_INVALID, "gi_rc_create: k_interval must be > 0");
+  CK(cudaSetDevice(ctx->device), "gi_rc_create: cudaSetDevice");
+  gi_rc *r = new (std::nothrow) gi_rc;
+  if (!r) return fail(GI_ERR_OOM, "gi_rc_create: host allocation");
+  memset(&r->dev, 0, sizeof r->dev);
+  r->ctx = ctx; r->p = *p; r->W = W; r->H = H;
+  RcDev &d = r->dev;
+  d.cascades = p->cascades; d.width = W; d.height = H; d.atlas = p->atlas;
+  d.vox_scale = p->vox_scale; d.vox_offset = p->vox_offset; d.level_map = p->level_map; d.vox_skip = p->vox_skip;
+  d.dda_cap = p->dda_cap; d.stats = p->stats;
+  // cascade layout (rc.ts:1027-1035)
+  uint64_t probe_total = 0, ray_total = 0;
+  for (uint32_t i = 0; i < p->cascades; i++) {
+    CascDev &c = d.c[i];
+    uint32_t rc_ = i < p->res_cap ? i : p->res_cap;
+    if (rc_ > 10) return delete r, fail(GI_ERR_INVALID, "gi_rc_create: directions per cascade past 4096^2");
+    c.res = 4u << rc_;
+    uint64_t ts = (uint64_t)p->P << i;
+    if (ts > (1u << 20)) return delete r, fail(GI_ERR_INVALID, "gi_rc_create: tile size overflow");
+    c.tile_size = (uint32_t)ts;
+    c.tiles_x = (uint32_t)((W + ts - 1) / ts);
+    c.tiles_y = (uint32_t)((H + ts - 1) / ts);
+    c.probe_off = (uint32_t)probe_total;
+    c.rad_off = (uint32_t)ray_total;
+    c.ray_off = (uint32_t)ray_total;
+    double b0 = (double)p->k_interval * (pow(4.0, (double)i) - 1.0) / 3.0;
+    double b1 = (double)p->k_interval * (pow(4.0, (double)(i + 1)) - 1.0) / 3.0;
+    c.b0 = (float)b0; c.b1 = (float)b1;
+    probe_total += (uint64_t)c.tiles_x * c.tiles_y;
+    ray_total += (uint64_t)c.tiles_x * c.tiles_y * c.res * c.res;
+  }
+  if (ray_total >= (1ull << 31)) return delete r, fail(GI_ERR_INVALID, "gi_rc_create: %llu rays past 2^31", (unsigned long long)ray_total);
+  d.probes_total = (uint32_t)probe_total;
+  d.rays_total = (uint32_t)ray_total;
+  r->rad_elem_bytes = atlas_elem_bytes(p->atlas);
+  r->sh_elems = (size_t)d.c[0].tiles_x * d.c[0].tiles_y * 8u;
+  size_t npx = (size_t)W * H;
+  cudaError_t e;
+  ProbeDev *probes = nullptr;
+  void *rad = nullptr, *sh = nullptr, *irr = nullptr;
+  uint32_t *counts = nullptr;
+  if ((e = dalloc(&r->frame, 160)) || (e = dalloc(&r->depth, npx)) || (e = dalloc(&r->normal, npx)) ||
+      (e = dalloc(&r->keys, npx)) || (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
+      (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->rad_elem_bytes)) ||
+      (e = cudaMalloc(&irr, npx * atlas_elem_bytes(p->atlas))) || (e = dalloc(&counts, 96))) {
+    d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts;
+    free_rc(r);
+    delete r;
+    return cuda_fail(e, "gi_rc_create");
+  }
+  d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts;
+  d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
+  cudaMemset(counts, 0, 96 * 4);
+  r->bytes = 160 * 4 + npx * (4 + 8 + 8 + 16) + probe_total * 48 + ray_total * r->rad_elem_bytes +
+             r->sh_elems * r->rad_elem_bytes + npx * atlas_elem_bytes(p->atlas) + 96 * 4;
+  *out = r;
+  return GI_OK;
+}
+
+int gi_rc_set_frame(gi_rc *r, const void *frame640, void *stream) {
+  if (!r || !frame640) return fail(GI_ERR_INVALID, "gi_rc_set_frame: NULL argument");
+  const float *f = (const float *)frame640;
+  if (f[100] != (float)r->W || f[101] != (float)r->H)
+    return fail(GI_ERR_INVALID, "gi_rc_set_frame: frame size %gx%g, cascades made for %ux%u", f[100], f[101], r->W, r->H);
+  if (!(f[83] > 0.0f)) return fail(GI_ERR_INVALID, "gi_rc_set_frame: near plane must be > 0");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_frame: cudaSetDevice");
+  CK(cudaMemcpyAsync(r->frame, frame640, 640, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_frame: copy");
+  r->frame_set = true;
+  return GI_OK;
+}
+
+int gi_rc_set_gbuffer(gi_rc *r, const float *depth, const float *normal4, void *stream) {
+  if (!r || !depth || !normal4) return fail(GI_ERR_INVALID, "gi_rc_set_gbuffer: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_gbuffer: cudaSetDevice");
+  size_t npx = (size_t)r->W * r->H;
+  CK(cudaMemcpyAsync(r->depth, depth, npx * 4u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer: depth");
+  CK(cudaMemcpyAsync(r->stage, normal4, npx * 16u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer: normal");
+  CK(gi_launch_normal_f32_to_f16(r->stage, r->normal, (uint32_t)npx, S(stream)), "gi_rc_set_gbuffer: convert");
+  r->gbuf_set = true;
+  return GI_OK;
+}
+
+int gi_rc_set_gbuffer_f16(gi_rc *r, const float *depth, const uint16_t *normal, void *stream) {
+  if (!r || !depth || !normal) return fail(GI_ERR_INVALID, "gi_rc_set_gbuffer_f16: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_gbuffer_f16: cudaSetDevice");
+  size_t npx = (size_t)r->W * r->H;
+  CK(cudaMemcpyAsync(r->depth, depth, npx * 4u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_f16: depth");
+  CK(cudaMemcpyAsync(r->normal, normal, npx * 8u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_f16: normal");
+  r->gbuf_set = true;
+  return GI_OK;
+}
+
+int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
+  if (!r || !s) return fail(GI_ERR_INVALID, "gi_rc_render_gbuffer: NULL argument");
+  if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_render_gbuffer: no frame set");
+  if (s->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_render_gbuffer: scene on another device");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_render_gbuffer: cudaSetDevice");
+  CK(gi_launch_gbuffer(s->dev(), r->frame, r->W, r->H, r->depth, r->normal, r->keys, s->raster_big, s->ntris,
+                       s->raster_counter, r->ctx->sm_count, S(stream)), "gi_rc_render_gbuffer: launch");
+  r->gbuf_set = true;
+  return GI_OK;
+}
+
+int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
+  if (!r || !v) return fail(GI_ERR_INVALID, "gi_rc_solve: NULL argument");
+  if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_solve: no frame set");
+  if (!r->gbuf_set) return fail(GI_ERR_STATE, "gi_rc_solve: no G-buffer set");
+  if (!v->updated) return fail(GI_ERR_STATE, "gi_rc_solve: the voxel world was never updated");
+  if (v->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_solve: voxel world on another device");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_solve: cudaSetDevice");
+  r->dev.hits = r->debug_hits ? r->hits : nullptr;
+  r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
+  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream)), "gi_rc_solve: launch");
+  return GI_OK;
+}
+
+int gi_solve(gi_rc *r, gi_vox *v, void *stream) {
+  int st = gi_vox_build(v, stream);
+  if (st != GI_OK) return st;
+  return gi_rc_solve(r, v, stream);
+}
+
+int gi_rc_read_irradiance(gi_rc *r, float *rgba, void *stream) {
+  if (!r || !rgba) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance: cudaSetDevice");
+  size_t npx = (size_t)r->W * r->H;
+  CK(gi_launch_irr_to_f32(r->dev, r->stage, S(stream)), "gi_rc_read_irradiance: convert");
+  CK(cudaMemcpyAsync(rgba, r->stage, npx * 16u, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_irradiance: sync");
+  return GI_OK;
+}
+
+int gi_rc_read_irradiance_raw(gi_rc *r, void *out, size_t bytes, void *stream) {
+  if (!r || !out) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_raw: NULL argument");
+  size_t need = (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas);
+  if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_raw: %zu bytes, need %zu", bytes, need);
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_raw: cudaSetDevice");
+  CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance_raw: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_irradiance_raw: sync");
+  return GI_OK;
+}
+
+int gi_rc_read_counts(gi_rc *r, uint32_t counts[80], void *stream) {
+  if (!r || !counts) return fail(GI_ERR_INVALID, "gi_rc_read_counts: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_counts: cudaSetDevice");
+  CK(cudaMemcpyAsync(counts, r->dev.counts, 80 * 4, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_counts: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_counts: sync");
+  return GI_OK;
+}
+
+int gi_rc_set_stats(gi_rc *r, uint32_t level) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_stats: NULL rc");
+  if (level > 1) return fail(GI_ERR_INVALID, "gi_rc_set_stats: level %u (0 off, 1 DDA steps; the triangle comparison is not built)", level);
+  r->p.stats = level;
+  r->dev.stats = level;
+  return GI_OK;
+}
+
+int gi_rc_bytes(gi_rc *r, uint64_t *bytes) {
+  if (!r || !bytes) return fail(GI_ERR_INVALID, "gi_rc_bytes: NULL argument");
+  *bytes = r->bytes;
+  return GI_OK;
+}
+
+int gi_rc_set_debug_hits(gi_rc *r, int on) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_debug_hits: NULL rc");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_debug_hits: cudaSetDevice");
+  if (on && !r->hits) {
+    cudaError_t e;
+    if ((e = dalloc(&r->hits, r->dev.rays_total)) || (e = cudaMalloc(&r->rad_traced, (size_t)r->dev.rays_total * r->rad_elem_bytes)))
+      return cuda_fail(e, "gi_rc_set_debug_hits");
+  }
+  r->debug_hits = on != 0;
+  return GI_OK;
+}
+
+int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
+  if (!r || !bytes) return fail(GI_ERR_INVALID, "gi_rc_buffer_bytes: NULL argument");
+  size_t npx = (size_t)r->W * r->H;
+  switch (what) {
+    case GI_RC_PROBES: *bytes = (size_t)r->dev.probes_total * 48u; break;
+    case GI_RC_RAD: case GI_RC_RAD_TRACED: *bytes = (size_t)r->dev.rays_total * r->rad_elem_bytes; break;
+    case GI_RC_SH: *bytes = r->sh_elems * r->rad_elem_bytes; break;
+    case GI_RC_DEPTH: *bytes = npx * 4u; break;
+    case GI_RC_NORMAL: *bytes = npx * 8u; break;
+    case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;
+    default: return fail(GI_ERR_INVALID, "gi_rc_buffer_bytes: unknown buffer %d", what);
+  }
+  return GI_OK;
+}
+
+int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream) {
+  if (!r || !out) return fail(GI_ERR_INVALID, "gi_rc_read_buffer: NULL argument");
+  size_t need = 0;
+  int st = gi_rc_buffer_bytes(r, what, &need);
+  if (st) return st;
+  if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_buffer: %zu bytes, need %zu", bytes, need);
+  const void *src = nullptr;
+  switch (what) {
+    case GI_RC_PROBES: src = r->dev.probes; break;
+    case GI_RC_RAD: src = r->dev.rad; break;
+    case GI_RC_SH: src = r->dev.sh; break;
+    case GI_RC_DEPTH: src = r->depth; break;
+    case GI_RC_NORMAL: src = r->normal; break;
+    case GI_RC_HITS: src = r->hits; break;
+    case GI_RC_RAD_TRACED: src = r->rad_traced; break;
+  }
+  if (!src) return fail(GI_ERR_STATE, "gi_rc_read_buffer: buffer %d not kept (enable gi_rc_set_debug_hits first)", what);
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_buffer: cudaSetDevice");
+  CK(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_buffer: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_buffer: sync");
+  return GI_OK;
+}
+
+int gi_rc_destroy(gi_rc *r) {
+  if (!r) return GI_OK;
+  cudaSetDevice(r->ctx->device);
+  free_rc(r);
+  delete r;
+  return GI_OK;
+}
+
+}  // extern "C"

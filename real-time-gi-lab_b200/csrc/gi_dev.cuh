@@ -1,0 +1,224 @@
+// Device-side types and helpers of the GI path.  Compiled with -fmad=false: every f32 operation rounds separately,
+// in the order the reference's WGSL writes it (left to right), so the integer/index results (voxel bits, DDA hit
+// cells) are reproducible bit for bit on any IEEE f32 machine.
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/gi.h"
+
+#define GI_EMPTY 0xffffffffu
+#define GI_DROP 0xfffffffeu
+#define GI_MARK 0xfffffffdu
+#define GI_HDR 64
+#define GI_BIG_SMALL 8u          // triangles covering more than 8 cells go to the big lists (voxel.ts:223)
+#define GI_PI 3.14159265f
+
+namespace gi {
+
+struct f3 { float x, y, z; };
+struct i3 { int x, y, z; };
+
+__host__ __device__ __forceinline__ f3 mk(float x, float y, float z) { f3 r; r.x = x; r.y = y; r.z = z; return r; }
+__host__ __device__ __forceinline__ i3 mki(int x, int y, int z) { i3 r; r.x = x; r.y = y; r.z = z; return r; }
+__device__ __forceinline__ f3 operator+(f3 a, f3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ f3 operator-(f3 a, f3 b) { return mk(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, f3 b) { return mk(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ f3 operator*(f3 a, float s) { return mk(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ f3 operator/(f3 a, float s) { return mk(a.x / s, a.y / s, a.z / s); }
+__device__ __forceinline__ f3 operator-(f3 a) { return mk(-a.x, -a.y, -a.z); }
+__device__ __forceinline__ f3 adds(f3 a, float s) { return mk(a.x + s, a.y + s, a.z + s); }
+__device__ __forceinline__ float dot(f3 a, f3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ f3 cross(f3 a, f3 b) { return mk(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
+// min/max as `a < b ? a : b` (the oracle's definition; no NaNs reach them)
+__device__ __forceinline__ float mn(float a, float b) { return a < b ? a : b; }
+__device__ __forceinline__ float mx(float a, float b) { return a > b ? a : b; }
+__device__ __forceinline__ f3 vmin(f3 a, f3 b) { return mk(mn(a.x, b.x), mn(a.y, b.y), mn(a.z, b.z)); }
+__device__ __forceinline__ f3 vmax(f3 a, f3 b) { return mk(mx(a.x, b.x), mx(a.y, b.y), mx(a.z, b.z)); }
+__device__ __forceinline__ f3 vabs(f3 a) { return mk(fabsf(a.x), fabsf(a.y), fabsf(a.z)); }
+__device__ __forceinline__ f3 vfloor(f3 a) { return mk(floorf(a.x), floorf(a.y), floorf(a.z)); }
+__device__ __forceinline__ float length3(f3 a) { return sqrtf(dot(a, a)); }
+// normalize(v) = v / sqrt(dot(v, v)), IEEE sqrt and division
+__device__ __forceinline__ f3 normalize3(f3 a) { float l = length3(a); return mk(a.x / l, a.y / l, a.z / l); }
+__device__ __forceinline__ f3 ld3(float4 v) { return mk(v.x, v.y, v.z); }
+// f32 -> i32 truncating and saturating (NaN -> 0), WGSL's conversion
+__device__ __forceinline__ int f2i(float f) { return __float2int_rz(f); }
+__device__ __forceinline__ i3 vf2i(f3 a) { return mki(f2i(a.x), f2i(a.y), f2i(a.z)); }
+__device__ __forceinline__ f3 vi2f(i3 a) { return mk((float)a.x, (float)a.y, (float)a.z); }
+__device__ __forceinline__ int iclamp(int x, int lo, int hi) { return min(max(x, lo), hi); }
+__device__ __forceinline__ i3 iclamp3(i3 a, i3 lo, i3 hi) {
+  return mki(iclamp(a.x, lo.x, hi.x), iclamp(a.y, lo.y, hi.y), iclamp(a.z, lo.z, hi.z));
+}
+__device__ __forceinline__ float fclampf(float x, float lo, float hi) { return mn(mx(x, lo), hi); }
+// exp2 of an integral value is exact; libdevice exp2f otherwise (only non-integral level_map overrides reach it)
+__device__ __forceinline__ float exp2_(float x) {
+  if (x == floorf(x) && fabsf(x) < 126.0f) return ldexpf(1.0f, (int)x);
+  return exp2f(x);
+}
+// round(log2(x)) exactly: x = m 2^e, m in [0.5, 1): log2 m >= -1/2 <=> m^2 >= 1/2 (exact in double)
+__device__ __forceinline__ int round_log2(float x) {
+  if (!(x > 0.0f)) return -2147483647 - 1;
+  if (isinf(x)) return 2147483647;
+  int e;
+  float m = frexpf(x, &e);
+  double mm = (double)m * (double)m;
+  return mm >= 0.5 ? e : e - 1;
+}
+
+// ---- WGSL packing builtins (public WGSL spec formulas) -------------------------------------------------------------
+__device__ __forceinline__ uint32_t pack4x8unorm(float a, float b, float c, float d) {
+  float v[4] = {a, b, c, d};
+  uint32_t r = 0;
+#pragma unroll
+  for (int i = 0; i < 4; i++) {
+    float cc = mn(mx(v[i], 0.0f), 1.0f);
+    uint32_t q = (uint32_t)floorf(0.5f + 255.0f * cc);
+    r |= (q & 0xffu) << (8 * i);
+  }
+  return r;
+}
+__device__ __forceinline__ uint32_t pack2x16snorm(float a, float b) {
+  float ca = mn(mx(a, -1.0f), 1.0f), cb = mn(mx(b, -1.0f), 1.0f);
+  int ia = (int)floorf(0.5f + 32767.0f * ca), ib = (int)floorf(0.5f + 32767.0f * cb);
+  return ((uint32_t)ia & 0xffffu) | (((uint32_t)ib & 0xffffu) << 16);
+}
+__device__ __forceinline__ uint16_t f2h(float x) { return __half_as_ushort(__float2half_rn(x)); }
+__device__ __forceinline__ float h2f(uint16_t h) { return __half2float(__ushort_as_half(h)); }
+__device__ __forceinline__ uint16_t f2bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
+__device__ __forceinline__ float bf2f(uint16_t h) { return __uint_as_float((uint32_t)h << 16); }
+
+// ---- atlas storage ---------------------------------------------------------------------------------------------------
+// F32: float4 per element; F16 / BF16: 4 x 16 bits in a uint2.
+template <int A> struct Atlas;
+template <> struct Atlas<GI_ATLAS_F32> {
+  typedef float4 T;
+  __device__ static __forceinline__ float4 load(const T *p, size_t i) { return p[i]; }
+  __device__ static __forceinline__ void store(T *p, size_t i, float4 v) { p[i] = v; }
+  __device__ static __forceinline__ float round(float x) { return x; }
+};
+template <> struct Atlas<GI_ATLAS_F16> {
+  typedef uint2 T;
+  __device__ static __forceinline__ float4 load(const T *p, size_t i) {
+    uint2 u = p[i];
+    return make_float4(h2f(u.x & 0xffffu), h2f(u.x >> 16), h2f(u.y & 0xffffu), h2f(u.y >> 16));
+  }
+  __device__ static __forceinline__ void store(T *p, size_t i, float4 v) {
+    p[i] = make_uint2((uint32_t)f2h(v.x) | ((uint32_t)f2h(v.y) << 16), (uint32_t)f2h(v.z) | ((uint32_t)f2h(v.w) << 16));
+  }
+  __device__ static __forceinline__ float round(float x) { return h2f(f2h(x)); }
+};
+template <> struct Atlas<GI_ATLAS_BF16> {
+  typedef uint2 T;
+  __device__ static __forceinline__ float4 load(const T *p, size_t i) {
+    uint2 u = p[i];
+    return make_float4(bf2f(u.x & 0xffffu), bf2f(u.x >> 16), bf2f(u.y & 0xffffu), bf2f(u.y >> 16));
+  }
+  __device__ static __forceinline__ void store(T *p, size_t i, float4 v) {
+    p[i] = make_uint2((uint32_t)f2bf(v.x) | ((uint32_t)f2bf(v.y) << 16), (uint32_t)f2bf(v.z) | ((uint32_t)f2bf(v.w) << 16));
+  }
+  __device__ static __forceinline__ float round(float x) { return bf2f(f2bf(x)); }
+};
+
+// ---- device views ----------------------------------------------------------------------------------------------------
+struct SceneDev {
+  const float4 *pos;       // xyz, w = 0
+  const float4 *nrm;       // xyz, w = 0
+  const uint4 *tri;        // i0, i1, i2, material
+  const gi_material *mats;
+  uint32_t ntris, nverts, nmats, pad;
+};
+
+// Voxel world in device memory (struct of arrays; the reference packs the same data in one `vox` buffer,
+// voxel.ts:753-760).
+struct VoxDev {
+  float v0;
+  uint32_t levels, G, max_bricks, max_voxels, big_cap;
+  int32_t origin[8][4];
+  uint32_t *hdr;       // GI_HDR counter words
+  uint32_t *ptr;       // levels * G^3 brick pointers
+  uint32_t *occ;       // max_bricks * 16 occupancy words (64 bytes per brick)
+  uint32_t *base;      // max_bricks first attribute
+  uint32_t *code;      // max_bricks level << 27 | bx << 18 | by << 9 | bz
+  uint32_t *rep;       // max_bricks * 512 representative triangle + 1 (build temporary)
+  uint32_t *big;       // 16 * big_cap big-triangle lists (build temporary)
+  uint4 *attr;         // max_voxels: albedo, normal, emissive rg, emissive b (one 16-byte load per hit)
+  float *plane;        // max_voxels
+  float *sunvis;       // max_voxels
+  uint32_t *scan;      // build temporary: block sums of the ordered allocations
+};
+
+__device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return ldexpf(v.v0, (int)L); }
+__device__ __forceinline__ i3 org(const VoxDev &v, uint32_t L) { return mki(v.origin[L][0], v.origin[L][1], v.origin[L][2]); }
+__device__ __forceinline__ uint32_t ptr_index(const VoxDev &v, uint32_t L, i3 b) {
+  uint32_t G = v.G;
+  return L * G * G * G + ((uint32_t)b.z * G + (uint32_t)b.y) * G + (uint32_t)b.x;
+}
+// regionLo (voxel.ts:289)
+__device__ __forceinline__ f3 region_lo(const VoxDev &v, uint32_t L) { return (vi2f(org(v, L)) * vox_size(v, L)) * 8.0f; }
+
+// Akenine-Moller triangle / box overlap (voxel.ts:231-248)
+__device__ __forceinline__ bool axis_test(f3 a, f3 v0, f3 v1, f3 v2, f3 h) {
+  float p0 = dot(v0, a), p1 = dot(v1, a), p2 = dot(v2, a);
+  float r = dot(h, vabs(a));
+  return !(mn(mn(p0, p1), p2) > r || mx(mx(p0, p1), p2) < -r);
+}
+__device__ __forceinline__ bool tri_box(f3 c, f3 h, f3 a, f3 b, f3 cc) {
+  f3 v0 = a - c, v1 = b - c, v2 = cc - c;
+  f3 lo = vmin(vmin(v0, v1), v2), hi = vmax(vmax(v0, v1), v2);
+  if (lo.x > h.x || lo.y > h.y || lo.z > h.z || hi.x < -h.x || hi.y < -h.y || hi.z < -h.z) return false;
+  f3 e0 = v1 - v0, e1 = v2 - v1, e2 = v0 - v2;
+  f3 n = cross(e0, e1);
+  if (fabsf(dot(n, v0)) > dot(h, vabs(n))) return false;
+  return axis_test(mk(0.0f, -e0.z, e0.y), v0, v1, v2, h) && axis_test(mk(0.0f, -e1.z, e1.y), v0, v1, v2, h)
+      && axis_test(mk(0.0f, -e2.z, e2.y), v0, v1, v2, h) && axis_test(mk(e0.z, 0.0f, -e0.x), v0, v1, v2, h)
+      && axis_test(mk(e1.z, 0.0f, -e1.x), v0, v1, v2, h) && axis_test(mk(e2.z, 0.0f, -e2.x), v0, v1, v2, h)
+      && axis_test(mk(-e0.y, e0.x, 0.0f), v0, v1, v2, h) && axis_test(mk(-e1.y, e1.x, 0.0f), v0, v1, v2, h)
+      && axis_test(mk(-e2.y, e2.x, 0.0f), v0, v1, v2, h);
+}
+
+// Frame word offsets (frame.ts:4-21).
+enum { F_VP = 0, F_IVP = 16, F_EYE = 80, F_FWD = 84, F_SUN = 88, F_SUNE = 92, F_SKY = 96, F_SIZE = 100, F_RC = 104,
+       F_RC2 = 108, F_RU = 112, F_RU2 = 116, F_OMEGA = 120, F_STYLE = 136 };
+
+// worldAt (frame.ts:22-26), mat4 * vec4 summed in column order
+__device__ __forceinline__ f3 world_at(const float *__restrict__ F, int px, int py, float d) {
+  float nx = ((float)px + 0.5f) * F[F_SIZE + 2] * 2.0f - 1.0f;
+  float ny = 1.0f - ((float)py + 0.5f) * F[F_SIZE + 3] * 2.0f;
+  const float *m = F + F_IVP;
+  float h[4];
+#pragma unroll
+  for (int i = 0; i < 4; i++) h[i] = m[i] * nx + m[4 + i] * ny + m[8 + i] * d + m[12 + i] * 1.0f;
+  return mk(h[0] / h[3], h[1] / h[3], h[2] / h[3]);
+}
+__device__ __forceinline__ float view_z(const float *__restrict__ F, f3 p) {
+  return dot(p - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2]), mk(F[F_FWD], F[F_FWD + 1], F[F_FWD + 2]));
+}
+
+// octDecode / dirOf (rc.ts:291-308)
+__device__ __forceinline__ f3 dir_of(uint32_t di, uint32_t res) {
+  float u = ((float)(di % res) + 0.5f) / (float)res, v = ((float)(di / res) + 0.5f) / (float)res;
+  float fx = u * 2.0f - 1.0f, fy = v * 2.0f - 1.0f;
+  f3 n = mk(fx, fy, 1.0f - fabsf(fx) - fabsf(fy));
+  float t = mx(-n.z, 0.0f);
+  n.x += n.x >= 0.0f ? -t : t;
+  n.y += n.y >= 0.0f ? -t : t;
+  return normalize3(n);
+}
+
+// Warp-aggregated atomicAdd: one atomic per distinct address among the active lanes would need a match; the lists
+// and counters here use one address per call, so the active lanes share it.
+__device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool want) {
+  uint32_t active = __activemask();
+  uint32_t m = __ballot_sync(active, want);
+  if (!want) return 0;
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t leader = __ffs(m) - 1u;
+  uint32_t rank = __popc(m & ((1u << lane) - 1u));
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(counter, (uint32_t)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  return base + rank;
+}
+
+}  // namespace gi

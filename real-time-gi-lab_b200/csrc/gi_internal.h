@@ -1,0 +1,43 @@
+// Host/device shared declarations of the library (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "gi_dev.cuh"
+
+namespace gi {
+
+struct CascDev {
+  uint32_t probe_off, rad_off, res, tile_size, tiles_x, tiles_y, ray_off, pad;
+  float b0, b1, pad2[2];
+};
+
+struct ProbeDev { float4 pos; float4 nrm; int4 grid; };   // rc.ts:157 Probe, 48 bytes
+
+// Radiance-cascade state of one solve in device memory.
+struct RcDev {
+  uint32_t cascades, width, height, atlas;
+  CascDev c[8];
+  float vox_scale, vox_offset, level_map, vox_skip;
+  uint32_t dda_cap, stats, probes_total, rays_total;
+  const float *frame;      // 160 words (packFrame)
+  const float *depth;      // W*H
+  const uint2 *normal;     // W*H rgba16f
+  ProbeDev *probes;
+  void *rad;               // rays_total atlas elements
+  void *sh;                // probes of cascade 0 x 8 atlas elements
+  void *irr;               // W*H: float4 (atlas F32) or rgba16f (uint2)
+  uint32_t *counts;        // 80 words
+  uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
+  void *rad_traced;        // optional: copy of the atlas after the trace
+};
+
+}  // namespace gi
+
+cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
+cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st);
+cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
+                              uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
+                              uint32_t *counter, uint32_t sm_count, cudaStream_t st);
+cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
+cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);

@@ -1,0 +1,501 @@
+// Screen-probe radiance cascades traced in the voxel clipmap, on sm_100a (src/core/rc.ts, method 'screen', world
+// tracer 'voxel': setupScreen :572, trace :600 -> traceWorld :216 -> traceVox voxel.ts:121, mergeScreen :710,
+// projectSH :752, gatherScreen :929).
+//
+// Form changes from the reference's dispatches, results unchanged:
+//  * setupScreen and trace each run once over all cascades (the reference dispatches them per cascade);
+//  * the trace kernel is persistent: each warp takes 32 rays at a time from a global ray counter;
+//  * indirect dispatches become launches sized from the host-known probe counts (screen probes: tiles).
+#include <cuda_runtime.h>
+
+#include "gi_dev.cuh"
+#include "gi_internal.h"
+
+namespace gi {
+
+// voxRank (voxel.ts:81-87)
+__device__ __forceinline__ uint32_t vox_rank(const VoxDev &v, uint32_t brick, uint32_t bit) {
+  uint32_t w = bit >> 5;
+  const uint32_t *o = v.occ + brick * 16u;
+  uint32_t r = __popc(o[w] & ((1u << (bit & 31u)) - 1u));
+  for (uint32_t i = 0; i < w; i++) r += __popc(o[i]);
+  return v.base[brick] + r;
+}
+
+// voxAt (voxel.ts:90-107): brick, bit, level (brick GI_EMPTY when empty)
+__device__ __forceinline__ uint3 vox_at(const VoxDev &v, uint32_t L, i3 c) {
+  uint32_t l = L;
+  i3 cc = c;
+  int n8 = (int)v.G * 8;
+  for (;;) {
+    uint32_t ptr = v.ptr[ptr_index(v, l, mki(cc.x >> 3, cc.y >> 3, cc.z >> 3))];
+    if (ptr != GI_DROP) {
+      if (ptr >= GI_MARK) return make_uint3(GI_EMPTY, 0u, l);
+      uint32_t bit = (uint32_t)((cc.x & 7) + 8 * (cc.y & 7) + 64 * (cc.z & 7));
+      if ((v.occ[ptr * 16u + (bit >> 5)] & (1u << (bit & 31u))) == 0u) return make_uint3(GI_EMPTY, 0u, l);
+      return make_uint3(ptr, bit, l);
+    }
+    if (l + 1u >= v.levels) return make_uint3(GI_EMPTY, 0u, l);
+    i3 o = org(v, l);
+    i3 w = mki((o.x * 8 + cc.x) >> 1, (o.y * 8 + cc.y) >> 1, (o.z * 8 + cc.z) >> 1);
+    l++;
+    i3 o1 = org(v, l);
+    cc = mki(w.x - o1.x * 8, w.y - o1.y * 8, w.z - o1.z * 8);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= n8 || cc.y >= n8 || cc.z >= n8) return make_uint3(GI_EMPTY, 0u, l);
+  }
+}
+
+// voxInside / voxLevelFor (voxel.ts:108-119)
+__device__ __forceinline__ bool vox_inside(const VoxDev &v, uint32_t L, f3 p) {
+  float bs = vox_size(v, L) * 8.0f;
+  f3 lo = vi2f(org(v, L)) * bs;
+  f3 hi = adds(lo, (float)v.G * bs);
+  return p.x > lo.x && p.y > lo.y && p.z > lo.z && p.x < hi.x && p.y < hi.y && p.z < hi.z;
+}
+__device__ __forceinline__ uint32_t vox_level_for(const VoxDev &v, uint32_t L, f3 e) {
+  uint32_t l = L;
+  while (l + 1u < v.levels && !vox_inside(v, l, e)) l++;
+  return l;
+}
+
+// style.ts:18-25
+__device__ __forceinline__ f3 toon_albedo(f3 a) {
+  float l = dot(a, mk(0.2126f, 0.7152f, 0.0722f));
+  f3 r = mk(l, l, l) + (a - mk(l, l, l)) * 1.6f;
+  return mk(fclampf(r.x, 0.0f, 1.0f), fclampf(r.y, 0.0f, 1.0f), fclampf(r.z, 0.0f, 1.0f));
+}
+__device__ __forceinline__ float toon_ramp(float x) { return x > 0.3f ? 1.0f : (x > 0.05f ? 0.5f : 0.0f); }
+
+// voxShade (rc.ts:136-140) -> shadeHitV (rc.ts:108-116) with no multi-bounce, plus the voxel's emissive radiance
+__device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restrict__ F, uint32_t brick, uint32_t bit, f3 d) {
+  uint4 w = make_uint4(0, 0, 0, 0);
+  float vis = 0.0f;
+  if (v.base[brick] != GI_EMPTY) {
+    uint32_t ai = vox_rank(v, brick, bit);
+    w = v.attr[ai];
+    vis = v.sunvis[ai];
+  }
+  float alb0 = (float)(w.x & 0xffu) / 255.0f, alb1 = (float)((w.x >> 8) & 0xffu) / 255.0f;
+  float alb2 = (float)((w.x >> 16) & 0xffu) / 255.0f, alb3 = (float)(w.x >> 24) / 255.0f;
+  float nx = mx((float)(int16_t)(w.y & 0xffffu) / 32767.0f, -1.0f);
+  float ny = mx((float)(int16_t)(w.y >> 16) / 32767.0f, -1.0f);
+  f3 n0 = mk(nx, ny, 1.0f - fabsf(nx) - fabsf(ny));
+  float q = mx(-n0.z, 0.0f);
+  n0.x += n0.x >= 0.0f ? -q : q;
+  n0.y += n0.y >= 0.0f ? -q : q;
+  // shadeHitV
+  f3 n = dot(n0, n0) > 0.01f ? n0 : -d;
+  if (dot(n, d) > 0.0f) n = -n;
+  f3 a = mk(alb0, alb1, alb2);
+  f3 r = (a / GI_PI) * mk(0.0f, 0.0f, 0.0f);
+  float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
+  if (ndl > 0.0f) {
+    f3 sunE = mk(F[F_SUNE], F[F_SUNE + 1], F[F_SUNE + 2]);
+    if (alb3 > 0.5f && F[F_STYLE] > 0.5f) r = r + ((toon_albedo(a) / 3.14159265f) * sunE) * toon_ramp(ndl * vis);
+    else r = r + (((a / GI_PI) * sunE) * ndl) * vis;
+  }
+  return r + mk(h2f(w.z & 0xffffu), h2f(w.z >> 16), h2f(w.w & 0xffffu));
+}
+
+struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
+
+// traceVox (voxel.ts:121-202) with a configurable step cap
+__device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, f3 o, f3 d, float t0, float t1,
+                                          float tskip, uint32_t L, uint32_t cap, TraceOut &out) {
+  out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
+  out.steps = 0;
+  float vs = vox_size(v, L);
+  int G = (int)v.G;
+  f3 lo = (vi2f(org(v, L)) * vs) * 8.0f;
+  f3 hi = adds(lo, (float)G * vs * 8.0f);
+  f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
+  f3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+  f3 ta = (lo - o) * inv, tb = (hi - o) * inv;
+  f3 tn = vmin(ta, tb), tf = vmax(ta, tb);
+  float t = mx(mx(mx(tn.x, tn.y), tn.z), t0);
+  float tEnd = mn(mn(mn(tf.x, tf.y), tf.z), t1);
+  if (t >= tEnd) return;
+  i3 st = mki(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
+  f3 sp = mk(st.x > 0 ? 1.0f : 0.0f, st.y > 0 ? 1.0f : 0.0f, st.z > 0 ? 1.0f : 0.0f);
+  int nVox = G * 8;
+  i3 c = iclamp3(vf2i(vfloor(((o + d * t) - lo) / vs)), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
+  f3 tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
+  f3 tDelta = vabs(inv * vs);
+  float tIn = t;
+  const uint32_t Lbase = L * (uint32_t)(G * G * G);
+  for (uint32_t it = 0; it < cap; it++) {
+    out.steps++;
+    i3 b = mki(c.x >> 3, c.y >> 3, c.z >> 3);
+    uint32_t ptr = __ldg(&v.ptr[Lbase + ((uint32_t)b.z * (uint32_t)G + (uint32_t)b.y) * (uint32_t)G + (uint32_t)b.x]);
+    if (ptr == GI_DROP) {
+      uint3 r = vox_at(v, L, c);
+      if (r.x != GI_EMPTY && tIn >= tskip) {
+        out.rad = shade_voxel(v, F, r.x, r.y, d); out.T = 0.0f;
+        out.lvl = r.z; out.ptr = r.x; out.bit = r.y; out.tin = __float_as_uint(tIn);
+        return;
+      }
+      float tx = mn(mn(tMax.x, tMax.y), tMax.z);
+      if (tx >= tEnd) break;
+      tIn = tx;
+      if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
+      else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
+      else { c.z += st.z; tMax.z += tDelta.z; }
+      if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
+      continue;
+    }
+    if (ptr >= GI_MARK) {
+      // empty brick: jump to its exit
+      f3 bt = (((vi2f(mki(b.x * 8, b.y * 8, b.z * 8)) + sp * 8.0f) * vs + lo) - o) * inv;
+      float te = mn(mn(bt.x, bt.y), bt.z);
+      if (te >= tEnd) break;
+      i3 nb = b;
+      if (bt.x <= bt.y && bt.x <= bt.z) nb.x += st.x; else if (bt.y <= bt.z) nb.y += st.y; else nb.z += st.z;
+      if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) break;
+      t = te; tIn = te;
+      c = iclamp3(vf2i(vfloor(((o + d * t) - lo) / vs)), mki(nb.x * 8, nb.y * 8, nb.z * 8),
+                  mki(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
+      tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
+      continue;
+    }
+    uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
+    uint32_t occ = __ldg(&v.occ[ptr * 16u + (bit >> 5)]);
+    float tExit = mn(mn(tMax.x, tMax.y), tMax.z);
+    if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
+      out.rad = shade_voxel(v, F, ptr, bit, d); out.T = 0.0f;
+      out.lvl = L; out.ptr = ptr; out.bit = bit; out.tin = __float_as_uint(tIn);
+      return;
+    }
+    if (tExit >= tEnd) break;
+    tIn = tExit;
+    if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
+    else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
+    else { c.z += st.z; tMax.z += tDelta.z; }
+    if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
+  }
+}
+
+// voxLevel (rc.ts:210-213), round(log2) taken exactly
+__device__ __forceinline__ uint32_t vox_level(const VoxDev &v, const RcDev &r, float s0, uint32_t c) {
+  float vv = r.vox_scale * s0 * exp2_(r.level_map * (float)c);
+  int k = round_log2(vv / v.v0);
+  int top = (int)v.levels - 1;
+  return (uint32_t)(k < 0 ? 0 : (k > top ? top : k));
+}
+
+__device__ __forceinline__ uint32_t casc_of_ray(const RcDev &r, uint32_t i) {
+  uint32_t c = 0;
+#pragma unroll
+  for (uint32_t k = 1; k < 8; k++) if (k < r.cascades && i >= r.c[k].ray_off) c = k;
+  return c;
+}
+
+// setupScreen (rc.ts:572-590), every cascade in one launch
+__global__ void k_setup_screen(RcDev r) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.probes_total) return;
+  uint32_t c = 0;
+  for (uint32_t k = 1; k < r.cascades; k++) if (i >= r.c[k].probe_off) c = k;
+  const CascDev &L = r.c[c];
+  uint32_t t = i - L.probe_off;
+  if (t == 0) r.counts[c] = L.tiles_x * L.tiles_y;
+  const float *F = r.frame;
+  uint32_t tx = t % L.tiles_x, ty = t / L.tiles_x;
+  int px = min((int)(tx * L.tile_size + L.tile_size / 2u), (int)r.width - 1);
+  int py = min((int)(ty * L.tile_size + L.tile_size / 2u), (int)r.height - 1);
+  size_t q = (size_t)py * r.width + (size_t)px;
+  float d = r.depth[q];
+  ProbeDev pr;
+  pr.pos = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  pr.nrm = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  pr.grid = make_int4((int)tx, (int)ty, 0, 0);
+  if (d > 0.0f) {
+    f3 x = world_at(F, px, py, d);
+    uint2 nn = r.normal[q];
+    f3 nrm = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
+    float s0 = length3(x - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2])) * F[F_RC + 1] * F[F_RC + 2];
+    f3 p = x + ((nrm * F[F_RC2]) * s0) * exp2_((float)c);
+    pr.pos = make_float4(p.x, p.y, p.z, s0);
+    pr.nrm = make_float4(nrm.x, nrm.y, nrm.z, view_z(F, x));
+  }
+  r.probes[i] = pr;
+}
+
+// trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245).  Persistent: every warp takes rays from a global counter, 32 at
+// a time.
+template <int A>
+__global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
+  typedef typename Atlas<A>::T T;
+  T *rad = reinterpret_cast<T *>(r.rad);
+  const float *F = r.frame;
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t steps_acc = 0, traces_acc = 0, cap_acc = 0;
+  uint32_t cur_c = 0xffffffffu;
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(ray_counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= r.rays_total) break;
+    uint32_t i = base + lane;
+    bool live = i < r.rays_total;
+    uint32_t c = live ? casc_of_ray(r, i) : 0u;
+    TraceOut out;
+    out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
+    out.steps = 0;
+    bool traced = false;
+    if (live) {
+      const CascDev &L = r.c[c];
+      uint32_t t = i - L.ray_off;
+      uint32_t dirs = L.res * L.res;
+      uint32_t pi = t / dirs, di = t % dirs;
+      ProbeDev pr = r.probes[L.probe_off + pi];
+      if (pr.pos.w > 0.0f) {
+        f3 dir = dir_of(di, L.res);
+        float s0 = pr.pos.w;
+        float t0 = L.b0 * s0, t1 = L.b1 * s0;
+        f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
+        uint32_t Lv = vox_level_for(v, vox_level(v, r, s0, c), po + dir * t1);
+        float vs = vox_size(v, Lv);
+        trace_vox(v, F, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
+        traced = true;
+      }
+      Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
+      if (r.hits) r.hits[i] = make_uint4(out.lvl, out.ptr, out.bit, out.tin);
+      if (r.rad_traced) Atlas<A>::store(reinterpret_cast<T *>(r.rad_traced), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
+    }
+    if (r.stats) {
+      // per-cascade counters (rc.ts:232-235); flush when the lane's cascade changes
+      if (live && traced) {
+        if (c != cur_c && cur_c != 0xffffffffu) {
+          atomicAdd(&r.counts[24 + cur_c], traces_acc); atomicAdd(&r.counts[32 + cur_c], steps_acc);
+          atomicAdd(&r.counts[64 + cur_c], cap_acc);
+          traces_acc = steps_acc = cap_acc = 0;
+        }
+        cur_c = c;
+        traces_acc++; steps_acc += out.steps; cap_acc += out.steps >= r.dda_cap ? 1u : 0u;
+      }
+    }
+  }
+  if (r.stats && cur_c != 0xffffffffu) {
+    atomicAdd(&r.counts[24 + cur_c], traces_acc); atomicAdd(&r.counts[32 + cur_c], steps_acc);
+    atomicAdd(&r.counts[64 + cur_c], cap_acc);
+  }
+}
+
+// upperAvg (rc.ts:681-686)
+template <int A>
+__device__ __forceinline__ f3 upper_avg(const RcDev &r, const typename Atlas<A>::T *rad, uint32_t cu, uint32_t q,
+                                        uint32_t u, uint32_t vv, uint32_t lr) {
+  const CascDev &U = r.c[cu];
+  if (U.res == lr) {
+    float4 p = Atlas<A>::load(rad, (size_t)U.rad_off + q * U.res * U.res + vv * U.res + u);
+    return mk(p.x, p.y, p.z);
+  }
+  size_t base = (size_t)U.rad_off + q * U.res * U.res + vv * 2u * U.res + u * 2u;
+  float4 a = Atlas<A>::load(rad, base), b = Atlas<A>::load(rad, base + 1u);
+  float4 c = Atlas<A>::load(rad, base + U.res), d = Atlas<A>::load(rad, base + U.res + 1u);
+  return (((mk(a.x, a.y, a.z) + mk(b.x, b.y, b.z)) + mk(c.x, c.y, c.z)) + mk(d.x, d.y, d.z)) * 0.25f;
+}
+
+// mergeScreen (rc.ts:710-743) for cascade c, in place
+template <int A>
+__global__ void __launch_bounds__(256) k_merge(RcDev r, uint32_t c) {
+  typedef typename Atlas<A>::T T;
+  T *rad = reinterpret_cast<T *>(r.rad);
+  const CascDev &L = r.c[c];
+  uint32_t dirs = L.res * L.res;
+  uint32_t n = L.tiles_x * L.tiles_y * dirs;
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const float *F = r.frame;
+  uint32_t pi = t / dirs, di = t % dirs;
+  float4 vv = Atlas<A>::load(rad, (size_t)L.rad_off + t);
+  f3 up = mk(F[F_SKY], F[F_SKY + 1], F[F_SKY + 2]);
+  if (c + 1u < r.cascades && vv.w > 0.0f) {
+    up = mk(0.0f, 0.0f, 0.0f);
+    ProbeDev pr = r.probes[L.probe_off + pi];
+    if (pr.pos.w > 0.0f) {
+      const CascDev &U = r.c[c + 1u];
+      float cx = ((float)(pi % L.tiles_x) + 0.5f) * (float)L.tile_size;
+      float cy = ((float)(pi / L.tiles_x) + 0.5f) * (float)L.tile_size;
+      float ux = cx / (float)U.tile_size - 0.5f, uy = cy / (float)U.tile_size - 0.5f;
+      int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+      float fx = ux - (float)bx, fy = uy - (float)by;
+      uint32_t u0 = di % L.res, v0 = di / L.res;
+      f3 acc = mk(0.0f, 0.0f, 0.0f);
+      float ws = 0.0f;
+#pragma unroll
+      for (uint32_t k = 0; k < 4; k++) {
+        int ox = (int)(k & 1u), oy = (int)(k >> 1);
+        int qx = iclamp(bx + ox, 0, (int)U.tiles_x - 1), qy = iclamp(by + oy, 0, (int)U.tiles_y - 1);
+        uint32_t qi = (uint32_t)qy * U.tiles_x + (uint32_t)qx;
+        ProbeDev qp = r.probes[U.probe_off + qi];
+        if (qp.pos.w <= 0.0f) continue;
+        float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
+        float rel = fabsf(qp.nrm.w - pr.nrm.w) / pr.nrm.w;
+        float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f);
+        acc = acc + upper_avg<A>(r, rad, c + 1u, qi, u0, v0, L.res) * w;
+        ws += w;
+      }
+      if (ws > 0.0f) up = acc / ws;
+    }
+  }
+  f3 m = mk(vv.x, vv.y, vv.z) + up * vv.w;
+  Atlas<A>::store(rad, (size_t)L.rad_off + t, make_float4(m.x, m.y, m.z, 1.0f));
+}
+
+__device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
+  y[0] = 0.282095f; y[1] = 0.488603f * n.y; y[2] = 0.488603f * n.z; y[3] = 0.488603f * n.x;
+  y[4] = 1.092548f * n.x * n.y; y[5] = 1.092548f * n.y * n.z; y[6] = 0.315392f * (3.0f * n.z * n.z - 1.0f);
+  y[7] = 1.092548f * n.x * n.z; y[8] = 0.546274f * (n.x * n.x - n.y * n.y);
+}
+
+// projectSH (rc.ts:752-774): c0's 16 directions -> L2 SH of irradiance
+template <int A>
+__global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
+  typedef typename Atlas<A>::T T;
+  const T *rad = reinterpret_cast<const T *>(r.rad);
+  T *sh = reinterpret_cast<T *>(r.sh);
+  const CascDev &L = r.c[0];
+  uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pi >= L.tiles_x * L.tiles_y) return;
+  const float *F = r.frame;
+  f3 cf[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) cf[k] = mk(0.0f, 0.0f, 0.0f);
+  for (uint32_t d = 0; d < 16; d++) {
+    float4 rp = Atlas<A>::load(rad, (size_t)L.rad_off + pi * 16u + d);
+    f3 rr = mk(rp.x, rp.y, rp.z) * F[F_OMEGA + d];
+    float y[9];
+    sh_basis(dir_of(d, 4u), y);
+#pragma unroll
+    for (int k = 0; k < 9; k++) cf[k] = cf[k] + rr * y[k];
+  }
+  float vals[32];
+#pragma unroll
+  for (int k = 0; k < 32; k++) vals[k] = 0.0f;
+  const float a0 = GI_PI, a1 = 2.0f * GI_PI / 3.0f, a2 = GI_PI / 4.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    float a = k == 0 ? a0 : (k < 4 ? a1 : a2);
+    vals[k * 3 + 0] = cf[k].x * a; vals[k * 3 + 1] = cf[k].y * a; vals[k * 3 + 2] = cf[k].z * a;
+  }
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+    Atlas<A>::store(sh, (size_t)pi * 8u + q, make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]));
+}
+
+// gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829)
+template <int A>
+__global__ void __launch_bounds__(256) k_gather(RcDev r) {
+  typedef typename Atlas<A>::T T;
+  const T *sh = reinterpret_cast<const T *>(r.sh);
+  uint32_t px = blockIdx.x * 16u + (threadIdx.x & 15u), py = blockIdx.y * 16u + (threadIdx.x >> 4);
+  if (px >= r.width || py >= r.height) return;
+  size_t q = (size_t)py * r.width + px;
+  const float *F = r.frame;
+  float d = r.depth[q];
+  f3 res = mk(0.0f, 0.0f, 0.0f);
+  float alpha = 0.0f;
+  if (d > 0.0f) {
+    alpha = 1.0f;
+    const CascDev &L = r.c[0];
+    f3 x = world_at(F, (int)px, (int)py, d);
+    uint2 nn = r.normal[q];
+    f3 n = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
+    float z = view_z(F, x);
+    float ux = ((float)px + 0.5f) / (float)L.tile_size - 0.5f, uy = ((float)py + 0.5f) / (float)L.tile_size - 0.5f;
+    int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+    float fx = ux - (float)bx, fy = uy - (float)by;
+    float y[9];
+    sh_basis(n, y);
+    f3 e = mk(0.0f, 0.0f, 0.0f);
+    float ws = 0.0f;
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) {
+      int ox = (int)(k & 1u), oy = (int)(k >> 1);
+      int qx = iclamp(bx + ox, 0, (int)L.tiles_x - 1), qy = iclamp(by + oy, 0, (int)L.tiles_y - 1);
+      uint32_t qi = (uint32_t)qy * L.tiles_x + (uint32_t)qx;
+      ProbeDev pr = r.probes[L.probe_off + qi];
+      if (pr.pos.w <= 0.0f) continue;
+      float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
+      float rel = fabsf(pr.nrm.w - z) / z;
+      float nd = mx(dot(n, ld3(pr.nrm)), 0.0f);
+      float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
+      float v[32];
+#pragma unroll
+      for (int j = 0; j < 8; j++) {
+        float4 s = Atlas<A>::load(sh, (size_t)qi * 8u + j);
+        v[4 * j] = s.x; v[4 * j + 1] = s.y; v[4 * j + 2] = s.z; v[4 * j + 3] = s.w;
+      }
+      f3 es = mk(0.0f, 0.0f, 0.0f);
+#pragma unroll
+      for (int k2 = 0; k2 < 9; k2++) es = es + mk(v[3 * k2], v[3 * k2 + 1], v[3 * k2 + 2]) * y[k2];
+      es = vmax(es, mk(0.0f, 0.0f, 0.0f));
+      e = e + es * w;
+      ws += w;
+    }
+    if (ws > 0.0f) res = e / ws;
+  }
+  if (A == GI_ATLAS_F32) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
+  else reinterpret_cast<uint2 *>(r.irr)[q] = make_uint2((uint32_t)f2h(res.x) | ((uint32_t)f2h(res.y) << 16),
+                                                       (uint32_t)f2h(res.z) | ((uint32_t)f2h(alpha) << 16));
+}
+
+__global__ void k_irr_to_f32(RcDev r, float4 *dst) {
+  size_t n = (size_t)r.width * r.height;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    if (r.atlas == GI_ATLAS_F32) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
+    else {
+      uint2 u = reinterpret_cast<const uint2 *>(r.irr)[i];
+      dst[i] = make_float4(h2f(u.x & 0xffffu), h2f(u.x >> 16), h2f(u.y & 0xffffu), h2f(u.y >> 16));
+    }
+  }
+}
+
+__global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float4 s = src[i];
+    dst[i] = make_uint2((uint32_t)f2h(s.x) | ((uint32_t)f2h(s.y) << 16), (uint32_t)f2h(s.z) | ((uint32_t)f2h(s.w) << 16));
+  }
+}
+
+template <int A>
+static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st) {
+  uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
+  cudaMemsetAsync(r.counts, 0, 81 * sizeof(uint32_t), st);
+  k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r);
+  uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * 8u);
+  k_trace<A><<<tb, 256, 0, st>>>(r, v, counter);
+  for (int c = (int)r.cascades - 1; c >= 0; c--) {
+    const CascDev &L = r.c[c];
+    uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
+    k_merge<A><<<(n + 255u) / 256u, 256, 0, st>>>(r, (uint32_t)c);
+  }
+  k_project_sh<A><<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r);
+  dim3 gg((r.width + 15u) / 16u, (r.height + 15u) / 16u);
+  k_gather<A><<<gg, 256, 0, st>>>(r);
+  return cudaGetLastError();
+}
+
+}  // namespace gi
+
+using namespace gi;
+
+cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st) {
+  switch (r.atlas) {
+    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st);
+    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st);
+    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t gi_launch_irr_to_f32(const RcDev &r, float4 *dst, cudaStream_t st) {
+  k_irr_to_f32<<<256, 256, 0, st>>>(r, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st) {
+  k_normal_f32_to_f16<<<256, 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}

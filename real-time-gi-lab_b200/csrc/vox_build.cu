@@ -1,0 +1,551 @@
+// Voxel clipmap rebuild on sm_100a (the reference's VOX_STAGES, src/core/voxel.ts:338-620, as CUDA passes).
+//
+// Differences of form, not of result, from the reference's dispatch graph:
+//  * brick pointers are allocated in one fixed order, coarse levels first then pointer index, whether or not the
+//    pool holds them all (the reference uses that order only when it overflows, voxel.ts:405-410, and an atomic
+//    counter otherwise); voxel attribute bases are an exclusive scan in brick order.  Both are orders the reference
+//    can produce; they make the whole state deterministic, so the GPU state equals the oracle's word for word.
+//  * the brick init and the representative-table clear (clearKeys) are fused into the allocation pass;
+//  * indirect dispatches (writeArgs) become grid-stride loops that read the device-side counts;
+//  * the big-triangle passes run one warp per (triangle, level) instead of one 64-wide workgroup;
+//  * list appends are warp-aggregated atomics.
+#include <cuda_runtime.h>
+
+#include "gi_dev.cuh"
+#include "gi_internal.h"
+
+namespace gi {
+
+struct Tri { f3 a, b, c; uint4 idx; };
+
+__device__ __forceinline__ Tri load_tri(const SceneDev &s, uint32_t t) {
+  Tri T;
+  T.idx = s.tri[t];
+  T.a = ld3(s.pos[T.idx.x]);
+  T.b = ld3(s.pos[T.idx.y]);
+  T.c = ld3(s.pos[T.idx.z]);
+  return T;
+}
+
+struct Range { i3 lo, n; };
+
+// voxRange (voxel.ts:293-300)
+__device__ __forceinline__ Range vox_range(const VoxDev &v, const Tri &T, uint32_t L, float cell) {
+  f3 lo = region_lo(v, L);
+  f3 a_ = vmin(vmin(T.a, T.b), T.c), b_ = vmax(vmax(T.a, T.b), T.c);
+  int lim = f2i((float)v.G * vox_size(v, L) * 8.0f / cell);
+  i3 a = vf2i(vfloor((a_ - lo) / cell));
+  i3 b = vf2i(vfloor((b_ - lo) / cell));
+  a = iclamp3(a, mki(0, 0, 0), mki(lim, lim, lim));
+  b = iclamp3(mki(b.x + 1, b.y + 1, b.z + 1), mki(0, 0, 0), mki(lim, lim, lim));
+  Range r;
+  r.lo = a;
+  r.n = mki(max(b.x - a.x, 0), max(b.y - a.y, 0), max(b.z - a.z, 0));
+  return r;
+}
+
+// finerHolds (voxel.ts:303-307)
+__device__ __forceinline__ i3 finer_cell(const VoxDev &v, uint32_t L, i3 c) {
+  i3 o = org(v, L), of = org(v, L - 1);
+  return mki((o.x * 8 + c.x) * 2 - of.x * 8, (o.y * 8 + c.y) * 2 - of.y * 8, (o.z * 8 + c.z) * 2 - of.z * 8);
+}
+__device__ __forceinline__ bool finer_holds(const VoxDev &v, uint32_t L, i3 c) {
+  if (L == 0) return false;
+  i3 f = finer_cell(v, L, c);
+  int n = (int)v.G * 8;
+  return f.x >= 0 && f.y >= 0 && f.z >= 0 && f.x < n && f.y < n && f.z < n;
+}
+__device__ __forceinline__ bool finer_holds_range(const VoxDev &v, uint32_t L, Range r, int s) {
+  return finer_holds(v, L, mki(r.lo.x * s, r.lo.y * s, r.lo.z * s))
+      && finer_holds(v, L, mki((r.lo.x + r.n.x) * s - 1, (r.lo.y + r.n.y) * s - 1, (r.lo.z + r.n.z) * s - 1));
+}
+// finerBuilt / finerBuiltRange (voxel.ts:314-320); hdr[2] (brick overflow) is final before the voxel passes run
+__device__ __forceinline__ bool finer_built(const VoxDev &v, uint32_t L, i3 c, uint32_t brick_overflow) {
+  if (!finer_holds(v, L, c)) return false;
+  if (brick_overflow == 0) return true;
+  i3 f = finer_cell(v, L, c);
+  return v.ptr[ptr_index(v, L - 1, mki(f.x >> 3, f.y >> 3, f.z >> 3))] != GI_DROP;
+}
+
+__device__ __forceinline__ i3 range_cell(Range r, int q) {
+  return mki(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y));
+}
+
+// markBrick (voxel.ts:347): read before the atomic
+__device__ __forceinline__ void mark_brick(const VoxDev &v, uint32_t i) {
+  if (v.ptr[i] == GI_EMPTY) atomicMin(&v.ptr[i], GI_MARK);
+}
+
+// markRange body for one brick j of the range (voxel.ts:348-358)
+__device__ __forceinline__ void mark_one(const VoxDev &v, const Tri &T, uint32_t L, Range r, uint32_t n, uint32_t j) {
+  i3 b = range_cell(r, (int)j);
+  if (finer_holds(v, L, mki(b.x * 8, b.y * 8, b.z * 8)) && finer_holds(v, L, mki(b.x * 8 + 7, b.y * 8 + 7, b.z * 8 + 7))) return;
+  float bs = vox_size(v, L) * 8.0f;
+  f3 c = region_lo(v, L) + adds(vi2f(b), 0.5f) * bs;
+  float hh = 0.5f * bs * 1.0001f;
+  if (n == 1u || tri_box(c, mk(hh, hh, hh), T.a, T.b, T.c)) mark_brick(v, ptr_index(v, L, b));
+}
+
+// clear (voxel.ts:338-344)
+__global__ void k_clear(VoxDev v) {
+  uint32_t n = v.levels * v.G * v.G * v.G;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < GI_HDR; i += gridDim.x * blockDim.x) {
+    if (i < GI_HDR) v.hdr[i] = 0u;
+    if (i < n) v.ptr[i] = GI_EMPTY;
+  }
+}
+
+// markBricks (voxel.ts:359-376): one thread per triangle; every lane walks the same levels so that the list appends
+// are warp-aggregated.
+__global__ void __launch_bounds__(256) k_mark_bricks(VoxDev v, SceneDev s) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = t < s.ntris;
+  Tri T;
+  if (live) T = load_tri(s, t);
+  for (uint32_t L = 0; L < v.levels; L++) {
+    bool big = false;
+    Range r;
+    int n = 0;
+    if (live) {
+      r = vox_range(v, T, L, vox_size(v, L) * 8.0f);
+      n = r.n.x * r.n.y * r.n.z;
+      if (n != 0 && !finer_holds_range(v, L, r, 8)) big = n > 8;
+      else n = 0;
+    }
+    uint32_t k = warp_append(&v.hdr[24 + L], big);
+    if (big) {
+      if (k < v.big_cap) v.big[(8u + L) * v.big_cap + k] = t; else atomicAdd(&v.hdr[3], 1u);
+    } else if (n > 0) {
+      for (uint32_t j = 0; j < (uint32_t)n; j++) mark_one(v, T, L, r, (uint32_t)n, j);
+    }
+  }
+}
+
+// The list entry of global item w among the levels' lists starting at segment seg0 (markBricksBig / voxelizeBig
+// level walk, voxel.ts:378-384).  Returns false past the end.
+__device__ __forceinline__ bool big_item(const VoxDev &v, uint32_t seg0, uint32_t hdr0, uint32_t w, uint32_t &L, uint32_t &t) {
+  uint32_t k = w;
+  for (L = 0; L < v.levels; L++) {
+    uint32_t n = min(v.hdr[hdr0 + L], v.big_cap);
+    if (k < n) { t = v.big[(seg0 + L) * v.big_cap + k]; return true; }
+    k -= n;
+  }
+  return false;
+}
+
+// markBricksBig (voxel.ts:377-387): one warp per big (triangle, level), lanes over the range's bricks.
+__global__ void __launch_bounds__(256) k_mark_bricks_big(VoxDev v, SceneDev s) {
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    uint32_t L, t;
+    if (!big_item(v, 8u, 24u, w, L, t)) break;
+    Tri T = load_tri(s, t);
+    Range r = vox_range(v, T, L, vox_size(v, L) * 8.0f);
+    uint32_t n = (uint32_t)(r.n.x * r.n.y * r.n.z);
+    for (uint32_t j = lane; j < n; j += 32u) mark_one(v, T, L, r, n, j);
+  }
+}
+
+// markParents (voxel.ts:390-403)
+__global__ void k_mark_parents(VoxDev v) {
+  uint32_t G = v.G, per = G * G * G, NL = v.levels;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (NL - 1u) * per; i += gridDim.x * blockDim.x) {
+    if (v.ptr[i] != GI_MARK) continue;
+    uint32_t L = i / per, r = i % per;
+    i3 o = org(v, L);
+    i3 w = mki(o.x + (int)(r % G), o.y + (int)((r / G) % G), o.z + (int)(r / (G * G)));
+    for (L++; L < NL; L++) {
+      w = mki(w.x >> 1, w.y >> 1, w.z >> 1);
+      i3 ol = org(v, L);
+      i3 b = mki(w.x - ol.x, w.y - ol.y, w.z - ol.z);
+      if (b.x < 0 || b.y < 0 || b.z < 0 || b.x >= (int)G || b.y >= (int)G || b.z >= (int)G) break;
+      mark_brick(v, ptr_index(v, L, b));
+    }
+  }
+}
+
+// ---- ordered allocation of the marked bricks (countMarks / scanMarks / allocBricks, voxel.ts:411-470) ---------------
+// Order space o in [0, levels * G^3): level levels-1 first, pointer index within a level.
+constexpr uint32_t ALLOC_CHUNK = 2048;   // entries per block (256 threads x 8)
+
+__device__ __forceinline__ uint32_t order_to_ptr(uint32_t o, uint32_t per, uint32_t NL) {
+  return (NL - 1u - o / per) * per + o % per;
+}
+
+// Block-wide exclusive scan of one value per thread (256 threads).  Returns the exclusive prefix; *total = sum.
+__device__ __forceinline__ uint32_t block_scan_256(uint32_t x, uint32_t *total) {
+  __shared__ uint32_t warp_sums[8];
+  __shared__ uint32_t s_total;
+  uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  uint32_t inc = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= (uint32_t)d) inc += y;
+  }
+  if (lane == 31u) warp_sums[wid] = inc;
+  __syncthreads();
+  if (wid == 0) {
+    uint32_t ws = lane < 8u ? warp_sums[lane] : 0u;
+    uint32_t wi = ws;
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, wi, d);
+      if (lane >= (uint32_t)d) wi += y;
+    }
+    if (lane < 8u) warp_sums[lane] = wi - ws;   // exclusive prefix of the warps
+    if (lane == 7u) s_total = wi;
+  }
+  __syncthreads();
+  uint32_t excl = warp_sums[wid] + inc - x;
+  if (total) *total = s_total;
+  __syncthreads();   // the next call may overwrite warp_sums / s_total
+  return excl;
+}
+
+// Per block: the number of marked entries of its chunk of the order space.
+__global__ void __launch_bounds__(256) k_count_marks(VoxDev v) {
+  uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per;
+  uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
+  uint32_t c = 0;
+  for (uint32_t k = threadIdx.x; k < ALLOC_CHUNK; k += 256u) {
+    uint32_t o = o0 + k;
+    if (o < n && v.ptr[order_to_ptr(o, per, NL)] == GI_MARK) c++;
+  }
+  uint32_t tot;
+  block_scan_256(c, &tot);
+  if (threadIdx.x == 0) v.scan[blockIdx.x] = tot;
+}
+
+// Exclusive scan of the block sums (one block, nblocks <= 256 * 16); writes the total to hdr[0] and hdr[5].
+__global__ void __launch_bounds__(256) k_scan_sums(uint32_t *sums, uint32_t nblocks, uint32_t *hdr) {
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < nblocks; b0 += 256u) {
+    uint32_t i = b0 + threadIdx.x;
+    uint32_t x = i < nblocks ? sums[i] : 0u;
+    uint32_t tot;
+    uint32_t ex = block_scan_256(x, &tot);
+    if (i < nblocks) sums[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && hdr) { hdr[0] = carry; hdr[5] = carry; }
+}
+
+// allocBricks (voxel.ts:450-470) in the fixed order, with the brick init and clearKeys (voxel.ts:471-474) fused.
+__global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
+  uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per, G = v.G;
+  uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
+  // each thread owns 8 consecutive entries of the chunk
+  uint32_t flags = 0, c = 0;
+#pragma unroll
+  for (uint32_t k = 0; k < 8u; k++) {
+    uint32_t o = o0 + threadIdx.x * 8u + k;
+    bool m = o < n && v.ptr[order_to_ptr(o, per, NL)] == GI_MARK;
+    flags |= (m ? 1u : 0u) << k;
+    c += m ? 1u : 0u;
+  }
+  uint32_t tot;
+  uint32_t ex = block_scan_256(c, &tot) + v.scan[blockIdx.x];
+  __shared__ uint32_t s_idx[ALLOC_CHUNK];
+  __shared__ uint32_t s_cnt;
+  if (threadIdx.x == 0) s_cnt = 0;
+  __syncthreads();
+#pragma unroll
+  for (uint32_t k = 0; k < 8u; k++) {
+    if (!((flags >> k) & 1u)) continue;
+    uint32_t o = o0 + threadIdx.x * 8u + k;
+    uint32_t i = order_to_ptr(o, per, NL);
+    uint32_t idx = ex++;
+    if (idx >= v.max_bricks) { v.ptr[i] = GI_DROP; atomicAdd(&v.hdr[2], 1u); continue; }
+    uint32_t L = i / per, r = i % per;
+    atomicAdd(&v.hdr[8 + L], 1u);
+    v.ptr[i] = idx;
+    v.base[idx] = 0u;
+    v.code[idx] = (L << 27) | ((r % G) << 18) | (((r / G) % G) << 9) | (r / (G * G));
+    s_idx[atomicAdd(&s_cnt, 1u)] = idx;
+  }
+  __syncthreads();
+  // zero the occupancy (64 B) and representatives (2 KB) of the bricks this block allocated
+  uint32_t nb = s_cnt;
+  for (uint32_t q = threadIdx.x; q < nb * 132u; q += 256u) {
+    uint32_t b = s_idx[q / 132u], w = q % 132u;
+    if (w < 4u) reinterpret_cast<uint4 *>(v.occ)[b * 4u + w] = make_uint4(0, 0, 0, 0);
+    else reinterpret_cast<uint4 *>(v.rep)[b * 128u + (w - 4u)] = make_uint4(0, 0, 0, 0);
+  }
+}
+
+// voxelizeOne (voxel.ts:476-490)
+__device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t t, uint32_t L,
+                                             i3 c, bool single, uint32_t brick_overflow) {
+  if (finer_built(v, L, c, brick_overflow)) return;
+  float vs = vox_size(v, L);
+  f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
+  float hh = 0.5f * vs * 1.0001f;
+  if (!single && !tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return;
+  uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
+  if (ptr >= GI_MARK) return;
+  uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
+  // surfaceAt's alpha test (voxel.ts:325-332): untextured, so the sampled alpha is the factor's
+  const gi_material &m = s.mats[T.idx.w];
+  if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return;
+  uint32_t wi = ptr * 16u + (bit >> 5);
+  uint32_t msk = 1u << (bit & 31u);
+  if ((v.occ[wi] & msk) == 0u) atomicOr(&v.occ[wi], msk);
+  uint32_t ri = ptr * 512u + bit;
+  if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
+}
+
+// voxBits (voxel.ts:492-513)
+__global__ void __launch_bounds__(256) k_vox_bits(VoxDev v, SceneDev s) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = t < s.ntris;
+  uint32_t bo = v.hdr[2];
+  Tri T;
+  if (live) T = load_tri(s, t);
+  for (uint32_t L = 0; L < v.levels; L++) {
+    bool big = false;
+    Range r;
+    int n = 0;
+    if (live) {
+      r = vox_range(v, T, L, vox_size(v, L));
+      n = r.n.x * r.n.y * r.n.z;
+      bool skip = n == 0 || (bo == 0u && finer_holds_range(v, L, r, 1));
+      if (skip) n = 0;
+      else big = (uint32_t)n > GI_BIG_SMALL;
+    }
+    uint32_t k = warp_append(&v.hdr[16 + L], big);
+    if (big) {
+      if (k < v.big_cap) v.big[L * v.big_cap + k] = t; else atomicAdd(&v.hdr[3], 1u);
+    } else if (n > 0) {
+      for (int q = 0; q < n; q++) voxelize_one(v, s, T, t, L, range_cell(r, q), n == 1, bo);
+    }
+  }
+}
+
+// voxBitsBig (voxel.ts:515-534): one warp per big (triangle, level)
+__global__ void __launch_bounds__(256) k_vox_bits_big(VoxDev v, SceneDev s) {
+  uint32_t lane = threadIdx.x & 31u;
+  uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  uint32_t bo = v.hdr[2];
+  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+    uint32_t L, t;
+    if (!big_item(v, 0u, 16u, w, L, t)) break;
+    Tri T = load_tri(s, t);
+    Range r = vox_range(v, T, L, vox_size(v, L));
+    int n = r.n.x * r.n.y * r.n.z;
+    for (int q = (int)lane; q < n; q += 32) voxelize_one(v, s, T, t, L, range_cell(r, q), false, bo);
+  }
+}
+
+// First brick index and count of level l (bricks are allocated coarse levels first).
+__device__ __forceinline__ void level_bricks(const VoxDev &v, uint32_t l, uint32_t &first, uint32_t &count) {
+  first = 0;
+  for (uint32_t k = v.levels - 1u; k > l; k--) first += v.hdr[8 + k];
+  count = v.hdr[8 + l];
+}
+
+// reduce (voxel.ts:540-577): level L from level L-1, one thread per occupancy word of a level L-1 brick
+__global__ void __launch_bounds__(256) k_reduce(VoxDev v, uint32_t L) {
+  uint32_t first, count;
+  level_bricks(v, L - 1u, first, count);
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count * 16u; i += gridDim.x * blockDim.x) {
+    uint32_t ptr = first + (i >> 4), w = i & 15u;
+    uint32_t word = v.occ[ptr * 16u + w];
+    if (word == 0u) continue;
+    uint32_t code = v.code[ptr];
+    uint32_t Lc = code >> 27;
+    i3 b = mki((int)((code >> 18) & 511u), (int)((code >> 9) & 511u), (int)(code & 511u));
+    i3 c0 = mki(b.x * 8, b.y * 8 + (int)((w & 1u) * 4u), b.z * 8 + (int)(w >> 1));
+    i3 oc = org(v, Lc), ol = org(v, L);
+    i3 pc0 = mki(((oc.x * 8 + c0.x) >> 1) - ol.x * 8, ((oc.y * 8 + c0.y) >> 1) - ol.y * 8, ((oc.z * 8 + c0.z) >> 1) - ol.z * 8);
+    uint32_t pptr = v.ptr[ptr_index(v, L, mki(pc0.x >> 3, pc0.y >> 3, pc0.z >> 3))];
+    if (pptr >= GI_MARK) continue;
+    uint32_t pbit0 = (uint32_t)((pc0.x & 7) + 8 * (pc0.y & 7) + 64 * (pc0.z & 7));
+    uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+    const uint32_t *rp = v.rep + ptr * 512u + w * 32u;
+    while (word != 0u) {
+      uint32_t k = __ffs(word) - 1u;
+      word &= word - 1u;
+      uint32_t px = (k & 7u) >> 1, py = k >> 4;
+      mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
+      uint32_t rv = rp[k];
+      if (py == 0u) lo[px] = max(lo[px], rv); else hi[px] = max(hi[px], rv);
+    }
+    uint32_t wi = pptr * 16u + (pbit0 >> 5);
+    if ((v.occ[wi] & mask) != mask) atomicOr(&v.occ[wi], mask);
+#pragma unroll
+    for (uint32_t px = 0; px < 4u; px++)
+#pragma unroll
+      for (uint32_t py = 0; py < 2u; py++) {
+        uint32_t rv = py == 0u ? lo[px] : hi[px];
+        if (rv == 0u) continue;
+        uint32_t ri = pptr * 512u + pbit0 + px + 8u * py;
+        if (v.rep[ri] < rv) atomicMax(&v.rep[ri], rv);
+      }
+  }
+}
+
+// ---- allocVoxels (voxel.ts:579-588): attribute bases as an exclusive scan of the bricks' popcounts -------------------
+constexpr uint32_t VOX_CHUNK = 256;   // bricks per block
+
+__device__ __forceinline__ uint32_t brick_pop(const VoxDev &v, uint32_t b) {
+  const uint4 *o = reinterpret_cast<const uint4 *>(v.occ) + b * 4u;
+  uint32_t n = 0;
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    uint4 q = o[k];
+    n += __popc(q.x) + __popc(q.y) + __popc(q.z) + __popc(q.w);
+  }
+  return n;
+}
+
+__global__ void __launch_bounds__(256) k_count_voxels(VoxDev v) {
+  uint32_t nb = min(v.hdr[0], v.max_bricks);
+  uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
+  uint32_t c = b < nb ? brick_pop(v, b) : 0u;
+  uint32_t tot;
+  block_scan_256(c, &tot);
+  if (threadIdx.x == 0) v.scan[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks) {
+  uint32_t nb = min(v.hdr[0], v.max_bricks);
+  uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
+  uint32_t c = b < nb ? brick_pop(v, b) : 0u;
+  uint32_t tot;
+  uint32_t first = block_scan_256(c, &tot) + v.scan[blockIdx.x];
+  if (b < nb) {
+    if (first + c > v.max_voxels) { v.base[b] = GI_EMPTY; atomicAdd(&v.hdr[4], 1u); }
+    else v.base[b] = first;
+  }
+  if (blockIdx.x == nblocks - 1u && threadIdx.x == 255u) v.hdr[1] = first + c;
+}
+
+// closestBary (voxel.ts:250-267)
+__device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
+  f3 ab = b - a, ac = c - a, ap = p - a;
+  float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) return mk(1.0f, 0.0f, 0.0f);
+  f3 bp = p - b;
+  float d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) return mk(0.0f, 1.0f, 0.0f);
+  float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) { float w = d1 / (d1 - d3); return mk(1.0f - w, w, 0.0f); }
+  f3 cp = p - c;
+  float d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) return mk(0.0f, 0.0f, 1.0f);
+  float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) { float w = d2 / (d2 - d6); return mk(1.0f - w, 0.0f, w); }
+  float va = d3 * d6 - d5 * d4;
+  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    return mk(0.0f, 1.0f - w, w);
+  }
+  float dn = 1.0f / (va + vb + vc);
+  float vv = vb * dn, ww = vc * dn;
+  return mk(1.0f - vv - ww, vv, ww);
+}
+
+// resolveAttr (voxel.ts:596-620): one warp per brick.  The brick's occupied slots are compacted into shared memory
+// in rank order, so the lanes work on occupied voxels only and the attribute writes are contiguous.
+__global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
+  __shared__ uint16_t s_bits[8][512];
+  uint32_t lane = threadIdx.x & 31u, wl = threadIdx.x >> 5;
+  uint32_t nb = min(v.hdr[0], v.max_bricks);
+  uint32_t warps = gridDim.x * (blockDim.x >> 5);
+  for (uint32_t ptr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ptr < nb; ptr += warps) {
+    uint32_t first = v.base[ptr];
+    if (first == GI_EMPTY) continue;
+    uint32_t word = lane < 16u ? v.occ[ptr * 16u + lane] : 0u;
+    uint32_t pc = __popc(word), inc = pc;
+#pragma unroll
+    for (int d = 1; d < 16; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= (uint32_t)d) inc += y;
+    }
+    uint32_t excl = inc - pc;
+    uint32_t total = __shfl_sync(0xffffffffu, inc, 15);
+    for (uint32_t w = 0; w < 16u; w++) {
+      uint32_t ww = __shfl_sync(0xffffffffu, word, w);
+      uint32_t base_w = __shfl_sync(0xffffffffu, excl, w);
+      if ((ww >> lane) & 1u) s_bits[wl][base_w + __popc(ww & ((1u << lane) - 1u))] = (uint16_t)(w * 32u + lane);
+    }
+    __syncwarp();
+    uint32_t code = v.code[ptr];
+    uint32_t L = code >> 27;
+    i3 b = mki((int)((code >> 18) & 511u), (int)((code >> 9) & 511u), (int)(code & 511u));
+    float vs = vox_size(v, L);
+    f3 rl = region_lo(v, L);
+    for (uint32_t r = lane; r < total; r += 32u) {
+      uint32_t bit = s_bits[wl][r];
+      uint32_t ai = first + r;
+      i3 c = mki(b.x * 8 + (int)(bit & 7u), b.y * 8 + (int)((bit >> 3) & 7u), b.z * 8 + (int)(bit >> 6));
+      f3 p = rl + adds(vi2f(c), 0.5f) * vs;
+      uint32_t rv = v.rep[ptr * 512u + bit];
+      if (rv == 0u || rv > s.ntris) {   // no representative (cannot happen for a set bit): no attributes
+        v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f; v.sunvis[ai] = 1.0f;
+        continue;
+      }
+      Tri T = load_tri(s, rv - 1u);
+      const gi_material &m = s.mats[T.idx.w];
+      // surfaceAt(..., wantAttr = true) (voxel.ts:325-336), untextured
+      f3 wb = closest_bary(p, T.a, T.b, T.c);
+      f3 n0 = ld3(s.nrm[T.idx.x]), n1 = ld3(s.nrm[T.idx.y]), n2 = ld3(s.nrm[T.idx.z]);
+      f3 n = (n0 * wb.x + n1 * wb.y) + n2 * wb.z;
+      if (!(dot(n, n) > 1e-12f)) n = cross(T.b - T.a, T.c - T.a);
+      n = normalize3(n);
+      f3 q = (T.a * wb.x + T.b * wb.y) + T.c * wb.z;
+      float toon = (m.flags & 4u) ? 1.0f : 0.0f;
+      // octEnc (voxel.ts:590-594)
+      float sa = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
+      float ox = n.x / sa, oy = n.y / sa;
+      if (n.z < 0.0f) {
+        float tx = ox, ty = oy;
+        ox = (1.0f - fabsf(ty)) * (tx >= 0.0f ? 1.0f : -1.0f);
+        oy = (1.0f - fabsf(tx)) * (ty >= 0.0f ? 1.0f : -1.0f);
+      }
+      uint4 rec;
+      rec.x = pack4x8unorm(m.base_color[0], m.base_color[1], m.base_color[2], toon);
+      rec.y = pack2x16snorm(ox, oy);
+      rec.z = (uint32_t)f2h(m.emissive[0]) | ((uint32_t)f2h(m.emissive[1]) << 16);
+      rec.w = (uint32_t)f2h(m.emissive[2]);
+      v.attr[ai] = rec;
+      v.plane[ai] = dot(n, q - p);
+      v.sunvis[ai] = 1.0f;
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace gi
+
+using namespace gi;
+
+// The rebuild's launches (VOX_STAGES minus sun, voxel.ts:708), stream-ordered.
+cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_count, cudaStream_t st) {
+  uint32_t per = v.G * v.G * v.G, nptr = v.levels * per;
+  uint32_t persist = sm_count * 8u;   // 8 blocks of 256 threads per SM for the grid-stride passes
+  k_clear<<<min((nptr + 255u) / 256u + 1u, persist), 256, 0, st>>>(v);
+  uint32_t tb = (s.ntris + 255u) / 256u;
+  if (tb) k_mark_bricks<<<tb, 256, 0, st>>>(v, s);
+  k_mark_bricks_big<<<persist, 256, 0, st>>>(v, s);
+  if (v.levels > 1) k_mark_parents<<<min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, 0, st>>>(v);
+  uint32_t ab = (nptr + ALLOC_CHUNK - 1u) / ALLOC_CHUNK;
+  k_count_marks<<<ab, 256, 0, st>>>(v);
+  k_scan_sums<<<1, 256, 0, st>>>(v.scan, ab, v.hdr);
+  k_alloc_bricks<<<ab, 256, 0, st>>>(v);
+  if (tb) k_vox_bits<<<tb, 256, 0, st>>>(v, s);
+  k_vox_bits_big<<<persist, 256, 0, st>>>(v, s);
+  for (uint32_t L = 1; L < v.levels; L++) k_reduce<<<persist, 256, 0, st>>>(v, L);
+  uint32_t vb = (v.max_bricks + VOX_CHUNK - 1u) / VOX_CHUNK;
+  k_count_voxels<<<vb, 256, 0, st>>>(v);
+  k_scan_sums<<<1, 256, 0, st>>>(v.scan, vb, nullptr);
+  k_alloc_voxels<<<vb, 256, 0, st>>>(v, vb);
+  k_resolve_attr<<<persist, 256, 0, st>>>(v, s);
+  return cudaGetLastError();
+}

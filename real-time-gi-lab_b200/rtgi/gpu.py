@@ -1,0 +1,211 @@
+"""Host objects over the C-ABI: Context, SceneGpu (scene_gpu.ts uploadScene), VoxWorld (voxel.ts:710-727) and
+Rc (rc.ts:980-992).  Method names follow the reference (update, encode, readCounters, usedBytes, readCounts,
+setStats, destroy); errors raise GiError where the reference throws."""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from .configs import RcParams, VoxParams, cascade_layout
+from .scenes import Scene
+
+_P = C.c_void_p
+
+
+def _ptr(a: np.ndarray) -> int:
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be C-contiguous")
+    return a.ctypes.data
+
+
+def _stream(stream) -> Optional[int]:
+    """A cudaStream_t from None, an int, or a torch.cuda.Stream."""
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+class Context:
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = _P()
+        _lib.call("gi_ctx_create", device, C.byref(h))
+        self.handle = h
+        self.device = device
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_ctx_destroy", self.handle)
+            self.handle = None
+
+
+class SceneGpu:
+    """uploadScene (scene_gpu.ts:56): vertices, triangle table and materials in device memory."""
+
+    def __init__(self, ctx: Context, scene: Scene):
+        self.ctx = ctx
+        self.scene = scene
+        pos = np.ascontiguousarray(scene.positions, dtype=np.float32)
+        nrm = np.ascontiguousarray(scene.normals, dtype=np.float32)
+        tri = np.ascontiguousarray(scene.tri, dtype=np.uint32)
+        mats = scene.material_array()
+        h = _P()
+        _lib.call("gi_scene_upload", ctx.handle, _ptr(pos), _ptr(nrm), pos.shape[0], _ptr(tri), tri.shape[0],
+                  _ptr(mats), len(mats), C.byref(h))
+        self.handle = h
+
+    def update_vertices(self, first: int, pos: np.ndarray, nrm: np.ndarray, stream=None):
+        pos = np.ascontiguousarray(pos, dtype=np.float32)
+        nrm = np.ascontiguousarray(nrm, dtype=np.float32)
+        _lib.call("gi_scene_update_vertices", self.handle, first, pos.shape[0], _ptr(pos), _ptr(nrm), _stream(stream))
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_scene_destroy", self.handle)
+            self.handle = None
+
+
+class VoxWorld:
+    """createVoxWorld (voxel.ts:746) / VoxWorld (voxel.ts:710-727)."""
+
+    def __init__(self, scene: SceneGpu, params: VoxParams):
+        self.scene = scene
+        self.params = params
+        p = _lib.GiVoxParams(float(params.v0), params.levels, params.G, params.maxBricks, params.maxVoxels,
+                             params.dynBricks, 0)
+        h = _P()
+        _lib.call("gi_vox_create", scene.handle, C.byref(p), C.byref(h))
+        self.handle = h
+
+    def update(self, eye) -> None:
+        e = (C.c_double * 3)(*[float(x) for x in eye])
+        _lib.call("gi_vox_update", self.handle, e)
+
+    def encode(self, stream=None) -> None:
+        _lib.call("gi_vox_build", self.handle, _stream(stream))
+
+    def read_counters(self, stream=None) -> dict:
+        hdr = np.zeros(64, np.uint32)
+        _lib.call("gi_vox_read_counters", self.handle, _ptr(hdr), _stream(stream))
+        NL, mb = self.params.levels, self.params.maxBricks
+        return {"bricks": int(min(hdr[0], mb)), "voxels": int(hdr[1]), "brickOverflow": int(hdr[2]),
+                "bigOverflow": int(hdr[3]), "voxelOverflow": int(hdr[4]), "bricksPerLevel": [int(x) for x in hdr[8:8 + NL]],
+                "bigPerLevel": [int(x) for x in hdr[16:16 + NL]], "hdr": hdr}
+
+    def used_bytes(self) -> dict:
+        a, b = C.c_uint64(), C.c_uint64()
+        _lib.call("gi_vox_used_bytes", self.handle, C.byref(a), C.byref(b))
+        return {"persistent": a.value, "buildTemp": b.value}
+
+    def read_state(self, stream=None) -> dict:
+        p = self.params
+        per = p.G ** 3
+        st = {"ptr": np.zeros(p.levels * per, np.uint32), "occ": np.zeros(p.maxBricks * 16, np.uint32),
+              "base": np.zeros(p.maxBricks, np.uint32), "code": np.zeros(p.maxBricks, np.uint32),
+              "rep": np.zeros(p.maxBricks * 512, np.uint32), "attr": np.zeros(p.maxVoxels * 4, np.uint32),
+              "plane": np.zeros(p.maxVoxels, np.float32), "sunvis": np.zeros(p.maxVoxels, np.float32)}
+        _lib.call("gi_vox_read_state", self.handle, *[_ptr(st[k]) for k in ("ptr", "occ", "base", "code", "rep", "attr", "plane", "sunvis")],
+                  _stream(stream))
+        st["hdr"] = self.read_counters(stream)["hdr"]
+        return st
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_vox_destroy", self.handle)
+            self.handle = None
+
+
+ATLAS_CODES = {"f32": _lib.GI_ATLAS_F32, "f16": _lib.GI_ATLAS_F16, "bf16": _lib.GI_ATLAS_BF16}
+
+
+class Rc:
+    """createRc (rc.ts:1019) / Rc (rc.ts:980-992) for the screen method traced in the voxel world."""
+
+    def __init__(self, ctx: Context, params: RcParams, width: int, height: int):
+        if params.method != "screen" or params.world != "voxel" or params.depthCascades != 0:
+            raise _lib.GiError(_lib.GI_ERR_INVALID, f"unsupported configuration (method {params.method}, world "
+                               f"{params.world}, depthCascades {params.depthCascades}): this library runs screen "
+                               "probes traced in the voxel world (token 'voxel')")
+        if params.cascades > 8:
+            raise _lib.GiError(_lib.GI_ERR_INVALID, "at most 8 cascades")
+        self.ctx, self.params, self.width, self.height = ctx, params, width, height
+        self.layout = cascade_layout(params, width, height)
+        p = _lib.GiRcParams()
+        p.cascades, p.P, p.k_interval = params.cascades, params.P, params.kInterval
+        p.vox_scale, p.vox_offset, p.vox_skip, p.level_map = params.voxScale, params.voxOffset, params.voxSkip, params.levelMap
+        p.res_cap, p.dda_cap, p.stats, p.atlas = params.resCap, params.ddaCap, params.stats, ATLAS_CODES[params.atlas]
+        h = _P()
+        _lib.call("gi_rc_create", ctx.handle, C.byref(p), width, height, C.byref(h))
+        self.handle = h
+
+    def set_frame(self, frame: np.ndarray, stream=None):
+        frame = np.ascontiguousarray(frame, dtype=np.float32)
+        assert frame.size == 160
+        _lib.call("gi_rc_set_frame", self.handle, _ptr(frame), _stream(stream))
+
+    def set_gbuffer(self, depth: np.ndarray, normal: np.ndarray, stream=None):
+        depth = np.ascontiguousarray(depth, dtype=np.float32)
+        if normal.dtype == np.float16 or normal.dtype == np.uint16:
+            n16 = np.ascontiguousarray(normal).view(np.uint16)
+            _lib.call("gi_rc_set_gbuffer_f16", self.handle, _ptr(depth), _ptr(n16), _stream(stream))
+        else:
+            n32 = np.ascontiguousarray(normal, dtype=np.float32)
+            _lib.call("gi_rc_set_gbuffer", self.handle, _ptr(depth), _ptr(n32), _stream(stream))
+
+    def render_gbuffer(self, scene: SceneGpu, stream=None):
+        _lib.call("gi_rc_render_gbuffer", self.handle, scene.handle, _stream(stream))
+
+    def encode(self, vox: VoxWorld, stream=None):
+        _lib.call("gi_rc_solve", self.handle, vox.handle, _stream(stream))
+
+    def solve(self, vox: VoxWorld, stream=None):
+        """One frame of the GI path: the voxel rebuild, then the cascades."""
+        _lib.call("gi_solve", self.handle, vox.handle, _stream(stream))
+
+    def read_irradiance(self, stream=None) -> np.ndarray:
+        out = np.zeros((self.height, self.width, 4), np.float32)
+        _lib.call("gi_rc_read_irradiance", self.handle, _ptr(out), _stream(stream))
+        return out
+
+    def read_counts(self, stream=None) -> np.ndarray:
+        out = np.zeros(80, np.uint32)
+        _lib.call("gi_rc_read_counts", self.handle, _ptr(out), _stream(stream))
+        return out
+
+    def set_stats(self, level: int):
+        _lib.call("gi_rc_set_stats", self.handle, level)
+        self.params.stats = level
+
+    def set_debug_hits(self, on: bool):
+        _lib.call("gi_rc_set_debug_hits", self.handle, 1 if on else 0)
+
+    def bytes(self) -> int:
+        b = C.c_uint64()
+        _lib.call("gi_rc_bytes", self.handle, C.byref(b))
+        return b.value
+
+    def read_buffer(self, what: int, stream=None) -> np.ndarray:
+        n = C.c_size_t()
+        _lib.call("gi_rc_buffer_bytes", self.handle, what, C.byref(n))
+        out = np.zeros(n.value, np.uint8)
+        _lib.call("gi_rc_read_buffer", self.handle, what, _ptr(out), n.value, _stream(stream))
+        return out
+
+    def read_atlas(self, what: int = _lib.GI_RC_RAD, stream=None) -> np.ndarray:
+        """The atlas (or SH) as f32 values, (n, 4)."""
+        raw = self.read_buffer(what, stream)
+        if self.params.atlas == "f32":
+            return raw.view(np.float32).reshape(-1, 4)
+        if self.params.atlas == "f16":
+            return raw.view(np.float16).astype(np.float32).reshape(-1, 4)
+        return (raw.view(np.uint16).astype(np.uint32) << 16).view(np.float32).reshape(-1, 4)
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_rc_destroy", self.handle)
+            self.handle = None

@@ -1,0 +1,75 @@
+"""Parity cases shared by the tests: the two benchmark configurations plus lit and overflow variants that make every
+branch of the path carry non-zero values (config 0's two cascades stop short of its lamp, so its irradiance is 0)."""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from rtgi import configs, frame as fr, scenes
+
+
+@dataclass
+class Case:
+    name: str
+    scene: scenes.Scene
+    width: int
+    height: int
+    vox: configs.VoxParams
+    rc: configs.RcParams
+    frame: np.ndarray = field(default=None)
+
+
+def _frame(scene, W, H, p: configs.RcParams, sun_e=None, sky=None):
+    return fr.pack_frame(fr.FrameParams(cam=scene.camera, width=W, height=H, sun_dir=scene.sun_dir,
+                                        sun_e=scene.sun_e if sun_e is None else sun_e,
+                                        sky=scene.sky if sky is None else sky, cascades=p.cascades, P=p.P,
+                                        s_min=p.sMin, lift=p.lift))
+
+
+def config0(atlas: str = "f32") -> Case:
+    """Room of 200 boxes, 1 level of 64^3 voxels of 0.16 m, 256x256, 2 cascades, DDA cap 64."""
+    s = scenes.room_scene(0)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda64", {"cascades": 2})
+    v = configs.vox_params({"v0": 0.16, "levels": 1, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 18})
+    c = Case("config0", s, 256, 256, v, p)
+    c.frame = _frame(s, 256, 256, p)
+    return c
+
+
+def config1(atlas: str = "f32", width: int = 1920, height: int = 1080) -> Case:
+    """Colonnade of ~260k triangles, 4 levels of 128^3 voxels from 0.1 m, 1920x1080, 5 cascades, DDA cap 256."""
+    s = scenes.colonnade_scene(0)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": 5})
+    v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
+    c = Case("config1", s, width, height, v, p)
+    c.frame = _frame(s, width, height, p)
+    return c
+
+
+def room_lit(atlas: str = "f16") -> Case:
+    """The room under sun and sky, 3 levels (reduce, voxLevelFor), 5 cascades (merge of every kind)."""
+    s = scenes.room_scene(0)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": 5})
+    v = configs.vox_params({"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 8192, "maxVoxels": 1 << 20})
+    c = Case("room_lit", s, 320, 240, v, p)
+    c.frame = _frame(s, 320, 240, p, sun_e=fr.SUN_E, sky=fr.SKY)
+    return c
+
+
+def leak(t: float = 0.1, atlas: str = "bf16") -> Case:
+    """The reference's leak room (scenes.ts:261) with its recorded voxel parameters, 5 cascades, sun and sky."""
+    s = scenes.leak_room(t)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}", {"cascades": 5})
+    v = configs.vox_params({"v0": 0.1, "levels": 5, "G": 64, "maxBricks": 32768, "maxVoxels": 4194304})
+    c = Case(f"leak-{t}", s, 320, 180, v, p)
+    c.frame = _frame(s, 320, 180, p, sun_e=fr.SUN_E, sky=fr.SKY)
+    return c
+
+
+def overflow(atlas: str = "f32") -> Case:
+    """room_lit with pools too small: dropped bricks (read at the coarser level) and voxels without attributes."""
+    c = room_lit(atlas)
+    c.name = "overflow"
+    c.vox = configs.vox_params({"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 300, "maxVoxels": 20000})
+    return c

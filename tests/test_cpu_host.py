@@ -1,0 +1,188 @@
+"""CPU-only checks: the C-ABI library loads and exports every symbol include/gi.h declares, the host mirror of the
+reference's frame math and config grammar, and the oracle's builtins against their specifications."""
+import ctypes as C
+import math
+import os
+import re
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+from oracle import bind
+from rtgi import _lib, configs, frame as fr, mathx, scenes
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "gi.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:int|const char \*)\s*(gi_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    syms = header_symbols()
+    assert len(syms) >= 30
+    for s in syms:
+        assert hasattr(lib, s), f"{s} declared in gi.h but not exported"
+        assert s in _lib.SIGNATURES, f"{s} has no ctypes signature"
+    assert set(_lib.SIGNATURES) == set(syms)
+    assert lib.gi_version() == 1
+    assert lib.gi_status_string(-1) == b"invalid argument"
+
+
+def test_no_device_is_an_error_not_a_fallback():
+    # without a GPU the context cannot be made; the call returns a status, it does not run anything on the CPU
+    lib = _lib.load()
+    h = C.c_void_p()
+    st = lib.gi_ctx_create(0, C.byref(h))
+    try:
+        import torch
+        has_gpu = torch.cuda.is_available()
+    except Exception:
+        has_gpu = False
+    if has_gpu:
+        assert st == 0
+        lib.gi_ctx_destroy(h)
+    else:
+        assert st in (_lib.GI_ERR_CUDA, _lib.GI_ERR_INVALID)
+        assert lib.gi_last_error()
+
+
+def test_null_arguments_are_rejected():
+    lib = _lib.load()
+    assert lib.gi_ctx_create(0, None) == _lib.GI_ERR_INVALID
+    assert lib.gi_vox_build(None, None) == _lib.GI_ERR_INVALID
+    assert b"NULL" in lib.gi_last_error()
+    assert lib.gi_rc_solve(None, None, None) == _lib.GI_ERR_INVALID
+
+
+def test_parse_config_grammar():
+    p = configs.parse_config("screen-8-voxel-rc2-vs0.5-vo2-vk0.25-l2-dda64-bf16")
+    assert (p.method, p.P, p.world, p.depthCascades, p.resCap) == ("screen", 8, "voxel", 0, 2)
+    assert (p.voxScale, p.voxOffset, p.voxSkip, p.levelMap, p.ddaCap, p.atlas) == (0.5, 2.0, 0.25, 2, 64, "bf16")
+    assert configs.parse_config("world-32").world == "none"
+    assert configs.parse_config("screen-8-hybrid").depthCascades == 1
+    with pytest.raises(ValueError, match="unknown config token"):
+        configs.parse_config("screen-8-bogus")
+    with pytest.raises(ValueError, match="unknown voxel parameter"):
+        configs.vox_params({"v1": 0.1})
+    assert configs.vox_params({"G": 16}).G == 16 and configs.DEFAULT_VOX.G == 32
+
+
+def test_cascade_layout_config1():
+    p = configs.parse_config("screen-8-voxel", {"cascades": 5})
+    lay = configs.cascade_layout(p, 1920, 1080)
+    tiles = [(c["tiles_x"], c["tiles_y"]) for c in lay["casc"]]
+    assert tiles == [(240, 135), (120, 68), (60, 34), (30, 17), (15, 9)]
+    assert [c["res"] for c in lay["casc"]] == [4, 8, 16, 32, 64]
+    assert [(c["b0"], c["b1"]) for c in lay["casc"]][:3] == [(0.0, 1.0), (1.0, 5.0), (5.0, 21.0)]
+    assert lay["rays_total"] == 2638080
+
+
+def test_v8_hypot_and_matrices():
+    assert mathx.hypot(3, 4) == 5.0
+    assert mathx.hypot(0, 0, 0) == 0.0
+    cam = fr.Camera((2.6, 1.6, 1.8), (0.2, 1.0, -1.4), 75, 0.05)
+    m = fr.camera_matrices(cam, 1920, 1080)
+    vp = np.array(m["viewProj"], np.float64).reshape(4, 4).T
+    ivp = np.array(m["invViewProj"], np.float64).reshape(4, 4).T
+    assert np.allclose(vp @ ivp, np.eye(4), atol=1e-5)
+    # the near plane maps to depth 1, the eye looks along fwd
+    p = np.array([*np.add(cam.eye, np.multiply(m["fwd"], 0.05)), 1.0])
+    c = vp @ p
+    assert abs(c[2] / c[3] - 1.0) < 1e-4
+
+
+def test_pack_frame_layout():
+    cam = fr.Camera((1.0, 2.0, 3.0), (0.0, 2.0, 0.0), 60, 0.1)
+    F = fr.pack_frame(fr.FrameParams(cam=cam, width=640, height=360, cascades=3, P=8, sun_dir=(0, 2, 0)))
+    u = F.view(np.uint32)
+    assert F.size == 160 and F.dtype == np.float32
+    assert list(F[80:84]) == [1.0, 2.0, 3.0, np.float32(0.1)]
+    assert list(F[88:91]) == [0.0, 1.0, 0.0]
+    assert list(F[100:104]) == [640, 360, np.float32(1 / 640), np.float32(1 / 360)]
+    assert F[105] == np.float32(2 * math.tan(math.pi / 6) / 360)
+    assert u[112] == 3
+    assert abs(F[120:136].sum() - 4 * math.pi) < 1e-4   # octSolidAngles covers the sphere
+
+
+def test_oct_solid_angles_symmetry():
+    w = fr.oct_solid_angles(4)
+    assert np.allclose(w.reshape(4, 4), w.reshape(4, 4)[::-1, ::-1], rtol=1e-3)
+    assert abs(w.sum() - 4 * math.pi) < 1e-4
+
+
+def test_pack_builtins_known_answers():
+    lib = bind.lib()
+    # WGSL: pack4x8unorm(e) = floor(0.5 + 255 * clamp(e, 0, 1)) per byte, x lowest
+    v = (C.c_float * 4)(0.0, 1.0, 0.5, 2.0)
+    assert lib.orc_pack4x8unorm(v) == (0 | (255 << 8) | (128 << 16) | (255 << 24))
+    # pack2x16snorm: floor(0.5 + 32767 * clamp(e, -1, 1)) as i16
+    assert lib.orc_pack2x16snorm(1.0, -1.0) == (32767 | ((-32767 & 0xffff) << 16))
+    assert lib.orc_pack2x16snorm(0.0, -0.5) == (0 | ((-16383 & 0xffff) << 16))
+
+
+def test_f16_bf16_conversions_match_numpy():
+    lib = bind.lib()
+    rng = np.random.default_rng(1)
+    xs = np.concatenate([rng.standard_normal(2000) * 10, rng.standard_normal(500) * 1e-5, [65504, 65520, 1e6, -0.0, 6e-8]]).astype(np.float32)
+    for x in xs:
+        h = lib.orc_f32_to_f16(float(x))
+        assert h == np.float16(x).view(np.uint16), x
+        assert lib.orc_f16_to_f32(h) == np.float32(np.float16(x)) or math.isnan(x)
+
+
+def _sat_exact(c, h, a, b, cc):
+    """Separating-axis test in exact rationals: does the closed box (c, h) meet the triangle?"""
+    F = lambda v: [Fraction(float(x)) for x in v]
+    c, h, a, b, cc = F(c), F(h), F(a), F(b), F(cc)
+    v = [[a[i] - c[i] for i in range(3)], [b[i] - c[i] for i in range(3)], [cc[i] - c[i] for i in range(3)]]
+    e = [[v[1][i] - v[0][i] for i in range(3)], [v[2][i] - v[1][i] for i in range(3)], [v[0][i] - v[2][i] for i in range(3)]]
+    axes = [[1, 0, 0], [0, 1, 0], [0, 0, 1]]
+    cr = lambda p, q: [p[1] * q[2] - p[2] * q[1], p[2] * q[0] - p[0] * q[2], p[0] * q[1] - p[1] * q[0]]
+    axes.append(cr(e[0], e[1]))
+    for ei in e:
+        for u in ([1, 0, 0], [0, 1, 0], [0, 0, 1]):
+            axes.append(cr(u, ei))
+    for ax in axes:
+        p = [sum(vi[k] * ax[k] for k in range(3)) for vi in v]
+        r = sum(h[k] * abs(ax[k]) for k in range(3))
+        if min(p) > r or max(p) < -r:
+            return False
+    return True
+
+
+def test_tri_box_against_exact_separating_axes():
+    lib = bind.lib()
+    rng = np.random.default_rng(7)
+    agree = 0
+    n = 3000
+    for _ in range(n):
+        c = rng.uniform(-1, 1, 3).astype(np.float32)
+        h = np.full(3, rng.uniform(0.05, 0.5), np.float32)
+        tri = (c + rng.uniform(-1, 1, (3, 3)) * rng.uniform(0.1, 2.0)).astype(np.float32)
+        args = [np.ascontiguousarray(x, np.float32) for x in (c, h, tri[0], tri[1], tri[2])]
+        got = lib.orc_tri_box(*[x.ctypes.data for x in args])
+        agree += int(bool(got) == _sat_exact(*args))
+    assert agree >= n - 3   # f32 rounding may flip grazing contacts only
+
+
+def test_round_log2_exact():
+    lib = bind.lib()
+    for x in [1.0, 1.4142135, 1.4142137, 0.7071067, 0.7071068, 3.0, 0.1, 1e-3, 1234.5]:
+        r = np.int32(np.uint32(lib.orc_round_log2(x)))
+        assert r == round(math.log2(np.float32(x))), x
+
+
+def test_scenes_shapes():
+    s = scenes.room_scene(0)
+    assert s.triangle_count == 12 + 2 + 200 * 12
+    assert s.tri[:, 3].max() < len(s.materials)
+    c = scenes.colonnade_scene(0)
+    assert 255_000 < c.triangle_count < 265_000
+    assert scenes.leak_room(0.1).triangle_count == 1212
+    # Builder quads: face normal = normalize(cross(b - a, c - a)) per vertex
+    n = s.normals[s.tri[0, 0]]
+    assert abs(np.linalg.norm(n) - 1) < 1e-6

@@ -1,0 +1,96 @@
+"""Parity of the CUDA path (through the C-ABI) with the oracle, on the same inputs.
+
+Bar: voxel state, G-buffer and DDA hit cells bit-exact; traced radiance, merged atlas and irradiance within 1e-4
+relative in f32 (f16/bf16 atlases: within one rounding step of the stored type, because the oracle rounds at the
+same points and only expf may differ by an ulp before the rounding)."""
+import numpy as np
+import pytest
+
+import gi_cases
+from oracle import bind
+from rtgi import _lib, gpu
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = gpu.Context(0)
+    yield c
+    c.destroy()
+
+
+def _tol(atlas):
+    return {"f32": 1e-4, "f16": 2.0 ** -10, "bf16": 2.0 ** -7}[atlas]
+
+
+def _close(a, b, rel, what):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    bad = np.abs(a - b) > rel * np.abs(b) + 1e-6
+    assert not bad.any(), f"{what}: {bad.sum()} of {bad.size} differ; first {np.argwhere(bad)[:3].tolist()} " \
+                          f"gpu {a[bad][:3]} oracle {b[bad][:3]}"
+
+
+def run_gpu(ctx, case, debug=True):
+    sg = gpu.SceneGpu(ctx, case.scene)
+    vw = gpu.VoxWorld(sg, case.vox)
+    rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    rc.set_frame(case.frame)
+    rc.render_gbuffer(sg)
+    vw.update(case.scene.camera.eye)
+    rc.set_debug_hits(debug)
+    rc.solve(vw)
+    res = {"vox": vw.read_state(), "irr": rc.read_irradiance(), "counts": rc.read_counts(),
+           "depth": rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width),
+           "normal": rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4),
+           "probes": rc.read_buffer(_lib.GI_RC_PROBES).view(bind.PROBE_DTYPE),
+           "rad": rc.read_atlas(_lib.GI_RC_RAD), "sh": rc.read_atlas(_lib.GI_RC_SH)}
+    if debug:
+        res["hits"] = rc.read_buffer(_lib.GI_RC_HITS).view(np.uint32).reshape(-1, 4)
+        res["rad_traced"] = rc.read_atlas(_lib.GI_RC_RAD_TRACED)
+    for h in (rc, vw, sg):
+        h.destroy()
+    return res
+
+
+def run_oracle(case, depth, normal):
+    v = case.vox
+    st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+    lay = dict(gi_cases.configs.cascade_layout(case.rc, case.width, case.height))
+    out = bind.rc_solve(st, lay, case.frame, depth, normal, want_hit=True)
+    return st, out
+
+
+CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_cases.leak,
+         "overflow": gi_cases.overflow, "config1": gi_cases.config1}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_parity(ctx, name):
+    case = CASES[name]()
+    g = run_gpu(ctx, case)
+    # G-buffer: the GPU raster against the oracle's, bit for bit
+    depth, normal, _ = bind.raster_gbuffer(case.scene, case.frame, case.width, case.height)
+    assert np.array_equal(g["depth"].view(np.uint32), depth.view(np.uint32)), "G-buffer depth differs"
+    assert np.array_equal(g["normal"].astype(np.float32), normal), "G-buffer normal differs"
+    st, o = run_oracle(case, depth, normal)
+    # voxel world: every counter and every allocated word
+    gv = g["vox"]
+    assert np.array_equal(gv["hdr"], st["hdr"]), f"counters differ: {gv['hdr'][:32]} vs {st['hdr'][:32]}"
+    nb = int(min(st["hdr"][0], case.vox.maxBricks))
+    nv = int(min(st["hdr"][1], case.vox.maxVoxels))
+    assert np.array_equal(gv["ptr"], st["ptr"]), "brick pointers differ"
+    for k, n in (("occ", nb * 16), ("base", nb), ("code", nb), ("rep", nb * 512)):
+        assert np.array_equal(gv[k][:n], st[k][:n]), f"{k} differs"
+    assert np.array_equal(gv["attr"][:nv * 4], st["attr"][:nv * 4]), "voxel attributes differ"
+    assert np.array_equal(gv["plane"][:nv].view(np.uint32), st["plane"][:nv].view(np.uint32)), "plane offsets differ"
+    # probes and DDA hits
+    assert np.array_equal(g["probes"].view(np.uint32), o["probes"].view(np.uint32)), "probes differ"
+    assert np.array_equal(g["hits"], o["hit"]), f"DDA hits differ at {np.argwhere((g['hits'] != o['hit']).any(1))[:5].ravel()}"
+    tol = _tol(case.rc.atlas)
+    _close(g["rad_traced"], o["rad_traced"], tol, "traced radiance")
+    _close(g["rad"], o["rad"], tol, "merged atlas")
+    _close(g["sh"].reshape(-1)[: o["sh"].size], o["sh"].reshape(-1), tol, "SH")
+    _close(g["irr"], o["irr"], tol, "irradiance")
+    assert np.array_equal(g["counts"][:8], o["counts"][:8])
