@@ -1,0 +1,363 @@
+#!/usr/bin/env python
+"""GI solves/s of the B200 path on the large procedural workload (the colonnade: ~260k triangles, a clipmap of
+4 levels of 128^3 voxels from 0.1 m, 5 radiance cascades at 1920x1080, DDA capped at 256 steps, f32 atlases).
+
+A step is one GI solve: the voxel clipmap rebuild from the triangles (voxel.ts VOX_STAGES) and the cascades
+(giBuild setupScreen, giTrace, giMerge + projectSH, giGather), replayed from one captured CUDA graph.  Inputs (scene,
+frame, G-buffer) are resident in HBM; L2 is flushed (a 256 MiB write) between steps, outside the step's events.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload colonnade|room]
+
+One process per GPU (torchrun for N > 1); every rank solves its own replica (no data-path collective), the job's
+value is all ranks' solves over the slowest rank's device time.  Rank 0 prints one JSON line.
+``--impl reference`` times the reference's algorithm on the host cores instead: the reference itself (TypeScript +
+WGSL through Dawn) cannot run here, so its CPU restatement (oracle/) runs with every host thread.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "real-time-gi-lab_b200"))
+
+import numpy as np
+
+METRIC = "GI solves/s & p99 ms (served batch vs plain), DDA steps/s, % HBM roofline"
+
+
+def workload(name):
+    from rtgi import configs, frame as fr, scenes
+    if name == "colonnade":
+        s = scenes.colonnade_scene(0)
+        W, H = 1920, 1080
+        p = configs.parse_config("screen-8-voxel-f32-dda256", {"cascades": 5})
+        v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
+        sun_e, sky = s.sun_e, s.sky
+    else:
+        s = scenes.room_scene(0)
+        W, H = 256, 256
+        p = configs.parse_config("screen-8-voxel-f32-dda64", {"cascades": 2})
+        v = configs.vox_params({"v0": 0.16, "levels": 1, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 18})
+        sun_e, sky = (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
+    F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=sun_e, sky=sky,
+                                     cascades=p.cascades, P=p.P))
+    desc = {"workload": f"{name}: {s.triangle_count} triangles, clipmap {v.levels} x {v.G * 8}^3 voxels from "
+                        f"{v.v0} m, {p.cascades} cascades at {W}x{H}, DDA cap {p.ddaCap}, atlas {p.atlas}",
+            "triangles": s.triangle_count, "resolution": [W, H], "cascades": p.cascades, "levels": v.levels,
+            "G": v.G, "v0": v.v0, "dda_cap": p.ddaCap, "atlas": p.atlas, "method": "screen-8-voxel"}
+    return s, W, H, p, v, F, desc
+
+
+class ClockSampler:
+    """nvidia-smi samples of the SM clock and throttle reasons while the timed region runs."""
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device, self.proc, self.path = device, None, None
+
+    def start(self):
+        try:
+            import tempfile
+            self.path = tempfile.mktemp(suffix=".csv")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self, t0=None, t1=None):
+        """Summary of the samples taken between wall-clock times t0 and t1 (all samples when none fall there)."""
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [l.split(", ") for l in open(self.path).read().strip().splitlines() if l.strip()]
+        os.unlink(self.path)
+        if t0 is not None:
+            import datetime
+            def ts(r):
+                try:
+                    return datetime.datetime.strptime(r[0].strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                except Exception:
+                    return None
+            inside = [r for r in rows if ts(r) is not None and t0 <= ts(r) <= t1]
+            if inside:
+                rows = inside
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows if r[2].replace(".", "").isdigit())
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, n in enumerate(names):
+                if len(r) > 5 + k and r[5 + k].strip().lower() == "active":
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def measured_peak():
+    try:
+        m = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        return float(m["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(name):
+    """DRAM bytes per launch of the trace kernel from the committed ncu summary (profiles/), or None."""
+    p = os.path.join(ROOT, "profiles", f"ncu_trace_{name}.txt")
+    if not os.path.exists(p):
+        return None
+    for line in open(p):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1])
+    return None
+
+
+def trace_algorithmic_bytes(rc_layout, hdr, vox):
+    """Compulsory bytes of one giTrace launch: probes read (48 B each), the atlas written (16 B per ray in f32), the
+    clipmap read once (brick pointers, occupancy + first attribute per brick, 16-byte attribute record + sun
+    visibility per voxel)."""
+    nb = int(min(hdr[0], vox.maxBricks))
+    nv = int(min(hdr[1], vox.maxVoxels))
+    elem = 16 if rc_layout["atlas"] == 0 else 8
+    return (48 * rc_layout["probes_total"] + elem * rc_layout["rays_total"] + 4 * vox.levels * vox.G ** 3
+            + 68 * nb + 20 * nv)
+
+
+def cpu_solve_once(bind, s, v, lay, F, depth, normal):
+    st = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, s.camera.eye)
+    bind.rc_solve(st, lay, F, depth, normal)
+
+
+def cpu_baseline(s, v, p, F, depth, normal, budget_s=12.0, min_solves=2):
+    """The oracle (a CPU restatement of the reference's shaders) timed on this host's cores, bounded sample."""
+    from oracle import bind
+    from rtgi import configs
+    lay = configs.cascade_layout(p, depth.shape[1], depth.shape[0])
+    cpu_solve_once(bind, s, v, lay, F, depth, normal)   # warm
+    n, t0 = 0, time.perf_counter()
+    while n < min_solves or time.perf_counter() - t0 < budget_s:
+        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+        n += 1
+    dt = time.perf_counter() - t0
+    cores = int(os.environ.get("ORC_THREADS", os.cpu_count() or 1))
+    return {"value": n / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": f"{n} full solves of the workload (voxel rebuild + setup/trace/merge/SH/gather; voxel passes "
+                      f"single-threaded, ray/pixel loops on {cores} threads) in {dt:.1f} s"}
+
+
+def run_reference(args, rank):
+    """The reference's algorithm on the host cores (oracle/), on the same workload, config and metric."""
+    if rank != 0:
+        return
+    from oracle import bind
+    from rtgi import configs
+    s, W, H, p, v, F, desc = workload(args.workload)
+    depth, normal, _ = bind.raster_gbuffer(s, F, W, H)   # input, not timed
+    lay = configs.cascade_layout(p, W, H)
+    for _ in range(args.warmup):
+        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+    # a bounded sample: at most ~90 s of solves
+    t_one = time.perf_counter()
+    cpu_solve_once(bind, s, v, lay, F, depth, normal)
+    t_one = time.perf_counter() - t_one
+    k = max(1, min(args.steps, int(90.0 / max(t_one, 1e-3))))
+    times = []
+    for _ in range(k):
+        t0 = time.perf_counter()
+        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    value = k / total
+    cores = int(os.environ.get("ORC_THREADS", os.cpu_count() or 1))
+    times.sort()
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": k, "warmup": args.warmup, "ms_per_step": 1000 * total / k, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene)",
+            "config": {**desc, "parallelism": "host threads"},
+            "p50_ms": 1000 * times[len(times) // 2], "p99_ms": 1000 * times[min(len(times) - 1, int(0.99 * len(times)))],
+            "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"{k} of the requested {args.steps} steps (each one full solve; bounded to ~90 s); "
+                                       "the reference itself (WGSL through Dawn on Node) cannot run on this host"},
+            "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    from rtgi import _lib, configs, gpu
+
+    s, W, H, p, v, F, desc = workload(args.workload)
+    stream = torch.cuda.Stream()
+    ctx = gpu.Context(local_rank)
+    sg = gpu.SceneGpu(ctx, s)
+    vw = gpu.VoxWorld(sg, v)
+    rc = gpu.Rc(ctx, p, W, H)
+    with torch.cuda.stream(stream):
+        rc.set_frame(F, stream)
+        rc.render_gbuffer(sg, stream)
+        vw.update(s.camera.eye)
+        # DDA work of one solve (steps counted as rc.ts:232-235)
+        rc.set_stats(1)
+        rc.solve(vw, stream)
+        counts = rc.read_counts(stream)
+        rc.set_stats(0)
+        hdr = vw.read_counters(stream)["hdr"]
+        steps_per_solve = int(counts[32:32 + p.cascades].sum())
+        at_cap = int(counts[64:64 + p.cascades].sum())
+        # per-pass times and the trace kernel's live duration (events between the passes)
+        rc.set_timing(True)
+        pass_ms = {k: [] for k in rc.PASSES}
+        for _ in range(max(5, args.warmup)):
+            rc.solve(vw, stream)
+            for k, x in rc.pass_times().items():
+                pass_ms[k].append(x)
+        rc.set_timing(False)
+        rc.graph_capture(vw, stream)
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        for _ in range(args.warmup):
+            flush.zero_()
+            rc.graph_launch(stream)
+        stream.synchronize()
+    n_ev = args.steps
+    ev_s = [torch.cuda.Event(enable_timing=True) for _ in range(n_ev)]
+    ev_e = [torch.cuda.Event(enable_timing=True) for _ in range(n_ev)]
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    time.sleep(0.5)   # nvidia-smi is sampling before the timed region starts
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    unix0 = time.time()
+    with torch.cuda.stream(stream):
+        for k in range(n_ev):
+            flush.zero_()
+            ev_s[k].record(stream)
+            rc.graph_launch(stream)
+            ev_e[k].record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    wall = time.perf_counter() - wall0
+    clk = clocks.stop(unix0, unix0 + wall)
+    step_ms = [a.elapsed_time(b) for a, b in zip(ev_s, ev_e)]
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    max_total = float(t.item())
+    value = world * n_ev / (max_total / 1000.0)
+
+    # end to end through the C-ABI with host buffers: frame + G-buffer H2D from pinned memory, solve, irradiance D2H
+    depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
+    normal_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_NORMAL).view(np.uint16).copy()).pin_memory()
+    frame_h = torch.from_numpy(F.copy()).pin_memory()
+    irr_h = torch.empty(rc.irr_bytes(), dtype=torch.uint8).pin_memory()
+    n_e2e = max(3, min(n_ev, 200))
+    with torch.cuda.stream(stream):
+        for _ in range(3):
+            rc.set_frame_ptr(frame_h.data_ptr(), stream)
+            rc.set_gbuffer_ptrs(depth_h.data_ptr(), normal_h.data_ptr(), stream)
+            rc.graph_launch(stream)
+            rc.read_irradiance_raw_ptr(irr_h.data_ptr(), stream)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = time.perf_counter()
+        for _ in range(n_e2e):
+            rc.set_frame_ptr(frame_h.data_ptr(), stream)
+            rc.set_gbuffer_ptrs(depth_h.data_ptr(), normal_h.data_ptr(), stream)
+            rc.graph_launch(stream)
+            rc.read_irradiance_raw_ptr(irr_h.data_ptr(), stream)   # synchronises the stream
+        torch.cuda.synchronize()
+        e2e_s = time.perf_counter() - e0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    e2e_value = world * n_e2e / float(te.item())
+
+    trace_ms = statistics.mean(pass_ms["giTrace"])
+    alg = trace_algorithmic_bytes(rc.layout, hdr, v)
+    peak, peak_kind = measured_peak()
+    achieved = alg / (trace_ms / 1000.0) / 1e9
+    traffic = ncu_traffic(args.workload)
+    step_sorted = sorted(step_ms)
+    out = None
+    if rank == 0:
+        out = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": n_ev,
+               "warmup": args.warmup, "ms_per_step": max_total / n_ev, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded procedural scene, no dataset)",
+               "config": {**desc, "parallelism": f"replicas x{world} (one solve stream per GPU)",
+                          "l2": "flushed between steps (256 MiB write outside the step events)",
+                          "timing": "CUDA events per step on the solve stream, max over ranks"},
+               "p50_ms": step_sorted[len(step_sorted) // 2],
+               "p99_ms": step_sorted[min(len(step_sorted) - 1, int(math.ceil(0.99 * len(step_sorted))) - 1)],
+               "dda_steps_per_solve": steps_per_solve, "dda_at_cap": at_cap,
+               "dda_steps_per_s": steps_per_solve * value,
+               "passes_ms": {k: statistics.median(x) for k, x in pass_ms.items()},
+               "vox_counters": {"bricks": int(min(hdr[0], v.maxBricks)), "voxels": int(hdr[1]),
+                                "bricksPerLevel": [int(x) for x in hdr[8:8 + v.levels]]},
+               "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                            "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
+                            "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": trace_ms},
+               "e2e": {"value": e2e_value, "unit": "solves/s",
+                       "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
+                       "d2h_bytes_per_step": int(irr_h.numel())},
+               "gpu_launches": n_ev * (13 + (v.levels - 1) + 4 + p.cascades),
+               "clocks": clk, "wall_s": wall}
+    # the oracle on the host cores, rank 0 at N = 1 only
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(s, v, p, F, depth_h.numpy().reshape(H, W),
+                                           normal_h.numpy().view(np.float16).reshape(H, W, 4).astype(np.float32))
+    for h in (rc, vw, sg, ctx):
+        h.destroy()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="colonnade", choices=["colonnade", "room"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args, rank)
+    else:
+        run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

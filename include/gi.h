@@ -148,6 +148,17 @@ int gi_rc_read_irradiance_raw(gi_rc *rc, void *out, size_t bytes, void *stream);
 int gi_rc_read_counts(gi_rc *rc, uint32_t counts[80], void *stream);
 /* setStats (rc.ts:1233): 0 off, 1 DDA step counters. */
 int gi_rc_set_stats(gi_rc *rc, uint32_t level);
+/* CUDA graph of one gi_solve(rc, vox) captured on `stream` (not the legacy default stream), replayed by
+ * gi_rc_graph_launch.  The graph reads the frame, G-buffer and scene vertices from their device buffers at replay, so
+ * gi_rc_set_frame / gi_rc_set_gbuffer* / gi_scene_update_vertices before a launch take effect; the voxel windows
+ * (gi_vox_update) and the parameters are those of capture time: capture again after moving the windows. */
+int gi_rc_graph_capture(gi_rc *rc, gi_vox *vox, void *stream);
+int gi_rc_graph_launch(gi_rc *rc, void *stream);
+/* Pass timing (the reference's per-pass timestamps, rcrun.ts:325-372): when on, every solve records CUDA events
+ * between its passes; gi_rc_pass_times then gives the last solve's milliseconds of [vox (gi_solve only), giBuild,
+ * giTrace, giMerge, giGather] (synchronises on the last event). */
+int gi_rc_set_timing(gi_rc *rc, int on);
+int gi_rc_pass_times(gi_rc *rc, float ms[5]);
 /* Bytes of device memory the handle holds (rc.ts `bytes`). */
 int gi_rc_bytes(gi_rc *rc, uint64_t *bytes);
 

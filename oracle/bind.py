@@ -133,7 +133,7 @@ def vox_build(scene, v0: float, levels: int, G: int, max_bricks: int, max_voxels
     vx.v0 = np.float32(v0)
     vx.levels, vx.G, vx.max_bricks, vx.max_voxels, vx.big_cap = levels, G, max_bricks, max_voxels, big_cap
     vx.coarse_from_triangles = 1 if coarse_from_triangles else 0
-    org = vox_origins(float(np.float32(v0)), levels, G, eye)
+    org = vox_origins(float(v0), levels, G, eye)   # f64 v0, as the reference's numbers (voxel.ts:873)
     for L in range(8):
         for a in range(4):
             vx.origin[L][a] = int(org[L, a])

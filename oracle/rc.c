@@ -379,7 +379,7 @@ static void merge_range(void *p, uint64_t b, uint64_t e) {
           if (qp->pos[3] <= 0.0f) continue;
           float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
           float rel = fabsf(qp->nrm[3] - pr->nrm[3]) / pr->nrm[3];
-          float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f);
+          float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f);
           acc = add(acc, muls(upper_avg(ly, o->rad, c + 1u, qi, u0, v0, L->res), w));
           ws += w;
         }
@@ -456,7 +456,7 @@ static void gather_range(void *p, uint64_t b, uint64_t e) {
         float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
         float rel = fabsf(pr->nrm[3] - z) / z;
         float nd = fmaxf_(dot(n, V(pr->nrm[0], pr->nrm[1], pr->nrm[2])), 0.0f);
-        float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
+        float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
         /* evalSH (rc.ts:819-829) */
         const float *sh = o->sh + 32u * qi;
         v3 es = V(0.0f, 0.0f, 0.0f);

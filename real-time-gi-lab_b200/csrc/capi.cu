@@ -93,6 +93,12 @@ struct gi_rc {
   size_t rad_elem_bytes = 0, sh_elems = 0;
   bool frame_set = false, gbuf_set = false, debug_hits = false;
   uint64_t bytes = 0;
+  bool timing = false;
+  bool timed = false;        // the last gi_solve / gi_rc_solve recorded its events
+  bool timed_vox = false;    // ... and the voxel build's
+  cudaEvent_t ev[7] = {};    // vox start, vox end = giBuild start, giBuild end, giTrace end, giMerge end, giGather end
+  cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
+  gi_vox *graph_vox = nullptr;
 };
 
 static void free_scene(gi_scene *s) {
@@ -105,6 +111,9 @@ static void free_vox(gi_vox *v) {
   cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
 }
 static void free_rc(gi_rc *r) {
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
+  for (cudaEvent_t &e : r->ev)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
   cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->keys); cudaFree(r->stage);
   cudaFree(r->hits); cudaFree(r->rad_traced);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
@@ -178,7 +187,7 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
         (e = dalloc(&s->stage, (size_t)nverts * 2u)))
       break;
     h4 = new (std::nothrow) float4[nverts ? nverts : 1];
-    if (!h4) { delete s; return fail(GI_ERR_OOM, "gi_scene_upload: host staging"); }
+    if (!h4) { free_scene(s); delete s; return fail(GI_ERR_OOM, "gi_scene_upload: host staging"); }
     for (uint32_t i = 0; i < nverts; i++) h4[i] = make_float4(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2], 0.0f);
     if ((e = cudaMemcpy(s->pos, h4, nverts * sizeof(float4), cudaMemcpyHostToDevice))) break;
     for (uint32_t i = 0; i < nverts; i++) h4[i] = make_float4(nrm[3 * i], nrm[3 * i + 1], nrm[3 * i + 2], 0.0f);
@@ -457,14 +466,74 @@ int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_solve: cudaSetDevice");
   r->dev.hits = r->debug_hits ? r->hits : nullptr;
   r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
-  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream)), "gi_rc_solve: launch");
+  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr), "gi_rc_solve: launch");
+  r->timed = r->timing;
+  r->timed_vox = false;
   return GI_OK;
 }
 
 int gi_solve(gi_rc *r, gi_vox *v, void *stream) {
+  if (!r || !v) return fail(GI_ERR_INVALID, "gi_solve: NULL argument");
+  if (r->timing) {
+    CK(cudaSetDevice(r->ctx->device), "gi_solve: cudaSetDevice");
+    CK(cudaEventRecord(r->ev[0], S(stream)), "gi_solve: event");
+  }
   int st = gi_vox_build(v, stream);
   if (st != GI_OK) return st;
-  return gi_rc_solve(r, v, stream);
+  st = gi_rc_solve(r, v, stream);
+  r->timed_vox = st == GI_OK && r->timing;
+  return st;
+}
+
+int gi_rc_graph_capture(gi_rc *r, gi_vox *v, void *stream) {
+  if (!r || !v) return fail(GI_ERR_INVALID, "gi_rc_graph_capture: NULL argument");
+  if (!stream) return fail(GI_ERR_INVALID, "gi_rc_graph_capture: the legacy default stream cannot be captured; pass a stream");
+  if (!r->frame_set || !r->gbuf_set || !v->updated) return fail(GI_ERR_STATE, "gi_rc_graph_capture: frame, G-buffer and voxel window must be set first");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_graph_capture: cudaSetDevice");
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; r->graph_vox = nullptr; }
+  bool timing = r->timing;
+  r->timing = false;   // no event records inside the graph
+  CK(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeThreadLocal), "gi_rc_graph_capture: begin");
+  int st = gi_solve(r, v, stream);
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(S(stream), &g);
+  r->timing = timing;
+  if (st != GI_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return cuda_fail(e, "gi_rc_graph_capture: end");
+  e = cudaGraphInstantiate(&r->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture: instantiate"); }
+  r->graph_vox = v;
+  return GI_OK;
+}
+
+int gi_rc_graph_launch(gi_rc *r, void *stream) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_graph_launch: NULL rc");
+  if (!r->graph) return fail(GI_ERR_STATE, "gi_rc_graph_launch: no graph captured");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_graph_launch: cudaSetDevice");
+  CK(cudaGraphLaunch(r->graph, S(stream)), "gi_rc_graph_launch");
+  r->timed = false;
+  return GI_OK;
+}
+
+int gi_rc_set_timing(gi_rc *r, int on) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_timing: NULL rc");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_timing: cudaSetDevice");
+  if (on && !r->ev[0])
+    for (cudaEvent_t &e : r->ev) CK(cudaEventCreate(&e), "gi_rc_set_timing: cudaEventCreate");
+  r->timing = on != 0;
+  return GI_OK;
+}
+
+int gi_rc_pass_times(gi_rc *r, float ms[5]) {
+  if (!r || !ms) return fail(GI_ERR_INVALID, "gi_rc_pass_times: NULL argument");
+  if (!r->timed) return fail(GI_ERR_STATE, "gi_rc_pass_times: the last solve was not timed (gi_rc_set_timing)");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_pass_times: cudaSetDevice");
+  CK(cudaEventSynchronize(r->ev[5]), "gi_rc_pass_times: sync");
+  ms[0] = 0.0f;
+  if (r->timed_vox) CK(cudaEventElapsedTime(&ms[0], r->ev[0], r->ev[1]), "gi_rc_pass_times: vox");
+  for (int i = 0; i < 4; i++) CK(cudaEventElapsedTime(&ms[i + 1], r->ev[i + 1], r->ev[i + 2]), "gi_rc_pass_times: pass");
+  return GI_OK;
 }
 
 int gi_rc_read_irradiance(gi_rc *r, float *rgba, void *stream) {

@@ -66,6 +66,27 @@ __device__ __forceinline__ int round_log2(float x) {
   return mm >= 0.5 ? e : e - 1;
 }
 
+// e^x of the merge and gather weights: Cody & Waite's two-constant reduction x = k ln2 + r (|r| <= ln2/2, the split of
+// ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form, e^x = 2^k e^r.  Relative error below
+// 3e-7 on [-80, 88]; below -80 the result is 0.  The oracle evaluates the same f32 sequence (no fused multiply-add on
+// either side), so the weights agree bit for bit.
+__device__ __forceinline__ float gi_exp(float x) {
+  if (x != x) return x;
+  if (x < -80.0f) return 0.0f;
+  if (x > 88.0f) return __int_as_float(0x7f800000);
+  float k = rintf(x * 0x1.715476p+0f);
+  float r = (x - k * 0x1.62e4p-1f) - k * 0x1.7f7d1cp-20f;
+  float p = 0x1.a01a02p-13f;
+  p = p * r + 0x1.6c16c2p-10f;
+  p = p * r + 0x1.111112p-7f;
+  p = p * r + 0x1.555556p-5f;
+  p = p * r + 0x1.555556p-3f;
+  p = p * r + 0.5f;
+  p = p * r + 1.0f;
+  p = p * r + 1.0f;
+  return ldexpf(p, (int)k);
+}
+
 // ---- WGSL packing builtins (public WGSL spec formulas) -------------------------------------------------------------
 __device__ __forceinline__ uint32_t pack4x8unorm(float a, float b, float c, float d) {
   float v[4] = {a, b, c, d};

@@ -35,7 +35,9 @@ struct RcDev {
 }  // namespace gi
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
-cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st);
+// ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
+cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
+                               cudaEvent_t *ev = nullptr);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
                               uint32_t *counter, uint32_t sm_count, cudaStream_t st);

@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(256) k_merge(RcDev r, uint32_t c) {
         if (qp.pos.w <= 0.0f) continue;
         float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
         float rel = fabsf(qp.nrm.w - pr.nrm.w) / pr.nrm.w;
-        float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f);
+        float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f);
         acc = acc + upper_avg<A>(r, rad, c + 1u, qi, u0, v0, L.res) * w;
         ws += w;
       }
@@ -420,7 +420,7 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
       float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
       float rel = fabsf(pr.nrm.w - z) / z;
       float nd = mx(dot(n, ld3(pr.nrm)), 0.0f);
-      float w = (fwx * fwy + 1e-4f) * (expf(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
+      float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f) * (nd * nd * nd * nd + 1e-3f);
       float v[32];
 #pragma unroll
       for (int j = 0; j < 8; j++) {
@@ -460,20 +460,25 @@ __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
 }
 
 template <int A>
-static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st) {
+static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev) {
   uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
   cudaMemsetAsync(r.counts, 0, 81 * sizeof(uint32_t), st);
+  if (ev) cudaEventRecord(ev[0], st);
   k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r);
+  if (ev) cudaEventRecord(ev[1], st);
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * 8u);
   k_trace<A><<<tb, 256, 0, st>>>(r, v, counter);
+  if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
     uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
     k_merge<A><<<(n + 255u) / 256u, 256, 0, st>>>(r, (uint32_t)c);
   }
   k_project_sh<A><<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r);
+  if (ev) cudaEventRecord(ev[3], st);
   dim3 gg((r.width + 15u) / 16u, (r.height + 15u) / 16u);
   k_gather<A><<<gg, 256, 0, st>>>(r);
+  if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
 
@@ -481,11 +486,11 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
 
 using namespace gi;
 
-cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st) {
+cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev) {
   switch (r.atlas) {
-    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st);
-    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st);
-    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st);
+    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev);
+    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev);
+    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st, ev);
   }
   return cudaErrorInvalidValue;
 }

@@ -184,6 +184,40 @@ class Rc:
     def set_debug_hits(self, on: bool):
         _lib.call("gi_rc_set_debug_hits", self.handle, 1 if on else 0)
 
+    def graph_capture(self, vox: VoxWorld, stream):
+        """Captures one solve (voxel rebuild + cascades) into a CUDA graph owned by this Rc."""
+        _lib.call("gi_rc_graph_capture", self.handle, vox.handle, _stream(stream))
+
+    def graph_launch(self, stream):
+        _lib.call("gi_rc_graph_launch", self.handle, _stream(stream))
+
+    def read_irradiance_raw(self, out: np.ndarray, stream=None):
+        _lib.call("gi_rc_read_irradiance_raw", self.handle, out.ctypes.data if isinstance(out, np.ndarray) else out,
+                  out.nbytes if isinstance(out, np.ndarray) else self.irr_bytes(), _stream(stream))
+
+    def irr_bytes(self) -> int:
+        return self.width * self.height * (16 if self.params.atlas == "f32" else 8)
+
+    def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None):
+        """G-buffer from host pointers (pinned memory makes the copies asynchronous)."""
+        _lib.call("gi_rc_set_gbuffer_f16", self.handle, depth_ptr, normal_f16_ptr, _stream(stream))
+
+    def set_frame_ptr(self, frame_ptr: int, stream=None):
+        _lib.call("gi_rc_set_frame", self.handle, frame_ptr, _stream(stream))
+
+    def read_irradiance_raw_ptr(self, ptr: int, stream=None):
+        _lib.call("gi_rc_read_irradiance_raw", self.handle, ptr, self.irr_bytes(), _stream(stream))
+
+    PASSES = ("vox", "giBuild", "giTrace", "giMerge", "giGather")
+
+    def set_timing(self, on: bool):
+        _lib.call("gi_rc_set_timing", self.handle, 1 if on else 0)
+
+    def pass_times(self) -> dict:
+        ms = np.zeros(5, np.float32)
+        _lib.call("gi_rc_pass_times", self.handle, _ptr(ms))
+        return dict(zip(self.PASSES, [float(x) for x in ms]))
+
     def bytes(self) -> int:
         b = C.c_uint64()
         _lib.call("gi_rc_bytes", self.handle, C.byref(b))
