@@ -124,6 +124,22 @@ int gi_vox_used_bytes(gi_vox *vox, uint64_t *persistent, uint64_t *build_temp);
 int gi_vox_read_state(gi_vox *vox, uint32_t *ptr, uint32_t *occ, uint32_t *base, uint32_t *code, uint32_t *rep,
                       uint32_t *attr, float *plane, float *sunvis, void *stream);
 int gi_vox_destroy(gi_vox *vox);
+/* The voxel rebuild for callers that cannot allocate device memory (no counterpart in the reference).  Some callers
+ * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
+ * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point
+ * takes the scene and every output in the caller's device memory and allocates nothing: its scratch (representatives,
+ * big-triangle lists, scan sums) is a static device array of 12.1 MiB that the library holds on every GPU it is loaded
+ * on.  Limits: max_bricks <= 4096, levels * G^3 <= 2^25, 65,536 big triangles per list (more count as bigOverflow,
+ * header word 3).  Inputs: pos4/nrm4 4 floats per vertex (w ignored), tri4 (i0, i1, i2, material) with indices below
+ * nverts / nmats (not checked: they are device memory), mats device gi_material[nmats]; pos4, nrm4, tri4, occ, attr
+ * 16-byte aligned.  Outputs as gi_vox_read_state lays them out (hdr 64 words, ptr levels*G^3, occ max_bricks*16,
+ * base/code max_bricks, attr max_voxels*4, plane/sunvis max_voxels).  Runs on the current device and `stream`; the
+ * first call on a device looks up the scratch's address there.  All calls share the scratch: two calls that overlap
+ * on the GPU race and corrupt each other, so serialise them. */
+int gi_vox_build_noalloc(const gi_vox_params *params, const double eye[3], const float *pos4, const float *nrm4,
+                         uint32_t nverts, const uint32_t *tri4, uint32_t ntris, const gi_material *mats, uint32_t nmats,
+                         uint32_t *hdr, uint32_t *ptr, uint32_t *occ, uint32_t *base, uint32_t *code, uint32_t *attr,
+                         float *plane, float *sunvis, void *stream);
 
 /* ---- radiance cascades (rc.ts Rc), screen probes traced in the voxel world --------------------------------------- */
 int gi_rc_create(gi_ctx *ctx, const gi_rc_params *params, uint32_t width, uint32_t height, gi_rc **out);

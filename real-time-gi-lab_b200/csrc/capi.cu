@@ -49,6 +49,9 @@ inline cudaStream_t S(void *stream) { return (cudaStream_t)stream; }
 
 }  // namespace
 
+// Error reporting for the library's other C-ABI files (gi_last_error returns it).
+void gi_set_error(const char *msg) { g_err = msg; }
+
 struct gi_ctx {
   int device;
   uint32_t sm_count;

@@ -31,6 +31,8 @@ SIGNATURES = {
     "gi_vox_used_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gi_vox_read_state": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "gi_vox_destroy": (C.c_int, [_P]),
+    "gi_vox_build_noalloc": (C.c_int, [_P, C.POINTER(C.c_double), _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
+                                       _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "gi_rc_create": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "gi_rc_set_frame": (C.c_int, [_P, _P, _P]),
     "gi_rc_set_gbuffer": (C.c_int, [_P, _P, _P, _P]),
