@@ -128,7 +128,7 @@ int gi_vox_destroy(gi_vox *vox);
  * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
  * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point
  * takes the scene and every output in the caller's device memory and allocates nothing: its scratch (representatives,
- * big-triangle lists, scan sums) is a static device array of 12.1 MiB that the library holds on every GPU it is loaded
+ * big-triangle lists, scan sums) is a static device array of 14.1 MiB that the library holds on every GPU it is loaded
  * on.  Limits: max_bricks <= 4096, levels * G^3 <= 2^25, 65,536 big triangles per list (more count as bigOverflow,
  * header word 3).  Inputs: pos4/nrm4 4 floats per vertex (w ignored), tri4 (i0, i1, i2, material) with indices below
  * nverts / nmats (not checked: they are device memory), mats device gi_material[nmats]; pos4, nrm4, tri4, occ, attr

@@ -112,6 +112,7 @@ static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
   cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
   cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
+  cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre);
 }
 static void free_rc(gi_rc *r) {
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
@@ -120,6 +121,7 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->keys); cudaFree(r->stage);
   cudaFree(r->hits); cudaFree(r->rad_traced);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
+  cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs);
 }
 
 extern "C" {
@@ -257,18 +259,22 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
   uint32_t vscan = (p->max_bricks + 255u) / 256u;
   if (vscan > scan_words) scan_words = vscan;
+  uint32_t cscan = 8u * d.big_cap / 256u;   // chunk-prefix block sums of the voxBits big lists
+  if (cscan > scan_words) scan_words = cscan;
   cudaError_t e;
   if ((e = dalloc(&d.hdr, GI_HDR)) || (e = dalloc(&d.ptr, nptr)) || (e = dalloc(&d.occ, (size_t)p->max_bricks * 16u)) ||
       (e = dalloc(&d.base, p->max_bricks)) || (e = dalloc(&d.code, p->max_bricks)) ||
       (e = dalloc(&d.rep, (size_t)p->max_bricks * 512u)) || (e = dalloc(&d.big, (size_t)16u * d.big_cap)) ||
       (e = dalloc(&d.attr, p->max_voxels)) || (e = dalloc(&d.plane, p->max_voxels)) ||
-      (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words))) {
+      (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words)) ||
+      (e = dalloc(&d.vpre, (size_t)p->max_bricks + 1u)) || (e = dalloc(&d.work, 4)) ||
+      (e = dalloc(&d.cpre, (size_t)8u * d.big_cap))) {
     free_vox(v);
     delete v;
     return cuda_fail(e, "gi_vox_create");
   }
   v->bytes = (GI_HDR + nptr + (uint64_t)p->max_bricks * (16u + 2u + 512u) + (uint64_t)16u * d.big_cap +
-              (uint64_t)p->max_voxels * 6u + scan_words) * 4u;
+              (uint64_t)p->max_voxels * 6u + scan_words + p->max_bricks + 5u + (uint64_t)8u * d.big_cap) * 4u;
   memset(v->hdr, 0, sizeof v->hdr);
   *out = v;
   return GI_OK;
@@ -368,7 +374,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   d.vox_scale = p->vox_scale; d.vox_offset = p->vox_offset; d.level_map = p->level_map; d.vox_skip = p->vox_skip;
   d.dda_cap = p->dda_cap; d.stats = p->stats;
   // cascade layout (rc.ts:1027-1035)
-  uint64_t probe_total = 0, ray_total = 0;
+  uint64_t probe_total = 0, ray_total = 0, dir_total = 0;
   for (uint32_t i = 0; i < p->cascades; i++) {
     CascDev &c = d.c[i];
     uint32_t rc_ = i < p->res_cap ? i : p->res_cap;
@@ -382,6 +388,8 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     c.probe_off = (uint32_t)probe_total;
     c.rad_off = (uint32_t)ray_total;
     c.ray_off = (uint32_t)ray_total;
+    c.dir_off = (uint32_t)dir_total;
+    dir_total += (uint64_t)c.res * c.res;
     double b0 = (double)p->k_interval * (pow(4.0, (double)i) - 1.0) / 3.0;
     double b1 = (double)p->k_interval * (pow(4.0, (double)(i + 1)) - 1.0) / 3.0;
     c.b0 = (float)b0; c.b1 = (float)b1;
@@ -397,20 +405,27 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   cudaError_t e;
   ProbeDev *probes = nullptr;
   void *rad = nullptr, *sh = nullptr, *irr = nullptr;
-  uint32_t *counts = nullptr;
+  uint32_t *counts = nullptr, *plevel = nullptr;
+  float4 *dirs = nullptr;
   if ((e = dalloc(&r->frame, 160)) || (e = dalloc(&r->depth, npx)) || (e = dalloc(&r->normal, npx)) ||
       (e = dalloc(&r->keys, npx)) || (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->rad_elem_bytes)) ||
-      (e = cudaMalloc(&irr, npx * atlas_elem_bytes(p->atlas))) || (e = dalloc(&counts, 96))) {
-    d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts;
+      (e = cudaMalloc(&irr, npx * atlas_elem_bytes(p->atlas))) || (e = dalloc(&counts, 96)) ||
+      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, dir_total))) {
+    d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
     free_rc(r);
     delete r;
     return cuda_fail(e, "gi_rc_create");
   }
-  d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts;
+  d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
   d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
   cudaMemset(counts, 0, 96 * 4);
-  r->bytes = 160 * 4 + npx * (4 + 8 + 8 + 16) + probe_total * 48 + ray_total * r->rad_elem_bytes +
+  if ((e = gi_launch_init_dirs(d, dirs, (uint32_t)dir_total, 0)) || (e = cudaDeviceSynchronize())) {
+    free_rc(r);
+    delete r;
+    return cuda_fail(e, "gi_rc_create: direction table");
+  }
+  r->bytes = 160 * 4 + npx * (4 + 8 + 8 + 16) + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->rad_elem_bytes + npx * atlas_elem_bytes(p->atlas) + 96 * 4;
   *out = r;
   return GI_OK;

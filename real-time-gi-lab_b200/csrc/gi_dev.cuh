@@ -167,6 +167,9 @@ struct VoxDev {
   float *plane;        // max_voxels
   float *sunvis;       // max_voxels
   uint32_t *scan;      // build temporary: block sums of the ordered allocations
+  uint32_t *vpre;      // build temporary: max_bricks + 1 exclusive prefix of the bricks' voxel counts
+  uint32_t *work;      // build temporary: 4 words, queue counters and the chunk total of the big-triangle passes
+  uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
 };
 
 __device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return ldexpf(v.v0, (int)L); }

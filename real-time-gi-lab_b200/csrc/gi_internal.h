@@ -8,7 +8,7 @@
 namespace gi {
 
 struct CascDev {
-  uint32_t probe_off, rad_off, res, tile_size, tiles_x, tiles_y, ray_off, pad;
+  uint32_t probe_off, rad_off, res, tile_size, tiles_x, tiles_y, ray_off, dir_off;
   float b0, b1, pad2[2];
 };
 
@@ -24,6 +24,8 @@ struct RcDev {
   const float *depth;      // W*H
   const uint2 *normal;     // W*H rgba16f
   ProbeDev *probes;
+  uint32_t *plevel;        // per probe: voxLevel(s0, c) (rc.ts:210-213), computed once by setupScreen
+  const float4 *dirs;      // per cascade, res^2 texel directions dirOf(di, res) (rc.ts:308), computed at creation
   void *rad;               // rays_total atlas elements
   void *sh;                // probes of cascade 0 x 8 atlas elements
   void *irr;               // W*H: float4 (atlas F32) or rgba16f (uint2)
@@ -43,3 +45,4 @@ cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uin
                               uint32_t *counter, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
+cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);

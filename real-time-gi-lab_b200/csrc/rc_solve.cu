@@ -3,7 +3,8 @@
 // projectSH :752, gatherScreen :929).
 //
 // Form changes from the reference's dispatches, results unchanged:
-//  * setupScreen and trace each run once over all cascades (the reference dispatches them per cascade);
+//  * setupScreen and trace each run once over all cascades (the reference dispatches them per cascade); the texel
+//    directions are tabulated once per Rc and each probe's voxel level once per solve (same functions, same bits);
 //  * the trace kernel is persistent: each warp takes 32 rays at a time from a global ray counter;
 //  * indirect dispatches become launches sized from the host-known probe counts (screen probes: tiles).
 #include <cuda_runtime.h>
@@ -190,7 +191,7 @@ __device__ __forceinline__ uint32_t casc_of_ray(const RcDev &r, uint32_t i) {
 }
 
 // setupScreen (rc.ts:572-590), every cascade in one launch
-__global__ void k_setup_screen(RcDev r) {
+__global__ void k_setup_screen(RcDev r, VoxDev v) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.probes_total) return;
   uint32_t c = 0;
@@ -218,6 +219,7 @@ __global__ void k_setup_screen(RcDev r) {
     pr.nrm = make_float4(nrm.x, nrm.y, nrm.z, view_z(F, x));
   }
   r.probes[i] = pr;
+  r.plevel[i] = pr.pos.w > 0.0f ? vox_level(v, r, pr.pos.w, c) : 0u;
 }
 
 // trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245).  Persistent: every warp takes rays from a global counter, 32 at
@@ -249,11 +251,12 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
       uint32_t pi = t / dirs, di = t % dirs;
       ProbeDev pr = r.probes[L.probe_off + pi];
       if (pr.pos.w > 0.0f) {
-        f3 dir = dir_of(di, L.res);
+        float4 dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
+        f3 dir = mk(dv.x, dv.y, dv.z);
         float s0 = pr.pos.w;
         float t0 = L.b0 * s0, t1 = L.b1 * s0;
         f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
-        uint32_t Lv = vox_level_for(v, vox_level(v, r, s0, c), po + dir * t1);
+        uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
         float vs = vox_size(v, Lv);
         trace_vox(v, F, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
         traced = true;
@@ -452,6 +455,16 @@ __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
   }
 }
 
+// dirOf(di, res) (rc.ts:308) of every texel of every cascade, once per Rc
+__global__ void k_init_dirs(RcDev r, float4 *dirs, uint32_t ndirs) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= ndirs) return;
+  uint32_t c = 0;
+  for (uint32_t k = 1; k < r.cascades; k++) if (i >= r.c[k].dir_off) c = k;
+  f3 d = dir_of(i - r.c[c].dir_off, r.c[c].res);
+  dirs[i] = make_float4(d.x, d.y, d.z, 0.0f);
+}
+
 __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 s = src[i];
@@ -464,7 +477,7 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
   cudaMemsetAsync(r.counts, 0, 81 * sizeof(uint32_t), st);
   if (ev) cudaEventRecord(ev[0], st);
-  k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r);
+  k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r, v);
   if (ev) cudaEventRecord(ev[1], st);
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * 8u);
   k_trace<A><<<tb, 256, 0, st>>>(r, v, counter);
@@ -497,6 +510,11 @@ cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_coun
 
 cudaError_t gi_launch_irr_to_f32(const RcDev &r, float4 *dst, cudaStream_t st) {
   k_irr_to_f32<<<256, 256, 0, st>>>(r, dst);
+  return cudaGetLastError();
+}
+
+cudaError_t gi_launch_init_dirs(const RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st) {
+  k_init_dirs<<<(ndirs + 255u) / 256u, 256, 0, st>>>(r, dirs, ndirs);
   return cudaGetLastError();
 }
 

@@ -5,9 +5,10 @@
 //    pool holds them all (the reference uses that order only when it overflows, voxel.ts:405-410, and an atomic
 //    counter otherwise); voxel attribute bases are an exclusive scan in brick order.  Both are orders the reference
 //    can produce; they make the whole state deterministic, so the GPU state equals the oracle's word for word.
-//  * the brick init and the representative-table clear (clearKeys) are fused into the allocation pass;
+//  * the representative-table clear (clearKeys) zeroes every allocated brick in one full-grid pass;
 //  * indirect dispatches (writeArgs) become grid-stride loops that read the device-side counts;
-//  * the big-triangle passes run one warp per (triangle, level) instead of one 64-wide workgroup;
+//  * the big-triangle passes run one warp per (triangle, level), taken from a queue, instead of one 64-wide
+//    workgroup; resolveAttr runs one thread per voxel;
 //  * list appends are warp-aggregated atomics.
 #include <cuda_runtime.h>
 
@@ -91,13 +92,14 @@ __global__ void k_clear(VoxDev v) {
   uint32_t n = v.levels * v.G * v.G * v.G;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < GI_HDR; i += gridDim.x * blockDim.x) {
     if (i < GI_HDR) v.hdr[i] = 0u;
+    if (i < 4u) v.work[i] = 0u;
     if (i < n) v.ptr[i] = GI_EMPTY;
   }
 }
 
 // markBricks (voxel.ts:359-376): one thread per triangle; every lane walks the same levels so that the list appends
 // are warp-aggregated.
-__global__ void __launch_bounds__(256) k_mark_bricks(VoxDev v, SceneDev s) {
+__global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = t < s.ntris;
   Tri T;
@@ -133,11 +135,19 @@ __device__ __forceinline__ bool big_item(const VoxDev &v, uint32_t seg0, uint32_
   return false;
 }
 
+__device__ __forceinline__ uint32_t big_total(const VoxDev &v, uint32_t hdr0) {
+  uint32_t n = 0;
+  for (uint32_t L = 0; L < v.levels; L++) n += min(v.hdr[hdr0 + L], v.big_cap);
+  return n;
+}
+
 // markBricksBig (voxel.ts:377-387): one warp per big (triangle, level), lanes over the range's bricks.
-__global__ void __launch_bounds__(256) k_mark_bricks_big(VoxDev v, SceneDev s) {
+__global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s) {
   uint32_t lane = threadIdx.x & 31u;
-  uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+  for (;;) {
+    uint32_t w = 0;
+    if (lane == 0) w = atomicAdd(&v.work[0], 1u);   // warps take items from a queue: long items do not stall others
+    w = __shfl_sync(0xffffffffu, w, 0);
     uint32_t L, t;
     if (!big_item(v, 8u, 24u, w, L, t)) break;
     Tri T = load_tri(s, t);
@@ -236,7 +246,26 @@ __global__ void __launch_bounds__(256) k_scan_sums(uint32_t *sums, uint32_t nblo
   if (threadIdx.x == 0 && hdr) { hdr[0] = carry; hdr[5] = carry; }
 }
 
-// allocBricks (voxel.ts:450-470) in the fixed order, with the brick init and clearKeys (voxel.ts:471-474) fused.
+// The chunk prefix's block offsets (k_count_chunks wrote one sum per 256 items) and the chunk total (work[2]).
+__global__ void __launch_bounds__(256) k_scan_chunks(VoxDev v) {
+  uint32_t nblocks = (big_total(v, 16u) + 255u) / 256u;
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < nblocks; b0 += 256u) {
+    uint32_t i = b0 + threadIdx.x;
+    uint32_t x = i < nblocks ? v.scan[i] : 0u;
+    uint32_t tot;
+    uint32_t ex = block_scan_256(x, &tot);
+    if (i < nblocks) v.scan[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) v.work[2] = carry;
+}
+
+// allocBricks (voxel.ts:450-470) in the fixed order.
 __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per, G = v.G;
   uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
@@ -251,10 +280,6 @@ __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
   }
   uint32_t tot;
   uint32_t ex = block_scan_256(c, &tot) + v.scan[blockIdx.x];
-  __shared__ uint32_t s_idx[ALLOC_CHUNK];
-  __shared__ uint32_t s_cnt;
-  if (threadIdx.x == 0) s_cnt = 0;
-  __syncthreads();
 #pragma unroll
   for (uint32_t k = 0; k < 8u; k++) {
     if (!((flags >> k) & 1u)) continue;
@@ -267,15 +292,19 @@ __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
     v.ptr[i] = idx;
     v.base[idx] = 0u;
     v.code[idx] = (L << 27) | ((r % G) << 18) | (((r / G) % G) << 9) | (r / (G * G));
-    s_idx[atomicAdd(&s_cnt, 1u)] = idx;
   }
-  __syncthreads();
-  // zero the occupancy (64 B) and representatives (2 KB) of the bricks this block allocated
-  uint32_t nb = s_cnt;
-  for (uint32_t q = threadIdx.x; q < nb * 132u; q += 256u) {
-    uint32_t b = s_idx[q / 132u], w = q % 132u;
-    if (w < 4u) reinterpret_cast<uint4 *>(v.occ)[b * 4u + w] = make_uint4(0, 0, 0, 0);
-    else reinterpret_cast<uint4 *>(v.rep)[b * 128u + (w - 4u)] = make_uint4(0, 0, 0, 0);
+}
+
+// The rest of the brick init and clearKeys (voxel.ts:467, :471-474): zero the occupancy (64 B) and representatives
+// (2 KB) of every allocated brick, over the whole grid.
+__global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
+  uint32_t nb = min(v.hdr[0], v.max_bricks);
+  uint4 z = make_uint4(0u, 0u, 0u, 0u);
+  uint4 *occ = reinterpret_cast<uint4 *>(v.occ), *rep = reinterpret_cast<uint4 *>(v.rep);
+  if (blockIdx.x == 0 && threadIdx.x == 0) v.work[1] = 0u;   // the voxBitsBig item counter
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q < nb * 132u; q += gridDim.x * blockDim.x) {
+    if (q < nb * 4u) occ[q] = z;
+    else rep[q - nb * 4u] = z;
   }
 }
 
@@ -301,7 +330,7 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
 }
 
 // voxBits (voxel.ts:492-513)
-__global__ void __launch_bounds__(256) k_vox_bits(VoxDev v, SceneDev s) {
+__global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = t < s.ntris;
   uint32_t bo = v.hdr[2];
@@ -327,18 +356,87 @@ __global__ void __launch_bounds__(256) k_vox_bits(VoxDev v, SceneDev s) {
   }
 }
 
-// voxBitsBig (voxel.ts:515-534): one warp per big (triangle, level)
-__global__ void __launch_bounds__(256) k_vox_bits_big(VoxDev v, SceneDev s) {
+// voxBitsBig (voxel.ts:515-534), balanced: every big (triangle, level) is cut into chunks of VB_CHUNK cells (a wall
+// triangle clipped to a window covers ~10^4 cells; one warp per triangle left one warp working long after the rest).
+// k_count_chunks: per item its chunk count, an exclusive prefix within blocks of 256 items and the block sums;
+// k_scan_sums turns those into block offsets and the total; warps of k_vox_bits_big take chunks from a queue and
+// find their item by binary search over the prefix.
+constexpr uint32_t VB_CHUNK = 128;
+
+__global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
+  uint32_t items = big_total(v, 16u);
+  uint32_t nblk = (items + 255u) / 256u;
+  for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    uint32_t w = b * 256u + threadIdx.x, L, t, c = 0;
+    if (w < items && big_item(v, 0u, 16u, w, L, t)) {
+      Tri T = load_tri(s, t);
+      Range r = vox_range(v, T, L, vox_size(v, L));
+      c = ((uint32_t)(r.n.x * r.n.y * r.n.z) + VB_CHUNK - 1u) / VB_CHUNK;
+    }
+    uint32_t tot;
+    uint32_t ex = block_scan_256(c, &tot);
+    if (w < items) v.cpre[w] = ex;
+    if (threadIdx.x == 0) v.scan[b] = tot;
+  }
+}
+
+// voxelizeOne's tests (voxel.ts:477-485) without the writes: true and the occupancy word / bit / representative slot
+// when the voxel takes the triangle.
+__device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t L, i3 c,
+                                            uint32_t brick_overflow, uint32_t &wi, uint32_t &msk, uint32_t &ri) {
+  if (finer_built(v, L, c, brick_overflow)) return false;
+  float vs = vox_size(v, L);
+  f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
+  float hh = 0.5f * vs * 1.0001f;
+  if (!tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return false;
+  uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
+  if (ptr >= GI_MARK) return false;
+  const gi_material &m = s.mats[T.idx.w];
+  if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;
+  uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
+  wi = ptr * 16u + (bit >> 5);
+  msk = 1u << (bit & 31u);
+  ri = ptr * 512u + bit;
+  return true;
+}
+
+// One warp per chunk.  The lanes' occupancy bits are ORed per word inside the warp (neighbouring cells share a
+// word), one atomic per word.
+__global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
   uint32_t lane = threadIdx.x & 31u;
-  uint32_t warps = gridDim.x * (blockDim.x >> 5);
   uint32_t bo = v.hdr[2];
-  for (uint32_t w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;; w += warps) {
+  uint32_t items = big_total(v, 16u);
+  uint32_t chunks = v.work[2];
+  for (;;) {
+    uint32_t ch = 0;
+    if (lane == 0) ch = atomicAdd(&v.work[1], 1u);
+    ch = __shfl_sync(0xffffffffu, ch, 0);
+    if (ch >= chunks) break;
+    uint32_t lo = 0, hi = items;   // the last item whose first chunk is <= ch
+    while (hi - lo > 1u) {
+      uint32_t m = (lo + hi) >> 1;
+      if (v.cpre[m] + v.scan[m >> 8] <= ch) lo = m; else hi = m;
+    }
     uint32_t L, t;
-    if (!big_item(v, 0u, 16u, w, L, t)) break;
+    big_item(v, 0u, 16u, lo, L, t);
+    uint32_t part = ch - (v.cpre[lo] + v.scan[lo >> 8]);
     Tri T = load_tri(s, t);
     Range r = vox_range(v, T, L, vox_size(v, L));
     int n = r.n.x * r.n.y * r.n.z;
-    for (int q = (int)lane; q < n; q += 32) voxelize_one(v, s, T, t, L, range_cell(r, q), false, bo);
+    int q_end = min(n, (int)((part + 1u) * VB_CHUNK));
+    for (int q0 = (int)(part * VB_CHUNK); q0 < q_end; q0 += 32) {
+      int q = q0 + (int)lane;
+      uint32_t wi = 0xffffffffu, msk = 0u, ri = 0u;
+      bool ok = q < q_end && voxel_takes(v, s, T, L, range_cell(r, q), bo, wi, msk, ri);
+      uint32_t any = __ballot_sync(0xffffffffu, ok);
+      if (any == 0u) continue;
+      uint32_t grp = __match_any_sync(0xffffffffu, ok ? wi : 0xffffffffu);
+      uint32_t m = __reduce_or_sync(grp, msk);
+      if (ok) {
+        if ((uint32_t)(__ffs(grp) - 1) == lane && (v.occ[wi] & m) != m) atomicOr(&v.occ[wi], m);
+        if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
+      }
+    }
   }
 }
 
@@ -367,14 +465,24 @@ __global__ void __launch_bounds__(256) k_reduce(VoxDev v, uint32_t L) {
     if (pptr >= GI_MARK) continue;
     uint32_t pbit0 = (uint32_t)((pc0.x & 7) + 8 * (pc0.y & 7) + 64 * (pc0.z & 7));
     uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
-    const uint32_t *rp = v.rep + ptr * 512u + w * 32u;
+    // the word's 32 representatives in 8 independent 128-bit loads; bit k = x + 8 y of the word, parent (x/2, y/2)
+    const uint4 *rp = reinterpret_cast<const uint4 *>(v.rep + ptr * 512u + w * 32u);
+    uint4 rq[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) rq[q] = rp[q];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      uint32_t b4 = (word >> (4 * q)) & 15u;
+      uint32_t px = 2u * (uint32_t)(q & 1);
+      uint32_t a = max((b4 & 1u) ? rq[q].x : 0u, (b4 & 2u) ? rq[q].y : 0u);
+      uint32_t c = max((b4 & 4u) ? rq[q].z : 0u, (b4 & 8u) ? rq[q].w : 0u);
+      if (q < 4) { lo[px] = max(lo[px], a); lo[px + 1u] = max(lo[px + 1u], c); }
+      else { hi[px] = max(hi[px], a); hi[px + 1u] = max(hi[px + 1u], c); }
+    }
     while (word != 0u) {
       uint32_t k = __ffs(word) - 1u;
       word &= word - 1u;
-      uint32_t px = (k & 7u) >> 1, py = k >> 4;
-      mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
-      uint32_t rv = rp[k];
-      if (py == 0u) lo[px] = max(lo[px], rv); else hi[px] = max(hi[px], rv);
+      mask |= 1u << ((pbit0 + ((k & 7u) >> 1) + 8u * (k >> 4)) & 31u);
     }
     uint32_t wi = pptr * 16u + (pbit0 >> 5);
     if ((v.occ[wi] & mask) != mask) atomicOr(&v.occ[wi], mask);
@@ -422,7 +530,10 @@ __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks
   if (b < nb) {
     if (first + c > v.max_voxels) { v.base[b] = GI_EMPTY; atomicAdd(&v.hdr[4], 1u); }
     else v.base[b] = first;
+    v.vpre[b] = first;
+    if (b == nb - 1u) v.vpre[nb] = first + c;
   }
+  if (nb == 0u && b == 0u) v.vpre[0] = 0u;
   if (blockIdx.x == nblocks - 1u && threadIdx.x == 255u) v.hdr[1] = first + c;
 }
 
@@ -451,74 +562,75 @@ __device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
   return mk(1.0f - vv - ww, vv, ww);
 }
 
-// resolveAttr (voxel.ts:596-620): one warp per brick.  The brick's occupied slots are compacted into shared memory
-// in rank order, so the lanes work on occupied voxels only and the attribute writes are contiguous.
+// resolveAttr (voxel.ts:596-620): one thread per voxel of the attribute pool (voxel ai of brick b is rank
+// ai - vpre[b] of b's occupancy), so every occupied voxel is resolved in parallel and the attribute writes are
+// contiguous.
 __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
-  __shared__ uint16_t s_bits[8][512];
-  uint32_t lane = threadIdx.x & 31u, wl = threadIdx.x >> 5;
   uint32_t nb = min(v.hdr[0], v.max_bricks);
-  uint32_t warps = gridDim.x * (blockDim.x >> 5);
-  for (uint32_t ptr = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; ptr < nb; ptr += warps) {
-    uint32_t first = v.base[ptr];
-    if (first == GI_EMPTY) continue;
-    uint32_t word = lane < 16u ? v.occ[ptr * 16u + lane] : 0u;
-    uint32_t pc = __popc(word), inc = pc;
+  uint32_t nv = nb ? min(v.vpre[nb], v.max_voxels) : 0u;
+  for (uint32_t ai = blockIdx.x * blockDim.x + threadIdx.x; ai < nv; ai += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nb;   // the last brick b with vpre[b] <= ai
+    while (hi - lo > 1u) {
+      uint32_t m = (lo + hi) >> 1;
+      if (v.vpre[m] <= ai) lo = m; else hi = m;
+    }
+    uint32_t ptr = lo;
+    if (v.base[ptr] == GI_EMPTY) continue;   // past the voxel pool: no attributes (voxel.ts:586)
+    uint32_t r = ai - v.vpre[ptr];
+    const uint4 *o4 = reinterpret_cast<const uint4 *>(v.occ) + ptr * 4u;
+    uint32_t bit = 0;
 #pragma unroll
-    for (int d = 1; d < 16; d <<= 1) {
-      uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
-      if (lane >= (uint32_t)d) inc += y;
+    for (int q = 0; q < 4; q++) {
+      uint4 o = o4[q];
+      uint32_t ws[4] = {o.x, o.y, o.z, o.w};
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        uint32_t pc = __popc(ws[j]);
+        if (r < pc && bit == 0u) {
+          uint32_t wd = ws[j];
+          for (uint32_t k = 0; k < r; k++) wd &= wd - 1u;
+          bit = (uint32_t)(q * 4 + j) * 32u + (uint32_t)(__ffs(wd) - 1) + 1u;   // + 1: found
+        }
+        if (bit == 0u) r -= pc;
+      }
     }
-    uint32_t excl = inc - pc;
-    uint32_t total = __shfl_sync(0xffffffffu, inc, 15);
-    for (uint32_t w = 0; w < 16u; w++) {
-      uint32_t ww = __shfl_sync(0xffffffffu, word, w);
-      uint32_t base_w = __shfl_sync(0xffffffffu, excl, w);
-      if ((ww >> lane) & 1u) s_bits[wl][base_w + __popc(ww & ((1u << lane) - 1u))] = (uint16_t)(w * 32u + lane);
-    }
-    __syncwarp();
+    bit -= 1u;
     uint32_t code = v.code[ptr];
     uint32_t L = code >> 27;
     i3 b = mki((int)((code >> 18) & 511u), (int)((code >> 9) & 511u), (int)(code & 511u));
-    float vs = vox_size(v, L);
-    f3 rl = region_lo(v, L);
-    for (uint32_t r = lane; r < total; r += 32u) {
-      uint32_t bit = s_bits[wl][r];
-      uint32_t ai = first + r;
-      i3 c = mki(b.x * 8 + (int)(bit & 7u), b.y * 8 + (int)((bit >> 3) & 7u), b.z * 8 + (int)(bit >> 6));
-      f3 p = rl + adds(vi2f(c), 0.5f) * vs;
-      uint32_t rv = v.rep[ptr * 512u + bit];
-      if (rv == 0u || rv > s.ntris) {   // no representative (cannot happen for a set bit): no attributes
-        v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f; v.sunvis[ai] = 1.0f;
-        continue;
-      }
-      Tri T = load_tri(s, rv - 1u);
-      const gi_material &m = s.mats[T.idx.w];
-      // surfaceAt(..., wantAttr = true) (voxel.ts:325-336), untextured
-      f3 wb = closest_bary(p, T.a, T.b, T.c);
-      f3 n0 = ld3(s.nrm[T.idx.x]), n1 = ld3(s.nrm[T.idx.y]), n2 = ld3(s.nrm[T.idx.z]);
-      f3 n = (n0 * wb.x + n1 * wb.y) + n2 * wb.z;
-      if (!(dot(n, n) > 1e-12f)) n = cross(T.b - T.a, T.c - T.a);
-      n = normalize3(n);
-      f3 q = (T.a * wb.x + T.b * wb.y) + T.c * wb.z;
-      float toon = (m.flags & 4u) ? 1.0f : 0.0f;
-      // octEnc (voxel.ts:590-594)
-      float sa = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
-      float ox = n.x / sa, oy = n.y / sa;
-      if (n.z < 0.0f) {
-        float tx = ox, ty = oy;
-        ox = (1.0f - fabsf(ty)) * (tx >= 0.0f ? 1.0f : -1.0f);
-        oy = (1.0f - fabsf(tx)) * (ty >= 0.0f ? 1.0f : -1.0f);
-      }
-      uint4 rec;
-      rec.x = pack4x8unorm(m.base_color[0], m.base_color[1], m.base_color[2], toon);
-      rec.y = pack2x16snorm(ox, oy);
-      rec.z = (uint32_t)f2h(m.emissive[0]) | ((uint32_t)f2h(m.emissive[1]) << 16);
-      rec.w = (uint32_t)f2h(m.emissive[2]);
-      v.attr[ai] = rec;
-      v.plane[ai] = dot(n, q - p);
-      v.sunvis[ai] = 1.0f;
+    i3 c = mki(b.x * 8 + (int)(bit & 7u), b.y * 8 + (int)((bit >> 3) & 7u), b.z * 8 + (int)(bit >> 6));
+    f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vox_size(v, L);
+    uint32_t rv = v.rep[ptr * 512u + bit];
+    if (rv == 0u || rv > s.ntris) {   // no representative (cannot happen for a set bit): no attributes
+      v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f; v.sunvis[ai] = 1.0f;
+      continue;
     }
-    __syncwarp();
+    Tri T = load_tri(s, rv - 1u);
+    const gi_material &m = s.mats[T.idx.w];
+    // surfaceAt(..., wantAttr = true) (voxel.ts:325-336), untextured
+    f3 wb = closest_bary(p, T.a, T.b, T.c);
+    f3 n0 = ld3(s.nrm[T.idx.x]), n1 = ld3(s.nrm[T.idx.y]), n2 = ld3(s.nrm[T.idx.z]);
+    f3 n = (n0 * wb.x + n1 * wb.y) + n2 * wb.z;
+    if (!(dot(n, n) > 1e-12f)) n = cross(T.b - T.a, T.c - T.a);
+    n = normalize3(n);
+    f3 q = (T.a * wb.x + T.b * wb.y) + T.c * wb.z;
+    float toon = (m.flags & 4u) ? 1.0f : 0.0f;
+    // octEnc (voxel.ts:590-594)
+    float sa = fabsf(n.x) + fabsf(n.y) + fabsf(n.z);
+    float ox = n.x / sa, oy = n.y / sa;
+    if (n.z < 0.0f) {
+      float tx = ox, ty = oy;
+      ox = (1.0f - fabsf(ty)) * (tx >= 0.0f ? 1.0f : -1.0f);
+      oy = (1.0f - fabsf(tx)) * (ty >= 0.0f ? 1.0f : -1.0f);
+    }
+    uint4 rec;
+    rec.x = pack4x8unorm(m.base_color[0], m.base_color[1], m.base_color[2], toon);
+    rec.y = pack2x16snorm(ox, oy);
+    rec.z = (uint32_t)f2h(m.emissive[0]) | ((uint32_t)f2h(m.emissive[1]) << 16);
+    rec.w = (uint32_t)f2h(m.emissive[2]);
+    v.attr[ai] = rec;
+    v.plane[ai] = dot(n, q - p);
+    v.sunvis[ai] = 1.0f;
   }
 }
 
@@ -539,7 +651,10 @@ cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_
   k_count_marks<<<ab, 256, 0, st>>>(v);
   k_scan_sums<<<1, 256, 0, st>>>(v.scan, ab, v.hdr);
   k_alloc_bricks<<<ab, 256, 0, st>>>(v);
+  k_init_bricks<<<persist, 256, 0, st>>>(v);
   if (tb) k_vox_bits<<<tb, 256, 0, st>>>(v, s);
+  k_count_chunks<<<persist, 256, 0, st>>>(v, s);
+  k_scan_chunks<<<1, 256, 0, st>>>(v);
   k_vox_bits_big<<<persist, 256, 0, st>>>(v, s);
   for (uint32_t L = 1; L < v.levels; L++) k_reduce<<<persist, 256, 0, st>>>(v, L);
   uint32_t vb = (v.max_bricks + VOX_CHUNK - 1u) / VOX_CHUNK;
