@@ -159,6 +159,59 @@ def cpu_baseline(s, v, p, F, depth, normal, budget_s=12.0, min_solves=2):
                       f"single-threaded, ray/pixel loops on {cores} threads) in {dt:.1f} s"}
 
 
+def run_batched(args, ctx, stream, flush):
+    """The uneven batch (64 seeded specs): every solve replayed alone from its own graph, one after another, and all of
+    them as one batch graph of parallel solve chains.  Device time with CUDA events, L2 flushed between replays."""
+    import torch
+    from rtgi import batch, scenes
+    specs = [scenes.batch_spec(s) for s in range(args.batch)]
+    solves = [batch.make_solve(ctx, sp, stream=stream) for sp in specs]
+    for x in solves:
+        x.rc.graph_capture(x.vox, stream)
+    b = batch.make_batch(ctx, solves, stream)
+    reps = 5
+    ev = lambda: torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        for x in solves:   # warm-up
+            x.rc.graph_launch(stream)
+        b.launch(stream)
+        stream.synchronize()
+        per = [[] for _ in solves]
+        for _ in range(reps):
+            for i, x in enumerate(solves):
+                flush.zero_()
+                e0, e1 = ev(), ev()
+                e0.record(stream)
+                x.rc.graph_launch(stream)
+                e1.record(stream)
+                per[i].append((e0, e1))
+        bt = []
+        for _ in range(reps * 4):
+            flush.zero_()
+            e0, e1 = ev(), ev()
+            e0.record(stream)
+            b.launch(stream)
+            e1.record(stream)
+            bt.append((e0, e1))
+        torch.cuda.synchronize()
+    alone_ms = [statistics.median(a.elapsed_time(c) for a, c in per[i]) for i in range(len(solves))]
+    batch_ms = sorted(a.elapsed_time(c) for a, c in bt)
+    plain_total = sum(alone_ms)
+    out = {"solves": len(solves), "triangles": sum(x.scene.triangle_count for x in solves),
+           "rays": sum(x.rc.layout["rays_total"] for x in solves),
+           "plain_solves_per_s": len(solves) / (plain_total / 1000.0),
+           "plain_p50_ms": statistics.median(alone_ms), "plain_p99_ms": sorted(alone_ms)[-1],
+           "batch_ms_p50": statistics.median(batch_ms), "batch_ms_p99": batch_ms[-1],
+           "batched_solves_per_s": len(solves) / (statistics.median(batch_ms) / 1000.0),
+           "mode": "one CUDA graph of parallel per-solve kernel chains (gi_batch)",
+           "spec": "scenes.batch_spec(0..63): tris log-U(5k, 500k), G 4..32 x 1-4 levels, 320x180..1920x1080, 2-5 cascades"}
+    out["speedup"] = out["batched_solves_per_s"] / out["plain_solves_per_s"]
+    b.destroy()
+    for x in solves:
+        x.destroy()
+    return out
+
+
 def run_reference(args, rank):
     """The reference's algorithm on the host cores (oracle/), on the same workload, config and metric."""
     if rank != 0:
@@ -326,6 +379,10 @@ def run_ours(args, rank, world, local_rank):
                        "d2h_bytes_per_step": int(irr_h.numel())},
                "gpu_launches": n_ev * (13 + (v.levels - 1) + 4 + p.cascades),
                "clocks": clk, "wall_s": wall}
+    if args.batch > 0:
+        bt = run_batched(args, ctx, stream, flush)
+        if out is not None:
+            out["batched"] = bt
     # the oracle on the host cores, rank 0 at N = 1 only
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, v, p, F, depth_h.numpy().reshape(H, W),
@@ -347,6 +404,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="colonnade", choices=["colonnade", "room"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -170,6 +170,16 @@ int gi_rc_set_stats(gi_rc *rc, uint32_t level);
  * (gi_vox_update) and the parameters are those of capture time: capture again after moving the windows. */
 int gi_rc_graph_capture(gi_rc *rc, gi_vox *vox, void *stream);
 int gi_rc_graph_launch(gi_rc *rc, void *stream);
+/* Batches (no counterpart in the reference, which solves one frame per queue submit): n independent solves, each
+ * an (rc, vox) pair with its own frame, G-buffer and scene, captured into ONE CUDA graph whose n solve chains are
+ * parallel branches, so the GPU runs the small kernels of uneven solves side by side.  Every handle may appear once.
+ * gi_batch_capture needs a stream that is not the legacy default stream; the graph reads frames, G-buffers and
+ * vertices at launch; capture again after moving a voxel window. */
+typedef struct gi_batch gi_batch;
+int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32_t n, gi_batch **out);
+int gi_batch_capture(gi_batch *batch, void *stream);
+int gi_batch_launch(gi_batch *batch, void *stream);
+int gi_batch_destroy(gi_batch *batch);
 /* Pass timing (the reference's per-pass timestamps, rcrun.ts:325-372): when on, every solve records CUDA events
  * between its passes; gi_rc_pass_times then gives the last solve's milliseconds of [vox (gi_solve only), giBuild,
  * giTrace, giMerge, giGather] (synchronises on the last event). */

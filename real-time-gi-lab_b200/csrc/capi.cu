@@ -534,6 +534,111 @@ int gi_rc_graph_launch(gi_rc *r, void *stream) {
   return GI_OK;
 }
 
+// ---- batches of solves --------------------------------------------------------------------------------------------------
+struct gi_batch {
+  gi_ctx *ctx;
+  uint32_t n = 0;
+  gi_rc **rcs = nullptr;
+  gi_vox **voxes = nullptr;
+  cudaStream_t *streams = nullptr;
+  cudaEvent_t *done = nullptr;
+  cudaEvent_t start = nullptr;
+  cudaGraphExec_t graph = nullptr;
+};
+
+static void free_batch(gi_batch *b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  for (uint32_t i = 0; i < b->n; i++) {
+    if (b->streams && b->streams[i]) cudaStreamDestroy(b->streams[i]);
+    if (b->done && b->done[i]) cudaEventDestroy(b->done[i]);
+  }
+  if (b->start) cudaEventDestroy(b->start);
+  delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done;
+}
+
+int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32_t n, gi_batch **out) {
+  if (!ctx || !rcs || !voxes || !out) return fail(GI_ERR_INVALID, "gi_batch_create: NULL argument");
+  *out = nullptr;
+  if (n < 1 || n > 4096) return fail(GI_ERR_INVALID, "gi_batch_create: %u solves (1..4096)", n);
+  for (uint32_t i = 0; i < n; i++) {
+    if (!rcs[i] || !voxes[i]) return fail(GI_ERR_INVALID, "gi_batch_create: solve %u has a NULL handle", i);
+    if (rcs[i]->ctx->device != ctx->device || voxes[i]->scene->ctx->device != ctx->device)
+      return fail(GI_ERR_INVALID, "gi_batch_create: solve %u lives on another device", i);
+    for (uint32_t j = 0; j < i; j++)
+      if (rcs[j] == rcs[i] || voxes[j] == voxes[i])
+        return fail(GI_ERR_INVALID, "gi_batch_create: solves %u and %u share a handle (their work would race)", j, i);
+  }
+  CK(cudaSetDevice(ctx->device), "gi_batch_create: cudaSetDevice");
+  gi_batch *b = new (std::nothrow) gi_batch;
+  if (!b) return fail(GI_ERR_OOM, "gi_batch_create: host allocation");
+  b->ctx = ctx;
+  b->rcs = new (std::nothrow) gi_rc *[n];
+  b->voxes = new (std::nothrow) gi_vox *[n];
+  b->streams = new (std::nothrow) cudaStream_t[n]();
+  b->done = new (std::nothrow) cudaEvent_t[n]();
+  if (!b->rcs || !b->voxes || !b->streams || !b->done) { free_batch(b); delete b; return fail(GI_ERR_OOM, "gi_batch_create: host allocation"); }
+  b->n = n;
+  cudaError_t e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming);
+  for (uint32_t i = 0; i < n && e == cudaSuccess; i++) {
+    b->rcs[i] = rcs[i];
+    b->voxes[i] = voxes[i];
+    e = cudaStreamCreateWithFlags(&b->streams[i], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done[i], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) { free_batch(b); delete b; return cuda_fail(e, "gi_batch_create"); }
+  *out = b;
+  return GI_OK;
+}
+
+int gi_batch_capture(gi_batch *b, void *stream) {
+  if (!b) return fail(GI_ERR_INVALID, "gi_batch_capture: NULL batch");
+  if (!stream) return fail(GI_ERR_INVALID, "gi_batch_capture: the legacy default stream cannot be captured; pass a stream");
+  for (uint32_t i = 0; i < b->n; i++)
+    if (!b->rcs[i]->frame_set || !b->rcs[i]->gbuf_set || !b->voxes[i]->updated)
+      return fail(GI_ERR_STATE, "gi_batch_capture: solve %u lacks its frame, G-buffer or voxel window", i);
+  CK(cudaSetDevice(b->ctx->device), "gi_batch_capture: cudaSetDevice");
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  cudaStream_t st = S(stream);
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "gi_batch_capture: begin");
+  int status = GI_OK;
+  cudaError_t e = cudaEventRecord(b->start, st);
+  for (uint32_t i = 0; i < b->n && e == cudaSuccess && status == GI_OK; i++) {
+    e = cudaStreamWaitEvent(b->streams[i], b->start, 0);   // fork: every solve's chain starts from the batch start
+    if (e != cudaSuccess) break;
+    bool timing = b->rcs[i]->timing;
+    b->rcs[i]->timing = false;
+    status = gi_solve(b->rcs[i], b->voxes[i], b->streams[i]);
+    b->rcs[i]->timing = timing;
+    if (status == GI_OK) e = cudaEventRecord(b->done[i], b->streams[i]);
+    if (e == cudaSuccess && status == GI_OK) e = cudaStreamWaitEvent(st, b->done[i], 0);   // join
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(st, &g);
+  if (status != GI_OK) { if (g) cudaGraphDestroy(g); return status; }
+  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture"); }
+  if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture: end");
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture: instantiate"); }
+  return GI_OK;
+}
+
+int gi_batch_launch(gi_batch *b, void *stream) {
+  if (!b) return fail(GI_ERR_INVALID, "gi_batch_launch: NULL batch");
+  if (!b->graph) return fail(GI_ERR_STATE, "gi_batch_launch: no graph captured");
+  CK(cudaSetDevice(b->ctx->device), "gi_batch_launch: cudaSetDevice");
+  CK(cudaGraphLaunch(b->graph, S(stream)), "gi_batch_launch");
+  return GI_OK;
+}
+
+int gi_batch_destroy(gi_batch *b) {
+  if (!b) return GI_OK;
+  cudaSetDevice(b->ctx->device);
+  free_batch(b);
+  delete b;
+  return GI_OK;
+}
+
 int gi_rc_set_timing(gi_rc *r, int on) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_timing: NULL rc");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_set_timing: cudaSetDevice");

@@ -243,3 +243,28 @@ class Rc:
         if self.handle:
             _lib.call("gi_rc_destroy", self.handle)
             self.handle = None
+
+
+class Batch:
+    """n independent solves captured into one CUDA graph of parallel solve chains (gi_batch_*)."""
+
+    def __init__(self, ctx: Context, rcs, voxes):
+        assert len(rcs) == len(voxes)
+        self.ctx, self.rcs, self.voxes = ctx, list(rcs), list(voxes)
+        n = len(rcs)
+        ra = (_P * n)(*[r.handle for r in rcs])
+        va = (_P * n)(*[v.handle for v in voxes])
+        h = _P()
+        _lib.call("gi_batch_create", ctx.handle, ra, va, n, C.byref(h))
+        self.handle = h
+
+    def capture(self, stream):
+        _lib.call("gi_batch_capture", self.handle, _stream(stream))
+
+    def launch(self, stream):
+        _lib.call("gi_batch_launch", self.handle, _stream(stream))
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_batch_destroy", self.handle)
+            self.handle = None

@@ -264,3 +264,63 @@ def colonnade_scene(seed: int = 0, nx: int = 40, nz: int = 16, rings: int = 8, s
     cam = Camera((1.25 + 0.0, 1.7, 1.25), (21.25, 1.3, -3.75), 60, 0.05)
     from .frame import SUN_E, SKY
     return b.scene(f"colonnade-{seed}", cam, sun_dir=(-0.4, 1.0, 0.3), sun_e=SUN_E, sky=SKY)
+
+
+def mixed_scene(seed: int, target_tris: int, area: float = 40.0, name: str = "") -> Scene:
+    """Procedural box/column mix of about target_tris triangles: a tiled ground, columns (16-segment cylinders) for
+    ~70 % of the triangles and axis-aligned boxes for the rest, two emissive panels, sun and sky."""
+    rng = PCG32(seed, stream=11)
+    mats = [Material("ground", (0.55, 0.52, 0.48, 1.0)), Material("stone", (0.78, 0.76, 0.7, 1.0)),
+            Material("lamp0", (0.9, 0.9, 0.9, 1.0), emissive=(10.0, 9.5, 8.5)),
+            Material("lamp1", (0.9, 0.9, 0.9, 1.0), emissive=(8.0, 9.0, 10.0))]
+    nbox_mats = 6
+    for k in range(nbox_mats):
+        mats.append(Material(f"box{k}", (rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), rng.uniform(0.1, 0.9), 1.0)))
+    b = Builder(mats)
+    h = area / 2
+    cells = 8
+    step = area / cells
+    b.mat = 0
+    for j in range(cells):
+        for i in range(cells):
+            x0, z0 = -h + i * step, -h + j * step
+            b.quad([x0, 0, z0 + step], [x0 + step, 0, z0 + step], [x0 + step, 0, z0], [x0, 0, z0])
+    col_budget = int(0.7 * target_tris)
+    seg, rings = 16, 8
+    per_col = 2 * seg * rings
+    ncol = max(1, col_budget // per_col)
+    b.mat = 1
+    for _ in range(ncol):
+        cx, cz = rng.uniform(-h + 1, h - 1), rng.uniform(-h + 1, h - 1)
+        if abs(cx) < 2 and abs(cz) < 2:
+            cx += 4.0
+        pos, nrm, tris = _cylinder(cx, cz, rng.uniform(0.15, 0.5), rng.uniform(2.0, 8.0), seg, rings)
+        b.mesh(pos, nrm, tris)
+    nbox = max(1, (target_tris - 2 * cells * cells - ncol * per_col) // 12)
+    for _ in range(nbox):
+        b.mat = 4 + int(rng.uniform(0, nbox_mats - 1e-9))
+        c = [rng.uniform(-h + 1, h - 1), rng.uniform(0.1, 5.0), rng.uniform(-h + 1, h - 1)]
+        if abs(c[0]) < 1.5 and abs(c[2]) < 1.5:
+            c[0] += 3.0
+        b.box(c, [rng.uniform(0.1, 1.0), rng.uniform(0.1, 1.0), rng.uniform(0.1, 1.0)])
+    for k in range(2):
+        b.mat = 2 + k
+        cx, cz = rng.uniform(-h / 2, h / 2), rng.uniform(-h / 2, h / 2)
+        b.quad_facing([cx - 1, 6.0, cz + 1], [cx + 1, 6.0, cz + 1], [cx + 1, 6.0, cz - 1], [cx - 1, 6.0, cz - 1], (0, -1, 0))
+    cam = Camera((0.0, 1.7, 0.0), (10.0, 1.2, 3.0), 60, 0.05)
+    from .frame import SUN_E, SKY
+    return b.scene(name or f"mix-{seed}", cam, sun_dir=(-0.3, 1.0, 0.4), sun_e=SUN_E, sky=SKY)
+
+
+def batch_spec(seed: int) -> dict:
+    """One solve of the uneven batch: triangle count log-uniform 5k-500k, a clipmap of 32^3-256^3 voxels per level
+    with 1-4 levels, a resolution of 320x180-1920x1080 (16:9) and 2-5 cascades, all drawn from PCG32(seed)."""
+    rng = PCG32(seed, stream=23)
+    tris = int(math.exp(rng.uniform(math.log(5_000), math.log(500_000))))
+    G = [4, 8, 16, 32][int(rng.uniform(0, 4 - 1e-9))]
+    levels = 1 + int(rng.uniform(0, 4 - 1e-9))
+    W = 320 + 16 * int(rng.uniform(0, (1920 - 320) / 16 + 1 - 1e-9))
+    H = max(180, (W * 9 // 16) // 4 * 4)
+    cascades = 2 + int(rng.uniform(0, 4 - 1e-9))
+    v0 = [0.1, 0.15, 0.2][int(rng.uniform(0, 3 - 1e-9))]
+    return {"seed": seed, "tris": tris, "G": G, "levels": levels, "width": W, "height": H, "cascades": cascades, "v0": v0}
