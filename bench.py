@@ -212,6 +212,33 @@ def run_batched(args, ctx, stream, flush):
     return out
 
 
+def run_served(args, ctx):
+    """The serving loop (continuous batching, 8 slots, HBM budget 150 GB, f16 atlases) against the plain one-at-a-time
+    loop, on Poisson request streams at several rates over 12 resident scenes of the batch distribution, each with
+    1-200 moving objects.  Latency = arrival to irradiance in host memory (host wall clock)."""
+    from rtgi import scenes, serve
+    specs = [scenes.batch_spec(1000 + s) for s in range(12)]
+    ex = serve.GpuExecutor(ctx, slots=8, atlas="f16")
+    srv = serve.Server(ex, specs, slots=8, hbm_budget=150e9)
+    for i, sp in enumerate(specs):   # scenes resident before the streams start
+        srv._ensure_resident(i, 0.0)
+    # warm-up
+    serve.plain_loop(ex, serve.poisson_arrivals(1000.0, 24, len(specs), seed=7))
+    rates = []
+    for rate in args.serve_rates:
+        n = int(min(args.serve_max, max(50, rate * args.serve_seconds)))
+        st = srv.run(serve.poisson_arrivals(rate, n, len(specs)))
+        pl = serve.plain_loop(ex, serve.poisson_arrivals(rate, n, len(specs)))
+        rates.append({"rate": rate, "requests": n, "served": st, "plain": pl,
+                      "throughput_ratio": st["solves_per_s"] / pl["solves_per_s"]})
+    res_bytes = srv.resident_bytes()
+    ex.destroy()
+    return {"scenes": len(specs), "slots": 8, "atlas": "f16", "hbm_budget_bytes": 150e9, "resident_bytes": res_bytes,
+            "objects_per_scene": [ex.n_objects(sp) for sp in specs], "rates": rates,
+            "latency": "arrival -> irradiance in pinned host memory, host wall clock",
+            "request": "pose objects (vertex upload), G-buffer, voxel rebuild, cascades, irradiance readback (f16)"}
+
+
 def run_reference(args, rank):
     """The reference's algorithm on the host cores (oracle/), on the same workload, config and metric."""
     if rank != 0:
@@ -383,6 +410,10 @@ def run_ours(args, rank, world, local_rank):
         bt = run_batched(args, ctx, stream, flush)
         if out is not None:
             out["batched"] = bt
+    if args.serve_rates:
+        sv = run_served(args, ctx)
+        if out is not None:
+            out["served"] = sv
     # the oracle on the host cores, rank 0 at N = 1 only
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, v, p, F, depth_h.numpy().reshape(H, W),
@@ -405,6 +436,10 @@ def main():
     ap.add_argument("--workload", default="colonnade", choices=["colonnade", "room"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
+    ap.add_argument("--serve-rates", type=float, nargs="*", default=[100, 500, 1000, 2000, 5000],
+                    help="request rates of the serving measurement (none: skip)")
+    ap.add_argument("--serve-seconds", type=float, default=1.0)
+    ap.add_argument("--serve-max", type=int, default=2000)
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

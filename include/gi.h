@@ -124,6 +124,9 @@ int gi_vox_used_bytes(gi_vox *vox, uint64_t *persistent, uint64_t *build_temp);
 int gi_vox_read_state(gi_vox *vox, uint32_t *ptr, uint32_t *occ, uint32_t *base, uint32_t *code, uint32_t *rep,
                       uint32_t *attr, float *plane, float *sunvis, void *stream);
 int gi_vox_destroy(gi_vox *vox);
+/* Bytes of device memory a voxel world / a scene holds (voxel.ts VoxWorld.bytes; the serving loop's HBM budget). */
+int gi_vox_bytes(gi_vox *vox, uint64_t *bytes);
+int gi_scene_bytes(gi_scene *scene, uint64_t *bytes);
 /* The voxel rebuild for callers that cannot allocate device memory (no counterpart in the reference).  Some callers
  * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
  * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point
@@ -160,6 +163,8 @@ int gi_solve(gi_rc *rc, gi_vox *vox, void *stream);
 int gi_rc_read_irradiance(gi_rc *rc, float *rgba, void *stream);
 /* The irradiance as stored: rgba16float (atlas F16/BF16) or rgba f32 (atlas F32).  Synchronises. */
 int gi_rc_read_irradiance_raw(gi_rc *rc, void *out, size_t bytes, void *stream);
+/* The same without synchronising: a stream-ordered copy into `out` (pinned memory makes it asynchronous). */
+int gi_rc_read_irradiance_async(gi_rc *rc, void *out, size_t bytes, void *stream);
 /* readCounts (rc.ts:1223-1232): the 80 counter words (rc.ts:173-175).  Synchronises. */
 int gi_rc_read_counts(gi_rc *rc, uint32_t counts[80], void *stream);
 /* setStats (rc.ts:1233): 0 off, 1 DDA step counters. */

@@ -63,7 +63,7 @@ struct gi_scene {
   uint4 *tri = nullptr;
   gi_material *mats = nullptr;
   uint32_t nverts = 0, ntris = 0, nmats = 0;
-  uint32_t *raster_big = nullptr, *raster_counter = nullptr;
+  uint32_t *raster_big = nullptr, *raster_counter = nullptr, *raster_pre = nullptr, *raster_sums = nullptr;
   float4 *stage = nullptr;   // vertex staging for updates (nverts * 2)
   SceneDev dev() const {
     SceneDev s;
@@ -106,7 +106,7 @@ struct gi_rc {
 
 static void free_scene(gi_scene *s) {
   cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
-  cudaFree(s->raster_big); cudaFree(s->raster_counter); cudaFree(s->stage);
+  cudaFree(s->raster_big); cudaFree(s->raster_counter); cudaFree(s->stage); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
 }
 static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
@@ -188,7 +188,8 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
   float4 *h4 = nullptr;
   do {
     if ((e = dalloc(&s->pos, nverts)) || (e = dalloc(&s->nrm, nverts)) || (e = dalloc(&s->tri, ntris)) ||
-        (e = dalloc(&s->mats, nmats)) || (e = dalloc(&s->raster_big, ntris)) || (e = dalloc(&s->raster_counter, 1)) ||
+        (e = dalloc(&s->mats, nmats)) || (e = dalloc(&s->raster_big, ntris)) || (e = dalloc(&s->raster_counter, 4)) ||
+        (e = dalloc(&s->raster_pre, ntris)) || (e = dalloc(&s->raster_sums, ntris / 256u + 1u)) ||
         (e = dalloc(&s->stage, (size_t)nverts * 2u)))
       break;
     h4 = new (std::nothrow) float4[nverts ? nverts : 1];
@@ -344,6 +345,19 @@ int gi_vox_read_state(gi_vox *v, uint32_t *ptr, uint32_t *occ, uint32_t *base, u
   return GI_OK;
 }
 
+int gi_vox_bytes(gi_vox *v, uint64_t *bytes) {
+  if (!v || !bytes) return fail(GI_ERR_INVALID, "gi_vox_bytes: NULL argument");
+  *bytes = v->bytes;
+  return GI_OK;
+}
+
+int gi_scene_bytes(gi_scene *s, uint64_t *bytes) {
+  if (!s || !bytes) return fail(GI_ERR_INVALID, "gi_scene_bytes: NULL argument");
+  *bytes = (uint64_t)s->nverts * (16u + 16u + 32u) + (uint64_t)s->ntris * (16u + 4u + 4u + 4u) +
+           (uint64_t)s->nmats * sizeof(gi_material) + 16u + (s->ntris / 256u + 1u) * 4u;
+  return GI_OK;
+}
+
 int gi_vox_destroy(gi_vox *v) {
   if (!v) return GI_OK;
   cudaSetDevice(v->scene->ctx->device);
@@ -470,7 +484,8 @@ int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   if (s->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_render_gbuffer: scene on another device");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_render_gbuffer: cudaSetDevice");
   CK(gi_launch_gbuffer(s->dev(), r->frame, r->W, r->H, r->depth, r->normal, r->keys, s->raster_big, s->ntris,
-                       s->raster_counter, r->ctx->sm_count, S(stream)), "gi_rc_render_gbuffer: launch");
+                       s->raster_counter, s->raster_pre, s->raster_sums, r->ctx->sm_count, S(stream)),
+     "gi_rc_render_gbuffer: launch");
   r->gbuf_set = true;
   return GI_OK;
 }
@@ -676,6 +691,15 @@ int gi_rc_read_irradiance_raw(gi_rc *r, void *out, size_t bytes, void *stream) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_raw: cudaSetDevice");
   CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance_raw: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_irradiance_raw: sync");
+  return GI_OK;
+}
+
+int gi_rc_read_irradiance_async(gi_rc *r, void *out, size_t bytes, void *stream) {
+  if (!r || !out) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_async: NULL argument");
+  size_t need = (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas);
+  if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_async: %zu bytes, need %zu", bytes, need);
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_async: cudaSetDevice");
+  CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance_async: copy");
   return GI_OK;
 }
 

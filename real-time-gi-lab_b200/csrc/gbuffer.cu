@@ -7,7 +7,7 @@
 //   depth  the largest wins (reversed Z, compare 'greater'); equal depths keep the smaller triangle index
 //          (one 64-bit atomicMax of depth bits << 32 | ~triangle per sample, order independent)
 //   normal normalize(interpolated vertex normal) * (front ? 1 : -1) (gbuffer.ts:94-95), stored as f16; w = 0
-// Triangles whose box covers more than 256 pixels go to a list processed one block per triangle.
+// Triangles whose box covers more than 256 pixels go to a list, cut into 256-pixel tiles taken from a queue.
 #include <cuda_runtime.h>
 
 #include "gi_dev.cuh"
@@ -113,19 +113,100 @@ __global__ void __launch_bounds__(256) k_raster_small(SceneDev s, const float *_
     for (int x = box[0]; x <= box[1]; x++) sample_pixel(F, W, x, y, p, t, keys);
 }
 
+// Big triangles, balanced: each one's box is cut into tiles of 256 pixels; k_raster_count gives every listed triangle
+// its tile count and an exclusive prefix within blocks of 256 triangles, k_raster_scan the block offsets and the
+// total, and blocks of k_raster_big take tiles from a queue (counter[1]) and find their triangle by binary search.
+__device__ __forceinline__ bool big_box(const SceneDev &s, const float *__restrict__ F, uint32_t W, uint32_t H,
+                                        uint32_t t, f3 p[3], int box[4]) {
+  uint4 idx = s.tri[t];
+  p[0] = ld3(s.pos[idx.x]); p[1] = ld3(s.pos[idx.y]); p[2] = ld3(s.pos[idx.z]);
+  return screen_box(F, W, H, p, box);
+}
+
+__device__ __forceinline__ uint32_t block_sum_256(uint32_t x, uint32_t *excl) {
+  __shared__ uint32_t ws[8];
+  __shared__ uint32_t tot;
+  uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5, inc = x;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+    if (lane >= (uint32_t)d) inc += y;
+  }
+  if (lane == 31u) ws[wid] = inc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t a = 0;
+    for (int k = 0; k < 8; k++) { uint32_t q = ws[k]; ws[k] = a; a += q; }
+    tot = a;
+  }
+  __syncthreads();
+  *excl = ws[wid] + inc - x;
+  uint32_t r = tot;
+  __syncthreads();
+  return r;
+}
+
+__global__ void __launch_bounds__(256) k_raster_count(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
+                                                      const uint32_t *big, uint32_t big_cap, uint32_t *counter,
+                                                      uint32_t *pre, uint32_t *sums) {
+  uint32_t items = min(counter[0], big_cap);
+  uint32_t nblk = (items + 255u) / 256u;
+  for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+    uint32_t it = b * 256u + threadIdx.x, tiles = 0;
+    if (it < items) {
+      f3 p[3];
+      int box[4];
+      if (big_box(s, F, W, H, big[it], p, box))
+        tiles = ((uint32_t)(box[1] - box[0] + 1) * (uint32_t)(box[3] - box[2] + 1) + 255u) / 256u;
+    }
+    uint32_t ex;
+    uint32_t tot = block_sum_256(tiles, &ex);
+    if (it < items) pre[it] = ex;
+    if (threadIdx.x == 0) sums[b] = tot;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_raster_scan(uint32_t big_cap, uint32_t *counter, uint32_t *sums) {
+  uint32_t nblk = (min(counter[0], big_cap) + 255u) / 256u;
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t b0 = 0; b0 < nblk; b0 += 256u) {
+    uint32_t i = b0 + threadIdx.x;
+    uint32_t ex;
+    uint32_t tot = block_sum_256(i < nblk ? sums[i] : 0u, &ex);
+    if (i < nblk) sums[i] = carry + ex;
+    __syncthreads();
+    if (threadIdx.x == 0) carry += tot;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { counter[2] = carry; counter[1] = 0u; }
+}
+
 __global__ void __launch_bounds__(256) k_raster_big(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
                                                     unsigned long long *keys, const uint32_t *big, uint32_t big_cap,
-                                                    const uint32_t *counter) {
-  uint32_t n = min(*counter, big_cap);
-  for (uint32_t item = blockIdx.x; item < n; item += gridDim.x) {
-    uint32_t t = big[item];
-    uint4 idx = s.tri[t];
-    f3 p[3] = {ld3(s.pos[idx.x]), ld3(s.pos[idx.y]), ld3(s.pos[idx.z])};
+                                                    uint32_t *counter, const uint32_t *pre, const uint32_t *sums) {
+  uint32_t items = min(counter[0], big_cap);
+  uint32_t tiles = counter[2];
+  __shared__ uint32_t s_tile;
+  for (;;) {
+    if (threadIdx.x == 0) s_tile = atomicAdd(&counter[1], 1u);
+    __syncthreads();
+    uint32_t tile = s_tile;
+    __syncthreads();
+    if (tile >= tiles) break;
+    uint32_t lo = 0, hi = items;   // the last triangle whose first tile is <= tile
+    while (hi - lo > 1u) {
+      uint32_t m = (lo + hi) >> 1;
+      if (pre[m] + sums[m >> 8] <= tile) lo = m; else hi = m;
+    }
+    uint32_t t = big[lo];
+    f3 p[3];
     int box[4];
-    if (!screen_box(F, W, H, p, box)) continue;
+    if (!big_box(s, F, W, H, t, p, box)) continue;
     uint32_t bw = (uint32_t)(box[1] - box[0] + 1), bh = (uint32_t)(box[3] - box[2] + 1);
-    for (uint32_t q = threadIdx.x; q < bw * bh; q += blockDim.x)
-      sample_pixel(F, W, box[0] + (int)(q % bw), box[2] + (int)(q / bw), p, t, keys);
+    uint32_t q = (tile - (pre[lo] + sums[lo >> 8])) * 256u + threadIdx.x;
+    if (q < bw * bh) sample_pixel(F, W, box[0] + (int)(q % bw), box[2] + (int)(q / bw), p, t, keys);
   }
 }
 
@@ -157,11 +238,13 @@ using namespace gi;
 
 cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
-                              uint32_t *counter, uint32_t sm_count, cudaStream_t st) {
+                              uint32_t *counter, uint32_t *pre, uint32_t *sums, uint32_t sm_count, cudaStream_t st) {
   cudaMemsetAsync(keys, 0, (size_t)W * H * sizeof(unsigned long long), st);
-  cudaMemsetAsync(counter, 0, sizeof(uint32_t), st);
+  cudaMemsetAsync(counter, 0, 4 * sizeof(uint32_t), st);
   if (s.ntris) k_raster_small<<<(s.ntris + 255u) / 256u, 256, 0, st>>>(s, frame_dev, W, H, keys, big, big_cap, counter);
-  k_raster_big<<<sm_count * 4u, 256, 0, st>>>(s, frame_dev, W, H, keys, big, big_cap, counter);
+  k_raster_count<<<sm_count * 2u, 256, 0, st>>>(s, frame_dev, W, H, big, big_cap, counter, pre, sums);
+  k_raster_scan<<<1, 256, 0, st>>>(big_cap, counter, sums);
+  k_raster_big<<<sm_count * 8u, 256, 0, st>>>(s, frame_dev, W, H, keys, big, big_cap, counter, pre, sums);
   dim3 g((W + 15u) / 16u, (H + 15u) / 16u);
   k_raster_resolve<<<g, 256, 0, st>>>(s, frame_dev, W, H, keys, depth, normal);
   return cudaGetLastError();

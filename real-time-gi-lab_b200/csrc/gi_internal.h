@@ -42,7 +42,7 @@ cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t
                                cudaEvent_t *ev = nullptr);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
-                              uint32_t *counter, uint32_t sm_count, cudaStream_t st);
+                              uint32_t *counter, uint32_t *pre, uint32_t *sums, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);

@@ -31,6 +31,8 @@ SIGNATURES = {
     "gi_vox_used_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gi_vox_read_state": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "gi_vox_destroy": (C.c_int, [_P]),
+    "gi_vox_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "gi_scene_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "gi_vox_build_noalloc": (C.c_int, [_P, C.POINTER(C.c_double), _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32,
                                        _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "gi_rc_create": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
@@ -42,6 +44,7 @@ SIGNATURES = {
     "gi_solve": (C.c_int, [_P, _P, _P]),
     "gi_rc_read_irradiance": (C.c_int, [_P, _P, _P]),
     "gi_rc_read_irradiance_raw": (C.c_int, [_P, _P, C.c_size_t, _P]),
+    "gi_rc_read_irradiance_async": (C.c_int, [_P, _P, C.c_size_t, _P]),
     "gi_rc_read_counts": (C.c_int, [_P, _P, _P]),
     "gi_rc_set_stats": (C.c_int, [_P, C.c_uint32]),
     "gi_rc_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),

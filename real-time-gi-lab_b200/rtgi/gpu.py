@@ -64,6 +64,11 @@ class SceneGpu:
         nrm = np.ascontiguousarray(nrm, dtype=np.float32)
         _lib.call("gi_scene_update_vertices", self.handle, first, pos.shape[0], _ptr(pos), _ptr(nrm), _stream(stream))
 
+    def bytes(self) -> int:
+        b = C.c_uint64()
+        _lib.call("gi_scene_bytes", self.handle, C.byref(b))
+        return b.value
+
     def destroy(self):
         if self.handle:
             _lib.call("gi_scene_destroy", self.handle)
@@ -113,6 +118,11 @@ class VoxWorld:
                   _stream(stream))
         st["hdr"] = self.read_counters(stream)["hdr"]
         return st
+
+    def bytes(self) -> int:
+        b = C.c_uint64()
+        _lib.call("gi_vox_bytes", self.handle, C.byref(b))
+        return b.value
 
     def destroy(self):
         if self.handle:
@@ -194,6 +204,10 @@ class Rc:
     def read_irradiance_raw(self, out: np.ndarray, stream=None):
         _lib.call("gi_rc_read_irradiance_raw", self.handle, out.ctypes.data if isinstance(out, np.ndarray) else out,
                   out.nbytes if isinstance(out, np.ndarray) else self.irr_bytes(), _stream(stream))
+
+    def read_irradiance_async(self, ptr: int, stream):
+        """Stream-ordered copy of the stored irradiance into host memory at ptr (irr_bytes() bytes), no sync."""
+        _lib.call("gi_rc_read_irradiance_async", self.handle, ptr, self.irr_bytes(), _stream(stream))
 
     def irr_bytes(self) -> int:
         return self.width * self.height * (16 if self.params.atlas == "f32" else 8)

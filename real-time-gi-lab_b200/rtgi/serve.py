@@ -1,0 +1,339 @@
+"""Serving loop for GI solves (no counterpart in the reference, which renders one frame per queue submit).
+
+Requests are frames of resident scenes: (scene, time).  Each scene has moving rigid objects whose pose follows from
+the time; a request poses them (vertex update), redraws the G-buffer, rebuilds the voxel clipmap and solves the
+cascades on the device, and reads the irradiance back.
+
+Continuous batching: requests that arrive while others are on the GPU are admitted as soon as a slot (a CUDA stream)
+and their scene are free, and run concurrently with the requests already in flight; a scene is never solved by two
+requests at once (its buffers are reused).  Residency: scenes stay on the device between requests; a request for a
+scene that is not resident loads it if the HBM budget holds it, after evicting scenes that are idle, least recently
+used first; otherwise it waits.  The plain loop serves the same requests one at a time in arrival order.
+
+The scheduler talks to an executor (GpuExecutor on the device; tests also drive it with a simulated one), so the
+admission and ordering logic runs without a GPU.
+"""
+from __future__ import annotations
+
+import collections
+import math
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional
+
+import numpy as np
+
+from . import configs, frame as fr, scenes
+
+
+@dataclass
+class Request:
+    rid: int
+    scene: int
+    t: float            # the frame's time (s): object poses follow from it
+    arrival: float      # arrival time (s after the start of the stream)
+    start: float = -1.0
+    done: float = -1.0
+    slot: int = -1
+
+    @property
+    def latency_ms(self) -> float:
+        return 1000.0 * (self.done - self.arrival)
+
+
+def poisson_arrivals(rate: float, n: int, n_scenes: int, seed: int = 1) -> List[Request]:
+    """n requests of a Poisson stream of `rate` per second (numpy PCG64, seed 1), scenes uniform."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    gaps = rng.exponential(1.0 / rate, n)
+    arr = np.cumsum(gaps) - gaps[0]
+    sc = rng.integers(0, n_scenes, n)
+    return [Request(i, int(sc[i]), float(arr[i]), float(arr[i])) for i in range(n)]
+
+
+class MovingObjects:
+    """Rigid boxes at the end of a scene's vertex array: rest vertices, and a pose (rotation about y through the
+    box centre, then a translation along a constant velocity, wrapped into the scene's area) at time t."""
+
+    def __init__(self, first_vertex: int, pos: np.ndarray, nrm: np.ndarray, centres: np.ndarray, vel: np.ndarray,
+                 omega: np.ndarray, half_area: float):
+        self.first = first_vertex
+        self.rest_pos = pos.astype(np.float64)
+        self.rest_nrm = nrm.astype(np.float64)
+        self.centres = centres
+        self.vel = vel
+        self.omega = omega
+        self.h = half_area
+        self.per = pos.shape[0] // max(1, centres.shape[0])
+
+    def pose(self, t: float):
+        k = self.centres.shape[0]
+        c = self.centres + self.vel * t
+        c[:, 0] = (c[:, 0] + self.h) % (2 * self.h) - self.h
+        c[:, 2] = (c[:, 2] + self.h) % (2 * self.h) - self.h
+        a = self.omega * t
+        ca, sa = np.cos(a), np.sin(a)
+        rel = self.rest_pos.reshape(k, self.per, 3) - self.centres[:, None, :]
+        x, y, z = rel[..., 0], rel[..., 1], rel[..., 2]
+        pos = np.stack([c[:, None, 0] + ca[:, None] * x + sa[:, None] * z, c[:, None, 1] + y,
+                        c[:, None, 2] - sa[:, None] * x + ca[:, None] * z], -1).reshape(-1, 3)
+        n = self.rest_nrm.reshape(k, self.per, 3)
+        nrm = np.stack([ca[:, None] * n[..., 0] + sa[:, None] * n[..., 2], n[..., 1],
+                        -sa[:, None] * n[..., 0] + ca[:, None] * n[..., 2]], -1).reshape(-1, 3)
+        return pos.astype(np.float32), nrm.astype(np.float32)
+
+
+def serving_scene(spec: dict, n_objects: int):
+    """A mixed scene of the batch distribution with n_objects moving boxes (sides 0.2-1 m, speeds 0-2 m/s)."""
+    base = scenes.mixed_scene(spec["seed"], max(1000, spec["tris"] - 12 * n_objects))
+    rng = scenes.PCG32(spec["seed"], stream=31)
+    b = scenes.Builder(list(base.materials) + [scenes.Material("object", (0.8, 0.3, 0.2, 1.0))])
+    # re-add the base geometry as one mesh per material, keeping its triangle order
+    b.pos = base.positions.astype(np.float64).reshape(-1).tolist()
+    b.nrm = base.normals.astype(np.float64).reshape(-1).tolist()
+    for m in range(len(base.materials)):
+        rows = base.tri[base.tri[:, 3] == m, :3]
+        b.idx[m] = rows.reshape(-1).tolist()
+    first = len(b.pos) // 3
+    b.mat = len(base.materials)
+    centres, vel, omega = [], [], []
+    for _ in range(n_objects):
+        c = [rng.uniform(-15, 15), rng.uniform(0.2, 1.5), rng.uniform(-15, 15)]
+        hs = [rng.uniform(0.1, 0.5) for _ in range(3)]
+        b.box(c, hs)
+        sp, ang = rng.uniform(0, 2), rng.uniform(0, 2 * math.pi)
+        centres.append(c)
+        vel.append([sp * math.cos(ang), 0.0, sp * math.sin(ang)])
+        omega.append(rng.uniform(-1, 1))
+    s = b.scene(base.name + f"-obj{n_objects}", base.camera, sun_dir=base.sun_dir, sun_e=base.sun_e, sky=base.sky)
+    objs = MovingObjects(first, s.positions[first:], s.normals[first:], np.array(centres), np.array(vel),
+                         np.array(omega), 20.0)
+    return s, objs
+
+
+@dataclass
+class SceneSlot:
+    spec: dict
+    bytes: int = 0
+    busy: bool = False
+    last_used: float = 0.0
+
+
+class Server:
+    """Continuous-batching scheduler over an executor with `slots` concurrent streams and an HBM budget."""
+
+    def __init__(self, executor, specs: List[dict], slots: int, hbm_budget: float):
+        self.ex = executor
+        self.specs = specs
+        self.slots = slots
+        self.budget = hbm_budget
+        self.resident: Dict[int, SceneSlot] = {}
+        self.stats = collections.Counter()
+
+    def resident_bytes(self) -> int:
+        return sum(s.bytes for s in self.resident.values())
+
+    def _ensure_resident(self, sid: int, now: float) -> bool:
+        if sid in self.resident:
+            return True
+        need = self.ex.scene_bytes(self.specs[sid])
+        if need > self.budget:
+            raise MemoryError(f"scene {sid} needs {need} bytes, more than the whole HBM budget {self.budget}")
+        while self.resident_bytes() + need > self.budget:
+            idle = [(s.last_used, k) for k, s in self.resident.items() if not s.busy]
+            if not idle:
+                return False
+            _, victim = min(idle)
+            self.ex.unload(victim)
+            del self.resident[victim]
+            self.stats["evictions"] += 1
+        self.resident[sid] = SceneSlot(self.specs[sid], self.ex.load(sid, self.specs[sid]), False, now)
+        self.stats["loads"] += 1
+        return True
+
+    def run(self, requests: List[Request], clock=None, on_done=None) -> dict:
+        """Serves the requests (sorted by arrival) in real time; returns latency and throughput statistics.
+        on_done(request, slot) runs at each completion, while the slot still holds the request's result."""
+        clock = clock or _WallClock()
+        pending: collections.deque = collections.deque()
+        inflight: Dict[int, Request] = {}
+        free = list(range(self.slots))
+        nxt = 0
+        done: List[Request] = []
+        t0 = clock.start()
+        while len(done) < len(requests):
+            now = clock.now()
+            while nxt < len(requests) and requests[nxt].arrival <= now:
+                pending.append(requests[nxt])
+                nxt += 1
+            # completions free slots and scenes
+            for slot, rq in list(inflight.items()):
+                if self.ex.poll(slot):
+                    rq.done = clock.now()
+                    if on_done is not None:
+                        on_done(rq, slot)
+                    done.append(rq)
+                    del inflight[slot]
+                    free.append(slot)
+                    self.resident[rq.scene].busy = False
+                    self.resident[rq.scene].last_used = rq.done
+            # admission: oldest first, skipping requests whose scene is busy or cannot be made resident yet
+            if free and pending:
+                keep = collections.deque()
+                while pending and free:
+                    rq = pending.popleft()
+                    sc = self.resident.get(rq.scene)
+                    if (sc is not None and sc.busy) or not self._ensure_resident(rq.scene, now):
+                        keep.append(rq)
+                        continue
+                    slot = free.pop()
+                    sc = self.resident[rq.scene]
+                    sc.busy = True
+                    rq.start, rq.slot = clock.now(), slot
+                    self.ex.launch(slot, rq.scene, rq.t)
+                    inflight[slot] = rq
+                keep.extend(pending)
+                pending = keep
+            self.stats["max_pending"] = max(self.stats["max_pending"], len(pending))
+            self.stats["max_inflight"] = max(self.stats["max_inflight"], len(inflight))
+            if not inflight and not pending and nxt < len(requests):
+                clock.sleep_until(requests[nxt].arrival)
+            else:
+                clock.idle()
+        return summarize(done, dict(self.stats))
+
+
+def plain_loop(executor, requests: List[Request], clock=None, on_done=None) -> dict:
+    """The plain per-solve loop: one request at a time, in arrival order, on one stream."""
+    clock = clock or _WallClock()
+    clock.start()
+    done = []
+    for rq in requests:
+        clock.sleep_until(rq.arrival)
+        rq.start, rq.slot = clock.now(), 0
+        executor.launch(0, rq.scene, rq.t)
+        executor.wait(0)
+        rq.done = clock.now()
+        if on_done is not None:
+            on_done(rq, 0)
+        done.append(rq)
+    return summarize(done, {})
+
+
+def summarize(done: List[Request], extra: dict) -> dict:
+    if not done:
+        return {"completed": 0}
+    lat = sorted(r.latency_ms for r in done)
+    span = max(r.done for r in done) - min(r.arrival for r in done)
+    p = lambda q: lat[min(len(lat) - 1, int(math.ceil(q * len(lat))) - 1)]
+    return {"completed": len(done), "solves_per_s": len(done) / span if span > 0 else float("inf"),
+            "p50_ms": p(0.5), "p99_ms": p(0.99), "max_ms": lat[-1], **extra}
+
+
+class _WallClock:
+    def start(self):
+        self.t0 = time.perf_counter()
+        return 0.0
+
+    def now(self):
+        return time.perf_counter() - self.t0
+
+    def sleep_until(self, t):
+        while self.now() < t:
+            pass
+
+    def idle(self):
+        pass
+
+
+class GpuExecutor:
+    """Runs requests on the device: per slot a CUDA stream, a completion event and a pinned readback buffer; per
+    resident scene its SceneGpu, VoxWorld, Rc (f16 atlases) and captured solve graph."""
+
+    def __init__(self, ctx, slots: int, atlas: str = "f16", n_objects=None):
+        import torch
+        from . import gpu
+        self.torch, self.gpu = torch, gpu
+        self.ctx = ctx
+        self.atlas = atlas
+        self.streams = [torch.cuda.Stream() for _ in range(max(1, slots))]
+        self.events = [None] * len(self.streams)
+        self.host = [None] * len(self.streams)
+        self.res: Dict[int, dict] = {}
+        self.n_objects = n_objects or (lambda spec: 1 + int(scenes.PCG32(spec["seed"], stream=41).uniform(0, 200)))
+        self.results: Dict[int, np.ndarray] = {}
+
+    def scene_bytes(self, spec: dict) -> int:
+        p, v = _params(spec, self.atlas)
+        W, H = spec["width"], spec["height"]
+        lay = configs.cascade_layout(p, W, H)
+        elem = 16 if self.atlas == "f32" else 8
+        rc = W * H * (4 + 8 + 8 + 16 + elem) + lay["probes_total"] * 52 + lay["rays_total"] * elem * 1
+        vox = (v.levels * v.G ** 3 + v.maxBricks * (530 + 1) + 16 * (1 << 18) + 8 * (1 << 18) + v.maxVoxels * 6) * 4
+        return int(rc + vox + 64 * spec["tris"])
+
+    def load(self, sid: int, spec: dict) -> int:
+        s, objs = serving_scene(spec, self.n_objects(spec))
+        p, v = _params(spec, self.atlas)
+        W, H = spec["width"], spec["height"]
+        F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=s.sun_e, sky=s.sky,
+                                         cascades=p.cascades, P=p.P))
+        st = self.streams[0]
+        sg = self.gpu.SceneGpu(self.ctx, s)
+        vw = self.gpu.VoxWorld(sg, v)
+        rc = self.gpu.Rc(self.ctx, p, W, H)
+        rc.set_frame(F, st)
+        pos, nrm = objs.pose(0.0)
+        sg.update_vertices(objs.first, pos, nrm, st)
+        rc.render_gbuffer(sg, st)
+        vw.update(s.camera.eye)
+        rc.graph_capture(vw, st)
+        st.synchronize()
+        self.res[sid] = {"sg": sg, "vw": vw, "rc": rc, "objs": objs, "scene": s}
+        return sg.bytes() + vw.bytes() + rc.bytes()
+
+    def unload(self, sid: int):
+        r = self.res.pop(sid)
+        self.torch.cuda.synchronize()
+        for k in ("rc", "vw", "sg"):
+            r[k].destroy()
+
+    def launch(self, slot: int, sid: int, t: float):
+        r = self.res[sid]
+        st = self.streams[slot]
+        pos, nrm = r["objs"].pose(t)
+        r["sg"].update_vertices(r["objs"].first, pos, nrm, st)
+        r["rc"].render_gbuffer(r["sg"], st)
+        r["rc"].graph_launch(st)
+        n = r["rc"].irr_bytes()
+        if self.host[slot] is None or self.host[slot].numel() < n:
+            self.host[slot] = self.torch.empty(n, dtype=self.torch.uint8).pin_memory()
+        r["rc"].read_irradiance_async(self.host[slot].data_ptr(), st)
+        ev = self.torch.cuda.Event()
+        ev.record(st)
+        self.events[slot] = (ev, sid, n)
+
+    def poll(self, slot: int) -> bool:
+        e = self.events[slot]
+        return e is None or e[0].query()
+
+    def wait(self, slot: int):
+        e = self.events[slot]
+        if e is not None:
+            e[0].synchronize()
+
+    def result(self, slot: int) -> np.ndarray:
+        ev, sid, n = self.events[slot]
+        ev.synchronize()
+        return self.host[slot][:n].numpy().copy()
+
+    def destroy(self):
+        for sid in list(self.res):
+            self.unload(sid)
+
+
+def _params(spec: dict, atlas: str):
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": spec["cascades"]})
+    G, L = spec["G"], spec["levels"]
+    v = configs.vox_params({"v0": spec["v0"], "levels": L, "G": G, "maxBricks": min(L * G ** 3, 32768),
+                            "maxVoxels": 1 << 21})
+    return p, v
