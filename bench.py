@@ -212,6 +212,16 @@ def run_batched(args, ctx, stream, flush):
     return out
 
 
+def run_precision(args, ctx):
+    """Irradiance error of the f32/f16/bf16 atlases against the FP64 merge + gather, colonnade with 64 moving boxes,
+    clipmap rebuilt every frame (rtgi.precision)."""
+    from rtgi import precision
+    t0 = time.time()
+    r = precision.run(ctx, frames=args.precision_frames)
+    r["wall_s"] = time.time() - t0
+    return r
+
+
 def run_served(args, ctx):
     """The serving loop (continuous batching, 8 slots, HBM budget 150 GB, f16 atlases) against the plain one-at-a-time
     loop, on Poisson request streams at several rates over 12 resident scenes of the batch distribution, each with
@@ -404,7 +414,7 @@ def run_ours(args, rank, world, local_rank):
                "e2e": {"value": e2e_value, "unit": "solves/s",
                        "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
                        "d2h_bytes_per_step": int(irr_h.numel())},
-               "gpu_launches": n_ev * (13 + (v.levels - 1) + 4 + p.cascades),
+               "gpu_launches": n_ev * (16 + (v.levels - 1) + 4 + p.cascades),
                "clocks": clk, "wall_s": wall}
     if args.batch > 0:
         bt = run_batched(args, ctx, stream, flush)
@@ -414,6 +424,10 @@ def run_ours(args, rank, world, local_rank):
         sv = run_served(args, ctx)
         if out is not None:
             out["served"] = sv
+    if args.precision_frames > 0:
+        pr = run_precision(args, ctx)
+        if out is not None:
+            out["precision"] = pr
     # the oracle on the host cores, rank 0 at N = 1 only
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, v, p, F, depth_h.numpy().reshape(H, W),
@@ -440,6 +454,8 @@ def main():
                     help="request rates of the serving measurement (none: skip)")
     ap.add_argument("--serve-seconds", type=float, default=1.0)
     ap.add_argument("--serve-max", type=int, default=2000)
+    ap.add_argument("--precision-frames", type=int, default=100,
+                    help="frames of the atlas precision study (colonnade + 64 moving boxes; 0: skip)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -163,7 +163,8 @@ int gi_solve(gi_rc *rc, gi_vox *vox, void *stream);
 int gi_rc_read_irradiance(gi_rc *rc, float *rgba, void *stream);
 /* The irradiance as stored: rgba16float (atlas F16/BF16) or rgba f32 (atlas F32).  Synchronises. */
 int gi_rc_read_irradiance_raw(gi_rc *rc, void *out, size_t bytes, void *stream);
-/* The same without synchronising: a stream-ordered copy into `out` (pinned memory makes it asynchronous). */
+/* The same without synchronising: a stream-ordered copy into `out`, host or device memory (pinned host memory makes
+ * it asynchronous). */
 int gi_rc_read_irradiance_async(gi_rc *rc, void *out, size_t bytes, void *stream);
 /* readCounts (rc.ts:1223-1232): the 80 counter words (rc.ts:173-175).  Synchronises. */
 int gi_rc_read_counts(gi_rc *rc, uint32_t counts[80], void *stream);
@@ -206,6 +207,15 @@ enum {
 int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
 int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);
 int gi_rc_set_debug_hits(gi_rc *rc, int on);
+/* FP64 reference of the merge, SH projection and gather (no counterpart in the reference, whose atlases are f16): the
+ * last solve's traced intervals, kept in f32 by gi_rc_set_debug_hits, merged (mergeScreen rc.ts:710-743), projected
+ * (projectSH rc.ts:752-774) and gathered (gatherScreen rc.ts:929-954) in double precision with no rounding between
+ * the stages.  The yardstick of the f32/f16/bf16 atlas error.  Needs an F32 atlas with debug hits on (GI_ERR_STATE
+ * otherwise); allocates its f64 buffers (32 bytes per ray and per pixel) on the first call.  Stream-ordered. */
+int gi_rc_merge_gather_f64(gi_rc *rc, void *stream);
+/* W*H*4 doubles (rgb, a = 1 valid / 0 background) of the last gi_rc_merge_gather_f64, into host or device memory.
+ * Synchronises. */
+int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);
 int gi_rc_destroy(gi_rc *rc);
 
 #ifdef __cplusplus

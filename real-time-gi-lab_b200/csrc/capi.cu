@@ -93,6 +93,9 @@ struct gi_rc {
   float4 *stage = nullptr;
   uint4 *hits = nullptr;
   void *rad_traced = nullptr;
+  void *rad64 = nullptr, *irr64 = nullptr;   // FP64 reference buffers (gi_rc_merge_gather_f64), on first use
+  double *sh64 = nullptr;
+  bool have64 = false;
   size_t rad_elem_bytes = 0, sh_elems = 0;
   bool frame_set = false, gbuf_set = false, debug_hits = false;
   uint64_t bytes = 0;
@@ -119,7 +122,7 @@ static void free_rc(gi_rc *r) {
   for (cudaEvent_t &e : r->ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
   cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->keys); cudaFree(r->stage);
-  cudaFree(r->hits); cudaFree(r->rad_traced);
+  cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs);
 }
@@ -699,7 +702,7 @@ int gi_rc_read_irradiance_async(gi_rc *r, void *out, size_t bytes, void *stream)
   size_t need = (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas);
   if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_async: %zu bytes, need %zu", bytes, need);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_async: cudaSetDevice");
-  CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance_async: copy");
+  CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDefault, S(stream)), "gi_rc_read_irradiance_async: copy");
   return GI_OK;
 }
 
@@ -772,6 +775,38 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_buffer: cudaSetDevice");
   CK(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_buffer: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_buffer: sync");
+  return GI_OK;
+}
+
+int gi_rc_merge_gather_f64(gi_rc *r, void *stream) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_merge_gather_f64: NULL rc");
+  if (r->p.atlas != GI_ATLAS_F32) return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: needs an F32 atlas");
+  if (!r->debug_hits || !r->rad_traced)
+    return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: the traced intervals are not kept (gi_rc_set_debug_hits)");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_merge_gather_f64: cudaSetDevice");
+  size_t npx = (size_t)r->W * r->H, np0 = (size_t)r->dev.c[0].tiles_x * r->dev.c[0].tiles_y;
+  if (!r->rad64) {
+    cudaError_t e;
+    if ((e = cudaMalloc(&r->rad64, (size_t)r->dev.rays_total * 32u)) || (e = cudaMalloc(&r->sh64, np0 * 27u * 8u)) ||
+        (e = cudaMalloc(&r->irr64, npx * 32u))) {
+      cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
+      r->rad64 = r->irr64 = nullptr; r->sh64 = nullptr;
+      return cuda_fail(e, "gi_rc_merge_gather_f64: allocate");
+    }
+  }
+  CK(gi_launch_merge_gather_f64(r->dev, reinterpret_cast<const float4 *>(r->rad_traced), r->rad64, r->sh64, r->irr64,
+                                S(stream)), "gi_rc_merge_gather_f64: launch");
+  r->have64 = true;
+  return GI_OK;
+}
+
+int gi_rc_read_irradiance_f64(gi_rc *r, double *rgba, void *stream) {
+  if (!r || !rgba) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_f64: NULL argument");
+  if (!r->have64) return fail(GI_ERR_STATE, "gi_rc_read_irradiance_f64: no gi_rc_merge_gather_f64 ran");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_f64: cudaSetDevice");
+  CK(cudaMemcpyAsync(rgba, r->irr64, (size_t)r->W * r->H * 32u, cudaMemcpyDefault, S(stream)),
+     "gi_rc_read_irradiance_f64: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_irradiance_f64: sync");
   return GI_OK;
 }
 

@@ -46,3 +46,7 @@ cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uin
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);
+// FP64 reference of merge + SH + gather from the f32 traced atlas: rad64 rays_total x 4 doubles, sh64 27 doubles per
+// cascade-0 probe, irr64 W*H x 4 doubles.
+cudaError_t gi_launch_merge_gather_f64(const gi::RcDev &r, const float4 *traced, void *rad64, double *sh64, void *irr64,
+                                       cudaStream_t st);

@@ -205,8 +205,21 @@ class Rc:
         _lib.call("gi_rc_read_irradiance_raw", self.handle, out.ctypes.data if isinstance(out, np.ndarray) else out,
                   out.nbytes if isinstance(out, np.ndarray) else self.irr_bytes(), _stream(stream))
 
+    def merge_gather_f64(self, stream=None):
+        """FP64 reference of merge + SH + gather from the last trace (f32 atlas, debug hits on)."""
+        _lib.call("gi_rc_merge_gather_f64", self.handle, _stream(stream))
+
+    def read_irradiance_f64(self, ptr: Optional[int] = None, stream=None) -> Optional[np.ndarray]:
+        """The FP64 irradiance, (H, W, 4) doubles; into the host or device memory at ptr when given."""
+        if ptr is not None:
+            _lib.call("gi_rc_read_irradiance_f64", self.handle, ptr, _stream(stream))
+            return None
+        out = np.zeros((self.height, self.width, 4), np.float64)
+        _lib.call("gi_rc_read_irradiance_f64", self.handle, _ptr(out), _stream(stream))
+        return out
+
     def read_irradiance_async(self, ptr: int, stream):
-        """Stream-ordered copy of the stored irradiance into host memory at ptr (irr_bytes() bytes), no sync."""
+        """Stream-ordered copy of the stored irradiance into host or device memory at ptr (irr_bytes() bytes)."""
         _lib.call("gi_rc_read_irradiance_async", self.handle, ptr, self.irr_bytes(), _stream(stream))
 
     def irr_bytes(self) -> int:

@@ -24,6 +24,7 @@ from typing import Dict, List, Optional
 import numpy as np
 
 from . import configs, frame as fr, scenes
+from .movers import MovingObjects, with_moving_boxes  # noqa: F401  (MovingObjects: re-exported)
 
 
 @dataclass
@@ -50,64 +51,10 @@ def poisson_arrivals(rate: float, n: int, n_scenes: int, seed: int = 1) -> List[
     return [Request(i, int(sc[i]), float(arr[i]), float(arr[i])) for i in range(n)]
 
 
-class MovingObjects:
-    """Rigid boxes at the end of a scene's vertex array: rest vertices, and a pose (rotation about y through the
-    box centre, then a translation along a constant velocity, wrapped into the scene's area) at time t."""
-
-    def __init__(self, first_vertex: int, pos: np.ndarray, nrm: np.ndarray, centres: np.ndarray, vel: np.ndarray,
-                 omega: np.ndarray, half_area: float):
-        self.first = first_vertex
-        self.rest_pos = pos.astype(np.float64)
-        self.rest_nrm = nrm.astype(np.float64)
-        self.centres = centres
-        self.vel = vel
-        self.omega = omega
-        self.h = half_area
-        self.per = pos.shape[0] // max(1, centres.shape[0])
-
-    def pose(self, t: float):
-        k = self.centres.shape[0]
-        c = self.centres + self.vel * t
-        c[:, 0] = (c[:, 0] + self.h) % (2 * self.h) - self.h
-        c[:, 2] = (c[:, 2] + self.h) % (2 * self.h) - self.h
-        a = self.omega * t
-        ca, sa = np.cos(a), np.sin(a)
-        rel = self.rest_pos.reshape(k, self.per, 3) - self.centres[:, None, :]
-        x, y, z = rel[..., 0], rel[..., 1], rel[..., 2]
-        pos = np.stack([c[:, None, 0] + ca[:, None] * x + sa[:, None] * z, c[:, None, 1] + y,
-                        c[:, None, 2] - sa[:, None] * x + ca[:, None] * z], -1).reshape(-1, 3)
-        n = self.rest_nrm.reshape(k, self.per, 3)
-        nrm = np.stack([ca[:, None] * n[..., 0] + sa[:, None] * n[..., 2], n[..., 1],
-                        -sa[:, None] * n[..., 0] + ca[:, None] * n[..., 2]], -1).reshape(-1, 3)
-        return pos.astype(np.float32), nrm.astype(np.float32)
-
-
 def serving_scene(spec: dict, n_objects: int):
     """A mixed scene of the batch distribution with n_objects moving boxes (sides 0.2-1 m, speeds 0-2 m/s)."""
     base = scenes.mixed_scene(spec["seed"], max(1000, spec["tris"] - 12 * n_objects))
-    rng = scenes.PCG32(spec["seed"], stream=31)
-    b = scenes.Builder(list(base.materials) + [scenes.Material("object", (0.8, 0.3, 0.2, 1.0))])
-    # re-add the base geometry as one mesh per material, keeping its triangle order
-    b.pos = base.positions.astype(np.float64).reshape(-1).tolist()
-    b.nrm = base.normals.astype(np.float64).reshape(-1).tolist()
-    for m in range(len(base.materials)):
-        rows = base.tri[base.tri[:, 3] == m, :3]
-        b.idx[m] = rows.reshape(-1).tolist()
-    first = len(b.pos) // 3
-    b.mat = len(base.materials)
-    centres, vel, omega = [], [], []
-    for _ in range(n_objects):
-        c = [rng.uniform(-15, 15), rng.uniform(0.2, 1.5), rng.uniform(-15, 15)]
-        hs = [rng.uniform(0.1, 0.5) for _ in range(3)]
-        b.box(c, hs)
-        sp, ang = rng.uniform(0, 2), rng.uniform(0, 2 * math.pi)
-        centres.append(c)
-        vel.append([sp * math.cos(ang), 0.0, sp * math.sin(ang)])
-        omega.append(rng.uniform(-1, 1))
-    s = b.scene(base.name + f"-obj{n_objects}", base.camera, sun_dir=base.sun_dir, sun_e=base.sun_e, sky=base.sky)
-    objs = MovingObjects(first, s.positions[first:], s.normals[first:], np.array(centres), np.array(vel),
-                         np.array(omega), 20.0)
-    return s, objs
+    return with_moving_boxes(base, n_objects, scenes.PCG32(spec["seed"], stream=31))
 
 
 @dataclass

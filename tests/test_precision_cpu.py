@@ -1,0 +1,62 @@
+"""Host logic of the precision study and the moving boxes, on the CPU."""
+import numpy as np
+import torch
+
+from rtgi import movers, precision, scenes, serve
+
+
+def _small_base():
+    b = scenes.Builder([scenes.Material("ground", (0.5, 0.5, 0.5, 1.0))])
+    b.quad([-5, 0, 5], [5, 0, 5], [5, 0, -5], [-5, 0, -5])
+    return b.scene("ground", scenes.Camera((0, 1.7, 0), (5, 1.5, 0), 60, 0.05))
+
+
+def test_moving_boxes_are_rigid_and_wrap():
+    base = _small_base()
+    s, objs = movers.with_moving_boxes(base, 5, scenes.PCG32(3, stream=41), area=(2.0, -1.0, 3.0, 2.0))
+    assert s.triangle_count == base.triangle_count + 5 * 12
+    assert objs.first == base.positions.shape[0]
+    p0, n0 = objs.pose(0.0)
+    np.testing.assert_allclose(p0, s.positions[objs.first:], atol=1e-6)
+    p1, n1 = objs.pose(7.3)
+    a, b = p0.reshape(5, -1, 3).astype(np.float64), p1.reshape(5, -1, 3).astype(np.float64)
+    da = np.linalg.norm(a[:, :, None] - a[:, None], axis=-1)
+    db = np.linalg.norm(b[:, :, None] - b[:, None], axis=-1)
+    np.testing.assert_allclose(da, db, atol=1e-4)                     # rigid
+    np.testing.assert_allclose(np.linalg.norm(n1, axis=-1), 1.0, atol=1e-6)
+    c = b.mean(axis=1)
+    ax, az, hx, hz = objs.area
+    assert (np.abs(c[:, 0] - ax) <= hx + 1.0).all() and (np.abs(c[:, 2] - az) <= hz + 1.0).all()
+    np.testing.assert_allclose(c[:, 1], a.mean(axis=1)[:, 1], atol=1e-5)   # no vertical motion
+
+
+def test_serving_scene_unchanged_by_the_movers_module():
+    spec = scenes.batch_spec(2)
+    s1, o1 = serve.serving_scene(spec, 9)
+    s2, o2 = serve.serving_scene(spec, 9)
+    assert np.array_equal(s1.positions, s2.positions) and o1.first == o2.first
+    assert o1.area == (0.0, 0.0, 20.0, 20.0)
+
+
+def test_error_stats_quantiles_and_norms():
+    st = precision.ErrorStats(torch, torch.device("cpu"))
+    ref = torch.ones((4, 8, 4), dtype=torch.float64)
+    ref[0, 0, 3] = 0.0                       # background pixel: not counted
+    x = (ref * (1 + 1e-3)).to(torch.float32)
+    x[..., 3] = ref[..., 3].to(torch.float32)
+    st.add(x, ref)
+    s = st.summary()
+    assert s["values"] == 31 * 3 and s["alpha_mismatch"] == 0
+    assert 0.9e-3 < s["mean_rel"] < 1.1e-3 and 0.9e-3 < s["rel_l2"] < 1.1e-3
+    assert 1e-3 <= s["p50_rel"] <= 10 ** -2.8 and 1e-3 <= s["p99_rel"] <= 10 ** -2.8
+    x2 = x.clone()
+    x2[1, 1, 3] = 0.0
+    st.add(x2, ref)
+    assert st.summary()["alpha_mismatch"] == 1
+
+
+def test_colonnade_precision_scene():
+    s, objs = precision.precision_scene(0, 64)
+    assert s.triangle_count == scenes.colonnade_scene(0).triangle_count + 64 * 12
+    p, v = precision.colonnade_params("f16")
+    assert p.atlas == "f16" and p.cascades == 5 and v.levels == 4 and v.G == 16
