@@ -127,6 +127,10 @@ int gi_vox_destroy(gi_vox *vox);
 /* Bytes of device memory a voxel world / a scene holds (voxel.ts VoxWorld.bytes; the serving loop's HBM budget). */
 int gi_vox_bytes(gi_vox *vox, uint64_t *bytes);
 int gi_scene_bytes(gi_scene *scene, uint64_t *bytes);
+/* Capacity, in entries, of the G-buffer raster's per-tile triangle lists (default 8 per triangle, at least 2^20).
+ * Triangles past it are tested by every tile instead: slower, the same G-buffer.  Frees the old list (which waits for
+ * work still using it). */
+int gi_scene_set_raster_capacity(gi_scene *scene, uint32_t entries);
 /* The voxel rebuild for callers that cannot allocate device memory (no counterpart in the reference).  Some callers
  * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
  * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point

@@ -57,13 +57,24 @@ struct gi_ctx {
   uint32_t sm_count;
 };
 
+// Capacity of the raster's per-tile lists: 8 tiles per triangle, at least 2^20 entries (triangles past it are walked
+// by every tile instead, so the G-buffer does not depend on it)
+static uint32_t raster_list_cap(uint32_t ntris) {
+  uint64_t c = (uint64_t)ntris * 8u;
+  return (uint32_t)(c < (1u << 20) ? (1u << 20) : (c > 0xffffffffull ? 0xffffffffull : c));
+}
+
 struct gi_scene {
   gi_ctx *ctx;
   float4 *pos = nullptr, *nrm = nullptr;
   uint4 *tri = nullptr;
   gi_material *mats = nullptr;
   uint32_t nverts = 0, ntris = 0, nmats = 0;
-  uint32_t *raster_big = nullptr, *raster_counter = nullptr, *raster_pre = nullptr, *raster_sums = nullptr;
+  // G-buffer raster scratch (gbuffer.cu): two renders of one scene must not overlap on the GPU
+  float4 *raster_rec = nullptr;
+  uint32_t *raster_ntile = nullptr, *raster_pre = nullptr, *raster_sums = nullptr, *raster_counter = nullptr;
+  uint32_t *raster_list = nullptr, *raster_over = nullptr;
+  uint32_t raster_cap = 0;
   float4 *stage = nullptr;   // vertex staging for updates (nverts * 2)
   SceneDev dev() const {
     SceneDev s;
@@ -89,7 +100,8 @@ struct gi_rc {
   float *frame = nullptr;
   float *depth = nullptr;
   uint2 *normal = nullptr;
-  unsigned long long *keys = nullptr;
+  uint32_t *tile_cnt = nullptr, *tile_fill = nullptr;   // G-buffer raster: per 16 x 16 tile (+1)
+  uint32_t ntiles = 0;
   float4 *stage = nullptr;
   uint4 *hits = nullptr;
   void *rad_traced = nullptr;
@@ -109,7 +121,8 @@ struct gi_rc {
 
 static void free_scene(gi_scene *s) {
   cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
-  cudaFree(s->raster_big); cudaFree(s->raster_counter); cudaFree(s->stage); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
+  cudaFree(s->raster_rec); cudaFree(s->raster_ntile); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
+  cudaFree(s->raster_counter); cudaFree(s->raster_list); cudaFree(s->raster_over); cudaFree(s->stage);
 }
 static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
@@ -121,7 +134,7 @@ static void free_rc(gi_rc *r) {
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
   for (cudaEvent_t &e : r->ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
-  cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->keys); cudaFree(r->stage);
+  cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->tile_cnt); cudaFree(r->tile_fill); cudaFree(r->stage);
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs);
@@ -187,12 +200,15 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
   gi_scene *s = new (std::nothrow) gi_scene;
   if (!s) return fail(GI_ERR_OOM, "gi_scene_upload: host allocation");
   s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats;
+  s->raster_cap = raster_list_cap(ntris);
   cudaError_t e = cudaSuccess;
   float4 *h4 = nullptr;
   do {
     if ((e = dalloc(&s->pos, nverts)) || (e = dalloc(&s->nrm, nverts)) || (e = dalloc(&s->tri, ntris)) ||
-        (e = dalloc(&s->mats, nmats)) || (e = dalloc(&s->raster_big, ntris)) || (e = dalloc(&s->raster_counter, 4)) ||
-        (e = dalloc(&s->raster_pre, ntris)) || (e = dalloc(&s->raster_sums, ntris / 256u + 1u)) ||
+        (e = dalloc(&s->mats, nmats)) || (e = dalloc(&s->raster_rec, (size_t)3u * ntris)) ||
+        (e = dalloc(&s->raster_ntile, ntris)) || (e = dalloc(&s->raster_pre, ntris)) ||
+        (e = dalloc(&s->raster_sums, ntris / 256u + 1u)) || (e = dalloc(&s->raster_counter, 4)) ||
+        (e = dalloc(&s->raster_list, s->raster_cap)) || (e = dalloc(&s->raster_over, ntris)) ||
         (e = dalloc(&s->stage, (size_t)nverts * 2u)))
       break;
     h4 = new (std::nothrow) float4[nverts ? nverts : 1];
@@ -354,10 +370,23 @@ int gi_vox_bytes(gi_vox *v, uint64_t *bytes) {
   return GI_OK;
 }
 
+int gi_scene_set_raster_capacity(gi_scene *s, uint32_t entries) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_set_raster_capacity: NULL scene");
+  if (entries < 1) return fail(GI_ERR_INVALID, "gi_scene_set_raster_capacity: capacity must be >= 1");
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_set_raster_capacity: cudaSetDevice");
+  uint32_t *list = nullptr;
+  cudaError_t e = dalloc(&list, entries);
+  if (e) return cuda_fail(e, "gi_scene_set_raster_capacity");
+  cudaFree(s->raster_list);   // synchronises with work still using the old list
+  s->raster_list = list;
+  s->raster_cap = entries;
+  return GI_OK;
+}
+
 int gi_scene_bytes(gi_scene *s, uint64_t *bytes) {
   if (!s || !bytes) return fail(GI_ERR_INVALID, "gi_scene_bytes: NULL argument");
-  *bytes = (uint64_t)s->nverts * (16u + 16u + 32u) + (uint64_t)s->ntris * (16u + 4u + 4u + 4u) +
-           (uint64_t)s->nmats * sizeof(gi_material) + 16u + (s->ntris / 256u + 1u) * 4u;
+  *bytes = (uint64_t)s->nverts * (16u + 16u + 32u) + (uint64_t)s->ntris * (16u + 48u + 4u + 4u + 4u) +
+           (uint64_t)s->nmats * sizeof(gi_material) + 16u + (s->ntris / 256u + 1u) * 4u + (uint64_t)s->raster_cap * 4u;
   return GI_OK;
 }
 
@@ -419,13 +448,15 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   r->rad_elem_bytes = atlas_elem_bytes(p->atlas);
   r->sh_elems = (size_t)d.c[0].tiles_x * d.c[0].tiles_y * 8u;
   size_t npx = (size_t)W * H;
+  r->ntiles = gi_raster_tiles(W, H);
   cudaError_t e;
   ProbeDev *probes = nullptr;
   void *rad = nullptr, *sh = nullptr, *irr = nullptr;
   uint32_t *counts = nullptr, *plevel = nullptr;
   float4 *dirs = nullptr;
   if ((e = dalloc(&r->frame, 160)) || (e = dalloc(&r->depth, npx)) || (e = dalloc(&r->normal, npx)) ||
-      (e = dalloc(&r->keys, npx)) || (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
+      (e = dalloc(&r->tile_cnt, (size_t)r->ntiles + 1u)) || (e = dalloc(&r->tile_fill, r->ntiles)) ||
+      (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->rad_elem_bytes)) ||
       (e = cudaMalloc(&irr, npx * atlas_elem_bytes(p->atlas))) || (e = dalloc(&counts, 96)) ||
       (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, dir_total))) {
@@ -442,7 +473,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     delete r;
     return cuda_fail(e, "gi_rc_create: direction table");
   }
-  r->bytes = 160 * 4 + npx * (4 + 8 + 8 + 16) + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
+  r->bytes = 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->rad_elem_bytes + npx * atlas_elem_bytes(p->atlas) + 96 * 4;
   *out = r;
   return GI_OK;
@@ -486,8 +517,11 @@ int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_render_gbuffer: no frame set");
   if (s->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_render_gbuffer: scene on another device");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_render_gbuffer: cudaSetDevice");
-  CK(gi_launch_gbuffer(s->dev(), r->frame, r->W, r->H, r->depth, r->normal, r->keys, s->raster_big, s->ntris,
-                       s->raster_counter, s->raster_pre, s->raster_sums, r->ctx->sm_count, S(stream)),
+  RasterDev rd;
+  rd.rec = s->raster_rec; rd.ntile = s->raster_ntile; rd.pre = s->raster_pre; rd.sums = s->raster_sums;
+  rd.counter = s->raster_counter; rd.list = s->raster_list; rd.over = s->raster_over;
+  rd.tile_cnt = r->tile_cnt; rd.tile_fill = r->tile_fill; rd.list_cap = s->raster_cap; rd.ntiles = r->ntiles;
+  CK(gi_launch_gbuffer(s->dev(), r->frame, r->W, r->H, r->depth, r->normal, rd, r->ctx->sm_count, S(stream)),
      "gi_rc_render_gbuffer: launch");
   r->gbuf_set = true;
   return GI_OK;

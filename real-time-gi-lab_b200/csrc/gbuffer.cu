@@ -5,9 +5,16 @@
 //   hit    Moller-Trumbore against the triangles whose near-clipped screen box (one pixel of margin) holds the pixel;
 //          w = t * dot(dir, fwd) must be >= near, depth = near / w
 //   depth  the largest wins (reversed Z, compare 'greater'); equal depths keep the smaller triangle index
-//          (one 64-bit atomicMax of depth bits << 32 | ~triangle per sample, order independent)
+//          (the larger key depth bits << 32 | ~triangle, so the result does not depend on the order of the tests)
 //   normal normalize(interpolated vertex normal) * (front ? 1 : -1) (gbuffer.ts:94-95), stored as f16; w = 0
-// Triangles whose box covers more than 256 pixels go to a list, cut into 256-pixel tiles taken from a queue.
+//
+// Binned in 16 x 16 pixel tiles: k_rs_setup gives every triangle its screen box, tile range and a depth bound,
+// k_rs_bin lists each triangle in the tiles its box touches (count, scan, fill), and one block per tile keeps its
+// 256 pixels' keys in registers while it walks the tile's list front to back by depth bound, in sorted chunks of 256.
+// A triangle whose bound is below the depth every pixel of the tile already holds cannot win anywhere in the tile
+// and ends the chunk; below one pixel's depth it is skipped for that pixel.  Skipped pairs are exactly pairs whose
+// key would lose, so the result equals testing every (pixel, triangle whose box holds it) pair.  Triangles beyond the
+// list capacity go to an overflow list that every tile walks, so the result never depends on the capacity.
 #include <cuda_runtime.h>
 
 #include "gi_dev.cuh"
@@ -15,10 +22,11 @@
 
 namespace gi {
 
-constexpr uint32_t RASTER_SMALL = 256;
+constexpr uint32_t RT = 16;               // tile edge in pixels; one thread per pixel
+constexpr float DEPTH_MARGIN = 1.03125f;  // slack on the depth bound for the rounding of the ray test
 
-__device__ __forceinline__ bool ray_tri(f3 o, f3 dir, f3 a, f3 b, f3 c, float &t, float &u, float &v) {
-  f3 e1 = b - a, e2 = c - a;
+// Moller-Trumbore with the edges precomputed (e1 = b - a, e2 = c - a: the same f32 values as computing them here)
+__device__ __forceinline__ bool ray_tri(f3 o, f3 dir, f3 a, f3 e1, f3 e2, float &t, float &u, float &v) {
   f3 pv = cross(dir, e2);
   float det = dot(e1, pv);
   if (det == 0.0f) return false;
@@ -35,8 +43,10 @@ __device__ __forceinline__ bool ray_tri(f3 o, f3 dir, f3 a, f3 b, f3 c, float &t
   return true;
 }
 
-// Screen box of the triangle clipped to w >= near, one pixel of margin, clamped.  False when empty.
-__device__ __forceinline__ bool screen_box(const float *__restrict__ F, uint32_t W, uint32_t H, const f3 p[3], int box[4]) {
+// Screen box of the triangle clipped to w >= near, one pixel of margin, clamped.  False when empty.  min_w: the
+// smallest clip w of the clipped polygon (near when an edge crosses the near plane).
+__device__ __forceinline__ bool screen_box(const float *__restrict__ F, uint32_t W, uint32_t H, const f3 p[3], int box[4],
+                                           float &min_w) {
   const float *m = F + F_VP;
   float near = F[F_EYE + 3];
   float cl[3][4];
@@ -46,17 +56,19 @@ __device__ __forceinline__ bool screen_box(const float *__restrict__ F, uint32_t
     for (int i = 0; i < 4; i++) cl[k][i] = m[i] * p[k].x + m[4 + i] * p[k].y + m[8 + i] * p[k].z + m[12 + i] * 1.0f;
   float x0 = 1e30f, x1 = -1e30f, y0 = 1e30f, y1 = -1e30f;
   int np = 0;
+  min_w = 3.0e38f;
 #pragma unroll
   for (int k = 0; k < 3; k++) {
     const float *a = cl[k], *b = cl[(k + 1) % 3];
     bool ina = a[3] >= near, inb = b[3] >= near;
     float px[2], py[2];
     int cnt = 0;
-    if (ina) { px[cnt] = a[0] / a[3]; py[cnt] = a[1] / a[3]; cnt++; }
+    if (ina) { px[cnt] = a[0] / a[3]; py[cnt] = a[1] / a[3]; cnt++; min_w = mn(min_w, a[3]); }
     if (ina != inb) {
       float t = (a[3] - near) / (a[3] - b[3]);
       float x = a[0] + (b[0] - a[0]) * t, y = a[1] + (b[1] - a[1]) * t;
       px[cnt] = x / near; py[cnt] = y / near; cnt++;
+      min_w = mn(min_w, near);
     }
     for (int j = 0; j < cnt; j++) {
       float sx = (px[j] * 0.5f + 0.5f) * (float)W, sy = (0.5f - py[j] * 0.5f) * (float)H;
@@ -73,54 +85,16 @@ __device__ __forceinline__ bool screen_box(const float *__restrict__ F, uint32_t
   return true;
 }
 
-__device__ __forceinline__ void sample_pixel(const float *__restrict__ F, uint32_t W, int x, int y, const f3 p[3],
-                                             uint32_t t, unsigned long long *keys) {
-  f3 eye = mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2]);
-  f3 dir = world_at(F, x, y, 1.0f) - eye;
+// The key of (pixel ray, triangle): depth bits << 32 | ~t, or 0 when the ray misses or the hit is nearer than near
+__device__ __forceinline__ unsigned long long pixel_key(const float *__restrict__ F, f3 eye, f3 dir, f3 a, f3 e1, f3 e2,
+                                                        uint32_t t) {
   float tt, uu, vv;
-  if (!ray_tri(eye, dir, p[0], p[1], p[2], tt, uu, vv)) return;
+  if (!ray_tri(eye, dir, a, e1, e2, tt, uu, vv)) return 0ull;
   float w = tt * dot(dir, mk(F[F_FWD], F[F_FWD + 1], F[F_FWD + 2]));
   float near = F[F_EYE + 3];
-  if (!(w >= near)) return;
+  if (!(w >= near)) return 0ull;
   float depth = near / w;
-  unsigned long long k = ((unsigned long long)__float_as_uint(depth) << 32) | (unsigned long long)(0xffffffffu - t);
-  unsigned long long *kp = &keys[(size_t)y * W + (size_t)x];
-  if (k > *kp) atomicMax(kp, k);
-}
-
-__global__ void __launch_bounds__(256) k_raster_small(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                                      unsigned long long *keys, uint32_t *big, uint32_t big_cap,
-                                                      uint32_t *counter) {
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = t < s.ntris;
-  f3 p[3];
-  int box[4] = {0, -1, 0, -1};
-  bool any = false;
-  if (live) {
-    uint4 idx = s.tri[t];
-    p[0] = ld3(s.pos[idx.x]); p[1] = ld3(s.pos[idx.y]); p[2] = ld3(s.pos[idx.z]);
-    any = screen_box(F, W, H, p, box);
-  }
-  uint32_t area = any ? (uint32_t)(box[1] - box[0] + 1) * (uint32_t)(box[3] - box[2] + 1) : 0u;
-  bool is_big = area > RASTER_SMALL;
-  uint32_t k = warp_append(counter, is_big);
-  if (is_big) {
-    if (k < big_cap) big[k] = t;
-    return;
-  }
-  if (!any) return;
-  for (int y = box[2]; y <= box[3]; y++)
-    for (int x = box[0]; x <= box[1]; x++) sample_pixel(F, W, x, y, p, t, keys);
-}
-
-// Big triangles, balanced: each one's box is cut into tiles of 256 pixels; k_raster_count gives every listed triangle
-// its tile count and an exclusive prefix within blocks of 256 triangles, k_raster_scan the block offsets and the
-// total, and blocks of k_raster_big take tiles from a queue (counter[1]) and find their triangle by binary search.
-__device__ __forceinline__ bool big_box(const SceneDev &s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                        uint32_t t, f3 p[3], int box[4]) {
-  uint4 idx = s.tri[t];
-  p[0] = ld3(s.pos[idx.x]); p[1] = ld3(s.pos[idx.y]); p[2] = ld3(s.pos[idx.z]);
-  return screen_box(F, W, H, p, box);
+  return ((unsigned long long)__float_as_uint(depth) << 32) | (unsigned long long)(0xffffffffu - t);
 }
 
 __device__ __forceinline__ uint32_t block_sum_256(uint32_t x, uint32_t *excl) {
@@ -146,88 +120,208 @@ __device__ __forceinline__ uint32_t block_sum_256(uint32_t x, uint32_t *excl) {
   return r;
 }
 
-__global__ void __launch_bounds__(256) k_raster_count(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                                      const uint32_t *big, uint32_t big_cap, uint32_t *counter,
-                                                      uint32_t *pre, uint32_t *sums) {
-  uint32_t items = min(counter[0], big_cap);
-  uint32_t nblk = (items + 255u) / 256u;
-  for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x) {
-    uint32_t it = b * 256u + threadIdx.x, tiles = 0;
-    if (it < items) {
-      f3 p[3];
-      int box[4];
-      if (big_box(s, F, W, H, big[it], p, box))
-        tiles = ((uint32_t)(box[1] - box[0] + 1) * (uint32_t)(box[3] - box[2] + 1) + 255u) / 256u;
+// Per triangle: the record (a, bound; e1, x0 | x1 << 16; e2, y0 | y1 << 16), the tile count of its box, and the
+// exclusive prefix of the tile counts within its block of 256 triangles (block totals to sums)
+__global__ void __launch_bounds__(256) k_rs_setup(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
+                                                  RasterDev rd) {
+  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t nt = 0;
+  if (t < s.ntris) {
+    uint4 idx = s.tri[t];
+    f3 p[3];
+    p[0] = ld3(s.pos[idx.x]); p[1] = ld3(s.pos[idx.y]); p[2] = ld3(s.pos[idx.z]);
+    int box[4];
+    float min_w;
+    if (screen_box(F, W, H, p, box, min_w)) {
+      float near = F[F_EYE + 3];
+      // every hit of the triangle has w >= min_w up to rounding, so its depth near / w is at most near / min_w
+      float bound = min_w > near ? near / min_w * DEPTH_MARGIN : 3.0e38f;
+      f3 e1 = p[1] - p[0], e2 = p[2] - p[0];
+      rd.rec[3u * t] = make_float4(p[0].x, p[0].y, p[0].z, bound);
+      rd.rec[3u * t + 1u] = make_float4(e1.x, e1.y, e1.z, __uint_as_float((uint32_t)box[0] | ((uint32_t)box[1] << 16)));
+      rd.rec[3u * t + 2u] = make_float4(e2.x, e2.y, e2.z, __uint_as_float((uint32_t)box[2] | ((uint32_t)box[3] << 16)));
+      nt = ((uint32_t)box[1] / RT - (uint32_t)box[0] / RT + 1u) * ((uint32_t)box[3] / RT - (uint32_t)box[2] / RT + 1u);
     }
-    uint32_t ex;
-    uint32_t tot = block_sum_256(tiles, &ex);
-    if (it < items) pre[it] = ex;
-    if (threadIdx.x == 0) sums[b] = tot;
+    rd.ntile[t] = nt;
   }
+  uint32_t ex;
+  uint32_t tot = block_sum_256(nt, &ex);
+  if (t < s.ntris) rd.pre[t] = ex;
+  if (threadIdx.x == 0) rd.sums[blockIdx.x] = tot;
 }
 
-__global__ void __launch_bounds__(256) k_raster_scan(uint32_t big_cap, uint32_t *counter, uint32_t *sums) {
-  uint32_t nblk = (min(counter[0], big_cap) + 255u) / 256u;
+// Block offsets of the triangle prefix (in place in sums) and the pair total; clears the overflow count
+__global__ void __launch_bounds__(256) k_rs_scan(uint32_t nblk, RasterDev rd) {
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
   for (uint32_t b0 = 0; b0 < nblk; b0 += 256u) {
     uint32_t i = b0 + threadIdx.x;
     uint32_t ex;
-    uint32_t tot = block_sum_256(i < nblk ? sums[i] : 0u, &ex);
-    if (i < nblk) sums[i] = carry + ex;
+    uint32_t tot = block_sum_256(i < nblk ? rd.sums[i] : 0u, &ex);
+    if (i < nblk) rd.sums[i] = carry + ex;
     __syncthreads();
     if (threadIdx.x == 0) carry += tot;
     __syncthreads();
   }
-  if (threadIdx.x == 0) { counter[2] = carry; counter[1] = 0u; }
+  if (threadIdx.x == 0) { rd.counter[0] = carry; rd.counter[1] = 0u; }
 }
 
-__global__ void __launch_bounds__(256) k_raster_big(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                                    unsigned long long *keys, const uint32_t *big, uint32_t big_cap,
-                                                    uint32_t *counter, const uint32_t *pre, const uint32_t *sums) {
-  uint32_t items = min(counter[0], big_cap);
-  uint32_t tiles = counter[2];
-  __shared__ uint32_t s_tile;
-  for (;;) {
-    if (threadIdx.x == 0) s_tile = atomicAdd(&counter[1], 1u);
-    __syncthreads();
-    uint32_t tile = s_tile;
-    __syncthreads();
-    if (tile >= tiles) break;
-    uint32_t lo = 0, hi = items;   // the last triangle whose first tile is <= tile
+// Every (triangle, tile) pair: FILL = false counts the pairs of each tile and lists the triangles that do not fit the
+// list capacity; FILL = true writes each pair's triangle into its tile's range of the list
+template <bool FILL>
+__global__ void __launch_bounds__(256) k_rs_bin(uint32_t ntris, uint32_t tiles_x, RasterDev rd) {
+  uint32_t total = rd.counter[0];
+  for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = ntris;   // the last triangle whose first pair is <= p: the owner (it has pairs)
     while (hi - lo > 1u) {
       uint32_t m = (lo + hi) >> 1;
-      if (pre[m] + sums[m >> 8] <= tile) lo = m; else hi = m;
+      if (rd.pre[m] + rd.sums[m >> 8] <= p) lo = m; else hi = m;
     }
-    uint32_t t = big[lo];
-    f3 p[3];
-    int box[4];
-    if (!big_box(s, F, W, H, t, p, box)) continue;
-    uint32_t bw = (uint32_t)(box[1] - box[0] + 1), bh = (uint32_t)(box[3] - box[2] + 1);
-    uint32_t q = (tile - (pre[lo] + sums[lo >> 8])) * 256u + threadIdx.x;
-    if (q < bw * bh) sample_pixel(F, W, box[0] + (int)(q % bw), box[2] + (int)(q / bw), p, t, keys);
+    uint32_t first = rd.pre[lo] + rd.sums[lo >> 8], nt = rd.ntile[lo];
+    if (first + nt > rd.list_cap) {
+      if (!FILL && p == first) rd.over[atomicAdd(&rd.counter[1], 1u)] = lo;
+      continue;
+    }
+    uint32_t bx = __float_as_uint(rd.rec[3u * lo + 1u].w), by = __float_as_uint(rd.rec[3u * lo + 2u].w);
+    uint32_t tx0 = (bx & 0xffffu) / RT, tw = (bx >> 16) / RT - tx0 + 1u, ty0 = (by & 0xffffu) / RT;
+    uint32_t i = p - first;
+    uint32_t tile = (ty0 + i / tw) * tiles_x + tx0 + i % tw;
+    if (!FILL) {
+      atomicAdd(&rd.tile_cnt[tile], 1u);
+    } else {
+      uint32_t slot = atomicAdd(&rd.tile_fill[tile], 1u);
+      rd.list[rd.tile_cnt[tile] + slot] = lo;
+    }
   }
 }
 
-__global__ void __launch_bounds__(256) k_raster_resolve(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                                        const unsigned long long *keys, float *depth, uint2 *normal) {
-  uint32_t x = blockIdx.x * 16u + (threadIdx.x & 15u), y = blockIdx.y * 16u + (threadIdx.x >> 4);
-  if (x >= W || y >= H) return;
-  size_t q = (size_t)y * W + x;
-  unsigned long long k = keys[q];
-  if (k == 0ull) { depth[q] = 0.0f; normal[q] = make_uint2(0u, 0u); return; }
-  uint32_t t = 0xffffffffu - (uint32_t)(k & 0xffffffffull);
-  depth[q] = __uint_as_float((uint32_t)(k >> 32));
-  uint4 idx = s.tri[t];
-  f3 a = ld3(s.pos[idx.x]), b = ld3(s.pos[idx.y]), c = ld3(s.pos[idx.z]);
+// Exclusive scan of the tile counts in place (tile_cnt becomes the list offsets, tile_cnt[ntiles] the end); clears
+// the fill cursors
+__global__ void __launch_bounds__(1024) k_rs_tile_scan(RasterDev rd) {
+  __shared__ uint32_t ws[32];
+  __shared__ uint32_t carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  uint32_t lane = threadIdx.x & 31u, wid = threadIdx.x >> 5;
+  for (uint32_t b0 = 0; b0 < rd.ntiles; b0 += 1024u) {
+    uint32_t i = b0 + threadIdx.x;
+    uint32_t x = i < rd.ntiles ? rd.tile_cnt[i] : 0u, inc = x;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, inc, d);
+      if (lane >= (uint32_t)d) inc += y;
+    }
+    if (lane == 31u) ws[wid] = inc;
+    __syncthreads();
+    if (wid == 0) {
+      uint32_t v = ws[lane], vi = v;
+#pragma unroll
+      for (int d = 1; d < 32; d <<= 1) {
+        uint32_t y = __shfl_up_sync(0xffffffffu, vi, d);
+        if (lane >= (uint32_t)d) vi += y;
+      }
+      ws[lane] = vi - v;
+    }
+    __syncthreads();
+    if (i < rd.ntiles) { rd.tile_cnt[i] = carry + ws[wid] + inc - x; rd.tile_fill[i] = 0u; }
+    __syncthreads();
+    if (threadIdx.x == 1023u) carry += ws[wid] + inc;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) rd.tile_cnt[rd.ntiles] = carry;
+}
+
+// Smallest depth bits held by the block's 256 pixels (pixels off the screen hold +inf)
+__device__ __forceinline__ uint32_t block_min_256(uint32_t x, uint32_t *ws) {
+  uint32_t m = __reduce_min_sync(0xffffffffu, x);
+  if ((threadIdx.x & 31u) == 0) ws[threadIdx.x >> 5] = m;
+  __syncthreads();
+  uint32_t r = ws[0];
+#pragma unroll
+  for (int k = 1; k < 8; k++) r = min(r, ws[k]);
+  __syncthreads();
+  return r;
+}
+
+// One block per tile: the tile's list, then the overflow list, in chunks of 256 sorted by depth bound (largest
+// first); then the winner's depth and normal
+__global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
+                                                  uint32_t tiles_x, RasterDev rd, float *depth, uint2 *normal) {
+  __shared__ float4 sa[256], se1[256], se2[256];
+  __shared__ uint32_t skey[256], sval[256];
+  __shared__ uint32_t ws[8];
+  uint32_t tile = blockIdx.x;
+  uint32_t x = (tile % tiles_x) * RT + (threadIdx.x % RT), y = (tile / tiles_x) * RT + (threadIdx.x / RT);
+  bool inside = x < W && y < H;
   f3 eye = mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2]);
-  f3 dir = world_at(F, (int)x, (int)y, 1.0f) - eye;
+  f3 dir = mk(0.0f, 0.0f, 0.0f);
+  if (inside) dir = world_at(F, (int)x, (int)y, 1.0f) - eye;
+  unsigned long long best = 0ull;
+  uint32_t my_depth = inside ? 0u : 0x7f800000u;   // depth bits of best (positive floats order as integers)
+  for (int pass = 0; pass < 2; pass++) {
+    uint32_t beg = pass == 0 ? rd.tile_cnt[tile] : 0u, end = pass == 0 ? rd.tile_cnt[tile + 1u] : rd.counter[1];
+    const uint32_t *lst = pass == 0 ? rd.list : rd.over;
+    for (uint32_t c0 = beg; c0 < end; c0 += 256u) {
+      uint32_t n = min(256u, end - c0);
+      uint32_t t = 0, kb = 0;   // empty slots sort last (every bound is > 0)
+      if (threadIdx.x < n) {
+        t = lst[c0 + threadIdx.x];
+        kb = __float_as_uint(rd.rec[3u * t].w);
+      }
+      skey[threadIdx.x] = kb;
+      sval[threadIdx.x] = t;
+      __syncthreads();
+      for (uint32_t k = 2; k <= 256u; k <<= 1) {      // bitonic sort, descending
+        for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+          uint32_t i = threadIdx.x, l = i ^ j;
+          if (l > i) {
+            uint32_t a = skey[i], b = skey[l];
+            if ((i & k) == 0 ? a < b : a > b) {
+              skey[i] = b; skey[l] = a;
+              uint32_t v = sval[i]; sval[i] = sval[l]; sval[l] = v;
+            }
+          }
+          __syncthreads();
+        }
+      }
+      if (threadIdx.x < n) {
+        uint32_t u = sval[threadIdx.x];
+        sa[threadIdx.x] = rd.rec[3u * u];
+        se1[threadIdx.x] = rd.rec[3u * u + 1u];
+        se2[threadIdx.x] = rd.rec[3u * u + 2u];
+      }
+      __syncthreads();
+      uint32_t far = 0;
+      for (uint32_t j = 0; j < n; j++) {
+        if ((j & 31u) == 0) far = block_min_256(my_depth, ws);   // every thread reaches it at the same j
+        float4 a = sa[j];
+        uint32_t bound = __float_as_uint(a.w);
+        if (bound < far) break;                     // no pixel of the tile can take this or a later triangle
+        if (!inside || bound < my_depth) continue;  // this pixel cannot
+        float4 e1 = se1[j], e2 = se2[j];
+        uint32_t bx = __float_as_uint(e1.w), by = __float_as_uint(e2.w);
+        if (x < (bx & 0xffffu) || x > (bx >> 16) || y < (by & 0xffffu) || y > (by >> 16)) continue;
+        unsigned long long k = pixel_key(F, eye, dir, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
+                                         sval[j]);
+        if (k > best) { best = k; my_depth = (uint32_t)(k >> 32); }
+      }
+      __syncthreads();
+    }
+  }
+  if (!inside) return;
+  size_t q = (size_t)y * W + x;
+  if (best == 0ull) { depth[q] = 0.0f; normal[q] = make_uint2(0u, 0u); return; }
+  uint32_t t = 0xffffffffu - (uint32_t)(best & 0xffffffffull);
+  depth[q] = __uint_as_float((uint32_t)(best >> 32));
+  float4 a4 = rd.rec[3u * t], e14 = rd.rec[3u * t + 1u], e24 = rd.rec[3u * t + 2u];
+  f3 a = mk(a4.x, a4.y, a4.z), e1 = mk(e14.x, e14.y, e14.z), e2 = mk(e24.x, e24.y, e24.z);
   float tt = 0.0f, uu = 0.0f, vv = 0.0f;
-  ray_tri(eye, dir, a, b, c, tt, uu, vv);
+  ray_tri(eye, dir, a, e1, e2, tt, uu, vv);
+  uint4 idx = s.tri[t];
   f3 n0 = ld3(s.nrm[idx.x]), n1 = ld3(s.nrm[idx.y]), n2 = ld3(s.nrm[idx.z]);
   f3 nn = (n0 * (1.0f - uu - vv) + n1 * uu) + n2 * vv;
-  float flip = dot(cross(b - a, c - a), eye - a) > 0.0f ? 1.0f : -1.0f;
+  float flip = dot(cross(e1, e2), eye - a) > 0.0f ? 1.0f : -1.0f;
   nn = normalize3(nn) * flip;
   normal[q] = make_uint2((uint32_t)f2h(nn.x) | ((uint32_t)f2h(nn.y) << 16), (uint32_t)f2h(nn.z));
 }
@@ -236,16 +330,18 @@ __global__ void __launch_bounds__(256) k_raster_resolve(SceneDev s, const float 
 
 using namespace gi;
 
+uint32_t gi_raster_tiles(uint32_t W, uint32_t H) { return ((W + RT - 1u) / RT) * ((H + RT - 1u) / RT); }
+
 cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
-                              uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
-                              uint32_t *counter, uint32_t *pre, uint32_t *sums, uint32_t sm_count, cudaStream_t st) {
-  cudaMemsetAsync(keys, 0, (size_t)W * H * sizeof(unsigned long long), st);
-  cudaMemsetAsync(counter, 0, 4 * sizeof(uint32_t), st);
-  if (s.ntris) k_raster_small<<<(s.ntris + 255u) / 256u, 256, 0, st>>>(s, frame_dev, W, H, keys, big, big_cap, counter);
-  k_raster_count<<<sm_count * 2u, 256, 0, st>>>(s, frame_dev, W, H, big, big_cap, counter, pre, sums);
-  k_raster_scan<<<1, 256, 0, st>>>(big_cap, counter, sums);
-  k_raster_big<<<sm_count * 8u, 256, 0, st>>>(s, frame_dev, W, H, keys, big, big_cap, counter, pre, sums);
-  dim3 g((W + 15u) / 16u, (H + 15u) / 16u);
-  k_raster_resolve<<<g, 256, 0, st>>>(s, frame_dev, W, H, keys, depth, normal);
+                              uint2 *normal, const RasterDev &rd, uint32_t sm_count, cudaStream_t st) {
+  uint32_t tiles_x = (W + RT - 1u) / RT;
+  cudaMemsetAsync(rd.tile_cnt, 0, (size_t)(rd.ntiles + 1u) * sizeof(uint32_t), st);
+  uint32_t nblk = s.ntris ? (s.ntris + 255u) / 256u : 1u;
+  k_rs_setup<<<nblk, 256, 0, st>>>(s, frame_dev, W, H, rd);
+  k_rs_scan<<<1, 256, 0, st>>>(nblk, rd);
+  if (s.ntris) k_rs_bin<false><<<sm_count * 8u, 256, 0, st>>>(s.ntris, tiles_x, rd);
+  k_rs_tile_scan<<<1, 1024, 0, st>>>(rd);
+  if (s.ntris) k_rs_bin<true><<<sm_count * 8u, 256, 0, st>>>(s.ntris, tiles_x, rd);
+  k_rs_tiles<<<rd.ntiles, 256, 0, st>>>(s, frame_dev, W, H, tiles_x, rd, depth, normal);
   return cudaGetLastError();
 }

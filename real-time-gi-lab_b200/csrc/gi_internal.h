@@ -34,15 +34,25 @@ struct RcDev {
   void *rad_traced;        // optional: copy of the atlas after the trace
 };
 
+// Scratch of the binned G-buffer raster (gbuffer.cu)
+struct RasterDev {
+  float4 *rec;                     // 3 per triangle: (a, depth bound), (e1, x0 | x1 << 16), (e2, y0 | y1 << 16)
+  uint32_t *ntile, *pre, *sums;    // per triangle: tiles its box touches, prefix within its block; block offsets
+  uint32_t *counter;               // [0] (triangle, tile) pairs, [1] overflow triangles
+  uint32_t *list, *over;           // per-tile triangle lists (list_cap entries), overflow triangles (ntris)
+  uint32_t *tile_cnt, *tile_fill;  // per tile: count, then list offset (ntiles + 1); fill cursor (ntiles)
+  uint32_t list_cap, ntiles;
+};
+
 }  // namespace gi
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
                                cudaEvent_t *ev = nullptr);
+uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
-                              uint2 *normal, unsigned long long *keys, uint32_t *big, uint32_t big_cap,
-                              uint32_t *counter, uint32_t *pre, uint32_t *sums, uint32_t sm_count, cudaStream_t st);
+                              uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);

@@ -69,6 +69,10 @@ class SceneGpu:
         _lib.call("gi_scene_bytes", self.handle, C.byref(b))
         return b.value
 
+    def set_raster_capacity(self, entries: int):
+        """Entries of the G-buffer raster's per-tile lists (triangles past them are tested by every tile)."""
+        _lib.call("gi_scene_set_raster_capacity", self.handle, entries)
+
     def destroy(self):
         if self.handle:
             _lib.call("gi_scene_destroy", self.handle)
