@@ -131,6 +131,14 @@ int gi_scene_bytes(gi_scene *scene, uint64_t *bytes);
  * Triangles past it are tested by every tile instead: slower, the same G-buffer.  Frees the old list (which waits for
  * work still using it). */
 int gi_scene_set_raster_capacity(gi_scene *scene, uint32_t entries);
+/* Rigid objects (no counterpart in the reference's static scene upload; its moving objects go through dynlayer.ts):
+ * vertices [first, first + verts_per_object * n_objects) become n_objects rigid bodies whose current vertices are
+ * their rest vertices (copied now) under a per-object transform.  gi_scene_rigid_upload copies n_objects row-major
+ * 3x4 transforms [R | t] (12 floats each; R a rotation) from host memory (pinned: asynchronous); gi_scene_rigid_apply
+ * writes position = R * rest + t and normal = R * rest normal on the device (graph-capturable). */
+int gi_scene_rigid_define(gi_scene *scene, uint32_t first, uint32_t verts_per_object, uint32_t n_objects);
+int gi_scene_rigid_upload(gi_scene *scene, const float *m34, void *stream);
+int gi_scene_rigid_apply(gi_scene *scene, void *stream);
 /* The voxel rebuild for callers that cannot allocate device memory (no counterpart in the reference).  Some callers
  * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
  * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point
@@ -179,6 +187,12 @@ int gi_rc_set_stats(gi_rc *rc, uint32_t level);
  * gi_rc_set_frame / gi_rc_set_gbuffer* / gi_scene_update_vertices before a launch take effect; the voxel windows
  * (gi_vox_update) and the parameters are those of capture time: capture again after moving the windows. */
 int gi_rc_graph_capture(gi_rc *rc, gi_vox *vox, void *stream);
+/* CUDA graph of one whole frame: the scene's rigid objects posed from their last uploaded transforms (when defined),
+ * the G-buffer drawn, gi_solve, and the irradiance as stored copied into irr_out (pinned host or device memory,
+ * gi_rc_read_irradiance_raw's layout; NULL: no copy).  Replayed by gi_rc_graph_launch: per frame a caller uploads
+ * the transforms and launches.  The same conditions as gi_rc_graph_capture; the voxel world must be built from
+ * `scene`. */
+int gi_rc_graph_capture_frame(gi_rc *rc, gi_vox *vox, gi_scene *scene, void *irr_out, void *stream);
 int gi_rc_graph_launch(gi_rc *rc, void *stream);
 /* Batches (no counterpart in the reference, which solves one frame per queue submit): n independent solves, each
  * an (rc, vox) pair with its own frame, G-buffer and scene, captured into ONE CUDA graph whose n solve chains are

@@ -76,6 +76,10 @@ struct gi_scene {
   uint32_t *raster_list = nullptr, *raster_over = nullptr;
   uint32_t raster_cap = 0;
   float4 *stage = nullptr;   // vertex staging for updates (nverts * 2)
+  // rigid objects: a vertex range of n objects x per vertices posed on the device from a 3x4 transform per object
+  float4 *rigid_rest = nullptr;   // rest positions (per * n), then rest normals (per * n)
+  float *rigid_m = nullptr;       // n x 12 floats, row-major [R | t]
+  uint32_t rigid_first = 0, rigid_per = 0, rigid_n = 0;
   SceneDev dev() const {
     SceneDev s;
     s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
@@ -123,6 +127,7 @@ static void free_scene(gi_scene *s) {
   cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
   cudaFree(s->raster_rec); cudaFree(s->raster_ntile); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
   cudaFree(s->raster_counter); cudaFree(s->raster_list); cudaFree(s->raster_over); cudaFree(s->stage);
+  cudaFree(s->rigid_rest); cudaFree(s->rigid_m);
 }
 static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
@@ -244,6 +249,65 @@ int gi_scene_update_vertices(gi_scene *s, uint32_t first, uint32_t count, const 
   CK(cudaMemcpyAsync(st + (size_t)count * 4u, nrm, (size_t)count * 12u, cudaMemcpyHostToDevice, S(stream)), "gi_scene_update_vertices: normals");
   k_pack_vertices<<<(count + 255u) / 256u, 256, 0, S(stream)>>>(st + (size_t)count * 4u, s->nrm + first, count);
   CK(cudaGetLastError(), "gi_scene_update_vertices: launch");
+  return GI_OK;
+}
+
+__global__ void k_rigid_apply(float4 *pos, float4 *nrm, const float4 *rest, const float *m, uint32_t first,
+                              uint32_t per, uint32_t n) {
+  uint32_t total = per * n;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= total) return;
+  const float *M = m + 12u * (i / per);
+  float4 p = rest[i], q = rest[total + i];
+  pos[first + i] = make_float4(((M[0] * p.x + M[1] * p.y) + M[2] * p.z) + M[3],
+                               ((M[4] * p.x + M[5] * p.y) + M[6] * p.z) + M[7],
+                               ((M[8] * p.x + M[9] * p.y) + M[10] * p.z) + M[11], 0.0f);
+  nrm[first + i] = make_float4((M[0] * q.x + M[1] * q.y) + M[2] * q.z, (M[4] * q.x + M[5] * q.y) + M[6] * q.z,
+                               (M[8] * q.x + M[9] * q.y) + M[10] * q.z, 0.0f);
+}
+
+int gi_scene_rigid_define(gi_scene *s, uint32_t first, uint32_t verts_per_object, uint32_t n_objects) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_rigid_define: NULL scene");
+  uint64_t total = (uint64_t)verts_per_object * n_objects;
+  if (total == 0 || first + total > s->nverts)
+    return fail(GI_ERR_INVALID, "gi_scene_rigid_define: %u objects of %u vertices from %u do not fit %u vertices",
+                n_objects, verts_per_object, first, s->nverts);
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_rigid_define: cudaSetDevice");
+  float4 *rest = nullptr;
+  float *m = nullptr;
+  cudaError_t e;
+  if ((e = dalloc(&rest, 2u * total)) || (e = dalloc(&m, 12u * (size_t)n_objects))) {
+    cudaFree(rest);
+    return cuda_fail(e, "gi_scene_rigid_define");
+  }
+  if ((e = cudaMemcpy(rest, s->pos + first, total * sizeof(float4), cudaMemcpyDeviceToDevice)) ||
+      (e = cudaMemcpy(rest + total, s->nrm + first, total * sizeof(float4), cudaMemcpyDeviceToDevice))) {
+    cudaFree(rest); cudaFree(m);
+    return cuda_fail(e, "gi_scene_rigid_define: copy");
+  }
+  cudaFree(s->rigid_rest); cudaFree(s->rigid_m);
+  s->rigid_rest = rest; s->rigid_m = m;
+  s->rigid_first = first; s->rigid_per = verts_per_object; s->rigid_n = n_objects;
+  return GI_OK;
+}
+
+int gi_scene_rigid_upload(gi_scene *s, const float *m34, void *stream) {
+  if (!s || !m34) return fail(GI_ERR_INVALID, "gi_scene_rigid_upload: NULL argument");
+  if (!s->rigid_n) return fail(GI_ERR_STATE, "gi_scene_rigid_upload: no rigid objects defined");
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_rigid_upload: cudaSetDevice");
+  CK(cudaMemcpyAsync(s->rigid_m, m34, (size_t)s->rigid_n * 48u, cudaMemcpyHostToDevice, S(stream)),
+     "gi_scene_rigid_upload: copy");
+  return GI_OK;
+}
+
+int gi_scene_rigid_apply(gi_scene *s, void *stream) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_rigid_apply: NULL scene");
+  if (!s->rigid_n) return fail(GI_ERR_STATE, "gi_scene_rigid_apply: no rigid objects defined");
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_rigid_apply: cudaSetDevice");
+  uint32_t total = s->rigid_per * s->rigid_n;
+  k_rigid_apply<<<(total + 255u) / 256u, 256, 0, S(stream)>>>(s->pos, s->nrm, s->rigid_rest, s->rigid_m, s->rigid_first,
+                                                                s->rigid_per, s->rigid_n);
+  CK(cudaGetLastError(), "gi_scene_rigid_apply: launch");
   return GI_OK;
 }
 
@@ -573,6 +637,36 @@ int gi_rc_graph_capture(gi_rc *r, gi_vox *v, void *stream) {
   e = cudaGraphInstantiate(&r->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture: instantiate"); }
+  r->graph_vox = v;
+  return GI_OK;
+}
+
+int gi_rc_graph_capture_frame(gi_rc *r, gi_vox *v, gi_scene *sc, void *irr_out, void *stream) {
+  if (!r || !v || !sc) return fail(GI_ERR_INVALID, "gi_rc_graph_capture_frame: NULL argument");
+  if (!stream) return fail(GI_ERR_INVALID, "gi_rc_graph_capture_frame: the legacy default stream cannot be captured; pass a stream");
+  if (!r->frame_set || !v->updated) return fail(GI_ERR_STATE, "gi_rc_graph_capture_frame: frame and voxel window must be set first");
+  if (v->scene != sc) return fail(GI_ERR_INVALID, "gi_rc_graph_capture_frame: the voxel world is built from another scene");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_graph_capture_frame: cudaSetDevice");
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; r->graph_vox = nullptr; }
+  bool timing = r->timing;
+  r->timing = false;
+  CK(cudaStreamBeginCapture(S(stream), cudaStreamCaptureModeThreadLocal), "gi_rc_graph_capture_frame: begin");
+  int st = sc->rigid_n ? gi_scene_rigid_apply(sc, stream) : GI_OK;
+  if (st == GI_OK) st = gi_rc_render_gbuffer(r, sc, stream);
+  if (st == GI_OK) st = gi_solve(r, v, stream);
+  if (st == GI_OK && irr_out) {
+    cudaError_t ce = cudaMemcpyAsync(irr_out, r->dev.irr, (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas),
+                                     cudaMemcpyDefault, S(stream));
+    if (ce != cudaSuccess) st = cuda_fail(ce, "gi_rc_graph_capture_frame: readback");
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamEndCapture(S(stream), &g);
+  r->timing = timing;
+  if (st != GI_OK) { if (g) cudaGraphDestroy(g); return st; }
+  if (e != cudaSuccess) return cuda_fail(e, "gi_rc_graph_capture_frame: end");
+  e = cudaGraphInstantiate(&r->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture_frame: instantiate"); }
   r->graph_vox = v;
   return GI_OK;
 }

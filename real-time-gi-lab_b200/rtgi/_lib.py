@@ -53,6 +53,10 @@ SIGNATURES = {
     "gi_rc_set_debug_hits": (C.c_int, [_P, C.c_int]),
     "gi_rc_merge_gather_f64": (C.c_int, [_P, _P]),
     "gi_scene_set_raster_capacity": (C.c_int, [_P, C.c_uint32]),
+    "gi_scene_rigid_define": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "gi_scene_rigid_upload": (C.c_int, [_P, _P, _P]),
+    "gi_scene_rigid_apply": (C.c_int, [_P, _P]),
+    "gi_rc_graph_capture_frame": (C.c_int, [_P, _P, _P, _P, _P]),
     "gi_rc_read_irradiance_f64": (C.c_int, [_P, _P, _P]),
     "gi_rc_graph_capture": (C.c_int, [_P, _P, _P]),
     "gi_rc_graph_launch": (C.c_int, [_P, _P]),

@@ -69,6 +69,21 @@ class SceneGpu:
         _lib.call("gi_scene_bytes", self.handle, C.byref(b))
         return b.value
 
+    def rigid_define(self, first: int, verts_per_object: int, n_objects: int):
+        """The vertex range [first, first + verts_per_object * n_objects) becomes rigid objects (rest = current)."""
+        _lib.call("gi_scene_rigid_define", self.handle, first, verts_per_object, n_objects)
+
+    def rigid_upload(self, m34, stream=None):
+        """Row-major 3x4 transforms, one per object: a float32 array or a pointer to pinned host memory."""
+        if isinstance(m34, np.ndarray):
+            m34 = np.ascontiguousarray(m34, dtype=np.float32)
+            _lib.call("gi_scene_rigid_upload", self.handle, _ptr(m34), _stream(stream))
+        else:
+            _lib.call("gi_scene_rigid_upload", self.handle, m34, _stream(stream))
+
+    def rigid_apply(self, stream=None):
+        _lib.call("gi_scene_rigid_apply", self.handle, _stream(stream))
+
     def set_raster_capacity(self, entries: int):
         """Entries of the G-buffer raster's per-tile lists (triangles past them are tested by every tile)."""
         _lib.call("gi_scene_set_raster_capacity", self.handle, entries)
@@ -201,6 +216,10 @@ class Rc:
     def graph_capture(self, vox: VoxWorld, stream):
         """Captures one solve (voxel rebuild + cascades) into a CUDA graph owned by this Rc."""
         _lib.call("gi_rc_graph_capture", self.handle, vox.handle, _stream(stream))
+
+    def graph_capture_frame(self, vox: VoxWorld, scene: SceneGpu, irr_ptr: Optional[int], stream):
+        """Captures a whole frame: rigid pose, G-buffer, voxel rebuild, cascades, irradiance copy to irr_ptr."""
+        _lib.call("gi_rc_graph_capture_frame", self.handle, vox.handle, scene.handle, irr_ptr, _stream(stream))
 
     def graph_launch(self, stream):
         _lib.call("gi_rc_graph_launch", self.handle, _stream(stream))

@@ -28,6 +28,24 @@ class MovingObjects:
         self.area = area            # (centre x, centre z, half extent x, half extent z)
         self.per = pos.shape[0] // max(1, centres.shape[0])
 
+    def transforms(self, t: float) -> np.ndarray:
+        """(n, 12) float32 row-major [R | c(t) - R c0] per object: the pose at t as a transform of the rest vertices
+        (what pose() computes, for gi_scene_rigid_upload)."""
+        k = self.centres.shape[0]
+        ax, az, hx, hz = self.area
+        c = self.centres + self.vel * t
+        c[:, 0] = (c[:, 0] - ax + hx) % (2 * hx) - hx + ax
+        c[:, 2] = (c[:, 2] - az + hz) % (2 * hz) - hz + az
+        a = self.omega * t
+        ca, sa = np.cos(a), np.sin(a)
+        m = np.zeros((k, 12), np.float64)
+        m[:, 0], m[:, 2], m[:, 5], m[:, 8], m[:, 10] = ca, sa, 1.0, -sa, ca
+        c0 = self.centres
+        m[:, 3] = c[:, 0] - (ca * c0[:, 0] + sa * c0[:, 2])
+        m[:, 7] = c[:, 1] - c0[:, 1]
+        m[:, 11] = c[:, 2] - (-sa * c0[:, 0] + ca * c0[:, 2])
+        return m.astype(np.float32)
+
     def pose(self, t: float):
         k = self.centres.shape[0]
         ax, az, hx, hz = self.area

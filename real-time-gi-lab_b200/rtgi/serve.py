@@ -193,8 +193,10 @@ class _WallClock:
 
 
 class GpuExecutor:
-    """Runs requests on the device: per slot a CUDA stream, a completion event and a pinned readback buffer; per
-    resident scene its SceneGpu, VoxWorld, Rc (f16 atlases) and captured solve graph."""
+    """Runs requests on the device: per slot a CUDA stream and a completion event; per resident scene its SceneGpu
+    (moving objects as rigid bodies), VoxWorld, Rc (f16 atlases), pinned transform and result buffers, and one
+    captured graph of the whole frame (pose, G-buffer, voxel rebuild, cascades, irradiance copy).  A request uploads
+    its objects' transforms and launches the scene's graph: two calls."""
 
     def __init__(self, ctx, slots: int, atlas: str = "f16", n_objects=None):
         import torch
@@ -204,21 +206,20 @@ class GpuExecutor:
         self.atlas = atlas
         self.streams = [torch.cuda.Stream() for _ in range(max(1, slots))]
         self.events = [None] * len(self.streams)
-        self.host = [None] * len(self.streams)
         self.res: Dict[int, dict] = {}
         self.n_objects = n_objects or (lambda spec: 1 + int(scenes.PCG32(spec["seed"], stream=41).uniform(0, 200)))
-        self.results: Dict[int, np.ndarray] = {}
 
     def scene_bytes(self, spec: dict) -> int:
         p, v = _params(spec, self.atlas)
         W, H = spec["width"], spec["height"]
         lay = configs.cascade_layout(p, W, H)
         elem = 16 if self.atlas == "f32" else 8
-        rc = W * H * (4 + 8 + 8 + 16 + elem) + lay["probes_total"] * 52 + lay["rays_total"] * elem * 1
+        rc = W * H * (4 + 8 + 16 + elem) + lay["probes_total"] * 52 + lay["rays_total"] * elem * 1
         vox = (v.levels * v.G ** 3 + v.maxBricks * (530 + 1) + 16 * (1 << 18) + 8 * (1 << 18) + v.maxVoxels * 6) * 4
-        return int(rc + vox + 64 * spec["tris"])
+        return int(rc + vox + 140 * spec["tris"] + (4 << 20))
 
     def load(self, sid: int, spec: dict) -> int:
+        torch = self.torch
         s, objs = serving_scene(spec, self.n_objects(spec))
         p, v = _params(spec, self.atlas)
         W, H = spec["width"], spec["height"]
@@ -226,16 +227,19 @@ class GpuExecutor:
                                          cascades=p.cascades, P=p.P))
         st = self.streams[0]
         sg = self.gpu.SceneGpu(self.ctx, s)
+        sg.rigid_define(objs.first, objs.per, objs.centres.shape[0])
         vw = self.gpu.VoxWorld(sg, v)
         rc = self.gpu.Rc(self.ctx, p, W, H)
         rc.set_frame(F, st)
-        pos, nrm = objs.pose(0.0)
-        sg.update_vertices(objs.first, pos, nrm, st)
-        rc.render_gbuffer(sg, st)
         vw.update(s.camera.eye)
-        rc.graph_capture(vw, st)
+        m = torch.empty((objs.centres.shape[0], 12), dtype=torch.float32).pin_memory()
+        out = torch.empty(rc.irr_bytes(), dtype=torch.uint8).pin_memory()
+        m.numpy()[:] = objs.transforms(0.0)
+        sg.rigid_upload(m.data_ptr(), st)
+        rc.graph_capture_frame(vw, sg, out.data_ptr(), st)
+        rc.graph_launch(st)
         st.synchronize()
-        self.res[sid] = {"sg": sg, "vw": vw, "rc": rc, "objs": objs, "scene": s}
+        self.res[sid] = {"sg": sg, "vw": vw, "rc": rc, "objs": objs, "scene": s, "m": m, "out": out}
         return sg.bytes() + vw.bytes() + rc.bytes()
 
     def unload(self, sid: int):
@@ -247,17 +251,12 @@ class GpuExecutor:
     def launch(self, slot: int, sid: int, t: float):
         r = self.res[sid]
         st = self.streams[slot]
-        pos, nrm = r["objs"].pose(t)
-        r["sg"].update_vertices(r["objs"].first, pos, nrm, st)
-        r["rc"].render_gbuffer(r["sg"], st)
+        r["m"].numpy()[:] = r["objs"].transforms(t)
+        r["sg"].rigid_upload(r["m"].data_ptr(), st)
         r["rc"].graph_launch(st)
-        n = r["rc"].irr_bytes()
-        if self.host[slot] is None or self.host[slot].numel() < n:
-            self.host[slot] = self.torch.empty(n, dtype=self.torch.uint8).pin_memory()
-        r["rc"].read_irradiance_async(self.host[slot].data_ptr(), st)
         ev = self.torch.cuda.Event()
         ev.record(st)
-        self.events[slot] = (ev, sid, n)
+        self.events[slot] = (ev, sid)
 
     def poll(self, slot: int) -> bool:
         e = self.events[slot]
@@ -269,13 +268,45 @@ class GpuExecutor:
             e[0].synchronize()
 
     def result(self, slot: int) -> np.ndarray:
-        ev, sid, n = self.events[slot]
+        """The irradiance (as stored) of the slot's last request; valid until its scene is launched again."""
+        ev, sid = self.events[slot]
         ev.synchronize()
-        return self.host[slot][:n].numpy().copy()
+        return self.res[sid]["out"].numpy().copy()
 
     def destroy(self):
         for sid in list(self.res):
             self.unload(sid)
+
+
+class PlainExecutor:
+    """The plain per-solve path over a GpuExecutor's resident scenes: each request through the drop-in C-ABI calls
+    one by one (transforms, pose, G-buffer, gi_solve, irradiance readback), no graph, on one stream."""
+
+    def __init__(self, ex: GpuExecutor):
+        self.ex = ex
+
+    def launch(self, slot: int, sid: int, t: float):
+        ex = self.ex
+        r = ex.res[sid]
+        st = ex.streams[0]
+        r["m"].numpy()[:] = r["objs"].transforms(t)
+        r["sg"].rigid_upload(r["m"].data_ptr(), st)
+        r["sg"].rigid_apply(st)
+        r["rc"].render_gbuffer(r["sg"], st)
+        r["rc"].solve(r["vw"], st)
+        r["rc"].read_irradiance_async(r["out"].data_ptr(), st)
+        ev = ex.torch.cuda.Event()
+        ev.record(st)
+        ex.events[0] = (ev, sid)
+
+    def poll(self, slot: int) -> bool:
+        return self.ex.poll(0)
+
+    def wait(self, slot: int):
+        self.ex.wait(0)
+
+    def result(self, slot: int) -> np.ndarray:
+        return self.ex.result(0)
 
 
 def _params(spec: dict, atlas: str):

@@ -60,3 +60,17 @@ def test_colonnade_precision_scene():
     assert s.triangle_count == scenes.colonnade_scene(0).triangle_count + 64 * 12
     p, v = precision.colonnade_params("f16")
     assert p.atlas == "f16" and p.cascades == 5 and v.levels == 4 and v.G == 16
+
+
+def test_rigid_transforms_reproduce_pose():
+    base = _small_base()
+    s, objs = movers.with_moving_boxes(base, 6, scenes.PCG32(5, stream=41))
+    rest_p = s.positions[objs.first:].astype(np.float64).reshape(6, -1, 3)
+    rest_n = s.normals[objs.first:].astype(np.float64).reshape(6, -1, 3)
+    for t in (0.0, 0.4, 13.0):
+        m = objs.transforms(t).astype(np.float64).reshape(6, 3, 4)
+        p = np.einsum("oij,ovj->ovi", m[:, :, :3], rest_p) + m[:, None, :, 3]
+        n = np.einsum("oij,ovj->ovi", m[:, :, :3], rest_n)
+        pp, nn = objs.pose(t)
+        np.testing.assert_allclose(p.reshape(-1, 3), pp, atol=2e-5)
+        np.testing.assert_allclose(n.reshape(-1, 3), nn, atol=1e-6)

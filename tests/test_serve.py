@@ -133,5 +133,11 @@ def test_served_result_same_alone_and_in_mix():
     st = srv.run(reqs, on_done=lambda rq, slot: mixed.setdefault(rq.rid, ex.result(slot)) if rq.rid == 30 else None)
     assert st["completed"] == 60 and st["max_inflight"] >= 2
     assert np.array_equal(mixed[30], alone[0]), "a request's result changed when served in the mix"
+    # the plain path (the C-ABI calls one by one, no graph) computes the same frame identically
+    plain = {}
+    serve.plain_loop(serve.PlainExecutor(ex), [serve.Request(1, 2, 0.37, 0.0)],
+                     on_done=lambda rq, slot: plain.setdefault(rq.rid, ex.result(slot)))
+    assert np.array_equal(plain[1], alone[0])
+    assert np.any(alone[0] != 0)
     ex.destroy()
     ctx.destroy()
