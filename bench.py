@@ -291,14 +291,34 @@ def run_reference(args, rank):
     print(json.dumps(line), flush=True)
 
 
+def init_ranks(world: int, backend: str = "nccl", timeout_s: float = 120.0):
+    """torch.distributed for N > 1 replicas (env rendezvous: MASTER_ADDR/PORT, RANK, WORLD_SIZE), else None."""
+    if world <= 1:
+        return None
+    import datetime
+    import torch.distributed as dist
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest x of all ranks (every rank takes part; device: where the backend's tensors live)."""
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank: float, max_seconds: float, world: int) -> float:
+    """Units all ranks processed over the slowest rank's time (replicas: weak scaling)."""
+    return world * units_per_rank / max_seconds
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    dist = init_ranks(world)
     from rtgi import _lib, configs, gpu
 
     s, W, H, p, v, F, desc = workload(args.workload)
@@ -357,11 +377,8 @@ def run_ours(args, rank, world, local_rank):
     clk = clocks.stop(unix0, unix0 + wall)
     step_ms = [a.elapsed_time(b) for a, b in zip(ev_s, ev_e)]
     total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    max_total = float(t.item())
-    value = world * n_ev / (max_total / 1000.0)
+    max_total = max_over_ranks(total_ms, dist, "cuda")
+    value = whole_job_rate(n_ev, max_total / 1000.0, world)
 
     # end to end through the C-ABI with host buffers: frame + G-buffer H2D from pinned memory, solve, irradiance D2H
     depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
@@ -386,11 +403,9 @@ def run_ours(args, rank, world, local_rank):
             rc.read_irradiance_raw_ptr(irr_h.data_ptr(), stream)   # synchronises the stream
         torch.cuda.synchronize()
         e2e_s = time.perf_counter() - e0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    e2e_value = whole_job_rate(n_e2e, max_over_ranks(e2e_s, dist, "cuda"), world)
     if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
         dist.barrier()
-    e2e_value = world * n_e2e / float(te.item())
 
     trace_ms = statistics.mean(pass_ms["giTrace"])
     alg = trace_algorithmic_bytes(rc.layout, hdr, v)
