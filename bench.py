@@ -160,31 +160,45 @@ def cpu_baseline(s, v, p, F, depth, normal, budget_s=12.0, min_solves=2):
 
 
 def run_batched(args, ctx, stream, flush):
-    """The uneven batch (64 seeded specs): every solve replayed alone from its own graph, one after another, and all of
-    them as one batch graph of parallel solve chains.  Device time with CUDA events, L2 flushed between replays."""
+    """The uneven batch (64 seeded specs): every solve replayed alone from its own graph, one after another, with the
+    default launch shapes and with the autotuner's, and all of them (autotuned) as one batch graph of parallel solve
+    chains.  Device time with CUDA events, L2 flushed between replays."""
+    import collections
     import torch
-    from rtgi import batch, scenes
+    from rtgi import autotune, batch, scenes
     specs = [scenes.batch_spec(s) for s in range(args.batch)]
     solves = [batch.make_solve(ctx, sp, stream=stream) for sp in specs]
-    for x in solves:
-        x.rc.graph_capture(x.vox, stream)
-    b = batch.make_batch(ctx, solves, stream)
     reps = 5
     ev = lambda: torch.cuda.Event(enable_timing=True)
+
+    def time_alone():
+        for x in solves:
+            x.rc.graph_capture(x.vox, stream)
+        with torch.cuda.stream(stream):
+            for x in solves:   # warm-up
+                x.rc.graph_launch(stream)
+            per = [[] for _ in solves]
+            for _ in range(reps):
+                for i, x in enumerate(solves):
+                    flush.zero_()
+                    e0, e1 = ev(), ev()
+                    e0.record(stream)
+                    x.rc.graph_launch(stream)
+                    e1.record(stream)
+                    per[i].append((e0, e1))
+            torch.cuda.synchronize()
+        return [statistics.median(a.elapsed_time(c) for a, c in per[i]) for i in range(len(solves))]
+
+    alone_default = time_alone()
+    t0 = time.perf_counter()
+    tuner = autotune.Autotuner(reps=3)
+    picks = [tuner.tune(x.rc, x.vox, stream) for x in solves]
+    tune_s = time.perf_counter() - t0
+    alone_ms = time_alone()
+    b = batch.make_batch(ctx, solves, stream)
     with torch.cuda.stream(stream):
-        for x in solves:   # warm-up
-            x.rc.graph_launch(stream)
         b.launch(stream)
         stream.synchronize()
-        per = [[] for _ in solves]
-        for _ in range(reps):
-            for i, x in enumerate(solves):
-                flush.zero_()
-                e0, e1 = ev(), ev()
-                e0.record(stream)
-                x.rc.graph_launch(stream)
-                e1.record(stream)
-                per[i].append((e0, e1))
         bt = []
         for _ in range(reps * 4):
             flush.zero_()
@@ -194,18 +208,23 @@ def run_batched(args, ctx, stream, flush):
             e1.record(stream)
             bt.append((e0, e1))
         torch.cuda.synchronize()
-    alone_ms = [statistics.median(a.elapsed_time(c) for a, c in per[i]) for i in range(len(solves))]
     batch_ms = sorted(a.elapsed_time(c) for a, c in bt)
-    plain_total = sum(alone_ms)
+    chosen = collections.Counter()
+    for pk in picks:
+        for k, val in list(pk["rc"].items()) + list(pk["vox"].items()):
+            chosen[f"{k}={val}"] += 1
     out = {"solves": len(solves), "triangles": sum(x.scene.triangle_count for x in solves),
            "rays": sum(x.rc.layout["rays_total"] for x in solves),
-           "plain_solves_per_s": len(solves) / (plain_total / 1000.0),
-           "plain_p50_ms": statistics.median(alone_ms), "plain_p99_ms": sorted(alone_ms)[-1],
+           "plain_solves_per_s": len(solves) / (sum(alone_default) / 1000.0),
+           "plain_tuned_solves_per_s": len(solves) / (sum(alone_ms) / 1000.0),
+           "plain_p50_ms": statistics.median(alone_default), "plain_p99_ms": sorted(alone_default)[-1],
            "batch_ms_p50": statistics.median(batch_ms), "batch_ms_p99": batch_ms[-1],
            "batched_solves_per_s": len(solves) / (statistics.median(batch_ms) / 1000.0),
-           "mode": "one CUDA graph of parallel per-solve kernel chains (gi_batch)",
+           "autotune_s": tune_s, "autotune_choices": dict(sorted(chosen.items())),
+           "mode": "one CUDA graph of parallel per-solve kernel chains (gi_batch), launch shapes from the autotuner",
            "spec": "scenes.batch_spec(0..63): tris log-U(5k, 500k), G 4..32 x 1-4 levels, 320x180..1920x1080, 2-5 cascades"}
     out["speedup"] = out["batched_solves_per_s"] / out["plain_solves_per_s"]
+    out["speedup_vs_tuned_plain"] = out["batched_solves_per_s"] / out["plain_tuned_solves_per_s"]
     b.destroy()
     for x in solves:
         x.destroy()
@@ -226,9 +245,9 @@ def run_served(args, ctx):
     """The serving loop (continuous batching, 8 slots, HBM budget 150 GB, f16 atlases) against the plain one-at-a-time
     loop, on Poisson request streams at several rates over 12 resident scenes of the batch distribution, each with
     1-200 moving objects.  Latency = arrival to irradiance in host memory (host wall clock)."""
-    from rtgi import scenes, serve
+    from rtgi import autotune, scenes, serve
     specs = [scenes.batch_spec(1000 + s) for s in range(12)]
-    ex = serve.GpuExecutor(ctx, slots=8, atlas="f16")
+    ex = serve.GpuExecutor(ctx, slots=8, atlas="f16", tuner=autotune.Autotuner(reps=3))
     srv = serve.Server(ex, specs, slots=8, hbm_budget=150e9)
     for i, sp in enumerate(specs):   # scenes resident before the streams start
         srv._ensure_resident(i, 0.0)

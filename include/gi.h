@@ -234,6 +234,27 @@ int gi_rc_merge_gather_f64(gi_rc *rc, void *stream);
 /* W*H*4 doubles (rgb, a = 1 valid / 0 background) of the last gi_rc_merge_gather_f64, into host or device memory.
  * Synchronises. */
 int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);
+/* Launch tuning (no counterpart in the reference; results do not depend on it, tested bit-exact).  Picked per solve
+ * shape by the autotuner (rtgi/autotune.py); takes effect at the next solve or graph capture. */
+typedef struct gi_rc_tuning {
+  uint32_t trace_order;    /* 0: probe-major (a warp's lanes take consecutive directions of a probe, coalesced atlas
+                              writes), 1: direction-major (a warp's lanes take one direction of 32 neighbouring probes,
+                              coherent voxel paths) */
+  uint32_t trace_rays;     /* rays per lane per queue fetch: 1, 2 or 4 */
+  uint32_t trace_blocks;   /* resident 256-thread blocks per SM of the persistent trace: 1..16 (default 8) */
+  uint32_t gather_shape;   /* gather block of 256 pixels: 0 16x16 (default), 1 32x8, 2 8x32 */
+  uint32_t merge_threads;  /* threads per merge block: 64, 128, 256 (default) or 512 */
+  uint32_t reserved[3];
+} gi_rc_tuning;
+int gi_rc_set_tuning(gi_rc *rc, const gi_rc_tuning *t);
+int gi_rc_get_tuning(gi_rc *rc, gi_rc_tuning *t);
+typedef struct gi_vox_tuning {
+  uint32_t chunk_cells;    /* cells per big-triangle work item of voxBits: a power of two 32..1024 (default 128) */
+  uint32_t blocks;         /* resident 256-thread blocks per SM of the grid-stride rebuild passes: 1..16 (default 8) */
+  uint32_t reserved[6];
+} gi_vox_tuning;
+int gi_vox_set_tuning(gi_vox *vox, const gi_vox_tuning *t);
+int gi_vox_get_tuning(gi_vox *vox, gi_vox_tuning *t);
 int gi_rc_destroy(gi_rc *rc);
 
 #ifdef __cplusplus

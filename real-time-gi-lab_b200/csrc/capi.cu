@@ -119,6 +119,7 @@ struct gi_rc {
   bool timed = false;        // the last gi_solve / gi_rc_solve recorded its events
   bool timed_vox = false;    // ... and the voxel build's
   cudaEvent_t ev[7] = {};    // vox start, vox end = giBuild start, giBuild end, giTrace end, giMerge end, giGather end
+  RcLaunch launch = {8u, 0u, 256u};   // gi_rc_tuning launch shapes
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
 };
@@ -339,6 +340,8 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   d.v0 = (float)p->v0;
   d.levels = p->levels; d.G = p->G; d.max_bricks = p->max_bricks; d.max_voxels = p->max_voxels;
   d.big_cap = 1u << 18;   // BIG_CAP (voxel.ts:224)
+  d.chunk_log2 = 7;       // default gi_vox_tuning: 128 cells per big-triangle work item, 8 blocks per SM
+  d.blocks = 8;
   uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
   uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
   uint32_t vscan = (p->max_bricks + 255u) / 256u;
@@ -483,6 +486,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   d.cascades = p->cascades; d.width = W; d.height = H; d.atlas = p->atlas;
   d.vox_scale = p->vox_scale; d.vox_offset = p->vox_offset; d.level_map = p->level_map; d.vox_skip = p->vox_skip;
   d.dda_cap = p->dda_cap; d.stats = p->stats;
+  d.trace_order = 0; d.trace_rays = 1;
   // cascade layout (rc.ts:1027-1035)
   uint64_t probe_total = 0, ray_total = 0, dir_total = 0;
   for (uint32_t i = 0; i < p->cascades; i++) {
@@ -503,6 +507,8 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     double b0 = (double)p->k_interval * (pow(4.0, (double)i) - 1.0) / 3.0;
     double b1 = (double)p->k_interval * (pow(4.0, (double)(i + 1)) - 1.0) / 3.0;
     c.b0 = (float)b0; c.b1 = (float)b1;
+    c.dirs_log2 = 2u * (2u + rc_);
+    c.np = c.tiles_x * c.tiles_y;
     probe_total += (uint64_t)c.tiles_x * c.tiles_y;
     ray_total += (uint64_t)c.tiles_x * c.tiles_y * c.res * c.res;
   }
@@ -600,7 +606,8 @@ int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_solve: cudaSetDevice");
   r->dev.hits = r->debug_hits ? r->hits : nullptr;
   r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
-  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr), "gi_rc_solve: launch");
+  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr, &r->launch),
+     "gi_rc_solve: launch");
   r->timed = r->timing;
   r->timed_vox = false;
   return GI_OK;
@@ -847,6 +854,51 @@ int gi_rc_set_stats(gi_rc *r, uint32_t level) {
   if (level > 1) return fail(GI_ERR_INVALID, "gi_rc_set_stats: level %u (0 off, 1 DDA steps; the triangle comparison is not built)", level);
   r->p.stats = level;
   r->dev.stats = level;
+  return GI_OK;
+}
+
+int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
+  if (!r || !t) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: NULL argument");
+  if (t->trace_order > 1) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_order %u", t->trace_order);
+  if (t->trace_rays != 1 && t->trace_rays != 2 && t->trace_rays != 4)
+    return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_rays %u (1, 2 or 4)", t->trace_rays);
+  if (t->trace_blocks < 1 || t->trace_blocks > 16) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_blocks %u", t->trace_blocks);
+  if (t->gather_shape > 2) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: gather_shape %u", t->gather_shape);
+  if (t->merge_threads != 64 && t->merge_threads != 128 && t->merge_threads != 256 && t->merge_threads != 512)
+    return fail(GI_ERR_INVALID, "gi_rc_set_tuning: merge_threads %u", t->merge_threads);
+  r->dev.trace_order = t->trace_order;
+  r->dev.trace_rays = t->trace_rays;
+  r->launch.trace_blocks = t->trace_blocks;
+  r->launch.gather_shape = t->gather_shape;
+  r->launch.merge_threads = t->merge_threads;
+  return GI_OK;
+}
+
+int gi_rc_get_tuning(gi_rc *r, gi_rc_tuning *t) {
+  if (!r || !t) return fail(GI_ERR_INVALID, "gi_rc_get_tuning: NULL argument");
+  *t = gi_rc_tuning{};
+  t->trace_order = r->dev.trace_order; t->trace_rays = r->dev.trace_rays; t->trace_blocks = r->launch.trace_blocks;
+  t->gather_shape = r->launch.gather_shape; t->merge_threads = r->launch.merge_threads;
+  return GI_OK;
+}
+
+int gi_vox_set_tuning(gi_vox *v, const gi_vox_tuning *t) {
+  if (!v || !t) return fail(GI_ERR_INVALID, "gi_vox_set_tuning: NULL argument");
+  uint32_t c = t->chunk_cells, lg = 0;
+  while ((1u << lg) < c && lg < 31) lg++;
+  if (c < 32 || c > 1024 || (1u << lg) != c)
+    return fail(GI_ERR_INVALID, "gi_vox_set_tuning: chunk_cells %u (a power of two, 32..1024)", c);
+  if (t->blocks < 1 || t->blocks > 16) return fail(GI_ERR_INVALID, "gi_vox_set_tuning: blocks %u", t->blocks);
+  v->dev.chunk_log2 = lg;
+  v->dev.blocks = t->blocks;
+  return GI_OK;
+}
+
+int gi_vox_get_tuning(gi_vox *v, gi_vox_tuning *t) {
+  if (!v || !t) return fail(GI_ERR_INVALID, "gi_vox_get_tuning: NULL argument");
+  *t = gi_vox_tuning{};
+  t->chunk_cells = 1u << v->dev.chunk_log2;
+  t->blocks = v->dev.blocks;
   return GI_OK;
 }
 

@@ -155,6 +155,7 @@ struct SceneDev {
 struct VoxDev {
   float v0;
   uint32_t levels, G, max_bricks, max_voxels, big_cap;
+  uint32_t chunk_log2, blocks;   // tuning: cells per big-triangle work item (log2), resident blocks per SM
   int32_t origin[8][4];
   uint32_t *hdr;       // GI_HDR counter words
   uint32_t *ptr;       // levels * G^3 brick pointers

@@ -9,7 +9,8 @@ namespace gi {
 
 struct CascDev {
   uint32_t probe_off, rad_off, res, tile_size, tiles_x, tiles_y, ray_off, dir_off;
-  float b0, b1, pad2[2];
+  float b0, b1;
+  uint32_t dirs_log2, np;   // log2(res * res) (res is a power of two); probes (tiles_x * tiles_y)
 };
 
 struct ProbeDev { float4 pos; float4 nrm; int4 grid; };   // rc.ts:157 Probe, 48 bytes
@@ -20,6 +21,7 @@ struct RcDev {
   CascDev c[8];
   float vox_scale, vox_offset, level_map, vox_skip;
   uint32_t dda_cap, stats, probes_total, rays_total;
+  uint32_t trace_order, trace_rays, pad_t[2];   // tuning of k_trace (gi_rc_tuning)
   const float *frame;      // 160 words (packFrame)
   const float *depth;      // W*H
   const uint2 *normal;     // W*H rgba16f
@@ -48,8 +50,10 @@ struct RasterDev {
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
+// Launch shapes of the cascade passes (the result does not depend on them)
+struct RcLaunch { uint32_t trace_blocks, gather_shape, merge_threads; };
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
-                               cudaEvent_t *ev = nullptr);
+                               cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr);
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);

@@ -232,23 +232,31 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
   uint32_t lane = threadIdx.x & 31u;
   uint32_t steps_acc = 0, traces_acc = 0, cap_acc = 0;
   uint32_t cur_c = 0xffffffffu;
+  const uint32_t per = 32u * r.trace_rays;
   for (;;) {
     uint32_t base = 0;
-    if (lane == 0) base = atomicAdd(ray_counter, 32u);
+    if (lane == 0) base = atomicAdd(ray_counter, per);
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= r.rays_total) break;
-    uint32_t i = base + lane;
-    bool live = i < r.rays_total;
-    uint32_t c = live ? casc_of_ray(r, i) : 0u;
+   for (uint32_t k = 0; k < r.trace_rays; k++) {
+    uint32_t j = base + k * 32u + lane;   // position in the trace order
+    bool live = j < r.rays_total;
+    uint32_t c = live ? casc_of_ray(r, j) : 0u;
     TraceOut out;
     out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
     out.steps = 0;
     bool traced = false;
     if (live) {
       const CascDev &L = r.c[c];
-      uint32_t t = i - L.ray_off;
-      uint32_t dirs = L.res * L.res;
-      uint32_t pi = t / dirs, di = t % dirs;
+      uint32_t t = j - L.ray_off, pi, di;
+      if (r.trace_order == 0) {           // probe-major: the atlas order
+        pi = t >> L.dirs_log2;
+        di = t & ((1u << L.dirs_log2) - 1u);
+      } else {                            // direction-major: one direction over consecutive probes
+        di = t / L.np;
+        pi = t - di * L.np;
+      }
+      uint32_t i = L.ray_off + (pi << L.dirs_log2) + di;   // the ray's atlas element
       ProbeDev pr = r.probes[L.probe_off + pi];
       if (pr.pos.w > 0.0f) {
         float4 dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
@@ -277,6 +285,7 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
         traces_acc++; steps_acc += out.steps; cap_acc += out.steps >= r.dda_cap ? 1u : 0u;
       }
     }
+   }
   }
   if (r.stats && cur_c != 0xffffffffu) {
     atomicAdd(&r.counts[24 + cur_c], traces_acc); atomicAdd(&r.counts[32 + cur_c], steps_acc);
@@ -301,7 +310,7 @@ __device__ __forceinline__ f3 upper_avg(const RcDev &r, const typename Atlas<A>:
 
 // mergeScreen (rc.ts:710-743) for cascade c, in place
 template <int A>
-__global__ void __launch_bounds__(256) k_merge(RcDev r, uint32_t c) {
+__global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const CascDev &L = r.c[c];
@@ -388,11 +397,11 @@ __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
 }
 
 // gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829)
-template <int A>
+template <int A, uint32_t BX>
 __global__ void __launch_bounds__(256) k_gather(RcDev r) {
   typedef typename Atlas<A>::T T;
   const T *sh = reinterpret_cast<const T *>(r.sh);
-  uint32_t px = blockIdx.x * 16u + (threadIdx.x & 15u), py = blockIdx.y * 16u + (threadIdx.x >> 4);
+  uint32_t px = blockIdx.x * BX + threadIdx.x % BX, py = blockIdx.y * (256u / BX) + threadIdx.x / BX;
   if (px >= r.width || py >= r.height) return;
   size_t q = (size_t)py * r.width + px;
   const float *F = r.frame;
@@ -473,24 +482,30 @@ __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
 }
 
 template <int A>
-static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev) {
+static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
+                                const RcLaunch *ls) {
   uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
   cudaMemsetAsync(r.counts, 0, 81 * sizeof(uint32_t), st);
   if (ev) cudaEventRecord(ev[0], st);
   k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r, v);
   if (ev) cudaEventRecord(ev[1], st);
-  uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * 8u);
+  RcLaunch d = {8u, 0u, 256u};
+  if (ls) d = *ls;
+  uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
   k_trace<A><<<tb, 256, 0, st>>>(r, v, counter);
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
     uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
-    k_merge<A><<<(n + 255u) / 256u, 256, 0, st>>>(r, (uint32_t)c);
+    k_merge<A><<<(n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, 0, st>>>(r, (uint32_t)c);
   }
   k_project_sh<A><<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r);
   if (ev) cudaEventRecord(ev[3], st);
-  dim3 gg((r.width + 15u) / 16u, (r.height + 15u) / 16u);
-  k_gather<A><<<gg, 256, 0, st>>>(r);
+  uint32_t bx = d.gather_shape == 1 ? 32u : (d.gather_shape == 2 ? 8u : 16u), by = 256u / bx;
+  dim3 gg((r.width + bx - 1u) / bx, (r.height + by - 1u) / by);
+  if (bx == 32u) k_gather<A, 32u><<<gg, 256, 0, st>>>(r);
+  else if (bx == 8u) k_gather<A, 8u><<<gg, 256, 0, st>>>(r);
+  else k_gather<A, 16u><<<gg, 256, 0, st>>>(r);
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }
@@ -499,11 +514,12 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
 
 using namespace gi;
 
-cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev) {
+cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
+                               const RcLaunch *ls) {
   switch (r.atlas) {
-    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev);
-    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev);
-    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st, ev);
+    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev, ls);
+    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev, ls);
+    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st, ev, ls);
   }
   return cudaErrorInvalidValue;
 }

@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
 // k_count_chunks: per item its chunk count, an exclusive prefix within blocks of 256 items and the block sums;
 // k_scan_sums turns those into block offsets and the total; warps of k_vox_bits_big take chunks from a queue and
 // find their item by binary search over the prefix.
-constexpr uint32_t VB_CHUNK = 128;
+// VB_CHUNK = 1 << v.chunk_log2 cells per work item (gi_vox_tuning; default 128)
 
 __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
   uint32_t items = big_total(v, 16u);
@@ -371,7 +371,7 @@ __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
     if (w < items && big_item(v, 0u, 16u, w, L, t)) {
       Tri T = load_tri(s, t);
       Range r = vox_range(v, T, L, vox_size(v, L));
-      c = ((uint32_t)(r.n.x * r.n.y * r.n.z) + VB_CHUNK - 1u) / VB_CHUNK;
+      c = ((uint32_t)(r.n.x * r.n.y * r.n.z) + (1u << v.chunk_log2) - 1u) >> v.chunk_log2;
     }
     uint32_t tot;
     uint32_t ex = block_scan_256(c, &tot);
@@ -423,8 +423,8 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
     Tri T = load_tri(s, t);
     Range r = vox_range(v, T, L, vox_size(v, L));
     int n = r.n.x * r.n.y * r.n.z;
-    int q_end = min(n, (int)((part + 1u) * VB_CHUNK));
-    for (int q0 = (int)(part * VB_CHUNK); q0 < q_end; q0 += 32) {
+    int q_end = min(n, (int)((part + 1u) << v.chunk_log2));
+    for (int q0 = (int)(part << v.chunk_log2); q0 < q_end; q0 += 32) {
       int q = q0 + (int)lane;
       uint32_t wi = 0xffffffffu, msk = 0u, ri = 0u;
       bool ok = q < q_end && voxel_takes(v, s, T, L, range_cell(r, q), bo, wi, msk, ri);
@@ -641,7 +641,7 @@ using namespace gi;
 // The rebuild's launches (VOX_STAGES minus sun, voxel.ts:708), stream-ordered.
 cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_count, cudaStream_t st) {
   uint32_t per = v.G * v.G * v.G, nptr = v.levels * per;
-  uint32_t persist = sm_count * 8u;   // 8 blocks of 256 threads per SM for the grid-stride passes
+  uint32_t persist = sm_count * v.blocks;   // blocks of 256 threads per SM for the grid-stride passes (default 8)
   k_clear<<<min((nptr + 255u) / 256u + 1u, persist), 256, 0, st>>>(v);
   uint32_t tb = (s.ntris + 255u) / 256u;
   if (tb) k_mark_bricks<<<tb, 256, 0, st>>>(v, s);

@@ -57,6 +57,10 @@ SIGNATURES = {
     "gi_scene_rigid_upload": (C.c_int, [_P, _P, _P]),
     "gi_scene_rigid_apply": (C.c_int, [_P, _P]),
     "gi_rc_graph_capture_frame": (C.c_int, [_P, _P, _P, _P, _P]),
+    "gi_rc_set_tuning": (C.c_int, [_P, _P]),
+    "gi_rc_get_tuning": (C.c_int, [_P, _P]),
+    "gi_vox_set_tuning": (C.c_int, [_P, _P]),
+    "gi_vox_get_tuning": (C.c_int, [_P, _P]),
     "gi_rc_read_irradiance_f64": (C.c_int, [_P, _P, _P]),
     "gi_rc_graph_capture": (C.c_int, [_P, _P, _P]),
     "gi_rc_graph_launch": (C.c_int, [_P, _P]),
@@ -87,6 +91,15 @@ class GiRcParams(C.Structure):
     _fields_ = [("cascades", C.c_uint32), ("P", C.c_uint32), ("k_interval", C.c_float), ("vox_scale", C.c_float),
                 ("vox_offset", C.c_float), ("vox_skip", C.c_float), ("level_map", C.c_float), ("res_cap", C.c_uint32),
                 ("dda_cap", C.c_uint32), ("stats", C.c_uint32), ("atlas", C.c_uint32), ("reserved", C.c_uint32 * 5)]
+
+
+class GiRcTuning(C.Structure):
+    _fields_ = [("trace_order", C.c_uint32), ("trace_rays", C.c_uint32), ("trace_blocks", C.c_uint32),
+                ("gather_shape", C.c_uint32), ("merge_threads", C.c_uint32), ("reserved", C.c_uint32 * 3)]
+
+
+class GiVoxTuning(C.Structure):
+    _fields_ = [("chunk_cells", C.c_uint32), ("blocks", C.c_uint32), ("reserved", C.c_uint32 * 6)]
 
 
 _lib = None

@@ -143,6 +143,20 @@ class VoxWorld:
         _lib.call("gi_vox_bytes", self.handle, C.byref(b))
         return b.value
 
+    TUNING = ("chunk_cells", "blocks")
+
+    def set_tuning(self, **kw):
+        """Launch tuning of the rebuild (gi_vox_tuning): chunk_cells, blocks; unnamed fields keep their values."""
+        cur = self.get_tuning()
+        cur.update(kw)
+        t = _lib.GiVoxTuning(*[cur[k] for k in self.TUNING])
+        _lib.call("gi_vox_set_tuning", self.handle, C.byref(t))
+
+    def get_tuning(self) -> dict:
+        t = _lib.GiVoxTuning()
+        _lib.call("gi_vox_get_tuning", self.handle, C.byref(t))
+        return {k: int(getattr(t, k)) for k in self.TUNING}
+
     def destroy(self):
         if self.handle:
             _lib.call("gi_vox_destroy", self.handle)
@@ -259,6 +273,19 @@ class Rc:
         _lib.call("gi_rc_read_irradiance_raw", self.handle, ptr, self.irr_bytes(), _stream(stream))
 
     PASSES = ("vox", "giBuild", "giTrace", "giMerge", "giGather")
+    TUNING = ("trace_order", "trace_rays", "trace_blocks", "gather_shape", "merge_threads")
+
+    def set_tuning(self, **kw):
+        """Launch tuning of the cascade passes (gi_rc_tuning); unnamed fields keep their values."""
+        cur = self.get_tuning()
+        cur.update(kw)
+        t = _lib.GiRcTuning(*[cur[k] for k in self.TUNING])
+        _lib.call("gi_rc_set_tuning", self.handle, C.byref(t))
+
+    def get_tuning(self) -> dict:
+        t = _lib.GiRcTuning()
+        _lib.call("gi_rc_get_tuning", self.handle, C.byref(t))
+        return {k: int(getattr(t, k)) for k in self.TUNING}
 
     def set_timing(self, on: bool):
         _lib.call("gi_rc_set_timing", self.handle, 1 if on else 0)

@@ -198,12 +198,13 @@ class GpuExecutor:
     captured graph of the whole frame (pose, G-buffer, voxel rebuild, cascades, irradiance copy).  A request uploads
     its objects' transforms and launches the scene's graph: two calls."""
 
-    def __init__(self, ctx, slots: int, atlas: str = "f16", n_objects=None):
+    def __init__(self, ctx, slots: int, atlas: str = "f16", n_objects=None, tuner=None):
         import torch
         from . import gpu
         self.torch, self.gpu = torch, gpu
         self.ctx = ctx
         self.atlas = atlas
+        self.tuner = tuner          # an autotune.Autotuner: launch shapes picked per scene at load
         self.streams = [torch.cuda.Stream() for _ in range(max(1, slots))]
         self.events = [None] * len(self.streams)
         self.res: Dict[int, dict] = {}
@@ -236,6 +237,10 @@ class GpuExecutor:
         out = torch.empty(rc.irr_bytes(), dtype=torch.uint8).pin_memory()
         m.numpy()[:] = objs.transforms(0.0)
         sg.rigid_upload(m.data_ptr(), st)
+        if self.tuner is not None:
+            sg.rigid_apply(st)
+            rc.render_gbuffer(sg, st)
+            self.tuner.tune(rc, vw, st)
         rc.graph_capture_frame(vw, sg, out.data_ptr(), st)
         rc.graph_launch(st)
         st.synchronize()
