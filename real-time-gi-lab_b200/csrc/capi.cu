@@ -106,6 +106,7 @@ struct gi_rc {
   uint2 *normal = nullptr;
   uint32_t *tile_cnt = nullptr, *tile_fill = nullptr;   // G-buffer raster: per 16 x 16 tile (+1)
   uint32_t ntiles = 0;
+  uint64_t mavg_bytes = 0;
   float4 *stage = nullptr;
   uint4 *hits = nullptr;
   void *rad_traced = nullptr;
@@ -143,7 +144,7 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->tile_cnt); cudaFree(r->tile_fill); cudaFree(r->stage);
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
-  cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs);
+  cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
 }
 
 extern "C" {
@@ -537,13 +538,27 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   }
   d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
   d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
+  // the merge's quad averages of a cascade whose resolution is twice the one below
+  size_t avg_elems = 1;
+  for (uint32_t i = 1; i < p->cascades; i++)
+    if (d.c[i].res == 2u * d.c[i - 1].res) {
+      size_t n = (size_t)d.c[i].np * d.c[i].res * d.c[i].res / 4u;
+      if (n > avg_elems) avg_elems = n;
+    }
+  d.mavg[0] = d.mavg[1] = nullptr;
+  if ((e = dalloc(&d.mavg[0], avg_elems)) || (e = dalloc(&d.mavg[1], avg_elems))) {
+    free_rc(r);
+    delete r;
+    return cuda_fail(e, "gi_rc_create: merge averages");
+  }
+  r->mavg_bytes = 2u * avg_elems * sizeof(float4);
   cudaMemset(counts, 0, 96 * 4);
   if ((e = gi_launch_init_dirs(d, dirs, (uint32_t)dir_total, 0)) || (e = cudaDeviceSynchronize())) {
     free_rc(r);
     delete r;
     return cuda_fail(e, "gi_rc_create: direction table");
   }
-  r->bytes = 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
+  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->rad_elem_bytes + npx * atlas_elem_bytes(p->atlas) + 96 * 4;
   *out = r;
   return GI_OK;

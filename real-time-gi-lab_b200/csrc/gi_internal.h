@@ -34,6 +34,7 @@ struct RcDev {
   uint32_t *counts;        // 80 words
   uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
   void *rad_traced;        // optional: copy of the atlas after the trace
+  float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
 };
 
 // Scratch of the binned G-buffer raster (gbuffer.cu)

@@ -293,66 +293,89 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
   }
 }
 
-// upperAvg (rc.ts:681-686)
+// mergeScreen (rc.ts:710-743) for cascade c, in place, one 2x2 quad of directions (four rays) per thread.  The four
+// upper probes and their weights depend only on the probe, so a thread computes them once for its four rays.
+// upperAvg (rc.ts:681-686) of the upper cascade comes from up_avg, the quad averages the upper cascade's merge wrote
+// from its stored (rounded) texels: the same four values summed in the same order, so the same bits.  When this
+// cascade's resolution is twice the lower one's, the thread writes its own quad's average for the merge below.
 template <int A>
-__device__ __forceinline__ f3 upper_avg(const RcDev &r, const typename Atlas<A>::T *rad, uint32_t cu, uint32_t q,
-                                        uint32_t u, uint32_t vv, uint32_t lr) {
-  const CascDev &U = r.c[cu];
-  if (U.res == lr) {
-    float4 p = Atlas<A>::load(rad, (size_t)U.rad_off + q * U.res * U.res + vv * U.res + u);
-    return mk(p.x, p.y, p.z);
-  }
-  size_t base = (size_t)U.rad_off + q * U.res * U.res + vv * 2u * U.res + u * 2u;
-  float4 a = Atlas<A>::load(rad, base), b = Atlas<A>::load(rad, base + 1u);
-  float4 c = Atlas<A>::load(rad, base + U.res), d = Atlas<A>::load(rad, base + U.res + 1u);
-  return (((mk(a.x, a.y, a.z) + mk(b.x, b.y, b.z)) + mk(c.x, c.y, c.z)) + mk(d.x, d.y, d.z)) * 0.25f;
-}
-
-// mergeScreen (rc.ts:710-743) for cascade c, in place
-template <int A>
-__global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c) {
+__global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4 *__restrict__ up_avg,
+                                               float4 *__restrict__ my_avg) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const CascDev &L = r.c[c];
-  uint32_t dirs = L.res * L.res;
-  uint32_t n = L.tiles_x * L.tiles_y * dirs;
+  uint32_t hr = L.res >> 1, hq_log2 = L.dirs_log2 - 2u;   // quads per row, log2 quads per probe
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+  if (t >= (L.np << hq_log2)) return;
+  uint32_t pi = t >> hq_log2, qd = t & ((1u << hq_log2) - 1u);
+  uint32_t u0 = (qd % hr) * 2u, v0 = (qd / hr) * 2u;
   const float *F = r.frame;
-  uint32_t pi = t / dirs, di = t % dirs;
-  float4 vv = Atlas<A>::load(rad, (size_t)L.rad_off + t);
-  f3 up = mk(F[F_SKY], F[F_SKY + 1], F[F_SKY + 2]);
-  if (c + 1u < r.cascades && vv.w > 0.0f) {
-    up = mk(0.0f, 0.0f, 0.0f);
+  const bool has_up = c + 1u < r.cascades;
+  bool pr_ok = false;
+  float w[4];
+  uint32_t qi[4];
+  bool qok[4];
+  if (has_up) {
     ProbeDev pr = r.probes[L.probe_off + pi];
-    if (pr.pos.w > 0.0f) {
+    pr_ok = pr.pos.w > 0.0f;
+    if (pr_ok) {
       const CascDev &U = r.c[c + 1u];
       float cx = ((float)(pi % L.tiles_x) + 0.5f) * (float)L.tile_size;
       float cy = ((float)(pi / L.tiles_x) + 0.5f) * (float)L.tile_size;
       float ux = cx / (float)U.tile_size - 0.5f, uy = cy / (float)U.tile_size - 0.5f;
       int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
       float fx = ux - (float)bx, fy = uy - (float)by;
-      uint32_t u0 = di % L.res, v0 = di / L.res;
-      f3 acc = mk(0.0f, 0.0f, 0.0f);
-      float ws = 0.0f;
 #pragma unroll
       for (uint32_t k = 0; k < 4; k++) {
         int ox = (int)(k & 1u), oy = (int)(k >> 1);
         int qx = iclamp(bx + ox, 0, (int)U.tiles_x - 1), qy = iclamp(by + oy, 0, (int)U.tiles_y - 1);
-        uint32_t qi = (uint32_t)qy * U.tiles_x + (uint32_t)qx;
-        ProbeDev qp = r.probes[U.probe_off + qi];
-        if (qp.pos.w <= 0.0f) continue;
+        qi[k] = (uint32_t)qy * U.tiles_x + (uint32_t)qx;
+        ProbeDev qp = r.probes[U.probe_off + qi[k]];
+        qok[k] = qp.pos.w > 0.0f;
         float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
         float rel = fabsf(qp.nrm.w - pr.nrm.w) / pr.nrm.w;
-        float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f);
-        acc = acc + upper_avg<A>(r, rad, c + 1u, qi, u0, v0, L.res) * w;
-        ws += w;
+        w[k] = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f);
       }
-      if (ws > 0.0f) up = acc / ws;
     }
   }
-  f3 m = mk(vv.x, vv.y, vv.z) + up * vv.w;
-  Atlas<A>::store(rad, (size_t)L.rad_off + t, make_float4(m.x, m.y, m.z, 1.0f));
+  f3 qsum = mk(0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (uint32_t j = 0; j < 4; j++) {   // (0,0) (1,0) (0,1) (1,1): upperAvg's a, b, c, d order
+    uint32_t u = u0 + (j & 1u), v = v0 + (j >> 1);
+    size_t idx = (size_t)L.rad_off + ((size_t)pi << L.dirs_log2) + v * L.res + u;
+    float4 vv = Atlas<A>::load(rad, idx);
+    f3 up = mk(F[F_SKY], F[F_SKY + 1], F[F_SKY + 2]);
+    if (has_up && vv.w > 0.0f) {
+      up = mk(0.0f, 0.0f, 0.0f);
+      if (pr_ok) {
+        const CascDev &U = r.c[c + 1u];
+        f3 acc = mk(0.0f, 0.0f, 0.0f);
+        float ws = 0.0f;
+#pragma unroll
+        for (uint32_t k = 0; k < 4; k++) {
+          if (!qok[k]) continue;
+          f3 ua;
+          if (U.res == L.res) {
+            float4 p = Atlas<A>::load(rad, (size_t)U.rad_off + ((size_t)qi[k] << U.dirs_log2) + v * U.res + u);
+            ua = mk(p.x, p.y, p.z);
+          } else {
+            float4 p = up_avg[((size_t)qi[k] << L.dirs_log2) + v * L.res + u];
+            ua = mk(p.x, p.y, p.z);
+          }
+          acc = acc + ua * w[k];
+          ws += w[k];
+        }
+        if (ws > 0.0f) up = acc / ws;
+      }
+    }
+    f3 m = mk(vv.x, vv.y, vv.z) + up * vv.w;
+    Atlas<A>::store(rad, idx, make_float4(m.x, m.y, m.z, 1.0f));
+    if (my_avg) qsum = qsum + mk(Atlas<A>::round(m.x), Atlas<A>::round(m.y), Atlas<A>::round(m.z));
+  }
+  if (my_avg) {
+    f3 a = qsum * 0.25f;
+    my_avg[((size_t)pi << hq_log2) + (v0 >> 1) * hr + (u0 >> 1)] = make_float4(a.x, a.y, a.z, 0.0f);
+  }
 }
 
 __device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
@@ -496,8 +519,11 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
-    uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
-    k_merge<A><<<(n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, 0, st>>>(r, (uint32_t)c);
+    uint32_t n = L.np * (L.res * L.res / 4u);   // quads
+    // quad averages: written when the cascade below has half this resolution, read from the cascade above
+    float4 *mine = (c > 0 && r.c[c - 1].res * 2u == L.res) ? r.mavg[c & 1] : nullptr;
+    const float4 *above = r.mavg[(c + 1) & 1];
+    k_merge<A><<<(n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, 0, st>>>(r, (uint32_t)c, above, mine);
   }
   k_project_sh<A><<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r);
   if (ev) cudaEventRecord(ev[3], st);

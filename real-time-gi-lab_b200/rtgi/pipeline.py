@@ -1,0 +1,76 @@
+"""Frames streamed through the drop-in path with the host copies overlapped (no counterpart in the reference, which
+submits one frame per queue and maps its readback buffer when the frame is done, rcrun.ts:322-335).
+
+Each frame's inputs (the 640-byte frame block, depth f32, normal rgba16f) are copied from pinned host memory on an
+upload stream, the frame is solved (voxel rebuild + cascades, one captured graph) on the compute stream, and its
+irradiance is copied back on a download stream.  `slots` cascade sets take turns, so frame k+1's upload and frame
+k-1's download run while frame k is solved: the step time approaches the slower of the PCIe copies and the solve
+instead of their sum.  The voxel world is shared and only the compute stream touches it, so solves stay in order.
+"""
+from __future__ import annotations
+
+from typing import List
+
+from . import gpu
+
+
+class FramePipeline:
+    def __init__(self, ctx: gpu.Context, vox: gpu.VoxWorld, params, width: int, height: int, frame, depth_ptr: int,
+                 normal_f16_ptr: int, slots: int = 2):
+        """frame/depth/normal: a first frame's inputs (frame as an array, the G-buffer as pinned host pointers), used
+        to capture each slot's graph."""
+        import torch
+        self.torch = torch
+        self.vox = vox
+        self.up, self.comp, self.down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
+        self.rcs: List[gpu.Rc] = []
+        for _ in range(slots):
+            rc = gpu.Rc(ctx, params, width, height)
+            rc.set_frame(frame, self.comp)
+            rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.comp)
+            rc.graph_capture(vox, self.comp)
+            self.rcs.append(rc)
+        self.uploaded = [torch.cuda.Event() for _ in range(slots)]
+        self.solved = [torch.cuda.Event() for _ in range(slots)]
+        self.downloaded = [torch.cuda.Event() for _ in range(slots)]
+        for i in range(slots):
+            self.uploaded[i].record(self.up)
+            self.solved[i].record(self.comp)
+            self.downloaded[i].record(self.down)
+        self.k = 0
+        self.comp.synchronize()
+
+    @property
+    def irr_bytes(self) -> int:
+        return self.rcs[0].irr_bytes()
+
+    def submit(self, frame_ptr: int, depth_ptr: int, normal_f16_ptr: int, out_ptr: int) -> int:
+        """Queues one frame: inputs from pinned host memory, irradiance (as stored) into pinned host memory at out_ptr.
+        Returns the slot; the output is complete once done(slot) (or wait()) says so."""
+        s = self.k % len(self.rcs)
+        rc = self.rcs[s]
+        self.up.wait_event(self.solved[s])          # the slot's previous solve has read its inputs
+        rc.set_frame_ptr(frame_ptr, self.up)
+        rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.up)
+        self.uploaded[s].record(self.up)
+        self.comp.wait_event(self.uploaded[s])
+        self.comp.wait_event(self.downloaded[s])   # the slot's previous irradiance has been read back
+        rc.graph_launch(self.comp)
+        self.solved[s].record(self.comp)
+        self.down.wait_event(self.solved[s])
+        rc.read_irradiance_async(out_ptr, self.down)
+        self.downloaded[s].record(self.down)
+        self.k += 1
+        return s
+
+    def done(self, slot: int) -> bool:
+        return self.downloaded[slot].query()
+
+    def wait(self):
+        self.down.synchronize()
+
+    def destroy(self):
+        self.torch.cuda.synchronize()
+        for rc in self.rcs:
+            rc.destroy()
+        self.rcs = []
