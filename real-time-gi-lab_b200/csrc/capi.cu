@@ -145,6 +145,7 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
+  cudaFree((void *)r->dev.unorm8);
 }
 
 extern "C" {
@@ -343,6 +344,7 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   d.big_cap = 1u << 18;   // BIG_CAP (voxel.ts:224)
   d.chunk_log2 = 7;       // default gi_vox_tuning: 128 cells per big-triangle work item, 8 blocks per SM
   d.blocks = 8;
+  vox_derived(d);
   uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
   uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
   uint32_t vscan = (p->max_bricks + 255u) / 256u;
@@ -510,6 +512,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     c.b0 = (float)b0; c.b1 = (float)b1;
     c.dirs_log2 = 2u * (2u + rc_);
     c.np = c.tiles_x * c.tiles_y;
+    c.inv_tile = (c.tile_size & (c.tile_size - 1u)) == 0u ? 1.0f / (float)c.tile_size : 0.0f;
     probe_total += (uint64_t)c.tiles_x * c.tiles_y;
     ray_total += (uint64_t)c.tiles_x * c.tiles_y * c.res * c.res;
   }
@@ -546,6 +549,18 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
       if (n > avg_elems) avg_elems = n;
     }
   d.mavg[0] = d.mavg[1] = nullptr;
+  {
+    float tab[256];
+    for (int k = 0; k < 256; k++) tab[k] = (float)k / 255.0f;
+    float *u8 = nullptr;
+    if ((e = dalloc(&u8, 256)) || (e = cudaMemcpy(u8, tab, sizeof tab, cudaMemcpyHostToDevice))) {
+      cudaFree(u8);
+      free_rc(r);
+      delete r;
+      return cuda_fail(e, "gi_rc_create: tables");
+    }
+    d.unorm8 = u8;
+  }
   if ((e = dalloc(&d.mavg[0], avg_elems)) || (e = dalloc(&d.mavg[1], avg_elems))) {
     free_rc(r);
     delete r;

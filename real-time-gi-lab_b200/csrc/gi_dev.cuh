@@ -156,6 +156,8 @@ struct VoxDev {
   float v0;
   uint32_t levels, G, max_bricks, max_voxels, big_cap;
   uint32_t chunk_log2, blocks;   // tuning: cells per big-triangle work item (log2), resident blocks per SM
+  float vs[8];         // voxel size per level, ldexpf(v0, L) (vox_derived)
+  int32_t lim_vox[8], lim_brick[8];   // voxRange's limit f2i(G * size * 8 / cell), voxel and brick cells (vox_derived)
   int32_t origin[8][4];
   uint32_t *hdr;       // GI_HDR counter words
   uint32_t *ptr;       // levels * G^3 brick pointers
@@ -173,7 +175,7 @@ struct VoxDev {
   uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
 };
 
-__device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return ldexpf(v.v0, (int)L); }
+__device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return v.vs[L]; }
 __device__ __forceinline__ i3 org(const VoxDev &v, uint32_t L) { return mki(v.origin[L][0], v.origin[L][1], v.origin[L][2]); }
 __device__ __forceinline__ uint32_t ptr_index(const VoxDev &v, uint32_t L, i3 b) {
   uint32_t G = v.G;

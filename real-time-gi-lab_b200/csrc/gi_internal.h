@@ -1,6 +1,7 @@
 // Host/device shared declarations of the library (not part of the C-ABI).
 #pragma once
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include "gi_dev.cuh"
@@ -11,7 +12,14 @@ struct CascDev {
   uint32_t probe_off, rad_off, res, tile_size, tiles_x, tiles_y, ray_off, dir_off;
   float b0, b1;
   uint32_t dirs_log2, np;   // log2(res * res) (res is a power of two); probes (tiles_x * tiles_y)
+  float inv_tile;           // 1 / tile_size when tile_size is a power of two (x * inv_tile == x / tile_size), else 0
+  uint32_t pad3[3];
 };
+
+// x / tile_size: a multiplication when the tile is a power of two (exact), else the division
+__device__ __forceinline__ float div_tile(float x, const CascDev &L) {
+  return L.inv_tile != 0.0f ? x * L.inv_tile : x / (float)L.tile_size;
+}
 
 struct ProbeDev { float4 pos; float4 nrm; int4 grid; };   // rc.ts:157 Probe, 48 bytes
 
@@ -35,6 +43,7 @@ struct RcDev {
   uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
   void *rad_traced;        // optional: copy of the atlas after the trace
   float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
+  const float *unorm8;     // k / 255.0f for k = 0..255 (IEEE quotients, computed on the host)
 };
 
 // Scratch of the binned G-buffer raster (gbuffer.cu)
@@ -46,6 +55,25 @@ struct RasterDev {
   uint32_t *tile_cnt, *tile_fill;  // per tile: count, then list offset (ntiles + 1); fill cursor (ntiles)
   uint32_t list_cap, ntiles;
 };
+
+// Per-level constants of a voxel world computed once on the host with the same f32 operations the kernels would do:
+// the voxel size ldexpf(v0, L) (a power-of-two scaling, exact) and voxRange's cell limit f2i(G * size * 8 / cell)
+// (voxel.ts:295) for voxel cells (cell = size) and brick cells (cell = size * 8).  Call after v0 and G are set.
+static inline int32_t f2i_host(float q) {   // f32 -> i32 truncation, saturating (the kernels' f2i)
+  return q >= 2147483648.0f ? 2147483647 : (q <= -2147483648.0f ? (-2147483647 - 1) : (q != q ? 0 : (int32_t)q));
+}
+inline void vox_derived(VoxDev &d) {
+  for (uint32_t L = 0; L < 8; L++) {
+    volatile float vs = ldexpf(d.v0, (int)L);
+    volatile float a = (float)d.G * vs;
+    volatile float b = a * 8.0f;
+    volatile float cb = vs * 8.0f;
+    volatile float qv = b / vs, qb = b / cb;
+    d.vs[L] = vs;
+    d.lim_vox[L] = f2i_host(qv);
+    d.lim_brick[L] = f2i_host(qb);
+  }
+}
 
 }  // namespace gi
 

@@ -15,11 +15,21 @@
 namespace gi {
 
 // voxRank (voxel.ts:81-87)
+// (the brick's 16 words in four 128-bit loads; words past the bit's word masked out)
 __device__ __forceinline__ uint32_t vox_rank(const VoxDev &v, uint32_t brick, uint32_t bit) {
-  uint32_t w = bit >> 5;
-  const uint32_t *o = v.occ + brick * 16u;
-  uint32_t r = __popc(o[w] & ((1u << (bit & 31u)) - 1u));
-  for (uint32_t i = 0; i < w; i++) r += __popc(o[i]);
+  uint32_t w = bit >> 5, part = (1u << (bit & 31u)) - 1u;
+  const uint4 *o = reinterpret_cast<const uint4 *>(v.occ + brick * 16u);
+  uint32_t r = 0;
+#pragma unroll
+  for (uint32_t q = 0; q < 4; q++) {
+    uint4 x = __ldg(&o[q]);
+    uint32_t wd[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+    for (uint32_t k = 0; k < 4; k++) {
+      uint32_t i = 4u * q + k;
+      r += __popc(wd[k] & (i < w ? 0xffffffffu : (i == w ? part : 0u)));
+    }
+  }
   return v.base[brick] + r;
 }
 
@@ -68,7 +78,8 @@ __device__ __forceinline__ f3 toon_albedo(f3 a) {
 __device__ __forceinline__ float toon_ramp(float x) { return x > 0.3f ? 1.0f : (x > 0.05f ? 0.5f : 0.0f); }
 
 // voxShade (rc.ts:136-140) -> shadeHitV (rc.ts:108-116) with no multi-bounce, plus the voxel's emissive radiance
-__device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restrict__ F, uint32_t brick, uint32_t bit, f3 d) {
+__device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ r_unorm8,
+                                          uint32_t brick, uint32_t bit, f3 d) {
   uint4 w = make_uint4(0, 0, 0, 0);
   float vis = 0.0f;
   if (v.base[brick] != GI_EMPTY) {
@@ -76,8 +87,9 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
     w = v.attr[ai];
     vis = v.sunvis[ai];
   }
-  float alb0 = (float)(w.x & 0xffu) / 255.0f, alb1 = (float)((w.x >> 8) & 0xffu) / 255.0f;
-  float alb2 = (float)((w.x >> 16) & 0xffu) / 255.0f, alb3 = (float)(w.x >> 24) / 255.0f;
+  // k / 255 for a byte k: the quotients, tabulated (the same IEEE quotients as dividing)
+  float alb0 = __ldg(&r_unorm8[w.x & 0xffu]), alb1 = __ldg(&r_unorm8[(w.x >> 8) & 0xffu]);
+  float alb2 = __ldg(&r_unorm8[(w.x >> 16) & 0xffu]), alb3 = __ldg(&r_unorm8[w.x >> 24]);
   float nx = mx((float)(int16_t)(w.y & 0xffffu) / 32767.0f, -1.0f);
   float ny = mx((float)(int16_t)(w.y >> 16) / 32767.0f, -1.0f);
   f3 n0 = mk(nx, ny, 1.0f - fabsf(nx) - fabsf(ny));
@@ -88,7 +100,7 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   f3 n = dot(n0, n0) > 0.01f ? n0 : -d;
   if (dot(n, d) > 0.0f) n = -n;
   f3 a = mk(alb0, alb1, alb2);
-  f3 r = (a / GI_PI) * mk(0.0f, 0.0f, 0.0f);
+  f3 r = mk(0.0f, 0.0f, 0.0f);   // shadeHitV's bounce term (a / pi) * E with E = 0: +0 for finite albedo
   float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
   if (ndl > 0.0f) {
     f3 sunE = mk(F[F_SUNE], F[F_SUNE + 1], F[F_SUNE + 2]);
@@ -101,7 +113,8 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
 struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 
 // traceVox (voxel.ts:121-202) with a configurable step cap
-__device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, f3 o, f3 d, float t0, float t1,
+__device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
+                                          f3 o, f3 d, float t0, float t1,
                                           float tskip, uint32_t L, uint32_t cap, TraceOut &out) {
   out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
   out.steps = 0;
@@ -131,7 +144,7 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
     if (ptr == GI_DROP) {
       uint3 r = vox_at(v, L, c);
       if (r.x != GI_EMPTY && tIn >= tskip) {
-        out.rad = shade_voxel(v, F, r.x, r.y, d); out.T = 0.0f;
+        out.rad = shade_voxel(v, F, unorm8, r.x, r.y, d); out.T = 0.0f;
         out.lvl = r.z; out.ptr = r.x; out.bit = r.y; out.tin = __float_as_uint(tIn);
         return;
       }
@@ -162,7 +175,7 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
     uint32_t occ = __ldg(&v.occ[ptr * 16u + (bit >> 5)]);
     float tExit = mn(mn(tMax.x, tMax.y), tMax.z);
     if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
-      out.rad = shade_voxel(v, F, ptr, bit, d); out.T = 0.0f;
+      out.rad = shade_voxel(v, F, unorm8, ptr, bit, d); out.T = 0.0f;
       out.lvl = L; out.ptr = ptr; out.bit = bit; out.tin = __float_as_uint(tIn);
       return;
     }
@@ -266,7 +279,7 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
         f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
         uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
         float vs = vox_size(v, Lv);
-        trace_vox(v, F, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
+        trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
         traced = true;
       }
       Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -322,7 +335,7 @@ __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4
       const CascDev &U = r.c[c + 1u];
       float cx = ((float)(pi % L.tiles_x) + 0.5f) * (float)L.tile_size;
       float cy = ((float)(pi / L.tiles_x) + 0.5f) * (float)L.tile_size;
-      float ux = cx / (float)U.tile_size - 0.5f, uy = cy / (float)U.tile_size - 0.5f;
+      float ux = div_tile(cx, U) - 0.5f, uy = div_tile(cy, U) - 0.5f;
       int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
       float fx = ux - (float)bx, fy = uy - (float)by;
 #pragma unroll
@@ -438,7 +451,7 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
     uint2 nn = r.normal[q];
     f3 n = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
     float z = view_z(F, x);
-    float ux = ((float)px + 0.5f) / (float)L.tile_size - 0.5f, uy = ((float)py + 0.5f) / (float)L.tile_size - 0.5f;
+    float ux = div_tile((float)px + 0.5f, L) - 0.5f, uy = div_tile((float)py + 0.5f, L) - 0.5f;
     int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
     float fx = ux - (float)bx, fy = uy - (float)by;
     float y[9];

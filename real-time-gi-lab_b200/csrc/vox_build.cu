@@ -31,10 +31,12 @@ __device__ __forceinline__ Tri load_tri(const SceneDev &s, uint32_t t) {
 struct Range { i3 lo, n; };
 
 // voxRange (voxel.ts:293-300)
-__device__ __forceinline__ Range vox_range(const VoxDev &v, const Tri &T, uint32_t L, float cell) {
+// `bricks`: the cell is a brick (size * 8), else a voxel
+__device__ __forceinline__ Range vox_range(const VoxDev &v, const Tri &T, uint32_t L, bool bricks) {
+  float cell = bricks ? vox_size(v, L) * 8.0f : vox_size(v, L);
   f3 lo = region_lo(v, L);
   f3 a_ = vmin(vmin(T.a, T.b), T.c), b_ = vmax(vmax(T.a, T.b), T.c);
-  int lim = f2i((float)v.G * vox_size(v, L) * 8.0f / cell);
+  int lim = bricks ? v.lim_brick[L] : v.lim_vox[L];   // f2i(G * size * 8 / cell) (vox_derived)
   i3 a = vf2i(vfloor((a_ - lo) / cell));
   i3 b = vf2i(vfloor((b_ - lo) / cell));
   a = iclamp3(a, mki(0, 0, 0), mki(lim, lim, lim));
@@ -109,7 +111,7 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
     Range r;
     int n = 0;
     if (live) {
-      r = vox_range(v, T, L, vox_size(v, L) * 8.0f);
+      r = vox_range(v, T, L, true);
       n = r.n.x * r.n.y * r.n.z;
       if (n != 0 && !finer_holds_range(v, L, r, 8)) big = n > 8;
       else n = 0;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s
     uint32_t L, t;
     if (!big_item(v, 8u, 24u, w, L, t)) break;
     Tri T = load_tri(s, t);
-    Range r = vox_range(v, T, L, vox_size(v, L) * 8.0f);
+    Range r = vox_range(v, T, L, true);
     uint32_t n = (uint32_t)(r.n.x * r.n.y * r.n.z);
     for (uint32_t j = lane; j < n; j += 32u) mark_one(v, T, L, r, n, j);
   }
@@ -341,7 +343,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
     Range r;
     int n = 0;
     if (live) {
-      r = vox_range(v, T, L, vox_size(v, L));
+      r = vox_range(v, T, L, false);
       n = r.n.x * r.n.y * r.n.z;
       bool skip = n == 0 || (bo == 0u && finer_holds_range(v, L, r, 1));
       if (skip) n = 0;
@@ -370,7 +372,7 @@ __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
     uint32_t w = b * 256u + threadIdx.x, L, t, c = 0;
     if (w < items && big_item(v, 0u, 16u, w, L, t)) {
       Tri T = load_tri(s, t);
-      Range r = vox_range(v, T, L, vox_size(v, L));
+      Range r = vox_range(v, T, L, false);
       c = ((uint32_t)(r.n.x * r.n.y * r.n.z) + (1u << v.chunk_log2) - 1u) >> v.chunk_log2;
     }
     uint32_t tot;
@@ -421,7 +423,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
     big_item(v, 0u, 16u, lo, L, t);
     uint32_t part = ch - (v.cpre[lo] + v.scan[lo >> 8]);
     Tri T = load_tri(s, t);
-    Range r = vox_range(v, T, L, vox_size(v, L));
+    Range r = vox_range(v, T, L, false);
     int n = r.n.x * r.n.y * r.n.z;
     int q_end = min(n, (int)((part + 1u) << v.chunk_log2));
     for (int q0 = (int)(part << v.chunk_log2); q0 < q_end; q0 += 32) {
