@@ -59,6 +59,9 @@ struct gi_ctx {
 
 // Capacity of the raster's per-tile lists: 8 tiles per triangle, at least 2^20 entries (triangles past it are walked
 // by every tile instead, so the G-buffer does not depend on it)
+// Entries of the voxel rebuild's chunk-to-item table (chunks past it are found by binary search)
+constexpr uint32_t VOX_CITEM_CAP = 1u << 20;
+
 static uint32_t raster_list_cap(uint32_t ntris) {
   uint64_t c = (uint64_t)ntris * 8u;
   return (uint32_t)(c < (1u << 20) ? (1u << 20) : (c > 0xffffffffull ? 0xffffffffull : c));
@@ -135,7 +138,7 @@ static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
   cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
   cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
-  cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre);
+  cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre); cudaFree(d.citem);
 }
 static void free_rc(gi_rc *r) {
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
@@ -345,6 +348,7 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   d.chunk_log2 = 7;       // default gi_vox_tuning: 128 cells per big-triangle work item, 8 blocks per SM
   d.blocks = 8;
   vox_derived(d);
+  d.citem_cap = VOX_CITEM_CAP;
   uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
   uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
   uint32_t vscan = (p->max_bricks + 255u) / 256u;
@@ -358,13 +362,14 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
       (e = dalloc(&d.attr, p->max_voxels)) || (e = dalloc(&d.plane, p->max_voxels)) ||
       (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words)) ||
       (e = dalloc(&d.vpre, (size_t)p->max_bricks + 1u)) || (e = dalloc(&d.work, 4)) ||
-      (e = dalloc(&d.cpre, (size_t)8u * d.big_cap))) {
+      (e = dalloc(&d.cpre, (size_t)8u * d.big_cap)) || (e = dalloc(&d.citem, (size_t)VOX_CITEM_CAP))) {
     free_vox(v);
     delete v;
     return cuda_fail(e, "gi_vox_create");
   }
   v->bytes = (GI_HDR + nptr + (uint64_t)p->max_bricks * (16u + 2u + 512u) + (uint64_t)16u * d.big_cap +
-              (uint64_t)p->max_voxels * 6u + scan_words + p->max_bricks + 5u + (uint64_t)8u * d.big_cap) * 4u;
+              (uint64_t)p->max_voxels * 6u + scan_words + p->max_bricks + 5u + (uint64_t)8u * d.big_cap +
+              VOX_CITEM_CAP) * 4u;
   memset(v->hdr, 0, sizeof v->hdr);
   *out = v;
   return GI_OK;

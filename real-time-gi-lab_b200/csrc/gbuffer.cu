@@ -124,7 +124,9 @@ __device__ __forceinline__ uint32_t block_sum_256(uint32_t x, uint32_t *excl) {
 // exclusive prefix of the tile counts within its block of 256 triangles (block totals to sums)
 __global__ void __launch_bounds__(256) k_rs_setup(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
                                                   RasterDev rd) {
+  grid_dep_wait();
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  for (uint32_t i = t; i <= rd.ntiles; i += gridDim.x * blockDim.x) rd.tile_cnt[i] = 0u;   // counted by k_rs_bin
   uint32_t nt = 0;
   if (t < s.ntris) {
     uint4 idx = s.tri[t];
@@ -152,6 +154,7 @@ __global__ void __launch_bounds__(256) k_rs_setup(SceneDev s, const float *__res
 
 // Block offsets of the triangle prefix (in place in sums) and the pair total; clears the overflow count
 __global__ void __launch_bounds__(256) k_rs_scan(uint32_t nblk, RasterDev rd) {
+  grid_dep_wait();
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -171,6 +174,7 @@ __global__ void __launch_bounds__(256) k_rs_scan(uint32_t nblk, RasterDev rd) {
 // list capacity; FILL = true writes each pair's triangle into its tile's range of the list
 template <bool FILL>
 __global__ void __launch_bounds__(256) k_rs_bin(uint32_t ntris, uint32_t tiles_x, RasterDev rd) {
+  grid_dep_wait();
   uint32_t total = rd.counter[0];
   for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
     uint32_t lo = 0, hi = ntris;   // the last triangle whose first pair is <= p: the owner (it has pairs)
@@ -199,6 +203,7 @@ __global__ void __launch_bounds__(256) k_rs_bin(uint32_t ntris, uint32_t tiles_x
 // Exclusive scan of the tile counts in place (tile_cnt becomes the list offsets, tile_cnt[ntiles] the end); clears
 // the fill cursors
 __global__ void __launch_bounds__(1024) k_rs_tile_scan(RasterDev rd) {
+  grid_dep_wait();
   __shared__ uint32_t ws[32];
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -248,6 +253,7 @@ __device__ __forceinline__ uint32_t block_min_256(uint32_t x, uint32_t *ws) {
 // first); then the winner's depth and normal
 __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
                                                   uint32_t tiles_x, RasterDev rd, float *depth, uint2 *normal) {
+  grid_dep_wait();
   __shared__ float4 sa[256], se1[256], se2[256];
   __shared__ uint32_t skey[256], sval[256];
   __shared__ uint32_t ws[8];
@@ -335,13 +341,12 @@ uint32_t gi_raster_tiles(uint32_t W, uint32_t H) { return ((W + RT - 1u) / RT) *
 cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, const RasterDev &rd, uint32_t sm_count, cudaStream_t st) {
   uint32_t tiles_x = (W + RT - 1u) / RT;
-  cudaMemsetAsync(rd.tile_cnt, 0, (size_t)(rd.ntiles + 1u) * sizeof(uint32_t), st);
   uint32_t nblk = s.ntris ? (s.ntris + 255u) / 256u : 1u;
-  k_rs_setup<<<nblk, 256, 0, st>>>(s, frame_dev, W, H, rd);
-  k_rs_scan<<<1, 256, 0, st>>>(nblk, rd);
-  if (s.ntris) k_rs_bin<false><<<sm_count * 8u, 256, 0, st>>>(s.ntris, tiles_x, rd);
-  k_rs_tile_scan<<<1, 1024, 0, st>>>(rd);
-  if (s.ntris) k_rs_bin<true><<<sm_count * 8u, 256, 0, st>>>(s.ntris, tiles_x, rd);
-  k_rs_tiles<<<rd.ntiles, 256, 0, st>>>(s, frame_dev, W, H, tiles_x, rd, depth, normal);
+  GI_TRY(gi_launch(k_rs_setup, nblk, 256, st, s, frame_dev, W, H, rd));
+  GI_TRY(gi_launch(k_rs_scan, 1, 256, st, nblk, rd));
+  if (s.ntris) GI_TRY(gi_launch(k_rs_bin<false>, sm_count * 8u, 256, st, s.ntris, tiles_x, rd));
+  GI_TRY(gi_launch(k_rs_tile_scan, 1, 1024, st, rd));
+  if (s.ntris) GI_TRY(gi_launch(k_rs_bin<true>, sm_count * 8u, 256, st, s.ntris, tiles_x, rd));
+  GI_TRY(gi_launch(k_rs_tiles, rd.ntiles, 256, st, s, frame_dev, W, H, tiles_x, rd, depth, normal));
   return cudaGetLastError();
 }

@@ -141,6 +141,10 @@ template <> struct Atlas<GI_ATLAS_BF16> {
   __device__ static __forceinline__ float round(float x) { return bf2f(f2bf(x)); }
 };
 
+// Waits until the grid this one programmatically depends on (gi_launch) has completed and its writes are visible;
+// a no-op without such a dependency.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ---- device views ----------------------------------------------------------------------------------------------------
 struct SceneDev {
   const float4 *pos;       // xyz, w = 0
@@ -156,6 +160,7 @@ struct VoxDev {
   float v0;
   uint32_t levels, G, max_bricks, max_voxels, big_cap;
   uint32_t chunk_log2, blocks;   // tuning: cells per big-triangle work item (log2), resident blocks per SM
+  uint32_t citem_cap, pad_ci;    // entries of citem (0: no table)
   float vs[8];         // voxel size per level, ldexpf(v0, L) (vox_derived)
   int32_t lim_vox[8], lim_brick[8];   // voxRange's limit f2i(G * size * 8 / cell), voxel and brick cells (vox_derived)
   int32_t origin[8][4];
@@ -173,6 +178,7 @@ struct VoxDev {
   uint32_t *vpre;      // build temporary: max_bricks + 1 exclusive prefix of the bricks' voxel counts
   uint32_t *work;      // build temporary: 4 words, queue counters and the chunk total of the big-triangle passes
   uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
+  uint32_t *citem;     // build temporary (optional): the item of each chunk, citem_cap entries
 };
 
 __device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return v.vs[L]; }

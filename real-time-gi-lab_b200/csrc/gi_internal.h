@@ -79,6 +79,29 @@ inline void vox_derived(VoxDev &d) {
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
+// Kernel launch with programmatic dependent launch allowed: the next kernel in the stream (or graph) may be scheduled
+// while this one's last blocks drain, hiding the launch gap between dependent kernels.  Every kernel launched this
+// way starts with grid_dep_wait(), so nothing it reads or writes is touched before its predecessor has finished.
+template <typename... P, typename... Args>
+inline cudaError_t gi_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_t st, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, k, args...);
+}
+#define GI_TRY(...)                                   \
+  do {                                                \
+    cudaError_t e_ = (__VA_ARGS__);                   \
+    if (e_ != cudaSuccess) return e_;                 \
+  } while (0)
+
 // Launch shapes of the cascade passes (the result does not depend on them)
 struct RcLaunch { uint32_t trace_blocks, gather_shape, merge_threads; };
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,

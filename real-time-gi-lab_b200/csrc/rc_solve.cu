@@ -205,6 +205,9 @@ __device__ __forceinline__ uint32_t casc_of_ray(const RcDev &r, uint32_t i) {
 
 // setupScreen (rc.ts:572-590), every cascade in one launch
 __global__ void k_setup_screen(RcDev r, VoxDev v) {
+  grid_dep_wait();
+  // the 80 counter words and the trace's ray counter start at zero (words below `cascades` are set below)
+  if (blockIdx.x == 0 && threadIdx.x < 81u && threadIdx.x >= r.cascades) r.counts[threadIdx.x] = 0u;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= r.probes_total) return;
   uint32_t c = 0;
@@ -239,6 +242,7 @@ __global__ void k_setup_screen(RcDev r, VoxDev v) {
 // a time.
 template <int A>
 __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
+  grid_dep_wait();
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const float *F = r.frame;
@@ -314,6 +318,7 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
 template <int A>
 __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4 *__restrict__ up_avg,
                                                float4 *__restrict__ my_avg) {
+  grid_dep_wait();
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const CascDev &L = r.c[c];
@@ -400,6 +405,7 @@ __device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
 // projectSH (rc.ts:752-774): c0's 16 directions -> L2 SH of irradiance
 template <int A>
 __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
+  grid_dep_wait();
   typedef typename Atlas<A>::T T;
   const T *rad = reinterpret_cast<const T *>(r.rad);
   T *sh = reinterpret_cast<T *>(r.sh);
@@ -435,6 +441,7 @@ __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
 // gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829)
 template <int A, uint32_t BX>
 __global__ void __launch_bounds__(256) k_gather(RcDev r) {
+  grid_dep_wait();
   typedef typename Atlas<A>::T T;
   const T *sh = reinterpret_cast<const T *>(r.sh);
   uint32_t px = blockIdx.x * BX + threadIdx.x % BX, py = blockIdx.y * (256u / BX) + threadIdx.x / BX;
@@ -490,6 +497,7 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
 }
 
 __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
+  grid_dep_wait();
   size_t n = (size_t)r.width * r.height;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
     if (r.atlas == GI_ATLAS_F32) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
@@ -502,6 +510,7 @@ __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
 
 // dirOf(di, res) (rc.ts:308) of every texel of every cascade, once per Rc
 __global__ void k_init_dirs(RcDev r, float4 *dirs, uint32_t ndirs) {
+  grid_dep_wait();
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= ndirs) return;
   uint32_t c = 0;
@@ -511,6 +520,7 @@ __global__ void k_init_dirs(RcDev r, float4 *dirs, uint32_t ndirs) {
 }
 
 __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
+  grid_dep_wait();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     float4 s = src[i];
     dst[i] = make_uint2((uint32_t)f2h(s.x) | ((uint32_t)f2h(s.y) << 16), (uint32_t)f2h(s.z) | ((uint32_t)f2h(s.w) << 16));
@@ -521,14 +531,13 @@ template <int A>
 static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
                                 const RcLaunch *ls) {
   uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
-  cudaMemsetAsync(r.counts, 0, 81 * sizeof(uint32_t), st);
   if (ev) cudaEventRecord(ev[0], st);
-  k_setup_screen<<<(r.probes_total + 255u) / 256u, 256, 0, st>>>(r, v);
+  GI_TRY(gi_launch(k_setup_screen, (r.probes_total + 255u) / 256u, 256, st, r, v));
   if (ev) cudaEventRecord(ev[1], st);
   RcLaunch d = {8u, 0u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
-  k_trace<A><<<tb, 256, 0, st>>>(r, v, counter);
+  GI_TRY(gi_launch(k_trace<A>, tb, 256, st, r, v, counter));
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
@@ -536,15 +545,15 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
     // quad averages: written when the cascade below has half this resolution, read from the cascade above
     float4 *mine = (c > 0 && r.c[c - 1].res * 2u == L.res) ? r.mavg[c & 1] : nullptr;
     const float4 *above = r.mavg[(c + 1) & 1];
-    k_merge<A><<<(n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, 0, st>>>(r, (uint32_t)c, above, mine);
+    GI_TRY(gi_launch(k_merge<A>, (n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, st, r, (uint32_t)c, above, mine));
   }
-  k_project_sh<A><<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r);
+  GI_TRY(gi_launch(k_project_sh<A>, (r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, st, r));
   if (ev) cudaEventRecord(ev[3], st);
   uint32_t bx = d.gather_shape == 1 ? 32u : (d.gather_shape == 2 ? 8u : 16u), by = 256u / bx;
   dim3 gg((r.width + bx - 1u) / bx, (r.height + by - 1u) / by);
-  if (bx == 32u) k_gather<A, 32u><<<gg, 256, 0, st>>>(r);
-  else if (bx == 8u) k_gather<A, 8u><<<gg, 256, 0, st>>>(r);
-  else k_gather<A, 16u><<<gg, 256, 0, st>>>(r);
+  if (bx == 32u) GI_TRY(gi_launch(k_gather<A, 32u>, gg, 256, st, r));
+  else if (bx == 8u) GI_TRY(gi_launch(k_gather<A, 8u>, gg, 256, st, r));
+  else GI_TRY(gi_launch(k_gather<A, 16u>, gg, 256, st, r));
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }

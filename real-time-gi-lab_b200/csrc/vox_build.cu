@@ -91,6 +91,7 @@ __device__ __forceinline__ void mark_one(const VoxDev &v, const Tri &T, uint32_t
 
 // clear (voxel.ts:338-344)
 __global__ void k_clear(VoxDev v) {
+  grid_dep_wait();
   uint32_t n = v.levels * v.G * v.G * v.G;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < GI_HDR; i += gridDim.x * blockDim.x) {
     if (i < GI_HDR) v.hdr[i] = 0u;
@@ -102,6 +103,7 @@ __global__ void k_clear(VoxDev v) {
 // markBricks (voxel.ts:359-376): one thread per triangle; every lane walks the same levels so that the list appends
 // are warp-aggregated.
 __global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = t < s.ntris;
   Tri T;
@@ -145,6 +147,7 @@ __device__ __forceinline__ uint32_t big_total(const VoxDev &v, uint32_t hdr0) {
 
 // markBricksBig (voxel.ts:377-387): one warp per big (triangle, level), lanes over the range's bricks.
 __global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
   for (;;) {
     uint32_t w = 0;
@@ -161,6 +164,7 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s
 
 // markParents (voxel.ts:390-403)
 __global__ void k_mark_parents(VoxDev v) {
+  grid_dep_wait();
   uint32_t G = v.G, per = G * G * G, NL = v.levels;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (NL - 1u) * per; i += gridDim.x * blockDim.x) {
     if (v.ptr[i] != GI_MARK) continue;
@@ -218,6 +222,7 @@ __device__ __forceinline__ uint32_t block_scan_256(uint32_t x, uint32_t *total) 
 
 // Per block: the number of marked entries of its chunk of the order space.
 __global__ void __launch_bounds__(256) k_count_marks(VoxDev v) {
+  grid_dep_wait();
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per;
   uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
   uint32_t c = 0;
@@ -232,6 +237,7 @@ __global__ void __launch_bounds__(256) k_count_marks(VoxDev v) {
 
 // Exclusive scan of the block sums (one block, nblocks <= 256 * 16); writes the total to hdr[0] and hdr[5].
 __global__ void __launch_bounds__(256) k_scan_sums(uint32_t *sums, uint32_t nblocks, uint32_t *hdr) {
+  grid_dep_wait();
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
   __syncthreads();
@@ -250,6 +256,7 @@ __global__ void __launch_bounds__(256) k_scan_sums(uint32_t *sums, uint32_t nblo
 
 // The chunk prefix's block offsets (k_count_chunks wrote one sum per 256 items) and the chunk total (work[2]).
 __global__ void __launch_bounds__(256) k_scan_chunks(VoxDev v) {
+  grid_dep_wait();
   uint32_t nblocks = (big_total(v, 16u) + 255u) / 256u;
   __shared__ uint32_t carry;
   if (threadIdx.x == 0) carry = 0;
@@ -269,6 +276,7 @@ __global__ void __launch_bounds__(256) k_scan_chunks(VoxDev v) {
 
 // allocBricks (voxel.ts:450-470) in the fixed order.
 __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
+  grid_dep_wait();
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per, G = v.G;
   uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
   // each thread owns 8 consecutive entries of the chunk
@@ -300,6 +308,7 @@ __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
 // The rest of the brick init and clearKeys (voxel.ts:467, :471-474): zero the occupancy (64 B) and representatives
 // (2 KB) of every allocated brick, over the whole grid.
 __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
+  grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint4 z = make_uint4(0u, 0u, 0u, 0u);
   uint4 *occ = reinterpret_cast<uint4 *>(v.occ), *rep = reinterpret_cast<uint4 *>(v.rep);
@@ -333,6 +342,7 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
 
 // voxBits (voxel.ts:492-513)
 __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = t < s.ntris;
   uint32_t bo = v.hdr[2];
@@ -366,6 +376,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
 // VB_CHUNK = 1 << v.chunk_log2 cells per work item (gi_vox_tuning; default 128)
 
 __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t items = big_total(v, 16u);
   uint32_t nblk = (items + 255u) / 256u;
   for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x) {
@@ -379,6 +390,18 @@ __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
     uint32_t ex = block_scan_256(c, &tot);
     if (w < items) v.cpre[w] = ex;
     if (threadIdx.x == 0) v.scan[b] = tot;
+  }
+}
+
+// The item of every chunk below citem_cap (the rest are found by binary search over the prefix): a table lookup
+// instead of ~16 dependent loads per chunk.
+__global__ void __launch_bounds__(256) k_fill_chunks(VoxDev v) {
+  grid_dep_wait();
+  uint32_t items = big_total(v, 16u), total = v.work[2];
+  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < items; w += gridDim.x * blockDim.x) {
+    uint32_t first = v.cpre[w] + v.scan[w >> 8];
+    uint32_t end = w + 1u < items ? v.cpre[w + 1u] + v.scan[(w + 1u) >> 8] : total;
+    for (uint32_t ch = first; ch < end && ch < v.citem_cap; ch++) v.citem[ch] = w;
   }
 }
 
@@ -405,6 +428,7 @@ __device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, 
 // One warp per chunk.  The lanes' occupancy bits are ORed per word inside the warp (neighbouring cells share a
 // word), one atomic per word.
 __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
   uint32_t bo = v.hdr[2];
   uint32_t items = big_total(v, 16u);
@@ -414,10 +438,15 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
     if (lane == 0) ch = atomicAdd(&v.work[1], 1u);
     ch = __shfl_sync(0xffffffffu, ch, 0);
     if (ch >= chunks) break;
-    uint32_t lo = 0, hi = items;   // the last item whose first chunk is <= ch
-    while (hi - lo > 1u) {
-      uint32_t m = (lo + hi) >> 1;
-      if (v.cpre[m] + v.scan[m >> 8] <= ch) lo = m; else hi = m;
+    uint32_t lo = 0;
+    if (ch < v.citem_cap) {
+      lo = v.citem[ch];              // the chunk's item, tabulated by k_fill_chunks
+    } else {
+      uint32_t hi = items;           // the last item whose first chunk is <= ch
+      while (hi - lo > 1u) {
+        uint32_t m = (lo + hi) >> 1;
+        if (v.cpre[m] + v.scan[m >> 8] <= ch) lo = m; else hi = m;
+      }
     }
     uint32_t L, t;
     big_item(v, 0u, 16u, lo, L, t);
@@ -451,6 +480,7 @@ __device__ __forceinline__ void level_bricks(const VoxDev &v, uint32_t l, uint32
 
 // reduce (voxel.ts:540-577): level L from level L-1, one thread per occupancy word of a level L-1 brick
 __global__ void __launch_bounds__(256) k_reduce(VoxDev v, uint32_t L) {
+  grid_dep_wait();
   uint32_t first, count;
   level_bricks(v, L - 1u, first, count);
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count * 16u; i += gridDim.x * blockDim.x) {
@@ -515,6 +545,7 @@ __device__ __forceinline__ uint32_t brick_pop(const VoxDev &v, uint32_t b) {
 }
 
 __global__ void __launch_bounds__(256) k_count_voxels(VoxDev v) {
+  grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
   uint32_t c = b < nb ? brick_pop(v, b) : 0u;
@@ -524,6 +555,7 @@ __global__ void __launch_bounds__(256) k_count_voxels(VoxDev v) {
 }
 
 __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks) {
+  grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
   uint32_t c = b < nb ? brick_pop(v, b) : 0u;
@@ -568,6 +600,7 @@ __device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
 // ai - vpre[b] of b's occupancy), so every occupied voxel is resolved in parallel and the attribute writes are
 // contiguous.
 __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
+  grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t nv = nb ? min(v.vpre[nb], v.max_voxels) : 0u;
   for (uint32_t ai = blockIdx.x * blockDim.x + threadIdx.x; ai < nv; ai += gridDim.x * blockDim.x) {
@@ -644,25 +677,26 @@ using namespace gi;
 cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_count, cudaStream_t st) {
   uint32_t per = v.G * v.G * v.G, nptr = v.levels * per;
   uint32_t persist = sm_count * v.blocks;   // blocks of 256 threads per SM for the grid-stride passes (default 8)
-  k_clear<<<min((nptr + 255u) / 256u + 1u, persist), 256, 0, st>>>(v);
+  GI_TRY(gi_launch(k_clear, min((nptr + 255u) / 256u + 1u, persist), 256, st, v));
   uint32_t tb = (s.ntris + 255u) / 256u;
-  if (tb) k_mark_bricks<<<tb, 256, 0, st>>>(v, s);
-  k_mark_bricks_big<<<persist, 256, 0, st>>>(v, s);
-  if (v.levels > 1) k_mark_parents<<<min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, 0, st>>>(v);
+  if (tb) GI_TRY(gi_launch(k_mark_bricks, tb, 256, st, v, s));
+  GI_TRY(gi_launch(k_mark_bricks_big, persist, 256, st, v, s));
+  if (v.levels > 1) GI_TRY(gi_launch(k_mark_parents, min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, st, v));
   uint32_t ab = (nptr + ALLOC_CHUNK - 1u) / ALLOC_CHUNK;
-  k_count_marks<<<ab, 256, 0, st>>>(v);
-  k_scan_sums<<<1, 256, 0, st>>>(v.scan, ab, v.hdr);
-  k_alloc_bricks<<<ab, 256, 0, st>>>(v);
-  k_init_bricks<<<persist, 256, 0, st>>>(v);
-  if (tb) k_vox_bits<<<tb, 256, 0, st>>>(v, s);
-  k_count_chunks<<<persist, 256, 0, st>>>(v, s);
-  k_scan_chunks<<<1, 256, 0, st>>>(v);
-  k_vox_bits_big<<<persist, 256, 0, st>>>(v, s);
-  for (uint32_t L = 1; L < v.levels; L++) k_reduce<<<persist, 256, 0, st>>>(v, L);
+  GI_TRY(gi_launch(k_count_marks, ab, 256, st, v));
+  GI_TRY(gi_launch(k_scan_sums, 1, 256, st, v.scan, ab, v.hdr));
+  GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v));
+  GI_TRY(gi_launch(k_init_bricks, persist, 256, st, v));
+  if (tb) GI_TRY(gi_launch(k_vox_bits, tb, 256, st, v, s));
+  GI_TRY(gi_launch(k_count_chunks, persist, 256, st, v, s));
+  GI_TRY(gi_launch(k_scan_chunks, 1, 256, st, v));
+  if (v.citem_cap) GI_TRY(gi_launch(k_fill_chunks, persist, 256, st, v));
+  GI_TRY(gi_launch(k_vox_bits_big, persist, 256, st, v, s));
+  for (uint32_t L = 1; L < v.levels; L++) GI_TRY(gi_launch(k_reduce, persist, 256, st, v, L));
   uint32_t vb = (v.max_bricks + VOX_CHUNK - 1u) / VOX_CHUNK;
-  k_count_voxels<<<vb, 256, 0, st>>>(v);
-  k_scan_sums<<<1, 256, 0, st>>>(v.scan, vb, nullptr);
-  k_alloc_voxels<<<vb, 256, 0, st>>>(v, vb);
-  k_resolve_attr<<<persist, 256, 0, st>>>(v, s);
+  GI_TRY(gi_launch(k_count_voxels, vb, 256, st, v));
+  GI_TRY(gi_launch(k_scan_sums, 1, 256, st, v.scan, vb, nullptr));
+  GI_TRY(gi_launch(k_alloc_voxels, vb, 256, st, v, vb));
+  GI_TRY(gi_launch(k_resolve_attr, persist, 256, st, v, s));
   return cudaGetLastError();
 }

@@ -216,7 +216,7 @@ class GpuExecutor:
         lay = configs.cascade_layout(p, W, H)
         elem = 16 if self.atlas == "f32" else 8
         rc = W * H * (4 + 8 + 16 + elem) + lay["probes_total"] * 52 + lay["rays_total"] * elem * 1
-        vox = (v.levels * v.G ** 3 + v.maxBricks * (530 + 1) + 16 * (1 << 18) + 8 * (1 << 18) + v.maxVoxels * 6) * 4
+        vox = (v.levels * v.G ** 3 + v.maxBricks * (530 + 1) + 16 * (1 << 18) + 8 * (1 << 18) + v.maxVoxels * 6 + (1 << 20)) * 4
         return int(rc + vox + 140 * spec["tris"] + (4 << 20))
 
     def load(self, sid: int, spec: dict) -> int:
