@@ -242,7 +242,9 @@ typedef struct gi_rc_tuning {
                               coherent voxel paths) */
   uint32_t trace_rays;     /* rays per lane per queue fetch: 1, 2 or 4 */
   uint32_t trace_blocks;   /* resident 256-thread blocks per SM of the persistent trace: 1..16 (default 8) */
-  uint32_t gather_shape;   /* gather block of 256 pixels: 0 16x16 (default), 1 32x8, 2 8x32 */
+  uint32_t gather_shape;   /* gather: 0, 1, 2 blocks of 16x16, 32x8, 8x32 pixels; 3 (default) warps on pixel tiles
+                              aligned to the probe cells, the shared probes staged in shared memory (cascade-0 tile
+                              size 8, 16 or 32; otherwise 16x16) */
   uint32_t merge_threads;  /* threads per merge block: 64, 128, 256 (default) or 512 */
   uint32_t reserved[3];
 } gi_rc_tuning;

@@ -123,7 +123,7 @@ struct gi_rc {
   bool timed = false;        // the last gi_solve / gi_rc_solve recorded its events
   bool timed_vox = false;    // ... and the voxel build's
   cudaEvent_t ev[7] = {};    // vox start, vox end = giBuild start, giBuild end, giTrace end, giMerge end, giGather end
-  RcLaunch launch = {8u, 0u, 256u};   // gi_rc_tuning launch shapes
+  RcLaunch launch = {8u, 3u, 256u};   // gi_rc_tuning launch shapes
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
 };
@@ -898,7 +898,7 @@ int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
   if (t->trace_rays != 1 && t->trace_rays != 2 && t->trace_rays != 4)
     return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_rays %u (1, 2 or 4)", t->trace_rays);
   if (t->trace_blocks < 1 || t->trace_blocks > 16) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_blocks %u", t->trace_blocks);
-  if (t->gather_shape > 2) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: gather_shape %u", t->gather_shape);
+  if (t->gather_shape > 3) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: gather_shape %u", t->gather_shape);
   if (t->merge_threads != 64 && t->merge_threads != 128 && t->merge_threads != 256 && t->merge_threads != 512)
     return fail(GI_ERR_INVALID, "gi_rc_set_tuning: merge_threads %u", t->merge_threads);
   r->dev.trace_order = t->trace_order;

@@ -438,14 +438,10 @@ __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
     Atlas<A>::store(sh, (size_t)pi * 8u + q, make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]));
 }
 
-// gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829)
-template <int A, uint32_t BX>
-__global__ void __launch_bounds__(256) k_gather(RcDev r) {
-  grid_dep_wait();
-  typedef typename Atlas<A>::T T;
-  const T *sh = reinterpret_cast<const T *>(r.sh);
-  uint32_t px = blockIdx.x * BX + threadIdx.x % BX, py = blockIdx.y * (256u / BX) + threadIdx.x / BX;
-  if (px >= r.width || py >= r.height) return;
+// gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829) for one pixel.  Src supplies the 2x2 cascade-0 probes around
+// the pixel: probe(k, qi) and coef(k, qi, j), the j-th 4-component group of its SH as f32.
+template <int A, class Src>
+__device__ __forceinline__ void gather_pixel(const RcDev &r, uint32_t px, uint32_t py, const Src &src) {
   size_t q = (size_t)py * r.width + px;
   const float *F = r.frame;
   float d = r.depth[q];
@@ -470,7 +466,7 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
       int ox = (int)(k & 1u), oy = (int)(k >> 1);
       int qx = iclamp(bx + ox, 0, (int)L.tiles_x - 1), qy = iclamp(by + oy, 0, (int)L.tiles_y - 1);
       uint32_t qi = (uint32_t)qy * L.tiles_x + (uint32_t)qx;
-      ProbeDev pr = r.probes[L.probe_off + qi];
+      ProbeDev pr = src.probe(k, qi);
       if (pr.pos.w <= 0.0f) continue;
       float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
       float rel = fabsf(pr.nrm.w - z) / z;
@@ -479,8 +475,8 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
       float v[32];
 #pragma unroll
       for (int j = 0; j < 8; j++) {
-        float4 s = Atlas<A>::load(sh, (size_t)qi * 8u + j);
-        v[4 * j] = s.x; v[4 * j + 1] = s.y; v[4 * j + 2] = s.z; v[4 * j + 3] = s.w;
+        float4 sc = src.coef(k, qi, j);
+        v[4 * j] = sc.x; v[4 * j + 1] = sc.y; v[4 * j + 2] = sc.z; v[4 * j + 3] = sc.w;
       }
       f3 es = mk(0.0f, 0.0f, 0.0f);
 #pragma unroll
@@ -494,6 +490,77 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
   if (A == GI_ATLAS_F32) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
   else reinterpret_cast<uint2 *>(r.irr)[q] = make_uint2((uint32_t)f2h(res.x) | ((uint32_t)f2h(res.y) << 16),
                                                        (uint32_t)f2h(res.z) | ((uint32_t)f2h(alpha) << 16));
+}
+
+template <int A>
+struct GlobalProbes {   // each lane reads its own probes
+  const RcDev &r;
+  __device__ __forceinline__ ProbeDev probe(uint32_t, uint32_t qi) const { return r.probes[r.c[0].probe_off + qi]; }
+  __device__ __forceinline__ float4 coef(uint32_t, uint32_t qi, int j) const {
+    return Atlas<A>::load(reinterpret_cast<const typename Atlas<A>::T *>(r.sh), (size_t)qi * 8u + j);
+  }
+};
+
+struct SharedProbes {   // the warp's four probes, staged in shared memory (k = the 2x2 corner)
+  const float4 *pn;      // [2k] pos, [2k + 1] nrm
+  const float4 *coefs;   // [8k + j]
+  __device__ __forceinline__ ProbeDev probe(uint32_t k, uint32_t) const {
+    ProbeDev p;
+    p.pos = pn[2u * k];
+    p.nrm = pn[2u * k + 1u];
+    p.grid = make_int4(0, 0, 0, 0);
+    return p;
+  }
+  __device__ __forceinline__ float4 coef(uint32_t k, uint32_t, int j) const { return coefs[8u * k + (uint32_t)j]; }
+};
+
+// One thread per pixel, BX x (256 / BX) pixels per block
+template <int A, uint32_t BX>
+__global__ void __launch_bounds__(256) k_gather(RcDev r) {
+  grid_dep_wait();
+  uint32_t px = blockIdx.x * BX + threadIdx.x % BX, py = blockIdx.y * (256u / BX) + threadIdx.x / BX;
+  if (px >= r.width || py >= r.height) return;
+  gather_pixel<A>(r, px, py, GlobalProbes<A>{r});
+}
+
+// Warp tiles of P x (32 / P) pixels aligned to the cascade-0 probe cells (P = the tile size): every pixel of a tile
+// interpolates the same four probes, so the warp loads their records and SH once into shared memory (one 128-bit load
+// per lane) and the pixels read them as broadcasts.  A warp whose pixels turn out not to share their probes (they
+// always do for these P; the check keeps it exact regardless) reads them per lane.  Blocks of 2 x 4 warp tiles.
+template <int A, uint32_t P>
+__global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
+  grid_dep_wait();
+  constexpr uint32_t TH = 32u / P;
+  __shared__ float4 s_coef[8][32];
+  __shared__ float4 s_pn[8][8];
+  const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const int tx = (int)(blockIdx.x * 2u + (warp & 1u)), ty = (int)(blockIdx.y * 4u + (warp >> 1));
+  const int px = tx * (int)P - (int)(P / 2u) + (int)(lane % P), py = ty * (int)TH - (int)(P / 2u) + (int)(lane / P);
+  const bool on = px >= 0 && py >= 0 && px < (int)r.width && py < (int)r.height;
+  const unsigned on_mask = __ballot_sync(0xffffffffu, on);
+  if (on_mask == 0u) return;   // whole warp off the screen
+  const CascDev &L = r.c[0];
+  int bx = f2i(floorf(div_tile((float)px + 0.5f, L) - 0.5f)), by = f2i(floorf(div_tile((float)py + 0.5f, L) - 0.5f));
+  const int src_lane = __ffs(on_mask) - 1;
+  const int bx0 = __shfl_sync(0xffffffffu, bx, src_lane), by0 = __shfl_sync(0xffffffffu, by, src_lane);
+  if (!__all_sync(0xffffffffu, !on || (bx == bx0 && by == by0))) {
+    if (on) gather_pixel<A>(r, (uint32_t)px, (uint32_t)py, GlobalProbes<A>{r});
+    return;
+  }
+  {
+    uint32_t k = lane >> 3, j = lane & 7u;
+    int qx = iclamp(bx0 + (int)(k & 1u), 0, (int)L.tiles_x - 1), qy = iclamp(by0 + (int)(k >> 1), 0, (int)L.tiles_y - 1);
+    uint32_t qi = (uint32_t)qy * L.tiles_x + (uint32_t)qx;
+    s_coef[warp][lane] = Atlas<A>::load(reinterpret_cast<const typename Atlas<A>::T *>(r.sh), (size_t)qi * 8u + j);
+    if (lane < 8u) {
+      uint32_t kk = lane >> 1;
+      int qx2 = iclamp(bx0 + (int)(kk & 1u), 0, (int)L.tiles_x - 1), qy2 = iclamp(by0 + (int)(kk >> 1), 0, (int)L.tiles_y - 1);
+      const ProbeDev &pr = r.probes[L.probe_off + (uint32_t)qy2 * L.tiles_x + (uint32_t)qx2];
+      s_pn[warp][lane] = (lane & 1u) ? pr.nrm : pr.pos;
+    }
+  }
+  __syncwarp();
+  if (on) gather_pixel<A>(r, (uint32_t)px, (uint32_t)py, SharedProbes{s_pn[warp], s_coef[warp]});
 }
 
 __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
@@ -534,7 +601,7 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   if (ev) cudaEventRecord(ev[0], st);
   GI_TRY(gi_launch(k_setup_screen, (r.probes_total + 255u) / 256u, 256, st, r, v));
   if (ev) cudaEventRecord(ev[1], st);
-  RcLaunch d = {8u, 0u, 256u};
+  RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
   GI_TRY(gi_launch(k_trace<A>, tb, 256, st, r, v, counter));
@@ -549,11 +616,21 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   }
   GI_TRY(gi_launch(k_project_sh<A>, (r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, st, r));
   if (ev) cudaEventRecord(ev[3], st);
-  uint32_t bx = d.gather_shape == 1 ? 32u : (d.gather_shape == 2 ? 8u : 16u), by = 256u / bx;
-  dim3 gg((r.width + bx - 1u) / bx, (r.height + by - 1u) / by);
-  if (bx == 32u) GI_TRY(gi_launch(k_gather<A, 32u>, gg, 256, st, r));
-  else if (bx == 8u) GI_TRY(gi_launch(k_gather<A, 8u>, gg, 256, st, r));
-  else GI_TRY(gi_launch(k_gather<A, 16u>, gg, 256, st, r));
+  const uint32_t P0 = r.c[0].tile_size;
+  if (d.gather_shape == 3 && (P0 == 8u || P0 == 16u || P0 == 32u)) {
+    uint32_t th = 32u / P0;   // warp tiles start half a probe cell before the screen
+    uint32_t ntx = (r.width + P0 / 2u + P0 - 1u) / P0, nty = (r.height + P0 / 2u + th - 1u) / th;
+    dim3 gg((ntx + 1u) / 2u, (nty + 3u) / 4u);
+    if (P0 == 8u) GI_TRY(gi_launch(k_gather_tiled<A, 8u>, gg, 256, st, r));
+    else if (P0 == 16u) GI_TRY(gi_launch(k_gather_tiled<A, 16u>, gg, 256, st, r));
+    else GI_TRY(gi_launch(k_gather_tiled<A, 32u>, gg, 256, st, r));
+  } else {
+    uint32_t bx = d.gather_shape == 1 ? 32u : (d.gather_shape == 2 ? 8u : 16u), by = 256u / bx;
+    dim3 gg((r.width + bx - 1u) / bx, (r.height + by - 1u) / by);
+    if (bx == 32u) GI_TRY(gi_launch(k_gather<A, 32u>, gg, 256, st, r));
+    else if (bx == 8u) GI_TRY(gi_launch(k_gather<A, 8u>, gg, 256, st, r));
+    else GI_TRY(gi_launch(k_gather<A, 16u>, gg, 256, st, r));
+  }
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }

@@ -5,7 +5,7 @@ WGSL).  The tunables change how work is laid onto the GPU, never the result (tes
             direction-major: one direction over 32 neighbouring probes, coherent voxel paths), trace_rays (rays per
             lane per queue fetch), trace_blocks (resident blocks per SM of the persistent trace)
   giMerge   merge_threads (block size)
-  giGather  gather_shape (16x16, 32x8 or 8x32 pixels per block)
+  giGather  gather_shape (16x16, 32x8 or 8x32 pixels per block, or warps on probe-aligned tiles)
   vox       chunk_cells (cells per big-triangle work item of voxBits), blocks (resident blocks per SM)
 
 Each pass's tunables only move that pass's time, so the search is per pass: every combination of one pass's
@@ -23,7 +23,7 @@ from typing import Dict, Optional
 RC_GROUPS = {
     "giTrace": {"trace_order": [0, 1], "trace_rays": [1, 2, 4], "trace_blocks": [4, 8, 16]},
     "giMerge": {"merge_threads": [128, 256, 512]},
-    "giGather": {"gather_shape": [0, 1, 2]},
+    "giGather": {"gather_shape": [0, 1, 2, 3]},
 }
 VOX_GROUPS = {"vox": {"chunk_cells": [32, 64, 128, 256, 512], "blocks": [4, 8, 16]}}
 

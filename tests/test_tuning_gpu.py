@@ -47,6 +47,7 @@ VARIANTS = [
     ({"trace_order": 1}, None),
     ({"trace_rays": 4, "trace_blocks": 2}, None),
     ({"trace_order": 1, "trace_rays": 2, "trace_blocks": 16}, None),
+    ({"gather_shape": 0}, None),
     ({"gather_shape": 1, "merge_threads": 64}, None),
     ({"gather_shape": 2, "merge_threads": 512}, None),
     (None, {"chunk_cells": 32, "blocks": 2}),
@@ -69,11 +70,11 @@ def test_tuning_rejects_bad_values(ctx):
     case = gi_cases.config0()
     rc = gpu.Rc(ctx, case.rc, case.width, case.height)
     try:
-        for bad in ({"trace_rays": 3}, {"trace_order": 2}, {"trace_blocks": 0}, {"gather_shape": 3},
+        for bad in ({"trace_rays": 3}, {"trace_order": 2}, {"trace_blocks": 0}, {"gather_shape": 4},
                     {"merge_threads": 100}):
             with pytest.raises(_lib.GiError):
                 rc.set_tuning(**bad)
-        assert rc.get_tuning() == {"trace_order": 0, "trace_rays": 1, "trace_blocks": 8, "gather_shape": 0,
+        assert rc.get_tuning() == {"trace_order": 0, "trace_rays": 1, "trace_blocks": 8, "gather_shape": 3,
                                    "merge_threads": 256}
     finally:
         rc.destroy()
