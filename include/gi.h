@@ -84,7 +84,9 @@ typedef struct {
   uint32_t dda_cap;      /* DDA step cap (the reference hard-codes 1024, voxel.ts:142) */
   uint32_t stats;        /* 0 off, 1 DDA step counters (rc.ts:232-235) */
   uint32_t atlas;        /* gi_atlas */
-  uint32_t reserved[5];
+  uint32_t f32_out;      /* 1: SH and irradiance stored as f32 whatever the atlas (the reference stores both f16,
+                            rc.ts:768-773, :1073); 0: stored like the atlas, f16 for F16/BF16 */
+  uint32_t reserved[4];
 } gi_rc_params;
 
 int gi_version(void);

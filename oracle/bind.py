@@ -82,7 +82,7 @@ class OrcCasc(C.Structure):
 class OrcLayout(C.Structure):
     _fields_ = [("cascades", C.c_uint32), ("c", OrcCasc * 8), ("vox_scale", C.c_float), ("vox_offset", C.c_float),
                 ("level_map", C.c_float), ("vox_skip", C.c_float), ("dda_cap", C.c_uint32), ("stats", C.c_uint32),
-                ("atlas", C.c_uint32), ("pad", C.c_uint32)]
+                ("atlas", C.c_uint32), ("f32_out", C.c_uint32)]
 
 
 class OrcGbuf(C.Structure):
@@ -168,6 +168,7 @@ def layout_struct(lay: dict) -> OrcLayout:
         ly.c[i].b0, ly.c[i].b1 = c["b0"], c["b1"]
     ly.vox_scale, ly.vox_offset, ly.level_map, ly.vox_skip = lay["vox_scale"], lay["vox_offset"], lay["level_map"], lay["vox_skip"]
     ly.dda_cap, ly.stats, ly.atlas = lay["dda_cap"], lay["stats"], lay["atlas"]
+    ly.f32_out = lay.get("f32_out", 0)
     return ly
 
 

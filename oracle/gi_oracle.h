@@ -95,7 +95,7 @@ typedef struct {
   uint32_t dda_cap;       /* DDA step cap (the reference hard-codes 1024, voxel.ts:142) */
   uint32_t stats;         /* 0 off, 1 DDA step counters (rc.ts:232-235) */
   uint32_t atlas;         /* 0: f32 storage, 1: f16 (the reference's rgba16 packing), 2: bf16 */
-  uint32_t pad;
+  uint32_t f32_out;       /* 1: SH and irradiance stored as f32 whatever the atlas */
 } orc_layout;
 
 /* One probe (rc.ts:157): pos.xyz + s0, nrm.xyz + view depth, grid. 48 bytes. */

@@ -414,9 +414,9 @@ static void sh_range(void *p, uint64_t b, uint64_t e) {
     for (int k = 0; k < 32; k++) sh[k] = 0.0f;
     for (int k = 0; k < 9; k++) {
       float a = k == 0 ? a_k[0] : (k < 4 ? a_k[1] : a_k[2]);
-      sh[k * 3 + 0] = round_store(cf[k].x * a, ly->atlas);
-      sh[k * 3 + 1] = round_store(cf[k].y * a, ly->atlas);
-      sh[k * 3 + 2] = round_store(cf[k].z * a, ly->atlas);
+      sh[k * 3 + 0] = round_store(cf[k].x * a, ly->f32_out ? 0u : ly->atlas);
+      sh[k * 3 + 1] = round_store(cf[k].y * a, ly->f32_out ? 0u : ly->atlas);
+      sh[k * 3 + 2] = round_store(cf[k].z * a, ly->f32_out ? 0u : ly->atlas);
     }
   }
 }
@@ -430,7 +430,7 @@ static void gather_range(void *p, uint64_t b, uint64_t e) {
   const float *F = g->frame;
   const orc_casc *L0 = &ly->c[0];
   int32_t W = (int32_t)g->width;
-  uint32_t out_fmt = ly->atlas == 0 ? 0u : 1u;
+  uint32_t out_fmt = (ly->atlas == 0 || ly->f32_out) ? 0u : 1u;
   for (int32_t py = (int32_t)b; py < (int32_t)e; py++)
     for (int32_t px = 0; px < W; px++) {
       size_t q = (size_t)py * (size_t)W + (size_t)px;

@@ -116,7 +116,7 @@ struct gi_rc {
   void *rad64 = nullptr, *irr64 = nullptr;   // FP64 reference buffers (gi_rc_merge_gather_f64), on first use
   double *sh64 = nullptr;
   bool have64 = false;
-  size_t rad_elem_bytes = 0, sh_elems = 0;
+  size_t rad_elem_bytes = 0, sh_elems = 0, sh_elem_bytes = 0, irr_elem_bytes = 0;
   bool frame_set = false, gbuf_set = false, debug_hits = false;
   uint64_t bytes = 0;
   bool timing = false;
@@ -495,6 +495,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   d.vox_scale = p->vox_scale; d.vox_offset = p->vox_offset; d.level_map = p->level_map; d.vox_skip = p->vox_skip;
   d.dda_cap = p->dda_cap; d.stats = p->stats;
   d.trace_order = 0; d.trace_rays = 1;
+  d.f32_out = p->f32_out ? 1u : 0u;
   // cascade layout (rc.ts:1027-1035)
   uint64_t probe_total = 0, ray_total = 0, dir_total = 0;
   for (uint32_t i = 0; i < p->cascades; i++) {
@@ -525,6 +526,8 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   d.probes_total = (uint32_t)probe_total;
   d.rays_total = (uint32_t)ray_total;
   r->rad_elem_bytes = atlas_elem_bytes(p->atlas);
+  r->sh_elem_bytes = p->f32_out ? 16u : r->rad_elem_bytes;
+  r->irr_elem_bytes = p->f32_out ? 16u : atlas_elem_bytes(p->atlas);
   r->sh_elems = (size_t)d.c[0].tiles_x * d.c[0].tiles_y * 8u;
   size_t npx = (size_t)W * H;
   r->ntiles = gi_raster_tiles(W, H);
@@ -536,8 +539,8 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   if ((e = dalloc(&r->frame, 160)) || (e = dalloc(&r->depth, npx)) || (e = dalloc(&r->normal, npx)) ||
       (e = dalloc(&r->tile_cnt, (size_t)r->ntiles + 1u)) || (e = dalloc(&r->tile_fill, r->ntiles)) ||
       (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
-      (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->rad_elem_bytes)) ||
-      (e = cudaMalloc(&irr, npx * atlas_elem_bytes(p->atlas))) || (e = dalloc(&counts, 96)) ||
+      (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->sh_elem_bytes)) ||
+      (e = cudaMalloc(&irr, npx * r->irr_elem_bytes)) || (e = dalloc(&counts, 96)) ||
       (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, dir_total))) {
     d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
     free_rc(r);
@@ -579,7 +582,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     return cuda_fail(e, "gi_rc_create: direction table");
   }
   r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
-             r->sh_elems * r->rad_elem_bytes + npx * atlas_elem_bytes(p->atlas) + 96 * 4;
+             r->sh_elems * r->sh_elem_bytes + npx * r->irr_elem_bytes + 96 * 4;
   *out = r;
   return GI_OK;
 }
@@ -697,7 +700,7 @@ int gi_rc_graph_capture_frame(gi_rc *r, gi_vox *v, gi_scene *sc, void *irr_out, 
   if (st == GI_OK) st = gi_rc_render_gbuffer(r, sc, stream);
   if (st == GI_OK) st = gi_solve(r, v, stream);
   if (st == GI_OK && irr_out) {
-    cudaError_t ce = cudaMemcpyAsync(irr_out, r->dev.irr, (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas),
+    cudaError_t ce = cudaMemcpyAsync(irr_out, r->dev.irr, (size_t)r->W * r->H * r->irr_elem_bytes,
                                      cudaMemcpyDefault, S(stream));
     if (ce != cudaSuccess) st = cuda_fail(ce, "gi_rc_graph_capture_frame: readback");
   }
@@ -859,7 +862,7 @@ int gi_rc_read_irradiance(gi_rc *r, float *rgba, void *stream) {
 
 int gi_rc_read_irradiance_raw(gi_rc *r, void *out, size_t bytes, void *stream) {
   if (!r || !out) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_raw: NULL argument");
-  size_t need = (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas);
+  size_t need = (size_t)r->W * r->H * r->irr_elem_bytes;
   if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_raw: %zu bytes, need %zu", bytes, need);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_raw: cudaSetDevice");
   CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_irradiance_raw: copy");
@@ -869,7 +872,7 @@ int gi_rc_read_irradiance_raw(gi_rc *r, void *out, size_t bytes, void *stream) {
 
 int gi_rc_read_irradiance_async(gi_rc *r, void *out, size_t bytes, void *stream) {
   if (!r || !out) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_async: NULL argument");
-  size_t need = (size_t)r->W * r->H * atlas_elem_bytes(r->p.atlas);
+  size_t need = (size_t)r->W * r->H * r->irr_elem_bytes;
   if (bytes < need) return fail(GI_ERR_INVALID, "gi_rc_read_irradiance_async: %zu bytes, need %zu", bytes, need);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_irradiance_async: cudaSetDevice");
   CK(cudaMemcpyAsync(out, r->dev.irr, need, cudaMemcpyDefault, S(stream)), "gi_rc_read_irradiance_async: copy");
@@ -961,7 +964,7 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
   switch (what) {
     case GI_RC_PROBES: *bytes = (size_t)r->dev.probes_total * 48u; break;
     case GI_RC_RAD: case GI_RC_RAD_TRACED: *bytes = (size_t)r->dev.rays_total * r->rad_elem_bytes; break;
-    case GI_RC_SH: *bytes = r->sh_elems * r->rad_elem_bytes; break;
+    case GI_RC_SH: *bytes = r->sh_elems * r->sh_elem_bytes; break;
     case GI_RC_DEPTH: *bytes = npx * 4u; break;
     case GI_RC_NORMAL: *bytes = npx * 8u; break;
     case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;

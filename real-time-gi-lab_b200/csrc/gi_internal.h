@@ -29,7 +29,8 @@ struct RcDev {
   CascDev c[8];
   float vox_scale, vox_offset, level_map, vox_skip;
   uint32_t dda_cap, stats, probes_total, rays_total;
-  uint32_t trace_order, trace_rays, pad_t[2];   // tuning of k_trace (gi_rc_tuning)
+  uint32_t trace_order, trace_rays;   // tuning of k_trace (gi_rc_tuning)
+  uint32_t f32_out, pad_t;            // SH and irradiance stored as f32 whatever the atlas
   const float *frame;      // 160 words (packFrame)
   const float *depth;      // W*H
   const uint2 *normal;     // W*H rgba16f

@@ -435,7 +435,18 @@ __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
   }
 #pragma unroll
   for (int q = 0; q < 8; q++)
-    Atlas<A>::store(sh, (size_t)pi * 8u + q, make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]));
+  {
+    float4 val = make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
+    if (r.f32_out) reinterpret_cast<float4 *>(r.sh)[(size_t)pi * 8u + q] = val;
+    else Atlas<A>::store(sh, (size_t)pi * 8u + q, val);
+  }
+}
+
+// SH element i as f32: stored as f32 with f32_out, else in the atlas format
+template <int A>
+__device__ __forceinline__ float4 sh_load(const RcDev &r, size_t i) {
+  if (r.f32_out) return reinterpret_cast<const float4 *>(r.sh)[i];
+  return Atlas<A>::load(reinterpret_cast<const typename Atlas<A>::T *>(r.sh), i);
 }
 
 // gatherScreen (rc.ts:929-954), evalSH (rc.ts:819-829) for one pixel.  Src supplies the 2x2 cascade-0 probes around
@@ -487,7 +498,7 @@ __device__ __forceinline__ void gather_pixel(const RcDev &r, uint32_t px, uint32
     }
     if (ws > 0.0f) res = e / ws;
   }
-  if (A == GI_ATLAS_F32) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
+  if (A == GI_ATLAS_F32 || r.f32_out) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
   else reinterpret_cast<uint2 *>(r.irr)[q] = make_uint2((uint32_t)f2h(res.x) | ((uint32_t)f2h(res.y) << 16),
                                                        (uint32_t)f2h(res.z) | ((uint32_t)f2h(alpha) << 16));
 }
@@ -496,9 +507,7 @@ template <int A>
 struct GlobalProbes {   // each lane reads its own probes
   const RcDev &r;
   __device__ __forceinline__ ProbeDev probe(uint32_t, uint32_t qi) const { return r.probes[r.c[0].probe_off + qi]; }
-  __device__ __forceinline__ float4 coef(uint32_t, uint32_t qi, int j) const {
-    return Atlas<A>::load(reinterpret_cast<const typename Atlas<A>::T *>(r.sh), (size_t)qi * 8u + j);
-  }
+  __device__ __forceinline__ float4 coef(uint32_t, uint32_t qi, int j) const { return sh_load<A>(r, (size_t)qi * 8u + j); }
 };
 
 struct SharedProbes {   // the warp's four probes, staged in shared memory (k = the 2x2 corner)
@@ -551,7 +560,7 @@ __global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
     uint32_t k = lane >> 3, j = lane & 7u;
     int qx = iclamp(bx0 + (int)(k & 1u), 0, (int)L.tiles_x - 1), qy = iclamp(by0 + (int)(k >> 1), 0, (int)L.tiles_y - 1);
     uint32_t qi = (uint32_t)qy * L.tiles_x + (uint32_t)qx;
-    s_coef[warp][lane] = Atlas<A>::load(reinterpret_cast<const typename Atlas<A>::T *>(r.sh), (size_t)qi * 8u + j);
+    s_coef[warp][lane] = sh_load<A>(r, (size_t)qi * 8u + j);
     if (lane < 8u) {
       uint32_t kk = lane >> 1;
       int qx2 = iclamp(bx0 + (int)(kk & 1u), 0, (int)L.tiles_x - 1), qy2 = iclamp(by0 + (int)(kk >> 1), 0, (int)L.tiles_y - 1);
@@ -567,7 +576,7 @@ __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
   grid_dep_wait();
   size_t n = (size_t)r.width * r.height;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    if (r.atlas == GI_ATLAS_F32) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
+    if (r.atlas == GI_ATLAS_F32 || r.f32_out) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
     else {
       uint2 u = reinterpret_cast<const uint2 *>(r.irr)[i];
       dst[i] = make_float4(h2f(u.x & 0xffffu), h2f(u.x >> 16), h2f(u.y & 0xffffu), h2f(u.y >> 16));

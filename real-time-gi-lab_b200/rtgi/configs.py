@@ -2,8 +2,9 @@
 VoxParams / DEFAULT_VOX / voxParams, src/runner/configs.ts:47-73 parseConfig).
 
 Same names, defaults and error behaviour: unknown config tokens and unknown voxel parameters raise.  This build adds
-three RcParams fields and their tokens: ``ddaCap`` (token ``dda<N>``; the reference hard-codes 1024 steps,
-voxel.ts:142), ``atlas`` (tokens ``f32``/``f16``/``bf16``; the reference stores f16) and ``stats``.
+four RcParams fields and their tokens: ``ddaCap`` (token ``dda<N>``; the reference hard-codes 1024 steps,
+voxel.ts:142), ``atlas`` (tokens ``f32``/``f16``/``bf16``; the reference stores f16), ``f32Out`` (token ``f32out``:
+SH and irradiance kept in f32 whatever the atlas) and ``stats``.
 """
 from __future__ import annotations
 
@@ -47,6 +48,7 @@ class RcParams:
     # additions of this build
     ddaCap: int = 1024
     atlas: str = "f16"
+    f32Out: bool = False
 
 
 DEFAULT_PARAMS = RcParams()
@@ -80,6 +82,7 @@ def parse_config(name: str, overrides: Optional[dict] = None) -> RcParams:
         elif t == "obj": p.objects = True
         elif re.fullmatch(r"dda\d+", t): p.ddaCap = int(t[3:])
         elif t in ("f32", "f16", "bf16"): p.atlas = t
+        elif t == "f32out": p.f32Out = True
         else: raise ValueError(f"unknown config token {t} in {name}")
     return p
 
@@ -124,4 +127,5 @@ def cascade_layout(p: RcParams, width: int, height: int) -> dict:
     atlas = {"f32": 0, "f16": 1, "bf16": 2}[p.atlas]
     return {"cascades": p.cascades, "casc": casc, "vox_scale": p.voxScale, "vox_offset": p.voxOffset,
             "level_map": p.levelMap, "vox_skip": p.voxSkip, "dda_cap": p.ddaCap, "stats": p.stats, "atlas": atlas,
+            "f32_out": 1 if p.f32Out else 0,
             "probes_total": probe_off, "rays_total": rad_off}

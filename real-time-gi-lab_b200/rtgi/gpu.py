@@ -182,6 +182,7 @@ class Rc:
         p.cascades, p.P, p.k_interval = params.cascades, params.P, params.kInterval
         p.vox_scale, p.vox_offset, p.vox_skip, p.level_map = params.voxScale, params.voxOffset, params.voxSkip, params.levelMap
         p.res_cap, p.dda_cap, p.stats, p.atlas = params.resCap, params.ddaCap, params.stats, ATLAS_CODES[params.atlas]
+        p.f32_out = 1 if params.f32Out else 0
         h = _P()
         _lib.call("gi_rc_create", ctx.handle, C.byref(p), width, height, C.byref(h))
         self.handle = h
@@ -260,7 +261,7 @@ class Rc:
         _lib.call("gi_rc_read_irradiance_async", self.handle, ptr, self.irr_bytes(), _stream(stream))
 
     def irr_bytes(self) -> int:
-        return self.width * self.height * (16 if self.params.atlas == "f32" else 8)
+        return self.width * self.height * (16 if self.params.atlas == "f32" or self.params.f32Out else 8)
 
     def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None):
         """G-buffer from host pointers (pinned memory makes the copies asynchronous)."""
@@ -310,7 +311,7 @@ class Rc:
     def read_atlas(self, what: int = _lib.GI_RC_RAD, stream=None) -> np.ndarray:
         """The atlas (or SH) as f32 values, (n, 4)."""
         raw = self.read_buffer(what, stream)
-        if self.params.atlas == "f32":
+        if self.params.atlas == "f32" or (what == _lib.GI_RC_SH and self.params.f32Out):
             return raw.view(np.float32).reshape(-1, 4)
         if self.params.atlas == "f16":
             return raw.view(np.float16).astype(np.float32).reshape(-1, 4)

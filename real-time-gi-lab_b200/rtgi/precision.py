@@ -1,5 +1,7 @@
 """Atlas precision study: the irradiance of f32, f16 and bf16 cascade atlases against the FP64 reference of the merge
 and gather (gi_rc_merge_gather_f64), over frames of a scene with moving boxes whose clipmap is rebuilt every frame.
+Modes "f16"/"bf16" also store the SH and the irradiance in 16 bits (the reference's f16 storage); "-f32out" keeps
+those two in f32, so only the atlas and the merge are in 16 bits.
 
 The reference stores its atlases, SH and irradiance in f16 (rc.ts:309-310, 768-773, 1073) with f32 arithmetic; this
 study states what that storage costs.  All atlas modes trace the same intervals with the same f32 arithmetic, so the
@@ -26,7 +28,8 @@ def precision_scene(seed: int = 0, n_boxes: int = 64):
 
 
 def colonnade_params(atlas: str, width: int = 1920, height: int = 1080):
-    """The colonnade workload's clipmap (4 levels x 128^3 voxels from 0.1 m) and cascades (5, DDA cap 256)."""
+    """The colonnade workload's clipmap (4 levels x 128^3 voxels from 0.1 m) and cascades (5, DDA cap 256).  atlas: a
+    storage mode, optionally with "-f32out" (SH and irradiance kept in f32)."""
     p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": 5})
     v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
     return p, v
@@ -85,7 +88,8 @@ class ErrorStats:
                 "values": self.n, "frames": self.frames, "alpha_mismatch": self.alpha_mismatch}
 
 
-def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0, atlases: Sequence[str] = ("f32", "f16", "bf16"),
+def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
+        atlases: Sequence[str] = ("f32", "f16", "bf16", "f16-f32out", "bf16-f32out"),
         seed: int = 0, n_boxes: int = 64, width: int = 1920, height: int = 1080, device: int = 0) -> dict:
     """The study: per frame, pose the boxes, rebuild the clipmap, solve the cascades in every atlas mode, run the FP64
     merge and gather from the f32 mode's trace, and accumulate each mode's irradiance error.  Also times each mode's
@@ -112,8 +116,9 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0, atlases: Se
             rc.set_frame(F, stream)
         vox.update(s.camera.eye)
         ref = torch.empty((height, width, 4), dtype=torch.float64, device=dev)
-        outs = {a: torch.empty((height, width, 4), dtype=torch.float32 if a == "f32" else torch.float16, device=dev)
-                for a in rcs}
+        outs = {a: torch.empty((height, width, 4), device=dev,
+                               dtype=torch.float32 if rc.irr_bytes() == 16 * width * height else torch.float16)
+                for a, rc in rcs.items()}
         stats = {a: ErrorStats(torch, dev) for a in rcs}
         times = {a: [] for a in rcs}
         counters = []

@@ -186,3 +186,10 @@ def test_scenes_shapes():
     # Builder quads: face normal = normalize(cross(b - a, c - a)) per vertex
     n = s.normals[s.tri[0, 0]]
     assert abs(np.linalg.norm(n) - 1) < 1e-6
+
+
+def test_f32out_token_and_layout():
+    p = configs.parse_config("screen-8-voxel-f16-f32out-dda256", {"cascades": 3})
+    assert p.atlas == "f16" and p.f32Out
+    assert configs.cascade_layout(p, 64, 32)["f32_out"] == 1
+    assert configs.cascade_layout(configs.parse_config("screen-8-voxel-f16"), 64, 32)["f32_out"] == 0

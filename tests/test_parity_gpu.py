@@ -68,6 +68,7 @@ def run_oracle(case, depth, normal):
 
 
 CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_cases.leak,
+         "room_lit_f32out": lambda: gi_cases.room_lit("f16-f32out"),
          "overflow": gi_cases.overflow, "config1": gi_cases.config1}
 
 

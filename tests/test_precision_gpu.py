@@ -68,10 +68,12 @@ def test_precision_study_small(ctx):
     """Three frames of the study at 480x270: every mode valid where the reference is, errors ordered by precision."""
     r = precision.run(ctx, frames=3, width=480, height=270)
     a = r["atlases"]
-    for m in ("f32", "f16", "bf16"):
+    for m in ("f32", "f16", "bf16", "f16-f32out", "bf16-f32out"):
         assert a[m]["alpha_mismatch"] == 0
         assert a[m]["values"] > 0
     assert a["f32"]["rel_l2"] < 1e-5
     assert a["f32"]["rel_l2"] < a["f16"]["rel_l2"] < a["bf16"]["rel_l2"]
     assert a["f16"]["rel_l2"] < 2e-3
     assert a["bf16"]["rel_l2"] < 2e-2
+    # SH and irradiance in f32: only the atlas and the merge round to 16 bits
+    assert a["f16-f32out"]["rel_l2"] < a["f16"]["rel_l2"] and a["bf16-f32out"]["rel_l2"] < a["bf16"]["rel_l2"]
