@@ -74,6 +74,50 @@ __device__ __forceinline__ i3 range_cell(Range r, int q) {
   return mki(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y));
 }
 
+// Warp-balanced small work: every lane holds one (triangle, level) item of n <= 8 cells (or bricks); the warp's cells
+// are dealt out 32 at a time, so a lane with one cell does not idle while another works through eight.  The owner of
+// cell g is the first lane whose inclusive prefix exceeds g (a 5-step search over the prefixes with shuffles); its
+// triangle, range and count come over with shuffles.  Each (item, cell) pair is visited once, as in the per-lane loop.
+struct SmallItem { Tri T; uint32_t t; Range r; int n; };
+
+__device__ __forceinline__ SmallItem shfl_item(const SmallItem &x, int src) {
+  SmallItem y;
+  y.T.a = mk(__shfl_sync(0xffffffffu, x.T.a.x, src), __shfl_sync(0xffffffffu, x.T.a.y, src), __shfl_sync(0xffffffffu, x.T.a.z, src));
+  y.T.b = mk(__shfl_sync(0xffffffffu, x.T.b.x, src), __shfl_sync(0xffffffffu, x.T.b.y, src), __shfl_sync(0xffffffffu, x.T.b.z, src));
+  y.T.c = mk(__shfl_sync(0xffffffffu, x.T.c.x, src), __shfl_sync(0xffffffffu, x.T.c.y, src), __shfl_sync(0xffffffffu, x.T.c.z, src));
+  y.T.idx = make_uint4(0u, 0u, 0u, __shfl_sync(0xffffffffu, x.T.idx.w, src));
+  y.t = __shfl_sync(0xffffffffu, x.t, src);
+  y.r.lo = mki(__shfl_sync(0xffffffffu, x.r.lo.x, src), __shfl_sync(0xffffffffu, x.r.lo.y, src), __shfl_sync(0xffffffffu, x.r.lo.z, src));
+  y.r.n = mki(__shfl_sync(0xffffffffu, x.r.n.x, src), __shfl_sync(0xffffffffu, x.r.n.y, src), 0);
+  y.n = __shfl_sync(0xffffffffu, x.n, src);
+  return y;
+}
+
+// Calls f(item, q) for every lane's item and q < item.n (mine = the lane's count, 0 for none); all lanes call it.
+template <class F>
+__device__ __forceinline__ void warp_deal(const SmallItem &it, uint32_t mine, F f) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t incl = mine;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  for (uint32_t base = 0; base < total; base += 32u) {
+    uint32_t g = base + lane, o = 0;
+#pragma unroll
+    for (uint32_t bit = 16; bit >= 1; bit >>= 1) {
+      uint32_t val = __shfl_sync(0xffffffffu, incl, (int)(o + bit - 1u));
+      if (val <= g) o += bit;
+    }
+    o = min(o, 31u);
+    SmallItem w = shfl_item(it, (int)o);
+    uint32_t start = __shfl_sync(0xffffffffu, incl - mine, (int)o);
+    if (g < total) f(w, (int)(g - start));
+  }
+}
+
 // markBrick (voxel.ts:347): read before the atomic
 __device__ __forceinline__ void mark_brick(const VoxDev &v, uint32_t i) {
   if (v.ptr[i] == GI_EMPTY) atomicMin(&v.ptr[i], GI_MARK);
@@ -107,10 +151,13 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   bool live = t < s.ntris;
   Tri T;
+  T.a = T.b = T.c = mk(0.0f, 0.0f, 0.0f);
+  T.idx = make_uint4(0u, 0u, 0u, 0u);
   if (live) T = load_tri(s, t);
   for (uint32_t L = 0; L < v.levels; L++) {
     bool big = false;
     Range r;
+    r.lo = r.n = mki(0, 0, 0);
     int n = 0;
     if (live) {
       r = vox_range(v, T, L, true);
@@ -121,9 +168,12 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
     uint32_t k = warp_append(&v.hdr[24 + L], big);
     if (big) {
       if (k < v.big_cap) v.big[(8u + L) * v.big_cap + k] = t; else atomicAdd(&v.hdr[3], 1u);
-    } else if (n > 0) {
-      for (uint32_t j = 0; j < (uint32_t)n; j++) mark_one(v, T, L, r, (uint32_t)n, j);
     }
+    SmallItem it;
+    it.T = T; it.t = t; it.r = r; it.n = n;
+    warp_deal(it, (!big && n > 0) ? (uint32_t)n : 0u, [&](const SmallItem &w, int j) {
+      mark_one(v, w.T, L, w.r, (uint32_t)w.n, (uint32_t)j);
+    });
   }
 }
 
@@ -320,6 +370,7 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
 }
 
 // voxelizeOne (voxel.ts:476-490)
+
 __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t t, uint32_t L,
                                              i3 c, bool single, uint32_t brick_overflow) {
   if (finer_built(v, L, c, brick_overflow)) return;
@@ -347,10 +398,13 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
   bool live = t < s.ntris;
   uint32_t bo = v.hdr[2];
   Tri T;
+  T.a = T.b = T.c = mk(0.0f, 0.0f, 0.0f);
+  T.idx = make_uint4(0u, 0u, 0u, 0u);
   if (live) T = load_tri(s, t);
   for (uint32_t L = 0; L < v.levels; L++) {
     bool big = false;
     Range r;
+    r.lo = r.n = mki(0, 0, 0);
     int n = 0;
     if (live) {
       r = vox_range(v, T, L, false);
@@ -362,9 +416,12 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
     uint32_t k = warp_append(&v.hdr[16 + L], big);
     if (big) {
       if (k < v.big_cap) v.big[L * v.big_cap + k] = t; else atomicAdd(&v.hdr[3], 1u);
-    } else if (n > 0) {
-      for (int q = 0; q < n; q++) voxelize_one(v, s, T, t, L, range_cell(r, q), n == 1, bo);
     }
+    SmallItem it;
+    it.T = T; it.t = t; it.r = r; it.n = n;
+    warp_deal(it, (!big && n > 0) ? (uint32_t)n : 0u, [&](const SmallItem &w, int q) {
+      voxelize_one(v, s, w.T, w.t, L, range_cell(w.r, q), w.n == 1, bo);
+    });
   }
 }
 
