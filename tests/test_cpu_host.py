@@ -193,3 +193,16 @@ def test_f32out_token_and_layout():
     assert p.atlas == "f16" and p.f32Out
     assert configs.cascade_layout(p, 64, 32)["f32_out"] == 1
     assert configs.cascade_layout(configs.parse_config("screen-8-voxel-f16"), 64, 32)["f32_out"] == 0
+
+
+def test_quotient_shortcuts_of_the_shading_are_exact():
+    """The hit shading replaces two f32 divisions by f64 products rounded to f32: k / 32767 for every 16-bit k (the
+    snorm normal) and a / pi for the 256 albedo bytes a = k / 255.  Both equal the IEEE f32 quotients everywhere."""
+    x = np.arange(-32768, 32768).astype(np.float32)
+    q = x / np.float32(32767)
+    alt = (x.astype(np.float64) * (1.0 / 32767.0)).astype(np.float32)
+    assert np.array_equal(q.view(np.uint32), alt.view(np.uint32))
+    a = np.arange(256).astype(np.float32) / np.float32(255)
+    pi = np.float32(3.14159265)
+    assert np.array_equal((a / pi).view(np.uint32),
+                          (a.astype(np.float64) * (1.0 / np.float64(pi))).astype(np.float32).view(np.uint32))
