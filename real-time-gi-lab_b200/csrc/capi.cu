@@ -350,11 +350,12 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   vox_derived(d);
   d.citem_cap = VOX_CITEM_CAP;
   uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
-  uint32_t scan_words = (uint32_t)((nptr + 2047u) / 2048u);
+  uint32_t scan_words = (uint32_t)((nptr + 255u) / 256u);   // block sums of the brick allocation, 256 entries each
   uint32_t vscan = (p->max_bricks + 255u) / 256u;
   if (vscan > scan_words) scan_words = vscan;
   uint32_t cscan = 8u * d.big_cap / 256u;   // chunk-prefix block sums of the voxBits big lists
   if (cscan > scan_words) scan_words = cscan;
+  d.scan_cap = scan_words;
   cudaError_t e;
   if ((e = dalloc(&d.hdr, GI_HDR)) || (e = dalloc(&d.ptr, nptr)) || (e = dalloc(&d.occ, (size_t)p->max_bricks * 16u)) ||
       (e = dalloc(&d.base, p->max_bricks)) || (e = dalloc(&d.code, p->max_bricks)) ||

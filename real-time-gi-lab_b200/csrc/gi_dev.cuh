@@ -160,7 +160,7 @@ struct VoxDev {
   float v0;
   uint32_t levels, G, max_bricks, max_voxels, big_cap;
   uint32_t chunk_log2, blocks;   // tuning: cells per big-triangle work item (log2), resident blocks per SM
-  uint32_t citem_cap, pad_ci;    // entries of citem (0: no table)
+  uint32_t citem_cap, scan_cap;  // entries of citem (0: no table); words of scan
   float vs[8];         // voxel size per level, ldexpf(v0, L) (vox_derived)
   int32_t lim_vox[8], lim_brick[8];   // voxRange's limit f2i(G * size * 8 / cell), voxel and brick cells (vox_derived)
   int32_t origin[8][4];

@@ -118,6 +118,7 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   v.chunk_log2 = 7;   // the default gi_vox_tuning
   v.blocks = 8;
   vox_derived(v);
+  v.scan_cap = NOALLOC_SCAN_WORDS;
   for (uint32_t L = 0; L < p->levels; L++) {
     double bs = p->v0 * ldexp(1.0, (int)L) * 8.0;   // writeUniform (voxel.ts:873-874)
     for (int a = 0; a < 3; a++) {

@@ -233,7 +233,8 @@ __global__ void k_mark_parents(VoxDev v) {
 
 // ---- ordered allocation of the marked bricks (countMarks / scanMarks / allocBricks, voxel.ts:411-470) ---------------
 // Order space o in [0, levels * G^3): level levels-1 first, pointer index within a level.
-constexpr uint32_t ALLOC_CHUNK = 2048;   // entries per block (256 threads x 8)
+// The ordered brick allocation takes 256 * k pointer entries per block, k per thread: k = 1 unless the block sums
+// would not fit the scan buffer (alloc_per_thread)
 
 __device__ __forceinline__ uint32_t order_to_ptr(uint32_t o, uint32_t per, uint32_t NL) {
   return (NL - 1u - o / per) * per + o % per;
@@ -271,12 +272,12 @@ __device__ __forceinline__ uint32_t block_scan_256(uint32_t x, uint32_t *total) 
 }
 
 // Per block: the number of marked entries of its chunk of the order space.
-__global__ void __launch_bounds__(256) k_count_marks(VoxDev v) {
+__global__ void __launch_bounds__(256) k_count_marks(VoxDev v, uint32_t kpt) {
   grid_dep_wait();
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per;
-  uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
+  uint32_t o0 = blockIdx.x * 256u * kpt;
   uint32_t c = 0;
-  for (uint32_t k = threadIdx.x; k < ALLOC_CHUNK; k += 256u) {
+  for (uint32_t k = threadIdx.x; k < 256u * kpt; k += 256u) {
     uint32_t o = o0 + k;
     if (o < n && v.ptr[order_to_ptr(o, per, NL)] == GI_MARK) c++;
   }
@@ -325,25 +326,23 @@ __global__ void __launch_bounds__(256) k_scan_chunks(VoxDev v) {
 }
 
 // allocBricks (voxel.ts:450-470) in the fixed order.
-__global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v) {
+__global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v, uint32_t kpt) {
   grid_dep_wait();
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per, G = v.G;
-  uint32_t o0 = blockIdx.x * ALLOC_CHUNK;
-  // each thread owns 8 consecutive entries of the chunk
+  uint32_t o0 = blockIdx.x * 256u * kpt;
+  // each thread owns kpt (<= 32) consecutive entries of the chunk
   uint32_t flags = 0, c = 0;
-#pragma unroll
-  for (uint32_t k = 0; k < 8u; k++) {
-    uint32_t o = o0 + threadIdx.x * 8u + k;
+  for (uint32_t k = 0; k < kpt; k++) {
+    uint32_t o = o0 + threadIdx.x * kpt + k;
     bool m = o < n && v.ptr[order_to_ptr(o, per, NL)] == GI_MARK;
     flags |= (m ? 1u : 0u) << k;
     c += m ? 1u : 0u;
   }
   uint32_t tot;
   uint32_t ex = block_scan_256(c, &tot) + v.scan[blockIdx.x];
-#pragma unroll
-  for (uint32_t k = 0; k < 8u; k++) {
+  for (uint32_t k = 0; k < kpt; k++) {
     if (!((flags >> k) & 1u)) continue;
-    uint32_t o = o0 + threadIdx.x * 8u + k;
+    uint32_t o = o0 + threadIdx.x * kpt + k;
     uint32_t i = order_to_ptr(o, per, NL);
     uint32_t idx = ex++;
     if (idx >= v.max_bricks) { v.ptr[i] = GI_DROP; atomicAdd(&v.hdr[2], 1u); continue; }
@@ -739,10 +738,12 @@ cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_
   if (tb) GI_TRY(gi_launch(k_mark_bricks, tb, 256, st, v, s));
   GI_TRY(gi_launch(k_mark_bricks_big, persist, 256, st, v, s));
   if (v.levels > 1) GI_TRY(gi_launch(k_mark_parents, min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, st, v));
-  uint32_t ab = (nptr + ALLOC_CHUNK - 1u) / ALLOC_CHUNK;
-  GI_TRY(gi_launch(k_count_marks, ab, 256, st, v));
+  uint32_t kpt = 1;
+  while ((nptr + 256u * kpt - 1u) / (256u * kpt) > v.scan_cap && kpt < 32u) kpt *= 2u;
+  uint32_t ab = (nptr + 256u * kpt - 1u) / (256u * kpt);
+  GI_TRY(gi_launch(k_count_marks, ab, 256, st, v, kpt));
   GI_TRY(gi_launch(k_scan_sums, 1, 256, st, v.scan, ab, v.hdr));
-  GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v));
+  GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v, kpt));
   GI_TRY(gi_launch(k_init_bricks, persist, 256, st, v));
   if (tb) GI_TRY(gi_launch(k_vox_bits, tb, 256, st, v, s));
   GI_TRY(gi_launch(k_count_chunks, persist, 256, st, v, s));
