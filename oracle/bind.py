@@ -51,6 +51,8 @@ def lib():
         _lib.orc_tri_box.restype = C.c_int
         _lib.orc_round_log2.argtypes = [C.c_float]
         _lib.orc_round_log2.restype = C.c_uint32
+        _lib.orc_gi_exp.argtypes = [C.c_float]
+        _lib.orc_gi_exp.restype = C.c_float
     return _lib
 
 

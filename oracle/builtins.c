@@ -71,6 +71,9 @@ uint32_t orc_round_log2(float x) {
   return (uint32_t)(mm >= 0.5 ? e : e - 1);
 }
 
+/* The merge and gather weights' e^x (orc_math.h gi_exp), for its accuracy test. */
+float orc_gi_exp(float x) { return gi_exp(x); }
+
 /* Akenine-Moller triangle / box overlap, voxel.ts:231-248, box at c with half size h. */
 static int axis_test(v3 a, v3 v0, v3 v1, v3 v2, v3 h) {
   float p0 = dot(v0, a), p1 = dot(v1, a), p2 = dot(v2, a);

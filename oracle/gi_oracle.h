@@ -142,6 +142,7 @@ uint16_t orc_f32_to_bf16(float x);
 float orc_bf16_to_f32(uint16_t h);
 int orc_tri_box(const float c[3], const float h[3], const float a[3], const float b[3], const float cc[3]);
 uint32_t orc_round_log2(float x);
+float orc_gi_exp(float x);
 
 #ifdef __cplusplus
 }

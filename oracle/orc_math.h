@@ -18,6 +18,9 @@ static inline v3 divv(v3 a, v3 b) { return V(a.x / b.x, a.y / b.y, a.z / b.z); }
 static inline v3 muls(v3 a, float s) { return V(a.x * s, a.y * s, a.z * s); }
 static inline v3 divs(v3 a, float s) { return V(a.x / s, a.y / s, a.z / s); }
 static inline v3 adds(v3 a, float s) { return V(a.x + s, a.y + s, a.z + s); }
+/* acc + a * s per component as one fused multiply-add (the definition chosen for the weighted sums of the merge,
+ * the SH projection and the gather; the CUDA path uses the same fmaf) */
+static inline v3 fmas(v3 a, float s, v3 acc) { return V(fmaf(a.x, s, acc.x), fmaf(a.y, s, acc.y), fmaf(a.z, s, acc.z)); }
 static inline v3 neg(v3 a) { return V(-a.x, -a.y, -a.z); }
 static inline float dot(v3 a, v3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 static inline v3 cross(v3 a, v3 b) { return V(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
@@ -59,7 +62,8 @@ static inline float exp2_(float x) {
   return exp2f(x);
 }
 /* e^x of the merge and gather weights: Cody & Waite's two-constant reduction x = k ln2 + r (|r| <= ln2/2, the split
- * of ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form, e^x = 2^k e^r.  Relative error
+ * of ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form with fused multiply-adds,
+ * e^x = 2^k e^r.  Relative error
  * below 3e-7 on [-80, 88]; below -80 the result is 0.  The CUDA path evaluates the same f32 sequence. */
 static inline float gi_exp(float x) {
   if (x != x) return x;
@@ -68,13 +72,13 @@ static inline float gi_exp(float x) {
   float k = rintf(x * 0x1.715476p+0f);
   float r = (x - k * 0x1.62e4p-1f) - k * 0x1.7f7d1cp-20f;
   float p = 0x1.a01a02p-13f;
-  p = p * r + 0x1.6c16c2p-10f;
-  p = p * r + 0x1.111112p-7f;
-  p = p * r + 0x1.555556p-5f;
-  p = p * r + 0x1.555556p-3f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
+  p = fmaf(p, r, 0x1.6c16c2p-10f);
+  p = fmaf(p, r, 0x1.111112p-7f);
+  p = fmaf(p, r, 0x1.555556p-5f);
+  p = fmaf(p, r, 0x1.555556p-3f);
+  p = fmaf(p, r, 0.5f);
+  p = fmaf(p, r, 1.0f);
+  p = fmaf(p, r, 1.0f);
   return ldexpf(p, (int)k);
 }
 #endif

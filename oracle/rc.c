@@ -380,13 +380,13 @@ static void merge_range(void *p, uint64_t b, uint64_t e) {
           float fwx = ox == 1 ? fx : 1.0f - fx, fwy = oy == 1 ? fy : 1.0f - fy;
           float rel = fabsf(qp->nrm[3] - pr->nrm[3]) / pr->nrm[3];
           float w = (fwx * fwy + 1e-4f) * (gi_exp(-20.0f * rel) + 1e-4f);
-          acc = add(acc, muls(upper_avg(ly, o->rad, c + 1u, qi, u0, v0, L->res), w));
+          acc = fmas(upper_avg(ly, o->rad, c + 1u, qi, u0, v0, L->res), w, acc);
           ws += w;
         }
         if (ws > 0.0f) up = divs(acc, ws);
       }
     }
-    v3 m = add(V(rv[0], rv[1], rv[2]), muls(up, rv[3]));
+    v3 m = fmas(up, rv[3], V(rv[0], rv[1], rv[2]));
     rv[0] = round_store(m.x, ly->atlas); rv[1] = round_store(m.y, ly->atlas); rv[2] = round_store(m.z, ly->atlas);
     rv[3] = round_store(1.0f, ly->atlas);
   }
@@ -408,7 +408,7 @@ static void sh_range(void *p, uint64_t b, uint64_t e) {
       v3 r = muls(V(rp[0], rp[1], rp[2]), F[F_OMEGA + d]);
       float y[9];
       sh_basis(dir_of(d, 4u), y);
-      for (int k = 0; k < 9; k++) cf[k] = add(cf[k], muls(r, y[k]));
+      for (int k = 0; k < 9; k++) cf[k] = fmas(r, y[k], cf[k]);
     }
     float *sh = o->sh + 32u * pi;
     for (int k = 0; k < 32; k++) sh[k] = 0.0f;
@@ -460,9 +460,9 @@ static void gather_range(void *p, uint64_t b, uint64_t e) {
         /* evalSH (rc.ts:819-829) */
         const float *sh = o->sh + 32u * qi;
         v3 es = V(0.0f, 0.0f, 0.0f);
-        for (int k2 = 0; k2 < 9; k2++) es = add(es, muls(V(sh[3 * k2], sh[3 * k2 + 1], sh[3 * k2 + 2]), y[k2]));
+        for (int k2 = 0; k2 < 9; k2++) es = fmas(V(sh[3 * k2], sh[3 * k2 + 1], sh[3 * k2 + 2]), y[k2], es);
         es = vmax(es, V(0.0f, 0.0f, 0.0f));
-        acc = add(acc, muls(es, w));
+        acc = fmas(es, w, acc);
         ws += w;
       }
       v3 r = ws > 0.0f ? divs(acc, ws) : V(0.0f, 0.0f, 0.0f);

@@ -67,9 +67,17 @@ __device__ __forceinline__ int round_log2(float x) {
 }
 
 // e^x of the merge and gather weights: Cody & Waite's two-constant reduction x = k ln2 + r (|r| <= ln2/2, the split of
-// ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form, e^x = 2^k e^r.  Relative error below
-// 3e-7 on [-80, 88]; below -80 the result is 0.  The oracle evaluates the same f32 sequence (no fused multiply-add on
-// either side), so the weights agree bit for bit.
+// ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form with fused multiply-adds,
+// e^x = 2^k e^r.  Relative error below 3e-7 on [-80, 88]; below -80 the result is 0.  The oracle evaluates the same f32
+// sequence (the same fmaf steps), so the weights agree bit for bit.
+__device__ __forceinline__ float gi_exp(float x);
+
+// acc + a * s per component as one fused multiply-add (the weighted sums of the merge, the SH projection and the
+// gather; the oracle uses the same fmaf)
+__device__ __forceinline__ f3 fma3(f3 a, float s, f3 acc) {
+  return mk(__fmaf_rn(a.x, s, acc.x), __fmaf_rn(a.y, s, acc.y), __fmaf_rn(a.z, s, acc.z));
+}
+
 __device__ __forceinline__ float gi_exp(float x) {
   if (x != x) return x;
   if (x < -80.0f) return 0.0f;
@@ -77,14 +85,15 @@ __device__ __forceinline__ float gi_exp(float x) {
   float k = rintf(x * 0x1.715476p+0f);
   float r = (x - k * 0x1.62e4p-1f) - k * 0x1.7f7d1cp-20f;
   float p = 0x1.a01a02p-13f;
-  p = p * r + 0x1.6c16c2p-10f;
-  p = p * r + 0x1.111112p-7f;
-  p = p * r + 0x1.555556p-5f;
-  p = p * r + 0x1.555556p-3f;
-  p = p * r + 0.5f;
-  p = p * r + 1.0f;
-  p = p * r + 1.0f;
-  return ldexpf(p, (int)k);
+  p = __fmaf_rn(p, r, 0x1.6c16c2p-10f);
+  p = __fmaf_rn(p, r, 0x1.111112p-7f);
+  p = __fmaf_rn(p, r, 0x1.555556p-5f);
+  p = __fmaf_rn(p, r, 0x1.555556p-3f);
+  p = __fmaf_rn(p, r, 0.5f);
+  p = __fmaf_rn(p, r, 1.0f);
+  p = __fmaf_rn(p, r, 1.0f);
+  // 2^k as a float: k is in [-116, 127] here and p in (0.7, 1.42), so the product is normal and exact (= ldexpf)
+  return p * __int_as_float((int)(k + 127.0f) << 23);
 }
 
 // ---- WGSL packing builtins (public WGSL spec formulas) -------------------------------------------------------------

@@ -390,13 +390,13 @@ __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4
             float4 p = up_avg[((size_t)qi[k] << L.dirs_log2) + v * L.res + u];
             ua = mk(p.x, p.y, p.z);
           }
-          acc = acc + ua * w[k];
+          acc = fma3(ua, w[k], acc);
           ws += w[k];
         }
         if (ws > 0.0f) up = acc / ws;
       }
     }
-    f3 m = mk(vv.x, vv.y, vv.z) + up * vv.w;
+    f3 m = fma3(up, vv.w, mk(vv.x, vv.y, vv.z));
     Atlas<A>::store(rad, idx, make_float4(m.x, m.y, m.z, 1.0f));
     if (my_avg) qsum = qsum + mk(Atlas<A>::round(m.x), Atlas<A>::round(m.y), Atlas<A>::round(m.z));
   }
@@ -432,7 +432,7 @@ __global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
     float y[9];
     sh_basis(dir_of(d, 4u), y);
 #pragma unroll
-    for (int k = 0; k < 9; k++) cf[k] = cf[k] + rr * y[k];
+    for (int k = 0; k < 9; k++) cf[k] = fma3(rr, y[k], cf[k]);
   }
   float vals[32];
 #pragma unroll
@@ -501,9 +501,9 @@ __device__ __forceinline__ void gather_pixel(const RcDev &r, uint32_t px, uint32
       }
       f3 es = mk(0.0f, 0.0f, 0.0f);
 #pragma unroll
-      for (int k2 = 0; k2 < 9; k2++) es = es + mk(v[3 * k2], v[3 * k2 + 1], v[3 * k2 + 2]) * y[k2];
+      for (int k2 = 0; k2 < 9; k2++) es = fma3(mk(v[3 * k2], v[3 * k2 + 1], v[3 * k2 + 2]), y[k2], es);
       es = vmax(es, mk(0.0f, 0.0f, 0.0f));
-      e = e + es * w;
+      e = fma3(es, w, e);
       ws += w;
     }
     if (ws > 0.0f) res = e / ws;

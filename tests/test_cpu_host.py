@@ -206,3 +206,15 @@ def test_quotient_shortcuts_of_the_shading_are_exact():
     pi = np.float32(3.14159265)
     assert np.array_equal((a / pi).view(np.uint32),
                           (a.astype(np.float64) * (1.0 / np.float64(pi))).astype(np.float32).view(np.uint32))
+
+
+def test_gi_exp_accuracy():
+    """The weights' e^x (Cody-Waite reduction, degree-7 Horner polynomial with fused multiply-adds): relative error
+    against the exact exponential below 3e-7 on [-80, 0] (the range -20 rel takes) and 0 below -80."""
+    lib = bind.lib()
+    xs = np.concatenate([np.linspace(-80.0, 0.0, 20001), -np.logspace(-8, 0, 2001)]).astype(np.float32)
+    got = np.array([lib.orc_gi_exp(float(x)) for x in xs], np.float64)
+    exact = np.exp(xs.astype(np.float64))
+    rel = np.abs(got - exact) / exact
+    assert rel.max() < 3e-7, rel.max()
+    assert lib.orc_gi_exp(-80.5) == 0.0 and lib.orc_gi_exp(0.0) == 1.0
