@@ -320,6 +320,55 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
   }
 }
 
+__device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
+  y[0] = 0.282095f; y[1] = 0.488603f * n.y; y[2] = 0.488603f * n.z; y[3] = 0.488603f * n.x;
+  y[4] = 1.092548f * n.x * n.y; y[5] = 1.092548f * n.y * n.z; y[6] = 0.315392f * (3.0f * n.z * n.z - 1.0f);
+  y[7] = 1.092548f * n.x * n.z; y[8] = 0.546274f * (n.x * n.x - n.y * n.y);
+}
+
+// projectSH (rc.ts:752-774) of cascade-0 probe pi, fused into its merge: the probe's 16 directions (res 4) are held by
+// its four quad threads, four consecutive lanes, 4 merged radiances each (as stored).  Every lane of the group collects
+// the 16 with shuffles and sums the 27 coefficients over the directions in order 0..15, with fused multiply-adds; lane
+// i of the group stores the probe's coefficient groups 2i and 2i+1.
+template <int A>
+__device__ __forceinline__ void project_sh_quads(const RcDev &r, uint32_t pi, const f3 mr[4]) {
+  const uint32_t lane = threadIdx.x & 31u, gbase = lane & ~3u;
+  const unsigned gmask = 0xFu << gbase;
+  const float *F = r.frame;
+  f3 cf[9];
+#pragma unroll
+  for (int k = 0; k < 9; k++) cf[k] = mk(0.0f, 0.0f, 0.0f);
+#pragma unroll
+  for (uint32_t d = 0; d < 16u; d++) {
+    const uint32_t u = d & 3u, vr = d >> 2, j = (vr & 1u) * 2u + (u & 1u);
+    const int src = (int)(gbase + (vr >> 1) * 2u + (u >> 1));
+    f3 rd = mk(__shfl_sync(gmask, mr[j].x, src), __shfl_sync(gmask, mr[j].y, src), __shfl_sync(gmask, mr[j].z, src));
+    f3 rr = rd * F[F_OMEGA + d];
+    float4 dv = r.dirs[r.c[0].dir_off + d];   // dirOf(d, 4), tabulated
+    float y[9];
+    sh_basis(mk(dv.x, dv.y, dv.z), y);
+#pragma unroll
+    for (int k = 0; k < 9; k++) cf[k] = fma3(rr, y[k], cf[k]);
+  }
+  float vals[32];
+#pragma unroll
+  for (int k = 0; k < 32; k++) vals[k] = 0.0f;
+  const float a0 = GI_PI, a1 = 2.0f * GI_PI / 3.0f, a2 = GI_PI / 4.0f;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    float a = k == 0 ? a0 : (k < 4 ? a1 : a2);
+    vals[k * 3 + 0] = cf[k].x * a; vals[k * 3 + 1] = cf[k].y * a; vals[k * 3 + 2] = cf[k].z * a;
+  }
+  typedef typename Atlas<A>::T T;
+#pragma unroll
+  for (uint32_t q = 0; q < 8u; q++) {
+    if ((q >> 1) != (lane & 3u)) continue;
+    float4 val = make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
+    if (r.f32_out) reinterpret_cast<float4 *>(r.sh)[(size_t)pi * 8u + q] = val;
+    else Atlas<A>::store(reinterpret_cast<T *>(r.sh), (size_t)pi * 8u + q, val);
+  }
+}
+
 // mergeScreen (rc.ts:710-743) for cascade c, in place, one 2x2 quad of directions (four rays) per thread.  The four
 // upper probes and their weights depend only on the probe, so a thread computes them once for its four rays.
 // upperAvg (rc.ts:681-686) of the upper cascade comes from up_avg, the quad averages the upper cascade's merge wrote
@@ -367,6 +416,7 @@ __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4
     }
   }
   f3 qsum = mk(0.0f, 0.0f, 0.0f);
+  f3 mr[4];   // the four merged radiances as stored (rounded to the atlas)
 #pragma unroll
   for (uint32_t j = 0; j < 4; j++) {   // (0,0) (1,0) (0,1) (1,1): upperAvg's a, b, c, d order
     uint32_t u = u0 + (j & 1u), v = v0 + (j >> 1);
@@ -398,59 +448,16 @@ __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4
     }
     f3 m = fma3(up, vv.w, mk(vv.x, vv.y, vv.z));
     Atlas<A>::store(rad, idx, make_float4(m.x, m.y, m.z, 1.0f));
-    if (my_avg) qsum = qsum + mk(Atlas<A>::round(m.x), Atlas<A>::round(m.y), Atlas<A>::round(m.z));
+    mr[j] = mk(Atlas<A>::round(m.x), Atlas<A>::round(m.y), Atlas<A>::round(m.z));
+    if (my_avg) qsum = qsum + mr[j];
   }
   if (my_avg) {
     f3 a = qsum * 0.25f;
     my_avg[((size_t)pi << hq_log2) + (v0 >> 1) * hr + (u0 >> 1)] = make_float4(a.x, a.y, a.z, 0.0f);
   }
+  if (c == 0u) project_sh_quads<A>(r, pi, mr);
 }
 
-__device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
-  y[0] = 0.282095f; y[1] = 0.488603f * n.y; y[2] = 0.488603f * n.z; y[3] = 0.488603f * n.x;
-  y[4] = 1.092548f * n.x * n.y; y[5] = 1.092548f * n.y * n.z; y[6] = 0.315392f * (3.0f * n.z * n.z - 1.0f);
-  y[7] = 1.092548f * n.x * n.z; y[8] = 0.546274f * (n.x * n.x - n.y * n.y);
-}
-
-// projectSH (rc.ts:752-774): c0's 16 directions -> L2 SH of irradiance
-template <int A>
-__global__ void __launch_bounds__(256) k_project_sh(RcDev r) {
-  grid_dep_wait();
-  typedef typename Atlas<A>::T T;
-  const T *rad = reinterpret_cast<const T *>(r.rad);
-  T *sh = reinterpret_cast<T *>(r.sh);
-  const CascDev &L = r.c[0];
-  uint32_t pi = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pi >= L.tiles_x * L.tiles_y) return;
-  const float *F = r.frame;
-  f3 cf[9];
-#pragma unroll
-  for (int k = 0; k < 9; k++) cf[k] = mk(0.0f, 0.0f, 0.0f);
-  for (uint32_t d = 0; d < 16; d++) {
-    float4 rp = Atlas<A>::load(rad, (size_t)L.rad_off + pi * 16u + d);
-    f3 rr = mk(rp.x, rp.y, rp.z) * F[F_OMEGA + d];
-    float y[9];
-    sh_basis(dir_of(d, 4u), y);
-#pragma unroll
-    for (int k = 0; k < 9; k++) cf[k] = fma3(rr, y[k], cf[k]);
-  }
-  float vals[32];
-#pragma unroll
-  for (int k = 0; k < 32; k++) vals[k] = 0.0f;
-  const float a0 = GI_PI, a1 = 2.0f * GI_PI / 3.0f, a2 = GI_PI / 4.0f;
-#pragma unroll
-  for (int k = 0; k < 9; k++) {
-    float a = k == 0 ? a0 : (k < 4 ? a1 : a2);
-    vals[k * 3 + 0] = cf[k].x * a; vals[k * 3 + 1] = cf[k].y * a; vals[k * 3 + 2] = cf[k].z * a;
-  }
-#pragma unroll
-  for (int q = 0; q < 8; q++)
-  {
-    float4 val = make_float4(vals[4 * q], vals[4 * q + 1], vals[4 * q + 2], vals[4 * q + 3]);
-    if (r.f32_out) reinterpret_cast<float4 *>(r.sh)[(size_t)pi * 8u + q] = val;
-    else Atlas<A>::store(sh, (size_t)pi * 8u + q, val);
-  }
-}
 
 // SH element i as f32: stored as f32 with f32_out, else in the atlas format
 template <int A>
@@ -633,7 +640,6 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
     const float4 *above = r.mavg[(c + 1) & 1];
     GI_TRY(gi_launch(k_merge<A>, (n + d.merge_threads - 1u) / d.merge_threads, d.merge_threads, st, r, (uint32_t)c, above, mine));
   }
-  GI_TRY(gi_launch(k_project_sh<A>, (r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, st, r));
   if (ev) cudaEventRecord(ev[3], st);
   const uint32_t P0 = r.c[0].tile_size;
   if (d.gather_shape == 3 && (P0 == 8u || P0 == 16u || P0 == 32u)) {
