@@ -458,7 +458,7 @@ def run_ours(args, rank, world, local_rank):
                        "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
                        "d2h_bytes_per_step": int(irr_h[0].numel()),
                        "mode": "rtgi.pipeline: copies of neighbouring frames overlap the solve (2 cascade sets)"},
-               "gpu_launches": n_ev * (17 + (v.levels - 1) + 3 + p.cascades),
+               "gpu_launches": n_ev * (11 + (1 if v.levels > 1 else 0) + 3 + p.cascades),
                "clocks": clk, "wall_s": wall}
     if args.batch > 0:
         bt = run_batched(args, ctx, stream, flush)

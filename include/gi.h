@@ -115,7 +115,8 @@ int gi_vox_update(gi_vox *vox, const double eye[3]);
 /* encode(pass) (voxel.ts:897-899): the whole rebuild, clear .. resolveAttr, stream-ordered. */
 int gi_vox_build(gi_vox *vox, void *stream);
 /* readCounters (voxel.ts:908-918): the 64 header words (0 bricks marked, 1 voxels, 2-4 brick/big/voxel overflow,
- * 8-15 bricks per level, 16-23 voxBits big triangles per level, 24-31 markBricks big triangles per level).
+ * 6 nonzero if a chained scan of the rebuild stopped waiting for a block (never expected), 8-15 bricks per level,
+ * 16-23 voxBits big triangles per level, 24-31 markBricks big triangles per level).
  * Synchronises the stream. */
 int gi_vox_read_counters(gi_vox *vox, uint32_t hdr[64], void *stream);
 /* usedBytes (voxel.ts:919-922) of the last counters read: persistent and build-temporary bytes. */
@@ -145,7 +146,7 @@ int gi_scene_rigid_apply(gi_scene *scene, void *stream);
  * cannot call cudaMalloc: a renderer that hands out every buffer from its own fixed device pool, a thread that is
  * capturing a CUDA graph, a serving loop that must not stall the GPU with an allocation mid-request.  This entry point
  * takes the scene and every output in the caller's device memory and allocates nothing: its scratch (representatives,
- * big-triangle lists, scan sums) is a static device array of 14.1 MiB that the library holds on every GPU it is loaded
+ * big-triangle lists, scan sums) is a static device array of 14.2 MiB that the library holds on every GPU it is loaded
  * on.  Limits: max_bricks <= 4096, levels * G^3 <= 2^25, 65,536 big triangles per list (more count as bigOverflow,
  * header word 3).  Inputs: pos4/nrm4 4 floats per vertex (w ignored), tri4 (i0, i1, i2, material) with indices below
  * nverts / nmats (not checked: they are device memory), mats device gi_material[nmats]; pos4, nrm4, tri4, occ, attr

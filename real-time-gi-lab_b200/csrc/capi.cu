@@ -138,7 +138,7 @@ static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
   cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
   cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
-  cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre); cudaFree(d.citem);
+  cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre); cudaFree(d.citem); cudaFree(d.look);
 }
 static void free_rc(gi_rc *r) {
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
@@ -363,14 +363,15 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
       (e = dalloc(&d.attr, p->max_voxels)) || (e = dalloc(&d.plane, p->max_voxels)) ||
       (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words)) ||
       (e = dalloc(&d.vpre, (size_t)p->max_bricks + 1u)) || (e = dalloc(&d.work, 4)) ||
-      (e = dalloc(&d.cpre, (size_t)8u * d.big_cap)) || (e = dalloc(&d.citem, (size_t)VOX_CITEM_CAP))) {
+      (e = dalloc(&d.cpre, (size_t)8u * d.big_cap)) || (e = dalloc(&d.citem, (size_t)VOX_CITEM_CAP)) ||
+      (e = dalloc(&d.look, (size_t)scan_words + 1u))) {
     free_vox(v);
     delete v;
     return cuda_fail(e, "gi_vox_create");
   }
   v->bytes = (GI_HDR + nptr + (uint64_t)p->max_bricks * (16u + 2u + 512u) + (uint64_t)16u * d.big_cap +
               (uint64_t)p->max_voxels * 6u + scan_words + p->max_bricks + 5u + (uint64_t)8u * d.big_cap +
-              VOX_CITEM_CAP) * 4u;
+              VOX_CITEM_CAP + 2u * ((uint64_t)scan_words + 1u)) * 4u;
   memset(v->hdr, 0, sizeof v->hdr);
   *out = v;
   return GI_OK;

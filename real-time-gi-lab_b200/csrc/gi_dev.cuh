@@ -188,6 +188,7 @@ struct VoxDev {
   uint32_t *work;      // build temporary: 4 words, queue counters and the chunk total of the big-triangle passes
   uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
   uint32_t *citem;     // build temporary (optional): the item of each chunk, citem_cap entries
+  unsigned long long *look;   // build temporary: scan_cap + 1 words, the chained scans' ticket and block states
 };
 
 __device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return v.vs[L]; }

@@ -7,7 +7,7 @@
 // representative table, the big-triangle lists, the scans' sums, the work queues).  Here that scratch is a file-scope static
 // device array, so this entry point allocates nothing.
 //
-// The array lives in every GPU that loads the library until the process exits (14.1 MiB).  All calls share it and it
+// The array lives in every GPU that loads the library until the process exits (14.2 MiB).  All calls share it and it
 // keeps the last call's contents: the rebuild clears what must start at zero itself (the lists' counters are header
 // words of the caller's output, the representatives of every allocated brick are zeroed by the allocation pass), but
 // two calls that overlap on the GPU (different streams, different host threads) race on the array and corrupt each
@@ -30,8 +30,10 @@ namespace {
 constexpr uint32_t NOALLOC_MAX_BRICKS = 4096;          // representative table: 4096 x 512 words = 8 MiB
 constexpr uint32_t NOALLOC_BIG_CAP = 1u << 16;         // per big-triangle list: 16 x 65536 words = 4 MiB
 constexpr uint32_t NOALLOC_SCAN_WORDS = 1u << 14;      // block sums: levels * G^3 <= 2^25 pointers
-constexpr uint32_t NOALLOC_WORDS = NOALLOC_MAX_BRICKS * 512u + 16u * NOALLOC_BIG_CAP + NOALLOC_SCAN_WORDS +
-                                   NOALLOC_MAX_BRICKS + 1u + 4u + 8u * NOALLOC_BIG_CAP;
+// the chained scans' states (64-bit words) start on an even word
+constexpr uint32_t NOALLOC_LOOK_AT = (NOALLOC_MAX_BRICKS * 512u + 16u * NOALLOC_BIG_CAP + NOALLOC_SCAN_WORDS +
+                                      NOALLOC_MAX_BRICKS + 1u + 4u + 8u * NOALLOC_BIG_CAP + 1u) & ~1u;
+constexpr uint32_t NOALLOC_WORDS = NOALLOC_LOOK_AT + 2u * (NOALLOC_SCAN_WORDS + 1u);
 
 // The scratch.  In host code `g_noalloc_scratch` only names the symbol; its device address comes from
 // cudaGetSymbolAddress, once per device (see scratch_address).
@@ -135,6 +137,7 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   v.vpre = v.scan + NOALLOC_SCAN_WORDS;
   v.work = v.vpre + NOALLOC_MAX_BRICKS + 1u;
   v.cpre = v.work + 4u;
+  v.look = reinterpret_cast<unsigned long long *>(scratch + NOALLOC_LOOK_AT);
 
   SceneDev s;
   s.pos = reinterpret_cast<const float4 *>(pos4); s.nrm = reinterpret_cast<const float4 *>(nrm4);

@@ -136,11 +136,12 @@ __device__ __forceinline__ void mark_one(const VoxDev &v, const Tri &T, uint32_t
 // clear (voxel.ts:338-344)
 __global__ void k_clear(VoxDev v) {
   grid_dep_wait();
-  uint32_t n = v.levels * v.G * v.G * v.G;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < GI_HDR; i += gridDim.x * blockDim.x) {
+  uint32_t n = v.levels * v.G * v.G * v.G, nl = v.scan_cap + 1u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n || i < GI_HDR || i < nl; i += gridDim.x * blockDim.x) {
     if (i < GI_HDR) v.hdr[i] = 0u;
     if (i < 4u) v.work[i] = 0u;
     if (i < n) v.ptr[i] = GI_EMPTY;
+    if (i < nl) v.look[i] = 0ull;   // the brick allocation's chained scan
   }
 }
 
@@ -271,66 +272,61 @@ __device__ __forceinline__ uint32_t block_scan_256(uint32_t x, uint32_t *total) 
   return excl;
 }
 
-// Per block: the number of marked entries of its chunk of the order space.
-__global__ void __launch_bounds__(256) k_count_marks(VoxDev v, uint32_t kpt) {
-  grid_dep_wait();
-  uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per;
-  uint32_t o0 = blockIdx.x * 256u * kpt;
-  uint32_t c = 0;
-  for (uint32_t k = threadIdx.x; k < 256u * kpt; k += 256u) {
-    uint32_t o = o0 + k;
-    if (o < n && v.ptr[order_to_ptr(o, per, NL)] == GI_MARK) c++;
-  }
-  uint32_t tot;
-  block_scan_256(c, &tot);
-  if (threadIdx.x == 0) v.scan[blockIdx.x] = tot;
+// ---- chained scans: one pass, decoupled look-back ---------------------------------------------------------------
+// look[0] hands out tickets (the order in which blocks take their part of the scan: every smaller ticket belongs to
+// a block that is already running); look[1 + k] is part k's state, status << 32 | value with status 1 = the part's
+// own sum, 2 = the inclusive prefix through the part.  A part waits only on smaller tickets, so every wait ends; the
+// spin is bounded all the same, and a part that gives up sets header word 6 and takes what it has.
+constexpr uint32_t LOOK_SPIN = 1u << 20;
+
+__device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long x) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(x) : "memory");
+}
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long *p) {
+  unsigned long long x;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(x) : "l"(p) : "memory");
+  return x;
 }
 
-// Exclusive scan of the block sums (one block, nblocks <= 256 * 16); writes the total to hdr[0] and hdr[5].
-__global__ void __launch_bounds__(256) k_scan_sums(uint32_t *sums, uint32_t nblocks, uint32_t *hdr) {
-  grid_dep_wait();
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
+// The block's ticket (block-uniform; all threads call it).
+__device__ __forceinline__ uint32_t chain_ticket(unsigned long long *look) {
+  __shared__ uint32_t s_ticket;
+  if (threadIdx.x == 0) s_ticket = (uint32_t)atomicAdd(look, 1ull);
   __syncthreads();
-  for (uint32_t b0 = 0; b0 < nblocks; b0 += 256u) {
-    uint32_t i = b0 + threadIdx.x;
-    uint32_t x = i < nblocks ? sums[i] : 0u;
-    uint32_t tot;
-    uint32_t ex = block_scan_256(x, &tot);
-    if (i < nblocks) sums[i] = carry + ex;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += tot;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0 && hdr) { hdr[0] = carry; hdr[5] = carry; }
-}
-
-// The chunk prefix's block offsets (k_count_chunks wrote one sum per 256 items) and the chunk total (work[2]).
-__global__ void __launch_bounds__(256) k_scan_chunks(VoxDev v) {
-  grid_dep_wait();
-  uint32_t nblocks = (big_total(v, 16u) + 255u) / 256u;
-  __shared__ uint32_t carry;
-  if (threadIdx.x == 0) carry = 0;
+  uint32_t t = s_ticket;
   __syncthreads();
-  for (uint32_t b0 = 0; b0 < nblocks; b0 += 256u) {
-    uint32_t i = b0 + threadIdx.x;
-    uint32_t x = i < nblocks ? v.scan[i] : 0u;
-    uint32_t tot;
-    uint32_t ex = block_scan_256(x, &tot);
-    if (i < nblocks) v.scan[i] = carry + ex;
-    __syncthreads();
-    if (threadIdx.x == 0) carry += tot;
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) v.work[2] = carry;
+  return t;
 }
 
-// allocBricks (voxel.ts:450-470) in the fixed order.
-__global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v, uint32_t kpt) {
+// One thread per block: publishes part k's sum, looks back for its exclusive prefix, publishes the inclusive prefix.
+__device__ __forceinline__ uint32_t chain_prefix(unsigned long long *look, uint32_t k, uint32_t sum, uint32_t *hdr) {
+  unsigned long long *st = look + 1;
+  if (k == 0u) { st_release_u64(st, (2ull << 32) | sum); return 0u; }
+  st_release_u64(st + k, (1ull << 32) | sum);
+  uint32_t excl = 0, j = k - 1u, spins = 0;
+  for (;;) {
+    unsigned long long x = ld_acquire_u64(st + j);
+    uint32_t f = (uint32_t)(x >> 32);
+    if (f == 0u) {
+      if (++spins > LOOK_SPIN) { atomicExch(&hdr[6], 1u); break; }
+      __nanosleep(32);
+      continue;
+    }
+    excl += (uint32_t)x;
+    if (f == 2u || j == 0u) break;
+    j--;
+  }
+  st_release_u64(st + k, (2ull << 32) | (excl + sum));
+  return excl;
+}
+
+// allocBricks (voxel.ts:411-470: countMarks, scanMarks, allocBricks) in the fixed order, one pass: each block takes
+// 256 * kpt consecutive entries of the order space, kpt per thread.
+__global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v, uint32_t kpt, uint32_t nblocks) {
   grid_dep_wait();
   uint32_t per = v.G * v.G * v.G, NL = v.levels, n = NL * per, G = v.G;
-  uint32_t o0 = blockIdx.x * 256u * kpt;
-  // each thread owns kpt (<= 32) consecutive entries of the chunk
+  uint32_t blk = chain_ticket(v.look);
+  uint32_t o0 = blk * 256u * kpt;
   uint32_t flags = 0, c = 0;
   for (uint32_t k = 0; k < kpt; k++) {
     uint32_t o = o0 + threadIdx.x * kpt + k;
@@ -339,7 +335,15 @@ __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v, uint32_t kpt) {
     c += m ? 1u : 0u;
   }
   uint32_t tot;
-  uint32_t ex = block_scan_256(c, &tot) + v.scan[blockIdx.x];
+  uint32_t ex = block_scan_256(c, &tot);
+  __shared__ uint32_t s_pre;
+  if (threadIdx.x == 0) {
+    uint32_t pre = chain_prefix(v.look, blk, tot, v.hdr);
+    s_pre = pre;
+    if (blk == nblocks - 1u) { v.hdr[0] = pre + tot; v.hdr[5] = pre + tot; }
+  }
+  __syncthreads();
+  ex += s_pre;
   for (uint32_t k = 0; k < kpt; k++) {
     if (!((flags >> k) & 1u)) continue;
     uint32_t o = o0 + threadIdx.x * kpt + k;
@@ -366,6 +370,8 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
     if (q < nb * 4u) occ[q] = z;
     else rep[q - nb * 4u] = z;
   }
+  // the big items' chunk scan
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= v.scan_cap; q += gridDim.x * blockDim.x) v.look[q] = 0ull;
 }
 
 // voxelizeOne (voxel.ts:476-490)
@@ -426,16 +432,20 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
 
 // voxBitsBig (voxel.ts:515-534), balanced: every big (triangle, level) is cut into chunks of VB_CHUNK cells (a wall
 // triangle clipped to a window covers ~10^4 cells; one warp per triangle left one warp working long after the rest).
-// k_count_chunks: per item its chunk count, an exclusive prefix within blocks of 256 items and the block sums;
-// k_scan_sums turns those into block offsets and the total; warps of k_vox_bits_big take chunks from a queue and
-// find their item by binary search over the prefix.
+// k_chunks, one chained scan over the items in blocks of 256: per item its chunk count, its prefix within the block
+// (cpre), the blocks' offsets (scan), the chunk total (work[2]) and, below citem_cap, the item of every chunk (a table
+// lookup for k_vox_bits_big instead of ~16 dependent loads of a binary search).  Warps of k_vox_bits_big take chunks
+// from a queue.
 // VB_CHUNK = 1 << v.chunk_log2 cells per work item (gi_vox_tuning; default 128)
 
-__global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
+__global__ void __launch_bounds__(256) k_chunks(VoxDev v, SceneDev s) {
   grid_dep_wait();
   uint32_t items = big_total(v, 16u);
   uint32_t nblk = (items + 255u) / 256u;
-  for (uint32_t b = blockIdx.x; b < nblk; b += gridDim.x) {
+  __shared__ uint32_t s_pre;
+  for (;;) {
+    uint32_t b = chain_ticket(v.look);
+    if (b >= nblk) break;
     uint32_t w = b * 256u + threadIdx.x, L, t, c = 0;
     if (w < items && big_item(v, 0u, 16u, w, L, t)) {
       Tri T = load_tri(s, t);
@@ -444,20 +454,19 @@ __global__ void __launch_bounds__(256) k_count_chunks(VoxDev v, SceneDev s) {
     }
     uint32_t tot;
     uint32_t ex = block_scan_256(c, &tot);
-    if (w < items) v.cpre[w] = ex;
-    if (threadIdx.x == 0) v.scan[b] = tot;
-  }
-}
-
-// The item of every chunk below citem_cap (the rest are found by binary search over the prefix): a table lookup
-// instead of ~16 dependent loads per chunk.
-__global__ void __launch_bounds__(256) k_fill_chunks(VoxDev v) {
-  grid_dep_wait();
-  uint32_t items = big_total(v, 16u), total = v.work[2];
-  for (uint32_t w = blockIdx.x * blockDim.x + threadIdx.x; w < items; w += gridDim.x * blockDim.x) {
-    uint32_t first = v.cpre[w] + v.scan[w >> 8];
-    uint32_t end = w + 1u < items ? v.cpre[w + 1u] + v.scan[(w + 1u) >> 8] : total;
-    for (uint32_t ch = first; ch < end && ch < v.citem_cap; ch++) v.citem[ch] = w;
+    if (threadIdx.x == 0) {
+      uint32_t pre = chain_prefix(v.look, b, tot, v.hdr);
+      s_pre = pre;
+      v.scan[b] = pre;
+      if (b == nblk - 1u) v.work[2] = pre + tot;
+    }
+    __syncthreads();
+    uint32_t first = s_pre + ex;
+    if (w < items) {
+      v.cpre[w] = ex;
+      for (uint32_t ch = first; ch < first + c && ch < v.citem_cap; ch++) v.citem[ch] = w;
+    }
+    __syncthreads();   // s_pre is rewritten by the next part
   }
 }
 
@@ -489,6 +498,8 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
   uint32_t bo = v.hdr[2];
   uint32_t items = big_total(v, 16u);
   uint32_t chunks = v.work[2];
+  // the attribute allocation's chained scan (the chunk scan is done: its offsets are in scan)
+  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= v.scan_cap; q += gridDim.x * blockDim.x) v.look[q] = 0ull;
   for (;;) {
     uint32_t ch = 0;
     if (lane == 0) ch = atomicAdd(&v.work[1], 1u);
@@ -496,7 +507,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
     if (ch >= chunks) break;
     uint32_t lo = 0;
     if (ch < v.citem_cap) {
-      lo = v.citem[ch];              // the chunk's item, tabulated by k_fill_chunks
+      lo = v.citem[ch];              // the chunk's item, tabulated by k_chunks
     } else {
       uint32_t hi = items;           // the last item whose first chunk is <= ch
       while (hi - lo > 1u) {
@@ -527,33 +538,30 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
   }
 }
 
-// First brick index and count of level l (bricks are allocated coarse levels first).
-__device__ __forceinline__ void level_bricks(const VoxDev &v, uint32_t l, uint32_t &first, uint32_t &count) {
-  first = 0;
-  for (uint32_t k = v.levels - 1u; k > l; k--) first += v.hdr[8 + k];
-  count = v.hdr[8 + l];
-}
-
-// reduce (voxel.ts:540-577): level L from level L-1, one thread per occupancy word of a level L-1 brick
-__global__ void __launch_bounds__(256) k_reduce(VoxDev v, uint32_t L) {
+// reduce (voxel.ts:540-577) for every level at once.  The reference runs reduce(L) for L = 1 .. levels-1 in turn, each
+// ORing the occupancy of level L-1 (its own voxels and what reduce(L-1) put there) into level L and taking the maximum
+// of the representatives, through the parent brick when it is allocated.  OR and max are associative, so level L ends
+// with its own voxels and those of every finer level l whose parent bricks l+1 .. L are all allocated: here one thread
+// per occupancy word of a level 0 .. levels-2 brick walks up the levels, the word's 8 x 4 cells becoming 4 x 2 parent
+// cells, then 2 x 1, then 1, and stops at the first level without a brick.  Same final state, one launch.
+__global__ void __launch_bounds__(256) k_reduce(VoxDev v) {
   grid_dep_wait();
-  uint32_t first, count;
-  level_bricks(v, L - 1u, first, count);
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count * 16u; i += gridDim.x * blockDim.x) {
+  const uint32_t NL = v.levels, nb = min(v.hdr[0], v.max_bricks);
+  const uint32_t first = v.hdr[8 + NL - 1u];   // bricks are allocated coarse levels first: the finer ones follow
+  const int lim = (int)v.G * 8;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (nb - first) * 16u; i += gridDim.x * blockDim.x) {
     uint32_t ptr = first + (i >> 4), w = i & 15u;
     uint32_t word = v.occ[ptr * 16u + w];
     if (word == 0u) continue;
     uint32_t code = v.code[ptr];
-    uint32_t Lc = code >> 27;
+    uint32_t l = code >> 27;
     i3 b = mki((int)((code >> 18) & 511u), (int)((code >> 9) & 511u), (int)(code & 511u));
-    i3 c0 = mki(b.x * 8, b.y * 8 + (int)((w & 1u) * 4u), b.z * 8 + (int)(w >> 1));
-    i3 oc = org(v, Lc), ol = org(v, L);
-    i3 pc0 = mki(((oc.x * 8 + c0.x) >> 1) - ol.x * 8, ((oc.y * 8 + c0.y) >> 1) - ol.y * 8, ((oc.z * 8 + c0.z) >> 1) - ol.z * 8);
-    uint32_t pptr = v.ptr[ptr_index(v, L, mki(pc0.x >> 3, pc0.y >> 3, pc0.z >> 3))];
-    if (pptr >= GI_MARK) continue;
-    uint32_t pbit0 = (uint32_t)((pc0.x & 7) + 8 * (pc0.y & 7) + 64 * (pc0.z & 7));
-    uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
-    // the word's 32 representatives in 8 independent 128-bit loads; bit k = x + 8 y of the word, parent (x/2, y/2)
+    // the word's first cell in level-l cells from the world origin
+    i3 oc = org(v, l);
+    i3 wc = mki(oc.x * 8 + b.x * 8, oc.y * 8 + b.y * 8 + (int)((w & 1u) * 4u), oc.z * 8 + b.z * 8 + (int)(w >> 1));
+    // 4 x 2 parent cells: occupancy (bit px + 4 py) and representatives; the word's 32 representatives in 8
+    // independent 128-bit loads; bit k = x + 8 y of the word, parent (x/2, y/2)
+    uint32_t lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0}, m1 = 0;
     const uint4 *rp = reinterpret_cast<const uint4 *>(v.rep + ptr * 512u + w * 32u);
     uint4 rq[8];
 #pragma unroll
@@ -566,23 +574,40 @@ __global__ void __launch_bounds__(256) k_reduce(VoxDev v, uint32_t L) {
       uint32_t c = max((b4 & 4u) ? rq[q].z : 0u, (b4 & 8u) ? rq[q].w : 0u);
       if (q < 4) { lo[px] = max(lo[px], a); lo[px + 1u] = max(lo[px + 1u], c); }
       else { hi[px] = max(hi[px], a); hi[px + 1u] = max(hi[px + 1u], c); }
+      uint32_t pa = ((b4 & 3u) ? 1u : 0u) | ((b4 & 12u) ? 2u : 0u);   // parents px, px + 1 of this row
+      m1 |= pa << (px + (q < 4 ? 0u : 4u));
     }
-    while (word != 0u) {
-      uint32_t k = __ffs(word) - 1u;
-      word &= word - 1u;
-      mask |= 1u << ((pbit0 + ((k & 7u) >> 1) + 8u * (k >> 4)) & 31u);
-    }
-    uint32_t wi = pptr * 16u + (pbit0 >> 5);
-    if ((v.occ[wi] & mask) != mask) atomicOr(&v.occ[wi], mask);
-#pragma unroll
-    for (uint32_t px = 0; px < 4u; px++)
-#pragma unroll
-      for (uint32_t py = 0; py < 2u; py++) {
-        uint32_t rv = py == 0u ? lo[px] : hi[px];
-        if (rv == 0u) continue;
-        uint32_t ri = pptr * 512u + pbit0 + px + 8u * py;
-        if (v.rep[ri] < rv) atomicMax(&v.rep[ri], rv);
+    for (uint32_t L = l + 1u, s = 1u; L < NL; L++, s++) {
+      wc = mki(wc.x >> 1, wc.y >> 1, wc.z >> 1);
+      i3 ol = org(v, L);
+      i3 pc = mki(wc.x - ol.x * 8, wc.y - ol.y * 8, wc.z - ol.z * 8);
+      if (pc.x < 0 || pc.y < 0 || pc.z < 0 || pc.x >= lim || pc.y >= lim || pc.z >= lim) break;
+      uint32_t pptr = v.ptr[ptr_index(v, L, mki(pc.x >> 3, pc.y >> 3, pc.z >> 3))];
+      if (pptr >= GI_MARK) break;
+      uint32_t pbit0 = (uint32_t)((pc.x & 7) + 8 * (pc.y & 7) + 64 * (pc.z & 7));
+      if (s == 2u) {   // 4 x 2 -> 2 x 1
+        lo[0] = max(max(lo[0], lo[1]), max(hi[0], hi[1]));
+        lo[1] = max(max(lo[2], lo[3]), max(hi[2], hi[3]));
+        m1 = ((m1 & 0x33u) ? 1u : 0u) | ((m1 & 0xCCu) ? 2u : 0u);
+      } else if (s == 3u) {   // 2 x 1 -> 1
+        lo[0] = max(lo[0], lo[1]);
+        m1 = m1 ? 1u : 0u;
       }
+      const uint32_t nx = s == 1u ? 4u : (s == 2u ? 2u : 1u), ny = s == 1u ? 2u : 1u;
+      uint32_t mask = 0;
+      for (uint32_t py = 0; py < ny; py++)
+        for (uint32_t px = 0; px < nx; px++)
+          if ((m1 >> (px + nx * py)) & 1u) mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
+      uint32_t wi = pptr * 16u + (pbit0 >> 5);
+      if ((v.occ[wi] & mask) != mask) atomicOr(&v.occ[wi], mask);
+      for (uint32_t py = 0; py < ny; py++)
+        for (uint32_t px = 0; px < nx; px++) {
+          uint32_t rv = py == 0u ? lo[px] : hi[px];
+          if (rv == 0u) continue;
+          uint32_t ri = pptr * 512u + pbit0 + px + 8u * py;
+          if (v.rep[ri] < rv) atomicMax(&v.rep[ri], rv);
+        }
+    }
   }
 }
 
@@ -600,23 +625,19 @@ __device__ __forceinline__ uint32_t brick_pop(const VoxDev &v, uint32_t b) {
   return n;
 }
 
-__global__ void __launch_bounds__(256) k_count_voxels(VoxDev v) {
-  grid_dep_wait();
-  uint32_t nb = min(v.hdr[0], v.max_bricks);
-  uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
-  uint32_t c = b < nb ? brick_pop(v, b) : 0u;
-  uint32_t tot;
-  block_scan_256(c, &tot);
-  if (threadIdx.x == 0) v.scan[blockIdx.x] = tot;
-}
-
+// allocVoxels in one pass: each block takes 256 bricks (chained scan of their popcounts).
 __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks) {
   grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
-  uint32_t b = blockIdx.x * VOX_CHUNK + threadIdx.x;
+  uint32_t blk = chain_ticket(v.look);
+  uint32_t b = blk * VOX_CHUNK + threadIdx.x;
   uint32_t c = b < nb ? brick_pop(v, b) : 0u;
   uint32_t tot;
-  uint32_t first = block_scan_256(c, &tot) + v.scan[blockIdx.x];
+  uint32_t ex = block_scan_256(c, &tot);
+  __shared__ uint32_t s_pre;
+  if (threadIdx.x == 0) s_pre = chain_prefix(v.look, blk, tot, v.hdr);
+  __syncthreads();
+  uint32_t first = ex + s_pre;
   if (b < nb) {
     if (first + c > v.max_voxels) { v.base[b] = GI_EMPTY; atomicAdd(&v.hdr[4], 1u); }
     else v.base[b] = first;
@@ -624,7 +645,7 @@ __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks
     if (b == nb - 1u) v.vpre[nb] = first + c;
   }
   if (nb == 0u && b == 0u) v.vpre[0] = 0u;
-  if (blockIdx.x == nblocks - 1u && threadIdx.x == 255u) v.hdr[1] = first + c;
+  if (blk == nblocks - 1u && threadIdx.x == 255u) v.hdr[1] = first + c;
 }
 
 // closestBary (voxel.ts:250-267)
@@ -741,19 +762,13 @@ cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_
   uint32_t kpt = 1;
   while ((nptr + 256u * kpt - 1u) / (256u * kpt) > v.scan_cap && kpt < 32u) kpt *= 2u;
   uint32_t ab = (nptr + 256u * kpt - 1u) / (256u * kpt);
-  GI_TRY(gi_launch(k_count_marks, ab, 256, st, v, kpt));
-  GI_TRY(gi_launch(k_scan_sums, 1, 256, st, v.scan, ab, v.hdr));
-  GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v, kpt));
+  GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v, kpt, ab));
   GI_TRY(gi_launch(k_init_bricks, persist, 256, st, v));
   if (tb) GI_TRY(gi_launch(k_vox_bits, tb, 256, st, v, s));
-  GI_TRY(gi_launch(k_count_chunks, persist, 256, st, v, s));
-  GI_TRY(gi_launch(k_scan_chunks, 1, 256, st, v));
-  if (v.citem_cap) GI_TRY(gi_launch(k_fill_chunks, persist, 256, st, v));
+  GI_TRY(gi_launch(k_chunks, persist, 256, st, v, s));
   GI_TRY(gi_launch(k_vox_bits_big, persist, 256, st, v, s));
-  for (uint32_t L = 1; L < v.levels; L++) GI_TRY(gi_launch(k_reduce, persist, 256, st, v, L));
+  if (v.levels > 1) GI_TRY(gi_launch(k_reduce, persist, 256, st, v));
   uint32_t vb = (v.max_bricks + VOX_CHUNK - 1u) / VOX_CHUNK;
-  GI_TRY(gi_launch(k_count_voxels, vb, 256, st, v));
-  GI_TRY(gi_launch(k_scan_sums, 1, 256, st, v.scan, vb, nullptr));
   GI_TRY(gi_launch(k_alloc_voxels, vb, 256, st, v, vb));
   GI_TRY(gi_launch(k_resolve_attr, persist, 256, st, v, s));
   return cudaGetLastError();
