@@ -74,6 +74,19 @@ __device__ __forceinline__ i3 range_cell(Range r, int q) {
   return mki(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y));
 }
 
+// q / n for q, n <= 8 (n >= 1) without a division: (q * ceil(64 / n)) >> 6, exact while q * (n * ceil(64 / n) - 64)
+// < 64, which holds for every such pair.
+__device__ __forceinline__ int div_small(int q, int n) {
+  int m = (int)((0x080A0B0D10162040ull >> (8u * (uint32_t)(n - 1))) & 0xFFull);
+  return (q * m) >> 6;
+}
+// range_cell of a range of at most 8 cells (q < 8)
+__device__ __forceinline__ i3 range_cell_small(Range r, int q) {
+  int t = div_small(q, r.n.x);        // q / nx
+  int z = div_small(t, r.n.y);        // q / (nx * ny)
+  return mki(r.lo.x + q - t * r.n.x, r.lo.y + t - z * r.n.y, r.lo.z + z);
+}
+
 // Warp-balanced small work: every lane holds one (triangle, level) item of n <= 8 cells (or bricks); the warp's cells
 // are dealt out 32 at a time, so a lane with one cell does not idle while another works through eight.  The owner of
 // cell g is the first lane whose inclusive prefix exceeds g (a 5-step search over the prefixes with shuffles); its
@@ -125,7 +138,7 @@ __device__ __forceinline__ void mark_brick(const VoxDev &v, uint32_t i) {
 
 // markRange body for one brick j of the range (voxel.ts:348-358)
 __device__ __forceinline__ void mark_one(const VoxDev &v, const Tri &T, uint32_t L, Range r, uint32_t n, uint32_t j) {
-  i3 b = range_cell(r, (int)j);
+  i3 b = n <= 8u ? range_cell_small(r, (int)j) : range_cell(r, (int)j);
   if (finer_holds(v, L, mki(b.x * 8, b.y * 8, b.z * 8)) && finer_holds(v, L, mki(b.x * 8 + 7, b.y * 8 + 7, b.z * 8 + 7))) return;
   float bs = vox_size(v, L) * 8.0f;
   f3 c = region_lo(v, L) + adds(vi2f(b), 0.5f) * bs;
@@ -425,7 +438,7 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
     SmallItem it;
     it.T = T; it.t = t; it.r = r; it.n = n;
     warp_deal(it, (!big && n > 0) ? (uint32_t)n : 0u, [&](const SmallItem &w, int q) {
-      voxelize_one(v, s, w.T, w.t, L, range_cell(w.r, q), w.n == 1, bo);
+      voxelize_one(v, s, w.T, w.t, L, range_cell_small(w.r, q), w.n == 1, bo);
     });
   }
 }
@@ -522,10 +535,16 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
     Range r = vox_range(v, T, L, false);
     int n = r.n.x * r.n.y * r.n.z;
     int q_end = min(n, (int)((part + 1u) << v.chunk_log2));
-    for (int q0 = (int)(part << v.chunk_log2); q0 < q_end; q0 += 32) {
-      int q = q0 + (int)lane;
+    // the lane's cell, then 32 cells further in range order per step: 32 = dz * nx * ny + dy * nx + dx
+    int q = (int)(part << v.chunk_log2) + (int)lane;
+    i3 cell = range_cell(r, q);
+    const int nxy = r.n.x * r.n.y, dz = 32 / nxy, dy = (32 - dz * nxy) / r.n.x, dx = 32 - dz * nxy - dy * r.n.x;
+    for (; q - (int)lane < q_end; q += 32) {
       uint32_t wi = 0xffffffffu, msk = 0u, ri = 0u;
-      bool ok = q < q_end && voxel_takes(v, s, T, L, range_cell(r, q), bo, wi, msk, ri);
+      bool ok = q < q_end && voxel_takes(v, s, T, L, cell, bo, wi, msk, ri);
+      cell = mki(cell.x + dx, cell.y + dy, cell.z + dz);
+      if (cell.x >= r.lo.x + r.n.x) { cell.x -= r.n.x; cell.y++; }
+      if (cell.y >= r.lo.y + r.n.y) { cell.y -= r.n.y; cell.z++; }
       uint32_t any = __ballot_sync(0xffffffffu, ok);
       if (any == 0u) continue;
       uint32_t grp = __match_any_sync(0xffffffffu, ok ? wi : 0xffffffffu);
