@@ -360,7 +360,14 @@ def run_ours(args, rank, world, local_rank):
         at_cap = int(counts[64:64 + p.cascades].sum())
         # launch shapes for this workload from the library's autotuner (results do not depend on them)
         from rtgi import autotune
-        tuned = autotune.Autotuner(reps=5).tune(rc, vw, stream)
+        if args.tuning:   # fixed launch shapes (profiling runs), else the autotuner's
+            fixed = json.loads(args.tuning)
+            tuned = {"rc": {k: fixed[k] for k in rc.TUNING if k in fixed},
+                     "vox": {k: fixed[k] for k in ("chunk_cells", "blocks") if k in fixed}}
+            rc.set_tuning(**tuned["rc"])
+            vw.set_tuning(**tuned["vox"])
+        else:
+            tuned = autotune.Autotuner(reps=5).tune(rc, vw, stream)
         # per-pass times and the trace kernel's live duration (events between the passes)
         rc.set_timing(True)
         pass_ms = {k: [] for k in rc.PASSES}
@@ -493,6 +500,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="colonnade", choices=["colonnade", "room"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
+    ap.add_argument("--tuning", default=None, help="fixed launch shapes as JSON (skips the autotuner)")
     ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[100, 500, 1000, 2000, 5000],
                     help="request rates of the serving measurement (none: skip)")

@@ -218,3 +218,51 @@ def test_gi_exp_accuracy():
     rel = np.abs(got - exact) / exact
     assert rel.max() < 3e-7, rel.max()
     assert lib.orc_gi_exp(-80.5) == 0.0 and lib.orc_gi_exp(0.0) == 1.0
+
+
+def _sat_axes(v, h, reduced):
+    """The nine edge-axis tests of the triangle/box overlap in numpy f32, per row: the reference's three-term dot
+    products, or the kernels' two-term form without the zero component."""
+    f = np.float32
+    v0, v1, v2 = v[:, 0], v[:, 1], v[:, 2]
+    e = [v1 - v0, v2 - v1, v0 - v2]
+    ok = np.ones(len(v), bool)
+    for k in range(3):              # axis (1,0,0) x e, (0,1,0) x e, (0,0,1) x e
+        for ei in e:
+            a = np.zeros_like(ei)
+            i, j = [(1, 2), (0, 2), (0, 1)][k]
+            if k == 0:
+                a[:, 1], a[:, 2] = -ei[:, 2], ei[:, 1]
+            elif k == 1:
+                a[:, 0], a[:, 2] = ei[:, 2], -ei[:, 0]
+            else:
+                a[:, 0], a[:, 1] = -ei[:, 1], ei[:, 0]
+            if reduced:
+                p = [vi[:, i] * a[:, i] + vi[:, j] * a[:, j] for vi in (v0, v1, v2)]
+                r = h[:, i] * np.abs(a[:, i]) + h[:, j] * np.abs(a[:, j])
+            else:
+                p = [(vi[:, 0] * a[:, 0] + vi[:, 1] * a[:, 1]) + vi[:, 2] * a[:, 2] for vi in (v0, v1, v2)]
+                r = (h[:, 0] * np.abs(a[:, 0]) + h[:, 1] * np.abs(a[:, 1])) + h[:, 2] * np.abs(a[:, 2])
+            lo = np.minimum(np.minimum(p[0], p[1]), p[2])
+            hi = np.maximum(np.maximum(p[0], p[1]), p[2])
+            ok &= ~((lo > r) | (hi < -r))
+            assert all(x.dtype == f for x in p)
+    return ok
+
+
+def test_sat_edge_axes_without_zero_terms_decide_the_same():
+    """The kernels' edge-axis tests drop each axis's zero component; on random, axis-aligned and grid-snapped
+    triangles against voxel boxes they decide exactly as the three-term form."""
+    rng = np.random.default_rng(11)
+    n = 400000
+    c = (np.floor(rng.uniform(-50, 50, (n, 1, 3))) * 0.1 + 0.05).astype(np.float32)
+    tri = rng.uniform(-0.3, 0.3, (n, 3, 3)).astype(np.float32)
+    snap = rng.random(n) < 0.5      # vertices on the 0.05 grid: many zero edges and products
+    tri[snap] = (np.round(tri[snap] / 0.05) * 0.05).astype(np.float32)
+    flat = rng.integers(0, 3, n)    # axis-aligned triangles
+    tri[np.arange(n), :, flat] = tri[np.arange(n), :1, flat]
+    v = (c + tri).astype(np.float32) - c
+    h = np.full((n, 3), np.float32(0.05 * 1.0001), np.float32)
+    full, red = _sat_axes(v, h, False), _sat_axes(v, h, True)
+    assert np.array_equal(full, red)
+    assert 0.05 < full.mean() < 0.95
