@@ -39,18 +39,27 @@ def workload(name):
         p = configs.parse_config("screen-8-voxel-f32-dda256", {"cascades": 5})
         v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
         sun_e, sky = s.sun_e, s.sky
+        shadow = fr.SHADOW_SIZE   # the sun's shadow map over the scene (voxSun in every rebuild)
     else:
         s = scenes.room_scene(0)
         W, H = 256, 256
         p = configs.parse_config("screen-8-voxel-f32-dda64", {"cascades": 2})
         v = configs.vox_params({"v0": 0.16, "levels": 1, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 18})
         sun_e, sky = (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
+        shadow = 0                # sun off
+    lvp, bias = [0.0] * 16, (0.0, 0.0)
+    if shadow:
+        bmin, bmax = fr.scene_bounds(s.positions)
+        lvp, bias = fr.scene_sun_view_proj(bmin, bmax, s.sun_dir), fr.SHADOW_BIAS
     F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=sun_e, sky=sky,
-                                     cascades=p.cascades, P=p.P))
+                                     cascades=p.cascades, P=p.P, light_view_proj=lvp, shadow_bias=bias))
     desc = {"workload": f"{name}: {s.triangle_count} triangles, clipmap {v.levels} x {v.G * 8}^3 voxels from "
                         f"{v.v0} m, {p.cascades} cascades at {W}x{H}, DDA cap {p.ddaCap}, atlas {p.atlas}",
             "triangles": s.triangle_count, "resolution": [W, H], "cascades": p.cascades, "levels": v.levels,
-            "G": v.G, "v0": v.v0, "dda_cap": p.ddaCap, "atlas": p.atlas, "method": "screen-8-voxel"}
+            "G": v.G, "v0": v.v0, "dda_cap": p.ddaCap, "atlas": p.atlas, "method": "screen-8-voxel",
+            "shadow_map": shadow}
+    if shadow:
+        desc["workload"] += f", sun shadow map {shadow}^2"
     return s, W, H, p, v, F, desc
 
 
@@ -137,20 +146,23 @@ def trace_algorithmic_bytes(rc_layout, hdr, vox):
             + 68 * nb + 20 * nv)
 
 
-def cpu_solve_once(bind, s, v, lay, F, depth, normal):
+def cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow=None):
     st = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, s.camera.eye)
+    if shadow is not None:
+        bind.vox_sun(st, F, shadow)
     bind.rc_solve(st, lay, F, depth, normal)
 
 
-def cpu_baseline(s, v, p, F, depth, normal, budget_s=12.0, min_solves=2):
+def cpu_baseline(s, v, p, F, depth, normal, shadow_size=0, budget_s=12.0, min_solves=2):
     """The oracle (a CPU restatement of the reference's shaders) timed on this host's cores, bounded sample."""
     from oracle import bind
     from rtgi import configs
     lay = configs.cascade_layout(p, depth.shape[1], depth.shape[0])
-    cpu_solve_once(bind, s, v, lay, F, depth, normal)   # warm
+    shadow = bind.shadow_render(s, F, shadow_size) if shadow_size else None   # an input, as the G-buffer
+    cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow)   # warm
     n, t0 = 0, time.perf_counter()
     while n < min_solves or time.perf_counter() - t0 < budget_s:
-        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+        cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow)
         n += 1
     dt = time.perf_counter() - t0
     cores = int(os.environ.get("ORC_THREADS", os.cpu_count() or 1))
@@ -280,19 +292,20 @@ def run_reference(args, rank):
     from oracle import bind
     from rtgi import configs
     s, W, H, p, v, F, desc = workload(args.workload)
-    depth, normal, _ = bind.raster_gbuffer(s, F, W, H)   # input, not timed
+    depth, normal, _ = bind.raster_gbuffer(s, F, W, H)   # inputs, not timed
+    shadow = bind.shadow_render(s, F, desc["shadow_map"]) if desc["shadow_map"] else None
     lay = configs.cascade_layout(p, W, H)
     for _ in range(args.warmup):
-        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+        cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow)
     # a bounded sample: at most ~90 s of solves
     t_one = time.perf_counter()
-    cpu_solve_once(bind, s, v, lay, F, depth, normal)
+    cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow)
     t_one = time.perf_counter() - t_one
     k = max(1, min(args.steps, int(90.0 / max(t_one, 1e-3))))
     times = []
     for _ in range(k):
         t0 = time.perf_counter()
-        cpu_solve_once(bind, s, v, lay, F, depth, normal)
+        cpu_solve_once(bind, s, v, lay, F, depth, normal, shadow)
         times.append(time.perf_counter() - t0)
     total = sum(times)
     value = k / total
@@ -349,6 +362,15 @@ def run_ours(args, rank, world, local_rank):
     with torch.cuda.stream(stream):
         rc.set_frame(F, stream)
         rc.render_gbuffer(sg, stream)
+        shadow_ms = None
+        if desc["shadow_map"]:   # an input of the solve, as the G-buffer: drawn once (static scene and sun)
+            rc.render_shadow(sg, desc["shadow_map"], stream)   # warm
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            rc.render_shadow(sg, desc["shadow_map"], stream)
+            e1.record(stream)
+            stream.synchronize()
+            shadow_ms = e0.elapsed_time(e1)
         vw.update(s.camera.eye)
         # DDA work of one solve (steps counted as rc.ts:232-235)
         rc.set_stats(1)
@@ -416,7 +438,8 @@ def run_ours(args, rank, world, local_rank):
     depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
     normal_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_NORMAL).view(np.uint16).copy()).pin_memory()
     frame_h = torch.from_numpy(F.copy()).pin_memory()
-    pipe = pipeline.FramePipeline(ctx, vw, p, W, H, F, depth_h.data_ptr(), normal_h.data_ptr(), slots=2)
+    pipe = pipeline.FramePipeline(ctx, vw, p, W, H, F, depth_h.data_ptr(), normal_h.data_ptr(), slots=2,
+                                  shadow=(sg, desc["shadow_map"]) if desc["shadow_map"] else None)
     irr_h = [torch.empty(pipe.irr_bytes, dtype=torch.uint8).pin_memory() for _ in range(2)]
     n_e2e = max(3, min(n_ev, 400))
     for k in range(4):
@@ -456,6 +479,7 @@ def run_ours(args, rank, world, local_rank):
                "dda_steps_per_solve": steps_per_solve, "dda_at_cap": at_cap,
                "dda_steps_per_s": steps_per_solve * value,
                "passes_ms": {k: statistics.median(x) for k, x in pass_ms.items()},
+               "shadow_map_ms": shadow_ms,
                "vox_counters": {"bricks": int(min(hdr[0], v.maxBricks)), "voxels": int(hdr[1]),
                                 "bricksPerLevel": [int(x) for x in hdr[8:8 + v.levels]]},
                "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -482,7 +506,8 @@ def run_ours(args, rank, world, local_rank):
     # the oracle on the host cores, rank 0 at N = 1 only
     if rank == 0 and world == 1 and not args.no_cpu:
         out["cpu_baseline"] = cpu_baseline(s, v, p, F, depth_h.numpy().reshape(H, W),
-                                           normal_h.numpy().view(np.float16).reshape(H, W, 4).astype(np.float32))
+                                           normal_h.numpy().view(np.float16).reshape(H, W, 4).astype(np.float32),
+                                           desc["shadow_map"])
     for h in (rc, vw, sg, ctx):
         h.destroy()
     if dist:

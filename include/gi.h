@@ -169,6 +169,13 @@ int gi_rc_set_gbuffer(gi_rc *rc, const float *depth, const float *normal4, void 
 int gi_rc_set_gbuffer_f16(gi_rc *rc, const float *depth, const uint16_t *normal_rgba16f, void *stream);
 /* G-buffer drawn on the device from the scene and the frame (one primary-ray sample per pixel centre). */
 int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
+/* The sun shadow map (encodeShadow, lighting.ts:175-189; depth32float, compare less, depth bias 2 + slope 2, cull
+ * none) drawn on the device from the frame's lightViewProj (words 64-79) over the scene's triangles: size x size
+ * f32 depths owned by the rc, 1 where nothing is drawn.  While the rc holds one, gi_solve's rebuild also runs voxSun
+ * (voxel.ts:633-671) with it, the frame's sun direction and shadow bias (word 157); without one every voxel's sun
+ * visibility is 1.  size 0 releases it.  Draw it again when the light matrix or the scene moves; a graph captured
+ * before a change of size must be captured again. */
+int gi_rc_render_shadow(gi_rc *rc, gi_scene *scene, uint32_t size, void *stream);
 /* encode(enc) (rc.ts:1169-1222): giBuild (setupScreen), giTrace, giMerge (mergeScreen N-1..0, projectSH),
  * giGather (gatherScreen) over the voxel world's current state. */
 int gi_rc_solve(gi_rc *rc, gi_vox *vox, void *stream);
@@ -223,7 +230,8 @@ enum {
   GI_RC_DEPTH = 3,      /* W*H f32 */
   GI_RC_NORMAL = 4,     /* W*H*4 halves */
   GI_RC_HITS = 5,       /* per ray: level, brick, bit, tIn bits (only after gi_rc_set_debug_hits(rc, 1)) */
-  GI_RC_RAD_TRACED = 6  /* the atlas right after the trace, before the merge (only with debug hits on) */
+  GI_RC_RAD_TRACED = 6, /* the atlas right after the trace, before the merge (only with debug hits on) */
+  GI_RC_SHADOW = 7      /* size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
 };
 int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
 int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);

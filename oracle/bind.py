@@ -51,6 +51,10 @@ def lib():
         _lib.orc_tri_box.restype = C.c_int
         _lib.orc_round_log2.argtypes = [C.c_float]
         _lib.orc_round_log2.restype = C.c_uint32
+        _lib.orc_shadow_render.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.orc_sun_tap.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
+        _lib.orc_sun_tap.restype = C.c_float
+        _lib.orc_vox_sun.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
         _lib.orc_gi_exp.argtypes = [C.c_float]
         _lib.orc_gi_exp.restype = C.c_float
     return _lib
@@ -226,3 +230,27 @@ def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int):
     if r != 0:
         raise MemoryError("oracle raster: out of memory")
     return depth, normal, tri
+
+
+def shadow_render(scene, frame: np.ndarray, S: int) -> np.ndarray:
+    """The sun shadow map (S x S depths, 1 = nothing drawn) from the frame's lightViewProj."""
+    s, keep = _scene_struct(scene)
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    out = np.zeros((S, S), np.float32)
+    lib().orc_shadow_render(C.byref(s), _p(frame), S, _p(out))
+    return out
+
+
+def sun_tap(frame: np.ndarray, shadow: np.ndarray, x) -> float:
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    shadow = np.ascontiguousarray(shadow, dtype=np.float32)
+    p = np.ascontiguousarray(x, dtype=np.float32)
+    return float(lib().orc_sun_tap(_p(frame), _p(shadow), shadow.shape[0], _p(p)))
+
+
+def vox_sun(vox: dict, frame: np.ndarray, shadow: np.ndarray) -> None:
+    """voxSun over a built world (vox from vox_build): fills vox['sunvis'] in place."""
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    shadow = np.ascontiguousarray(shadow, dtype=np.float32)
+    vx = _vox_struct(vox)
+    lib().orc_vox_sun(C.byref(vx), _p(frame), _p(shadow), shadow.shape[0])

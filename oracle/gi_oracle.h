@@ -12,6 +12,7 @@
  *     gather
  *   - the headless G-buffer raster         src/core/gbuffer.ts:82-103 (conventions only; the reference draws it
  *                                          with a graphics pipeline, restated here as a scanline raster)
+ *   - the sun shadow map and voxSun        src/core/lighting.ts:133-189, frame.ts:35-52, voxel.ts:633-671
  *
  * Arithmetic follows the WGSL expression order exactly (left-associative, no contraction: build with
  * -ffp-contract=off).  Where the WGSL leaves a builtin implementation-defined, the choice made here is stated
@@ -132,6 +133,16 @@ int orc_rc_merge_gather_f64(const orc_layout *ly, const orc_gbuf *g, const orc_p
  * tri_out (optional) receives the winning triangle per pixel (0xffffffff: none). */
 int orc_raster_gbuffer(const orc_scene *s, const float *frame, uint32_t width, uint32_t height, float *depth_out,
                        float *normal_out, uint32_t *tri_out);
+
+/* Sun shadow map (lighting.ts:133-140, 175-189, restated as a per-texel-centre raster of the light's orthographic
+ * clip space; the rules are stated in shadow.c): S*S depths, 1 where nothing is drawn, from the frame's
+ * lightViewProj (frame words 64-79). */
+int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float *map);
+/* shadowTap (frame.ts:47-52): the 'less-equal' comparison of x's biased light depth (frame word 157) with the map,
+ * bilinear over the four texels around it; 1 outside the map. */
+float orc_sun_tap(const float *frame, const float *map, uint32_t S, const float x[3]);
+/* voxSun (voxel.ts:633-671): the sun visibility of every occupied voxel of a built world (after orc_vox_build). */
+int orc_vox_sun(orc_vox *vx, const float *frame, const float *map, uint32_t S);
 
 /* WGSL builtins as the oracle defines them (exported for the known-answer tests). */
 uint32_t orc_pack4x8unorm(const float v[4]);

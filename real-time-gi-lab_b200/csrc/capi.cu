@@ -126,6 +126,11 @@ struct gi_rc {
   RcLaunch launch = {8u, 3u, 256u};   // gi_rc_tuning launch shapes
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
+  float *shadow = nullptr;           // gi_rc_render_shadow: shadow_size^2 depths
+  uint32_t shadow_size = 0;
+  float4 *sm_rec = nullptr;          // its raster scratch, for up to sm_tris triangles
+  uint32_t *sm_pre = nullptr, *sm_sums = nullptr, *sm_counter = nullptr;
+  uint32_t sm_tris = 0;
 };
 
 static void free_scene(gi_scene *s) {
@@ -149,6 +154,7 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
   cudaFree((void *)r->dev.unorm8);
+  cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
 }
 
 extern "C" {
@@ -394,13 +400,18 @@ int gi_vox_update(gi_vox *v, const double eye[3]) {
   return GI_OK;
 }
 
-int gi_vox_build(gi_vox *v, void *stream) {
+// The rebuild, with voxSun from a shadow map when one is given (gi_solve passes the rc's)
+static int vox_build_sun(gi_vox *v, const float *frame, const float *shadow, uint32_t size, void *stream) {
   if (!v) return fail(GI_ERR_INVALID, "gi_vox_build: NULL vox");
   if (!v->updated) return fail(GI_ERR_STATE, "gi_vox_build: gi_vox_update was not called");
   CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_build: cudaSetDevice");
-  CK(gi_launch_vox_build(v->dev, v->scene->dev(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
+  VoxDev d = v->dev;
+  d.sun_frame = frame; d.shadow = shadow; d.shadow_size = shadow ? size : 0u;
+  CK(gi_launch_vox_build(d, v->scene->dev(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
   return GI_OK;
 }
+
+int gi_vox_build(gi_vox *v, void *stream) { return vox_build_sun(v, nullptr, nullptr, 0u, stream); }
 
 int gi_vox_read_counters(gi_vox *v, uint32_t hdr[64], void *stream) {
   if (!v || !hdr) return fail(GI_ERR_INVALID, "gi_vox_read_counters: NULL argument");
@@ -637,6 +648,42 @@ int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   return GI_OK;
 }
 
+int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
+  if (!r || !s) return fail(GI_ERR_INVALID, "gi_rc_render_shadow: NULL argument");
+  if (size > 16384u) return fail(GI_ERR_INVALID, "gi_rc_render_shadow: size %u (at most 16384)", size);
+  if (s->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_render_shadow: scene on another device");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_render_shadow: cudaSetDevice");
+  if (size == 0) {
+    cudaFree(r->shadow);
+    r->shadow = nullptr;
+    r->shadow_size = 0;
+    return GI_OK;
+  }
+  if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_render_shadow: no frame set");
+  cudaError_t e;
+  if (size != r->shadow_size) {
+    cudaFree(r->shadow);
+    r->shadow = nullptr;
+    r->shadow_size = 0;
+    if ((e = dalloc(&r->shadow, (size_t)size * size))) return cuda_fail(e, "gi_rc_render_shadow");
+    r->shadow_size = size;
+  }
+  uint32_t nt = s->ntris;
+  if (nt > r->sm_tris || !r->sm_counter) {
+    cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
+    r->sm_rec = nullptr; r->sm_pre = r->sm_sums = r->sm_counter = nullptr; r->sm_tris = 0;
+    size_t cap = nt ? nt : 1u;
+    if ((e = dalloc(&r->sm_rec, 4u * cap)) || (e = dalloc(&r->sm_pre, cap)) || (e = dalloc(&r->sm_sums, (cap + 255u) / 256u)) ||
+        (e = dalloc(&r->sm_counter, 4)))
+      return cuda_fail(e, "gi_rc_render_shadow");
+    r->sm_tris = (uint32_t)cap;
+  }
+  ShadowRaster sr;
+  sr.map = r->shadow; sr.rec = r->sm_rec; sr.pre = r->sm_pre; sr.sums = r->sm_sums; sr.counter = r->sm_counter;
+  CK(gi_launch_shadow(s->dev(), r->frame, size, sr, r->ctx->sm_count, S(stream)), "gi_rc_render_shadow: launch");
+  return GI_OK;
+}
+
 int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   if (!r || !v) return fail(GI_ERR_INVALID, "gi_rc_solve: NULL argument");
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_solve: no frame set");
@@ -659,7 +706,7 @@ int gi_solve(gi_rc *r, gi_vox *v, void *stream) {
     CK(cudaSetDevice(r->ctx->device), "gi_solve: cudaSetDevice");
     CK(cudaEventRecord(r->ev[0], S(stream)), "gi_solve: event");
   }
-  int st = gi_vox_build(v, stream);
+  int st = vox_build_sun(v, r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, stream);
   if (st != GI_OK) return st;
   st = gi_rc_solve(r, v, stream);
   r->timed_vox = st == GI_OK && r->timing;
@@ -970,6 +1017,7 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
     case GI_RC_DEPTH: *bytes = npx * 4u; break;
     case GI_RC_NORMAL: *bytes = npx * 8u; break;
     case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;
+    case GI_RC_SHADOW: *bytes = (size_t)r->shadow_size * r->shadow_size * 4u; break;
     default: return fail(GI_ERR_INVALID, "gi_rc_buffer_bytes: unknown buffer %d", what);
   }
   return GI_OK;
@@ -990,8 +1038,9 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
     case GI_RC_NORMAL: src = r->normal; break;
     case GI_RC_HITS: src = r->hits; break;
     case GI_RC_RAD_TRACED: src = r->rad_traced; break;
+    case GI_RC_SHADOW: src = r->shadow; break;
   }
-  if (!src) return fail(GI_ERR_STATE, "gi_rc_read_buffer: buffer %d not kept (enable gi_rc_set_debug_hits first)", what);
+  if (!src) return fail(GI_ERR_STATE, "gi_rc_read_buffer: buffer %d not kept (debug hits off, or no shadow map)", what);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_buffer: cudaSetDevice");
   CK(cudaMemcpyAsync(out, src, need, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_buffer: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_buffer: sync");

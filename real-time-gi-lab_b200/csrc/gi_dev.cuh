@@ -189,6 +189,11 @@ struct VoxDev {
   uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
   uint32_t *citem;     // build temporary (optional): the item of each chunk, citem_cap entries
   unsigned long long *look;   // build temporary: scan_cap + 1 words, the chained scans' ticket and block states
+  // voxSun (voxel.ts:633-671): with a shadow map, resolveAttr also writes each voxel's sun visibility from it and
+  // the frame block (lightViewProj, sun direction, shadow bias); without one the visibility is 1
+  const float *sun_frame;
+  const float *shadow;        // shadow_size^2 depths
+  uint32_t shadow_size, pad_sun;
 };
 
 __device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return v.vs[L]; }
@@ -236,6 +241,59 @@ __device__ __forceinline__ bool tri_box(f3 c, f3 h, f3 a, f3 b, f3 cc) {
 // Frame word offsets (frame.ts:4-21).
 enum { F_VP = 0, F_IVP = 16, F_EYE = 80, F_FWD = 84, F_SUN = 88, F_SUNE = 92, F_SKY = 96, F_SIZE = 100, F_RC = 104,
        F_RC2 = 108, F_RU = 112, F_RU2 = 116, F_OMEGA = 120, F_STYLE = 136 };
+
+enum { F_LVP = 64, F_SHADOW = 156 };   // lightViewProj; shadow layers, layer-0 bias, layer-1 bias
+
+// x's light clip coordinates, mat4 * vec4 summed in column order
+__device__ __forceinline__ f3 light_clip(const float *__restrict__ F, f3 x) {
+  const float *m = F + F_LVP;
+  return mk(m[0] * x.x + m[4] * x.y + m[8] * x.z + m[12] * 1.0f, m[1] * x.x + m[5] * x.y + m[9] * x.z + m[13] * 1.0f,
+            m[2] * x.x + m[6] * x.y + m[10] * x.z + m[14] * 1.0f);
+}
+
+// shadowCoord (frame.ts:35-46, one layer) + textureSampleCompareLevel with the 'less-equal' comparison sampler
+// (linear, clamp-to-edge; lighting.ts:162): the four texels around x's map position compared with its biased light
+// depth and weighted bilinearly in f32; 1 (lit) outside the map.
+__device__ __forceinline__ float sun_tap(const float *__restrict__ F, const float *__restrict__ map, uint32_t S, f3 x) {
+  f3 c = light_clip(F, x);
+  float u = c.x * 0.5f + 0.5f, v = c.y * -0.5f + 0.5f;
+  if (!(u >= 0.0f && v >= 0.0f && u <= 1.0f && v <= 1.0f)) return 1.0f;
+  float ref = c.z - F[F_SHADOW + 1];
+  float tx = u * (float)S - 0.5f, ty = v * (float)S - 0.5f;
+  float fx = floorf(tx), fy = floorf(ty);
+  float ax = tx - fx, ay = ty - fy;
+  int i0 = f2i(fx), j0 = f2i(fy), n = (int)S - 1;
+  int ia = iclamp(i0, 0, n), ib = iclamp(i0 + 1, 0, n), ja = iclamp(j0, 0, n), jb = iclamp(j0 + 1, 0, n);
+  float c00 = ref <= __ldg(&map[(size_t)ja * S + ia]) ? 1.0f : 0.0f, c10 = ref <= __ldg(&map[(size_t)ja * S + ib]) ? 1.0f : 0.0f;
+  float c01 = ref <= __ldg(&map[(size_t)jb * S + ia]) ? 1.0f : 0.0f, c11 = ref <= __ldg(&map[(size_t)jb * S + ib]) ? 1.0f : 0.0f;
+  return (c00 * (1.0f - ax) + c10 * ax) * (1.0f - ay) + (c01 * (1.0f - ax) + c11 * ax) * ay;
+}
+
+// voxSun (voxel.ts:643-671) of one voxel: centre pc, size vs, packed oct normal and plane offset as resolveAttr stored
+// them.  The mean of four taps a quarter voxel from the centre's projection on the plane, along two tangents, lifted
+// (0.25 voxel + 3 cm) to the sunward side.
+__device__ __forceinline__ float voxel_sun(const float *__restrict__ F, const float *__restrict__ map, uint32_t S, f3 pc,
+                                           float vs, uint32_t npack, float plane) {
+  // unpack2x16snorm: k / 32767 as the f64 product rounded to f32 (the f32 quotient for every 16-bit k)
+  const double inv32767 = 1.0 / 32767.0;
+  float ex = mx(__double2float_rn((double)(int16_t)(npack & 0xffffu) * inv32767), -1.0f);
+  float ey = mx(__double2float_rn((double)(int16_t)(npack >> 16) * inv32767), -1.0f);
+  f3 n = mk(ex, ey, 1.0f - fabsf(ex) - fabsf(ey));
+  float q0 = mx(-n.z, 0.0f);
+  n.x += n.x >= 0.0f ? -q0 : q0;
+  n.y += n.y >= 0.0f ? -q0 : q0;
+  f3 q = pc;
+  if (dot(n, n) > 1e-4f) { n = normalize3(n); q = pc + n * plane; }
+  else n = mk(0.0f, 1.0f, 0.0f);
+  f3 ns = dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])) < 0.0f ? -n : n;
+  f3 t1 = normalize3(cross(ns, fabsf(ns.y) > 0.9f ? mk(1.0f, 0.0f, 0.0f) : mk(0.0f, 1.0f, 0.0f)));
+  f3 t2 = cross(ns, t1);
+  float h = 0.25f * vs;
+  f3 o = q + ns * (0.25f * vs + 0.03f);
+  f3 sp = t1 + t2, sm = t1 - t2;
+  return 0.25f * (((sun_tap(F, map, S, o + sp * h) + sun_tap(F, map, S, o + sm * h)) + sun_tap(F, map, S, o - sp * h))
+                  + sun_tap(F, map, S, o - sm * h));
+}
 
 // worldAt (frame.ts:22-26), mat4 * vec4 summed in column order
 __device__ __forceinline__ f3 world_at(const float *__restrict__ F, int px, int py, float d) {

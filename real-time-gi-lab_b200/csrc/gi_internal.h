@@ -57,6 +57,13 @@ struct RasterDev {
   uint32_t list_cap, ntiles;
 };
 
+// Sun shadow-map raster scratch (shadow.cu) and its output
+struct ShadowRaster {
+  float *map;                      // S x S depths
+  float4 *rec;                     // 4 per triangle: (c0, bias), (c1, i0 | j0 << 16), (c2, bw | bh << 16), unused
+  uint32_t *pre, *sums, *counter;  // per triangle chunk prefix within its block; block offsets; [0] chunk total
+};
+
 // Per-level constants of a voxel world computed once on the host with the same f32 operations the kernels would do:
 // the voxel size ldexpf(v0, L) (a power-of-two scaling, exact) and voxRange's cell limit f2i(G * size * 8 / cell)
 // (voxel.ts:295) for voxel cells (cell = size) and brick cells (cell = size * 8).  Call after v0 and G are set.
@@ -79,6 +86,8 @@ inline void vox_derived(VoxDev &d) {
 }  // namespace gi
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
+cudaError_t gi_launch_shadow(const gi::SceneDev &s, const float *frame_dev, uint32_t S, const gi::ShadowRaster &sr,
+                             uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
 // Kernel launch with programmatic dependent launch allowed: the next kernel in the stream (or graph) may be scheduled
 // while this one's last blocks drain, hiding the launch gap between dependent kernels.  Every kernel launched this

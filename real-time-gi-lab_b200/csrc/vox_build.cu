@@ -694,7 +694,7 @@ __device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
 
 // resolveAttr (voxel.ts:596-620): one thread per voxel of the attribute pool (voxel ai of brick b is rank
 // ai - vpre[b] of b's occupancy), so every occupied voxel is resolved in parallel and the attribute writes are
-// contiguous.
+// contiguous.  With a shadow map the same thread runs voxSun (the reference's next stage) on what it stored.
 __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
   grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
@@ -733,7 +733,8 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
     f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vox_size(v, L);
     uint32_t rv = v.rep[ptr * 512u + bit];
     if (rv == 0u || rv > s.ntris) {   // no representative (cannot happen for a set bit): no attributes
-      v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f; v.sunvis[ai] = 1.0f;
+      v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f;
+      v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, p, vox_size(v, L), 0u, 0.0f) : 1.0f;
       continue;
     }
     Tri T = load_tri(s, rv - 1u);
@@ -760,8 +761,10 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
     rec.z = (uint32_t)f2h(m.emissive[0]) | ((uint32_t)f2h(m.emissive[1]) << 16);
     rec.w = (uint32_t)f2h(m.emissive[2]);
     v.attr[ai] = rec;
-    v.plane[ai] = dot(n, q - p);
-    v.sunvis[ai] = 1.0f;
+    float pl = dot(n, q - p);
+    v.plane[ai] = pl;
+    // voxSun (voxel.ts:633-671) from the values just stored
+    v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, p, vox_size(v, L), rec.y, pl) : 1.0f;
   }
 }
 

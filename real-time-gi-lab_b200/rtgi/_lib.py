@@ -11,7 +11,7 @@ LIB_PATH = os.path.join(PKG, "lib", "libgi_b200.so")
 
 GI_OK, GI_ERR_INVALID, GI_ERR_OOM, GI_ERR_CUDA, GI_ERR_TIMEOUT, GI_ERR_OVERFLOW, GI_ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 GI_ATLAS_F32, GI_ATLAS_F16, GI_ATLAS_BF16 = 0, 1, 2
-GI_RC_PROBES, GI_RC_RAD, GI_RC_SH, GI_RC_DEPTH, GI_RC_NORMAL, GI_RC_HITS, GI_RC_RAD_TRACED = range(7)
+GI_RC_PROBES, GI_RC_RAD, GI_RC_SH, GI_RC_DEPTH, GI_RC_NORMAL, GI_RC_HITS, GI_RC_RAD_TRACED, GI_RC_SHADOW = range(8)
 
 # Every symbol include/gi.h declares, with its ctypes signature (restype, argtypes).
 _P = C.c_void_p
@@ -40,6 +40,7 @@ SIGNATURES = {
     "gi_rc_set_gbuffer": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_set_gbuffer_f16": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_render_gbuffer": (C.c_int, [_P, _P, _P]),
+    "gi_rc_render_shadow": (C.c_int, [_P, _P, C.c_uint32, _P]),
     "gi_rc_solve": (C.c_int, [_P, _P, _P]),
     "gi_solve": (C.c_int, [_P, _P, _P]),
     "gi_rc_read_irradiance": (C.c_int, [_P, _P, _P]),

@@ -22,6 +22,27 @@ F_VIEWPROJ, F_INVVIEWPROJ, F_EYE, F_FWD, F_SUNDIR, F_SUNE, F_SKY, F_SIZE = 0, 16
 F_RC, F_RC2, F_RU, F_RU2, F_OMEGA, F_STYLE = 104, 108, 112, 116, 120, 136
 
 
+SHADOW_SIZE = 4096               # createLighting's shadowSize (lighting.ts:113)
+SHADOW_BIAS = (0.0002, 0.0)      # one layer: the comparison bias of layer 0 (lighting.ts:134)
+
+
+def scene_sun_view_proj(bounds_min, bounds_max, sun_dir) -> list:
+    """sceneSunViewProj (lighting.ts:100-106): the sun's orthographic view-projection over the scene's bounding
+    sphere, depth 0 on the sunward side of the sphere and 1 on the far side."""
+    center = mathx.scale3(mathx.add3(bounds_min, bounds_max), 0.5)
+    radius = mathx.hypot(*mathx.sub(bounds_max, bounds_min)) / 2
+    d = mathx.scale3(sun_dir, 1 / mathx.hypot(*sun_dir))
+    up = [0, 0, 1] if abs(d[1]) > 0.99 else [0, 1, 0]
+    return mathx.mat_mul(mathx.ortho_zo(radius, radius, 0, 2 * radius),
+                         mathx.look_at(mathx.add3(center, mathx.scale3(d, radius)), center, up))
+
+
+def scene_bounds(positions) -> tuple:
+    """boundsMin / boundsMax (gltf.ts:147) of f32 vertex positions, as f64 values."""
+    p = np.asarray(positions, dtype=np.float32)
+    return [float(x) for x in p.min(axis=0)], [float(x) for x in p.max(axis=0)]
+
+
 @dataclass
 class Camera:
     eye: tuple

@@ -204,6 +204,16 @@ class Rc:
     def render_gbuffer(self, scene: SceneGpu, stream=None):
         _lib.call("gi_rc_render_gbuffer", self.handle, scene.handle, _stream(stream))
 
+    def render_shadow(self, scene: SceneGpu, size: int = 4096, stream=None):
+        """The sun shadow map from the frame's lightViewProj (encodeShadow, lighting.ts:175-189); while it is held,
+        solves run voxSun with it.  size 0 releases it."""
+        _lib.call("gi_rc_render_shadow", self.handle, scene.handle, int(size), _stream(stream))
+        self.shadow_size = int(size)
+
+    def read_shadow(self, stream=None) -> np.ndarray:
+        S = getattr(self, "shadow_size", 0)
+        return self.read_buffer(_lib.GI_RC_SHADOW, stream).view(np.float32).reshape(S, S)
+
     def encode(self, vox: VoxWorld, stream=None):
         _lib.call("gi_rc_solve", self.handle, vox.handle, _stream(stream))
 

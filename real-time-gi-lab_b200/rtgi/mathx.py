@@ -99,6 +99,12 @@ def look_at(eye: Vec3, target: Vec3, up: Vec3) -> list[float]:
     return [f32(v) for v in vals]
 
 
+def ortho_zo(half_w: float, half_h: float, near: float, far: float) -> list[float]:
+    """orthoZO (math.ts:102-109): depth 0 at near, 1 at far."""
+    return [f32(v) for v in [1 / half_w, 0, 0, 0, 0, 1 / half_h, 0, 0, 0, 0, -1 / (far - near), 0, 0, 0,
+                             -near / (far - near), 1]]
+
+
 def perspective_reversed_infinite(fov_y: float, aspect: float, near: float) -> list[float]:
     """perspectiveReversedInfinite (math.ts:37-45): depth 1 at the near plane, 0 at infinity."""
     f = 1 / math.tan(fov_y / 2)

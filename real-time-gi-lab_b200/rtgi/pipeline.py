@@ -16,9 +16,10 @@ from . import gpu
 
 class FramePipeline:
     def __init__(self, ctx: gpu.Context, vox: gpu.VoxWorld, params, width: int, height: int, frame, depth_ptr: int,
-                 normal_f16_ptr: int, slots: int = 2):
+                 normal_f16_ptr: int, slots: int = 2, shadow=None):
         """frame/depth/normal: a first frame's inputs (frame as an array, the G-buffer as pinned host pointers), used
-        to capture each slot's graph."""
+        to capture each slot's graph.  shadow: (SceneGpu, size) to give every slot the sun's shadow map drawn from
+        that frame (a static sun and scene; draw it again with Rc.render_shadow when they move)."""
         import torch
         self.torch = torch
         self.vox = vox
@@ -28,6 +29,8 @@ class FramePipeline:
             rc = gpu.Rc(ctx, params, width, height)
             rc.set_frame(frame, self.comp)
             rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.comp)
+            if shadow is not None:
+                rc.render_shadow(shadow[0], shadow[1], self.comp)
             rc.graph_capture(vox, self.comp)
             self.rcs.append(rc)
         self.uploaded = [torch.cuda.Event() for _ in range(slots)]

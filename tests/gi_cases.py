@@ -18,13 +18,18 @@ class Case:
     vox: configs.VoxParams
     rc: configs.RcParams
     frame: np.ndarray = field(default=None)
+    shadow: int = 0          # sun shadow map size (0: none, every voxel's sun visibility 1)
 
 
-def _frame(scene, W, H, p: configs.RcParams, sun_e=None, sky=None):
+def _frame(scene, W, H, p: configs.RcParams, sun_e=None, sky=None, shadow=False):
+    lvp, bias = [0.0] * 16, (0.0, 0.0)
+    if shadow:   # the sun's view-projection over the scene bounds (lighting.ts:100-106), one layer
+        bmin, bmax = fr.scene_bounds(scene.positions)
+        lvp, bias = fr.scene_sun_view_proj(bmin, bmax, scene.sun_dir), fr.SHADOW_BIAS
     return fr.pack_frame(fr.FrameParams(cam=scene.camera, width=W, height=H, sun_dir=scene.sun_dir,
                                         sun_e=scene.sun_e if sun_e is None else sun_e,
                                         sky=scene.sky if sky is None else sky, cascades=p.cascades, P=p.P,
-                                        s_min=p.sMin, lift=p.lift))
+                                        s_min=p.sMin, lift=p.lift, light_view_proj=lvp, shadow_bias=bias))
 
 
 def config0(atlas: str = "f32") -> Case:
@@ -38,12 +43,13 @@ def config0(atlas: str = "f32") -> Case:
 
 
 def config1(atlas: str = "f32", width: int = 1920, height: int = 1080) -> Case:
-    """Colonnade of ~260k triangles, 4 levels of 128^3 voxels from 0.1 m, 1920x1080, 5 cascades, DDA cap 256."""
+    """Colonnade of ~260k triangles, 4 levels of 128^3 voxels from 0.1 m, 1920x1080, 5 cascades, DDA cap 256, the
+    sun's 4096^2 shadow map (voxSun)."""
     s = scenes.colonnade_scene(0)
     p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": 5})
     v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
-    c = Case("config1", s, width, height, v, p)
-    c.frame = _frame(s, width, height, p)
+    c = Case("config1", s, width, height, v, p, shadow=fr.SHADOW_SIZE)
+    c.frame = _frame(s, width, height, p, shadow=True)
     return c
 
 
@@ -64,6 +70,14 @@ def leak(t: float = 0.1, atlas: str = "bf16") -> Case:
     v = configs.vox_params({"v0": 0.1, "levels": 5, "G": 64, "maxBricks": 32768, "maxVoxels": 4194304})
     c = Case(f"leak-{t}", s, 320, 180, v, p)
     c.frame = _frame(s, 320, 180, p, sun_e=fr.SUN_E, sky=fr.SKY)
+    return c
+
+
+def leak_sun(t: float = 0.1, atlas: str = "f32", size: int = 1024) -> Case:
+    """The leak room with the sun's shadow map (voxSun): sunlight through the openings only."""
+    c = leak(t, atlas)
+    c.name, c.shadow = f"leak-sun-{t}", size
+    c.frame = _frame(c.scene, c.width, c.height, c.rc, sun_e=fr.SUN_E, sky=fr.SKY, shadow=True)
     return c
 
 

@@ -43,6 +43,8 @@ def run_gpu(ctx, case, debug=True):
     rc = gpu.Rc(ctx, case.rc, case.width, case.height)
     rc.set_frame(case.frame)
     rc.render_gbuffer(sg)
+    if case.shadow:
+        rc.render_shadow(sg, case.shadow)
     vw.update(case.scene.camera.eye)
     rc.set_debug_hits(debug)
     rc.solve(vw)
@@ -51,6 +53,8 @@ def run_gpu(ctx, case, debug=True):
            "normal": rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4),
            "probes": rc.read_buffer(_lib.GI_RC_PROBES).view(bind.PROBE_DTYPE),
            "rad": rc.read_atlas(_lib.GI_RC_RAD), "sh": rc.read_atlas(_lib.GI_RC_SH)}
+    if case.shadow:
+        res["shadow"] = rc.read_shadow()
     if debug:
         res["hits"] = rc.read_buffer(_lib.GI_RC_HITS).view(np.uint32).reshape(-1, 4)
         res["rad_traced"] = rc.read_atlas(_lib.GI_RC_RAD_TRACED)
@@ -59,15 +63,18 @@ def run_gpu(ctx, case, debug=True):
     return res
 
 
-def run_oracle(case, depth, normal):
+def run_oracle(case, depth, normal, shadow=None):
     v = case.vox
     st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+    if shadow is not None:
+        bind.vox_sun(st, case.frame, shadow)
     lay = dict(gi_cases.configs.cascade_layout(case.rc, case.width, case.height))
     out = bind.rc_solve(st, lay, case.frame, depth, normal, want_hit=True)
     return st, out
 
 
 CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_cases.leak,
+         "leak_sun": gi_cases.leak_sun,
          "room_lit_f32out": lambda: gi_cases.room_lit("f16-f32out"),
          "overflow": gi_cases.overflow, "config1": gi_cases.config1}
 
@@ -80,7 +87,13 @@ def test_parity(ctx, name):
     depth, normal, _ = bind.raster_gbuffer(case.scene, case.frame, case.width, case.height)
     assert np.array_equal(g["depth"].view(np.uint32), depth.view(np.uint32)), "G-buffer depth differs"
     assert np.array_equal(g["normal"].astype(np.float32), normal), "G-buffer normal differs"
-    st, o = run_oracle(case, depth, normal)
+    shadow = None
+    if case.shadow:   # the sun shadow map, bit for bit
+        shadow = bind.shadow_render(case.scene, case.frame, case.shadow)
+        assert np.array_equal(g["shadow"].view(np.uint32), shadow.view(np.uint32)), \
+            f"shadow map differs at {(g['shadow'] != shadow).sum()} texels"
+        assert (shadow < 1.0).any()
+    st, o = run_oracle(case, depth, normal, shadow)
     # voxel world: every counter and every allocated word
     gv = g["vox"]
     assert np.array_equal(gv["hdr"], st["hdr"]), f"counters differ: {gv['hdr'][:32]} vs {st['hdr'][:32]}"
@@ -91,6 +104,10 @@ def test_parity(ctx, name):
         assert np.array_equal(gv[k][:n], st[k][:n]), f"{k} differs"
     assert np.array_equal(gv["attr"][:nv * 4], st["attr"][:nv * 4]), "voxel attributes differ"
     assert np.array_equal(gv["plane"][:nv].view(np.uint32), st["plane"][:nv].view(np.uint32)), "plane offsets differ"
+    if case.shadow:
+        assert np.array_equal(gv["sunvis"][:nv].view(np.uint32), st["sunvis"][:nv].view(np.uint32)), "sun visibility differs"
+        sv = st["sunvis"][:nv]
+        assert (sv == 0.0).any() and (sv == 1.0).any(), "the case should hold shadowed and lit voxels"
     # probes and DDA hits
     assert np.array_equal(g["probes"].view(np.uint32), o["probes"].view(np.uint32)), "probes differ"
     assert np.array_equal(g["hits"], o["hit"]), f"DDA hits differ at {np.argwhere((g['hits'] != o['hit']).any(1))[:5].ravel()}"
