@@ -314,9 +314,13 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
     }
    }
   }
-  if (r.stats && cur_c != 0xffffffffu) {
-    atomicAdd(&r.counts[24 + cur_c], traces_acc); atomicAdd(&r.counts[32 + cur_c], steps_acc);
-    atomicAdd(&r.counts[64 + cur_c], cap_acc);
+  if (r.stats) {   // the warp leaves the loop together: one atomic per cascade the warp's lanes hold
+    const unsigned grp = __match_any_sync(0xffffffffu, cur_c);
+    const uint32_t tr = __reduce_add_sync(grp, traces_acc), sp = __reduce_add_sync(grp, steps_acc);
+    const uint32_t cp = __reduce_add_sync(grp, cap_acc);
+    if (cur_c != 0xffffffffu && (uint32_t)(__ffs(grp) - 1) == lane) {
+      atomicAdd(&r.counts[24 + cur_c], tr); atomicAdd(&r.counts[32 + cur_c], sp); atomicAdd(&r.counts[64 + cur_c], cp);
+    }
   }
 }
 
