@@ -212,6 +212,11 @@ int gi_rc_graph_launch(gi_rc *rc, void *stream);
 typedef struct gi_batch gi_batch;
 int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32_t n, gi_batch **out);
 int gi_batch_capture(gi_batch *batch, void *stream);
+/* The same batch captured pass by pass: the n voxel rebuilds as parallel branches, then ONE launch per cascade pass
+ * over the work of every solve (setup, a persistent trace over all the rays, one merge launch per cascade step, the
+ * gather).  All solves need the same atlas format and probe spacing (8, 16 or 32 pixels); the solves' launch tuning
+ * does not apply to these launches (results are the same bits either way).  Replaces a graph captured before. */
+int gi_batch_capture_passes(gi_batch *batch, void *stream);
 int gi_batch_launch(gi_batch *batch, void *stream);
 int gi_batch_destroy(gi_batch *batch);
 /* Pass timing (the reference's per-pass timestamps, rcrun.ts:325-372): when on, every solve records CUDA events

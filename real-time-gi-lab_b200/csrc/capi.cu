@@ -5,8 +5,10 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <algorithm>
 #include <new>
 #include <string>
+#include <vector>
 
 #include "gi_dev.cuh"
 #include "gi_internal.h"
@@ -784,6 +786,10 @@ struct gi_batch {
   cudaEvent_t *done = nullptr;
   cudaEvent_t start = nullptr;
   cudaGraphExec_t graph = nullptr;
+  // gi_batch_capture_passes: the solves' descriptors and work prefixes on the device
+  RcDev *d_rc = nullptr;
+  VoxDev *d_vox = nullptr;
+  uint32_t *d_pre = nullptr;
 };
 
 static void free_batch(gi_batch *b) {
@@ -793,6 +799,7 @@ static void free_batch(gi_batch *b) {
     if (b->done && b->done[i]) cudaEventDestroy(b->done[i]);
   }
   if (b->start) cudaEventDestroy(b->start);
+  cudaFree(b->d_rc); cudaFree(b->d_vox); cudaFree(b->d_pre);
   delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done;
 }
 
@@ -860,6 +867,95 @@ int gi_batch_capture(gi_batch *b, void *stream) {
   e = cudaGraphInstantiate(&b->graph, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture: instantiate"); }
+  return GI_OK;
+}
+
+int gi_batch_capture_passes(gi_batch *b, void *stream) {
+  if (!b) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: NULL batch");
+  if (!stream) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: the legacy default stream cannot be captured; pass a stream");
+  const uint32_t n = b->n;
+  const RcDev &r0 = b->rcs[0]->dev;
+  for (uint32_t i = 0; i < n; i++) {
+    gi_rc *r = b->rcs[i];
+    if (!r->frame_set || !r->gbuf_set || !b->voxes[i]->updated)
+      return fail(GI_ERR_STATE, "gi_batch_capture_passes: solve %u lacks its frame, G-buffer or voxel window", i);
+    if (r->dev.atlas != r0.atlas || r->dev.c[0].tile_size != r0.c[0].tile_size)
+      return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has another atlas format or probe spacing than solve 0", i);
+  }
+  const uint32_t P0 = r0.c[0].tile_size;
+  if (P0 != 8u && P0 != 16u && P0 != 32u)
+    return fail(GI_ERR_INVALID, "gi_batch_capture_passes: probe spacing %u (8, 16 or 32)", P0);
+  CK(cudaSetDevice(b->ctx->device), "gi_batch_capture_passes: cudaSetDevice");
+  // descriptors and prefixes, built on the host
+  std::vector<RcDev> hrc(n);
+  std::vector<VoxDev> hvox(n);
+  uint32_t max_casc = 0;
+  for (uint32_t i = 0; i < n; i++) max_casc = std::max(max_casc, b->rcs[i]->dev.cascades);
+  const size_t stride = n + 1u;
+  std::vector<uint32_t> pre((3u + max_casc) * stride, 0u);   // setup, rays, gather, then merge steps
+  uint32_t *setup = pre.data(), *rays = setup + stride, *gath = rays + stride, *merge = gath + stride;
+  BatchSizes z = {};
+  z.atlas = r0.atlas;
+  z.P0 = P0;
+  for (uint32_t i = 0; i < n; i++) {
+    gi_rc *r = b->rcs[i];
+    r->dev.hits = r->debug_hits ? r->hits : nullptr;
+    r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
+    hrc[i] = r->dev;
+    hvox[i] = b->voxes[i]->dev;
+    const RcDev &d = r->dev;
+    setup[i + 1] = setup[i] + (d.probes_total + 255u) / 256u;
+    rays[i + 1] = rays[i] + (d.rays_total + 31u) / 32u * 32u;
+    const uint32_t th = 32u / P0, ntx = (r->W + P0 / 2u + P0 - 1u) / P0, nty = (r->H + P0 / 2u + th - 1u) / th;
+    gath[i + 1] = gath[i] + ((ntx + 1u) / 2u) * ((nty + 3u) / 4u);
+    for (uint32_t k = 0; k < max_casc; k++) {
+      uint32_t blocks = 0;
+      if (k < d.cascades) {
+        const CascDev &L = d.c[d.cascades - 1u - k];
+        blocks = (L.np * (L.res * L.res / 4u) + 255u) / 256u;
+      }
+      merge[k * stride + i + 1] = merge[k * stride + i] + blocks;
+    }
+  }
+  z.setup_blocks = setup[n];
+  z.gather_blocks = gath[n];
+  for (uint32_t k = 0; k < max_casc; k++) z.merge_blocks[k] = merge[k * stride + n];
+  cudaFree(b->d_rc); cudaFree(b->d_vox); cudaFree(b->d_pre);
+  b->d_rc = nullptr; b->d_vox = nullptr; b->d_pre = nullptr;
+  cudaError_t e;
+  if ((e = dalloc(&b->d_rc, n)) || (e = dalloc(&b->d_vox, n)) || (e = dalloc(&b->d_pre, pre.size() + 1u)))
+    return cuda_fail(e, "gi_batch_capture_passes");
+  CK(cudaMemcpy(b->d_rc, hrc.data(), n * sizeof(RcDev), cudaMemcpyHostToDevice), "gi_batch_capture_passes: copy");
+  CK(cudaMemcpy(b->d_vox, hvox.data(), n * sizeof(VoxDev), cudaMemcpyHostToDevice), "gi_batch_capture_passes: copy");
+  CK(cudaMemcpy(b->d_pre, pre.data(), pre.size() * 4u, cudaMemcpyHostToDevice), "gi_batch_capture_passes: copy");
+  BatchDev B;
+  B.rc = b->d_rc; B.vox = b->d_vox; B.n = n; B.max_casc = max_casc;
+  B.setup_blk = b->d_pre; B.ray_pre = b->d_pre + stride; B.gather_blk = b->d_pre + 2u * stride;
+  B.merge_blk = b->d_pre + 3u * stride; B.counter = b->d_pre + pre.size();
+  if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+  cudaStream_t st = S(stream);
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "gi_batch_capture_passes: begin");
+  int status = GI_OK;
+  e = cudaEventRecord(b->start, st);
+  // the rebuilds, each on its own stream from the batch start
+  for (uint32_t i = 0; i < n && e == cudaSuccess && status == GI_OK; i++) {
+    gi_rc *r = b->rcs[i];
+    e = cudaStreamWaitEvent(b->streams[i], b->start, 0);
+    if (e != cudaSuccess) break;
+    status = vox_build_sun(b->voxes[i], r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, b->streams[i]);
+    if (status == GI_OK) e = cudaEventRecord(b->done[i], b->streams[i]);
+    if (e == cudaSuccess && status == GI_OK) e = cudaStreamWaitEvent(st, b->done[i], 0);
+  }
+  // then one launch per pass over every solve
+  if (e == cudaSuccess && status == GI_OK) e = gi_launch_batch_passes(B, z, b->ctx->sm_count, st);
+  cudaGraph_t g = nullptr;
+  cudaError_t e2 = cudaStreamEndCapture(st, &g);
+  if (status != GI_OK) { if (g) cudaGraphDestroy(g); return status; }
+  if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture_passes"); }
+  if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture_passes: end");
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture_passes: instantiate"); }
   return GI_OK;
 }
 

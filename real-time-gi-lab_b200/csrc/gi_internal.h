@@ -114,6 +114,25 @@ inline cudaError_t gi_launch(void (*k)(P...), dim3 grid, dim3 block, cudaStream_
 
 // Launch shapes of the cascade passes (the result does not depend on them)
 struct RcLaunch { uint32_t trace_blocks, gather_shape, merge_threads; };
+
+// A batch of solves run pass by pass: one launch per pass over the work of every solve.  The solves' descriptors and
+// the work prefixes live in device memory; each block (each 32-ray fetch of the trace) belongs to one solve, found by
+// a binary search of the prefix.
+namespace gi {
+struct BatchDev {
+  const RcDev *rc;
+  const VoxDev *vox;
+  uint32_t n, max_casc;
+  const uint32_t *setup_blk;    // n + 1: first setup block of each solve (256 probes a block)
+  const uint32_t *ray_pre;      // n + 1: first ray of each solve in the batch's trace order (rays padded to 32)
+  const uint32_t *merge_blk;    // max_casc x (n + 1): per merge step k (cascade C - 1 - k), first block of each solve
+  const uint32_t *gather_blk;   // n + 1: first gather block of each solve
+  uint32_t *counter;            // [0]: rays handed out by the batched trace
+};
+// host copies of the launch sizes
+struct BatchSizes { uint32_t setup_blocks, merge_blocks[8], gather_blocks, atlas, P0; };
+}  // namespace gi
+cudaError_t gi_launch_batch_passes(const gi::BatchDev &b, const gi::BatchSizes &z, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
                                cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr);
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H);

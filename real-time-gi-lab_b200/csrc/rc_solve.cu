@@ -213,13 +213,8 @@ __device__ __forceinline__ uint32_t casc_of_ray(const RcDev &r, uint32_t i) {
   return c;
 }
 
-// setupScreen (rc.ts:572-590), every cascade in one launch
-__global__ void k_setup_screen(RcDev r, VoxDev v) {
-  grid_dep_wait();
-  // the 80 counter words and the trace's ray counter start at zero (words below `cascades` are set below)
-  if (blockIdx.x == 0 && threadIdx.x < 81u && threadIdx.x >= r.cascades) r.counts[threadIdx.x] = 0u;
-  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.probes_total) return;
+// setupScreen (rc.ts:572-590) of probe i (all cascades numbered together)
+__device__ __forceinline__ void setup_probe(const RcDev &r, const VoxDev &v, uint32_t i) {
   uint32_t c = 0;
   for (uint32_t k = 1; k < r.cascades; k++) if (i >= r.c[k].probe_off) c = k;
   const CascDev &L = r.c[c];
@@ -248,14 +243,57 @@ __global__ void k_setup_screen(RcDev r, VoxDev v) {
   r.plevel[i] = pr.pos.w > 0.0f ? vox_level(v, r, pr.pos.w, c) : 0u;
 }
 
-// trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245).  Persistent: every warp takes rays from a global counter, 32 at
-// a time.
-template <int A>
-__global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
+// every cascade in one launch
+__global__ void k_setup_screen(RcDev r, VoxDev v) {
   grid_dep_wait();
+  // the 80 counter words and the trace's ray counter start at zero (words below `cascades` are set by the probes)
+  if (blockIdx.x == 0 && threadIdx.x < 81u && threadIdx.x >= r.cascades) r.counts[threadIdx.x] = 0u;
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < r.probes_total) setup_probe(r, v, i);
+}
+
+// trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) of the ray at position j of the trace order (cascade c): writes
+// its atlas element (and the debug copies); true when its probe is valid and the ray was marched.
+template <int A>
+__device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, TraceOut &out) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const float *F = r.frame;
+  out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
+  out.steps = 0;
+  bool traced = false;
+  const CascDev &L = r.c[c];
+  uint32_t t = j - L.ray_off, pi, di;
+  if (r.trace_order == 0) {           // probe-major: the atlas order
+    pi = t >> L.dirs_log2;
+    di = t & ((1u << L.dirs_log2) - 1u);
+  } else {                            // direction-major: one direction over consecutive probes
+    di = t / L.np;
+    pi = t - di * L.np;
+  }
+  uint32_t i = L.ray_off + (pi << L.dirs_log2) + di;   // the ray's atlas element
+  ProbeDev pr = r.probes[L.probe_off + pi];
+  if (pr.pos.w > 0.0f) {
+    float4 dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
+    f3 dir = mk(dv.x, dv.y, dv.z);
+    float s0 = pr.pos.w;
+    float t0 = L.b0 * s0, t1 = L.b1 * s0;
+    f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
+    uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
+    float vs = vox_size(v, Lv);
+    trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
+    traced = true;
+  }
+  Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
+  if (r.hits) r.hits[i] = make_uint4(out.lvl, out.ptr, out.bit, out.tin);
+  if (r.rad_traced) Atlas<A>::store(reinterpret_cast<T *>(r.rad_traced), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
+  return traced;
+}
+
+// Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time.
+template <int A>
+__global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
+  grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
   uint32_t steps_acc = 0, traces_acc = 0, cap_acc = 0;
   uint32_t cur_c = 0xffffffffu;
@@ -270,36 +308,8 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
     bool live = j < r.rays_total;
     uint32_t c = live ? casc_of_ray(r, j) : 0u;
     TraceOut out;
-    out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
     out.steps = 0;
-    bool traced = false;
-    if (live) {
-      const CascDev &L = r.c[c];
-      uint32_t t = j - L.ray_off, pi, di;
-      if (r.trace_order == 0) {           // probe-major: the atlas order
-        pi = t >> L.dirs_log2;
-        di = t & ((1u << L.dirs_log2) - 1u);
-      } else {                            // direction-major: one direction over consecutive probes
-        di = t / L.np;
-        pi = t - di * L.np;
-      }
-      uint32_t i = L.ray_off + (pi << L.dirs_log2) + di;   // the ray's atlas element
-      ProbeDev pr = r.probes[L.probe_off + pi];
-      if (pr.pos.w > 0.0f) {
-        float4 dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
-        f3 dir = mk(dv.x, dv.y, dv.z);
-        float s0 = pr.pos.w;
-        float t0 = L.b0 * s0, t1 = L.b1 * s0;
-        f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
-        uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
-        float vs = vox_size(v, Lv);
-        trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
-        traced = true;
-      }
-      Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
-      if (r.hits) r.hits[i] = make_uint4(out.lvl, out.ptr, out.bit, out.tin);
-      if (r.rad_traced) Atlas<A>::store(reinterpret_cast<T *>(r.rad_traced), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
-    }
+    bool traced = live && trace_ray<A>(r, v, j, c, out);
     if (r.stats) {
       // per-cascade counters (rc.ts:232-235); flush when the lane's cascade changes
       if (live && traced) {
@@ -379,14 +389,12 @@ __device__ __forceinline__ void project_sh_quads(const RcDev &r, uint32_t pi, co
 // from its stored (rounded) texels: the same four values summed in the same order, so the same bits.  When this
 // cascade's resolution is twice the lower one's, the thread writes its own quad's average for the merge below.
 template <int A>
-__global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4 *__restrict__ up_avg,
-                                               float4 *__restrict__ my_avg) {
-  grid_dep_wait();
+__device__ __forceinline__ void merge_quad(const RcDev &r, uint32_t c, uint32_t t, const float4 *__restrict__ up_avg,
+                                           float4 *__restrict__ my_avg) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const CascDev &L = r.c[c];
   uint32_t hr = L.res >> 1, hq_log2 = L.dirs_log2 - 2u;   // quads per row, log2 quads per probe
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= (L.np << hq_log2)) return;
   uint32_t pi = t >> hq_log2, qd = t & ((1u << hq_log2) - 1u);
   uint32_t u0 = (qd % hr) * 2u, v0 = (qd / hr) * 2u;
@@ -460,6 +468,13 @@ __global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4
     my_avg[((size_t)pi << hq_log2) + (v0 >> 1) * hr + (u0 >> 1)] = make_float4(a.x, a.y, a.z, 0.0f);
   }
   if (c == 0u) project_sh_quads<A>(r, pi, mr);
+}
+
+template <int A>
+__global__ void __launch_bounds__(512) k_merge(RcDev r, uint32_t c, const float4 *__restrict__ up_avg,
+                                               float4 *__restrict__ my_avg) {
+  grid_dep_wait();
+  merge_quad<A>(r, c, blockIdx.x * blockDim.x + threadIdx.x, up_avg, my_avg);
 }
 
 
@@ -558,13 +573,12 @@ __global__ void __launch_bounds__(256) k_gather(RcDev r) {
 // per lane) and the pixels read them as broadcasts.  A warp whose pixels turn out not to share their probes (they
 // always do for these P; the check keeps it exact regardless) reads them per lane.  Blocks of 2 x 4 warp tiles.
 template <int A, uint32_t P>
-__global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
-  grid_dep_wait();
+__device__ __forceinline__ void gather_tiles(const RcDev &r, uint32_t blk_x, uint32_t blk_y) {
   constexpr uint32_t TH = 32u / P;
   __shared__ float4 s_coef[8][32];
   __shared__ float4 s_pn[8][8];
   const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
-  const int tx = (int)(blockIdx.x * 2u + (warp & 1u)), ty = (int)(blockIdx.y * 4u + (warp >> 1));
+  const int tx = (int)(blk_x * 2u + (warp & 1u)), ty = (int)(blk_y * 4u + (warp >> 1));
   const int px = tx * (int)P - (int)(P / 2u) + (int)(lane % P), py = ty * (int)TH - (int)(P / 2u) + (int)(lane / P);
   const bool on = px >= 0 && py >= 0 && px < (int)r.width && py < (int)r.height;
   const unsigned on_mask = __ballot_sync(0xffffffffu, on);
@@ -591,6 +605,94 @@ __global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
   }
   __syncwarp();
   if (on) gather_pixel<A>(r, (uint32_t)px, (uint32_t)py, SharedProbes{s_pn[warp], s_coef[warp]});
+}
+
+template <int A, uint32_t P>
+__global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
+  grid_dep_wait();
+  gather_tiles<A, P>(r, blockIdx.x, blockIdx.y);
+}
+
+// ---- batches of solves, one launch per pass (gi_batch_capture_passes) ----------------------------------------------
+
+// The last solve s with pre[s] <= x (the owner of item x: solves with no items share the next one's start)
+__device__ __forceinline__ uint32_t batch_owner(const uint32_t *__restrict__ pre, uint32_t n, uint32_t x) {
+  uint32_t lo = 0, hi = n;
+  while (hi - lo > 1u) {
+    uint32_t m = (lo + hi) >> 1;
+    if (__ldg(&pre[m]) <= x) lo = m; else hi = m;
+  }
+  return lo;
+}
+
+__global__ void __launch_bounds__(256) k_setup_batch(BatchDev B) {
+  grid_dep_wait();
+  const uint32_t s = batch_owner(B.setup_blk, B.n, blockIdx.x), b = blockIdx.x - B.setup_blk[s];
+  const RcDev &r = B.rc[s];
+  if (b == 0 && threadIdx.x < 81u && threadIdx.x >= r.cascades) r.counts[threadIdx.x] = 0u;
+  if (blockIdx.x == 0 && threadIdx.x == 0) B.counter[0] = 0u;
+  const uint32_t i = b * 256u + threadIdx.x;
+  if (i < r.probes_total) setup_probe(r, B.vox[s], i);
+}
+
+// Persistent over the rays of every solve: warps take 32 rays at a time; solves are padded to 32 rays, so a fetch
+// belongs to one solve
+template <int A>
+__global__ void __launch_bounds__(256) k_trace_batch(BatchDev B) {
+  grid_dep_wait();
+  const uint32_t lane = threadIdx.x & 31u, total = B.ray_pre[B.n];
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(B.counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= total) break;
+    const uint32_t s = batch_owner(B.ray_pre, B.n, base);
+    const RcDev &r = B.rc[s];
+    const uint32_t j = base - B.ray_pre[s] + lane;
+    if (j < r.rays_total) {
+      TraceOut out;
+      trace_ray<A>(r, B.vox[s], j, casc_of_ray(r, j), out);
+    }
+  }
+}
+
+// Merge step k: every solve merges its cascade C - 1 - k (solves with fewer cascades have no blocks)
+template <int A>
+__global__ void __launch_bounds__(256) k_merge_batch(BatchDev B, uint32_t k) {
+  grid_dep_wait();
+  const uint32_t *pre = B.merge_blk + k * (B.n + 1u);
+  const uint32_t s = batch_owner(pre, B.n, blockIdx.x);
+  const RcDev &r = B.rc[s];
+  const uint32_t c = r.cascades - 1u - k;
+  float4 *mine = (c > 0u && r.c[c - 1u].res * 2u == r.c[c].res) ? r.mavg[c & 1u] : nullptr;
+  merge_quad<A>(r, c, (blockIdx.x - pre[s]) * 256u + threadIdx.x, r.mavg[(c + 1u) & 1u], mine);
+}
+
+template <int A, uint32_t P>
+__global__ void __launch_bounds__(256) k_gather_batch(BatchDev B) {
+  grid_dep_wait();
+  const uint32_t s = batch_owner(B.gather_blk, B.n, blockIdx.x), lb = blockIdx.x - B.gather_blk[s];
+  const RcDev &r = B.rc[s];
+  const uint32_t gx = ((r.width + P / 2u + P - 1u) / P + 1u) / 2u;
+  gather_tiles<A, P>(r, lb % gx, lb / gx);
+}
+
+template <int A, uint32_t P>
+static cudaError_t launch_batch(const BatchDev &b, const BatchSizes &z, uint32_t sm_count, cudaStream_t st) {
+  GI_TRY(gi_launch(k_setup_batch, z.setup_blocks, 256, st, b));
+  GI_TRY(gi_launch(k_trace_batch<A>, sm_count * 4u, 256, st, b));
+  for (uint32_t k = 0; k < b.max_casc; k++)
+    if (z.merge_blocks[k]) GI_TRY(gi_launch(k_merge_batch<A>, z.merge_blocks[k], 256, st, b, k));
+  GI_TRY(gi_launch(k_gather_batch<A, P>, z.gather_blocks, 256, st, b));
+  return cudaGetLastError();
+}
+
+template <int A>
+static cudaError_t launch_batch_p(const BatchDev &b, const BatchSizes &z, uint32_t sm_count, cudaStream_t st) {
+  if (z.P0 == 8u) return launch_batch<A, 8u>(b, z, sm_count, st);
+  if (z.P0 == 16u) return launch_batch<A, 16u>(b, z, sm_count, st);
+  if (z.P0 == 32u) return launch_batch<A, 32u>(b, z, sm_count, st);
+  return cudaErrorInvalidValue;
 }
 
 __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
@@ -691,4 +793,13 @@ cudaError_t gi_launch_init_dirs(const RcDev &r, float4 *dirs, uint32_t ndirs, cu
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st) {
   k_normal_f32_to_f16<<<256, 256, 0, st>>>(src, dst, n);
   return cudaGetLastError();
+}
+
+cudaError_t gi_launch_batch_passes(const BatchDev &b, const BatchSizes &z, uint32_t sm_count, cudaStream_t st) {
+  switch (z.atlas) {
+    case GI_ATLAS_F32: return launch_batch_p<GI_ATLAS_F32>(b, z, sm_count, st);
+    case GI_ATLAS_F16: return launch_batch_p<GI_ATLAS_F16>(b, z, sm_count, st);
+    case GI_ATLAS_BF16: return launch_batch_p<GI_ATLAS_BF16>(b, z, sm_count, st);
+  }
+  return cudaErrorInvalidValue;
 }

@@ -67,6 +67,7 @@ SIGNATURES = {
     "gi_rc_graph_launch": (C.c_int, [_P, _P]),
     "gi_batch_create": (C.c_int, [_P, _P, _P, C.c_uint32, C.POINTER(_P)]),
     "gi_batch_capture": (C.c_int, [_P, _P]),
+    "gi_batch_capture_passes": (C.c_int, [_P, _P]),
     "gi_batch_launch": (C.c_int, [_P, _P]),
     "gi_batch_destroy": (C.c_int, [_P]),
     "gi_rc_set_timing": (C.c_int, [_P, C.c_int]),

@@ -334,7 +334,8 @@ class Rc:
 
 
 class Batch:
-    """n independent solves captured into one CUDA graph of parallel solve chains (gi_batch_*)."""
+    """n independent solves captured into one CUDA graph (gi_batch_*): parallel solve chains (capture), or the
+    rebuilds in parallel then one launch per cascade pass over every solve (capture_passes)."""
 
     def __init__(self, ctx: Context, rcs, voxes):
         assert len(rcs) == len(voxes)
@@ -348,6 +349,10 @@ class Batch:
 
     def capture(self, stream):
         _lib.call("gi_batch_capture", self.handle, _stream(stream))
+
+    def capture_passes(self, stream):
+        """The rebuilds as parallel branches, then one launch per cascade pass over every solve."""
+        _lib.call("gi_batch_capture_passes", self.handle, _stream(stream))
 
     def launch(self, stream):
         _lib.call("gi_batch_launch", self.handle, _stream(stream))

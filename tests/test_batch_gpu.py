@@ -53,6 +53,21 @@ def test_batch_equals_solves_alone():
     # a solve replayed alone after the batch still gives its own result
     solves[2].rc.graph_launch(stream)
     assert np.array_equal(solves[2].rc.read_irradiance(stream).view(np.uint32), alone[2].view(np.uint32))
+    # the same batch pass by pass: one launch per cascade pass over every solve
+    b.capture_passes(stream)
+    for x in solves:   # first overwrite every output with a solve under twice the sun
+        f2 = np.array(x.frame, np.float32).copy()
+        f2[92:95] *= 2.0
+        x.rc.set_frame(f2, stream)
+        x.rc.solve(x.vox, stream)
+        assert not np.array_equal(x.rc.read_irradiance(stream), alone[solves.index(x)])
+        x.rc.set_frame(x.frame, stream)
+    for rep in range(2):
+        b.launch(stream)
+        stream.synchronize()
+        for i, x in enumerate(solves):
+            got = x.rc.read_irradiance(stream)
+            assert np.array_equal(got.view(np.uint32), alone[i].view(np.uint32)), f"solve {i} differs pass by pass (launch {rep})"
     b.destroy()
     for x in solves:
         x.destroy()
