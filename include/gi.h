@@ -176,6 +176,18 @@ int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
  * visibility is 1.  size 0 releases it.  Draw it again when the light matrix or the scene moves; a graph captured
  * before a change of size must be captured again. */
 int gi_rc_render_shadow(gi_rc *rc, gi_scene *scene, uint32_t size, void *stream);
+/* Multi-bounce (bounce.ts; BounceParams, DEFAULT_BOUNCE {1.2, [32, 16, 32], 16, 2}): a camera-centred volume of
+ * dx*dy*dz irradiance probes `cell` metres apart, rebuilt every solve from the voxels (each probe near a surface traces
+ * `rays` rays plus six axis rays, every `div` solves by its position) and injected into the voxels, whose hits then
+ * add albedo / pi times it.  Bound to one voxel world (the volume's rays and the injected irradiance are its voxels');
+ * gi_solve / gi_rc_solve with another world fail.  rays <= 26.  params NULL turns it off.  The volume keeps one frame
+ * of history (the probes' rays read the previous volume), so results depend on the sequence of solves. */
+typedef struct {
+  float cell;
+  uint32_t dx, dy, dz, rays, div;
+  uint32_t reserved[2];
+} gi_bounce_params;
+int gi_rc_set_bounce(gi_rc *rc, gi_vox *vox, const gi_bounce_params *params);
 /* encode(enc) (rc.ts:1169-1222): giBuild (setupScreen), giTrace, giMerge (mergeScreen N-1..0, projectSH),
  * giGather (gatherScreen) over the voxel world's current state. */
 int gi_rc_solve(gi_rc *rc, gi_vox *vox, void *stream);
@@ -236,7 +248,10 @@ enum {
   GI_RC_NORMAL = 4,     /* W*H*4 halves */
   GI_RC_HITS = 5,       /* per ray: level, brick, bit, tIn bits (only after gi_rc_set_debug_hits(rc, 1)) */
   GI_RC_RAD_TRACED = 6, /* the atlas right after the trace, before the merge (only with debug hits on) */
-  GI_RC_SHADOW = 7      /* size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
+  GI_RC_SHADOW = 7,     /* size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
+  GI_RC_BOUNCE_VOL = 8, /* the two bounce volumes, dx*dy*(6dz+1) rgba16f texels each (only with multi-bounce on) */
+  GI_RC_BOUNCE_INJ = 9, /* per voxel the injected irradiance: 8 halves (front rgb, 0, back rgb, 0) (multi-bounce on) */
+  GI_RC_BOUNCE_LIST = 10 /* 4 + dx*dy*dz words: listed probes, frame counter, current volume, then the list */
 };
 int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
 int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);

@@ -6,6 +6,7 @@ __graft_entry__.smoke() and bench.py's cpu_baseline leg, never by the product pa
 from __future__ import annotations
 
 import ctypes as C
+import ctypes.util
 import os
 import subprocess
 from dataclasses import dataclass
@@ -55,6 +56,7 @@ def lib():
         _lib.orc_sun_tap.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.orc_sun_tap.restype = C.c_float
         _lib.orc_vox_sun.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
+        _lib.orc_bounce_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_gi_exp.argtypes = [C.c_float]
         _lib.orc_gi_exp.restype = C.c_float
     return _lib
@@ -76,7 +78,13 @@ class OrcVox(C.Structure):
                 ("origin", (C.c_int32 * 4) * 8),
                 ("hdr", C.c_void_p), ("ptr", C.c_void_p), ("occ", C.c_void_p), ("base", C.c_void_p),
                 ("code", C.c_void_p), ("rep", C.c_void_p), ("big", C.c_void_p), ("attr", C.c_void_p),
-                ("plane", C.c_void_p), ("sunvis", C.c_void_p)]
+                ("plane", C.c_void_p), ("sunvis", C.c_void_p), ("bn_inj", C.c_void_p)]
+
+
+class OrcBounce(C.Structure):
+    _fields_ = [("cell", C.c_float), ("v0", C.c_float), ("dx", C.c_uint32), ("dy", C.c_uint32), ("dz", C.c_uint32),
+                ("rays", C.c_uint32), ("div", C.c_uint32), ("dirs", C.c_void_p), ("vol", C.c_void_p * 2),
+                ("list", C.c_void_p)]
 
 
 class OrcCasc(C.Structure):
@@ -162,6 +170,7 @@ def _vox_struct(st: dict) -> OrcVox:
     for k in ("hdr", "ptr", "occ", "base", "code", "rep", "attr", "plane", "sunvis"):
         setattr(vx, k, _p(st[k]))
     vx.big = None
+    vx.bn_inj = _p(st["bn_inj"]) if st.get("bn_inj") is not None else None
     return vx
 
 
@@ -254,3 +263,46 @@ def vox_sun(vox: dict, frame: np.ndarray, shadow: np.ndarray) -> None:
     shadow = np.ascontiguousarray(shadow, dtype=np.float32)
     vx = _vox_struct(vox)
     lib().orc_vox_sun(C.byref(vx), _p(frame), _p(shadow), shadow.shape[0])
+
+
+def bounce_dirs(rays: int) -> np.ndarray:
+    """sfDir(i, rays) (bounce.ts:147-152) as the library tabulates it: the f32 steps of the shader, cos and sin of the
+    f32 phi in double precision (the shader's are implementation-defined)."""
+    f = np.float32
+    libm = C.CDLL(C.util.find_library("m") or "libm.so.6")   # the C library's cos / sin, as the library's host code
+    libm.cos.restype = libm.sin.restype = C.c_double
+    libm.cos.argtypes = libm.sin.argtypes = [C.c_double]
+    out = np.zeros((rays, 4), np.float32)
+    for i in range(rays):
+        fi, fn = f(i), f(rays)
+        z = f(f(1.0) - (f(2.0) * fi + f(1.0)) / fn)
+        zz = f(f(1.0) - z * z)
+        r = f(np.sqrt(zz if zz > 0 else f(0.0)))
+        xi = f(fi * f(0.618033988749))
+        fr = f(xi - f(np.floor(xi)))
+        phi = f(f(f(2.0) * f(3.14159265)) * fr)
+        out[i] = (f(r * f(libm.cos(float(phi)))), f(r * f(libm.sin(float(phi)))), z, 0.0)
+    return out
+
+
+class Bounce:
+    """The oracle's multi-bounce volume state (orc_bounce) across frames."""
+
+    def __init__(self, vox: dict, cell: float = 1.2, dims=(32, 16, 32), rays: int = 16, div: int = 2):
+        dx, dy, dz = dims
+        self.dirs = bounce_dirs(rays)
+        texels = dx * dy * (6 * dz + 1)
+        self.vol = [np.zeros(texels * 4, np.float32), np.zeros(texels * 4, np.float32)]
+        self.list = np.zeros(4 + dx * dy * dz, np.uint32)
+        self.b = OrcBounce(np.float32(cell), np.float32(vox["v0"]), dx, dy, dz, rays, div, _p(self.dirs),
+                           (C.c_void_p * 2)(_p(self.vol[0]), _p(self.vol[1])), _p(self.list))
+
+    def frame(self, vox: dict, frame: np.ndarray) -> np.ndarray:
+        """One frame over a built world; returns (and stores in vox['bn_inj']) the injected irradiance."""
+        frame = np.ascontiguousarray(frame, dtype=np.float32)
+        inj = np.zeros(vox["max_voxels"] * 6, np.float32)
+        vx = _vox_struct(vox)
+        vx.bn_inj = None
+        lib().orc_bounce_frame(C.byref(self.b), C.byref(vx), _p(frame), _p(inj))
+        vox["bn_inj"] = inj
+        return inj

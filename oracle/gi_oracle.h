@@ -75,6 +75,8 @@ typedef struct {
   uint32_t *attr;                  /* max_voxels * 4: albedo, normal, emissive rg (f16x2), emissive b (f16) */
   float *plane;                    /* max_voxels: representative plane offset from the voxel centre */
   float *sunvis;                   /* max_voxels: sun visibility of the voxel (1 when no visibility pass runs) */
+  const float *bn_inj;             /* NULL, or max_voxels * 6: the bounce volume's irradiance on the voxel's two sides
+                                      (front rgb, back rgb, f16 values; orc_bounce_frame writes it) */
 } orc_vox;
 
 /* Host writeUniform (voxel.ts:868-876): per level origin = floor(eye / bs) - G/2, bs = v0 * 2^L * 8 (f64 host math). */
@@ -143,6 +145,20 @@ int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float 
 float orc_sun_tap(const float *frame, const float *map, uint32_t S, const float x[3]);
 /* voxSun (voxel.ts:633-671): the sun visibility of every occupied voxel of a built world (after orc_vox_build). */
 int orc_vox_sun(orc_vox *vx, const float *frame, const float *map, uint32_t S);
+
+/* The multi-bounce volume (bounce.ts): dx * dy * dz probes around the camera, each an ambient cube (6 axes x rgba),
+ * stored in f16 (kept here as the f16 values in floats), two volumes swapped every frame.  Caller-allocated buffers. */
+typedef struct {
+  float cell, v0;                 /* probe spacing; the clipmap's level-0 voxel size */
+  uint32_t dx, dy, dz, rays, div;
+  const float *dirs;              /* rays * 4: sfDir(r, rays) (the same table the GPU path uses) */
+  float *vol[2];                  /* dx * dy * (6 dz + 1) * 4 each, texel (x, y, z) at ((z dy + y) dx + x) * 4 */
+  uint32_t *list;                 /* 4 + dx dy dz words: [0] listed, [1] frame counter, [2] this frame's volume */
+} orc_bounce;
+/* One frame of the volume (Bounce.encode, bounce.ts:356-368) over a built voxel world: clear, classify, update,
+ * inject (into inj_out, max_voxels * 6).  The list order is the probe order (the GPU's atomics order it otherwise;
+ * the result does not depend on it). */
+int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *frame, float *inj_out);
 
 /* WGSL builtins as the oracle defines them (exported for the known-answer tests). */
 uint32_t orc_pack4x8unorm(const float v[4]);

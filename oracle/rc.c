@@ -4,9 +4,9 @@
  * Follows rc.ts:95-141 (shading), :210-245 (traceWorld), :291-311 (octahedral maps, packing), :572-590
  * (setupScreen), :600-622 (trace), :681-743 (upperAvg, mergeScreen), :745-774 (shBasis, projectSH),
  * :819-829 (evalSH), :929-954 (gatherScreen), and voxel.ts:81-202 (voxRank, voxAt, voxLevelFor, traceVox).
- * Multi-bounce (BN_ON), the dynamic layer (dyn[0] = 0) and the triangle comparator are off, as in the
- * configurations this build measures.  The hit radiance adds the voxel's emissive radiance (the reference has no
- * emission). */
+ * Multi-bounce (bounce.ts) is restated too: the volume's frame (orc_bounce_frame) and the cascades' read of the
+ * irradiance it injects into the voxels (when orc_vox.bn_inj is set).  The dynamic layer (dyn[0] = 0) and the triangle
+ * comparator are off.  The hit radiance adds the voxel's emissive radiance (the reference has no emission). */
 #include <stdlib.h>
 #include "gi_oracle.h"
 #include "orc_math.h"
@@ -22,6 +22,8 @@ typedef struct {
   const orc_vox *vx;
   const float *F;
   float sky[3];
+  const orc_bounce *bn;   /* the volume's own rays: read the previous volume bn_prev at the hit (bounce.ts:90-93) */
+  const float *bn_prev;
 } ctx_t;
 
 static inline float vox_size(const orc_vox *vx, uint32_t L) { return scale2(vx->v0, (int)L); }
@@ -131,13 +133,69 @@ static v3 shade_hit_v(const float *F, v3 n0, const float alb[4], v3 d, v3 e, flo
 
 typedef struct { float r, g, b, T; uint32_t lvl, ptr, bit, tin; uint32_t steps; } trace_t;
 
-/* The hit: attributes of voxel (brick, bit), shaded (voxShade, rc.ts:136-140) plus the emissive radiance. */
-static void shade_voxel(const ctx_t *cx, uint32_t brick, uint32_t bit, v3 d, trace_t *out) {
+/* ---- multi-bounce reads (bounce.ts:44-75, 90-93; rc.ts:198-202) ---- */
+static float bn_get(const orc_bounce *b, const float *vol, int32_t x, int32_t y, int32_t z, int k) {
+  return vol[(((size_t)z * b->dy + (size_t)y) * b->dx + (size_t)x) * 4u + (size_t)k];
+}
+static float bn_axis_a(const orc_bounce *b, const float *vol, i3 c, int a) { return bn_get(b, vol, c.x, c.y, a * (int32_t)b->dz + c.z, 3); }
+static v3 bn_axis_rgb(const orc_bounce *b, const float *vol, i3 c, int a) {
+  int32_t z = a * (int32_t)b->dz + c.z;
+  return V(bn_get(b, vol, c.x, c.y, z, 0), bn_get(b, vol, c.x, c.y, z, 1), bn_get(b, vol, c.x, c.y, z, 2));
+}
+static i3 bn_origin(const orc_bounce *b, const float *vol) {
+  int32_t z = 6 * (int32_t)b->dz;
+  return I(f2i(bn_get(b, vol, 0, 0, z, 0)), f2i(bn_get(b, vol, 0, 0, z, 1)), f2i(bn_get(b, vol, 0, 0, z, 2)));
+}
+/* WGSL smoothstep */
+static float smoothstep_(float e0, float e1, float x) {
+  float t = fclampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+/* bnRead (bounce.ts:49-74) */
+static v3 bn_read(const orc_bounce *b, const float *vol, v3 q, v3 p, v3 n) {
+  i3 org0 = bn_origin(b, vol);
+  v3 g = sub(V(q.x / b->cell, q.y / b->cell, q.z / b->cell), vi2f(org0));
+  i3 bb = vf2i(vfloor(g));
+  v3 fr = sub(g, vi2f(bb)), n2 = mul(n, n);
+  float tol = 0.5f * b->v0;
+  v3 e = V(0.0f, 0.0f, 0.0f);
+  float ws = 0.0f;
+  for (int k = 0; k < 8; k++) {
+    i3 off = I(k & 1, (k >> 1) & 1, (k >> 2) & 1);
+    i3 cc = I(bb.x + off.x, bb.y + off.y, bb.z + off.z);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= (int32_t)b->dx || cc.y >= (int32_t)b->dy || cc.z >= (int32_t)b->dz) continue;
+    v3 pp = muls(vi2f(I(org0.x + cc.x, org0.y + cc.y, org0.z + cc.z)), b->cell);
+    v3 u = sub(q, pp);
+    if (bn_axis_a(b, vol, cc, 0) <= 0.0f) continue;
+    if (fabsf(u.x) > bn_axis_a(b, vol, cc, u.x >= 0.0f ? 0 : 1) + tol || fabsf(u.y) > bn_axis_a(b, vol, cc, u.y >= 0.0f ? 2 : 3) + tol
+        || fabsf(u.z) > bn_axis_a(b, vol, cc, u.z >= 0.0f ? 4 : 5) + tol) continue;
+    v3 t3 = V(off.x == 1 ? fr.x : 1.0f - fr.x, off.y == 1 ? fr.y : 1.0f - fr.y, off.z == 1 ? fr.z : 1.0f - fr.z);
+    float w = t3.x * t3.y * t3.z * smoothstep_(-0.05f, 0.25f, dot(sub(pp, p), n) / b->cell);
+    if (w <= 0.0f) continue;
+    v3 s = add(add(muls(bn_axis_rgb(b, vol, cc, n.x >= 0.0f ? 0 : 1), n2.x), muls(bn_axis_rgb(b, vol, cc, n.y >= 0.0f ? 2 : 3), n2.y)),
+               muls(bn_axis_rgb(b, vol, cc, n.z >= 0.0f ? 4 : 5), n2.z));
+    e = add(e, muls(s, w));
+    ws += w;
+  }
+  return ws > 1e-6f ? divs(e, ws) : V(0.0f, 0.0f, 0.0f);
+}
+/* voxSide (rc.ts:120-124) */
+static float vox_side(v3 p, v3 n, v3 d, v3 pc, float v) {
+  float s = dot(sub(p, pc), n);
+  if (fabsf(s) > 0.05f * v) return s > 0.0f ? 1.0f : -1.0f;
+  return dot(n, d) > 0.0f ? -1.0f : 1.0f;
+}
+
+/* The hit: attributes of voxel (brick, bit), shaded (voxShade, rc.ts:136-140) plus the emissive radiance.  entry: where
+ * the ray enters the voxel; pc, vsz: its centre and size (the multi-bounce term's side and shading point). */
+static void shade_voxel(const ctx_t *cx, uint32_t brick, uint32_t bit, v3 d, v3 entry, v3 pc, float vsz, trace_t *out) {
   const orc_vox *vx = cx->vx;
   uint32_t w[4] = {0, 0, 0, 0};
   float vis = 0.0f;
-  if (vx->base[brick] != ORC_EMPTY) {
-    uint32_t ai = vox_rank(vx, brick, bit);
+  uint32_t ai = 0;
+  int has = vx->base[brick] != ORC_EMPTY;
+  if (has) {
+    ai = vox_rank(vx, brick, bit);
     for (int k = 0; k < 4; k++) w[k] = vx->attr[ai * 4u + k];
     vis = vx->sunvis[ai];
   }
@@ -149,7 +207,17 @@ static void shade_voxel(const ctx_t *cx, uint32_t brick, uint32_t bit, v3 d, tra
   float q = fmaxf_(-n.z, 0.0f);
   n.x += n.x >= 0.0f ? -q : q;
   n.y += n.y >= 0.0f ? -q : q;
-  v3 r = shade_hit_v(cx->F, n, alb, d, V(0.0f, 0.0f, 0.0f), vis);
+  /* voxBounce: the irradiance e at the shading point p = entry - d vsz / 4 */
+  v3 e = V(0.0f, 0.0f, 0.0f);
+  v3 p = sub(entry, muls(d, 0.25f * vsz));
+  if (has && cx->bn) {
+    if (dot(n, n) <= 0.01f) e = bn_read(cx->bn, cx->bn_prev, p, p, neg(d));
+    else e = bn_read(cx->bn, cx->bn_prev, p, p, muls(n, vox_side(p, n, d, pc, vsz)));
+  } else if (has && vx->bn_inj) {
+    const float *q = vx->bn_inj + (size_t)ai * 6u + (vox_side(p, n, d, pc, vsz) < 0.0f ? 3u : 0u);
+    e = V(q[0], q[1], q[2]);
+  }
+  v3 r = shade_hit_v(cx->F, n, alb, d, e, vis);
   v3 em = V(orc_f16_to_f32((uint16_t)(w[2] & 0xffffu)), orc_f16_to_f32((uint16_t)(w[2] >> 16)), orc_f16_to_f32((uint16_t)(w[3] & 0xffffu)));
   r = add(r, em);
   out->r = r.x; out->g = r.y; out->b = r.z; out->T = 0.0f;
@@ -186,7 +254,10 @@ static void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tsk
       uint32_t r[3];
       vox_at(vx, L, c, r);
       if (r[0] != ORC_EMPTY && tIn >= tskip) {
-        shade_voxel(cx, r[0], r[1], d, out);
+        float vl = vox_size(vx, r[2]);
+        v3 pcl = add(lo, muls(adds(vi2f(c), 0.5f), v));
+        v3 pc = muls(adds(vfloor(divs(pcl, vl)), 0.5f), vl);
+        shade_voxel(cx, r[0], r[1], d, add(o, muls(d, tIn)), pc, vl, out);
         out->lvl = r[2]; out->ptr = r[0]; out->bit = r[1]; out->tin = ubits(tIn);
         return;
       }
@@ -216,7 +287,7 @@ static void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tsk
     uint32_t occ = vx->occ[ptr * 16u + (bit >> 5)];
     float tExit = fminf_(fminf_(tMax.x, tMax.y), tMax.z);
     if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
-      shade_voxel(cx, ptr, bit, d, out);
+      shade_voxel(cx, ptr, bit, d, add(o, muls(d, tIn)), add(lo, muls(adds(vi2f(c), 0.5f), v)), v, out);
       out->lvl = L; out->ptr = ptr; out->bit = bit; out->tin = ubits(tIn);
       return;
     }
@@ -283,7 +354,7 @@ static void trace_range(void *p, uint64_t b, uint64_t e) {
 }
 
 int orc_rc_trace(const orc_vox *vx, const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o) {
-  ctx_t cx = {vx, g->frame, {g->frame[F_SKY], g->frame[F_SKY + 1], g->frame[F_SKY + 2]}};
+  ctx_t cx = {vx, g->frame, {g->frame[F_SKY], g->frame[F_SKY + 1], g->frame[F_SKY + 2]}, NULL, NULL};
   const float *F = g->frame;
   int32_t W = (int32_t)g->width, H = (int32_t)g->height;
   memset(o->counts, 0, 80 * 4);
@@ -482,5 +553,142 @@ int orc_rc_merge_gather(const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o) 
   }
   orc_parallel((uint64_t)ly->c[0].tiles_x * ly->c[0].tiles_y, 256, sh_range, &j);
   orc_parallel(g->height, 4, gather_range, &j);
+  return 0;
+}
+
+/* ---- the multi-bounce volume's frame (bounce.ts:96-246, Bounce.encode :356-368) ---- */
+#define BN_DDA_CAP 1024u   /* traceVox's step cap (voxel.ts:142) for the volume's rays */
+
+static float f16r(float x) { return orc_f16_to_f32(orc_f32_to_f16(x)); }
+static void bn_put(const orc_bounce *b, float *vol, i3 c, int a, float x, float y, float z, float w) {
+  float *t = vol + (((size_t)(a * (int32_t)b->dz + c.z) * b->dy + (size_t)c.y) * b->dx + (size_t)c.x) * 4u;
+  t[0] = f16r(x); t[1] = f16r(y); t[2] = f16r(z); t[3] = f16r(w);
+}
+/* occAt (bounce.ts:99-104) */
+static int bn_occ_at(const orc_vox *vx, uint32_t L, v3 p) {
+  float vs = vox_size(vx, L);
+  i3 c = vf2i(vfloor(divs(sub(p, muls(muls(vi2f(org(vx, L)), vs), 8.0f)), vs)));
+  int32_t n = (int32_t)vx->G * 8;
+  if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= n || c.y >= n || c.z >= n) return 0;
+  uint32_t r[3];
+  vox_at(vx, L, c, r);
+  return r[0] != ORC_EMPTY;
+}
+/* bnTrace (bounce.ts:156-167) */
+static void bn_trace(const ctx_t *cx, const orc_bounce *b, v3 o, v3 d, float tmax, float out[4]) {
+  const orc_vox *vx = cx->vx;
+  float b0 = 0.0f;
+  for (uint32_t k = 0; k < vx->levels && b0 * b->cell < tmax; k++) {
+    float b1 = b0 * 4.0f + 1.0f;
+    uint32_t L = vox_level_for(vx, k, add(o, muls(muls(d, b1), b->cell)));
+    trace_t r;
+    trace_vox(cx, o, d, b0 * b->cell, fminf_(b1 * b->cell, tmax), 0.0f, L, BN_DDA_CAP, &r);
+    if (r.T < 0.5f) {
+      v3 entry = add(o, muls(d, fbits(r.tin)));
+      out[0] = r.r; out[1] = r.g; out[2] = r.b; out[3] = dot(sub(entry, o), d);
+      return;
+    }
+    b0 = b1;
+  }
+  out[0] = cx->sky[0]; out[1] = cx->sky[1]; out[2] = cx->sky[2]; out[3] = 1e9f;
+}
+static v3 bn_axis_vec(uint32_t a) {
+  float s = (a & 1u) == 1u ? -1.0f : 1.0f;
+  return a / 2u == 0u ? V(s, 0.0f, 0.0f) : (a / 2u == 1u ? V(0.0f, s, 0.0f) : V(0.0f, 0.0f, s));
+}
+
+int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *F, float *inj_out) {
+  /* bnClear */
+  b->list[0] = 0u; b->list[1] += 1u; b->list[2] ^= 1u;
+  float *cur = b->vol[b->list[2]];
+  const float *prev = b->vol[b->list[2] ^ 1u];
+  const uint32_t n = b->dx * b->dy * b->dz;
+  const i3 o = I(f2i(floorf(F[F_EYE] / b->cell)) - (int32_t)(b->dx / 2u), f2i(floorf(F[F_EYE + 1] / b->cell)) - (int32_t)(b->dy / 2u),
+                 f2i(floorf(F[F_EYE + 2] / b->cell)) - (int32_t)(b->dz / 2u));
+  /* bnClassify (bounce.ts:112-138) */
+  bn_put(b, cur, I(0, 0, 0), 6, (float)o.x, (float)o.y, (float)o.z, 0.0f);
+  int32_t lr = (int32_t)orc_round_log2(fmaxf_(b->cell, 1e-4f) / b->v0);
+  uint32_t L = (uint32_t)(lr < 0 ? 0 : (lr > (int32_t)vx->levels - 1 ? (int32_t)vx->levels - 1 : lr));
+  for (uint32_t i = 0; i < n; i++) {
+    i3 c = I((int32_t)(i % b->dx), (int32_t)((i / b->dx) % b->dy), (int32_t)(i / (b->dx * b->dy)));
+    v3 p = muls(vi2f(I(o.x + c.x, o.y + c.y, o.z + c.z)), b->cell);
+    int near = 0;
+    for (uint32_t k = 0; k < 8u && !near; k++)
+      near = bn_occ_at(vx, L, add(p, muls(adds(V((float)(k & 1u), (float)((k >> 1) & 1u), (float)(k >> 2)), -0.5f), b->cell)));
+    if (near && !bn_occ_at(vx, 0u, p)) {
+      i3 w = I(o.x + c.x, o.y + c.y, o.z + c.z);
+      if (b->div > 1u && ((uint32_t)(w.x + w.y + w.z + 1048576) + b->list[1]) % b->div != 0u) {
+        i3 po = bn_origin(b, prev);
+        i3 pc = I(w.x - po.x, w.y - po.y, w.z - po.z);
+        if (pc.x >= 0 && pc.y >= 0 && pc.z >= 0 && pc.x < (int32_t)b->dx && pc.y < (int32_t)b->dy && pc.z < (int32_t)b->dz
+            && bn_axis_a(b, prev, pc, 0) > 0.0f) {
+          for (int a = 0; a < 6; a++) {
+            v3 t = bn_axis_rgb(b, prev, pc, a);
+            bn_put(b, cur, c, a, t.x, t.y, t.z, bn_axis_a(b, prev, pc, a));
+          }
+          continue;
+        }
+      }
+      b->list[4u + b->list[0]++] = i;
+    } else {
+      for (int a = 0; a < 6; a++) bn_put(b, cur, c, a, 0.0f, 0.0f, 0.0f, 0.0f);
+    }
+  }
+  /* bnUpdate (bounce.ts:172-208) */
+  ctx_t cx = {vx, F, {F[F_SKY], F[F_SKY + 1], F[F_SKY + 2]}, b, prev};
+  float rad[64][4];
+  float reach[6];
+  for (uint32_t slot = 0; slot < b->list[0]; slot++) {
+    uint32_t i = b->list[4u + slot];
+    i3 c = I((int32_t)(i % b->dx), (int32_t)((i / b->dx) % b->dy), (int32_t)(i / (b->dx * b->dy)));
+    v3 p = muls(vi2f(I(o.x + c.x, o.y + c.y, o.z + c.z)), b->cell);
+    for (uint32_t r = 0; r < b->rays; r++) bn_trace(&cx, b, p, fromf(b->dirs + 4u * r), 1e9f, rad[r]);
+    for (uint32_t a = 0; a < 6u; a++) {
+      float t[4];
+      bn_trace(&cx, b, p, bn_axis_vec(a), 1.5f * b->cell, t);
+      reach[a] = fmaxf_(fminf_(t[3], 1.5f * b->cell), 1e-3f);
+    }
+    for (uint32_t a = 0; a < 6u; a++) {
+      v3 axis = bn_axis_vec(a), e = V(0.0f, 0.0f, 0.0f);
+      float ws = 0.0f;
+      for (uint32_t r = 0; r < b->rays; r++) {
+        float w = fmaxf_(dot(axis, fromf(b->dirs + 4u * r)), 0.0f);
+        e = add(e, muls(V(rad[r][0], rad[r][1], rad[r][2]), w));
+        ws += w;
+      }
+      v3 irr = divs(muls(e, PI_F), fmaxf_(ws, 1e-6f));
+      bn_put(b, cur, c, (int)a, irr.x, irr.y, irr.z, reach[a]);
+    }
+  }
+  /* bnInject (bounce.ts:213-246) */
+  uint32_t nb = vx->hdr[0] < vx->max_bricks ? vx->hdr[0] : vx->max_bricks;
+  for (uint32_t ptr = 0; ptr < nb; ptr++) {
+    uint32_t first = vx->base[ptr];
+    if (first >= ORC_MARK) continue;
+    uint32_t code = vx->code[ptr], Lv = code >> 27;
+    i3 bc = I((int32_t)((code >> 18) & 511u), (int32_t)((code >> 9) & 511u), (int32_t)(code & 511u));
+    float vs = vox_size(vx, Lv);
+    v3 lo = muls(muls(vi2f(org(vx, Lv)), vs), 8.0f);
+    uint32_t r = 0;
+    for (uint32_t bit = 0; bit < 512u; bit++) {
+      if ((vx->occ[ptr * 16u + (bit >> 5)] & (1u << (bit & 31u))) == 0u) continue;
+      uint32_t ai = first + r++;
+      i3 cc = I(bc.x * 8 + (int32_t)(bit & 7u), bc.y * 8 + (int32_t)((bit >> 3) & 7u), bc.z * 8 + (int32_t)(bit >> 6));
+      v3 p = add(lo, muls(adds(vi2f(cc), 0.5f), vs));
+      uint32_t e = vx->attr[ai * 4u + 1u];
+      float ex = fmaxf_((float)(int16_t)(e & 0xffffu) / 32767.0f, -1.0f);
+      float ey = fmaxf_((float)(int16_t)(e >> 16) / 32767.0f, -1.0f);
+      v3 nn = V(ex, ey, 1.0f - fabsf(ex) - fabsf(ey));
+      float q0 = fmaxf_(-nn.z, 0.0f);
+      nn.x += nn.x >= 0.0f ? -q0 : q0;
+      nn.y += nn.y >= 0.0f ? -q0 : q0;
+      v3 nf = dot(nn, nn) > 0.01f ? normalize3(nn) : V(0.0f, 1.0f, 0.0f);
+      float off = Lv == 0u ? 0.0f : 0.5f * vs;
+      v3 ef = bn_read(b, cur, add(p, muls(nf, off)), p, nf);
+      v3 eb = bn_read(b, cur, add(p, muls(neg(nf), off)), p, neg(nf));
+      float *q = inj_out + (size_t)ai * 6u;
+      q[0] = f16r(ef.x); q[1] = f16r(ef.y); q[2] = f16r(ef.z); q[3] = f16r(eb.x); q[4] = f16r(eb.y); q[5] = f16r(eb.z);
+    }
+  }
   return 0;
 }

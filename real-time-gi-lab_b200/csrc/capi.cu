@@ -133,6 +133,9 @@ struct gi_rc {
   float4 *sm_rec = nullptr;          // its raster scratch, for up to sm_tris triangles
   uint32_t *sm_pre = nullptr, *sm_sums = nullptr, *sm_counter = nullptr;
   uint32_t sm_tris = 0;
+  bool bounce = false;               // gi_rc_set_bounce: the volume, its buffers and the voxel world it is bound to
+  BounceDev bn = {};
+  gi_vox *bn_vox = nullptr;
 };
 
 static void free_scene(gi_scene *s) {
@@ -157,6 +160,10 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
   cudaFree((void *)r->dev.unorm8);
   cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
+  cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
+  r->bn = BounceDev{};
+  r->bounce = false;
+  r->dev.bn_inj = nullptr;
 }
 
 extern "C" {
@@ -686,8 +693,69 @@ int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
   return GI_OK;
 }
 
+// sfDir (bounce.ts:147-152): z = 1 - (2i + 1) / n, r = sqrt(max(0, 1 - z^2)), phi = 2 pi fract(i 0.618033988749), the
+// f32 steps as the shader does them and cos / sin of the f32 phi in double precision (the shader's are
+// implementation-defined)
+static void bounce_dirs(uint32_t n, float4 *out) {
+  for (uint32_t i = 0; i < n; i++) {
+    volatile float fi = (float)i, fn = (float)n;
+    volatile float z = 1.0f - (2.0f * fi + 1.0f) / fn;
+    volatile float zz = 1.0f - z * z;
+    float r = sqrtf(zz > 0.0f ? zz : 0.0f);
+    volatile float xi = fi * 0.618033988749f;
+    volatile float fr = xi - floorf(xi);
+    volatile float phi = 2.0f * 3.14159265f * fr;
+    volatile float cx = (float)cos((double)phi), sy = (float)sin((double)phi);
+    volatile float x = r * cx, y = r * sy;
+    out[i] = make_float4(x, y, z, 0.0f);
+  }
+}
+
+int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_bounce: NULL rc");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_bounce: cudaSetDevice");
+  cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
+  r->bn = BounceDev{};
+  r->bounce = false;
+  r->bn_vox = nullptr;
+  r->dev.bn_inj = nullptr;
+  if (!p) return GI_OK;
+  if (!v) return fail(GI_ERR_INVALID, "gi_rc_set_bounce: NULL voxel world");
+  if (v->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_set_bounce: voxel world on another device");
+  if (!(p->cell > 0.0f) || p->dx < 1 || p->dy < 1 || p->dz < 1 || p->dx > 1024 || p->dy > 1024 || p->dz > 1024 ||
+      (uint64_t)p->dx * p->dy * p->dz > (1u << 24) || p->rays < 1 || p->rays > 26 || p->div < 1)
+    return fail(GI_ERR_INVALID, "gi_rc_set_bounce: cell > 0, dims 1..1024 (at most 2^24 probes), rays 1..26, div >= 1");
+  BounceDev &b = r->bn;
+  b.cell = p->cell; b.v0 = v->dev.vs[0];
+  b.dx = p->dx; b.dy = p->dy; b.dz = p->dz; b.rays = p->rays; b.div = p->div; b.n = p->dx * p->dy * p->dz;
+  b.levels = v->dev.levels;
+  size_t texels = (size_t)b.dx * b.dy * (6u * b.dz + 1u);
+  float4 hdirs[32];
+  bounce_dirs(b.rays, hdirs);
+  float4 *dirs = nullptr;
+  cudaError_t e;
+  if ((e = dalloc(&dirs, b.rays)) || (e = dalloc(&b.vol[0], texels)) || (e = dalloc(&b.vol[1], texels)) ||
+      (e = dalloc(&b.list, 4u + (size_t)b.n)) || (e = dalloc(&b.inj, (size_t)v->p.max_voxels))) {
+    cudaFree(dirs); b.dirs = nullptr;
+    cudaFree(b.vol[0]); cudaFree(b.vol[1]); cudaFree(b.list); cudaFree(b.inj);
+    r->bn = BounceDev{};
+    return cuda_fail(e, "gi_rc_set_bounce");
+  }
+  b.dirs = dirs;
+  CK(cudaMemcpy(dirs, hdirs, b.rays * sizeof(float4), cudaMemcpyHostToDevice), "gi_rc_set_bounce: copy");
+  CK(cudaMemset(b.vol[0], 0, texels * sizeof(uint2)), "gi_rc_set_bounce: clear");
+  CK(cudaMemset(b.vol[1], 0, texels * sizeof(uint2)), "gi_rc_set_bounce: clear");
+  CK(cudaMemset(b.list, 0, (4u + (size_t)b.n) * 4u), "gi_rc_set_bounce: clear");
+  CK(cudaMemset(b.inj, 0, (size_t)v->p.max_voxels * sizeof(uint4)), "gi_rc_set_bounce: clear");
+  r->bounce = true;
+  r->bn_vox = v;
+  r->dev.bn_inj = b.inj;
+  return GI_OK;
+}
+
 int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   if (!r || !v) return fail(GI_ERR_INVALID, "gi_rc_solve: NULL argument");
+  if (r->bounce && v != r->bn_vox) return fail(GI_ERR_INVALID, "gi_rc_solve: multi-bounce is bound to another voxel world");
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_solve: no frame set");
   if (!r->gbuf_set) return fail(GI_ERR_STATE, "gi_rc_solve: no G-buffer set");
   if (!v->updated) return fail(GI_ERR_STATE, "gi_rc_solve: the voxel world was never updated");
@@ -695,7 +763,8 @@ int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_solve: cudaSetDevice");
   r->dev.hits = r->debug_hits ? r->hits : nullptr;
   r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
-  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr, &r->launch),
+  CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr, &r->launch,
+                        r->bounce ? &r->bn : nullptr),
      "gi_rc_solve: launch");
   r->timed = r->timing;
   r->timed_vox = false;
@@ -881,6 +950,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
       return fail(GI_ERR_STATE, "gi_batch_capture_passes: solve %u lacks its frame, G-buffer or voxel window", i);
     if (r->dev.atlas != r0.atlas || r->dev.c[0].tile_size != r0.c[0].tile_size)
       return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has another atlas format or probe spacing than solve 0", i);
+    if (r->bounce) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has multi-bounce on (capture its chain with gi_batch_capture)", i);
   }
   const uint32_t P0 = r0.c[0].tile_size;
   if (P0 != 8u && P0 != 16u && P0 != 32u)
@@ -1114,6 +1184,9 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
     case GI_RC_NORMAL: *bytes = npx * 8u; break;
     case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;
     case GI_RC_SHADOW: *bytes = (size_t)r->shadow_size * r->shadow_size * 4u; break;
+    case GI_RC_BOUNCE_VOL: *bytes = r->bounce ? 2u * (size_t)r->bn.dx * r->bn.dy * (6u * r->bn.dz + 1u) * 8u : 0u; break;
+    case GI_RC_BOUNCE_INJ: *bytes = r->bounce ? (size_t)r->bn_vox->p.max_voxels * 16u : 0u; break;
+    case GI_RC_BOUNCE_LIST: *bytes = r->bounce ? (4u + (size_t)r->bn.n) * 4u : 0u; break;
     default: return fail(GI_ERR_INVALID, "gi_rc_buffer_bytes: unknown buffer %d", what);
   }
   return GI_OK;
@@ -1135,6 +1208,18 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
     case GI_RC_HITS: src = r->hits; break;
     case GI_RC_RAD_TRACED: src = r->rad_traced; break;
     case GI_RC_SHADOW: src = r->shadow; break;
+    case GI_RC_BOUNCE_INJ: src = r->bn.inj; break;
+    case GI_RC_BOUNCE_LIST: src = r->bn.list; break;
+    case GI_RC_BOUNCE_VOL:
+      if (r->bounce) {   // two allocations: copy them one after the other
+        size_t half = need / 2u;
+        CK(cudaSetDevice(r->ctx->device), "gi_rc_read_buffer: cudaSetDevice");
+        CK(cudaMemcpyAsync(out, r->bn.vol[0], half, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_buffer: copy");
+        CK(cudaMemcpyAsync((char *)out + half, r->bn.vol[1], half, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_buffer: copy");
+        CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_buffer: sync");
+        return GI_OK;
+      }
+      break;
   }
   if (!src) return fail(GI_ERR_STATE, "gi_rc_read_buffer: buffer %d not kept (debug hits off, or no shadow map)", what);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_buffer: cudaSetDevice");

@@ -45,6 +45,20 @@ struct RcDev {
   void *rad_traced;        // optional: copy of the atlas after the trace
   float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
   const float *unorm8;     // k / 255.0f for k = 0..255 (IEEE quotients, computed on the host)
+  const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)
+};
+
+// The multi-bounce volume (bounce.ts): dx x dy x dz irradiance probes around the camera, rebuilt every frame from the
+// voxels, each an ambient cube (six axes: rgb irradiance, alpha the reach along the axis), stored rgba16f in two
+// volumes that swap every frame (this frame's is written, the previous one read by the probes' own rays).
+struct BounceDev {
+  float cell, v0;              // probe spacing (m); the clipmap's level-0 voxel size (the reach tolerance)
+  uint32_t dx, dy, dz, rays, div, n, levels;   // n = dx dy dz probes
+  const float4 *dirs;          // sfDir(r, rays) (bounce.ts:147-152), computed on the host
+  uint2 *vol[2];               // dx * dy * (6 dz + 1) texels, texel (x, y, z) at (z dy + y) dx + x; z = a dz + probe z,
+                               // texel (0, 0, 6 dz) holds the volume's origin in probe coordinates
+  uint32_t *list;              // [0] probes listed this frame, [1] frame counter, [2] this frame's volume, [4..) list
+  uint4 *inj;                  // per voxel: front rg, front b | 0, back rg, back b | 0 (f16 pairs)
 };
 
 // Scratch of the binned G-buffer raster (gbuffer.cu)
@@ -134,7 +148,7 @@ struct BatchSizes { uint32_t setup_blocks, merge_blocks[8], gather_blocks, atlas
 }  // namespace gi
 cudaError_t gi_launch_batch_passes(const gi::BatchDev &b, const gi::BatchSizes &z, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
-                               cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr);
+                               cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr, const gi::BounceDev *bn = nullptr);
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);

@@ -77,13 +77,93 @@ __device__ __forceinline__ f3 toon_albedo(f3 a) {
 }
 __device__ __forceinline__ float toon_ramp(float x) { return x > 0.3f ? 1.0f : (x > 0.05f ? 0.5f : 0.0f); }
 
-// voxShade (rc.ts:136-140) -> shadeHitV (rc.ts:108-116) with no multi-bounce, plus the voxel's emissive radiance
+// ---- multi-bounce reads (bounce.ts:44-75, 90-93; rc.ts:198-202) ---------------------------------------------------
+__device__ __forceinline__ float4 bn_texel(const BounceDev &b, const uint2 *vol, int x, int y, int z) {
+  uint2 u = vol[((size_t)z * b.dy + (size_t)y) * b.dx + (size_t)x];
+  return make_float4(h2f(u.x & 0xffffu), h2f(u.x >> 16), h2f(u.y & 0xffffu), h2f(u.y >> 16));
+}
+__device__ __forceinline__ float4 bn_axis(const BounceDev &b, const uint2 *vol, i3 c, int a) {
+  return bn_texel(b, vol, c.x, c.y, a * (int)b.dz + c.z);
+}
+__device__ __forceinline__ i3 bn_origin(const BounceDev &b, const uint2 *vol) {   // bnOrigin
+  float4 o = bn_texel(b, vol, 0, 0, 6 * (int)b.dz);
+  return mki(f2i(o.x), f2i(o.y), f2i(o.z));
+}
+// WGSL smoothstep: t = clamp((x - e0) / (e1 - e0), 0, 1), t t (3 - 2 t)
+__device__ __forceinline__ float smoothstep_(float e0, float e1, float x) {
+  float t = fclampf((x - e0) / (e1 - e0), 0.0f, 1.0f);
+  return t * t * (3.0f - 2.0f * t);
+}
+// bnRead (bounce.ts:49-74): the irradiance on the side n of a surface at p, read at q, trilinear over the 8 probes
+// around q that are active, on that side and whose reach along their axes covers q
+__device__ f3 bn_read(const BounceDev &b, const uint2 *vol, f3 q, f3 p, f3 n) {
+  const i3 org = bn_origin(b, vol);
+  const f3 g = mk(q.x / b.cell, q.y / b.cell, q.z / b.cell) - vi2f(org);
+  const i3 bb = vf2i(vfloor(g));
+  const f3 fr = g - vi2f(bb), n2 = n * n;
+  const float tol = 0.5f * b.v0;
+  f3 e = mk(0.0f, 0.0f, 0.0f);
+  float ws = 0.0f;
+  for (int k = 0; k < 8; k++) {
+    const i3 off = mki(k & 1, (k >> 1) & 1, (k >> 2) & 1);
+    const i3 cc = mki(bb.x + off.x, bb.y + off.y, bb.z + off.z);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= (int)b.dx || cc.y >= (int)b.dy || cc.z >= (int)b.dz) continue;
+    const f3 pp = vi2f(mki(org.x + cc.x, org.y + cc.y, org.z + cc.z)) * b.cell;
+    const f3 u = q - pp;
+    if (bn_axis(b, vol, cc, 0).w <= 0.0f) continue;
+    if (fabsf(u.x) > bn_axis(b, vol, cc, u.x >= 0.0f ? 0 : 1).w + tol || fabsf(u.y) > bn_axis(b, vol, cc, u.y >= 0.0f ? 2 : 3).w + tol
+        || fabsf(u.z) > bn_axis(b, vol, cc, u.z >= 0.0f ? 4 : 5).w + tol) continue;
+    const f3 t3 = mk(off.x == 1 ? fr.x : 1.0f - fr.x, off.y == 1 ? fr.y : 1.0f - fr.y, off.z == 1 ? fr.z : 1.0f - fr.z);
+    const float w = t3.x * t3.y * t3.z * smoothstep_(-0.05f, 0.25f, dot(pp - p, n) / b.cell);
+    if (w <= 0.0f) continue;
+    const float4 ax = bn_axis(b, vol, cc, n.x >= 0.0f ? 0 : 1), ay = bn_axis(b, vol, cc, n.y >= 0.0f ? 2 : 3);
+    const float4 az = bn_axis(b, vol, cc, n.z >= 0.0f ? 4 : 5);
+    e = e + ((mk(ax.x, ax.y, ax.z) * n2.x + mk(ay.x, ay.y, ay.z) * n2.y) + mk(az.x, az.y, az.z) * n2.z) * w;
+    ws += w;
+  }
+  return ws > 1e-6f ? e / ws : mk(0.0f, 0.0f, 0.0f);
+}
+// voxSide (rc.ts:120-124): the side of the voxel the ray comes from
+__device__ __forceinline__ float vox_side(f3 p, f3 n, f3 d, f3 pc, float v) {
+  float s = dot(p - pc, n);
+  if (fabsf(s) > 0.05f * v) return s > 0.0f ? 1.0f : -1.0f;
+  return dot(n, d) > 0.0f ? -1.0f : 1.0f;
+}
+// The cascades' voxBounce (rc.ts:198-202): the irradiance bnInject stored for the side the ray comes from; 0 with
+// multi-bounce off
+struct InjectedBounce {
+  const uint4 *inj;
+  __device__ __forceinline__ f3 operator()(uint32_t ai, bool has, f3 p, f3 n, f3 d, f3 pc, float v) const {
+    if (!inj || !has) return mk(0.0f, 0.0f, 0.0f);
+    const uint4 w = inj[ai];
+    const bool back = vox_side(p, n, d, pc, v) < 0.0f;
+    const uint32_t a = back ? w.z : w.x, c = back ? w.w : w.y;
+    return mk(h2f(a & 0xffffu), h2f(a >> 16), h2f(c & 0xffffu));
+  }
+};
+// The bounce volume's own rays (bounce.ts:90-93): the previous frame's volume, read at the hit
+struct VolumeBounce {
+  const BounceDev *b;
+  const uint2 *prev;
+  __device__ __forceinline__ f3 operator()(uint32_t, bool has, f3 p, f3 n, f3 d, f3 pc, float v) const {
+    if (!has) return mk(0.0f, 0.0f, 0.0f);   // no attributes: the albedo is 0 and so is the reflected term
+    if (dot(n, n) <= 0.01f) return bn_read(*b, prev, p, p, -d);
+    return bn_read(*b, prev, p, p, n * vox_side(p, n, d, pc, v));
+  }
+};
+
+// voxShade (rc.ts:136-140) -> shadeHitV (rc.ts:108-116), plus the voxel's emissive radiance.  entry: where the ray
+// enters the voxel; pc, vsz: the voxel's centre and size; bs: the irradiance e of the multi-bounce term at the shading
+// point p = entry - d vsz / 4.
+template <class BS>
 __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ r_unorm8,
-                                          uint32_t brick, uint32_t bit, f3 d) {
+                                          uint32_t brick, uint32_t bit, f3 d, f3 entry, f3 pc, float vsz, const BS &bs) {
   uint4 w = make_uint4(0, 0, 0, 0);
   float vis = 0.0f;
-  if (v.base[brick] != GI_EMPTY) {
-    uint32_t ai = vox_rank(v, brick, bit);
+  uint32_t ai = 0;
+  const bool has = v.base[brick] != GI_EMPTY;
+  if (has) {
+    ai = vox_rank(v, brick, bit);
     w = v.attr[ai];
     vis = v.sunvis[ai];
   }
@@ -103,19 +183,18 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   f3 n = dot(n0, n0) > 0.01f ? n0 : -d;
   if (dot(n, d) > 0.0f) n = -n;
   f3 a = mk(alb0, alb1, alb2);
-  f3 r = mk(0.0f, 0.0f, 0.0f);   // shadeHitV's bounce term (a / pi) * E with E = 0: +0 for finite albedo
+  // a / pi for the 256 albedo values k / 255 as f64 products rounded to f32: equal to the f32 quotients (checked
+  // exhaustively in the CPU tests)
+  const double inv_pi = 1.0 / (double)GI_PI;
+  const f3 api = mk(__double2float_rn((double)a.x * inv_pi), __double2float_rn((double)a.y * inv_pi),
+                    __double2float_rn((double)a.z * inv_pi));
+  // the multi-bounce term b = a / pi * e (+0 with e = 0)
+  f3 r = api * bs(ai, has, entry - d * (0.25f * vsz), n0, d, pc, vsz);
   float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
   if (ndl > 0.0f) {
     f3 sunE = mk(F[F_SUNE], F[F_SUNE + 1], F[F_SUNE + 2]);
     if (alb3 > 0.5f && F[F_STYLE] > 0.5f) r = r + ((toon_albedo(a) / 3.14159265f) * sunE) * toon_ramp(ndl * vis);
-    else {
-      // a / pi for the 256 albedo values k / 255 as f64 products rounded to f32: equal to the f32 quotients (checked
-      // exhaustively in the CPU tests)
-      const double inv_pi = 1.0 / (double)GI_PI;
-      f3 api = mk(__double2float_rn((double)a.x * inv_pi), __double2float_rn((double)a.y * inv_pi),
-                  __double2float_rn((double)a.z * inv_pi));
-      r = r + ((api * sunE) * ndl) * vis;
-    }
+    else r = r + ((api * sunE) * ndl) * vis;
   }
   return r + mk(h2f(w.z & 0xffffu), h2f(w.z >> 16), h2f(w.w & 0xffffu));
 }
@@ -123,9 +202,10 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
 struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 
 // traceVox (voxel.ts:121-202) with a configurable step cap
+template <class BS>
 __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
                                           f3 o, f3 d, float t0, float t1,
-                                          float tskip, uint32_t L, uint32_t cap, TraceOut &out) {
+                                          float tskip, uint32_t L, uint32_t cap, TraceOut &out, const BS &bs) {
   out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
   out.steps = 0;
   float vs = vox_size(v, L);
@@ -154,7 +234,11 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
     if (ptr == GI_DROP) {
       uint3 r = vox_at(v, L, c);
       if (r.x != GI_EMPTY && tIn >= tskip) {
-        out.rad = shade_voxel(v, F, unorm8, r.x, r.y, d); out.T = 0.0f;
+        // the coarser voxel that holds the cell: its size and centre
+        const float vl = vox_size(v, r.z);
+        const f3 pcl = lo + adds(vi2f(c), 0.5f) * vs;
+        const f3 pc = adds(vfloor(pcl / vl), 0.5f) * vl;
+        out.rad = shade_voxel(v, F, unorm8, r.x, r.y, d, o + d * tIn, pc, vl, bs); out.T = 0.0f;
         out.lvl = r.z; out.ptr = r.x; out.bit = r.y; out.tin = __float_as_uint(tIn);
         return;
       }
@@ -185,7 +269,7 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
     uint32_t occ = __ldg(&v.occ[ptr * 16u + (bit >> 5)]);
     float tExit = mn(mn(tMax.x, tMax.y), tMax.z);
     if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
-      out.rad = shade_voxel(v, F, unorm8, ptr, bit, d); out.T = 0.0f;
+      out.rad = shade_voxel(v, F, unorm8, ptr, bit, d, o + d * tIn, lo + adds(vi2f(c), 0.5f) * vs, vs, bs); out.T = 0.0f;
       out.lvl = L; out.ptr = ptr; out.bit = bit; out.tin = __float_as_uint(tIn);
       return;
     }
@@ -281,7 +365,8 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
     f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
     uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
     float vs = vox_size(v, Lv);
-    trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out);
+    trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out,
+              InjectedBounce{r.bn_inj});
     traced = true;
   }
   Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -613,6 +698,202 @@ __global__ void __launch_bounds__(256) k_gather_tiled(RcDev r) {
   gather_tiles<A, P>(r, blockIdx.x, blockIdx.y);
 }
 
+// ---- the multi-bounce volume (bounce.ts): clear, classify, update, inject ------------------------------------------
+constexpr uint32_t BN_DDA_CAP = 1024;   // traceVox's step cap (voxel.ts:142) for the volume's rays
+
+__device__ __forceinline__ uint2 bn_pack(float4 x) {
+  return make_uint2((uint32_t)f2h(x.x) | ((uint32_t)f2h(x.y) << 16), (uint32_t)f2h(x.z) | ((uint32_t)f2h(x.w) << 16));
+}
+__device__ __forceinline__ size_t bn_index(const BounceDev &b, i3 c, int a) {
+  return ((size_t)(a * (int)b.dz + c.z) * b.dy + (size_t)c.y) * b.dx + (size_t)c.x;
+}
+// bnOriginNow (bounce.ts:98): the probe coordinates of this frame's probe 0
+__device__ __forceinline__ i3 bn_origin_now(const BounceDev &b, const float *__restrict__ F) {
+  return mki(f2i(floorf(F[F_EYE] / b.cell)) - (int)(b.dx / 2u), f2i(floorf(F[F_EYE + 1] / b.cell)) - (int)(b.dy / 2u),
+             f2i(floorf(F[F_EYE + 2] / b.cell)) - (int)(b.dz / 2u));
+}
+// occAt (bounce.ts:99-104)
+__device__ __forceinline__ bool bn_occ_at(const VoxDev &v, uint32_t L, f3 p) {
+  const float vs = vox_size(v, L);
+  const i3 c = vf2i(vfloor((p - (vi2f(org(v, L)) * vs) * 8.0f) / vs));
+  const int n = (int)v.G * 8;
+  if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= n || c.y >= n || c.z >= n) return false;
+  return vox_at(v, L, c).x != GI_EMPTY;
+}
+
+// bnClear (bounce.ts:107): the list empty, the frame counter on, the volumes swapped
+__global__ void k_bn_clear(BounceDev b) {
+  grid_dep_wait();
+  if (threadIdx.x == 0) { b.list[0] = 0u; b.list[1] += 1u; b.list[2] ^= 1u; }
+}
+
+// bnClassify (bounce.ts:112-138): one thread per probe (and one for the origin texel)
+__global__ void __launch_bounds__(256) k_bn_classify(BounceDev b, VoxDev v, const float *__restrict__ F) {
+  grid_dep_wait();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t cur = b.list[2];
+  uint2 *out = b.vol[cur];
+  const uint2 *prev = b.vol[cur ^ 1u];
+  const i3 o = bn_origin_now(b, F);
+  if (i == b.n) out[bn_index(b, mki(0, 0, 0), 6)] = bn_pack(make_float4((float)o.x, (float)o.y, (float)o.z, 0.0f));
+  if (i >= b.n) return;
+  const i3 c = mki((int)(i % b.dx), (int)((i / b.dx) % b.dy), (int)(i / (b.dx * b.dy)));
+  const f3 p = vi2f(mki(o.x + c.x, o.y + c.y, o.z + c.z)) * b.cell;
+  // levelOf(BN_CELL): round(log2(max(size, 1e-4) / v0)) clamped to the levels
+  int lr = round_log2(mx(b.cell, 1e-4f) / b.v0);
+  const uint32_t L = (uint32_t)(lr < 0 ? 0 : (lr > (int)v.levels - 1 ? (int)v.levels - 1 : lr));
+  bool near = false;
+  for (uint32_t k = 0; k < 8u && !near; k++)
+    near = bn_occ_at(v, L, p + adds(mk((float)(k & 1u), (float)((k >> 1) & 1u), (float)(k >> 2)), -0.5f) * b.cell);
+  if (near && !bn_occ_at(v, 0u, p)) {
+    // staggered: a probe is traced every div frames (by its world position), kept from the previous volume between
+    const i3 w = mki(o.x + c.x, o.y + c.y, o.z + c.z);
+    if (b.div > 1u && ((uint32_t)(w.x + w.y + w.z + 1048576) + b.list[1]) % b.div != 0u) {
+      const i3 po = bn_origin(b, prev);
+      const i3 pc = mki(w.x - po.x, w.y - po.y, w.z - po.z);
+      if (pc.x >= 0 && pc.y >= 0 && pc.z >= 0 && pc.x < (int)b.dx && pc.y < (int)b.dy && pc.z < (int)b.dz
+          && bn_axis(b, prev, pc, 0).w > 0.0f) {
+        for (int a = 0; a < 6; a++) out[bn_index(b, c, a)] = prev[bn_index(b, pc, a)];
+        return;
+      }
+    }
+    const uint32_t s = atomicAdd(&b.list[0], 1u);
+    b.list[4u + s] = i;
+  } else {
+    for (int a = 0; a < 6; a++) out[bn_index(b, c, a)] = make_uint2(0u, 0u);
+  }
+}
+
+// bnTrace (bounce.ts:156-167): the ray in segments [b_k, b_k+1] cells (b_k = (4^k - 1) / 3) on level k's voxels;
+// rgb and the distance to the hit (sky and 1e9 past the last level)
+__device__ float4 bn_trace(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
+                           const BounceDev &b, const uint2 *prev, f3 o, f3 d, float tmax) {
+  float b0 = 0.0f;
+  for (uint32_t k = 0; k < v.levels && b0 * b.cell < tmax; k++) {
+    const float b1 = b0 * 4.0f + 1.0f;
+    const uint32_t L = vox_level_for(v, k, o + (d * b1) * b.cell);
+    TraceOut r;
+    trace_vox(v, F, unorm8, o, d, b0 * b.cell, mn(b1 * b.cell, tmax), 0.0f, L, BN_DDA_CAP, r, VolumeBounce{&b, prev});
+    if (r.T < 0.5f) {
+      const f3 entry = o + d * __uint_as_float(r.tin);
+      return make_float4(r.rad.x, r.rad.y, r.rad.z, dot(entry - o, d));
+    }
+    b0 = b1;
+  }
+  return make_float4(F[F_SKY], F[F_SKY + 1], F[F_SKY + 2], 1e9f);
+}
+
+// bnUpdate (bounce.ts:172-208): one warp per listed probe.  Lanes [0, rays) trace the irradiance rays, lanes
+// [rays, rays + 6) the axis rays (reach up to the first occupied voxel, at most 1.5 cells), then lanes 0-5 sum the
+// ambient cube over the rays in order.
+__global__ void __launch_bounds__(256) k_bn_update(BounceDev b, VoxDev v, const float *__restrict__ F,
+                                                    const float *__restrict__ unorm8) {
+  grid_dep_wait();
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5), w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const uint32_t cur = b.list[2], count = b.list[0];
+  uint2 *out = b.vol[cur];
+  const uint2 *prev = b.vol[cur ^ 1u];
+  const i3 o = bn_origin_now(b, F);
+  for (uint32_t slot = w0; slot < count; slot += nwarps) {
+    const uint32_t i = b.list[4u + slot];
+    const i3 c = mki((int)(i % b.dx), (int)((i / b.dx) % b.dy), (int)(i / (b.dx * b.dy)));
+    const f3 p = vi2f(mki(o.x + c.x, o.y + c.y, o.z + c.z)) * b.cell;
+    float4 res = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (lane < b.rays) {
+      const float4 dv = b.dirs[lane];
+      res = bn_trace(v, F, unorm8, b, prev, p, mk(dv.x, dv.y, dv.z), 1e9f);
+    } else if (lane < b.rays + 6u) {
+      const uint32_t a = lane - b.rays;
+      f3 axis = mk(0.0f, 0.0f, 0.0f);
+      const float sg = (a & 1u) == 1u ? -1.0f : 1.0f;
+      if (a / 2u == 0u) axis.x = sg; else if (a / 2u == 1u) axis.y = sg; else axis.z = sg;
+      res.w = mx(mn(bn_trace(v, F, unorm8, b, prev, p, axis, 1.5f * b.cell).w, 1.5f * b.cell), 1e-3f);
+    }
+    f3 e = mk(0.0f, 0.0f, 0.0f);
+    float ws = 0.0f;
+    f3 axis = mk(0.0f, 0.0f, 0.0f);
+    const float sg = (lane & 1u) == 1u ? -1.0f : 1.0f;
+    if (lane / 2u == 0u) axis.x = sg; else if (lane / 2u == 1u) axis.y = sg; else axis.z = sg;
+    for (uint32_t r = 0; r < b.rays; r++) {
+      const f3 rad = mk(__shfl_sync(0xffffffffu, res.x, (int)r), __shfl_sync(0xffffffffu, res.y, (int)r),
+                        __shfl_sync(0xffffffffu, res.z, (int)r));
+      const float4 dv = b.dirs[r];
+      const float w = mx(dot(axis, mk(dv.x, dv.y, dv.z)), 0.0f);
+      e = e + rad * w;
+      ws += w;
+    }
+    const float reach = __shfl_sync(0xffffffffu, res.w, (int)(b.rays + (lane < 6u ? lane : 0u)));
+    if (lane < 6u) {
+      const f3 irr = (e * GI_PI) / mx(ws, 1e-6f);
+      out[bn_index(b, c, (int)lane)] = bn_pack(make_float4(irr.x, irr.y, irr.z, reach));
+    }
+  }
+}
+
+// bnInject (bounce.ts:213-246): every occupied voxel stores this frame's volume read on its two sides.  One thread
+// per voxel of the attribute pool (its brick by a binary search of the voxel prefix, as resolveAttr).
+__global__ void __launch_bounds__(256) k_bn_inject(BounceDev b, VoxDev v) {
+  grid_dep_wait();
+  const uint2 *cur = b.vol[b.list[2]];
+  const uint32_t nb = min(v.hdr[0], v.max_bricks);
+  const uint32_t nv = nb ? min(v.vpre[nb], v.max_voxels) : 0u;
+  for (uint32_t ai = blockIdx.x * blockDim.x + threadIdx.x; ai < nv; ai += gridDim.x * blockDim.x) {
+    uint32_t lo = 0, hi = nb;
+    while (hi - lo > 1u) {
+      uint32_t m = (lo + hi) >> 1;
+      if (v.vpre[m] <= ai) lo = m; else hi = m;
+    }
+    const uint32_t ptr = lo;
+    if (v.base[ptr] == GI_EMPTY) continue;
+    uint32_t r = ai - v.vpre[ptr], bit = 0;
+    const uint4 *o4 = reinterpret_cast<const uint4 *>(v.occ) + ptr * 4u;
+    for (int q = 0; q < 4; q++) {
+      const uint4 o = o4[q];
+      const uint32_t ws4[4] = {o.x, o.y, o.z, o.w};
+      for (int j = 0; j < 4; j++) {
+        const uint32_t pc = __popc(ws4[j]);
+        if (r < pc && bit == 0u) {
+          uint32_t wd = ws4[j];
+          for (uint32_t k = 0; k < r; k++) wd &= wd - 1u;
+          bit = (uint32_t)(q * 4 + j) * 32u + (uint32_t)(__ffs(wd) - 1) + 1u;
+        }
+        if (bit == 0u) r -= pc;
+      }
+    }
+    bit -= 1u;
+    const uint32_t code = v.code[ptr], L = code >> 27;
+    const i3 bc = mki((int)((code >> 18) & 511u), (int)((code >> 9) & 511u), (int)(code & 511u));
+    const i3 cc = mki(bc.x * 8 + (int)(bit & 7u), bc.y * 8 + (int)((bit >> 3) & 7u), bc.z * 8 + (int)(bit >> 6));
+    const float vs = vox_size(v, L);
+    const f3 p = region_lo(v, L) + adds(vi2f(cc), 0.5f) * vs;
+    const uint32_t e = v.attr[ai].y;
+    const double inv32767 = 1.0 / 32767.0;   // unpack2x16snorm as the exact f64 product
+    const float ex = mx(__double2float_rn((double)(int16_t)(e & 0xffffu) * inv32767), -1.0f);
+    const float ey = mx(__double2float_rn((double)(int16_t)(e >> 16) * inv32767), -1.0f);
+    f3 n = mk(ex, ey, 1.0f - fabsf(ex) - fabsf(ey));
+    const float q0 = mx(-n.z, 0.0f);
+    n.x += n.x >= 0.0f ? -q0 : q0;
+    n.y += n.y >= 0.0f ? -q0 : q0;
+    const f3 nf = dot(n, n) > 0.01f ? normalize3(n) : mk(0.0f, 1.0f, 0.0f);
+    const float off = L == 0u ? 0.0f : 0.5f * vs;   // bnSide: coarser levels read half a voxel towards the side
+    const f3 ef = bn_read(b, cur, p + nf * off, p, nf);
+    const f3 eb = bn_read(b, cur, p + (-nf) * off, p, -nf);
+    b.inj[ai] = make_uint4((uint32_t)f2h(ef.x) | ((uint32_t)f2h(ef.y) << 16), (uint32_t)f2h(ef.z),
+                           (uint32_t)f2h(eb.x) | ((uint32_t)f2h(eb.y) << 16), (uint32_t)f2h(eb.z));
+  }
+}
+
+// One frame of the bounce volume (Bounce.encode, bounce.ts:356-368), at the start of the trace pass
+static cudaError_t launch_bounce(const BounceDev &b, const VoxDev &v, const float *frame, const float *unorm8,
+                                 uint32_t sm_count, cudaStream_t st) {
+  GI_TRY(gi_launch(k_bn_clear, 1, 32, st, b));
+  GI_TRY(gi_launch(k_bn_classify, (b.n + 1u + 255u) / 256u, 256, st, b, v, frame));
+  GI_TRY(gi_launch(k_bn_update, sm_count * 4u, 256, st, b, v, frame, unorm8));
+  GI_TRY(gi_launch(k_bn_inject, sm_count * 8u, 256, st, b, v));
+  return cudaSuccess;
+}
+
 // ---- batches of solves, one launch per pass (gi_batch_capture_passes) ----------------------------------------------
 
 // The last solve s with pre[s] <= x (the owner of item x: solves with no items share the next one's start)
@@ -728,11 +1009,12 @@ __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
 
 template <int A>
 static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
-                                const RcLaunch *ls) {
+                                const RcLaunch *ls, const BounceDev *bn) {
   uint32_t *counter = r.counts + 80;   // the trace's ray counter lives after the 80 counter words
   if (ev) cudaEventRecord(ev[0], st);
   GI_TRY(gi_launch(k_setup_screen, (r.probes_total + 255u) / 256u, 256, st, r, v));
   if (ev) cudaEventRecord(ev[1], st);
+  if (bn) GI_TRY(launch_bounce(*bn, v, r.frame, r.unorm8, sm_count, st));   // counted in giTrace, as the reference
   RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
@@ -771,11 +1053,11 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
 using namespace gi;
 
 cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
-                               const RcLaunch *ls) {
+                               const RcLaunch *ls, const BounceDev *bn) {
   switch (r.atlas) {
-    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev, ls);
-    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev, ls);
-    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st, ev, ls);
+    case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev, ls, bn);
+    case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev, ls, bn);
+    case GI_ATLAS_BF16: return launch_solve<GI_ATLAS_BF16>(r, v, sm_count, st, ev, ls, bn);
   }
   return cudaErrorInvalidValue;
 }

@@ -11,7 +11,8 @@ LIB_PATH = os.path.join(PKG, "lib", "libgi_b200.so")
 
 GI_OK, GI_ERR_INVALID, GI_ERR_OOM, GI_ERR_CUDA, GI_ERR_TIMEOUT, GI_ERR_OVERFLOW, GI_ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 GI_ATLAS_F32, GI_ATLAS_F16, GI_ATLAS_BF16 = 0, 1, 2
-GI_RC_PROBES, GI_RC_RAD, GI_RC_SH, GI_RC_DEPTH, GI_RC_NORMAL, GI_RC_HITS, GI_RC_RAD_TRACED, GI_RC_SHADOW = range(8)
+(GI_RC_PROBES, GI_RC_RAD, GI_RC_SH, GI_RC_DEPTH, GI_RC_NORMAL, GI_RC_HITS, GI_RC_RAD_TRACED, GI_RC_SHADOW, GI_RC_BOUNCE_VOL,
+ GI_RC_BOUNCE_INJ, GI_RC_BOUNCE_LIST) = range(11)
 
 # Every symbol include/gi.h declares, with its ctypes signature (restype, argtypes).
 _P = C.c_void_p
@@ -41,6 +42,7 @@ SIGNATURES = {
     "gi_rc_set_gbuffer_f16": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_render_gbuffer": (C.c_int, [_P, _P, _P]),
     "gi_rc_render_shadow": (C.c_int, [_P, _P, C.c_uint32, _P]),
+    "gi_rc_set_bounce": (C.c_int, [_P, _P, _P]),
     "gi_rc_solve": (C.c_int, [_P, _P, _P]),
     "gi_solve": (C.c_int, [_P, _P, _P]),
     "gi_rc_read_irradiance": (C.c_int, [_P, _P, _P]),
@@ -103,6 +105,11 @@ class GiRcTuning(C.Structure):
 
 class GiVoxTuning(C.Structure):
     _fields_ = [("chunk_cells", C.c_uint32), ("blocks", C.c_uint32), ("reserved", C.c_uint32 * 6)]
+
+
+class GiBounceParams(C.Structure):
+    _fields_ = [("cell", C.c_float), ("dx", C.c_uint32), ("dy", C.c_uint32), ("dz", C.c_uint32), ("rays", C.c_uint32),
+                ("div", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
 
 _lib = None

@@ -210,6 +210,14 @@ class Rc:
         _lib.call("gi_rc_render_shadow", self.handle, scene.handle, int(size), _stream(stream))
         self.shadow_size = int(size)
 
+    def set_bounce(self, vox: "VoxWorld", cell: float = 1.2, dims=(32, 16, 32), rays: int = 16, div: int = 2):
+        """Multi-bounce (bounce.ts, DEFAULT_BOUNCE) bound to `vox`; vox None turns it off."""
+        if vox is None:
+            _lib.call("gi_rc_set_bounce", self.handle, None, None)
+            return
+        p = _lib.GiBounceParams(cell, dims[0], dims[1], dims[2], rays, div)
+        _lib.call("gi_rc_set_bounce", self.handle, vox.handle, C.byref(p))
+
     def read_shadow(self, stream=None) -> np.ndarray:
         S = getattr(self, "shadow_size", 0)
         return self.read_buffer(_lib.GI_RC_SHADOW, stream).view(np.float32).reshape(S, S)

@@ -117,3 +117,49 @@ def test_parity(ctx, name):
     _close(g["sh"].reshape(-1)[: o["sh"].size], o["sh"].reshape(-1), tol, "SH")
     _close(g["irr"], o["irr"], tol, "irradiance")
     assert np.array_equal(g["counts"][:8], o["counts"][:8])
+
+
+def test_bounce_parity(ctx):
+    """Multi-bounce (bounce.ts) over three solves of the leak room with the sun's shadow map: the injected irradiance,
+    the probe list and the irradiance of every solve bit-exact with the oracle's frames (the volume carries one frame
+    of history, so the frames must agree in sequence)."""
+    case = gi_cases.leak_sun(0.1, "f32", 512)
+    sg = gpu.SceneGpu(ctx, case.scene)
+    vw = gpu.VoxWorld(sg, case.vox)
+    rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    rc.set_frame(case.frame)
+    rc.render_gbuffer(sg)
+    rc.render_shadow(sg, case.shadow)
+    vw.update(case.scene.camera.eye)
+    rc.set_bounce(vw)
+    depth, normal, _ = bind.raster_gbuffer(case.scene, case.frame, case.width, case.height)
+    shadow = bind.shadow_render(case.scene, case.frame, case.shadow)
+    v = case.vox
+    st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+    bind.vox_sun(st, case.frame, shadow)
+    ob = bind.Bounce(st)
+    lay = dict(gi_cases.configs.cascade_layout(case.rc, case.width, case.height))
+    nv = int(min(st["hdr"][1], v.maxVoxels))
+    irr_prev = None
+    try:
+        for f in range(3):
+            rc.solve(vw)
+            g_irr = rc.read_irradiance()
+            g_inj = rc.read_buffer(_lib.GI_RC_BOUNCE_INJ).view(np.float16).reshape(-1, 8)[:nv]
+            g_list = rc.read_buffer(_lib.GI_RC_BOUNCE_LIST).view(np.uint32)
+            inj = ob.frame(st, case.frame)[: nv * 6].reshape(nv, 6)
+            assert g_list[1] == ob.list[1] and g_list[2] == ob.list[2] and g_list[0] == ob.list[0], \
+                f"frame {f}: probe list {g_list[:3]} vs {ob.list[:3]}"
+            assert np.array_equal(np.sort(g_list[4:4 + g_list[0]]), ob.list[4:4 + ob.list[0]]), f"frame {f}: listed probes differ"
+            g6 = np.concatenate([g_inj[:, 0:3], g_inj[:, 4:7]], axis=1).astype(np.float32)
+            assert np.array_equal(g6.view(np.uint32), inj.view(np.uint32)), \
+                f"frame {f}: injected irradiance differs at {np.argwhere((g6 != inj).any(1))[:4].ravel()}"
+            o = bind.rc_solve(st, lay, case.frame, depth, normal)
+            _close(g_irr, o["irr"], 1e-4, f"irradiance, frame {f}")
+            assert (inj > 0).any()
+            if irr_prev is not None:
+                assert not np.array_equal(g_irr, irr_prev)   # the second bounce arrives one frame later
+            irr_prev = g_irr
+    finally:
+        for h in (rc, vw, sg):
+            h.destroy()
