@@ -478,6 +478,41 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
 
+    # the same solve with multi-bounce on (bounce.ts, DEFAULT_BOUNCE; the reference renderer's default): the volume
+    # traced at the start of the trace pass, its irradiance on the voxels' hits
+    bounce_out = None
+    if args.bounce:
+        with torch.cuda.stream(stream):
+            rc.set_bounce(vw)
+            for _ in range(max(4, args.warmup)):
+                rc.solve(vw, stream)
+            rc.set_timing(True)
+            b_pass = {k: [] for k in rc.PASSES}
+            for _ in range(5):
+                rc.solve(vw, stream)
+                for k, x in rc.pass_times().items():
+                    b_pass[k].append(x)
+            rc.set_timing(False)
+            rc.graph_capture(vw, stream)
+            n_b = max(3, min(n_ev, 200))
+            bs, be = ([torch.cuda.Event(enable_timing=True) for _ in range(n_b)] for _ in range(2))
+            for k in range(n_b):
+                flush.zero_()
+                bs[k].record(stream)
+                rc.graph_launch(stream)
+                be[k].record(stream)
+            torch.cuda.synchronize()
+            b_ms = sorted(a.elapsed_time(c) for a, c in zip(bs, be))
+            b_total = max_over_ranks(sum(b_ms), dist, "cuda")
+            bounce_out = {"value": whole_job_rate(n_b, b_total / 1000.0, world), "unit": "solves/s", "steps": n_b,
+                          "ms_per_step": b_total / n_b, "p50_ms": b_ms[n_b // 2],
+                          "p99_ms": b_ms[min(n_b - 1, int(math.ceil(0.99 * n_b)) - 1)],
+                          "passes_ms": {k: statistics.median(x) for k, x in b_pass.items()},
+                          "volume": "32 x 16 x 32 probes 1.2 m apart, 16 rays + 6 axis rays, every 2 frames",
+                          "listed_probes": int(rc.read_buffer(_lib.GI_RC_BOUNCE_LIST).view(np.uint32)[0])}
+            rc.set_bounce(None)
+            rc.graph_capture(vw, stream)
+
     trace_ms = statistics.mean(pass_ms["giTrace"])
     alg = trace_algorithmic_bytes(rc.layout, hdr, v)
     peak, peak_kind = measured_peak()
@@ -499,6 +534,7 @@ def run_ours(args, rank, world, local_rank):
                "dda_steps_per_s": steps_per_solve * value,
                "passes_ms": {k: statistics.median(x) for k, x in pass_ms.items()},
                "shadow_map_ms": shadow_ms,
+               "bounce": bounce_out,
                "vox_counters": {"bricks": int(min(hdr[0], v.maxBricks)), "voxels": int(hdr[1]),
                                 "bricksPerLevel": [int(x) for x in hdr[8:8 + v.levels]]},
                "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -545,6 +581,7 @@ def main():
     ap.add_argument("--workload", default="colonnade", choices=["colonnade", "room"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--tuning", default=None, help="fixed launch shapes as JSON (skips the autotuner)")
+    ap.add_argument("--no-bounce", dest="bounce", action="store_false", help="skip the multi-bounce measurement")
     ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[100, 500, 1000, 2000, 5000],
                     help="request rates of the serving measurement (none: skip)")

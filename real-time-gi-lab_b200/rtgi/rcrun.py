@@ -70,17 +70,27 @@ def load_scene(name: str, pose_frame: float = 0.0, fps: float = 30.0):
 
 
 def run_config(ctx, sg, scene, name: str, p: configs.RcParams, vp: configs.VoxParams, width: int, height: int,
-               warmup: int, frames: int, sky, log=print) -> dict:
+               warmup: int, frames: int, sky, log=print, shadow_size: int = fr.SHADOW_SIZE) -> dict:
     """runConfig (rcrun.ts) for one config, static camera: warm-up frames, then `frames` timed solves (per-pass CUDA
-    events), the DDA statistics of one more solve, the probe and voxel counters."""
+    events), the DDA statistics of one more solve, the probe and voxel counters.  As the reference's renderer: the
+    sun's shadow map over the scene (shadow_size 0: none) and multi-bounce when the config has it on (the default)."""
     from . import gpu
+    lvp, bias = [0.0] * 16, (0.0, 0.0)
+    if shadow_size:
+        bmin, bmax = fr.scene_bounds(scene.positions)
+        lvp, bias = fr.scene_sun_view_proj(bmin, bmax, scene.sun_dir), fr.SHADOW_BIAS
     F = fr.pack_frame(fr.FrameParams(cam=scene.camera, width=width, height=height, sun_dir=scene.sun_dir,
-                                     sun_e=scene.sun_e, sky=sky, cascades=p.cascades, P=p.P, s_min=p.sMin, lift=p.lift))
+                                     sun_e=scene.sun_e, sky=sky, cascades=p.cascades, P=p.P, s_min=p.sMin, lift=p.lift,
+                                     light_view_proj=lvp, shadow_bias=bias))
     vw = gpu.VoxWorld(sg, vp)
     rc = gpu.Rc(ctx, p, width, height)
     try:
         rc.set_frame(F)
         rc.render_gbuffer(sg)
+        if shadow_size:
+            rc.render_shadow(sg, shadow_size)
+        if p.bounce:
+            rc.set_bounce(vw)
         vw.update(scene.camera.eye)
         for _ in range(warmup):
             rc.solve(vw)
@@ -104,6 +114,7 @@ def run_config(ctx, sg, scene, name: str, p: configs.RcParams, vp: configs.VoxPa
                                   "bigPerLevel")}
         irr = rc.read_irradiance()
         out = {"config": name, "params": dataclasses.asdict(p), "voxParams": dataclasses.asdict(vp),
+               "shadowMap": shadow_size, "bounce": bool(p.bounce),
                "resolution": f"{width}x{height}", "allocatedBytes": rc.bytes(), "voxAllocatedBytes": vw.bytes(),
                "static": {"timing": timing, "counts": [int(x) for x in c[:p.cascades]], "vox": vox},
                "tracer": tracer, "_irr": irr}
@@ -170,9 +181,13 @@ def main(argv: Optional[List[str]] = None) -> int:
     ap.add_argument("--vox-bench", action="store_true")
     ap.add_argument("--tag", default="default")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--shadow-size", type=int, default=fr.SHADOW_SIZE, help="sun shadow map size (0: no sun visibility)")
+    ap.add_argument("--no-bounce", action="store_true", help="multi-bounce off whatever the config says")
     a = ap.parse_args(argv)
     overrides = json.loads(a.params)
     parsed = [(c, configs.parse_config(c, overrides)) for c in a.configs.split(",")]
+    if a.no_bounce:
+        parsed = [(c, dataclasses.replace(p, bounce=False)) for c, p in parsed]
     t0 = time.perf_counter()
     scene, vox_defaults = load_scene(a.scene, a.pose_frame)
     vp = configs.vox_params({**vox_defaults, **json.loads(a.vox)})
@@ -196,7 +211,7 @@ def main(argv: Optional[List[str]] = None) -> int:
         for name, p in parsed:
             print(name, flush=True)
             r = run_config(ctx, sg, scene, name, p, vp, a.width, a.height, a.warmup, a.frames, sky,
-                           log=lambda s: print(s, flush=True))
+                           log=lambda s: print(s, flush=True), shadow_size=a.shadow_size)
             irr = r.pop("_irr")
             if a.dump_irr:
                 pack_irradiance(irr).tofile(os.path.join(out_dir, f"{name}.static.irr.f32"))
