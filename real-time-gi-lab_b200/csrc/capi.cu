@@ -161,6 +161,7 @@ static void free_rc(gi_rc *r) {
   cudaFree((void *)r->dev.unorm8);
   cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
+  cudaFree(r->bn.ray_out);
   r->bn = BounceDev{};
   r->bounce = false;
   r->dev.bn_inj = nullptr;
@@ -715,6 +716,7 @@ int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_bounce: NULL rc");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_set_bounce: cudaSetDevice");
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
+  cudaFree(r->bn.ray_out);
   r->bn = BounceDev{};
   r->bounce = false;
   r->bn_vox = nullptr;
@@ -735,9 +737,10 @@ int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
   float4 *dirs = nullptr;
   cudaError_t e;
   if ((e = dalloc(&dirs, b.rays)) || (e = dalloc(&b.vol[0], texels)) || (e = dalloc(&b.vol[1], texels)) ||
-      (e = dalloc(&b.list, 4u + (size_t)b.n)) || (e = dalloc(&b.inj, (size_t)v->p.max_voxels))) {
+      (e = dalloc(&b.list, 4u + (size_t)b.n)) || (e = dalloc(&b.inj, (size_t)v->p.max_voxels)) ||
+      (e = dalloc(&b.ray_out, (size_t)b.n * (b.rays + 6u)))) {
     cudaFree(dirs); b.dirs = nullptr;
-    cudaFree(b.vol[0]); cudaFree(b.vol[1]); cudaFree(b.list); cudaFree(b.inj);
+    cudaFree(b.vol[0]); cudaFree(b.vol[1]); cudaFree(b.list); cudaFree(b.inj); cudaFree(b.ray_out);
     r->bn = BounceDev{};
     return cuda_fail(e, "gi_rc_set_bounce");
   }

@@ -59,6 +59,7 @@ struct BounceDev {
                                // texel (0, 0, 6 dz) holds the volume's origin in probe coordinates
   uint32_t *list;              // [0] probes listed this frame, [1] frame counter, [2] this frame's volume, [4..) list
   uint4 *inj;                  // per voxel: front rg, front b | 0, back rg, back b | 0 (f16 pairs)
+  float4 *ray_out;             // n * (rays + 6): each listed probe's ray results (rgb, reach) before the sums
 };
 
 // Scratch of the binned G-buffer raster (gbuffer.cu)

@@ -783,51 +783,56 @@ __device__ float4 bn_trace(const VoxDev &v, const float *__restrict__ F, const f
   return make_float4(F[F_SKY], F[F_SKY + 1], F[F_SKY + 2], 1e9f);
 }
 
-// bnUpdate (bounce.ts:172-208): one warp per listed probe.  Lanes [0, rays) trace the irradiance rays, lanes
-// [rays, rays + 6) the axis rays (reach up to the first occupied voxel, at most 1.5 cells), then lanes 0-5 sum the
-// ambient cube over the rays in order.
-__global__ void __launch_bounds__(256) k_bn_update(BounceDev b, VoxDev v, const float *__restrict__ F,
-                                                    const float *__restrict__ unorm8) {
+// bnUpdate (bounce.ts:172-208) in two launches.  k_bn_rays: one thread per ray of a listed probe, the probe's rays
+// [0, rays) the irradiance rays and [rays, rays + 6) the axis rays (reach up to the first occupied voxel, at most 1.5
+// cells), results kept per (probe, ray).  k_bn_sum: one thread per (probe, axis) sums the ambient cube over the rays
+// in order.  The same operations as the reference's one workgroup per probe, with every lane tracing a ray.
+__device__ __forceinline__ f3 bn_axis_vec(uint32_t a) {
+  const float sg = (a & 1u) == 1u ? -1.0f : 1.0f;
+  return a / 2u == 0u ? mk(sg, 0.0f, 0.0f) : (a / 2u == 1u ? mk(0.0f, sg, 0.0f) : mk(0.0f, 0.0f, sg));
+}
+__global__ void __launch_bounds__(256) k_bn_rays(BounceDev b, VoxDev v, const float *__restrict__ F,
+                                                 const float *__restrict__ unorm8) {
   grid_dep_wait();
-  const uint32_t lane = threadIdx.x & 31u;
-  const uint32_t nwarps = gridDim.x * (blockDim.x >> 5), w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const uint32_t cur = b.list[2], count = b.list[0];
-  uint2 *out = b.vol[cur];
-  const uint2 *prev = b.vol[cur ^ 1u];
+  const uint32_t per = b.rays + 6u, total = b.list[0] * per;
+  const uint2 *prev = b.vol[b.list[2] ^ 1u];
   const i3 o = bn_origin_now(b, F);
-  for (uint32_t slot = w0; slot < count; slot += nwarps) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const uint32_t slot = t / per, k = t - slot * per;
     const uint32_t i = b.list[4u + slot];
     const i3 c = mki((int)(i % b.dx), (int)((i / b.dx) % b.dy), (int)(i / (b.dx * b.dy)));
     const f3 p = vi2f(mki(o.x + c.x, o.y + c.y, o.z + c.z)) * b.cell;
-    float4 res = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (lane < b.rays) {
-      const float4 dv = b.dirs[lane];
+    float4 res;
+    if (k < b.rays) {
+      const float4 dv = b.dirs[k];
       res = bn_trace(v, F, unorm8, b, prev, p, mk(dv.x, dv.y, dv.z), 1e9f);
-    } else if (lane < b.rays + 6u) {
-      const uint32_t a = lane - b.rays;
-      f3 axis = mk(0.0f, 0.0f, 0.0f);
-      const float sg = (a & 1u) == 1u ? -1.0f : 1.0f;
-      if (a / 2u == 0u) axis.x = sg; else if (a / 2u == 1u) axis.y = sg; else axis.z = sg;
-      res.w = mx(mn(bn_trace(v, F, unorm8, b, prev, p, axis, 1.5f * b.cell).w, 1.5f * b.cell), 1e-3f);
+    } else {
+      res = make_float4(0.0f, 0.0f, 0.0f,
+                        mx(mn(bn_trace(v, F, unorm8, b, prev, p, bn_axis_vec(k - b.rays), 1.5f * b.cell).w, 1.5f * b.cell), 1e-3f));
     }
+    b.ray_out[t] = res;
+  }
+}
+__global__ void __launch_bounds__(256) k_bn_sum(BounceDev b) {
+  grid_dep_wait();
+  const uint32_t per = b.rays + 6u, total = b.list[0] * 6u;
+  uint2 *out = b.vol[b.list[2]];
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const uint32_t slot = t / 6u, a = t - slot * 6u;
+    const uint32_t i = b.list[4u + slot];
+    const i3 c = mki((int)(i % b.dx), (int)((i / b.dx) % b.dy), (int)(i / (b.dx * b.dy)));
+    const float4 *rr = b.ray_out + (size_t)slot * per;
+    const f3 axis = bn_axis_vec(a);
     f3 e = mk(0.0f, 0.0f, 0.0f);
     float ws = 0.0f;
-    f3 axis = mk(0.0f, 0.0f, 0.0f);
-    const float sg = (lane & 1u) == 1u ? -1.0f : 1.0f;
-    if (lane / 2u == 0u) axis.x = sg; else if (lane / 2u == 1u) axis.y = sg; else axis.z = sg;
     for (uint32_t r = 0; r < b.rays; r++) {
-      const f3 rad = mk(__shfl_sync(0xffffffffu, res.x, (int)r), __shfl_sync(0xffffffffu, res.y, (int)r),
-                        __shfl_sync(0xffffffffu, res.z, (int)r));
-      const float4 dv = b.dirs[r];
+      const float4 dv = b.dirs[r], x = rr[r];
       const float w = mx(dot(axis, mk(dv.x, dv.y, dv.z)), 0.0f);
-      e = e + rad * w;
+      e = e + mk(x.x, x.y, x.z) * w;
       ws += w;
     }
-    const float reach = __shfl_sync(0xffffffffu, res.w, (int)(b.rays + (lane < 6u ? lane : 0u)));
-    if (lane < 6u) {
-      const f3 irr = (e * GI_PI) / mx(ws, 1e-6f);
-      out[bn_index(b, c, (int)lane)] = bn_pack(make_float4(irr.x, irr.y, irr.z, reach));
-    }
+    const f3 irr = (e * GI_PI) / mx(ws, 1e-6f);
+    out[bn_index(b, c, (int)a)] = bn_pack(make_float4(irr.x, irr.y, irr.z, rr[b.rays + a].w));
   }
 }
 
@@ -889,7 +894,8 @@ static cudaError_t launch_bounce(const BounceDev &b, const VoxDev &v, const floa
                                  uint32_t sm_count, cudaStream_t st) {
   GI_TRY(gi_launch(k_bn_clear, 1, 32, st, b));
   GI_TRY(gi_launch(k_bn_classify, (b.n + 1u + 255u) / 256u, 256, st, b, v, frame));
-  GI_TRY(gi_launch(k_bn_update, sm_count * 4u, 256, st, b, v, frame, unorm8));
+  GI_TRY(gi_launch(k_bn_rays, sm_count * 4u, 256, st, b, v, frame, unorm8));
+  GI_TRY(gi_launch(k_bn_sum, sm_count, 256, st, b));
   GI_TRY(gi_launch(k_bn_inject, sm_count * 8u, 256, st, b, v));
   return cudaSuccess;
 }
