@@ -478,6 +478,46 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         dist.barrier()
 
+    # two frames in flight: a second voxel world and cascade set solve the same workload on a second stream, the two
+    # captured solves launched side by side (what a renderer does with consecutive frames); device time of the job
+    in_flight = None
+    if args.in_flight:
+        st2 = torch.cuda.Stream()
+        vw2, rc2 = gpu.VoxWorld(sg, v), gpu.Rc(ctx, p, W, H)
+        with torch.cuda.stream(st2):
+            rc2.set_frame(F, st2)
+            rc2.render_gbuffer(sg, st2)
+            if desc["shadow_map"]:
+                rc2.render_shadow(sg, desc["shadow_map"], st2)
+            vw2.update(s.camera.eye)
+            rc2.set_tuning(**tuned["rc"])
+            vw2.set_tuning(**tuned["vox"])
+            rc2.solve(vw2, st2)
+            rc2.graph_capture(vw2, st2)
+        torch.cuda.synchronize()
+        n_f = max(3, min(n_ev, 200))
+        for _ in range(3):
+            rc.graph_launch(stream)
+            rc2.graph_launch(st2)
+        torch.cuda.synchronize()
+        f0, f1, f2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        f0.record(stream)
+        st2.wait_event(f0)
+        for _ in range(n_f):
+            rc.graph_launch(stream)
+            rc2.graph_launch(st2)
+        f2.record(st2)
+        stream.wait_event(f2)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        f_ms = max_over_ranks(f0.elapsed_time(f1), dist, "cuda")
+        in_flight = {"frames": 2, "value": whole_job_rate(2 * n_f, f_ms / 1000.0, world), "unit": "solves/s",
+                     "solves": 2 * n_f, "ms_per_solve": f_ms / (2 * n_f),
+                     "mode": "two voxel worlds and cascade sets, each solve replayed from its graph on its own stream; "
+                             "device time from the first launch to the last solve's end, L2 not flushed between"}
+        rc2.destroy()
+        vw2.destroy()
+
     # the same solve with multi-bounce on (bounce.ts, DEFAULT_BOUNCE; the reference renderer's default): the volume
     # traced at the start of the trace pass, its irradiance on the voxels' hits
     bounce_out = None
@@ -535,6 +575,7 @@ def run_ours(args, rank, world, local_rank):
                "passes_ms": {k: statistics.median(x) for k, x in pass_ms.items()},
                "shadow_map_ms": shadow_ms,
                "bounce": bounce_out,
+               "in_flight": in_flight,
                "vox_counters": {"bricks": int(min(hdr[0], v.maxBricks)), "voxels": int(hdr[1]),
                                 "bricksPerLevel": [int(x) for x in hdr[8:8 + v.levels]]},
                "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -582,6 +623,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--tuning", default=None, help="fixed launch shapes as JSON (skips the autotuner)")
     ap.add_argument("--no-bounce", dest="bounce", action="store_false", help="skip the multi-bounce measurement")
+    ap.add_argument("--no-in-flight", dest="in_flight", action="store_false",
+                    help="skip the two-frames-in-flight measurement")
     ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
     ap.add_argument("--serve-rates", type=float, nargs="*", default=[100, 500, 1000, 2000, 5000],
                     help="request rates of the serving measurement (none: skip)")
