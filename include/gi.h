@@ -176,6 +176,9 @@ int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
  * visibility is 1.  size 0 releases it.  Draw it again when the light matrix or the scene moves; a graph captured
  * before a change of size must be captured again. */
 int gi_rc_render_shadow(gi_rc *rc, gi_scene *scene, uint32_t size, void *stream);
+/* The rebuild (gi_vox_build) with voxSun from rc's shadow map and frame, as gi_solve runs it, for callers that solve
+ * several cascade sets over one voxel world (gi_rc_solve each); the same as gi_vox_build when rc holds no map. */
+int gi_vox_build_sun(gi_vox *vox, gi_rc *rc, void *stream);
 /* Multi-bounce (bounce.ts; BounceParams, DEFAULT_BOUNCE {1.2, [32, 16, 32], 16, 2}): a camera-centred volume of
  * dx*dy*dz irradiance probes `cell` metres apart, rebuilt every solve from the voxels (each probe near a surface traces
  * `rays` rays plus six axis rays, every `div` solves by its position) and injected into the voxels, whose hits then

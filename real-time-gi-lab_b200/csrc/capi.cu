@@ -423,6 +423,12 @@ static int vox_build_sun(gi_vox *v, const float *frame, const float *shadow, uin
 
 int gi_vox_build(gi_vox *v, void *stream) { return vox_build_sun(v, nullptr, nullptr, 0u, stream); }
 
+int gi_vox_build_sun(gi_vox *v, gi_rc *r, void *stream) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_vox_build_sun: NULL rc");
+  if (v && v->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_vox_build_sun: rc on another device");
+  return vox_build_sun(v, r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, stream);
+}
+
 int gi_vox_read_counters(gi_vox *v, uint32_t hdr[64], void *stream) {
   if (!v || !hdr) return fail(GI_ERR_INVALID, "gi_vox_read_counters: NULL argument");
   CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_read_counters: cudaSetDevice");

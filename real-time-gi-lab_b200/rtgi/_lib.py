@@ -43,6 +43,7 @@ SIGNATURES = {
     "gi_rc_render_gbuffer": (C.c_int, [_P, _P, _P]),
     "gi_rc_render_shadow": (C.c_int, [_P, _P, C.c_uint32, _P]),
     "gi_rc_set_bounce": (C.c_int, [_P, _P, _P]),
+    "gi_vox_build_sun": (C.c_int, [_P, _P, _P]),
     "gi_rc_solve": (C.c_int, [_P, _P, _P]),
     "gi_solve": (C.c_int, [_P, _P, _P]),
     "gi_rc_read_irradiance": (C.c_int, [_P, _P, _P]),

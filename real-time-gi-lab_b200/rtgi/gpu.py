@@ -110,8 +110,12 @@ class VoxWorld:
         e = (C.c_double * 3)(*[float(x) for x in eye])
         _lib.call("gi_vox_update", self.handle, e)
 
-    def encode(self, stream=None) -> None:
-        _lib.call("gi_vox_build", self.handle, _stream(stream))
+    def encode(self, stream=None, sun_rc=None) -> None:
+        """The rebuild; with sun_rc, voxSun from that rc's shadow map and frame (gi_vox_build_sun)."""
+        if sun_rc is not None:
+            _lib.call("gi_vox_build_sun", self.handle, sun_rc.handle, _stream(stream))
+        else:
+            _lib.call("gi_vox_build", self.handle, _stream(stream))
 
     def read_counters(self, stream=None) -> dict:
         hdr = np.zeros(64, np.uint32)

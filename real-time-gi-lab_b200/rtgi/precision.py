@@ -90,10 +90,12 @@ class ErrorStats:
 
 def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
         atlases: Sequence[str] = ("f32", "f16", "bf16", "f16-f32out", "bf16-f32out"),
-        seed: int = 0, n_boxes: int = 64, width: int = 1920, height: int = 1080, device: int = 0) -> dict:
-    """The study: per frame, pose the boxes, rebuild the clipmap, solve the cascades in every atlas mode, run the FP64
-    merge and gather from the f32 mode's trace, and accumulate each mode's irradiance error.  Also times each mode's
-    cascade solve (CUDA events on the solve stream; median over frames)."""
+        seed: int = 0, n_boxes: int = 64, width: int = 1920, height: int = 1080, device: int = 0,
+        shadow_size: int = fr.SHADOW_SIZE) -> dict:
+    """The study: per frame, pose the boxes, draw the sun's shadow map (the boxes move; shadow_size 0: no sun
+    visibility), rebuild the clipmap with voxSun, solve the cascades in every atlas mode, run the FP64 merge and
+    gather from the f32 mode's trace, and accumulate each mode's irradiance error.  Also times each mode's cascade
+    solve (CUDA events on the solve stream; median over frames)."""
     import torch
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
@@ -110,8 +112,13 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
         if "f32" not in rcs:
             raise ValueError("the FP64 reference starts from the f32 atlas's trace: include 'f32'")
         rcs["f32"].set_debug_hits(True)
+        lvp, bias = [0.0] * 16, (0.0, 0.0)
+        if shadow_size:   # the light covers the scene's bounds at rest (the boxes stay inside the colonnade)
+            bmin, bmax = fr.scene_bounds(s.positions)
+            lvp, bias = fr.scene_sun_view_proj(bmin, bmax, s.sun_dir), fr.SHADOW_BIAS
         F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=width, height=height, sun_dir=s.sun_dir, sun_e=s.sun_e,
-                                         sky=s.sky, cascades=rcs["f32"].params.cascades, P=rcs["f32"].params.P))
+                                         sky=s.sky, cascades=rcs["f32"].params.cascades, P=rcs["f32"].params.P,
+                                         light_view_proj=lvp, shadow_bias=bias))
         for rc in rcs.values():
             rc.set_frame(F, stream)
         vox.update(s.camera.eye)
@@ -125,7 +132,9 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
         for f in range(frames):
             pos, nrm = objs.pose(f * dt)
             sg.update_vertices(objs.first, pos, nrm, stream)
-            vox.encode(stream)
+            if shadow_size:
+                rcs["f32"].render_shadow(sg, shadow_size, stream)
+            vox.encode(stream, sun_rc=rcs["f32"] if shadow_size else None)
             ev = {}
             for a, rc in rcs.items():
                 rc.render_gbuffer(sg, stream)
@@ -146,7 +155,7 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
                 counters.append(vox.read_counters(stream))
         out = {a: dict(stats[a].summary(), solve_ms=float(np.median(times[a]))) for a in rcs}
         return {"scene": f"colonnade + {n_boxes} moving boxes: {s.triangle_count} triangles", "frames": frames,
-                "dt_s": dt, "resolution": [width, height], "atlases": out,
+                "dt_s": dt, "resolution": [width, height], "atlases": out, "shadow_map": shadow_size,
                 "bricks_first_last": [c["bricks"] for c in counters],
                 "error": "per valid pixel and rgb channel |x - x64| / max(|x64|, 1e-3 x frame mean |x64|); "
                          "quantiles are upper edges of 0.1-decade histogram bins"}
