@@ -81,6 +81,41 @@ def leak_sun(t: float = 0.1, atlas: str = "f32", size: int = 1024) -> Case:
     return c
 
 
+def empty(atlas: str = "f32") -> Case:
+    """No triangles: an empty clipmap, a background-only G-buffer (no valid probe), at a ragged 100 x 37."""
+    s = scenes.Scene("empty", np.zeros((0, 3), np.float32), np.zeros((0, 3), np.float32), np.zeros((0, 4), np.uint32),
+                     [scenes.Material("grey", (0.5, 0.5, 0.5, 1.0))], scenes.Camera((0, 1.7, 5), (0, 1, 0), 60, 0.05),
+                     sun_dir=(0.3, 1.0, 0.2), sun_e=fr.SUN_E, sky=fr.SKY)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda64", {"cascades": 3})
+    v = configs.vox_params({"v0": 0.16, "levels": 2, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 16})
+    c = Case("empty", s, 100, 37, v, p)
+    c.frame = _frame(s, 100, 37, p)
+    return c
+
+
+def single_triangle(atlas: str = "f32") -> Case:
+    """One large triangle filling part of the view under sun and sky (the rest background), at a ragged 123 x 61."""
+    b = scenes.Builder([scenes.Material("grey", (0.7, 0.6, 0.5, 1.0))])
+    b.quad([-3, 0, 3], [3, 0, 3], [3, 0, -3], [-3, 0, -3])
+    s0 = b.scene("tri", scenes.Camera((0, 1.7, 5), (0, 0, 0), 60, 0.05), sun_dir=(0.3, 1.0, 0.2), sun_e=fr.SUN_E,
+                 sky=fr.SKY)
+    s = scenes.Scene("single-triangle", s0.positions, s0.normals, s0.tri[:1].copy(), s0.materials, s0.camera,
+                     sun_dir=s0.sun_dir, sun_e=s0.sun_e, sky=s0.sky)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda64", {"cascades": 3})
+    v = configs.vox_params({"v0": 0.08, "levels": 2, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 16})
+    c = Case("single-triangle", s, 123, 61, v, p, shadow=256)
+    c.frame = _frame(s, 123, 61, p, shadow=True)
+    return c
+
+
+def tiny(atlas: str = "f16") -> Case:
+    """room_lit at 7 x 5 pixels: a single probe per cascade, smaller than the 8-pixel probe cell."""
+    c = room_lit(atlas)
+    c.name, c.width, c.height = "tiny", 7, 5
+    c.frame = _frame(c.scene, 7, 5, c.rc, sun_e=fr.SUN_E, sky=fr.SKY)
+    return c
+
+
 def overflow(atlas: str = "f32") -> Case:
     """room_lit with pools too small: dropped bricks (read at the coarser level) and voxels without attributes."""
     c = room_lit(atlas)

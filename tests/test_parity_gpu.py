@@ -74,7 +74,8 @@ def run_oracle(case, depth, normal, shadow=None):
 
 
 CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_cases.leak,
-         "leak_sun": gi_cases.leak_sun,
+         "leak_sun": gi_cases.leak_sun, "empty": gi_cases.empty, "single_triangle": gi_cases.single_triangle,
+         "tiny": gi_cases.tiny,
          "room_lit_f32out": lambda: gi_cases.room_lit("f16-f32out"),
          "overflow": gi_cases.overflow, "config1": gi_cases.config1}
 
@@ -92,7 +93,7 @@ def test_parity(ctx, name):
         shadow = bind.shadow_render(case.scene, case.frame, case.shadow)
         assert np.array_equal(g["shadow"].view(np.uint32), shadow.view(np.uint32)), \
             f"shadow map differs at {(g['shadow'] != shadow).sum()} texels"
-        assert (shadow < 1.0).any()
+        assert (shadow < 1.0).any() or case.scene.triangle_count == 0
     st, o = run_oracle(case, depth, normal, shadow)
     # voxel world: every counter and every allocated word
     gv = g["vox"]
@@ -107,7 +108,8 @@ def test_parity(ctx, name):
     if case.shadow:
         assert np.array_equal(gv["sunvis"][:nv].view(np.uint32), st["sunvis"][:nv].view(np.uint32)), "sun visibility differs"
         sv = st["sunvis"][:nv]
-        assert (sv == 0.0).any() and (sv == 1.0).any(), "the case should hold shadowed and lit voxels"
+        if case.name.startswith("leak") or case.name == "config1":
+            assert (sv == 0.0).any() and (sv == 1.0).any(), "the case should hold shadowed and lit voxels"
     # probes and DDA hits
     assert np.array_equal(g["probes"].view(np.uint32), o["probes"].view(np.uint32)), "probes differ"
     assert np.array_equal(g["hits"], o["hit"]), f"DDA hits differ at {np.argwhere((g['hits'] != o['hit']).any(1))[:5].ravel()}"
