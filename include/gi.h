@@ -230,7 +230,8 @@ int gi_batch_capture(gi_batch *batch, void *stream);
 /* The same batch captured pass by pass: the n voxel rebuilds as parallel branches, then ONE launch per cascade pass
  * over the work of every solve (setup, a persistent trace over all the rays, one merge launch per cascade step, the
  * gather).  All solves need the same atlas format and probe spacing (8, 16 or 32 pixels); the solves' launch tuning
- * does not apply to these launches (results are the same bits either way).  Replaces a graph captured before. */
+ * does not apply to these launches (results are the same bits either way); a solve with multi-bounce on is
+ * refused (GI_ERR_INVALID: capture its chain with gi_batch_capture).  Replaces a graph captured before. */
 int gi_batch_capture_passes(gi_batch *batch, void *stream);
 int gi_batch_launch(gi_batch *batch, void *stream);
 int gi_batch_destroy(gi_batch *batch);
