@@ -15,7 +15,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgi_oracle.so")
-SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "orc_par.c", "gi_oracle.h", "orc_math.h", "orc_par.h", "Makefile"]
+SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "shadow.c", "world.c", "orc_par.c", "gi_oracle.h", "orc_math.h",
+           "orc_par.h", "orc_rc.h", "Makefile"]
 
 
 def build(force: bool = False) -> str:
@@ -35,6 +36,11 @@ def lib():
         _lib = C.CDLL(LIB_PATH)
         _lib.orc_vox_build.argtypes = [C.c_void_p, C.c_void_p]
         _lib.orc_rc_trace.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_world_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_hash32.argtypes = [C.c_uint32]
+        _lib.orc_hash32.restype = C.c_uint32
+        _lib.orc_lod_for.argtypes = [C.c_void_p, C.c_float]
+        _lib.orc_lod_for.restype = C.c_int32
         _lib.orc_rc_merge_gather.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_rc_merge_gather_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_raster_gbuffer.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
@@ -107,6 +113,16 @@ class OrcGbuf(C.Structure):
 class OrcRcOut(C.Structure):
     _fields_ = [("probes", C.c_void_p), ("rad", C.c_void_p), ("sh", C.c_void_p), ("irr", C.c_void_p),
                 ("counts", C.c_void_p), ("hit", C.c_void_p)]
+
+
+class OrcWLayout(C.Structure):
+    _fields_ = [("base", OrcLayout), ("hash_off", C.c_uint32 * 8), ("hash_mask", C.c_uint32 * 8),
+                ("hash_total", C.c_uint32), ("relocate", C.c_uint32)]
+
+
+class OrcWState(C.Structure):
+    _fields_ = [("keys", C.c_void_p), ("slot_probe", C.c_void_p), ("parents", C.c_void_p), ("hist_tab", C.c_void_p),
+                ("hist_grid", C.c_void_p), ("hist_sh", C.c_void_p), ("hist_par", C.c_uint32)]
 
 
 PROBE_DTYPE = np.dtype([("pos", "<f4", (4,)), ("nrm", "<f4", (4,)), ("grid", "<i4", (4,))])
@@ -306,3 +322,64 @@ class Bounce:
         lib().orc_bounce_frame(C.byref(self.b), C.byref(vx), _p(frame), _p(inj))
         vox["bn_inj"] = inj
         return inj
+
+
+class WorldState:
+    """What a world-probe solve keeps from one solve to the next (the hash tables, parents and the c0 history)."""
+
+    def __init__(self, lay: dict):
+        H0 = lay["casc"][0]["hash_mask"] + 1
+        cap0 = lay["casc"][0]["cap"]
+        self.keys = np.zeros(lay["hash_total"], np.uint32)
+        self.slot_probe = np.zeros(lay["hash_total"], np.uint32)
+        self.parents = np.zeros(lay["probes_total"] * 8, np.uint32)
+        self.hist_tab = np.zeros(2 * H0, np.uint32)
+        self.hist_grid = np.zeros(2 * cap0 * 4, np.int32)
+        self.hist_sh = np.zeros(2 * cap0 * 32, np.float32)
+        self.hist_par = 0
+
+
+def wlayout_struct(lay: dict) -> OrcWLayout:
+    wl = OrcWLayout()
+    wl.base = layout_struct(lay)
+    for i, c in enumerate(lay["casc"]):
+        wl.hash_off[i], wl.hash_mask[i] = c["hash_off"], c["hash_mask"]
+    wl.hash_total, wl.relocate = lay["hash_total"], lay["relocate"]
+    return wl
+
+
+def world_solve(vox: dict, lay: dict, state: WorldState, frame: np.ndarray, depth: np.ndarray, normal: np.ndarray,
+                want_hit: bool = False) -> dict:
+    """One world-probe solve (orc_world_solve) over a built voxel world; `state` carries over between solves."""
+    H, W = depth.shape
+    wl = wlayout_struct(lay)
+    cap0 = lay["casc"][0]["cap"]
+    out = {"probes": np.zeros(lay["probes_total"], PROBE_DTYPE), "rad": np.zeros((lay["rays_total"], 4), np.float32),
+           "sh": np.zeros((cap0, 32), np.float32), "irr": np.zeros((H, W, 4), np.float32),
+           "counts": np.zeros(80, np.uint32)}
+    if want_hit:
+        out["hit"] = np.zeros((lay["rays_total"], 4), np.uint32)
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    depth = np.ascontiguousarray(depth, dtype=np.float32)
+    normal = np.ascontiguousarray(normal, dtype=np.float32)
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    o = OrcRcOut(_p(out["probes"]), _p(out["rad"]), _p(out["sh"]), _p(out["irr"]), _p(out["counts"]),
+                 _p(out["hit"]) if want_hit else None)
+    ws = OrcWState(_p(state.keys), _p(state.slot_probe), _p(state.parents), _p(state.hist_tab), _p(state.hist_grid),
+                   _p(state.hist_sh), state.hist_par)
+    vx = _vox_struct(vox)
+    lib().orc_world_solve(C.byref(vx), C.byref(wl), C.byref(g), C.byref(ws), C.byref(o))
+    state.hist_par = ws.hist_par
+    out["keys"] = state.keys.copy()
+    out["slot_probe"] = state.slot_probe.copy()
+    out["parents"] = state.parents.copy()
+    return out
+
+
+def hash32(x: int) -> int:
+    return int(lib().orc_hash32(C.c_uint32(x)))
+
+
+def lod_for(frame: np.ndarray, dist: float) -> int:
+    frame = np.ascontiguousarray(frame, dtype=np.float32)
+    return int(lib().orc_lod_for(_p(frame), C.c_float(dist)))

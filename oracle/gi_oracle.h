@@ -13,6 +13,7 @@
  *   - the headless G-buffer raster         src/core/gbuffer.ts:82-103 (conventions only; the reference draws it
  *                                          with a graphics pipeline, restated here as a scanline raster)
  *   - the sun shadow map and voxSun        src/core/lighting.ts:133-189, frame.ts:35-52, voxel.ts:633-671
+ *   - world probes (method 'world')        src/core/rc.ts:248-570, :688-708, :775-927
  *
  * Arithmetic follows the WGSL expression order exactly (left-associative, no contraction: build with
  * -ffp-contract=off).  Where the WGSL leaves a builtin implementation-defined, the choice made here is stated
@@ -159,6 +160,29 @@ typedef struct {
  * inject (into inj_out, max_voxels * 6).  The list order is the probe order (the GPU's atomics order it otherwise;
  * the result does not depend on it). */
 int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *frame, float *inj_out);
+
+/* World probes (method 'world', rc.ts:253-570, 688-708, 775-927; world.c states the choices it makes).  The layout
+ * reuses orc_layout for the per-cascade probe / atlas offsets, capacities (caps), resolutions and intervals. */
+typedef struct {
+  orc_layout base;
+  uint32_t hash_off[8], hash_mask[8];   /* per cascade: its hash table's first slot, size - 1 (size = nextPow2(2 cap)) */
+  uint32_t hash_total;
+  uint32_t relocate;                     /* 0 'gbuffer' (relocate), 1 'none', 2 'voxel' (relocateVox + segOccluded) */
+} orc_wlayout;
+/* State a world solve keeps across solves (caller-allocated, zeroed before the first solve). */
+typedef struct {
+  uint32_t *keys, *slot_probe;   /* hash_total each */
+  uint32_t *parents;             /* probes * 8: the upper probes each probe merges (NONE = 0xffffffff) */
+  uint32_t *hist_tab;            /* 2 * H0 (H0 = hash_mask[0] + 1): the c0 history's tables, probe index + 1 or 0 */
+  int32_t *hist_grid;            /* 2 * cap0 * 4: per probe of each parity its grid point and LOD */
+  float *hist_sh;                /* 2 * cap0 * 32: per probe of each parity its SH as stored */
+  uint32_t hist_par;             /* parity of the last solve (0 before the first) */
+} orc_wstate;
+/* One solve: clearKeys .. linkParents, trace, mergeWorld N-1 .. 0, projectSH with the history, gatherWorld.
+ * o->probes / rad / sh / irr / counts / hit as for the screen method (rad indexed by the cap-based offsets). */
+int orc_world_solve(const orc_vox *vx, const orc_wlayout *wl, const orc_gbuf *g, orc_wstate *ws, orc_rc_out *o);
+uint32_t orc_hash32(uint32_t x);
+int32_t orc_lod_for(const float *frame, float dist);
 
 /* WGSL builtins as the oracle defines them (exported for the known-answer tests). */
 uint32_t orc_pack4x8unorm(const float v[4]);

@@ -11,30 +11,10 @@
 #include "gi_oracle.h"
 #include "orc_math.h"
 #include "orc_par.h"
-
-#define PI_F 3.14159265f
-
-/* Frame word offsets (frame.ts:4-21, packFrame :76-93). */
-enum { F_VP = 0, F_IVP = 16, F_EYE = 80, F_FWD = 84, F_SUN = 88, F_SUNE = 92, F_SKY = 96, F_SIZE = 100, F_RC = 104,
-       F_RC2 = 108, F_RU = 112, F_RU2 = 116, F_OMEGA = 120, F_STYLE = 136 };
-
-typedef struct {
-  const orc_vox *vx;
-  const float *F;
-  float sky[3];
-  const orc_bounce *bn;   /* the volume's own rays: read the previous volume bn_prev at the hit (bounce.ts:90-93) */
-  const float *bn_prev;
-} ctx_t;
-
-static inline float vox_size(const orc_vox *vx, uint32_t L) { return scale2(vx->v0, (int)L); }
-static inline i3 org(const orc_vox *vx, uint32_t L) { return I(vx->origin[L][0], vx->origin[L][1], vx->origin[L][2]); }
-static inline uint32_t ptr_index(const orc_vox *vx, uint32_t L, i3 b) {
-  uint32_t G = vx->G;
-  return L * G * G * G + ((uint32_t)b.z * G + (uint32_t)b.y) * G + (uint32_t)b.x;
-}
+#include "orc_rc.h"
 
 /* worldAt (frame.ts:22-26); mat4 * vec4 summed in column order. */
-static v3 world_at(const float *F, int32_t px, int32_t py, float d) {
+v3 world_at(const float *F, int32_t px, int32_t py, float d) {
   float nx = ((float)px + 0.5f) * F[F_SIZE + 2] * 2.0f - 1.0f;
   float ny = 1.0f - ((float)py + 0.5f) * F[F_SIZE + 3] * 2.0f;
   const float *m = F + F_IVP;
@@ -42,7 +22,7 @@ static v3 world_at(const float *F, int32_t px, int32_t py, float d) {
   for (int i = 0; i < 4; i++) h[i] = m[i] * nx + m[4 + i] * ny + m[8 + i] * d + m[12 + i] * 1.0f;
   return V(h[0] / h[3], h[1] / h[3], h[2] / h[3]);
 }
-static float view_z(const float *F, v3 p) { return dot(sub(p, fromf(F + F_EYE)), fromf(F + F_FWD)); }
+float view_z(const float *F, v3 p) { return dot(sub(p, fromf(F + F_EYE)), fromf(F + F_FWD)); }
 
 /* octDecode / dirOf (rc.ts:291-308) */
 static v3 oct_decode(float u, float v) {
@@ -53,25 +33,25 @@ static v3 oct_decode(float u, float v) {
   n.y += n.y >= 0.0f ? -t : t;
   return normalize3(n);
 }
-static v3 dir_of(uint32_t di, uint32_t res) {
+v3 dir_of(uint32_t di, uint32_t res) {
   return oct_decode(((float)(di % res) + 0.5f) / (float)res, ((float)(di / res) + 0.5f) / (float)res);
 }
 
-static float round_store(float x, uint32_t atlas) {
+float round_store(float x, uint32_t atlas) {
   if (atlas == 1) return orc_f16_to_f32(orc_f32_to_f16(x));
   if (atlas == 2) return orc_bf16_to_f32(orc_f32_to_bf16(x));
   return x;
 }
 
 /* voxRank (voxel.ts:81-87) */
-static uint32_t vox_rank(const orc_vox *vx, uint32_t brick, uint32_t bit) {
+uint32_t vox_rank(const orc_vox *vx, uint32_t brick, uint32_t bit) {
   uint32_t w = bit >> 5;
   uint32_t r = popc(vx->occ[brick * 16u + w] & ((1u << (bit & 31u)) - 1u));
   for (uint32_t i = 0; i < w; i++) r += popc(vx->occ[brick * 16u + i]);
   return vx->base[brick] + r;
 }
 /* voxAt (voxel.ts:90-107): (brick, bit, level) or brick ORC_EMPTY */
-static void vox_at(const orc_vox *vx, uint32_t L, i3 c, uint32_t out[3]) {
+void vox_at(const orc_vox *vx, uint32_t L, i3 c, uint32_t out[3]) {
   uint32_t l = L;
   i3 cc = c;
   int32_t n8 = (int32_t)vx->G * 8;
@@ -101,7 +81,7 @@ static int vox_inside(const orc_vox *vx, uint32_t L, v3 p) {
   v3 hi = adds(lo, ext);
   return p.x > lo.x && p.y > lo.y && p.z > lo.z && p.x < hi.x && p.y < hi.y && p.z < hi.z;
 }
-static uint32_t vox_level_for(const orc_vox *vx, uint32_t L, v3 e) {
+uint32_t vox_level_for(const orc_vox *vx, uint32_t L, v3 e) {
   uint32_t l = L;
   while (l + 1u < vx->levels && !vox_inside(vx, l, e)) l++;
   return l;
@@ -131,7 +111,6 @@ static v3 shade_hit_v(const float *F, v3 n0, const float alb[4], v3 d, v3 e, flo
   return add(b, muls(muls(mul(divs(a, PI_F), sunE), ndl), vis));
 }
 
-typedef struct { float r, g, b, T; uint32_t lvl, ptr, bit, tin; uint32_t steps; } trace_t;
 
 /* ---- multi-bounce reads (bounce.ts:44-75, 90-93; rc.ts:198-202) ---- */
 static float bn_get(const orc_bounce *b, const float *vol, int32_t x, int32_t y, int32_t z, int k) {
@@ -224,7 +203,7 @@ static void shade_voxel(const ctx_t *cx, uint32_t brick, uint32_t bit, v3 d, v3 
 }
 
 /* traceVox (voxel.ts:121-202) with a configurable step cap. */
-static void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tskip, uint32_t L, uint32_t cap, trace_t *out) {
+void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tskip, uint32_t L, uint32_t cap, trace_t *out) {
   const orc_vox *vx = cx->vx;
   out->r = out->g = out->b = 0.0f; out->T = 1.0f; out->lvl = ORC_EMPTY; out->ptr = ORC_EMPTY; out->bit = 0; out->tin = 0;
   out->steps = 0;
@@ -301,7 +280,7 @@ static void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tsk
 }
 
 /* voxLevel (rc.ts:210-213): round(log2(v / v0)) taken exactly, clamped to the levels. */
-static uint32_t vox_level(const orc_vox *vx, const orc_layout *ly, float s0, uint32_t c) {
+uint32_t vox_level(const orc_vox *vx, const orc_layout *ly, float s0, uint32_t c) {
   float v = ly->vox_scale * s0 * exp2_(ly->level_map * (float)c);
   int32_t r = (int32_t)orc_round_log2(v / vx->v0);
   int32_t top = (int32_t)vx->levels - 1;
@@ -396,7 +375,7 @@ int orc_rc_trace(const orc_vox *vx, const orc_layout *ly, const orc_gbuf *g, orc
 }
 
 /* upperAvg (rc.ts:681-686) */
-static v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_t q, uint32_t u, uint32_t v, uint32_t lr) {
+v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_t q, uint32_t u, uint32_t v, uint32_t lr) {
   const orc_casc *U = &ly->c[cu];
   if (U->res == lr) {
     const float *p = rad + 4u * ((size_t)U->rad_off + q * U->res * U->res + v * U->res + u);
@@ -407,7 +386,7 @@ static v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_
   return muls(add(add(add(V(a[0], a[1], a[2]), V(b[0], b[1], b[2])), V(c[0], c[1], c[2])), V(d[0], d[1], d[2])), 0.25f);
 }
 
-static void sh_basis(v3 n, float y[9]) {
+void sh_basis(v3 n, float y[9]) {
   y[0] = 0.282095f; y[1] = 0.488603f * n.y; y[2] = 0.488603f * n.z; y[3] = 0.488603f * n.x;
   y[4] = 1.092548f * n.x * n.y; y[5] = 1.092548f * n.y * n.z; y[6] = 0.315392f * (3.0f * n.z * n.z - 1.0f);
   y[7] = 1.092548f * n.x * n.z; y[8] = 0.546274f * (n.x * n.x - n.y * n.y);

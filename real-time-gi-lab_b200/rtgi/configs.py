@@ -129,3 +129,30 @@ def cascade_layout(p: RcParams, width: int, height: int) -> dict:
             "level_map": p.levelMap, "vox_skip": p.voxSkip, "dda_cap": p.ddaCap, "stats": p.stats, "atlas": atlas,
             "f32_out": 1 if p.f32Out else 0,
             "probes_total": probe_off, "rays_total": rad_off}
+
+
+def world_layout(p: RcParams) -> dict:
+    """The world-method cascade layout (rc.ts:1027-1035): per cascade res = 4 << min(i, resCap), capacity caps[i],
+    a hash table of nextPow2(2 cap) slots, interval [b_i, b_{i+1}]; probes and atlas entries by capacity."""
+    import numpy as np
+    casc = []
+    probe_off = rad_off = hash_off = 0
+    for i in range(p.cascades):
+        res = 4 << min(i, p.resCap)
+        cap = int(p.caps[i])
+        if cap < 1:
+            raise ValueError(f"cascade {i}: capacity {cap}")
+        hs = 1 << max(0, (2 * cap - 1).bit_length())
+        b = lambda k: p.kInterval * (4 ** k - 1) / 3
+        casc.append({"probe_off": probe_off, "cap": cap, "rad_off": rad_off, "res": res, "tile_size": 0,
+                     "tiles_x": 0, "tiles_y": 0, "hash_off": hash_off, "hash_mask": hs - 1,
+                     "b0": float(np.float32(b(i))), "b1": float(np.float32(b(i + 1)))})
+        probe_off += cap
+        rad_off += cap * res * res
+        hash_off += hs
+    atlas = {"f32": 0, "f16": 1, "bf16": 2}[p.atlas]
+    relocate = {"gbuffer": 0, "none": 1, "voxel": 2}[p.relocate]
+    return {"cascades": p.cascades, "casc": casc, "vox_scale": p.voxScale, "vox_offset": p.voxOffset,
+            "level_map": p.levelMap, "vox_skip": p.voxSkip, "dda_cap": p.ddaCap, "stats": p.stats, "atlas": atlas,
+            "f32_out": 1 if p.f32Out else 0, "probes_total": probe_off, "rays_total": rad_off,
+            "hash_total": hash_off, "relocate": relocate, "world": True}

@@ -261,7 +261,8 @@ def colonnade_scene(seed: int = 0, nx: int = 40, nz: int = 16, rings: int = 8, s
         cx = xs[int(rng.uniform(2, nx - 3))] + sp / 2
         cz = zs[int(rng.uniform(2, nz - 3))] + sp / 2
         b.quad_facing([cx - 1, 7.5, cz + 1], [cx + 1, 7.5, cz + 1], [cx + 1, 7.5, cz - 1], [cx - 1, 7.5, cz - 1], (0, -1, 0))
-    cam = Camera((1.25 + 0.0, 1.7, 1.25), (21.25, 1.3, -3.75), 60, 0.05)
+    # the eye stands in the aisle between four columns (columns stand at odd multiples of 1.25 m)
+    cam = Camera((0.0, 1.7, 0.0), (21.25, 1.3, -3.75), 60, 0.05)
     from .frame import SUN_E, SKY
     return b.scene(f"colonnade-{seed}", cam, sun_dir=(-0.4, 1.0, 0.3), sun_e=SUN_E, sky=SKY)
 
