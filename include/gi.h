@@ -89,6 +89,16 @@ typedef struct {
   uint32_t reserved[4];
 } gi_rc_params;
 
+/* World probes (RcParams.method 'world', rc.ts:253-570): probes on a world-space grid registered from the G-buffer's
+ * pixels, LOD by distance (spacing sMin * 2^lod, frame word 104; P, frame word 106), kept in one hash table per cascade,
+ * relocated out of the surface, merged through their parents, with a history on the c0 SH (rc.ts:775-816). */
+enum { GI_RELOCATE_GBUFFER = 0, GI_RELOCATE_NONE = 1, GI_RELOCATE_VOXEL = 2 };
+typedef struct {
+  uint32_t relocate;     /* params.relocate: GI_RELOCATE_GBUFFER (default), _NONE, _VOXEL (config token vrel) */
+  uint32_t caps[8];      /* params.caps: probes per cascade (default 2^18, 2^16, 2^14, 2^12, 2^11, 2^10, 2^9, 2^8) */
+  uint32_t reserved[3];
+} gi_world_params;
+
 int gi_version(void);
 const char *gi_status_string(int status);
 /* Message of the calling thread's last failed call ("" when none). */
@@ -161,6 +171,12 @@ int gi_vox_build_noalloc(const gi_vox_params *params, const double eye[3], const
 
 /* ---- radiance cascades (rc.ts Rc), screen probes traced in the voxel world --------------------------------------- */
 int gi_rc_create(gi_ctx *ctx, const gi_rc_params *params, uint32_t width, uint32_t height, gi_rc **out);
+/* createRc with params.method 'world' (rc.ts:1019) and the voxel world tracer: the same cascades (P unused, the
+ * frame's P and sMin set the probe spacing), probes and atlas laid out by capacity.  Every later gi_rc_solve /
+ * gi_solve runs registerPixels .. linkParents, the trace, mergeWorld, projectSH with the c0 history and gatherWorld;
+ * the history keeps one solve (a host that reorders or skips frames changes the result, as in the reference). */
+int gi_rc_create_world(gi_ctx *ctx, const gi_rc_params *params, const gi_world_params *world, uint32_t width,
+                       uint32_t height, gi_rc **out);
 /* The 640-byte Frame uniform exactly as packFrame (frame.ts:76-94) writes it. */
 int gi_rc_set_frame(gi_rc *rc, const void *frame640, void *stream);
 /* G-buffer from host memory: depth (W*H f32, reversed Z, 0 = background) and the shading normal, either as
@@ -255,7 +271,12 @@ enum {
   GI_RC_SHADOW = 7,     /* size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
   GI_RC_BOUNCE_VOL = 8, /* the two bounce volumes, dx*dy*(6dz+1) rgba16f texels each (only with multi-bounce on) */
   GI_RC_BOUNCE_INJ = 9, /* per voxel the injected irradiance: 8 halves (front rgb, 0, back rgb, 0) (multi-bounce on) */
-  GI_RC_BOUNCE_LIST = 10 /* 4 + dx*dy*dz words: listed probes, frame counter, current volume, then the list */
+  GI_RC_BOUNCE_LIST = 10, /* 4 + dx*dy*dz words: listed probes, frame counter, current volume, then the list */
+  GI_RC_WORLD_KEYS = 11,  /* world probes: every cascade's hash table of probe keys (0 = empty) */
+  GI_RC_WORLD_SLOTS = 12, /* world probes: per hash slot the key's probe (0xffffffff: none, or past the capacity) */
+  GI_RC_WORLD_PARENTS = 13, /* world probes: per probe the 8 probes of the cascade above it merges (0xffffffff: none) */
+  GI_RC_WORLD_STATE = 14  /* world probes: 64 words: [0] history parity, [7] nonzero if a compaction's scan stopped
+                             waiting (never expected), [8 + c] probes of cascade c, [16 + c] first ray of cascade c */
 };
 int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
 int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);

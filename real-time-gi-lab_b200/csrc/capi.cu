@@ -136,6 +136,8 @@ struct gi_rc {
   bool bounce = false;               // gi_rc_set_bounce: the volume, its buffers and the voxel world it is bound to
   BounceDev bn = {};
   gi_vox *bn_vox = nullptr;
+  bool world = false;                // world probes (gi_rc_create_world)
+  WorldDev w = {};
 };
 
 static void free_scene(gi_scene *s) {
@@ -162,6 +164,9 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
   cudaFree(r->bn.ray_out);
+  cudaFree(r->w.keys); cudaFree(r->w.slot_probe); cudaFree(r->w.parents); cudaFree(r->w.state); cudaFree(r->w.look);
+  cudaFree(r->w.hist_tab); cudaFree(r->w.hist_grid); cudaFree(r->w.hist_sh);
+  r->w = WorldDev{};
   r->bn = BounceDev{};
   r->bounce = false;
   r->dev.bn_inj = nullptr;
@@ -505,7 +510,8 @@ int gi_vox_destroy(gi_vox *v) {
 // ---- radiance cascades --------------------------------------------------------------------------------------------------
 static size_t atlas_elem_bytes(uint32_t atlas) { return atlas == GI_ATLAS_F32 ? 16u : 8u; }
 
-int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_rc **out) {
+// gi_rc_create and gi_rc_create_world (wp != NULL)
+static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *wp, uint32_t W, uint32_t H, gi_rc **out) {
   if (!ctx || !p || !out) return fail(GI_ERR_INVALID, "gi_rc_create: NULL argument");
   *out = nullptr;
   if (p->cascades < 1 || p->cascades > 8) return fail(GI_ERR_INVALID, "gi_rc_create: at most 8 cascades (rc.ts:1022), got %u", p->cascades);
@@ -514,6 +520,12 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   if (p->atlas > GI_ATLAS_BF16) return fail(GI_ERR_INVALID, "gi_rc_create: atlas %u", p->atlas);
   if (p->dda_cap < 1) return fail(GI_ERR_INVALID, "gi_rc_create: dda_cap must be >= 1");
   if (!(p->k_interval > 0.0f)) return fail(GI_ERR_INVALID, "gi_rc_create: k_interval must be > 0");
+  if (wp) {
+    if (wp->relocate > GI_RELOCATE_VOXEL) return fail(GI_ERR_INVALID, "gi_rc_create_world: relocate %u", wp->relocate);
+    for (uint32_t i = 0; i < p->cascades; i++)
+      if (wp->caps[i] < 1u || wp->caps[i] > (1u << 24))
+        return fail(GI_ERR_INVALID, "gi_rc_create_world: cascade %u capacity %u (1 .. 2^24)", i, wp->caps[i]);
+  }
   CK(cudaSetDevice(ctx->device), "gi_rc_create: cudaSetDevice");
   gi_rc *r = new (std::nothrow) gi_rc;
   if (!r) return fail(GI_ERR_OOM, "gi_rc_create: host allocation");
@@ -534,9 +546,13 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     c.res = 4u << rc_;
     uint64_t ts = (uint64_t)p->P << i;
     if (ts > (1u << 20)) return delete r, fail(GI_ERR_INVALID, "gi_rc_create: tile size overflow");
-    c.tile_size = (uint32_t)ts;
-    c.tiles_x = (uint32_t)((W + ts - 1) / ts);
-    c.tiles_y = (uint32_t)((H + ts - 1) / ts);
+    if (wp) {   // world probes: no screen tiles; probes and atlas entries by capacity (rc.ts:1029)
+      c.tile_size = 0; c.tiles_x = wp->caps[i]; c.tiles_y = 1;
+    } else {
+      c.tile_size = (uint32_t)ts;
+      c.tiles_x = (uint32_t)((W + ts - 1) / ts);
+      c.tiles_y = (uint32_t)((H + ts - 1) / ts);
+    }
     c.probe_off = (uint32_t)probe_total;
     c.rad_off = (uint32_t)ray_total;
     c.ray_off = (uint32_t)ray_total;
@@ -547,7 +563,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
     c.b0 = (float)b0; c.b1 = (float)b1;
     c.dirs_log2 = 2u * (2u + rc_);
     c.np = c.tiles_x * c.tiles_y;
-    c.inv_tile = (c.tile_size & (c.tile_size - 1u)) == 0u ? 1.0f / (float)c.tile_size : 0.0f;
+    c.inv_tile = c.tile_size && (c.tile_size & (c.tile_size - 1u)) == 0u ? 1.0f / (float)c.tile_size : 0.0f;
     probe_total += (uint64_t)c.tiles_x * c.tiles_y;
     ray_total += (uint64_t)c.tiles_x * c.tiles_y * c.res * c.res;
   }
@@ -580,7 +596,7 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
   // the merge's quad averages of a cascade whose resolution is twice the one below
   size_t avg_elems = 1;
-  for (uint32_t i = 1; i < p->cascades; i++)
+  for (uint32_t i = 1; i < p->cascades && !wp; i++)
     if (d.c[i].res == 2u * d.c[i - 1].res) {
       size_t n = (size_t)d.c[i].np * d.c[i].res * d.c[i].res / 4u;
       if (n > avg_elems) avg_elems = n;
@@ -612,8 +628,45 @@ int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_
   }
   r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->sh_elem_bytes + npx * r->irr_elem_bytes + 96 * 4;
+  if (wp) {
+    WorldDev &w = r->w;
+    uint64_t hash_total = 0, look_total = 0;
+    for (uint32_t i = 0; i < p->cascades; i++) {
+      uint32_t hs = 1;
+      while (hs < 2u * wp->caps[i]) hs <<= 1;   // nextPow2(2 cap) (rc.ts:978, :1030)
+      w.hash_off[i] = (uint32_t)hash_total; w.hash_mask[i] = hs - 1u; w.cap[i] = wp->caps[i];
+      w.look_off[i] = (uint32_t)look_total;
+      hash_total += hs;
+      look_total += (hs + 255u) / 256u + 1u;
+    }
+    w.hash_total = (uint32_t)hash_total; w.look_total = (uint32_t)look_total;
+    w.relocate = wp->relocate; w.hist_h = w.hash_mask[0] + 1u;
+    const size_t cap0 = wp->caps[0];
+    if ((e = dalloc(&w.keys, hash_total)) || (e = dalloc(&w.slot_probe, hash_total)) ||
+        (e = dalloc(&w.parents, probe_total * 8u)) || (e = dalloc(&w.state, 64)) || (e = dalloc(&w.look, look_total)) ||
+        (e = dalloc(&w.hist_tab, 2u * (size_t)w.hist_h)) || (e = dalloc(&w.hist_grid, 2u * cap0)) ||
+        (e = dalloc(&w.hist_sh, 16u * cap0)) || (e = cudaMemset(w.state, 0, 64 * 4)) ||
+        (e = cudaMemset(w.hist_tab, 0, 2u * (size_t)w.hist_h * 4u)) || (e = cudaMemset(w.parents, 0xff, probe_total * 32u))) {
+      free_rc(r);
+      delete r;
+      return cuda_fail(e, "gi_rc_create_world");
+    }
+    r->world = true;
+    r->bytes += hash_total * 8u + probe_total * 32u + 64 * 4 + look_total * 8u + 2u * (uint64_t)w.hist_h * 4u +
+                cap0 * (2u * 16u + 16u * 16u);
+  }
   *out = r;
   return GI_OK;
+}
+
+int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_rc **out) {
+  return rc_create(ctx, p, nullptr, W, H, out);
+}
+
+int gi_rc_create_world(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *world, uint32_t W, uint32_t H,
+                       gi_rc **out) {
+  if (!world) return fail(GI_ERR_INVALID, "gi_rc_create_world: NULL world parameters");
+  return rc_create(ctx, p, world, W, H, out);
 }
 
 int gi_rc_set_frame(gi_rc *r, const void *frame640, void *stream) {
@@ -723,6 +776,9 @@ int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_set_bounce: cudaSetDevice");
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
   cudaFree(r->bn.ray_out);
+  cudaFree(r->w.keys); cudaFree(r->w.slot_probe); cudaFree(r->w.parents); cudaFree(r->w.state); cudaFree(r->w.look);
+  cudaFree(r->w.hist_tab); cudaFree(r->w.hist_grid); cudaFree(r->w.hist_sh);
+  r->w = WorldDev{};
   r->bn = BounceDev{};
   r->bounce = false;
   r->bn_vox = nullptr;
@@ -773,7 +829,7 @@ int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   r->dev.hits = r->debug_hits ? r->hits : nullptr;
   r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
   CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr, &r->launch,
-                        r->bounce ? &r->bn : nullptr),
+                        r->bounce ? &r->bn : nullptr, r->world ? &r->w : nullptr),
      "gi_rc_solve: launch");
   r->timed = r->timing;
   r->timed_vox = false;
@@ -960,6 +1016,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
     if (r->dev.atlas != r0.atlas || r->dev.c[0].tile_size != r0.c[0].tile_size)
       return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has another atlas format or probe spacing than solve 0", i);
     if (r->bounce) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has multi-bounce on (capture its chain with gi_batch_capture)", i);
+    if (r->world) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has world probes (capture its chain with gi_batch_capture)", i);
   }
   const uint32_t P0 = r0.c[0].tile_size;
   if (P0 != 8u && P0 != 16u && P0 != 32u)
@@ -1196,6 +1253,9 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
     case GI_RC_BOUNCE_VOL: *bytes = r->bounce ? 2u * (size_t)r->bn.dx * r->bn.dy * (6u * r->bn.dz + 1u) * 8u : 0u; break;
     case GI_RC_BOUNCE_INJ: *bytes = r->bounce ? (size_t)r->bn_vox->p.max_voxels * 16u : 0u; break;
     case GI_RC_BOUNCE_LIST: *bytes = r->bounce ? (4u + (size_t)r->bn.n) * 4u : 0u; break;
+    case GI_RC_WORLD_KEYS: case GI_RC_WORLD_SLOTS: *bytes = r->world ? (size_t)r->w.hash_total * 4u : 0u; break;
+    case GI_RC_WORLD_PARENTS: *bytes = r->world ? (size_t)r->dev.probes_total * 32u : 0u; break;
+    case GI_RC_WORLD_STATE: *bytes = r->world ? 64u * 4u : 0u; break;
     default: return fail(GI_ERR_INVALID, "gi_rc_buffer_bytes: unknown buffer %d", what);
   }
   return GI_OK;
@@ -1219,6 +1279,10 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
     case GI_RC_SHADOW: src = r->shadow; break;
     case GI_RC_BOUNCE_INJ: src = r->bn.inj; break;
     case GI_RC_BOUNCE_LIST: src = r->bn.list; break;
+    case GI_RC_WORLD_KEYS: src = r->w.keys; break;
+    case GI_RC_WORLD_SLOTS: src = r->w.slot_probe; break;
+    case GI_RC_WORLD_PARENTS: src = r->w.parents; break;
+    case GI_RC_WORLD_STATE: src = r->w.state; break;
     case GI_RC_BOUNCE_VOL:
       if (r->bounce) {   // two allocations: copy them one after the other
         size_t half = need / 2u;
@@ -1239,6 +1303,7 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
 
 int gi_rc_merge_gather_f64(gi_rc *r, void *stream) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_merge_gather_f64: NULL rc");
+  if (r->world) return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: screen probes only");
   if (r->p.atlas != GI_ATLAS_F32) return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: needs an F32 atlas");
   if (!r->debug_hits || !r->rad_traced)
     return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: the traced intervals are not kept (gi_rc_set_debug_hits)");

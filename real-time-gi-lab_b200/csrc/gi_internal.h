@@ -48,6 +48,23 @@ struct RcDev {
   const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)
 };
 
+// World probes (the method 'world', rc.ts:253-570): per cascade a hash table of probe keys, the probes compacted from
+// it in slot order, and the parents each probe merges; the c0 history of two solves.  Probes and atlas entries are laid
+// out by capacity (RcDev.c[c].probe_off / rad_off); the counts are device-side.
+struct WorldDev {
+  uint32_t hash_off[8], hash_mask[8], cap[8], look_off[8];
+  uint32_t hash_total, look_total, relocate, hist_h;   // relocate: 0 'gbuffer', 1 'none', 2 'voxel'; hist_h = hash size of c0
+  uint32_t *keys;                  // hash_total: key or 0
+  uint32_t *slot_probe;            // hash_total: the key's probe or NONE
+  uint32_t *parents;               // probes * 8: the probes of the cascade above a probe merges (NONE: none)
+  uint32_t *state;                 // [0] the history parity of the current solve, [8 + c] probes of cascade c (min(keys,
+                                   // cap)), [16 + c] first ray of cascade c in the trace order (c <= cascades)
+  unsigned long long *look;        // the compactions' chained scans, cascade c at look_off[c]
+  uint32_t *hist_tab;              // 2 * hist_h: probe + 1 or 0, per parity
+  int4 *hist_grid;                 // 2 * cap0: grid point and LOD of each probe, per parity
+  float4 *hist_sh;                 // 2 * cap0 * 8: the SH as stored, per parity
+};
+
 // The multi-bounce volume (bounce.ts): dx x dy x dz irradiance probes around the camera, rebuilt every frame from the
 // voxels, each an ambient cube (six axes: rgb irradiance, alpha the reach along the axis), stored rgba16f in two
 // volumes that swap every frame (this frame's is written, the previous one read by the probes' own rays).
@@ -148,8 +165,10 @@ struct BatchDev {
 struct BatchSizes { uint32_t setup_blocks, merge_blocks[8], gather_blocks, atlas, P0; };
 }  // namespace gi
 cudaError_t gi_launch_batch_passes(const gi::BatchDev &b, const gi::BatchSizes &z, uint32_t sm_count, cudaStream_t st);
+// w: world probes (nullptr: screen probes)
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
-                               cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr, const gi::BounceDev *bn = nullptr);
+                               cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr, const gi::BounceDev *bn = nullptr,
+                               const gi::WorldDev *w = nullptr);
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);

@@ -11,6 +11,7 @@
 
 #include "gi_dev.cuh"
 #include "gi_internal.h"
+#include "gi_scan.cuh"
 
 namespace gi {
 
@@ -1054,12 +1055,23 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   return cudaGetLastError();
 }
 
+// ---- world probes (method 'world') ----------------------------------------------------------------------------------
+#include "world.cuh"
+
 }  // namespace gi
 
 using namespace gi;
 
 cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
-                               const RcLaunch *ls, const BounceDev *bn) {
+                               const RcLaunch *ls, const BounceDev *bn, const WorldDev *w) {
+  if (w) {
+    switch (r.atlas) {
+      case GI_ATLAS_F32: return launch_world<GI_ATLAS_F32>(r, v, *w, sm_count, st, ev, ls, bn);
+      case GI_ATLAS_F16: return launch_world<GI_ATLAS_F16>(r, v, *w, sm_count, st, ev, ls, bn);
+      case GI_ATLAS_BF16: return launch_world<GI_ATLAS_BF16>(r, v, *w, sm_count, st, ev, ls, bn);
+    }
+    return cudaErrorInvalidValue;
+  }
   switch (r.atlas) {
     case GI_ATLAS_F32: return launch_solve<GI_ATLAS_F32>(r, v, sm_count, st, ev, ls, bn);
     case GI_ATLAS_F16: return launch_solve<GI_ATLAS_F16>(r, v, sm_count, st, ev, ls, bn);

@@ -9,7 +9,7 @@ from typing import Optional
 import numpy as np
 
 from . import _lib
-from .configs import RcParams, VoxParams, cascade_layout
+from .configs import RcParams, VoxParams, cascade_layout, world_layout
 from .scenes import Scene
 
 _P = C.c_void_p
@@ -171,24 +171,33 @@ ATLAS_CODES = {"f32": _lib.GI_ATLAS_F32, "f16": _lib.GI_ATLAS_F16, "bf16": _lib.
 
 
 class Rc:
-    """createRc (rc.ts:1019) / Rc (rc.ts:980-992) for the screen method traced in the voxel world."""
+    """createRc (rc.ts:1019) / Rc (rc.ts:980-992): screen or world probes, traced in the voxel world."""
 
     def __init__(self, ctx: Context, params: RcParams, width: int, height: int):
-        if params.method != "screen" or params.world != "voxel" or params.depthCascades != 0:
+        if params.method not in ("screen", "world") or params.world != "voxel" or params.depthCascades != 0:
             raise _lib.GiError(_lib.GI_ERR_INVALID, f"unsupported configuration (method {params.method}, world "
-                               f"{params.world}, depthCascades {params.depthCascades}): this library runs screen "
-                               "probes traced in the voxel world (token 'voxel')")
+                               f"{params.world}, depthCascades {params.depthCascades}): this library runs screen or "
+                               "world probes traced in the voxel world (token 'voxel')")
         if params.cascades > 8:
             raise _lib.GiError(_lib.GI_ERR_INVALID, "at most 8 cascades")
         self.ctx, self.params, self.width, self.height = ctx, params, width, height
-        self.layout = cascade_layout(params, width, height)
+        self.world = params.method == "world"
+        self.layout = world_layout(params) if self.world else cascade_layout(params, width, height)
         p = _lib.GiRcParams()
         p.cascades, p.P, p.k_interval = params.cascades, params.P, params.kInterval
         p.vox_scale, p.vox_offset, p.vox_skip, p.level_map = params.voxScale, params.voxOffset, params.voxSkip, params.levelMap
         p.res_cap, p.dda_cap, p.stats, p.atlas = params.resCap, params.ddaCap, params.stats, ATLAS_CODES[params.atlas]
         p.f32_out = 1 if params.f32Out else 0
         h = _P()
-        _lib.call("gi_rc_create", ctx.handle, C.byref(p), width, height, C.byref(h))
+        if self.world:
+            wp = _lib.GiWorldParams()
+            wp.relocate = {"gbuffer": _lib.GI_RELOCATE_GBUFFER, "none": _lib.GI_RELOCATE_NONE,
+                           "voxel": _lib.GI_RELOCATE_VOXEL}[params.relocate]
+            for i in range(params.cascades):
+                wp.caps[i] = int(params.caps[i])
+            _lib.call("gi_rc_create_world", ctx.handle, C.byref(p), C.byref(wp), width, height, C.byref(h))
+        else:
+            _lib.call("gi_rc_create", ctx.handle, C.byref(p), width, height, C.byref(h))
         self.handle = h
 
     def set_frame(self, frame: np.ndarray, stream=None):
@@ -338,6 +347,12 @@ class Rc:
         if self.params.atlas == "f16":
             return raw.view(np.float16).astype(np.float32).reshape(-1, 4)
         return (raw.view(np.uint16).astype(np.uint32) << 16).view(np.float32).reshape(-1, 4)
+
+    def read_world(self, stream=None) -> dict:
+        """World probes: the hash tables, their slots' probes, the parents and the state words."""
+        u = lambda what: self.read_buffer(what, stream).view(np.uint32)
+        return {"keys": u(_lib.GI_RC_WORLD_KEYS), "slot_probe": u(_lib.GI_RC_WORLD_SLOTS),
+                "parents": u(_lib.GI_RC_WORLD_PARENTS), "state": u(_lib.GI_RC_WORLD_STATE)}
 
     def destroy(self):
         if self.handle:
