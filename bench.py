@@ -366,6 +366,71 @@ def whole_job_rate(units_per_rank: float, max_seconds: float, world: int) -> flo
     return world * units_per_rank / max_seconds
 
 
+def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
+    """World probes (gi_rc_create_world) on the workload's scene and clipmap: the config world-48-voxel-rc2-vrel-f32
+    with the default capacities, solves replayed from one graph (the c0 history carries between them), L2 flushed
+    between steps outside the step events."""
+    import torch
+    from rtgi import _lib, configs, frame as fr, gpu
+    p = configs.parse_config("world-48-voxel-rc2-vrel-f32-dda256", {"cascades": 5})
+    lvp, bias = [0.0] * 16, (0.0, 0.0)
+    if desc["shadow_map"]:
+        bmin, bmax = fr.scene_bounds(s.positions)
+        lvp, bias = fr.scene_sun_view_proj(bmin, bmax, s.sun_dir), fr.SHADOW_BIAS
+    F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=s.sun_e, sky=s.sky,
+                                     cascades=p.cascades, P=p.P, light_view_proj=lvp, shadow_bias=bias))
+    rc = gpu.Rc(ctx, p, W, H)
+    with torch.cuda.stream(stream):
+        rc.set_frame(F, stream)
+        rc.render_gbuffer(sg, stream)
+        if desc["shadow_map"]:
+            rc.render_shadow(sg, desc["shadow_map"], stream)
+        vw.update(s.camera.eye)
+        rc.set_stats(1)
+        rc.solve(vw, stream)
+        counts = rc.read_counts(stream)
+        rc.set_stats(0)
+        rc.set_timing(True)
+        w_pass = {k: [] for k in rc.PASSES}
+        for _ in range(max(5, args.warmup)):
+            rc.solve(vw, stream)
+            for k, x in rc.pass_times().items():
+                w_pass[k].append(x)
+        rc.set_timing(False)
+        rc.graph_capture(vw, stream)
+        for _ in range(args.warmup):
+            flush.zero_()
+            rc.graph_launch(stream)
+        n_w = max(3, min(args.steps, 500))
+        ws_, we_ = ([torch.cuda.Event(enable_timing=True) for _ in range(n_w)] for _ in range(2))
+        for k in range(n_w):
+            flush.zero_()
+            ws_[k].record(stream)
+            rc.graph_launch(stream)
+            we_[k].record(stream)
+        torch.cuda.synchronize()
+        counts2 = rc.read_counts(stream)
+    w_ms = sorted(a.elapsed_time(c) for a, c in zip(ws_, we_))
+    w_total = max_over_ranks(sum(w_ms), dist, "cuda")
+    lay = rc.layout
+    probes = [int(min(counts[c], lay["casc"][c]["cap"])) for c in range(p.cascades)]
+    rays = sum(n * lay["casc"][c]["res"] ** 2 for c, n in enumerate(probes))
+    valid = int((rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32) > 0).sum())
+    out = {"value": whole_job_rate(n_w, w_total / 1000.0, world), "unit": "solves/s", "steps": n_w,
+           "ms_per_step": w_total / n_w, "p50_ms": w_ms[n_w // 2],
+           "p99_ms": w_ms[min(n_w - 1, int(math.ceil(0.99 * n_w)) - 1)],
+           "config": "world-48-voxel-rc2-vrel-f32-dda256, 5 cascades, caps 2^18 .. 2^11, the same clipmap and shadow map",
+           "passes_ms": {k: statistics.median(x) for k, x in w_pass.items()},
+           "probes": probes, "rays": rays, "dda_steps": int(counts[32:32 + p.cascades].sum()),
+           "black_pixels_pct": 100.0 * float(counts2[72:80].sum()) / max(valid, 1),
+           # voxel rebuild, then clear, registerPixels, compact + relocateVox per cascade, registerUp + linkParents per
+           # cascade above c0, the trace, a merge per cascade, projectSH, the gather
+           "gpu_launches_per_solve": (11 + (1 if v.levels > 1 else 0)) + 2 + 2 * p.cascades + 2 * (p.cascades - 1) + 1
+                                     + p.cascades + 2}
+    rc.destroy()
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -553,6 +618,12 @@ def run_ours(args, rank, world, local_rank):
             rc.set_bounce(None)
             rc.graph_capture(vw, stream)
 
+    # the reference renderer's default method on the same scene and clipmap: world probes
+    # (world-48-voxel-rc2-vrel, docs/spec/20-renderer.md:21) with the c0 history; a frame of its own (P = 48)
+    world_out = None
+    if args.world:
+        world_out = run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world)
+
     trace_ms = statistics.mean(pass_ms["giTrace"])
     alg = trace_algorithmic_bytes(rc.layout, hdr, v)
     peak, peak_kind = measured_peak()
@@ -576,6 +647,7 @@ def run_ours(args, rank, world, local_rank):
                "shadow_map_ms": shadow_ms,
                "bounce": bounce_out,
                "in_flight": in_flight,
+               "world": world_out,
                "vox_counters": {"bricks": int(min(hdr[0], v.maxBricks)), "voxels": int(hdr[1]),
                                 "bricksPerLevel": [int(x) for x in hdr[8:8 + v.levels]]},
                "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -623,6 +695,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline leg")
     ap.add_argument("--tuning", default=None, help="fixed launch shapes as JSON (skips the autotuner)")
     ap.add_argument("--no-bounce", dest="bounce", action="store_false", help="skip the multi-bounce measurement")
+    ap.add_argument("--no-world", dest="world", action="store_false", help="skip the world-probe measurement")
     ap.add_argument("--no-in-flight", dest="in_flight", action="store_false",
                     help="skip the two-frames-in-flight measurement")
     ap.add_argument("--batch", type=int, default=64, help="uneven solves of the batched measurement (0: skip)")
