@@ -637,7 +637,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
       w.hash_off[i] = (uint32_t)hash_total; w.hash_mask[i] = hs - 1u; w.cap[i] = wp->caps[i];
       w.look_off[i] = (uint32_t)look_total;
       hash_total += hs;
-      look_total += (hs + 255u) / 256u + 1u;
+      look_total += (hs + 2047u) / 2048u + 1u;   // compact's blocks of 2048 slots, + the ticket word
     }
     w.hash_total = (uint32_t)hash_total; w.look_total = (uint32_t)look_total;
     w.relocate = wp->relocate; w.hist_h = w.hash_mask[0] + 1u;

@@ -16,6 +16,7 @@
 //  * the trace is the persistent ray loop of the screen path over the rays of every cascade's live probes.
 
 constexpr uint32_t W_NONE = 0xffffffffu;
+constexpr uint32_t W_COMPACT_SLOTS = 2048;   // hash slots per compact block (8 a thread)
 
 // hash32 (rc.ts:248-250)
 __device__ __forceinline__ uint32_t w_hash32(uint32_t x) {
@@ -37,12 +38,15 @@ __device__ __forceinline__ i3 w_origin(const float *__restrict__ F, float s) {
   const i3 o = vf2i(vfloor(mk(F[F_EYE] / s, F[F_EYE + 1] / s, F[F_EYE + 2] / s)));
   return mki(o.x - 256, o.y - 256, o.z - 256);
 }
-// keyFor (rc.ts:255-259)
-__device__ __forceinline__ uint32_t w_key(const float *__restrict__ F, i3 g, int lod, uint32_t c) {
-  const i3 o = w_origin(F, w_spacing(F, lod, c));
+// keyFor (rc.ts:255-259) with the origin of (lod, c) given: the origin depends only on them, so callers that make
+// several keys of one LOD and cascade compute it once
+__device__ __forceinline__ uint32_t w_key_at(i3 g, i3 o, int lod) {
   const i3 r = mki(g.x - o.x, g.y - o.y, g.z - o.z);
   if (r.x < 0 || r.y < 0 || r.z < 0 || r.x >= 512 || r.y >= 512 || r.z >= 512) return W_NONE;
   return 0x80000000u | ((uint32_t)lod << 27) | ((uint32_t)r.x << 18) | ((uint32_t)r.y << 9) | (uint32_t)r.z;
+}
+__device__ __forceinline__ uint32_t w_key(const float *__restrict__ F, i3 g, int lod, uint32_t c) {
+  return w_key_at(g, w_origin(F, w_spacing(F, lod, c)), lod);
 }
 __device__ __forceinline__ i3 w_corner(uint32_t k) { return mki((int)(k & 1u), (int)((k >> 1) & 1u), (int)((k >> 2) & 1u)); }
 
@@ -176,7 +180,7 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
   const uint32_t sx = (r.width + st - 1u) / st, sy = (r.height + st - 1u) / st;
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x, lane = threadIdx.x & 31u;
   int lod = 0;
-  i3 b = mki(0, 0, 0);
+  i3 b = mki(0, 0, 0), org0 = mki(0, 0, 0);
   bool live = false;
   if (i < sx * sy) {
     const int px = (int)((i % sx) * st + st / 2u), py = (int)((i / sx) * st + st / 2u);
@@ -187,6 +191,7 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
         lod = w_lod_for(F, length3(x - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2])));
         const float s = w_spacing(F, lod, 0u);
         b = vf2i(vfloor(mk(x.x / s, x.y / s, x.z / s)));
+        org0 = w_origin(F, s);
         live = true;
       }
     }
@@ -194,7 +199,7 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
 #pragma unroll 1
   for (uint32_t k = 0; k < 8u; k++) {
     const i3 o = w_corner(k);
-    const uint32_t key = live ? w_key(F, mki(b.x + o.x, b.y + o.y, b.z + o.z), lod, 0u) : W_NONE;
+    const uint32_t key = live ? w_key_at(mki(b.x + o.x, b.y + o.y, b.z + o.z), org0, lod) : W_NONE;
     const unsigned grp = __match_any_sync(0xffffffffu, key);
     if (key != W_NONE && (uint32_t)(__ffs(grp) - 1) == lane)
       if (!w_insert(w.keys + w.hash_off[0], w.hash_mask[0], key)) atomicAdd(&r.counts[16], 1u);
@@ -205,49 +210,22 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
 __global__ void __launch_bounds__(256) k_w_register_up(RcDev r, WorldDev w, uint32_t c) {
   grid_dep_wait();
   const float *F = r.frame;
-  const uint32_t n = w.state[8 + c - 1u];
+  const uint32_t n = w.state[8 + c - 1u] * 8u;   // one thread per (probe, corner)
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
-    const int4 g = r.probes[r.c[c - 1u].probe_off + t].grid;
-    const i3 lo = mki(g.x >> 1, g.y >> 1, g.z >> 1);
-    const bool ox = (g.x & 1) != 0, oy = (g.y & 1) != 0, oz = (g.z & 1) != 0;
-    for (uint32_t k = 0; k < 8u; k++) {
-      const i3 o = w_corner(k);
-      if ((o.x > 0 && !ox) || (o.y > 0 && !oy) || (o.z > 0 && !oz)) continue;
-      const uint32_t key = w_key(F, mki(lo.x + o.x, lo.y + o.y, lo.z + o.z), g.w, c);
-      if (key != W_NONE && !w_insert(w.keys + w.hash_off[c], w.hash_mask[c], key)) atomicAdd(&r.counts[16 + c], 1u);
-    }
+    const int4 g = r.probes[r.c[c - 1u].probe_off + (t >> 3)].grid;
+    const i3 o = w_corner(t & 7u);
+    if ((o.x > 0 && (g.x & 1) == 0) || (o.y > 0 && (g.y & 1) == 0) || (o.z > 0 && (g.z & 1) == 0)) continue;
+    const uint32_t key = w_key(F, mki((g.x >> 1) + o.x, (g.y >> 1) + o.y, (g.z >> 1) + o.z), g.w, c);
+    if (key != W_NONE && !w_insert(w.keys + w.hash_off[c], w.hash_mask[c], key)) atomicAdd(&r.counts[16 + c], 1u);
   }
 }
 
-// compact (rc.ts:520-537): a chained scan over the table's slots (256 a block) numbers the keys in slot order; the
-// probe of each key below the capacity is written (relocated from the G-buffer with relocate 'gbuffer'), the last part
-// publishes the count and the first ray of the next cascade.
-__global__ void __launch_bounds__(256) k_w_compact(RcDev r, VoxDev v, WorldDev w, uint32_t c) {
-  grid_dep_wait();
+// compact's write for the key in slot h with probe index idx: slotProbe, and the probe (relocated from the G-buffer
+// with relocate 'gbuffer') with its voxel level
+__device__ __forceinline__ void w_compact_slot(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t c, uint32_t h,
+                                               uint32_t key, uint32_t idx) {
   const float *F = r.frame;
-  const uint32_t size = w.hash_mask[c] + 1u, nblk = (size + 255u) / 256u, cap = w.cap[c];
-  unsigned long long *look = w.look + w.look_off[c];
-  const uint32_t blk = chain_ticket(look);
-  const uint32_t h = blk * 256u + threadIdx.x;
-  const uint32_t key = h < size ? w.keys[w.hash_off[c] + h] : 0u;
-  uint32_t tot;
-  const uint32_t ex = block_scan_256(key != 0u ? 1u : 0u, &tot);
-  __shared__ uint32_t s_pre;
-  if (threadIdx.x == 0) s_pre = chain_prefix(look, blk, tot, w.state + 1);   // a give-up sets state[7]
-  __syncthreads();
-  const uint32_t idx = s_pre + ex;
-  const int over = __syncthreads_count(key != 0u && idx >= cap);
-  if (threadIdx.x == 0) {
-    if (over) atomicAdd(&r.counts[8 + c], (uint32_t)over);
-    if (blk == nblk - 1u) {
-      const uint32_t total = s_pre + tot, np = min(total, cap);
-      r.counts[c] = total;
-      w.state[8 + c] = np;
-      w.state[16 + c + 1u] = w.state[16 + c] + (np << r.c[c].dirs_log2);
-    }
-  }
-  if (key == 0u) return;
-  if (idx >= cap) { w.slot_probe[w.hash_off[c] + h] = W_NONE; return; }
+  if (idx >= w.cap[c]) { w.slot_probe[w.hash_off[c] + h] = W_NONE; return; }
   w.slot_probe[w.hash_off[c] + h] = idx;
   const int lod = (int)((key >> 27) & 15u);
   const float s = w_spacing(F, lod, c);
@@ -263,6 +241,53 @@ __global__ void __launch_bounds__(256) k_w_compact(RcDev r, VoxDev v, WorldDev w
   pr.grid = make_int4(g.x, g.y, g.z, lod);
   r.probes[r.c[c].probe_off + idx] = pr;
   r.plevel[r.c[c].probe_off + idx] = vox_level(v, r, s0, c);
+}
+
+// compact (rc.ts:520-537): a chained scan over the table's slots (W_COMPACT_SLOTS a block, 8 a thread) numbers the
+// keys in slot order; the last part publishes the count and the first ray of the next cascade.
+__global__ void __launch_bounds__(256) k_w_compact(RcDev r, VoxDev v, WorldDev w, uint32_t c) {
+  grid_dep_wait();
+  const uint32_t size = w.hash_mask[c] + 1u, nblk = (size + W_COMPACT_SLOTS - 1u) / W_COMPACT_SLOTS, cap = w.cap[c];
+  unsigned long long *look = w.look + w.look_off[c];
+  const uint32_t blk = chain_ticket(look);
+  const uint32_t h0 = blk * W_COMPACT_SLOTS + threadIdx.x * 8u;
+  uint32_t keys8[8] = {0u, 0u, 0u, 0u, 0u, 0u, 0u, 0u};
+  if (h0 + 8u <= size && (w.hash_off[c] & 3u) == 0u) {   // two aligned 128-bit loads
+    const uint4 *kp = reinterpret_cast<const uint4 *>(w.keys + w.hash_off[c] + h0);
+    const uint4 ka = kp[0], kb = kp[1];
+    keys8[0] = ka.x; keys8[1] = ka.y; keys8[2] = ka.z; keys8[3] = ka.w;
+    keys8[4] = kb.x; keys8[5] = kb.y; keys8[6] = kb.z; keys8[7] = kb.w;
+  } else {
+    for (uint32_t k = 0; k < 8u && h0 + k < size; k++) keys8[k] = w.keys[w.hash_off[c] + h0 + k];
+  }
+  uint32_t mine = 0;
+#pragma unroll
+  for (int k = 0; k < 8; k++) mine += keys8[k] != 0u ? 1u : 0u;
+  uint32_t tot;
+  const uint32_t ex = block_scan_256(mine, &tot);
+  __shared__ uint32_t s_pre, s_over;
+  if (threadIdx.x == 0) {
+    s_pre = chain_prefix(look, blk, tot, w.state + 1);   // a give-up sets state[7]
+    s_over = 0u;
+  }
+  __syncthreads();
+  const uint32_t first = s_pre + ex;
+  const uint32_t over = first >= cap ? mine : (first + mine > cap ? first + mine - cap : 0u);
+  if (over) atomicAdd(&s_over, over);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (s_over) atomicAdd(&r.counts[8 + c], s_over);
+    if (blk == nblk - 1u) {
+      const uint32_t total = s_pre + tot, np = min(total, cap);
+      r.counts[c] = total;
+      w.state[8 + c] = np;
+      w.state[16 + c + 1u] = w.state[16 + c] + (np << r.c[c].dirs_log2);
+    }
+  }
+  uint32_t idx = first;
+#pragma unroll
+  for (uint32_t k = 0; k < 8u; k++)
+    if (keys8[k] != 0u) w_compact_slot(r, v, w, c, h0 + k, keys8[k], idx++);
 }
 
 // relocateVox (rc.ts:414-470), one warp per probe: lane l reads cube cells l and l + 32; lane 0 takes the sums in the
@@ -612,7 +637,7 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
     const int lod = w_lod_for(F, length3(x - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2])));
     const float s0 = w_spacing(F, lod, 0u);
     const f3 gp = mk(x.x / s0, x.y / s0, x.z / s0);
-    const i3 bb = vf2i(vfloor(gp));
+    const i3 bb = vf2i(vfloor(gp)), org0 = w_origin(F, s0);
     const f3 f = gp - vi2f(bb);
     const uint32_t Lo = vox_level_for(v, vox_level(v, r, s0, 0u), x);
     const f3 xo1 = x + n * (1.0f * vox_size(v, Lo));
@@ -624,7 +649,7 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
     const bool vrel = w.relocate == 2u;
     for (uint32_t k = 0; k < 8u; k++) {
       const i3 o = w_corner(k);
-      const uint32_t qi = w_lookup(w, 0u, w_key(F, mki(bb.x + o.x, bb.y + o.y, bb.z + o.z), lod, 0u));
+      const uint32_t qi = w_lookup(w, 0u, w_key_at(mki(bb.x + o.x, bb.y + o.y, bb.z + o.z), org0, lod));
       if (qi == W_NONE) continue;
       const f3 tw = mk(o.x == 1 ? f.x : 1.0f - f.x, o.y == 1 ? f.y : 1.0f - f.y, o.z == 1 ? f.z : 1.0f - f.z);
       const f3 pp = ld3(r.probes[r.c[0].probe_off + qi].pos);
@@ -672,8 +697,8 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
   GI_TRY(gi_launch(k_w_clear, blocks(clear_n), 256, st, r, w));
   GI_TRY(gi_launch(k_w_register_pixels, (r.width * r.height + 255u) / 256u, 256, st, r, w));
   for (uint32_t c = 0; c < N; c++) {
-    if (c > 0) GI_TRY(gi_launch(k_w_register_up, blocks(w.cap[c - 1u]), 256, st, r, w, c));
-    GI_TRY(gi_launch(k_w_compact, (w.hash_mask[c] + 1u + 255u) / 256u, 256, st, r, v, w, c));
+    if (c > 0) GI_TRY(gi_launch(k_w_register_up, blocks((uint64_t)w.cap[c - 1u] * 8u), 256, st, r, w, c));
+    GI_TRY(gi_launch(k_w_compact, (w.hash_mask[c] + W_COMPACT_SLOTS) / W_COMPACT_SLOTS, 256, st, r, v, w, c));
     if (w.relocate == 2u) GI_TRY(gi_launch(k_w_relocate_vox, blocks((uint64_t)w.cap[c] * 32u), 256, st, r, v, w, c));
     if (c > 0) GI_TRY(gi_launch(k_w_link_parents, blocks((uint64_t)w.cap[c - 1u] * 32u), 256, st, r, v, w, c - 1u));
   }
