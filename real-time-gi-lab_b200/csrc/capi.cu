@@ -646,7 +646,8 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
         (e = dalloc(&w.parents, probe_total * 8u)) || (e = dalloc(&w.state, 64)) || (e = dalloc(&w.look, look_total)) ||
         (e = dalloc(&w.hist_tab, 2u * (size_t)w.hist_h)) || (e = dalloc(&w.hist_grid, 2u * cap0)) ||
         (e = dalloc(&w.hist_sh, 16u * cap0)) || (e = cudaMemset(w.state, 0, 64 * 4)) ||
-        (e = cudaMemset(w.hist_tab, 0, 2u * (size_t)w.hist_h * 4u)) || (e = cudaMemset(w.parents, 0xff, probe_total * 32u))) {
+        (e = cudaMemset(w.hist_tab, 0, 2u * (size_t)w.hist_h * 4u)) || (e = cudaMemset(w.parents, 0xff, probe_total * 32u)) ||
+        (e = gi_world_tables())) {
       free_rc(r);
       delete r;
       return cuda_fail(e, "gi_rc_create_world");

@@ -165,6 +165,8 @@ struct BatchDev {
 struct BatchSizes { uint32_t setup_blocks, merge_blocks[8], gather_blocks, atlas, P0; };
 }  // namespace gi
 cudaError_t gi_launch_batch_passes(const gi::BatchDev &b, const gi::BatchSizes &z, uint32_t sm_count, cudaStream_t st);
+// The world probes' device tables (segment sample positions); called before their first solve
+cudaError_t gi_world_tables();
 // w: world probes (nullptr: screen probes)
 cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t sm_count, cudaStream_t st,
                                cudaEvent_t *ev = nullptr, const RcLaunch *ls = nullptr, const gi::BounceDev *bn = nullptr,

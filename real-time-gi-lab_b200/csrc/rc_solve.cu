@@ -1062,6 +1062,16 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
 
 using namespace gi;
 
+cudaError_t gi_world_tables() {
+  float t[16 * 16];
+  for (int k = 1; k <= 16; k++)
+    for (int i = 0; i < 16; i++) {
+      volatile float a = (float)i + 0.5f, b = (float)k;
+      t[(k - 1) * 16 + i] = i < k ? a / b : 0.0f;
+    }
+  return cudaMemcpyToSymbol(g_seg_t, t, sizeof t);
+}
+
 cudaError_t gi_launch_rc_solve(const RcDev &r, const VoxDev &v, uint32_t sm_count, cudaStream_t st, cudaEvent_t *ev,
                                const RcLaunch *ls, const BounceDev *bn, const WorldDev *w) {
   if (w) {

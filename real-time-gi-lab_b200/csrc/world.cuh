@@ -111,11 +111,14 @@ __device__ __forceinline__ f3 w_cube_off(uint32_t k, float vg) {
 __device__ __forceinline__ uint32_t w_seg_samples(const VoxDev &v, f3 d, uint32_t L) {
   return (uint32_t)mn(ceilf(length3(d) / vox_size(v, L)), 16.0f);
 }
+// (i + 0.5) / k for k = 1..16, i < k: the IEEE quotients, tabulated on the host (gi_world_tables)
+__device__ float g_seg_t[16 * 16];
+__device__ __forceinline__ float w_seg_t(uint32_t i, uint32_t k) { return g_seg_t[(k - 1u) * 16u + i]; }
 __device__ __forceinline__ bool w_seg_occluded(const VoxDev &v, f3 a, f3 b, uint32_t L) {
   const f3 d = b - a;
   const uint32_t k = w_seg_samples(v, d, L);
   for (uint32_t i = 0; i < k; i++)
-    if (w_vox_occ(v, L, a + d * (((float)i + 0.5f) / (float)k))) return true;
+    if (w_vox_occ(v, L, a + d * w_seg_t(i, k))) return true;
   return false;
 }
 
@@ -390,7 +393,7 @@ __global__ void __launch_bounds__(256) k_w_link_parents(RcDev r, VoxDev v, World
       const f3 d = ld3(r.probes[r.c[c + 1u].probe_off + q].pos) - a;
       const uint32_t kk = w_seg_samples(v, d, Lv);
       for (uint32_t i = j; i < kk; i += 4u)
-        if (w_vox_occ(v, Lv, a + d * (((float)i + 0.5f) / (float)kk))) { hid = true; break; }
+        if (w_vox_occ(v, Lv, a + d * w_seg_t(i, kk))) { hid = true; break; }
     }
     const uint32_t hm = __ballot_sync(0xffffffffu, hid);
     if (j == 0u) w.parents[(size_t)(r.c[c].probe_off + pi) * 8u + k] = ((hm >> (lane & ~3u)) & 0xFu) ? W_NONE : q;
