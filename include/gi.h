@@ -116,12 +116,26 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
 /* Replaces vertices [first, first + count) (the per-frame pose of moving objects, rcrun.ts:206-214). */
 int gi_scene_update_vertices(gi_scene *scene, uint32_t first, uint32_t count, const float *pos, const float *nrm,
                              void *stream);
+/* The rasters (G-buffer, shadow map) draw rows [0, count); rows past it are voxelised only (a world's clustered
+ * copies, world.ts:20-24).  All rows by default. */
+int gi_scene_set_draw_count(gi_scene *scene, uint32_t count);
 int gi_scene_destroy(gi_scene *scene);
 
 /* ---- voxel world (voxel.ts VoxWorld) ------------------------------------------------------------------------------ */
 int gi_vox_create(gi_scene *scene, const gi_vox_params *params, gi_vox **out);
 /* update(eye) (voxel.ts:868-892 writeUniform): the per-level windows around eye (f64, as the reference's numbers). */
 int gi_vox_update(gi_vox *vox, const double eye[3]);
+/* Worlds (world.ts; voxel.ts:270-288, :765-885): the scene's rows placed at ninst instance offsets (3 floats each,
+ * instance 0 at the origin), chunk row lists `lists` (table rows), key_stride = the scene's rows (a triangle's key is
+ * instance * key_stride + row).  From then on the rebuild reads only this frame's work items (gi_vox_set_items), not
+ * every row.  ninst 0 returns to every row once. */
+int gi_vox_set_world(gi_vox *vox, const float *instances, uint32_t ninst, const uint32_t *lists, uint32_t nlists,
+                     uint32_t key_stride);
+/* This frame's work items (selectItems, world.ts:179-199): nitems x (first thread, source, instance, first level), the
+ * source an offset into the lists or 0x80000000 | first row of a contiguous range; threads = the items' triangles.
+ * Set after gi_vox_update (the items follow the windows); a captured graph keeps the thread count it was captured
+ * with. */
+int gi_vox_set_items(gi_vox *vox, const uint32_t *items, uint32_t nitems, uint32_t threads);
 /* encode(pass) (voxel.ts:897-899): the whole rebuild, clear .. resolveAttr, stream-ordered. */
 int gi_vox_build(gi_vox *vox, void *stream);
 /* readCounters (voxel.ts:908-918): the 64 header words (0 bricks marked, 1 voxels, 2-4 brick/big/voxel overflow,

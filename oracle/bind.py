@@ -75,7 +75,9 @@ def _p(a: np.ndarray) -> int:
 
 class OrcScene(C.Structure):
     _fields_ = [("pos", C.c_void_p), ("nrm", C.c_void_p), ("nverts", C.c_uint32), ("tri", C.c_void_p),
-                ("ntris", C.c_uint32), ("mats", C.c_void_p), ("nmats", C.c_uint32)]
+                ("ntris", C.c_uint32), ("mats", C.c_void_p), ("nmats", C.c_uint32),
+                ("items", C.c_void_p), ("nitems", C.c_uint32), ("threads", C.c_uint32), ("key_stride", C.c_uint32),
+                ("ninst", C.c_uint32), ("lists", C.c_void_p), ("inst", C.c_void_p)]
 
 
 class OrcVox(C.Structure):
@@ -149,8 +151,22 @@ def vox_origins(v0: float, levels: int, G: int, eye) -> np.ndarray:
 
 
 def vox_build(scene, v0: float, levels: int, G: int, max_bricks: int, max_voxels: int, eye,
-              coarse_from_triangles: bool = False, big_cap: int = 1 << 18) -> dict:
+              coarse_from_triangles: bool = False, big_cap: int = 1 << 18, world=None) -> dict:
+    """The rebuild; with `world` (rtgi.world.World, the scene its with_world output) the work items of the windows
+    around eye (selectItems) instead of every row."""
     s, keep = _scene_struct(scene)
+    if world is not None:
+        from rtgi import world as W
+        items, threads = W.item_records(W.select_items(world, W.windows(float(v0), levels, G, eye)))
+        lists = world.lists()
+        inst = np.zeros((len(world.instances), 4), np.float32)
+        inst[:, :3] = np.asarray(world.instances, np.float64).astype(np.float32)
+        nitems = len(items)
+        items = np.ascontiguousarray(items if nitems else np.zeros((1, 4), np.uint32), np.uint32)
+        lists = np.ascontiguousarray(lists if lists.size else np.zeros(1, np.uint32), np.uint32)
+        keep = keep + (items, lists, inst)
+        s.items, s.nitems, s.threads = _p(items), nitems, threads
+        s.key_stride, s.ninst, s.lists, s.inst = world.rows, len(world.instances), _p(lists), _p(inst)
     per = G ** 3
     st = {
         "hdr": np.zeros(64, np.uint32), "ptr": np.zeros(levels * per, np.uint32),

@@ -55,6 +55,13 @@ typedef struct {
   uint32_t ntris;
   const orc_material *mats;
   uint32_t nmats;
+  /* World work items (world.ts; voxel.ts:270-288), NULL items: one contiguous item over every row, instance 0.
+   * items: nitems x (first thread, source, instance, first level), the source an offset into lists or
+   * 0x80000000 | first row; a triangle's key is instance * key_stride + row; inst: 4 floats per instance (offset). */
+  const uint32_t *items;
+  uint32_t nitems, threads, key_stride, ninst;
+  const uint32_t *lists;
+  const float *inst;
 } orc_scene;
 
 /* Voxel world state, laid out exactly as the CUDA path lays it out in device memory (struct of arrays). */

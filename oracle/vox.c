@@ -25,13 +25,32 @@ static inline i3 org(const orc_vox *vx, uint32_t L) { return I(vx->origin[L][0],
 static inline v3 region_lo(const orc_vox *vx, uint32_t L) { return muls(muls(vi2f(org(vx, L)), vox_size(vx, L)), 8.0f); }
 static inline i3 ishr(i3 a, int s) { return I(a.x >> s, a.y >> s, a.z >> s); }
 
-static tri_t load_tri(const orc_scene *s, uint32_t t) {
+/* loadTri (voxel.ts:270-276): key = instance * key_stride + row; the instance's offset moves the triangle */
+static tri_t load_tri(const orc_scene *s, uint32_t key) {
   tri_t T;
-  const uint32_t *i = s->tri + 4u * t;
+  uint32_t inst = s->items ? key / s->key_stride : 0u, row = key - inst * (s->items ? s->key_stride : 0u);
+  const uint32_t *i = s->tri + 4u * row;
   T.a = fromf(s->pos + 3u * i[0]); T.b = fromf(s->pos + 3u * i[1]); T.c = fromf(s->pos + 3u * i[2]);
+  if (s->items) {
+    v3 o = fromf(s->inst + 4u * inst);
+    T.a = add(T.a, o); T.b = add(T.b, o); T.c = add(T.c, o);
+  }
   T.idx = i;
   return T;
 }
+/* workAt (voxel.ts:280-288): thread i of a triangle pass -> its key and first level */
+static uint32_t work_at(const orc_scene *s, uint32_t i, uint32_t *first) {
+  if (!s->items) { *first = 0; return i; }
+  uint32_t lo = 0, hi = s->nitems;
+  while (hi - lo > 1u) { uint32_t m = (lo + hi) / 2u; if (s->items[m * 4u] <= i) lo = m; else hi = m; }
+  const uint32_t *b = s->items + lo * 4u;
+  uint32_t j = i - b[0], src = b[1];
+  uint32_t row = (src & 0x80000000u) ? (src & 0x7fffffffu) + j : s->lists[src + j];
+  *first = b[3];
+  return b[2] * s->key_stride + row;
+}
+static uint32_t threads_of(const orc_scene *s) { return s->items ? s->threads : s->ntris; }
+static uint32_t key_limit(const orc_scene *s) { return s->items ? s->ninst * s->key_stride : s->ntris; }
 
 /* voxRange (voxel.ts:293-300) */
 static range_t vox_range(const orc_vox *vx, const tri_t *T, uint32_t L, float cell) {
@@ -175,9 +194,10 @@ int orc_vox_build(const orc_scene *s, orc_vox *vx) {
   for (uint32_t i = 0; i < NL * per; i++) vx->ptr[i] = ORC_EMPTY;
 
   /* markBricks + markBricksBig (voxel.ts:359-387) */
-  for (uint32_t t = 0; t < s->ntris; t++) {
+  for (uint32_t i = 0; i < threads_of(s); i++) {
+    uint32_t L0, t = work_at(s, i, &L0);
     tri_t T = load_tri(s, t);
-    for (uint32_t L = 0; L < NL; L++) {
+    for (uint32_t L = L0; L < NL; L++) {
       range_t r = vox_range(vx, &T, L, vox_size(vx, L) * 8.0f);
       int32_t n = r.n.x * r.n.y * r.n.z;
       if (n == 0 || (!vx->coarse_from_triangles && finer_holds_range(vx, L, r, 8))) continue;
@@ -234,9 +254,10 @@ int orc_vox_build(const orc_scene *s, orc_vox *vx) {
   memset(vx->rep, 0, (size_t)nb * 512u * 4u);
 
   /* voxBits + voxBitsBig (voxel.ts:492-534) */
-  for (uint32_t t = 0; t < s->ntris; t++) {
+  for (uint32_t i = 0; i < threads_of(s); i++) {
+    uint32_t L0, t = work_at(s, i, &L0);
     tri_t T = load_tri(s, t);
-    for (uint32_t L = 0; L < NL; L++) {
+    for (uint32_t L = L0; L < NL; L++) {
       range_t r = vox_range(vx, &T, L, vox_size(vx, L));
       int32_t n = r.n.x * r.n.y * r.n.z;
       if (n == 0 || (!vx->coarse_from_triangles && finer_built_range(vx, L, r))) continue;
@@ -328,7 +349,7 @@ int orc_vox_build(const orc_scene *s, orc_vox *vx) {
       i3 c = I(b.x * 8 + (int32_t)(bit & 7u), b.y * 8 + (int32_t)((bit >> 3) & 7u), b.z * 8 + (int32_t)(bit >> 6));
       v3 p = add(region_lo(vx, L), muls(adds(vi2f(c), 0.5f), vox_size(vx, L)));
       uint32_t rv = vx->rep[ptr * 512u + bit];
-      if (rv == 0u || rv > s->ntris) {   /* no representative (cannot happen for a set bit): no attributes */
+      if (rv == 0u || rv > key_limit(s)) {   /* no representative (cannot happen for a set bit): no attributes */
         for (int k = 0; k < 4; k++) vx->attr[ai * 4u + k] = 0u;
         vx->plane[ai] = 0.0f; vx->sunvis[ai] = 1.0f;
         continue;

@@ -87,9 +87,12 @@ struct gi_scene {
   uint32_t rigid_first = 0, rigid_per = 0, rigid_n = 0;
   SceneDev dev() const {
     SceneDev s;
-    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ndraw; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+    s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
+    s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
     return s;
   }
+  uint32_t ndraw = 0;   // triangles the rasters draw ([0, ndraw); gi_scene_set_draw_count), all by default
 };
 
 struct gi_vox {
@@ -99,6 +102,23 @@ struct gi_vox {
   bool updated = false;
   uint32_t hdr[64];
   uint64_t bytes = 0;
+  // world work items (gi_vox_set_world / gi_vox_set_items): instance offsets, chunk row lists, this frame's items
+  float4 *w_inst = nullptr;
+  uint32_t *w_lists = nullptr;
+  uint4 *w_items = nullptr;
+  uint32_t w_ninst = 0, w_nlists = 0, w_items_cap = 0, w_nitems = 0, w_threads = 0, w_stride = 0;
+  bool world = false;
+  uint64_t items_gen = 0;   // bumped by gi_vox_set_world / gi_vox_set_items: graphs captured before are stale
+  // the scene as the rebuild reads it: every row once, or this frame's work items
+  SceneDev build_scene() const {
+    SceneDev d = scene->dev();
+    d.ntris = scene->ntris;
+    if (world) {
+      d.items = w_items; d.lists = w_lists; d.inst = w_inst; d.nitems = w_nitems; d.threads = w_threads;
+      d.key_stride = w_stride; d.key_limit = w_ninst * w_stride;
+    }
+    return d;
+  }
 };
 
 struct gi_rc {
@@ -128,6 +148,7 @@ struct gi_rc {
   RcLaunch launch = {8u, 3u, 256u};   // gi_rc_tuning launch shapes
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
+  uint64_t graph_items_gen = 0;      // the voxel world's work items the graph was captured with
   float *shadow = nullptr;           // gi_rc_render_shadow: shadow_size^2 depths
   uint32_t shadow_size = 0;
   float4 *sm_rec = nullptr;          // its raster scratch, for up to sm_tris triangles
@@ -151,6 +172,7 @@ static void free_vox(gi_vox *v) {
   cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
   cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
   cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre); cudaFree(d.citem); cudaFree(d.look);
+  cudaFree(v->w_inst); cudaFree(v->w_lists); cudaFree(v->w_items);
 }
 static void free_rc(gi_rc *r) {
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; }
@@ -231,7 +253,7 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
   CK(cudaSetDevice(ctx->device), "gi_scene_upload: cudaSetDevice");
   gi_scene *s = new (std::nothrow) gi_scene;
   if (!s) return fail(GI_ERR_OOM, "gi_scene_upload: host allocation");
-  s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats;
+  s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats; s->ndraw = ntris;
   s->raster_cap = raster_list_cap(ntris);
   cudaError_t e = cudaSuccess;
   float4 *h4 = nullptr;
@@ -422,11 +444,84 @@ static int vox_build_sun(gi_vox *v, const float *frame, const float *shadow, uin
   CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_build: cudaSetDevice");
   VoxDev d = v->dev;
   d.sun_frame = frame; d.shadow = shadow; d.shadow_size = shadow ? size : 0u;
-  CK(gi_launch_vox_build(d, v->scene->dev(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
+  CK(gi_launch_vox_build(d, v->build_scene(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
   return GI_OK;
 }
 
 int gi_vox_build(gi_vox *v, void *stream) { return vox_build_sun(v, nullptr, nullptr, 0u, stream); }
+
+int gi_vox_set_world(gi_vox *v, const float *instances, uint32_t ninst, const uint32_t *lists, uint32_t nlists,
+                     uint32_t key_stride) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_set_world: NULL vox");
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_set_world: cudaSetDevice");
+  cudaFree(v->w_inst); cudaFree(v->w_lists); cudaFree(v->w_items);
+  v->w_inst = nullptr; v->w_lists = nullptr; v->w_items = nullptr;
+  v->world = false; v->w_ninst = v->w_nlists = v->w_items_cap = v->w_nitems = v->w_threads = v->w_stride = 0;
+  v->items_gen++;
+  if (ninst == 0) return GI_OK;   // back to every row once
+  if (!instances || (nlists && !lists)) return fail(GI_ERR_INVALID, "gi_vox_set_world: NULL argument");
+  if (ninst > 64) return fail(GI_ERR_INVALID, "gi_vox_set_world: %u instances (at most 64)", ninst);
+  if (instances[0] != 0.0f || instances[1] != 0.0f || instances[2] != 0.0f)
+    return fail(GI_ERR_INVALID, "gi_vox_set_world: instance 0 must be at the origin");
+  if (key_stride != v->scene->ntris)
+    return fail(GI_ERR_INVALID, "gi_vox_set_world: key stride %u, the scene has %u rows", key_stride, v->scene->ntris);
+  if ((uint64_t)ninst * key_stride >= (1ull << 32)) return fail(GI_ERR_INVALID, "gi_vox_set_world: triangle keys overflow");
+  for (uint32_t k = 0; k < nlists; k++)
+    if (lists[k] >= key_stride) return fail(GI_ERR_INVALID, "gi_vox_set_world: list word %u names row %u", k, lists[k]);
+  std::vector<float4> inst(ninst);
+  for (uint32_t i = 0; i < ninst; i++) inst[i] = make_float4(instances[3 * i], instances[3 * i + 1], instances[3 * i + 2], 0.0f);
+  cudaError_t e;
+  if ((e = dalloc(&v->w_inst, ninst)) || (e = dalloc(&v->w_lists, nlists ? nlists : 1u)) ||
+      (e = cudaMemcpy(v->w_inst, inst.data(), ninst * sizeof(float4), cudaMemcpyHostToDevice)) ||
+      (nlists && (e = cudaMemcpy(v->w_lists, lists, nlists * 4u, cudaMemcpyHostToDevice))))
+    return cuda_fail(e, "gi_vox_set_world");
+  v->w_ninst = ninst; v->w_nlists = nlists; v->w_stride = key_stride;
+  v->world = true;   // no items yet: the rebuild reads nothing until gi_vox_set_items
+  return GI_OK;
+}
+
+int gi_vox_set_items(gi_vox *v, const uint32_t *items, uint32_t nitems, uint32_t threads) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_set_items: NULL vox");
+  if (!v->world) return fail(GI_ERR_STATE, "gi_vox_set_items: no world (gi_vox_set_world)");
+  if (nitems && !items) return fail(GI_ERR_INVALID, "gi_vox_set_items: NULL items");
+  uint32_t expect = 0;
+  for (uint32_t k = 0; k < nitems; k++) {
+    const uint32_t *it = items + 4u * k;
+    if (it[0] != expect) return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u starts at thread %u, not %u", k, it[0], expect);
+    if (it[2] >= v->w_ninst) return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u instance %u", k, it[2]);
+    if (it[3] >= v->p.levels) return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u level %u", k, it[3]);
+    const uint32_t next = k + 1 < nitems ? items[4u * (k + 1)] : threads;
+    if (next < it[0]) return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u out of order", k);
+    const uint64_t count = next - it[0];
+    if (it[1] & 0x80000000u) {
+      if ((uint64_t)(it[1] & 0x7fffffffu) + count > v->w_stride) return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u past the rows", k);
+    } else if ((uint64_t)it[1] + count > v->w_nlists) {
+      return fail(GI_ERR_INVALID, "gi_vox_set_items: item %u past the lists", k);
+    }
+    expect = next;
+  }
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_set_items: cudaSetDevice");
+  if (nitems > v->w_items_cap) {
+    cudaFree(v->w_items);
+    v->w_items = nullptr;
+    v->w_items_cap = 0;
+    cudaError_t e = dalloc(&v->w_items, nitems);
+    if (e) return cuda_fail(e, "gi_vox_set_items");
+    v->w_items_cap = nitems;
+  }
+  if (nitems) CK(cudaMemcpy(v->w_items, items, nitems * sizeof(uint4), cudaMemcpyHostToDevice), "gi_vox_set_items: copy");
+  v->w_nitems = nitems;
+  v->w_threads = nitems ? threads : 0u;
+  v->items_gen++;
+  return GI_OK;
+}
+
+int gi_scene_set_draw_count(gi_scene *s, uint32_t count) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_set_draw_count: NULL scene");
+  if (count > s->ntris) return fail(GI_ERR_INVALID, "gi_scene_set_draw_count: %u of %u rows", count, s->ntris);
+  s->ndraw = count;
+  return GI_OK;
+}
 
 int gi_vox_build_sun(gi_vox *v, gi_rc *r, void *stream) {
   if (!r) return fail(GI_ERR_INVALID, "gi_vox_build_sun: NULL rc");
@@ -869,6 +964,7 @@ int gi_rc_graph_capture(gi_rc *r, gi_vox *v, void *stream) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture: instantiate"); }
   r->graph_vox = v;
+  r->graph_items_gen = v->items_gen;
   return GI_OK;
 }
 
@@ -899,12 +995,15 @@ int gi_rc_graph_capture_frame(gi_rc *r, gi_vox *v, gi_scene *sc, void *irr_out, 
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture_frame: instantiate"); }
   r->graph_vox = v;
+  r->graph_items_gen = v->items_gen;
   return GI_OK;
 }
 
 int gi_rc_graph_launch(gi_rc *r, void *stream) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_graph_launch: NULL rc");
   if (!r->graph) return fail(GI_ERR_STATE, "gi_rc_graph_launch: no graph captured");
+  if (r->graph_vox && r->graph_vox->items_gen != r->graph_items_gen)
+    return fail(GI_ERR_STATE, "gi_rc_graph_launch: the voxel world's work items changed since the capture; capture again");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_graph_launch: cudaSetDevice");
   CK(cudaGraphLaunch(r->graph, S(stream)), "gi_rc_graph_launch");
   r->timed = false;

@@ -161,6 +161,13 @@ struct SceneDev {
   const uint4 *tri;        // i0, i1, i2, material
   const gi_material *mats;
   uint32_t ntris, nverts, nmats, pad;
+  // World work items of the voxel build (world.ts, voxel.ts:270-288); items NULL: every row once, instance 0.
+  // items: (first thread, source, instance, first level), the source an offset into lists or 0x80000000 | first row;
+  // a triangle's key is instance * key_stride + row, moved by inst[instance]
+  const uint4 *items;
+  const uint32_t *lists;
+  const float4 *inst;
+  uint32_t nitems, threads, key_stride, key_limit;   // threads of the triangle passes; keys below key_limit
 };
 
 // Voxel world in device memory (struct of arrays; the reference packs the same data in one `vox` buffer,

@@ -143,6 +143,8 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   s.pos = reinterpret_cast<const float4 *>(pos4); s.nrm = reinterpret_cast<const float4 *>(nrm4);
   s.tri = reinterpret_cast<const uint4 *>(tri4); s.mats = mats;
   s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+  s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
+  s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
   e = gi_launch_vox_build(v, s, sms, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(GI_ERR_CUDA, "gi_vox_build_noalloc: launch: %s", cudaGetErrorString(e));
   return GI_OK;

@@ -20,13 +20,39 @@ namespace gi {
 
 struct Tri { f3 a, b, c; uint4 idx; };
 
-__device__ __forceinline__ Tri load_tri(const SceneDev &s, uint32_t t) {
+// loadTri (voxel.ts:270-276): the triangle of key = instance * key_stride + row, moved by the instance's offset
+__device__ __forceinline__ Tri load_tri(const SceneDev &s, uint32_t key) {
   Tri T;
-  T.idx = s.tri[t];
+  if (s.items) {
+    const uint32_t inst = key / s.key_stride;
+    T.idx = s.tri[key - inst * s.key_stride];
+    const float4 o4 = s.inst[inst];
+    const f3 o = mk(o4.x, o4.y, o4.z);
+    T.a = ld3(s.pos[T.idx.x]) + o;
+    T.b = ld3(s.pos[T.idx.y]) + o;
+    T.c = ld3(s.pos[T.idx.z]) + o;
+    return T;
+  }
+  T.idx = s.tri[key];
   T.a = ld3(s.pos[T.idx.x]);
   T.b = ld3(s.pos[T.idx.y]);
   T.c = ld3(s.pos[T.idx.z]);
   return T;
+}
+// workAt (voxel.ts:280-288): thread i of a triangle pass -> its key and its first level
+__device__ __forceinline__ uint32_t work_at(const SceneDev &s, uint32_t i, uint32_t &first) {
+  first = 0;
+  if (!s.items) return i;
+  uint32_t lo = 0, hi = s.nitems;
+  while (hi - lo > 1u) {
+    const uint32_t m = (lo + hi) >> 1;
+    if (s.items[m].x <= i) lo = m; else hi = m;
+  }
+  const uint4 b = s.items[lo];
+  const uint32_t j = i - b.x;
+  const uint32_t row = (b.y & 0x80000000u) ? (b.y & 0x7fffffffu) + j : s.lists[b.y + j];
+  first = b.w;
+  return b.z * s.key_stride + row;
 }
 
 struct Range { i3 lo, n; };
@@ -163,18 +189,19 @@ __global__ void k_clear(VoxDev v) {
 // are warp-aggregated.
 __global__ void __launch_bounds__(256, 4) k_mark_bricks(VoxDev v, SceneDev s) {
   grid_dep_wait();
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = t < s.ntris;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < s.threads;
+  uint32_t t = 0, L0 = 0;
   Tri T;
   T.a = T.b = T.c = mk(0.0f, 0.0f, 0.0f);
   T.idx = make_uint4(0u, 0u, 0u, 0u);
-  if (live) T = load_tri(s, t);
+  if (live) { t = work_at(s, i, L0); T = load_tri(s, t); }
   for (uint32_t L = 0; L < v.levels; L++) {
     bool big = false;
     Range r;
     r.lo = r.n = mki(0, 0, 0);
     int n = 0;
-    if (live) {
+    if (live && L >= L0) {
       r = vox_range(v, T, L, true);
       n = r.n.x * r.n.y * r.n.z;
       if (n != 0 && !finer_holds_range(v, L, r, 8)) big = n > 8;
@@ -334,19 +361,20 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
 // voxBits (voxel.ts:492-513)
 __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
   grid_dep_wait();
-  uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
-  bool live = t < s.ntris;
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  bool live = i < s.threads;
   uint32_t bo = v.hdr[2];
+  uint32_t t = 0, L0 = 0;
   Tri T;
   T.a = T.b = T.c = mk(0.0f, 0.0f, 0.0f);
   T.idx = make_uint4(0u, 0u, 0u, 0u);
-  if (live) T = load_tri(s, t);
+  if (live) { t = work_at(s, i, L0); T = load_tri(s, t); }
   for (uint32_t L = 0; L < v.levels; L++) {
     bool big = false;
     Range r;
     r.lo = r.n = mki(0, 0, 0);
     int n = 0;
-    if (live) {
+    if (live && L >= L0) {
       r = vox_range(v, T, L, false);
       n = r.n.x * r.n.y * r.n.z;
       bool skip = n == 0 || (bo == 0u && finer_holds_range(v, L, r, 1));
@@ -654,7 +682,7 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
     i3 c = mki(b.x * 8 + (int)(bit & 7u), b.y * 8 + (int)((bit >> 3) & 7u), b.z * 8 + (int)(bit >> 6));
     f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vox_size(v, L);
     uint32_t rv = v.rep[ptr * 512u + bit];
-    if (rv == 0u || rv > s.ntris) {   // no representative (cannot happen for a set bit): no attributes
+    if (rv == 0u || rv > s.key_limit) {   // no representative (cannot happen for a set bit): no attributes
       v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f;
       v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, p, vox_size(v, L), 0u, 0.0f) : 1.0f;
       continue;
@@ -699,7 +727,7 @@ cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_
   uint32_t per = v.G * v.G * v.G, nptr = v.levels * per;
   uint32_t persist = sm_count * v.blocks;   // blocks of 256 threads per SM for the grid-stride passes (default 8)
   GI_TRY(gi_launch(k_clear, min((nptr + 255u) / 256u + 1u, persist), 256, st, v));
-  uint32_t tb = (s.ntris + 255u) / 256u;
+  uint32_t tb = (s.threads + 255u) / 256u;   // threads of the triangle passes (the work items' triangles)
   if (tb) GI_TRY(gi_launch(k_mark_bricks, tb, 256, st, v, s));
   GI_TRY(gi_launch(k_mark_bricks_big, persist, 256, st, v, s));
   if (v.levels > 1) GI_TRY(gi_launch(k_mark_parents, min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, st, v));

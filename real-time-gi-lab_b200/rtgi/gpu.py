@@ -59,6 +59,10 @@ class SceneGpu:
                   _ptr(mats), len(mats), C.byref(h))
         self.handle = h
 
+    def set_draw_count(self, count: int) -> None:
+        """The rasters draw rows [0, count) (a world's clustered copies are voxelised only)."""
+        _lib.call("gi_scene_set_draw_count", self.handle, int(count))
+
     def update_vertices(self, first: int, pos: np.ndarray, nrm: np.ndarray, stream=None):
         pos = np.ascontiguousarray(pos, dtype=np.float32)
         nrm = np.ascontiguousarray(nrm, dtype=np.float32)
@@ -106,9 +110,28 @@ class VoxWorld:
         _lib.call("gi_vox_create", scene.handle, C.byref(p), C.byref(h))
         self.handle = h
 
+    def set_world(self, world) -> None:
+        """Worlds (rtgi.world.World, the scene made by with_world): the instances and chunk lists; from the next update
+        on the rebuild reads that frame's work items.  None: every row once."""
+        self.world = world
+        if world is None:
+            _lib.call("gi_vox_set_world", self.handle, None, 0, None, 0, 0)
+            return
+        inst = np.ascontiguousarray(np.asarray(world.instances, np.float64).astype(np.float32).reshape(-1))
+        lists = np.ascontiguousarray(world.lists(), np.uint32)
+        _lib.call("gi_vox_set_world", self.handle, _ptr(inst), len(world.instances), _ptr(lists) if lists.size else None,
+                  int(lists.size), int(world.rows))
+
     def update(self, eye) -> None:
+        """writeUniform (voxel.ts:868-892): the windows around eye and, for a world, this frame's work items."""
         e = (C.c_double * 3)(*[float(x) for x in eye])
         _lib.call("gi_vox_update", self.handle, e)
+        if getattr(self, "world", None) is not None:
+            from . import world as W
+            p = self.params
+            rec, threads = W.item_records(W.select_items(self.world, W.windows(float(p.v0), p.levels, p.G, eye)))
+            rec = np.ascontiguousarray(rec, np.uint32)
+            _lib.call("gi_vox_set_items", self.handle, _ptr(rec) if len(rec) else None, len(rec), threads)
 
     def encode(self, stream=None, sun_rc=None) -> None:
         """The rebuild; with sun_rc, voxSun from that rc's shadow map and frame (gi_vox_build_sun)."""

@@ -169,3 +169,94 @@ def test_colonnade_view_is_open():
     near = s.camera.near
     # reversed-Z infinite projection: view distance ~ near / depth
     assert np.median(near / depth[depth > 0]) > 2.0
+
+
+# ---- worlds: instances, chunks and work items (world.ts) -------------------------------------------------------------
+
+from rtgi import world as W
+
+ROOM_V = {"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 8192, "maxVoxels": 1 << 20}
+INSTANCES = [(0, 0, 0), (12, 0, 0), (-14, 0, 3), (0, 0, 26)]
+
+
+@pytest.fixture(scope="module")
+def room_world():
+    s = scenes.room_scene(0)
+    v = configs.vox_params(ROOM_V)
+    s2, w = W.with_world(s, INSTANCES, float(v.v0), v.levels)
+    return s, s2, w, v
+
+
+def test_chunks_partition_the_rows(room_world):
+    s, s2, w, v = room_world
+    rows = np.sort(np.concatenate([ch.full for ch in w.chunks]))
+    assert np.array_equal(rows, np.arange(s.triangle_count))
+    P = np.asarray(s.positions, np.float64)
+    for ch in w.chunks:
+        tri = s.tri[ch.full]
+        pts = P[tri[:, :3].reshape(-1)]
+        assert np.all(pts.min(0) - W.MOTION_MARGIN >= np.array(ch.lo) - 1e-9)
+        assert np.all(pts.max(0) + W.MOTION_MARGIN <= np.array(ch.hi) + 1e-9)
+        c = P[tri[:, :3]].mean(1)        # every centroid in the chunk's 8 m cell
+        assert len({tuple(np.floor(x / W.CHUNK).astype(int)) for x in c}) == 1
+        assert ch.lod[0] is ch.full      # lod0Cell 0: level 0 voxelises the full triangles
+
+
+def test_clustered_copies(room_world):
+    s, s2, w, v = room_world
+    T, V = s.triangle_count, s.positions.shape[0]
+    assert w.rows == s2.tri.shape[0] == T + len(w.lod_table)
+    assert s2.positions.shape[0] == V + w.lod_vertex_count
+    assert (w.lod_table[:, :3] >= V).all() and (w.lod_table[:, :3] < V + w.lod_vertex_count).all()
+    for ch in w.chunks:
+        for L in range(1, v.levels):
+            if len(ch.lod[L]):
+                assert (ch.lod[L] >= T).all() and (ch.lod[L] < w.rows).all()
+                # a clustered vertex lies in the cell of the vertices it replaces: within one cell of its triangle's
+                cell = v.v0 * 2 ** (L - 1)
+                src = s.tri[ch.full][:, :3].reshape(-1)
+                lo = s.positions[src].min(0) - cell
+                hi = s.positions[src].max(0) + cell
+                pts = s2.positions[s2.tri[ch.lod[L]][:, :3].reshape(-1)]
+                assert (pts >= lo - 1e-6).all() and (pts <= hi + 1e-6).all()
+
+
+def test_items_start_at_the_finest_window(room_world):
+    s, s2, w, v = room_world
+    wins = W.windows(float(v.v0), v.levels, v.G, s.camera.eye)
+    items = W.select_items(w, wins)
+    assert {it.inst for it in items} == {0, 1, 2, 3} or {it.inst for it in items} >= {0, 1}
+    for it in items:
+        ch = next(c for c, ch in enumerate(w.chunks) if w.list_off[c][it.start] == it.list)
+        o = w.instances[it.inst]
+        box = (np.add(w.chunks[ch].lo, o), np.add(w.chunks[ch].hi, o))
+        inside = [all(box[0][a] < wins[L][1][a] and box[1][a] > wins[L][0][a] for a in range(3)) for L in range(v.levels)]
+        assert inside[it.start] and not any(inside[:it.start])
+    rec, threads = W.item_records(items)
+    assert threads == sum(it.count for it in items) and rec[0, 0] == 0
+
+
+def test_single_instance_world_is_the_plain_build():
+    s = scenes.room_scene(0)
+    v = configs.vox_params(ROOM_V)
+    s1, w1 = W.with_world(s, [(0, 0, 0)], float(v.v0), v.levels)
+    eye = s.camera.eye
+    a = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, eye)
+    b = bind.vox_build(s1, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, eye, world=w1)
+    assert all(it.start == 0 for it in W.select_items(w1, W.windows(float(v.v0), v.levels, v.G, eye)))
+    for k in ("hdr", "ptr", "occ", "base", "code", "attr", "plane"):
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_instances_fill_the_coarse_levels(room_world):
+    s, s2, w, v = room_world
+    eye = s.camera.eye
+    a = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, eye)
+    b = bind.vox_build(s2, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, eye, world=w)
+    assert b["hdr"][8] == a["hdr"][8]          # level 0 holds instance 0 only
+    assert b["hdr"][9] > a["hdr"][9] and b["hdr"][10] > a["hdr"][10]
+
+
+def test_world_requires_instance_zero_at_the_origin():
+    with pytest.raises(ValueError):
+        W.with_world(scenes.room_scene(0), [(1, 0, 0)], 0.08, 3)
