@@ -139,8 +139,8 @@ def load(path: str = LIB_PATH):
     global _lib
     if _lib is not None:
         return _lib
-    if not os.path.exists(path) and os.path.exists(os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")):
-        build()
+    if path == LIB_PATH and os.path.exists(os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")):
+        build()   # only when missing or older than its sources (build.py checks)
     if not os.path.exists(path):
         raise ImportError(f"libgi_b200.so not found at {path}; build it with real-time-gi-lab_b200/build.py")
     lib = C.CDLL(path)

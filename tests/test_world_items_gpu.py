@@ -71,21 +71,21 @@ def test_single_instance_world_equals_plain_build(ctx):
     s = scenes.room_scene(0)
     v = configs.vox_params(ROOM_V)
     s1, w1 = W.with_world(s, [(0, 0, 0)], float(v.v0), v.levels)
-    sg = gpu.SceneGpu(ctx, s1)
-    vw = gpu.VoxWorld(sg, v)
+    sg0, sg1 = gpu.SceneGpu(ctx, s), gpu.SceneGpu(ctx, s1)   # s1 = s + the clustered rows (unused by instance 0)
+    v0, v1 = gpu.VoxWorld(sg0, v), gpu.VoxWorld(sg1, v)
     try:
-        vw.update(s.camera.eye)
-        vw.encode()
-        plain = vw.read_state()
-        vw.set_world(w1)
-        vw.update(s.camera.eye)
-        vw.encode()
-        world = vw.read_state()
+        v0.update(s.camera.eye)
+        v0.encode()
+        plain = v0.read_state()
+        v1.set_world(w1)
+        v1.update(s.camera.eye)
+        v1.encode()
+        world = v1.read_state()
         for k in STATE:
             assert np.array_equal(plain[k], world[k]), k
     finally:
-        vw.destroy()
-        sg.destroy()
+        for h in (v0, v1, sg0, sg1):
+            h.destroy()
 
 
 def test_items_are_checked_and_stale_graphs_refused(ctx):
