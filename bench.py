@@ -366,6 +366,58 @@ def whole_job_rate(units_per_rank: float, max_seconds: float, world: int) -> flo
     return world * units_per_rank / max_seconds
 
 
+def run_world_items(args, ctx, stream):
+    """Worlds (world.ts): the room scene placed at 121 instances 12 m apart (a 130 m town of 292k triangles) read by the
+    voxel rebuild as per-frame work items (chunks inside the windows, clustered copies at the coarse levels), against
+    the same geometry baked into one flat scene that the rebuild reads whole.  Device time of the rebuild alone."""
+    import dataclasses
+    import torch
+    from rtgi import configs, gpu, scenes, world as W
+    room = scenes.room_scene(0)
+    v = configs.vox_params({"v0": 0.08, "levels": 4, "G": 16, "maxBricks": 32768, "maxVoxels": 1 << 22})
+    inst = [(12.0 * i, 0.0, 12.0 * j) for j in range(-5, 6) for i in range(-5, 6)]
+    inst.remove((0.0, 0.0, 0.0))
+    inst.insert(0, (0.0, 0.0, 0.0))
+    s2, w = W.with_world(room, inst, float(v.v0), v.levels)
+    P = np.asarray(room.positions, np.float32)
+    flat_pos = np.concatenate([P + np.asarray(o, np.float32) for o in inst])
+    flat_tri = np.concatenate([room.tri.astype(np.int64) + np.array([k * P.shape[0]] * 3 + [0]) for k in range(len(inst))])
+    flat = dataclasses.replace(room, positions=flat_pos, normals=np.concatenate([room.normals] * len(inst)),
+                               tri=flat_tri.astype(np.uint32))
+    eye = room.camera.eye
+    out = {"instances": len(inst), "triangles_per_instance": room.triangle_count,
+           "clipmap": f"{v.levels} x {v.G * 8}^3 voxels from {v.v0} m"}
+    for name, scene, world in (("items", s2, w), ("flat", flat, None)):
+        sg = gpu.SceneGpu(ctx, scene)
+        vw = gpu.VoxWorld(sg, v)
+        if world is not None:
+            vw.set_world(world)
+        vw.update(eye)
+        with torch.cuda.stream(stream):
+            for _ in range(5):
+                vw.encode(stream)
+            ms = []
+            for _ in range(50):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                vw.encode(stream)
+                e1.record(stream)
+                ms.append((e0, e1))
+            torch.cuda.synchronize()
+        hdr = vw.read_counters(stream)["hdr"]
+        out[name] = {"rebuild_ms": statistics.median(a.elapsed_time(b) for a, b in ms),
+                     "bricks": int(hdr[0]), "voxels": int(hdr[1])}
+        if world is not None:
+            items = W.select_items(world, W.windows(float(v.v0), v.levels, v.G, eye))
+            out[name].update(items=len(items), threads=sum(it.count for it in items),
+                             items_per_level=[sum(1 for it in items if it.start == L) for L in range(v.levels)])
+        else:
+            out[name]["threads"] = scene.triangle_count
+        vw.destroy()
+        sg.destroy()
+    return out
+
+
 def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
     """World probes (gi_rc_create_world) on the workload's scene and clipmap: the config world-48-voxel-rc2-vrel-f32
     with the default capacities, solves replayed from one graph (the c0 history carries between them), L2 flushed
@@ -623,6 +675,7 @@ def run_ours(args, rank, world, local_rank):
     world_out = None
     if args.world:
         world_out = run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world)
+        world_out["items"] = run_world_items(args, ctx, stream)
 
     trace_ms = statistics.mean(pass_ms["giTrace"])
     alg = trace_algorithmic_bytes(rc.layout, hdr, v)

@@ -460,7 +460,7 @@ int gi_vox_set_world(gi_vox *v, const float *instances, uint32_t ninst, const ui
   v->items_gen++;
   if (ninst == 0) return GI_OK;   // back to every row once
   if (!instances || (nlists && !lists)) return fail(GI_ERR_INVALID, "gi_vox_set_world: NULL argument");
-  if (ninst > 64) return fail(GI_ERR_INVALID, "gi_vox_set_world: %u instances (at most 64)", ninst);
+  if (ninst > 1024) return fail(GI_ERR_INVALID, "gi_vox_set_world: %u instances (at most 1024, voxel.ts:742)", ninst);
   if (instances[0] != 0.0f || instances[1] != 0.0f || instances[2] != 0.0f)
     return fail(GI_ERR_INVALID, "gi_vox_set_world: instance 0 must be at the origin");
   if (key_stride != v->scene->ntris)

@@ -21,7 +21,8 @@ CHUNK = 8                 # chunk cells (m), world.ts:21
 DEFAULT_LOD0_CELL = 0.1   # world.ts:24
 LOD0_KEEP = 0.5           # world.ts:28
 MOTION_MARGIN = 0.15      # world.ts:30
-MAX_INSTANCES = 64
+MAX_INSTANCES = 1024   # voxel.ts:742
+MAX_ITEMS = 16384       # voxel.ts:742
 
 
 @dataclass
@@ -228,6 +229,8 @@ def select_items(world: World, wins) -> List[WorkItem]:
             n = len(ch.lod[s])
             if n > 0:
                 items.append(WorkItem(inst, s, world.list_off[c][s], 0, n))
+    if len(items) > MAX_ITEMS:
+        raise ValueError(f"too many work items: {len(items)}")
     return items
 
 
