@@ -599,6 +599,11 @@ __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks
   grid_dep_wait();
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t blk = chain_ticket(v.look);
+  // the grid covers the pool; only the parts that hold bricks take part in the scan (a part waits on smaller tickets
+  // only, so the parts past the bricks can leave at once)
+  const uint32_t used = max((nb + VOX_CHUNK - 1u) / VOX_CHUNK, 1u);
+  if (blk >= used) return;
+  nblocks = used;
   uint32_t b = blk * VOX_CHUNK + threadIdx.x;
   uint32_t c = b < nb ? brick_pop(v, b) : 0u;
   uint32_t tot;
