@@ -464,6 +464,27 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
         counts2 = rc.read_counts(stream)
     w_ms = sorted(a.elapsed_time(c) for a, c in zip(ws_, we_))
     w_total = max_over_ranks(sum(w_ms), dist, "cuda")
+    # the reference renderer's default transport: the same with multi-bounce on (rc.ts:90)
+    with torch.cuda.stream(stream):
+        rc.set_bounce(vw)
+        rc.set_timing(True)
+        b_pass = {k: [] for k in rc.PASSES}
+        for _ in range(max(5, args.warmup)):
+            rc.solve(vw, stream)
+            for k, x in rc.pass_times().items():
+                b_pass[k].append(x)
+        rc.set_timing(False)
+        rc.graph_capture(vw, stream)
+        bs, be = ([torch.cuda.Event(enable_timing=True) for _ in range(n_w)] for _ in range(2))
+        for k in range(n_w):
+            flush.zero_()
+            bs[k].record(stream)
+            rc.graph_launch(stream)
+            be[k].record(stream)
+        torch.cuda.synchronize()
+        rc.set_bounce(None)
+    b_ms = sorted(a.elapsed_time(c) for a, c in zip(bs, be))
+    b_total = max_over_ranks(sum(b_ms), dist, "cuda")
     lay = rc.layout
     probes = [int(min(counts[c], lay["casc"][c]["cap"])) for c in range(p.cascades)]
     rays = sum(n * lay["casc"][c]["res"] ** 2 for c, n in enumerate(probes))
@@ -475,6 +496,9 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
            "passes_ms": {k: statistics.median(x) for k, x in w_pass.items()},
            "probes": probes, "rays": rays, "dda_steps": int(counts[32:32 + p.cascades].sum()),
            "black_pixels_pct": 100.0 * float(counts2[72:80].sum()) / max(valid, 1),
+           "bounce": {"value": whole_job_rate(n_w, b_total / 1000.0, world), "unit": "solves/s",
+                      "ms_per_step": b_total / n_w, "p99_ms": b_ms[min(n_w - 1, int(math.ceil(0.99 * n_w)) - 1)],
+                      "passes_ms": {k: statistics.median(x) for k, x in b_pass.items()}},
            # voxel rebuild, then clear, registerPixels, compact + relocateVox per cascade, registerUp + linkParents per
            # cascade above c0, the trace, a merge per cascade, projectSH, the gather
            "gpu_launches_per_solve": (11 + (1 if v.levels > 1 else 0)) + 2 + 2 * p.cascades + 2 * (p.cascades - 1) + 1

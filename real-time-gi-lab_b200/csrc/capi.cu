@@ -872,9 +872,6 @@ int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_set_bounce: cudaSetDevice");
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
   cudaFree(r->bn.ray_out);
-  cudaFree(r->w.keys); cudaFree(r->w.slot_probe); cudaFree(r->w.parents); cudaFree(r->w.state); cudaFree(r->w.look);
-  cudaFree(r->w.hist_tab); cudaFree(r->w.hist_grid); cudaFree(r->w.hist_sh);
-  r->w = WorldDev{};
   r->bn = BounceDev{};
   r->bounce = false;
   r->bn_vox = nullptr;
@@ -922,6 +919,7 @@ int gi_rc_solve(gi_rc *r, gi_vox *v, void *stream) {
   if (!v->updated) return fail(GI_ERR_STATE, "gi_rc_solve: the voxel world was never updated");
   if (v->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_solve: voxel world on another device");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_solve: cudaSetDevice");
+  if (r->world && !r->w.keys) return fail(GI_ERR_STATE, "gi_rc_solve: the world-probe buffers are missing");
   r->dev.hits = r->debug_hits ? r->hits : nullptr;
   r->dev.rad_traced = r->debug_hits ? r->rad_traced : nullptr;
   CK(gi_launch_rc_solve(r->dev, v->dev, r->ctx->sm_count, S(stream), r->timing ? r->ev + 1 : nullptr, &r->launch,

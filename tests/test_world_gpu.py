@@ -136,3 +136,43 @@ def test_world_parity(ctx, case):
     assert (g[1]["irr"][..., :3] > 0).mean() > 0.2
     if case.name.endswith("overflow"):
         assert g[0]["counts"][8:13].sum() > 0, "the small capacities must overflow"
+
+
+def test_world_with_bounce(ctx):
+    """The reference renderer's default: world probes with voxel relocation AND multi-bounce (rc.ts:90), three solves
+    of the lit room with its shadow map; the injected irradiance carries one frame of history, the c0 SH another."""
+    room = scenes.room_scene(0)
+    case = _case("room-vrel-bounce", room, 200, 150, "world-32-voxel-rc2-vrel-f32", ROOM_VOX, [4096, 2048, 1024, 512, 256],
+                 shadow=512)
+    lay = configs.world_layout(case.rc)
+    sg = gpu.SceneGpu(ctx, case.scene)
+    vw = gpu.VoxWorld(sg, case.vox)
+    rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    v = case.vox
+    try:
+        rc.set_frame(case.frame)
+        rc.render_gbuffer(sg)
+        rc.render_shadow(sg, case.shadow)
+        vw.update(case.scene.camera.eye)
+        rc.set_bounce(vw)
+        depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width)
+        normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4).astype(np.float32)
+        st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+        bind.vox_sun(st, case.frame, rc.read_shadow())
+        ob = bind.Bounce(st)
+        state = bind.WorldState(lay)
+        prev = None
+        for f in range(3):
+            rc.solve(vw)
+            g_irr, g_counts = rc.read_irradiance(), rc.read_counts()
+            ob.frame(st, case.frame)
+            o = bind.world_solve(st, lay, state, case.frame, depth, normal)
+            _eq(g_counts, o["counts"], f"frame {f} counts")
+            _eq(g_irr, o["irr"], f"frame {f} irradiance")
+            if prev is not None:
+                assert not np.array_equal(g_irr, prev)
+            prev = g_irr
+        assert (prev[..., :3] > 0).mean() > 0.2
+    finally:
+        for h in (rc, vw, sg):
+            h.destroy()
