@@ -681,13 +681,14 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
       (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->sh_elem_bytes)) ||
       (e = cudaMalloc(&irr, npx * r->irr_elem_bytes)) || (e = dalloc(&counts, 96)) ||
-      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, dir_total))) {
+      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, 2u * dir_total))) {
     d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
     free_rc(r);
     delete r;
     return cuda_fail(e, "gi_rc_create");
   }
   d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
+  d.idirs = dirs + dir_total;
   d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
   // the merge's quad averages of a cascade whose resolution is twice the one below
   size_t avg_elems = 1;
@@ -721,7 +722,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
     delete r;
     return cuda_fail(e, "gi_rc_create: direction table");
   }
-  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 16 + ray_total * r->rad_elem_bytes +
+  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 32 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->sh_elem_bytes + npx * r->irr_elem_bytes + 96 * 4;
   if (wp) {
     WorldDev &w = r->w;

@@ -37,6 +37,7 @@ struct RcDev {
   ProbeDev *probes;
   uint32_t *plevel;        // per probe: voxLevel(s0, c) (rc.ts:210-213), computed once by setupScreen
   const float4 *dirs;      // per cascade, res^2 texel directions dirOf(di, res) (rc.ts:308), computed at creation
+  const float4 *idirs;     // the same directions' 1 / d (tiny components clamped as traceVox does), after dirs
   void *rad;               // rays_total atlas elements
   void *sh;                // probes of cascade 0 x 8 atlas elements
   void *irr;               // W*H: float4 (atlas F32) or rgba16f (uint2)

@@ -206,7 +206,8 @@ struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 template <class BS>
 __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
                                           f3 o, f3 d, float t0, float t1,
-                                          float tskip, uint32_t L, uint32_t cap, TraceOut &out, const BS &bs) {
+                                          float tskip, uint32_t L, uint32_t cap, TraceOut &out, const BS &bs,
+                                          const float4 *inv_pre = nullptr) {
   out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
   out.steps = 0;
   float vs = vox_size(v, L);
@@ -214,7 +215,13 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
   f3 lo = (vi2f(org(v, L)) * vs) * 8.0f;
   f3 hi = adds(lo, (float)G * vs * 8.0f);
   f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
-  f3 inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+  f3 inv;
+  if (inv_pre) {   // the direction's 1 / dd, tabulated with the directions (the same IEEE quotients)
+    const float4 q = __ldg(inv_pre);
+    inv = mk(q.x, q.y, q.z);
+  } else {
+    inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+  }
   f3 ta = (lo - o) * inv, tb = (hi - o) * inv;
   f3 tn = vmin(ta, tb), tf = vmax(ta, tb);
   float t = mx(mx(mx(tn.x, tn.y), tn.z), t0);
@@ -367,7 +374,7 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
     uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
     float vs = vox_size(v, Lv);
     trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out,
-              InjectedBounce{r.bn_inj});
+              InjectedBounce{r.bn_inj}, r.idirs + L.dir_off + di);
     traced = true;
   }
   Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -1004,6 +1011,9 @@ __global__ void k_init_dirs(RcDev r, float4 *dirs, uint32_t ndirs) {
   for (uint32_t k = 1; k < r.cascades; k++) if (i >= r.c[k].dir_off) c = k;
   f3 d = dir_of(i - r.c[c].dir_off, r.c[c].res);
   dirs[i] = make_float4(d.x, d.y, d.z, 0.0f);
+  // traceVox's 1 / d with tiny components clamped (voxel.ts:127), as trace_vox computes it
+  const f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
+  dirs[ndirs + i] = make_float4(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z, 0.0f);
 }
 
 __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {

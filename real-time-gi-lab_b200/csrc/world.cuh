@@ -418,7 +418,7 @@ __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uin
     const uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
     const float vs = vox_size(v, Lv);
     trace_vox(v, r.frame, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out,
-              InjectedBounce{r.bn_inj});
+              InjectedBounce{r.bn_inj}, r.idirs + L.dir_off + di);
     traced = true;
   }
   Atlas<A>::store(reinterpret_cast<T *>(r.rad), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
