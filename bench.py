@@ -499,10 +499,9 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
            "bounce": {"value": whole_job_rate(n_w, b_total / 1000.0, world), "unit": "solves/s",
                       "ms_per_step": b_total / n_w, "p99_ms": b_ms[min(n_w - 1, int(math.ceil(0.99 * n_w)) - 1)],
                       "passes_ms": {k: statistics.median(x) for k, x in b_pass.items()}},
-           # voxel rebuild, then clear, registerPixels, compact + relocateVox per cascade, registerUp + linkParents per
-           # cascade above c0, the trace, a merge per cascade, projectSH, the gather
-           "gpu_launches_per_solve": (11 + (1 if v.levels > 1 else 0)) + 2 + 2 * p.cascades + 2 * (p.cascades - 1) + 1
-                                     + p.cascades + 2}
+           # voxel rebuild, then clear, registerPixels, the paired compact / relocateVox / registerUp / linkParents
+           # launches (2N + 1 with voxel relocation), the trace, a merge per cascade, projectSH, the gather
+           "gpu_launches_per_solve": (11 + (1 if v.levels > 1 else 0)) + 2 + 2 * p.cascades + 1 + 1 + p.cascades + 2}
     rc.destroy()
     return out
 

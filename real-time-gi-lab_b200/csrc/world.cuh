@@ -210,11 +210,10 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
 }
 
 // registerUp (rc.ts:503-518): the grid points of cascade c with a non-zero trilinear weight at each probe of c - 1
-__global__ void __launch_bounds__(256) k_w_register_up(RcDev r, WorldDev w, uint32_t c) {
-  grid_dep_wait();
+__device__ __forceinline__ void w_register_up(const RcDev &r, const WorldDev &w, uint32_t c, uint32_t bid, uint32_t nblk) {
   const float *F = r.frame;
   const uint32_t n = w.state[8 + c - 1u] * 8u;   // one thread per (probe, corner)
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n; t += gridDim.x * blockDim.x) {
+  for (uint32_t t = bid * blockDim.x + threadIdx.x; t < n; t += nblk * blockDim.x) {
     const int4 g = r.probes[r.c[c - 1u].probe_off + (t >> 3)].grid;
     const i3 o = w_corner(t & 7u);
     if ((o.x > 0 && (g.x & 1) == 0) || (o.y > 0 && (g.y & 1) == 0) || (o.z > 0 && (g.z & 1) == 0)) continue;
@@ -248,8 +247,7 @@ __device__ __forceinline__ void w_compact_slot(const RcDev &r, const VoxDev &v, 
 
 // compact (rc.ts:520-537): a chained scan over the table's slots (W_COMPACT_SLOTS a block, 8 a thread) numbers the
 // keys in slot order; the last part publishes the count and the first ray of the next cascade.
-__global__ void __launch_bounds__(256) k_w_compact(RcDev r, VoxDev v, WorldDev w, uint32_t c) {
-  grid_dep_wait();
+__device__ __forceinline__ void w_compact(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t c) {
   const uint32_t size = w.hash_mask[c] + 1u, nblk = (size + W_COMPACT_SLOTS - 1u) / W_COMPACT_SLOTS, cap = w.cap[c];
   unsigned long long *look = w.look + w.look_off[c];
   const uint32_t blk = chain_ticket(look);
@@ -295,11 +293,11 @@ __global__ void __launch_bounds__(256) k_w_compact(RcDev r, VoxDev v, WorldDev w
 
 // relocateVox (rc.ts:414-470), one warp per probe: lane l reads cube cells l and l + 32; lane 0 takes the sums in the
 // serial order; lanes 0..16 test the 17 steps of the march.
-__global__ void __launch_bounds__(256) k_w_relocate_vox(RcDev r, VoxDev v, WorldDev w, uint32_t c) {
-  grid_dep_wait();
+__device__ __forceinline__ void w_relocate_vox(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t c, uint32_t bid,
+                                               uint32_t nblk) {
   const float *F = r.frame;
   const uint32_t lane = threadIdx.x & 31u, n = w.state[8 + c];
-  for (uint32_t pi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pi < n; pi += (gridDim.x * blockDim.x) >> 5) {
+  for (uint32_t pi = (bid * blockDim.x + threadIdx.x) >> 5; pi < n; pi += (nblk * blockDim.x) >> 5) {
     ProbeDev *prp = &r.probes[r.c[c].probe_off + pi];
     const int4 g = prp->grid;
     const int lod = g.w;
@@ -372,11 +370,11 @@ __global__ void __launch_bounds__(256) k_w_relocate_vox(RcDev r, VoxDev v, World
 
 // linkParents (rc.ts:541-567) of cascade c, one warp per probe: parent k on lanes 4k..4k+3, which share its segment's
 // samples (hidden parents are not merged, relocate 'voxel' only)
-__global__ void __launch_bounds__(256) k_w_link_parents(RcDev r, VoxDev v, WorldDev w, uint32_t c) {
-  grid_dep_wait();
+__device__ __forceinline__ void w_link_parents(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t c, uint32_t bid,
+                                               uint32_t nblk) {
   const float *F = r.frame;
   const uint32_t lane = threadIdx.x & 31u, k = lane >> 2, j = lane & 3u, n = w.state[8 + c];
-  for (uint32_t pi = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; pi < n; pi += (gridDim.x * blockDim.x) >> 5) {
+  for (uint32_t pi = (bid * blockDim.x + threadIdx.x) >> 5; pi < n; pi += (nblk * blockDim.x) >> 5) {
     const ProbeDev pr = r.probes[r.c[c].probe_off + pi];
     uint32_t q = W_NONE;
     if (j == 0u) {
@@ -398,6 +396,27 @@ __global__ void __launch_bounds__(256) k_w_link_parents(RcDev r, VoxDev v, World
     const uint32_t hm = __ballot_sync(0xffffffffu, hid);
     if (j == 0u) w.parents[(size_t)(r.c[c].probe_off + pi) * 8u + k] = ((hm >> (lane & ~3u)) & 0xFu) ? W_NONE : q;
   }
+}
+
+// giBuild's steps after registerPixels, two to a launch where they are independent (the launch's blocks split between
+// them): compact of cascade c, relocateVox and registerUp (both need only the compaction before them), linkParents
+// (needs both cascades' probes in place).  A task's blocks see the task's own block index and count.
+enum { W_NONE_TASK = 0, W_COMPACT = 1, W_RELOCATE = 2, W_REGISTER_UP = 3, W_LINK = 4 };
+__device__ __forceinline__ void w_task(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t task, uint32_t c,
+                                       uint32_t bid, uint32_t nblk) {
+  switch (task) {
+    case W_COMPACT: w_compact(r, v, w, c); break;
+    case W_RELOCATE: w_relocate_vox(r, v, w, c, bid, nblk); break;
+    case W_REGISTER_UP: w_register_up(r, w, c, bid, nblk); break;
+    case W_LINK: w_link_parents(r, v, w, c, bid, nblk); break;
+    default: break;
+  }
+}
+__global__ void __launch_bounds__(256) k_w_build(RcDev r, VoxDev v, WorldDev w, uint32_t ta, uint32_t ca, uint32_t na,
+                                                 uint32_t tb, uint32_t cb, uint32_t nb) {
+  grid_dep_wait();
+  if (blockIdx.x < na) w_task(r, v, w, ta, ca, blockIdx.x, na);
+  else w_task(r, v, w, tb, cb, blockIdx.x - na, nb);
 }
 
 // trace (rc.ts:600-622) of ray (pi, di) of a world probe of cascade c into atlas element i
@@ -699,12 +718,28 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
   const uint32_t clear_n = max(max(w.hash_total, w.look_total), max(w.hist_h, 96u));
   GI_TRY(gi_launch(k_w_clear, blocks(clear_n), 256, st, r, w));
   GI_TRY(gi_launch(k_w_register_pixels, (r.width * r.height + 255u) / 256u, 256, st, r, w));
+  // blocks of each task (compact: one per 2048 slots; the others grid-stride over the probes' warps or threads)
+  auto nb_compact = [&](uint32_t c) { return (w.hash_mask[c] + W_COMPACT_SLOTS) / W_COMPACT_SLOTS; };
+  auto nb_warps = [&](uint32_t c) { return blocks((uint64_t)w.cap[c] * 32u); };
+  auto nb_up = [&](uint32_t c) { return blocks((uint64_t)w.cap[c - 1u] * 8u); };
+  auto pair = [&](uint32_t ta, uint32_t ca, uint32_t na, uint32_t tb, uint32_t cb, uint32_t nb) {
+    return gi_launch(k_w_build, na + nb, 256, st, r, v, w, ta, ca, na, tb, cb, nb);
+  };
+  const bool vrel = w.relocate == 2u;
+  // compact(c) waits on registerUp(c); relocateVox(c) and registerUp(c + 1) wait on compact(c) only; linkParents(c - 1)
+  // waits on compact(c) and on relocateVox(c - 1) and (c); so each launch pairs two steps that share their inputs
+  GI_TRY(pair(W_COMPACT, 0, nb_compact(0), W_NONE_TASK, 0, 0));
   for (uint32_t c = 0; c < N; c++) {
-    if (c > 0) GI_TRY(gi_launch(k_w_register_up, blocks((uint64_t)w.cap[c - 1u] * 8u), 256, st, r, w, c));
-    GI_TRY(gi_launch(k_w_compact, (w.hash_mask[c] + W_COMPACT_SLOTS) / W_COMPACT_SLOTS, 256, st, r, v, w, c));
-    if (w.relocate == 2u) GI_TRY(gi_launch(k_w_relocate_vox, blocks((uint64_t)w.cap[c] * 32u), 256, st, r, v, w, c));
-    if (c > 0) GI_TRY(gi_launch(k_w_link_parents, blocks((uint64_t)w.cap[c - 1u] * 32u), 256, st, r, v, w, c - 1u));
+    const bool up = c + 1u < N;
+    if (vrel) {
+      GI_TRY(pair(W_RELOCATE, c, nb_warps(c), up ? W_REGISTER_UP : W_NONE_TASK, c + 1u, up ? nb_up(c + 1u) : 0u));
+      if (up) GI_TRY(pair(W_COMPACT, c + 1u, nb_compact(c + 1u), c >= 1u ? W_LINK : W_NONE_TASK, c - 1u, c >= 1u ? nb_warps(c - 1u) : 0u));
+    } else {
+      if (up) GI_TRY(pair(W_REGISTER_UP, c + 1u, nb_up(c + 1u), c >= 1u ? W_LINK : W_NONE_TASK, c - 1u, c >= 1u ? nb_warps(c - 1u) : 0u));
+      if (up) GI_TRY(pair(W_COMPACT, c + 1u, nb_compact(c + 1u), W_NONE_TASK, 0, 0));
+    }
   }
+  if (N >= 2) GI_TRY(pair(W_LINK, N - 2u, nb_warps(N - 2u), W_NONE_TASK, 0, 0));
   if (ev) cudaEventRecord(ev[1], st);
   if (bn) GI_TRY(launch_bounce(*bn, v, r.frame, r.unorm8, sm_count, st));
   const uint32_t tb = sm_count * (ls ? ls->trace_blocks : 8u);
