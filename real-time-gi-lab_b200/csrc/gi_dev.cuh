@@ -327,6 +327,21 @@ __device__ __forceinline__ f3 dir_of(uint32_t di, uint32_t res) {
   return normalize3(n);
 }
 
+// Index of the r-th set bit (from 0) of w, r < popc(w): halves of the word selected by their popcounts, branch-free
+// (the same index as clearing the lowest set bit r times)
+__device__ __forceinline__ uint32_t nth_set_bit(uint32_t w, uint32_t r) {
+  uint32_t pos = 0;
+#pragma unroll
+  for (uint32_t s = 16; s >= 1; s >>= 1) {
+    const uint32_t c = __popc(w & ((1u << s) - 1u));
+    const bool up = r >= c;
+    r -= up ? c : 0u;
+    w >>= up ? s : 0u;
+    pos += up ? s : 0u;
+  }
+  return pos;
+}
+
 // Warp-aggregated atomicAdd: one atomic per distinct address among the active lanes would need a match; the lists
 // and counters here use one address per call, so the active lanes share it.
 __device__ __forceinline__ uint32_t warp_append(uint32_t *counter, bool want) {

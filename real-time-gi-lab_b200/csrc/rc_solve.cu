@@ -868,8 +868,7 @@ __global__ void __launch_bounds__(256) k_bn_inject(BounceDev b, VoxDev v) {
         const uint32_t pc = __popc(ws4[j]);
         if (r < pc && bit == 0u) {
           uint32_t wd = ws4[j];
-          for (uint32_t k = 0; k < r; k++) wd &= wd - 1u;
-          bit = (uint32_t)(q * 4 + j) * 32u + (uint32_t)(__ffs(wd) - 1) + 1u;
+          bit = (uint32_t)(q * 4 + j) * 32u + nth_set_bit(wd, r) + 1u;
         }
         if (bit == 0u) r -= pc;
       }

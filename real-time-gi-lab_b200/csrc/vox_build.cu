@@ -674,8 +674,7 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
         uint32_t pc = __popc(ws[j]);
         if (r < pc && bit == 0u) {
           uint32_t wd = ws[j];
-          for (uint32_t k = 0; k < r; k++) wd &= wd - 1u;
-          bit = (uint32_t)(q * 4 + j) * 32u + (uint32_t)(__ffs(wd) - 1) + 1u;   // + 1: found
+          bit = (uint32_t)(q * 4 + j) * 32u + nth_set_bit(wd, r) + 1u;   // + 1: found
         }
         if (bit == 0u) r -= pc;
       }
