@@ -119,6 +119,9 @@ int gi_scene_update_vertices(gi_scene *scene, uint32_t first, uint32_t count, co
 /* The rasters (G-buffer, shadow map) draw rows [0, count); rows past it are voxelised only (a world's clustered
  * copies, world.ts:20-24).  All rows by default. */
 int gi_scene_set_draw_count(gi_scene *scene, uint32_t count);
+/* The rasters draw those rows at n instance offsets (3 floats each, instance 0 at the origin; n <= 1: once), drawn
+ * triangle i * count + row for instance i (the instanced draws of a world, world.ts:4-6). */
+int gi_scene_set_draw_instances(gi_scene *scene, const float *offsets, uint32_t n);
 int gi_scene_destroy(gi_scene *scene);
 
 /* ---- voxel world (voxel.ts VoxWorld) ------------------------------------------------------------------------------ */

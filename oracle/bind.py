@@ -77,7 +77,8 @@ class OrcScene(C.Structure):
     _fields_ = [("pos", C.c_void_p), ("nrm", C.c_void_p), ("nverts", C.c_uint32), ("tri", C.c_void_p),
                 ("ntris", C.c_uint32), ("mats", C.c_void_p), ("nmats", C.c_uint32),
                 ("items", C.c_void_p), ("nitems", C.c_uint32), ("threads", C.c_uint32), ("key_stride", C.c_uint32),
-                ("ninst", C.c_uint32), ("lists", C.c_void_p), ("inst", C.c_void_p)]
+                ("ninst", C.c_uint32), ("lists", C.c_void_p), ("inst", C.c_void_p),
+                ("ndraw", C.c_uint32), ("draw_ninst", C.c_uint32), ("draw_inst", C.c_void_p)]
 
 
 class OrcVox(C.Structure):
@@ -261,8 +262,21 @@ def merge_gather_f64(lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np
     return irr
 
 
-def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int):
+def _drawn(s, keep, ndraw, draw_instances):
+    """The rasters' drawn rows and instances (instance 0 at the origin)."""
+    s.ndraw = int(ndraw)
+    if draw_instances is not None and len(draw_instances) > 1:
+        inst = np.zeros((len(draw_instances), 4), np.float32)
+        inst[:, :3] = np.asarray(draw_instances, np.float64).astype(np.float32)
+        s.draw_inst, s.draw_ninst = _p(inst), len(draw_instances)
+        keep = keep + (inst,)
+    return keep
+
+
+def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int, ndraw: int = 0, draw_instances=None):
+    """The G-buffer of rows [0, ndraw) (0: every row) at every draw instance."""
     s, keep = _scene_struct(scene)
+    keep = _drawn(s, keep, ndraw, draw_instances)
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     depth = np.zeros((H, W), np.float32)
     normal = np.zeros((H, W, 4), np.float32)
@@ -273,9 +287,10 @@ def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int):
     return depth, normal, tri
 
 
-def shadow_render(scene, frame: np.ndarray, S: int) -> np.ndarray:
+def shadow_render(scene, frame: np.ndarray, S: int, ndraw: int = 0, draw_instances=None) -> np.ndarray:
     """The sun shadow map (S x S depths, 1 = nothing drawn) from the frame's lightViewProj."""
     s, keep = _scene_struct(scene)
+    keep = _drawn(s, keep, ndraw, draw_instances)
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     out = np.zeros((S, S), np.float32)
     lib().orc_shadow_render(C.byref(s), _p(frame), S, _p(out))

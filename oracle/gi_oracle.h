@@ -62,6 +62,10 @@ typedef struct {
   uint32_t nitems, threads, key_stride, ninst;
   const uint32_t *lists;
   const float *inst;
+  /* The rasters (G-buffer, shadow map): rows [0, ndraw) at draw_ninst instances (4 floats each, draw_inst; NULL:
+   * one instance at the origin), drawn triangle i * ndraw + row; ndraw 0: every row */
+  uint32_t ndraw, draw_ninst;
+  const float *draw_inst;
 } orc_scene;
 
 /* Voxel world state, laid out exactly as the CUDA path lays it out in device memory (struct of arrays). */

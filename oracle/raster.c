@@ -85,9 +85,14 @@ int orc_raster_gbuffer(const orc_scene *s, const float *F, uint32_t W, uint32_t 
   float near = F[F_EYE + 3];
   for (uint32_t y = 0; y < H; y++)
     for (uint32_t x = 0; x < W; x++) dirs[(size_t)y * W + x] = sub(world_at(F, (int32_t)x, (int32_t)y, 1.0f), eye);
-  for (uint32_t t = 0; t < s->ntris; t++) {
-    const uint32_t *i = s->tri + 4u * t;
+  const uint32_t nd = s->ndraw ? s->ndraw : s->ntris, ni = s->draw_inst ? s->draw_ninst : 1u;
+  for (uint32_t t = 0; t < nd * ni; t++) {
+    const uint32_t *i = s->tri + 4u * (t % nd);
     v3 p[3] = {fromf(s->pos + 3u * i[0]), fromf(s->pos + 3u * i[1]), fromf(s->pos + 3u * i[2])};
+    if (s->draw_inst) {
+      v3 o = fromf(s->draw_inst + 4u * (t / nd));
+      p[0] = add(p[0], o); p[1] = add(p[1], o); p[2] = add(p[2], o);
+    }
     int32_t box[4];
     if (!screen_box(F, W, H, p, box)) continue;
     for (int32_t y = box[2]; y <= box[3]; y++)
@@ -112,8 +117,12 @@ int orc_raster_gbuffer(const orc_scene *s, const float *F, uint32_t W, uint32_t 
     uint32_t t = 0xffffffffu - (uint32_t)(key[q] & 0xffffffffu);
     depth_out[q] = fbits((uint32_t)(key[q] >> 32));
     if (tri_out) tri_out[q] = t;
-    const uint32_t *i = s->tri + 4u * t;
+    const uint32_t *i = s->tri + 4u * (t % nd);
     v3 a = fromf(s->pos + 3u * i[0]), b = fromf(s->pos + 3u * i[1]), c = fromf(s->pos + 3u * i[2]);
+    if (s->draw_inst) {
+      v3 o = fromf(s->draw_inst + 4u * (t / nd));
+      a = add(a, o); b = add(b, o); c = add(c, o);
+    }
     float tt = 0, uu = 0, vv = 0;
     ray_tri(eye, dirs[q], a, b, c, &tt, &uu, &vv);
     v3 n0 = fromf(s->nrm + 3u * i[0]), n1 = fromf(s->nrm + 3u * i[1]), n2 = fromf(s->nrm + 3u * i[2]);

@@ -40,13 +40,17 @@ int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float 
   const float *m = frame + F_LVP;
   for (size_t i = 0; i < (size_t)S * S; i++) map[i] = 1.0f;
   const float inv = 1.0f / (float)S, fS = (float)S;
-  for (uint32_t t = 0; t < s->ntris; t++) {
-    const uint32_t *idx = &s->tri[4u * t];
+  const uint32_t nd = s->ndraw ? s->ndraw : s->ntris, ni = s->draw_inst ? s->draw_ninst : 1u;
+  for (uint32_t t = 0; t < nd * ni; t++) {
+    const uint32_t *idx = &s->tri[4u * (t % nd)];
     const orc_material *mt = &s->mats[idx[3]];
     if ((mt->flags & 1u) != 0u && mt->base_color[3] < mt->alpha_cutoff) continue;   /* every fragment discarded */
-    v3 c0 = light_clip(m, fromf(&s->pos[3u * idx[0]]));
-    v3 c1 = light_clip(m, fromf(&s->pos[3u * idx[1]]));
-    v3 c2 = light_clip(m, fromf(&s->pos[3u * idx[2]]));
+    v3 o = s->draw_inst ? fromf(s->draw_inst + 4u * (t / nd)) : V(0.0f, 0.0f, 0.0f);
+    v3 pa = fromf(&s->pos[3u * idx[0]]), pb = fromf(&s->pos[3u * idx[1]]), pc = fromf(&s->pos[3u * idx[2]]);
+    if (s->draw_inst) { pa = add(pa, o); pb = add(pb, o); pc = add(pc, o); }
+    v3 c0 = light_clip(m, pa);
+    v3 c1 = light_clip(m, pb);
+    v3 c2 = light_clip(m, pc);
     float det = (c1.x - c0.x) * (c2.y - c0.y) - (c2.x - c0.x) * (c1.y - c0.y);
     if (!(det != 0.0f)) continue;
     float dzx = ((c1.z - c0.z) * (c2.y - c0.y) - (c2.z - c0.z) * (c1.y - c0.y)) / det;

@@ -87,12 +87,22 @@ struct gi_scene {
   uint32_t rigid_first = 0, rigid_per = 0, rigid_n = 0;
   SceneDev dev() const {
     SceneDev s;
-    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ndraw; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
     s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
     s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
     return s;
   }
-  uint32_t ndraw = 0;   // triangles the rasters draw ([0, ndraw); gi_scene_set_draw_count), all by default
+  // the scene as the rasters draw it: rows [0, ndraw) at every draw instance, triangle i * ndraw + row of instance i
+  SceneDev raster_dev() const {
+    SceneDev s = dev();
+    s.ntris = ndraw * draw_ninst;
+    if (draw_ninst > 1) { s.inst = draw_inst; s.key_stride = ndraw; }
+    return s;
+  }
+  uint32_t ndraw = 0;          // rows the rasters draw ([0, ndraw); gi_scene_set_draw_count), all by default
+  float4 *draw_inst = nullptr; // offsets of the drawn instances (gi_scene_set_draw_instances), instance 0 at the origin
+  uint32_t draw_ninst = 1;
+  uint32_t raster_tris = 0;    // triangles the raster scratch holds
 };
 
 struct gi_vox {
@@ -165,7 +175,7 @@ static void free_scene(gi_scene *s) {
   cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
   cudaFree(s->raster_rec); cudaFree(s->raster_ntile); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
   cudaFree(s->raster_counter); cudaFree(s->raster_list); cudaFree(s->raster_over); cudaFree(s->stage);
-  cudaFree(s->rigid_rest); cudaFree(s->rigid_m);
+  cudaFree(s->rigid_rest); cudaFree(s->rigid_m); cudaFree(s->draw_inst);
 }
 static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
@@ -253,7 +263,7 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
   CK(cudaSetDevice(ctx->device), "gi_scene_upload: cudaSetDevice");
   gi_scene *s = new (std::nothrow) gi_scene;
   if (!s) return fail(GI_ERR_OOM, "gi_scene_upload: host allocation");
-  s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats; s->ndraw = ntris;
+  s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats; s->ndraw = ntris; s->raster_tris = ntris;
   s->raster_cap = raster_list_cap(ntris);
   cudaError_t e = cudaSuccess;
   float4 *h4 = nullptr;
@@ -516,10 +526,64 @@ int gi_vox_set_items(gi_vox *v, const uint32_t *items, uint32_t nitems, uint32_t
   return GI_OK;
 }
 
+// The raster scratch for n drawn triangles (grown, never shrunk)
+static int ensure_raster_scratch(gi_scene *s, uint64_t n, const char *what) {
+  if (n >= (1ull << 31)) return fail(GI_ERR_INVALID, "%s: %llu drawn triangles", what, (unsigned long long)n);
+  if (n <= s->raster_tris) return GI_OK;
+  CK(cudaSetDevice(s->ctx->device), what);
+  float4 *rec = nullptr;
+  uint32_t *ntile = nullptr, *pre = nullptr, *sums = nullptr, *over = nullptr, *list = nullptr;
+  const uint32_t cap = raster_list_cap((uint32_t)n);
+  cudaError_t e;
+  if ((e = dalloc(&rec, (size_t)3u * n)) || (e = dalloc(&ntile, n)) || (e = dalloc(&pre, n)) ||
+      (e = dalloc(&sums, n / 256u + 1u)) || (e = dalloc(&over, n)) ||
+      (cap > s->raster_cap && (e = dalloc(&list, cap)))) {
+    cudaFree(rec); cudaFree(ntile); cudaFree(pre); cudaFree(sums); cudaFree(over); cudaFree(list);
+    return cuda_fail(e, what);
+  }
+  cudaFree(s->raster_rec); cudaFree(s->raster_ntile); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
+  cudaFree(s->raster_over);
+  s->raster_rec = rec; s->raster_ntile = ntile; s->raster_pre = pre; s->raster_sums = sums; s->raster_over = over;
+  if (list) { cudaFree(s->raster_list); s->raster_list = list; s->raster_cap = cap; }
+  s->raster_tris = (uint32_t)n;
+  return GI_OK;
+}
+
 int gi_scene_set_draw_count(gi_scene *s, uint32_t count) {
   if (!s) return fail(GI_ERR_INVALID, "gi_scene_set_draw_count: NULL scene");
   if (count > s->ntris) return fail(GI_ERR_INVALID, "gi_scene_set_draw_count: %u of %u rows", count, s->ntris);
+  int st = ensure_raster_scratch(s, (uint64_t)count * s->draw_ninst, "gi_scene_set_draw_count");
+  if (st) return st;
   s->ndraw = count;
+  return GI_OK;
+}
+
+int gi_scene_set_draw_instances(gi_scene *s, const float *offsets, uint32_t n) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_set_draw_instances: NULL scene");
+  if (n > 1024) return fail(GI_ERR_INVALID, "gi_scene_set_draw_instances: %u instances (at most 1024)", n);
+  if (n > 1 && !offsets) return fail(GI_ERR_INVALID, "gi_scene_set_draw_instances: NULL offsets");
+  if (n > 1 && (offsets[0] != 0.0f || offsets[1] != 0.0f || offsets[2] != 0.0f))
+    return fail(GI_ERR_INVALID, "gi_scene_set_draw_instances: instance 0 must be at the origin");
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_set_draw_instances: cudaSetDevice");
+  if (n <= 1) {
+    cudaFree(s->draw_inst);
+    s->draw_inst = nullptr;
+    s->draw_ninst = 1;
+    return GI_OK;
+  }
+  int st = ensure_raster_scratch(s, (uint64_t)s->ndraw * n, "gi_scene_set_draw_instances");
+  if (st) return st;
+  std::vector<float4> h(n);
+  for (uint32_t i = 0; i < n; i++) h[i] = make_float4(offsets[3 * i], offsets[3 * i + 1], offsets[3 * i + 2], 0.0f);
+  float4 *d = nullptr;
+  cudaError_t e;
+  if ((e = dalloc(&d, n)) || (e = cudaMemcpy(d, h.data(), n * sizeof(float4), cudaMemcpyHostToDevice))) {
+    cudaFree(d);
+    return cuda_fail(e, "gi_scene_set_draw_instances");
+  }
+  cudaFree(s->draw_inst);
+  s->draw_inst = d;
+  s->draw_ninst = n;
   return GI_OK;
 }
 
@@ -808,7 +872,7 @@ int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   rd.rec = s->raster_rec; rd.ntile = s->raster_ntile; rd.pre = s->raster_pre; rd.sums = s->raster_sums;
   rd.counter = s->raster_counter; rd.list = s->raster_list; rd.over = s->raster_over;
   rd.tile_cnt = r->tile_cnt; rd.tile_fill = r->tile_fill; rd.list_cap = s->raster_cap; rd.ntiles = r->ntiles;
-  CK(gi_launch_gbuffer(s->dev(), r->frame, r->W, r->H, r->depth, r->normal, rd, r->ctx->sm_count, S(stream)),
+  CK(gi_launch_gbuffer(s->raster_dev(), r->frame, r->W, r->H, r->depth, r->normal, rd, r->ctx->sm_count, S(stream)),
      "gi_rc_render_gbuffer: launch");
   r->gbuf_set = true;
   return GI_OK;
@@ -834,7 +898,7 @@ int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
     if ((e = dalloc(&r->shadow, (size_t)size * size))) return cuda_fail(e, "gi_rc_render_shadow");
     r->shadow_size = size;
   }
-  uint32_t nt = s->ntris;
+  uint32_t nt = s->ndraw * s->draw_ninst;   // the drawn triangles (ensure_raster_scratch bounds the product)
   if (nt > r->sm_tris || !r->sm_counter) {
     cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
     r->sm_rec = nullptr; r->sm_pre = r->sm_sums = r->sm_counter = nullptr; r->sm_tris = 0;
@@ -846,7 +910,7 @@ int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
   }
   ShadowRaster sr;
   sr.map = r->shadow; sr.rec = r->sm_rec; sr.pre = r->sm_pre; sr.sums = r->sm_sums; sr.counter = r->sm_counter;
-  CK(gi_launch_shadow(s->dev(), r->frame, size, sr, r->ctx->sm_count, S(stream)), "gi_rc_render_shadow: launch");
+  CK(gi_launch_shadow(s->raster_dev(), r->frame, size, sr, r->ctx->sm_count, S(stream)), "gi_rc_render_shadow: launch");
   return GI_OK;
 }
 

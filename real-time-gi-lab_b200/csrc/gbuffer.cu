@@ -129,9 +129,11 @@ __global__ void __launch_bounds__(256) k_rs_setup(SceneDev s, const float *__res
   for (uint32_t i = t; i <= rd.ntiles; i += gridDim.x * blockDim.x) rd.tile_cnt[i] = 0u;   // counted by k_rs_bin
   uint32_t nt = 0;
   if (t < s.ntris) {
-    uint4 idx = s.tri[t];
+    f3 off;
+    uint4 idx = drawn_tri(s, t, off);
     f3 p[3];
     p[0] = ld3(s.pos[idx.x]); p[1] = ld3(s.pos[idx.y]); p[2] = ld3(s.pos[idx.z]);
+    if (s.inst) { p[0] = p[0] + off; p[1] = p[1] + off; p[2] = p[2] + off; }
     int box[4];
     float min_w;
     if (screen_box(F, W, H, p, box, min_w)) {
@@ -324,7 +326,8 @@ __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__res
   f3 a = mk(a4.x, a4.y, a4.z), e1 = mk(e14.x, e14.y, e14.z), e2 = mk(e24.x, e24.y, e24.z);
   float tt = 0.0f, uu = 0.0f, vv = 0.0f;
   ray_tri(eye, dir, a, e1, e2, tt, uu, vv);
-  uint4 idx = s.tri[t];
+  f3 off;
+  uint4 idx = drawn_tri(s, t, off);
   f3 n0 = ld3(s.nrm[idx.x]), n1 = ld3(s.nrm[idx.y]), n2 = ld3(s.nrm[idx.z]);
   f3 nn = (n0 * (1.0f - uu - vv) + n1 * uu) + n2 * vv;
   float flip = dot(cross(e1, e2), eye - a) > 0.0f ? 1.0f : -1.0f;

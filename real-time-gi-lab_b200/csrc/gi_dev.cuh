@@ -170,6 +170,17 @@ struct SceneDev {
   uint32_t nitems, threads, key_stride, key_limit;   // threads of the triangle passes; keys below key_limit
 };
 
+// Drawn triangle t of a raster: row t of the table, or with drawn instances (inst set) row t mod key_stride of
+// instance t / key_stride, moved by its offset
+__device__ __forceinline__ uint4 drawn_tri(const SceneDev &s, uint32_t t, f3 &off) {
+  off = mk(0.0f, 0.0f, 0.0f);
+  if (!s.inst) return s.tri[t];
+  const uint32_t i = t / s.key_stride;
+  const float4 o = s.inst[i];
+  off = mk(o.x, o.y, o.z);
+  return s.tri[t - i * s.key_stride];
+}
+
 // Voxel world in device memory (struct of arrays; the reference packs the same data in one `vox` buffer,
 // voxel.ts:753-760).
 struct VoxDev {

@@ -62,10 +62,13 @@ __global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__res
     sr.map[i] = 1.0f;
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, nch = 0;
   if (t < s.ntris) {
-    uint4 idx = s.tri[t];
+    f3 off;
+    uint4 idx = drawn_tri(s, t, off);
     const gi_material &mt = s.mats[idx.w];
     if (!((mt.flags & 1u) != 0u && mt.base_color[3] < mt.alpha_cutoff)) {
-      f3 c0 = light_clip(F, ld3(s.pos[idx.x])), c1 = light_clip(F, ld3(s.pos[idx.y])), c2 = light_clip(F, ld3(s.pos[idx.z]));
+      f3 a = ld3(s.pos[idx.x]), b = ld3(s.pos[idx.y]), c = ld3(s.pos[idx.z]);
+      if (s.inst) { a = a + off; b = b + off; c = c + off; }
+      f3 c0 = light_clip(F, a), c1 = light_clip(F, b), c2 = light_clip(F, c);
       float det = (c1.x - c0.x) * (c2.y - c0.y) - (c2.x - c0.x) * (c1.y - c0.y);
       if (det != 0.0f) {
         const float inv = 1.0f / (float)S, fS = (float)S;

@@ -41,6 +41,7 @@ SIGNATURES = {
     "gi_vox_set_world": (C.c_int, [_P, _P, C.c_uint32, _P, C.c_uint32, C.c_uint32]),
     "gi_vox_set_items": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32]),
     "gi_scene_set_draw_count": (C.c_int, [_P, C.c_uint32]),
+    "gi_scene_set_draw_instances": (C.c_int, [_P, _P, C.c_uint32]),
     "gi_rc_create_world": (C.c_int, [_P, _P, _P, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
     "gi_rc_set_frame": (C.c_int, [_P, _P, _P]),
     "gi_rc_set_gbuffer": (C.c_int, [_P, _P, _P, _P]),

@@ -63,6 +63,14 @@ class SceneGpu:
         """The rasters draw rows [0, count) (a world's clustered copies are voxelised only)."""
         _lib.call("gi_scene_set_draw_count", self.handle, int(count))
 
+    def set_draw_instances(self, offsets) -> None:
+        """The rasters draw the drawn rows at every offset (instance 0 at the origin; None: once)."""
+        if offsets is None or len(offsets) <= 1:
+            _lib.call("gi_scene_set_draw_instances", self.handle, None, 1)
+            return
+        o = np.ascontiguousarray(np.asarray(offsets, np.float64).astype(np.float32).reshape(-1))
+        _lib.call("gi_scene_set_draw_instances", self.handle, _ptr(o), len(offsets))
+
     def update_vertices(self, first: int, pos: np.ndarray, nrm: np.ndarray, stream=None):
         pos = np.ascontiguousarray(pos, dtype=np.float32)
         nrm = np.ascontiguousarray(nrm, dtype=np.float32)

@@ -126,3 +126,45 @@ def test_items_are_checked_and_stale_graphs_refused(ctx):
     finally:
         for h in (rc, vw, sg):
             h.destroy()
+
+
+def test_instanced_rasters(ctx):
+    """The rasters draw the static rows at every instance (gi_scene_set_draw_instances): the G-buffer and the sun's
+    shadow map of four room instances seen from above, bit-exact with the oracle's rasters."""
+    s = scenes.room_scene(0)
+    v = configs.vox_params(ROOM_V)
+    s2, w = W.with_world(s, INSTANCES, float(v.v0), v.levels)
+    cam = fr.Camera((-18.0, 22.0, -16.0), (6.0, 0.0, 12.0), 60, 0.05)
+    W_, H_ = 200, 150
+    p = configs.parse_config("screen-8-voxel-f32-dda64", {"cascades": 2})
+    bmin = np.min([np.asarray(s.positions).min(0) + o for o in INSTANCES], axis=0)
+    bmax = np.max([np.asarray(s.positions).max(0) + o for o in INSTANCES], axis=0)
+    F = fr.pack_frame(fr.FrameParams(cam=cam, width=W_, height=H_, sun_dir=(0.3, 1.0, 0.2), cascades=p.cascades, P=p.P,
+                                     light_view_proj=fr.scene_sun_view_proj(tuple(map(float, bmin)), tuple(map(float, bmax)),
+                                                                            (0.3, 1.0, 0.2)),
+                                     shadow_bias=fr.SHADOW_BIAS))
+    sg = gpu.SceneGpu(ctx, s2)
+    rc = gpu.Rc(ctx, p, W_, H_)
+    try:
+        sg.set_draw_count(s.triangle_count)
+        sg.set_draw_instances(INSTANCES)
+        rc.set_frame(F)
+        rc.render_gbuffer(sg)
+        rc.render_shadow(sg, 256)
+        depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(H_, W_)
+        normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(H_, W_, 4).astype(np.float32)
+        shadow = rc.read_shadow()
+        d0, n0, tri = bind.raster_gbuffer(s2, F, W_, H_, ndraw=s.triangle_count, draw_instances=INSTANCES)
+        assert np.array_equal(depth.view(np.uint32), d0.view(np.uint32))
+        assert np.array_equal(normal.astype(np.float16).view(np.uint16), n0.astype(np.float16).view(np.uint16))
+        sm = bind.shadow_render(s2, F, 256, ndraw=s.triangle_count, draw_instances=INSTANCES)
+        assert np.array_equal(shadow.view(np.uint32), sm.view(np.uint32))
+        inst_of = tri[tri != 0xFFFFFFFF] // s.triangle_count
+        assert len(set(inst_of.tolist())) >= 3            # several instances are in view
+        sg.set_draw_instances(None)                       # back to one draw
+        rc.render_gbuffer(sg)
+        d1 = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(H_, W_)
+        assert (d1 > 0).sum() < (depth > 0).sum()
+    finally:
+        rc.destroy()
+        sg.destroy()
