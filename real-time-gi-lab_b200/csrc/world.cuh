@@ -9,7 +9,8 @@
 //    table does not depend on the order of the concurrent inserts (the phase-concurrent deterministic hash table of
 //    Shun & Blelloch, SPAA 2014); compact numbers the keys in slot order with a chained scan instead of an atomic
 //    counter.  The whole solve is then deterministic and equal to the oracle's state word for word;
-//  * registerPixels inserts each distinct key of a warp once (the lanes that hold the same key agree on a leader);
+//  * registerPixels inserts the 8 keys of each distinct grid cell of a warp once (the lanes in the same cell and LOD
+//    agree on a leader);
 //  * relocateVox and linkParents run one warp per probe (64 and 8 x 8 threads in the reference); the sums the
 //    reference takes on one thread are still taken by one lane, in the same order;
 //  * indirect dispatches become grid-stride loops over the device-side probe counts;
@@ -199,13 +200,16 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
       }
     }
   }
-#pragma unroll 1
-  for (uint32_t k = 0; k < 8u; k++) {
-    const i3 o = w_corner(k);
-    const uint32_t key = live ? w_key_at(mki(b.x + o.x, b.y + o.y, b.z + o.z), org0, lod) : W_NONE;
-    const unsigned grp = __match_any_sync(0xffffffffu, key);
-    if (key != W_NONE && (uint32_t)(__ffs(grp) - 1) == lane)
-      if (!w_insert(w.keys + w.hash_off[0], w.hash_mask[0], key)) atomicAdd(&r.counts[16], 1u);
+  // the lanes whose pixels fall in the same grid cell at the same LOD hold the same 8 keys: one of them inserts them
+  const unsigned long long xy = ((unsigned long long)(uint32_t)b.x << 32) | (uint32_t)b.y;
+  const unsigned long long zl = live ? (((unsigned long long)(uint32_t)b.z << 32) | (uint32_t)lod) : ~0ull;
+  const unsigned grp = __match_any_sync(0xffffffffu, xy) & __match_any_sync(0xffffffffu, zl);
+  if (live && (uint32_t)(__ffs(grp) - 1) == lane) {
+    for (uint32_t k = 0; k < 8u; k++) {
+      const i3 o = w_corner(k);
+      const uint32_t key = w_key_at(mki(b.x + o.x, b.y + o.y, b.z + o.z), org0, lod);
+      if (key != W_NONE && !w_insert(w.keys + w.hash_off[0], w.hash_mask[0], key)) atomicAdd(&r.counts[16], 1u);
+    }
   }
 }
 
