@@ -45,6 +45,8 @@ __device__ __forceinline__ f3 ld3(float4 v) { return mk(v.x, v.y, v.z); }
 // f32 -> i32 truncating and saturating (NaN -> 0), WGSL's conversion
 __device__ __forceinline__ int f2i(float f) { return __float2int_rz(f); }
 __device__ __forceinline__ i3 vf2i(f3 a) { return mki(f2i(a.x), f2i(a.y), f2i(a.z)); }
+// f2i(floorf(x)) in one conversion rounding toward -inf (saturating, NaN -> 0: the same integer for every input)
+__device__ __forceinline__ i3 vfloori(f3 a) { return mki(__float2int_rd(a.x), __float2int_rd(a.y), __float2int_rd(a.z)); }
 __device__ __forceinline__ f3 vi2f(i3 a) { return mk((float)a.x, (float)a.y, (float)a.z); }
 __device__ __forceinline__ int iclamp(int x, int lo, int hi) { return min(max(x, lo), hi); }
 __device__ __forceinline__ i3 iclamp3(i3 a, i3 lo, i3 hi) {

@@ -100,7 +100,7 @@ __device__ __forceinline__ float smoothstep_(float e0, float e1, float x) {
 __device__ f3 bn_read(const BounceDev &b, const uint2 *vol, f3 q, f3 p, f3 n) {
   const i3 org = bn_origin(b, vol);
   const f3 g = mk(q.x / b.cell, q.y / b.cell, q.z / b.cell) - vi2f(org);
-  const i3 bb = vf2i(vfloor(g));
+  const i3 bb = vfloori(g);
   const f3 fr = g - vi2f(bb), n2 = n * n;
   const float tol = 0.5f * b.v0;
   f3 e = mk(0.0f, 0.0f, 0.0f);
@@ -230,7 +230,7 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
   i3 st = mki(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
   f3 sp = mk(st.x > 0 ? 1.0f : 0.0f, st.y > 0 ? 1.0f : 0.0f, st.z > 0 ? 1.0f : 0.0f);
   int nVox = G * 8;
-  i3 c = iclamp3(vf2i(vfloor(((o + d * t) - lo) / vs)), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
+  i3 c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
   f3 tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
   f3 tDelta = vabs(inv * vs);
   float tIn = t;
@@ -268,7 +268,7 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
       if (bt.x <= bt.y && bt.x <= bt.z) nb.x += st.x; else if (bt.y <= bt.z) nb.y += st.y; else nb.z += st.z;
       if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) break;
       t = te; tIn = te;
-      c = iclamp3(vf2i(vfloor(((o + d * t) - lo) / vs)), mki(nb.x * 8, nb.y * 8, nb.z * 8),
+      c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(nb.x * 8, nb.y * 8, nb.z * 8),
                   mki(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
       tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
       continue;
@@ -505,7 +505,7 @@ __device__ __forceinline__ void merge_quad(const RcDev &r, uint32_t c, uint32_t 
       float cx = ((float)(pi % L.tiles_x) + 0.5f) * (float)L.tile_size;
       float cy = ((float)(pi / L.tiles_x) + 0.5f) * (float)L.tile_size;
       float ux = div_tile(cx, U) - 0.5f, uy = div_tile(cy, U) - 0.5f;
-      int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+      int bx = __float2int_rd(ux), by = __float2int_rd(uy);
       float fx = ux - (float)bx, fy = uy - (float)by;
 #pragma unroll
       for (uint32_t k = 0; k < 4; k++) {
@@ -595,7 +595,7 @@ __device__ __forceinline__ void gather_pixel(const RcDev &r, uint32_t px, uint32
     f3 n = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
     float z = view_z(F, x);
     float ux = div_tile((float)px + 0.5f, L) - 0.5f, uy = div_tile((float)py + 0.5f, L) - 0.5f;
-    int bx = f2i(floorf(ux)), by = f2i(floorf(uy));
+    int bx = __float2int_rd(ux), by = __float2int_rd(uy);
     float fx = ux - (float)bx, fy = uy - (float)by;
     float y[9];
     sh_basis(n, y);
@@ -677,7 +677,7 @@ __device__ __forceinline__ void gather_tiles(const RcDev &r, uint32_t blk_x, uin
   const unsigned on_mask = __ballot_sync(0xffffffffu, on);
   if (on_mask == 0u) return;   // whole warp off the screen
   const CascDev &L = r.c[0];
-  int bx = f2i(floorf(div_tile((float)px + 0.5f, L) - 0.5f)), by = f2i(floorf(div_tile((float)py + 0.5f, L) - 0.5f));
+  int bx = __float2int_rd(div_tile((float)px + 0.5f, L) - 0.5f), by = __float2int_rd(div_tile((float)py + 0.5f, L) - 0.5f);
   const int src_lane = __ffs(on_mask) - 1;
   const int bx0 = __shfl_sync(0xffffffffu, bx, src_lane), by0 = __shfl_sync(0xffffffffu, by, src_lane);
   if (!__all_sync(0xffffffffu, !on || (bx == bx0 && by == by0))) {
@@ -717,13 +717,13 @@ __device__ __forceinline__ size_t bn_index(const BounceDev &b, i3 c, int a) {
 }
 // bnOriginNow (bounce.ts:98): the probe coordinates of this frame's probe 0
 __device__ __forceinline__ i3 bn_origin_now(const BounceDev &b, const float *__restrict__ F) {
-  return mki(f2i(floorf(F[F_EYE] / b.cell)) - (int)(b.dx / 2u), f2i(floorf(F[F_EYE + 1] / b.cell)) - (int)(b.dy / 2u),
-             f2i(floorf(F[F_EYE + 2] / b.cell)) - (int)(b.dz / 2u));
+  return mki(__float2int_rd(F[F_EYE] / b.cell) - (int)(b.dx / 2u), __float2int_rd(F[F_EYE + 1] / b.cell) - (int)(b.dy / 2u),
+             __float2int_rd(F[F_EYE + 2] / b.cell) - (int)(b.dz / 2u));
 }
 // occAt (bounce.ts:99-104)
 __device__ __forceinline__ bool bn_occ_at(const VoxDev &v, uint32_t L, f3 p) {
   const float vs = vox_size(v, L);
-  const i3 c = vf2i(vfloor((p - (vi2f(org(v, L)) * vs) * 8.0f) / vs));
+  const i3 c = vfloori((p - (vi2f(org(v, L)) * vs) * 8.0f) / vs);
   const int n = (int)v.G * 8;
   if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= n || c.y >= n || c.z >= n) return false;
   return vox_at(v, L, c).x != GI_EMPTY;

@@ -81,10 +81,10 @@ __global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__res
         float ya = (1.0f - c0.y) * 0.5f * fS, yb = (1.0f - c1.y) * 0.5f * fS, yc = (1.0f - c2.y) * 0.5f * fS;
         float x0 = mn(mn(xa, xb), xc), x1 = mx(mx(xa, xb), xc), y0 = mn(mn(ya, yb), yc), y1 = mx(mx(ya, yb), yc);
         if (x1 >= -1.0f && y1 >= -1.0f && x0 <= fS + 1.0f && y0 <= fS + 1.0f) {
-          int i0 = iclamp(f2i(floorf(mx(x0, -2.0f))) - 1, 0, (int)S - 1);
-          int i1 = iclamp(f2i(floorf(mn(x1, fS + 2.0f))) + 1, 0, (int)S - 1);
-          int j0 = iclamp(f2i(floorf(mx(y0, -2.0f))) - 1, 0, (int)S - 1);
-          int j1 = iclamp(f2i(floorf(mn(y1, fS + 2.0f))) + 1, 0, (int)S - 1);
+          int i0 = iclamp(__float2int_rd(mx(x0, -2.0f)) - 1, 0, (int)S - 1);
+          int i1 = iclamp(__float2int_rd(mn(x1, fS + 2.0f)) + 1, 0, (int)S - 1);
+          int j0 = iclamp(__float2int_rd(mx(y0, -2.0f)) - 1, 0, (int)S - 1);
+          int j1 = iclamp(__float2int_rd(mn(y1, fS + 2.0f)) + 1, 0, (int)S - 1);
           uint32_t bw = (uint32_t)(i1 - i0 + 1), bh = (uint32_t)(j1 - j0 + 1);
           nch = (bw * bh + SM_CHUNK - 1u) / SM_CHUNK;
           sr.rec[4u * t] = make_float4(c0.x, c0.y, c0.z, bias);

@@ -64,8 +64,8 @@ __device__ __forceinline__ Range vox_range(const VoxDev &v, const Tri &T, uint32
   f3 lo = region_lo(v, L);
   f3 a_ = vmin(vmin(T.a, T.b), T.c), b_ = vmax(vmax(T.a, T.b), T.c);
   int lim = bricks ? v.lim_brick[L] : v.lim_vox[L];   // f2i(G * size * 8 / cell) (vox_derived)
-  i3 a = vf2i(vfloor((a_ - lo) / cell));
-  i3 b = vf2i(vfloor((b_ - lo) / cell));
+  i3 a = vfloori((a_ - lo) / cell);
+  i3 b = vfloori((b_ - lo) / cell);
   a = iclamp3(a, mki(0, 0, 0), mki(lim, lim, lim));
   b = iclamp3(mki(b.x + 1, b.y + 1, b.z + 1), mki(0, 0, 0), mki(lim, lim, lim));
   Range r;

@@ -36,7 +36,7 @@ __device__ __forceinline__ float w_spacing(const float *__restrict__ F, int lod,
 }
 // originOf (rc.ts:254)
 __device__ __forceinline__ i3 w_origin(const float *__restrict__ F, float s) {
-  const i3 o = vf2i(vfloor(mk(F[F_EYE] / s, F[F_EYE + 1] / s, F[F_EYE + 2] / s)));
+  const i3 o = vfloori(mk(F[F_EYE] / s, F[F_EYE + 1] / s, F[F_EYE + 2] / s));
   return mki(o.x - 256, o.y - 256, o.z - 256);
 }
 // keyFor (rc.ts:255-259) with the origin of (lod, c) given: the origin depends only on them, so callers that make
@@ -86,7 +86,7 @@ __device__ __forceinline__ uint32_t w_lookup(const WorldDev &w, uint32_t c, uint
 // voxCell (rc.ts:379-386): (brick, bit), brick GI_MARK when empty or outside the level's window
 __device__ __forceinline__ uint2 w_vox_cell(const VoxDev &v, uint32_t L, f3 p) {
   const float vs = vox_size(v, L);
-  const i3 c = vf2i(vfloor((p - (vi2f(org(v, L)) * vs) * 8.0f) / vs));
+  const i3 c = vfloori((p - (vi2f(org(v, L)) * vs) * 8.0f) / vs);
   const int n = (int)v.G * 8;
   if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= n || c.y >= n || c.z >= n) return make_uint2(GI_MARK, 0u);
   const uint3 r = vox_at(v, L, c);
@@ -194,7 +194,7 @@ __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) 
         const f3 x = world_at(F, px, py, d);
         lod = w_lod_for(F, length3(x - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2])));
         const float s = w_spacing(F, lod, 0u);
-        b = vf2i(vfloor(mk(x.x / s, x.y / s, x.z / s)));
+        b = vfloori(mk(x.x / s, x.y / s, x.z / s));
         org0 = w_origin(F, s);
         live = true;
       }
@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
     const int lod = w_lod_for(F, length3(x - mk(F[F_EYE], F[F_EYE + 1], F[F_EYE + 2])));
     const float s0 = w_spacing(F, lod, 0u);
     const f3 gp = mk(x.x / s0, x.y / s0, x.z / s0);
-    const i3 bb = vf2i(vfloor(gp)), org0 = w_origin(F, s0);
+    const i3 bb = vfloori(gp), org0 = w_origin(F, s0);
     const f3 f = gp - vi2f(bb);
     const uint32_t Lo = vox_level_for(v, vox_level(v, r, s0, 0u), x);
     const f3 xo1 = x + n * (1.0f * vox_size(v, Lo));
