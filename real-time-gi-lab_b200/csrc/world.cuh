@@ -123,41 +123,71 @@ __device__ __forceinline__ bool w_seg_occluded(const VoxDev &v, f3 a, f3 b, uint
   return false;
 }
 
-// relocate (rc.ts:345-366): the probe pushed out along a plane fitted to G-buffer samples within 1.5 spacings
-__device__ __forceinline__ void w_relocate_gbuffer(const RcDev &r, f3 p, float s, f3 &rp, f3 &rn) {
+// relocate (rc.ts:345-366): the probe pushed out along a plane fitted to G-buffer samples within 1.5 spacings.  Half a
+// warp per probe, lane j reading tap j (the 16 taps' loads in flight together); every lane then takes the sums in tap
+// order from its half's lanes.
+__device__ __forceinline__ void w_relocate_gbuffer(const RcDev &r, const WorldDev &w, uint32_t c, uint32_t bid,
+                                                   uint32_t nblk) {
   const float *F = r.frame;
-  rp = p;
-  rn = mk(0.0f, 0.0f, 0.0f);
-  const float *m = F + F_VP;
-  float c4[4];
+  const uint32_t lane = threadIdx.x & 31u, j = lane & 15u, n = w.state[8 + c];
+  // a warp's two probes: 2 * warp and 2 * warp + 1 (the loop bound is the warp's, so every lane shuffles)
+  for (uint32_t wp = (bid * blockDim.x + threadIdx.x) >> 5; 2u * wp < n; wp += (nblk * blockDim.x) >> 5) {
+    const uint32_t pi = 2u * wp + (lane >> 4);
+    const bool live = pi < n;
+    ProbeDev *prp = &r.probes[r.c[c].probe_off + (live ? pi : 2u * wp)];
+    const int4 g = prp->grid;
+    const float s = w_spacing(F, g.w, c);
+    const f3 p = vi2f(mki(g.x, g.y, g.z)) * s;
+    const float *m = F + F_VP;
+    float c4[4];
 #pragma unroll
-  for (int i = 0; i < 4; i++) c4[i] = m[i] * p.x + m[4 + i] * p.y + m[8 + i] * p.z + m[12 + i] * 1.0f;
-  if (c4[3] <= F[F_EYE + 3]) return;
-  const float nx = c4[0] / c4[3], ny = c4[1] / c4[3];
-  const float cx = (nx * 0.5f + 0.5f) * F[F_SIZE], cy = (0.5f - ny * 0.5f) * F[F_SIZE + 1];
-  const float rpx = s / (c4[3] * F[F_RC + 1]);
-  f3 sn = mk(0.0f, 0.0f, 0.0f);
-  float se = 0.0f, cnt = 0.0f;
-  for (uint32_t j = 0; j < 16u; j++) {
-    const float ox = ((float)(j % 4u) - 1.5f) / 1.5f * rpx, oy = ((float)(j / 4u) - 1.5f) / 1.5f * rpx;
-    const int qx = f2i(floorf(cx + ox)), qy = f2i(floorf(cy + oy));
-    if (qx < 0 || qy < 0 || qx >= (int)r.width || qy >= (int)r.height) continue;
-    const size_t q = (size_t)qy * r.width + (size_t)qx;
-    const float d = r.depth[q];
-    if (!(d > 0.0f)) continue;
-    const f3 x = world_at(F, qx, qy, d);
-    if (length3(x - p) > 1.5f * s) continue;
-    const uint2 nn = r.normal[q];
-    const f3 n = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
-    sn = sn + n;
-    se += dot(n, p - x) / s;
-    cnt += 1.0f;
+    for (int i = 0; i < 4; i++) c4[i] = m[i] * p.x + m[4 + i] * p.y + m[8 + i] * p.z + m[12 + i] * 1.0f;
+    const bool front = live && !(c4[3] <= F[F_EYE + 3]);
+    bool ok = false;
+    f3 tn = mk(0.0f, 0.0f, 0.0f);
+    float te = 0.0f;
+    if (front) {
+      const float nx = c4[0] / c4[3], ny = c4[1] / c4[3];
+      const float cx = (nx * 0.5f + 0.5f) * F[F_SIZE], cy = (0.5f - ny * 0.5f) * F[F_SIZE + 1];
+      const float rpx = s / (c4[3] * F[F_RC + 1]);
+      const float ox = ((float)(j % 4u) - 1.5f) / 1.5f * rpx, oy = ((float)(j / 4u) - 1.5f) / 1.5f * rpx;
+      const int qx = __float2int_rd(cx + ox), qy = __float2int_rd(cy + oy);
+      if (qx >= 0 && qy >= 0 && qx < (int)r.width && qy < (int)r.height) {
+        const size_t q = (size_t)qy * r.width + (size_t)qx;
+        const float d = r.depth[q];
+        if (d > 0.0f) {
+          const f3 x = world_at(F, qx, qy, d);
+          if (!(length3(x - p) > 1.5f * s)) {
+            const uint2 nn = r.normal[q];
+            tn = mk(h2f(nn.x & 0xffffu), h2f(nn.x >> 16), h2f(nn.y & 0xffffu));
+            te = dot(tn, p - x) / s;
+            ok = true;
+          }
+        }
+      }
+    }
+    f3 sn = mk(0.0f, 0.0f, 0.0f);
+    float se = 0.0f, cnt = 0.0f;
+    const unsigned okm = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (uint32_t t = 0; t < 16u; t++) {
+      const int src = (int)((lane & 16u) | t);
+      const f3 nt = mk(__shfl_sync(0xffffffffu, tn.x, src), __shfl_sync(0xffffffffu, tn.y, src),
+                       __shfl_sync(0xffffffffu, tn.z, src));
+      const float et = __shfl_sync(0xffffffffu, te, src);
+      if ((okm >> src) & 1u) {
+        sn = sn + nt;
+        se += et;
+        cnt += 1.0f;
+      }
+    }
+    if (!front || j != 0u || cnt < 1.0f || length3(sn) < 0.3f * cnt) continue;
+    const f3 mm = normalize3(sn);
+    const float e = se / cnt;
+    const f3 rp = e < F[F_RC2] ? p + (mm * (F[F_RC2] - e)) * s : p;
+    prp->pos = make_float4(rp.x, rp.y, rp.z, prp->pos.w);
+    prp->nrm = make_float4(mm.x, mm.y, mm.z, view_z(F, rp));
   }
-  if (cnt < 1.0f || length3(sn) < 0.3f * cnt) return;
-  const f3 mm = normalize3(sn);
-  const float e = se / cnt;
-  rn = mm;
-  if (e < F[F_RC2]) rp = p + (mm * (F[F_RC2] - e)) * s;
 }
 
 // clearKeys (rc.ts:472-476) + clearHist of this solve's parity; the counters, the trace's ray counter (word 80) and
@@ -226,8 +256,8 @@ __device__ __forceinline__ void w_register_up(const RcDev &r, const WorldDev &w,
   }
 }
 
-// compact's write for the key in slot h with probe index idx: slotProbe, and the probe (relocated from the G-buffer
-// with relocate 'gbuffer') with its voxel level
+// compact's write for the key in slot h with probe index idx: slotProbe, and the probe at its grid point with its voxel
+// level (the relocation step that follows moves it)
 __device__ __forceinline__ void w_compact_slot(const RcDev &r, const VoxDev &v, const WorldDev &w, uint32_t c, uint32_t h,
                                                uint32_t key, uint32_t idx) {
   const float *F = r.frame;
@@ -238,12 +268,10 @@ __device__ __forceinline__ void w_compact_slot(const RcDev &r, const VoxDev &v, 
   const i3 o = w_origin(F, s);
   const i3 g = mki((int)((key >> 18) & 511u) + o.x, (int)((key >> 9) & 511u) + o.y, (int)(key & 511u) + o.z);
   const f3 p = vi2f(g) * s;
-  f3 rp = p, rn = mk(0.0f, 0.0f, 0.0f);
-  if (w.relocate == 0u) w_relocate_gbuffer(r, p, s, rp, rn);
   const float s0 = w_spacing(F, lod, 0u);
   ProbeDev pr;
-  pr.pos = make_float4(rp.x, rp.y, rp.z, s0);
-  pr.nrm = make_float4(rn.x, rn.y, rn.z, view_z(F, rp));
+  pr.pos = make_float4(p.x, p.y, p.z, s0);
+  pr.nrm = make_float4(0.0f, 0.0f, 0.0f, view_z(F, p));
   pr.grid = make_int4(g.x, g.y, g.z, lod);
   r.probes[r.c[c].probe_off + idx] = pr;
   r.plevel[r.c[c].probe_off + idx] = vox_level(v, r, s0, c);
@@ -410,7 +438,10 @@ __device__ __forceinline__ void w_task(const RcDev &r, const VoxDev &v, const Wo
                                        uint32_t bid, uint32_t nblk) {
   switch (task) {
     case W_COMPACT: w_compact(r, v, w, c); break;
-    case W_RELOCATE: w_relocate_vox(r, v, w, c, bid, nblk); break;
+    case W_RELOCATE:
+      if (w.relocate == 2u) w_relocate_vox(r, v, w, c, bid, nblk);
+      else w_relocate_gbuffer(r, w, c, bid, nblk);
+      break;
     case W_REGISTER_UP: w_register_up(r, w, c, bid, nblk); break;
     case W_LINK: w_link_parents(r, v, w, c, bid, nblk); break;
     default: break;
@@ -729,13 +760,13 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
   auto pair = [&](uint32_t ta, uint32_t ca, uint32_t na, uint32_t tb, uint32_t cb, uint32_t nb) {
     return gi_launch(k_w_build, na + nb, 256, st, r, v, w, ta, ca, na, tb, cb, nb);
   };
-  const bool vrel = w.relocate == 2u;
+  const bool rel = w.relocate != 1u;   // 'gbuffer' and 'voxel' relocate in a step of their own
   // compact(c) waits on registerUp(c); relocateVox(c) and registerUp(c + 1) wait on compact(c) only; linkParents(c - 1)
   // waits on compact(c) and on relocateVox(c - 1) and (c); so each launch pairs two steps that share their inputs
   GI_TRY(pair(W_COMPACT, 0, nb_compact(0), W_NONE_TASK, 0, 0));
   for (uint32_t c = 0; c < N; c++) {
     const bool up = c + 1u < N;
-    if (vrel) {
+    if (rel) {
       GI_TRY(pair(W_RELOCATE, c, nb_warps(c), up ? W_REGISTER_UP : W_NONE_TASK, c + 1u, up ? nb_up(c + 1u) : 0u));
       if (up) GI_TRY(pair(W_COMPACT, c + 1u, nb_compact(c + 1u), c >= 1u ? W_LINK : W_NONE_TASK, c - 1u, c >= 1u ? nb_warps(c - 1u) : 0u));
     } else {
