@@ -679,7 +679,7 @@ template <int A>
 __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w) {
   grid_dep_wait();
   // a warp takes a 4 x 8 tile of the block's 16 x 16 pixels (neighbouring pixels share probes and segment lengths;
-  // 0.378 ms on the colonnade with 16 x 2 rows, 0.360 with 8 x 4 tiles, 0.354 with 4 x 8)
+  // 0.378 ms on the colonnade with 16 x 2 rows, 0.360 with 8 x 4 tiles, 0.354 with 4 x 8, 0.360 with 2 x 16)
   const uint32_t lane = threadIdx.x & 31u, wp = threadIdx.x >> 5;
   const uint32_t px = blockIdx.x * 16u + (wp & 3u) * 4u + (lane & 3u), py = blockIdx.y * 16u + (wp >> 2) * 8u + (lane >> 2);
   if (px >= r.width || py >= r.height) return;
