@@ -1,7 +1,7 @@
 """Extracts the voxel-build counters the reference recorded for its procedural leak rooms into leak_counters.json.
 
 Run in the container that holds the reference checkout (it reads it; nothing at test time does):
-    python tests/golden/make_leak_counters.py /root/reference
+    python tests/golden/make_leak_counters.py <reference checkout>
 The source files are the reference's own measurement summaries (docs/reference/measurements/s2-voxel-stratabrick/
 leak-<t>/world-32-voxel.summary.json): scene name and triangle count, voxParams, the static camera's readCounters()
 (voxel.ts:908-918) and the camera that the leak scenes use (scenes.ts:276).
@@ -10,7 +10,9 @@ import json
 import os
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_leak_counters.py <reference checkout>")
+ref = sys.argv[1]
 out = {}
 for t in ("0.02", "0.05", "0.1", "0.2", "0.4"):
     p = os.path.join(ref, "docs/reference/measurements/s2-voxel-stratabrick", f"leak-{t}", "world-32-voxel.summary.json")
