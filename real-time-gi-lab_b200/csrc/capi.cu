@@ -443,6 +443,7 @@ int gi_vox_update(gi_vox *v, const double eye[3]) {
       v->dev.origin[L][a] = (int32_t)o;
     }
   }
+  vox_bounds(v->dev);
   v->updated = true;
   return GI_OK;
 }
@@ -763,10 +764,16 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
     }
   d.mavg[0] = d.mavg[1] = nullptr;
   {
-    float tab[256];
-    for (int k = 0; k < 256; k++) tab[k] = (float)k / 255.0f;
+    // k / 255 and (k / 255) / pi for k = 0..255, IEEE f32 quotients
+    float tab[512];
+    for (int k = 0; k < 256; k++) {
+      volatile float a = (float)k / 255.0f;
+      volatile float ap = a / 3.14159265f;
+      tab[k] = a;
+      tab[256 + k] = ap;
+    }
     float *u8 = nullptr;
-    if ((e = dalloc(&u8, 256)) || (e = cudaMemcpy(u8, tab, sizeof tab, cudaMemcpyHostToDevice))) {
+    if ((e = dalloc(&u8, 512)) || (e = cudaMemcpy(u8, tab, sizeof tab, cudaMemcpyHostToDevice))) {
       cudaFree(u8);
       free_rc(r);
       delete r;

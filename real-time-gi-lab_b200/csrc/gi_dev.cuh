@@ -115,6 +115,16 @@ __device__ __forceinline__ uint32_t pack2x16snorm(float a, float b) {
   int ia = (int)floorf(0.5f + 32767.0f * ca), ib = (int)floorf(0.5f + 32767.0f * cb);
   return ((uint32_t)ia & 0xffffu) | (((uint32_t)ib & 0xffffu) << 16);
 }
+// unpack2x16snorm of one half: max(k / 32767, -1) for the 16-bit k, the IEEE quotient from its product with
+// r = RN(1 / 32767) and one fused correction step (equal to the quotient for all 65536 k, checked exhaustively on the
+// CPU against exact arithmetic)
+__device__ __forceinline__ float snorm16(uint32_t h) {
+  const float k = (float)(int16_t)(h & 0xffffu);
+  const float r = 1.0f / 32767.0f;
+  const float q = k * r;
+  const float e = __fmaf_rn(-q, 32767.0f, k);
+  return mx(__fmaf_rn(e, r, q), -1.0f);
+}
 __device__ __forceinline__ uint16_t f2h(float x) { return __half_as_ushort(__float2half_rn(x)); }
 __device__ __forceinline__ float h2f(uint16_t h) { return __half2float(__ushort_as_half(h)); }
 __device__ __forceinline__ uint16_t f2bf(float x) { return __bfloat16_as_ushort(__float2bfloat16_rn(x)); }
@@ -193,6 +203,8 @@ struct VoxDev {
   float vs[8];         // voxel size per level, ldexpf(v0, L) (vox_derived)
   int32_t lim_vox[8], lim_brick[8];   // voxRange's limit f2i(G * size * 8 / cell), voxel and brick cells (vox_derived)
   int32_t origin[8][4];
+  float inv_vs[8];     // RN(1 / vs[L]) (vox_derived)
+  float box_lo[8][4], box_hi[8][4];   // per level the clipmap's box: (origin * vs) * 8 and lo + (G * vs) * 8 (vox_bounds)
   uint32_t *hdr;       // GI_HDR counter words
   uint32_t *ptr;       // levels * G^3 brick pointers
   uint32_t *occ;       // max_bricks * 16 occupancy words (64 bytes per brick)

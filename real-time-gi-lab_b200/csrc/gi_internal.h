@@ -45,7 +45,7 @@ struct RcDev {
   uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
   void *rad_traced;        // optional: copy of the atlas after the trace
   float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
-  const float *unorm8;     // k / 255.0f for k = 0..255 (IEEE quotients, computed on the host)
+  const float *unorm8;     // [k] = k / 255.0f, [256 + k] = (k / 255.0f) / pi for k = 0..255 (IEEE quotients, host)
   const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)
 };
 
@@ -110,9 +110,30 @@ inline void vox_derived(VoxDev &d) {
     volatile float b = a * 8.0f;
     volatile float cb = vs * 8.0f;
     volatile float qv = b / vs, qb = b / cb;
+    volatile float iv = 1.0f / vs;
     d.vs[L] = vs;
+    d.inv_vs[L] = iv;
     d.lim_vox[L] = f2i_host(qv);
     d.lim_brick[L] = f2i_host(qb);
+  }
+}
+// Per-level box of the clipmap window after the origins are set, with the f32 operations traceVox uses
+// (voxel.ts:124-125: lo = (origin * vs) * 8, hi = lo + (G * vs) * 8; voxInside's lo = origin * (vs * 8) and
+// hi = lo + G * (vs * 8), voxel.ts:108-112, are the same numbers, a scaling by 8 being exact).
+inline void vox_bounds(VoxDev &d) {
+  for (uint32_t L = 0; L < 8; L++) {
+    volatile float vs = d.vs[L];
+    volatile float gs = (float)d.G * vs;
+    volatile float ext = gs * 8.0f;
+    for (int a = 0; a < 3; a++) {
+      volatile float o = (float)d.origin[L][a];
+      volatile float ov = o * vs;
+      volatile float lo = ov * 8.0f;
+      volatile float hi = lo + ext;
+      d.box_lo[L][a] = lo;
+      d.box_hi[L][a] = hi;
+    }
+    d.box_lo[L][3] = d.box_hi[L][3] = 0.0f;
   }
 }
 

@@ -129,6 +129,7 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
       v.origin[L][a] = (int32_t)o;
     }
   }
+  vox_bounds(v);
   v.hdr = hdr; v.ptr = ptr; v.occ = occ; v.base = base; v.code = code;
   v.attr = reinterpret_cast<uint4 *>(attr); v.plane = plane; v.sunvis = sunvis;
   v.rep = scratch;

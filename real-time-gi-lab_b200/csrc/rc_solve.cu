@@ -59,9 +59,13 @@ __device__ __forceinline__ uint3 vox_at(const VoxDev &v, uint32_t L, i3 c) {
 
 // voxInside / voxLevelFor (voxel.ts:108-119)
 __device__ __forceinline__ bool vox_inside(const VoxDev &v, uint32_t L, f3 p) {
+#if GI_X1
+  const f3 lo = mk(v.box_lo[L][0], v.box_lo[L][1], v.box_lo[L][2]), hi = mk(v.box_hi[L][0], v.box_hi[L][1], v.box_hi[L][2]);
+#else
   float bs = vox_size(v, L) * 8.0f;
   f3 lo = vi2f(org(v, L)) * bs;
   f3 hi = adds(lo, (float)v.G * bs);
+#endif
   return p.x > lo.x && p.y > lo.y && p.z > lo.z && p.x < hi.x && p.y < hi.y && p.z < hi.z;
 }
 __device__ __forceinline__ uint32_t vox_level_for(const VoxDev &v, uint32_t L, f3 e) {
@@ -173,9 +177,13 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   float alb2 = __ldg(&r_unorm8[(w.x >> 16) & 0xffu]), alb3 = __ldg(&r_unorm8[w.x >> 24]);
   // k / 32767 for a 16-bit k as the f64 product rounded to f32: equal to the f32 quotient for every k (checked
   // exhaustively in the CPU tests), without a division
+#if GI_X3
+  float nx = snorm16(w.y & 0xffffu), ny = snorm16(w.y >> 16);
+#else
   const double inv32767 = 1.0 / 32767.0;
   float nx = mx(__double2float_rn((double)(int16_t)(w.y & 0xffffu) * inv32767), -1.0f);
   float ny = mx(__double2float_rn((double)(int16_t)(w.y >> 16) * inv32767), -1.0f);
+#endif
   f3 n0 = mk(nx, ny, 1.0f - fabsf(nx) - fabsf(ny));
   float q = mx(-n0.z, 0.0f);
   n0.x += n0.x >= 0.0f ? -q : q;
@@ -186,9 +194,14 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   f3 a = mk(alb0, alb1, alb2);
   // a / pi for the 256 albedo values k / 255 as f64 products rounded to f32: equal to the f32 quotients (checked
   // exhaustively in the CPU tests)
+#if GI_X3
+  const f3 api = mk(__ldg(&r_unorm8[256u + (w.x & 0xffu)]), __ldg(&r_unorm8[256u + ((w.x >> 8) & 0xffu)]),
+                    __ldg(&r_unorm8[256u + ((w.x >> 16) & 0xffu)]));
+#else
   const double inv_pi = 1.0 / (double)GI_PI;
   const f3 api = mk(__double2float_rn((double)a.x * inv_pi), __double2float_rn((double)a.y * inv_pi),
                     __double2float_rn((double)a.z * inv_pi));
+#endif
   // the multi-bounce term b = a / pi * e (+0 with e = 0)
   f3 r = api * bs(ai, has, entry - d * (0.25f * vsz), n0, d, pc, vsz);
   float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
@@ -202,6 +215,18 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
 
 struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 
+// clamp(floor(x / vs), lo, hi) with x / vs the IEEE quotient, from the product q = x * RN(1 / vs): q is within
+// 1.5 ulp(q) of the exact quotient and the rounded quotient within 0.5 ulp, so both lie in [q - thr, q + thr] with
+// thr = |q| 2^-20 + 2^-20; when the clamped floors of both ends agree that is the result (floor and clamp are
+// monotonic), else (q within thr of an integer that the clamp does not absorb) the quotient is taken.
+__device__ __forceinline__ int floor_div_clamp(float x, float vs, float ivs, int lo, int hi) {
+  const float q = x * ivs;
+  const float thr = fabsf(q) * 0x1p-20f + 0x1p-20f;
+  const int a = iclamp(__float2int_rd(q - thr), lo, hi), b = iclamp(__float2int_rd(q + thr), lo, hi);
+  if (a == b) return a;
+  return iclamp(__float2int_rd(x / vs), lo, hi);
+}
+
 // traceVox (voxel.ts:121-202) with a configurable step cap
 template <class BS>
 __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
@@ -212,8 +237,12 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
   out.steps = 0;
   float vs = vox_size(v, L);
   int G = (int)v.G;
+#if GI_X1
+  const f3 lo = mk(v.box_lo[L][0], v.box_lo[L][1], v.box_lo[L][2]), hi = mk(v.box_hi[L][0], v.box_hi[L][1], v.box_hi[L][2]);
+#else
   f3 lo = (vi2f(org(v, L)) * vs) * 8.0f;
   f3 hi = adds(lo, (float)G * vs * 8.0f);
+#endif
   f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
   f3 inv;
   if (inv_pre) {   // the direction's 1 / dd, tabulated with the directions (the same IEEE quotients)
@@ -230,7 +259,17 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
   i3 st = mki(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
   f3 sp = mk(st.x > 0 ? 1.0f : 0.0f, st.y > 0 ? 1.0f : 0.0f, st.z > 0 ? 1.0f : 0.0f);
   int nVox = G * 8;
+#if GI_X2
+  const float ivs = v.inv_vs[L];
+  i3 c;
+  {
+    const f3 x = (o + d * t) - lo;
+    c = mki(floor_div_clamp(x.x, vs, ivs, 0, nVox - 1), floor_div_clamp(x.y, vs, ivs, 0, nVox - 1),
+            floor_div_clamp(x.z, vs, ivs, 0, nVox - 1));
+  }
+#else
   i3 c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
+#endif
   f3 tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
   f3 tDelta = vabs(inv * vs);
   float tIn = t;
@@ -268,8 +307,16 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
       if (bt.x <= bt.y && bt.x <= bt.z) nb.x += st.x; else if (bt.y <= bt.z) nb.y += st.y; else nb.z += st.z;
       if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) break;
       t = te; tIn = te;
+#if GI_X2
+      {
+        const f3 x = (o + d * t) - lo;
+        c = mki(floor_div_clamp(x.x, vs, ivs, nb.x * 8, nb.x * 8 + 7), floor_div_clamp(x.y, vs, ivs, nb.y * 8, nb.y * 8 + 7),
+                floor_div_clamp(x.z, vs, ivs, nb.z * 8, nb.z * 8 + 7));
+      }
+#else
       c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(nb.x * 8, nb.y * 8, nb.z * 8),
                   mki(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
+#endif
       tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
       continue;
     }

@@ -208,6 +208,53 @@ def test_quotient_shortcuts_of_the_shading_are_exact():
                           (a.astype(np.float64) * (1.0 / np.float64(pi))).astype(np.float32).view(np.uint32))
 
 
+def _round_f32(x: Fraction) -> np.float32:
+    """x rounded to the nearest f32, ties to even (exact: the f64 guess and its neighbours compared as fractions)."""
+    c = np.float32(float(x))
+    best = None
+    for y in (np.nextafter(c, np.float32(-np.inf)), c, np.nextafter(c, np.float32(np.inf))):
+        d = abs(Fraction(float(y)) - x)
+        if best is None or d < best[0] or (d == best[0] and int(y.view(np.uint32)) % 2 == 0):
+            best = (d, y)
+    return best[1]
+
+
+def test_snorm16_by_corrected_reciprocal_is_the_quotient():
+    """The hit shading decodes a snorm16 half as q = k * r, e = fma(-q, 32767, k), fma(e, r, q) with r = RN(1 / 32767)
+    (two fused multiply-adds instead of a division): equal to the IEEE f32 quotient k / 32767 for all 65536 k.  Every
+    step is evaluated exactly and rounded once, as the fused operations do."""
+    r = np.float32(1.0) / np.float32(32767.0)
+    fr, f32767 = Fraction(float(r)), Fraction(32767)
+    x = np.arange(-32768, 32768).astype(np.float32)
+    want = x / np.float32(32767.0)
+    for k, w in zip(x, want):
+        fk = Fraction(float(k))
+        q = _round_f32(fk * fr)
+        e = _round_f32(-Fraction(float(q)) * f32767 + fk)
+        got = _round_f32(Fraction(float(e)) * fr + Fraction(float(q)))
+        assert got.view(np.uint32) == w.view(np.uint32), int(k)
+    # the albedo / pi table the shading reads: (k / 255) / pi as f32 quotients, the numbers the f64 products give
+    a = np.arange(256).astype(np.float32) / np.float32(255)
+    assert np.array_equal((a / np.float32(3.14159265)).view(np.uint32),
+                          (a.astype(np.float64) * (1.0 / np.float64(np.float32(3.14159265)))).astype(np.float32).view(np.uint32))
+
+
+def test_floor_div_clamp_bound():
+    """The DDA takes clamp(floor(x / vs)) from q = x * RN(1 / vs) when the clamped floors of q -+ thr agree, thr =
+    |q| 2^-20 + 2^-20, else from the quotient.  The bound it rests on: the IEEE quotient lies within [q - thr, q + thr]
+    (the ends rounded to f32).  Checked over random x of every magnitude and every level size of the clipmaps here."""
+    rng = np.random.default_rng(5)
+    for v0 in (0.05, 0.08, 0.1, 0.16, 0.2, 0.25, 0.3):
+        for L in range(8):
+            vs = np.float32(np.ldexp(np.float32(v0), L))
+            ivs = np.float32(1.0) / vs
+            x = (rng.uniform(-1.0, 1.0, 200000) * rng.choice([1e-6, 1e-2, 1.0, 1e2, 1e3, 3e4], 200000)).astype(np.float32)
+            q = x * ivs
+            thr = np.abs(q) * np.float32(2.0 ** -20) + np.float32(2.0 ** -20)
+            exact = x / vs
+            assert ((exact >= q - thr) & (exact <= q + thr)).all()
+
+
 def test_gi_exp_accuracy():
     """The weights' e^x (Cody-Waite reduction, degree-7 Horner polynomial with fused multiply-adds): relative error
     against the exact exponential below 3e-7 on [-80, 0] (the range -20 rel takes) and 0 below -80."""
