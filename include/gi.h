@@ -144,8 +144,14 @@ int gi_vox_build(gi_vox *vox, void *stream);
 /* readCounters (voxel.ts:908-918): the 64 header words (0 bricks marked, 1 voxels, 2-4 brick/big/voxel overflow,
  * 6 nonzero if a chained scan of the rebuild stopped waiting for a block (never expected), 8-15 bricks per level,
  * 16-23 voxBits big triangles per level, 24-31 markBricks big triangles per level).
- * Synchronises the stream. */
+ * Synchronises the stream.  The words are copied out in every case; returns GI_ERR_TIMEOUT when word 6 is set (the
+ * rebuild's state is then not valid), as the reference's counters report its overflows (voxel.ts:463,586). */
 int gi_vox_read_counters(gi_vox *vox, uint32_t hdr[64], void *stream);
+/* Test hook for failure detection, no counterpart in the reference: part `part` (0-based, in ticket order) of the
+ * next rebuilds' brick-allocation scan publishes nothing, so the part after it waits until its bounded wait gives up
+ * (well under a second) and sets header word 6; gi_vox_read_counters then returns GI_ERR_TIMEOUT.  part < 0 turns it
+ * off.  A held rebuild's voxel state is not valid; nothing reads outside its buffers. */
+int gi_vox_debug_hold_scan(gi_vox *vox, int32_t part);
 /* usedBytes (voxel.ts:919-922) of the last counters read: persistent and build-temporary bytes. */
 int gi_vox_used_bytes(gi_vox *vox, uint64_t *persistent, uint64_t *build_temp);
 /* Copies the voxel world's buffers to the host (any pointer may be NULL).  Sizes: ptr levels*G^3, occ
@@ -236,7 +242,8 @@ int gi_rc_read_irradiance_raw(gi_rc *rc, void *out, size_t bytes, void *stream);
 /* The same without synchronising: a stream-ordered copy into `out`, host or device memory (pinned host memory makes
  * it asynchronous). */
 int gi_rc_read_irradiance_async(gi_rc *rc, void *out, size_t bytes, void *stream);
-/* readCounts (rc.ts:1223-1232): the 80 counter words (rc.ts:173-175).  Synchronises. */
+/* readCounts (rc.ts:1223-1232): the 80 counter words (rc.ts:173-175).  Synchronises.  World probes: returns
+ * GI_ERR_TIMEOUT (the words copied out) when a bounded wait of the solve's compaction gave up. */
 int gi_rc_read_counts(gi_rc *rc, uint32_t counts[80], void *stream);
 /* setStats (rc.ts:1233): 0 off, 1 DDA step counters. */
 int gi_rc_set_stats(gi_rc *rc, uint32_t level);

@@ -192,6 +192,7 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
+  cudaFree(r->dev.trec);
   cudaFree((void *)r->dev.unorm8);
   cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
@@ -600,6 +601,15 @@ int gi_vox_read_counters(gi_vox *v, uint32_t hdr[64], void *stream) {
   CK(cudaMemcpyAsync(v->hdr, v->dev.hdr, sizeof v->hdr, cudaMemcpyDeviceToHost, S(stream)), "gi_vox_read_counters: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_vox_read_counters: sync");
   memcpy(hdr, v->hdr, sizeof v->hdr);
+  if (v->hdr[6] != 0u)
+    return fail(GI_ERR_TIMEOUT, "gi_vox_read_counters: a bounded wait of the rebuild's chained scans gave up (header word 6); "
+                "this rebuild's voxel state is not valid");
+  return GI_OK;
+}
+
+int gi_vox_debug_hold_scan(gi_vox *v, int32_t part) {
+  if (!v) return fail(GI_ERR_INVALID, "gi_vox_debug_hold_scan: NULL vox");
+  v->dev.scan_hold = part < 0 ? 0u : (uint32_t)part + 1u;
   return GI_OK;
 }
 
@@ -746,7 +756,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
       (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->sh_elem_bytes)) ||
       (e = cudaMalloc(&irr, npx * r->irr_elem_bytes)) || (e = dalloc(&counts, 96)) ||
-      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, 2u * dir_total))) {
+      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, 2u * dir_total)) || (e = dalloc(&d.trec, ray_total))) {
     d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
     free_rc(r);
     delete r;
@@ -793,7 +803,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
     delete r;
     return cuda_fail(e, "gi_rc_create: direction table");
   }
-  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 32 + ray_total * r->rad_elem_bytes +
+  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 32 + ray_total * (r->rad_elem_bytes + 16u) +
              r->sh_elems * r->sh_elem_bytes + npx * r->irr_elem_bytes + 96 * 4;
   if (wp) {
     WorldDev &w = r->w;
@@ -1334,7 +1344,12 @@ int gi_rc_read_counts(gi_rc *r, uint32_t counts[80], void *stream) {
   if (!r || !counts) return fail(GI_ERR_INVALID, "gi_rc_read_counts: NULL argument");
   CK(cudaSetDevice(r->ctx->device), "gi_rc_read_counts: cudaSetDevice");
   CK(cudaMemcpyAsync(counts, r->dev.counts, 80 * 4, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_counts: copy");
+  uint32_t gave_up = 0;
+  if (r->world) CK(cudaMemcpyAsync(&gave_up, r->w.state + 7, 4, cudaMemcpyDeviceToHost, S(stream)), "gi_rc_read_counts: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_counts: sync");
+  if (gave_up)
+    return fail(GI_ERR_TIMEOUT, "gi_rc_read_counts: a bounded wait of the world probes' compaction gave up; this solve's "
+                "probes are not valid");
   return GI_OK;
 }
 

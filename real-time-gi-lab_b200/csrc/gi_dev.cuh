@@ -225,7 +225,8 @@ struct VoxDev {
   // the frame block (lightViewProj, sun direction, shadow bias); without one the visibility is 1
   const float *sun_frame;
   const float *shadow;        // shadow_size^2 depths
-  uint32_t shadow_size, pad_sun;
+  uint32_t shadow_size;
+  uint32_t scan_hold;          // test hook (gi_vox_debug_hold_scan): part + 1 of the brick scan that never publishes; 0 off
 };
 
 __device__ __forceinline__ float vox_size(const VoxDev &v, uint32_t L) { return v.vs[L]; }

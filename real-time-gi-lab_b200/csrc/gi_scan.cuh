@@ -40,7 +40,8 @@ __device__ __forceinline__ uint32_t block_scan_256(uint32_t x, uint32_t *total) 
 // look[0] hands out tickets (the order in which blocks take their part of the scan: every smaller ticket belongs to
 // a block that is already running); look[1 + k] is part k's state, status << 32 | value with status 1 = the part's
 // own sum, 2 = the inclusive prefix through the part.  A part waits only on smaller tickets, so every wait ends; the
-// spin is bounded all the same, and a part that gives up sets header word 6 and takes what it has.
+// spin is bounded all the same, and a part that gives up sets header word 6 and takes what it has (the host reports
+// it as GI_ERR_TIMEOUT when it reads the counters).
 constexpr uint32_t LOOK_SPIN = 1u << 20;
 
 __device__ __forceinline__ void st_release_u64(unsigned long long *p, unsigned long long x) {
@@ -63,7 +64,10 @@ __device__ __forceinline__ uint32_t chain_ticket(unsigned long long *look) {
 }
 
 // One thread per block: publishes part k's sum, looks back for its exclusive prefix, publishes the inclusive prefix.
-__device__ __forceinline__ uint32_t chain_prefix(unsigned long long *look, uint32_t k, uint32_t sum, uint32_t *hdr) {
+// hold = k + 1 makes part k publish nothing (a test of the bounded wait: the parts after it give up), else 0.
+__device__ __forceinline__ uint32_t chain_prefix(unsigned long long *look, uint32_t k, uint32_t sum, uint32_t *hdr,
+                                                 uint32_t hold = 0u) {
+  if (hold != 0u && hold == k + 1u) return 0u;
   unsigned long long *st = look + 1;
   if (k == 0u) { st_release_u64(st, (2ull << 32) | sum); return 0u; }
   st_release_u64(st + k, (1ull << 32) | sum);

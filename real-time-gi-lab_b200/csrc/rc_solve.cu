@@ -59,13 +59,7 @@ __device__ __forceinline__ uint3 vox_at(const VoxDev &v, uint32_t L, i3 c) {
 
 // voxInside / voxLevelFor (voxel.ts:108-119)
 __device__ __forceinline__ bool vox_inside(const VoxDev &v, uint32_t L, f3 p) {
-#if GI_X1
   const f3 lo = mk(v.box_lo[L][0], v.box_lo[L][1], v.box_lo[L][2]), hi = mk(v.box_hi[L][0], v.box_hi[L][1], v.box_hi[L][2]);
-#else
-  float bs = vox_size(v, L) * 8.0f;
-  f3 lo = vi2f(org(v, L)) * bs;
-  f3 hi = adds(lo, (float)v.G * bs);
-#endif
   return p.x > lo.x && p.y > lo.y && p.z > lo.z && p.x < hi.x && p.y < hi.y && p.z < hi.z;
 }
 __device__ __forceinline__ uint32_t vox_level_for(const VoxDev &v, uint32_t L, f3 e) {
@@ -175,15 +169,8 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   // k / 255 for a byte k: the quotients, tabulated (the same IEEE quotients as dividing)
   float alb0 = __ldg(&r_unorm8[w.x & 0xffu]), alb1 = __ldg(&r_unorm8[(w.x >> 8) & 0xffu]);
   float alb2 = __ldg(&r_unorm8[(w.x >> 16) & 0xffu]), alb3 = __ldg(&r_unorm8[w.x >> 24]);
-  // k / 32767 for a 16-bit k as the f64 product rounded to f32: equal to the f32 quotient for every k (checked
-  // exhaustively in the CPU tests), without a division
-#if GI_X3
+  // unpack2x16snorm: the IEEE quotients k / 32767 without a division (snorm16)
   float nx = snorm16(w.y & 0xffffu), ny = snorm16(w.y >> 16);
-#else
-  const double inv32767 = 1.0 / 32767.0;
-  float nx = mx(__double2float_rn((double)(int16_t)(w.y & 0xffffu) * inv32767), -1.0f);
-  float ny = mx(__double2float_rn((double)(int16_t)(w.y >> 16) * inv32767), -1.0f);
-#endif
   f3 n0 = mk(nx, ny, 1.0f - fabsf(nx) - fabsf(ny));
   float q = mx(-n0.z, 0.0f);
   n0.x += n0.x >= 0.0f ? -q : q;
@@ -192,16 +179,9 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
   f3 n = dot(n0, n0) > 0.01f ? n0 : -d;
   if (dot(n, d) > 0.0f) n = -n;
   f3 a = mk(alb0, alb1, alb2);
-  // a / pi for the 256 albedo values k / 255 as f64 products rounded to f32: equal to the f32 quotients (checked
-  // exhaustively in the CPU tests)
-#if GI_X3
+  // a / pi for the 256 albedo values a = k / 255: the f32 quotients, tabulated after the k / 255 table
   const f3 api = mk(__ldg(&r_unorm8[256u + (w.x & 0xffu)]), __ldg(&r_unorm8[256u + ((w.x >> 8) & 0xffu)]),
                     __ldg(&r_unorm8[256u + ((w.x >> 16) & 0xffu)]));
-#else
-  const double inv_pi = 1.0 / (double)GI_PI;
-  const f3 api = mk(__double2float_rn((double)a.x * inv_pi), __double2float_rn((double)a.y * inv_pi),
-                    __double2float_rn((double)a.z * inv_pi));
-#endif
   // the multi-bounce term b = a / pi * e (+0 with e = 0)
   f3 r = api * bs(ai, has, entry - d * (0.25f * vsz), n0, d, pc, vsz);
   float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
@@ -215,19 +195,112 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
 
 struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 
-// clamp(floor(x / vs), lo, hi) with x / vs the IEEE quotient, from the product q = x * RN(1 / vs): q is within
-// 1.5 ulp(q) of the exact quotient and the rounded quotient within 0.5 ulp, so both lie in [q - thr, q + thr] with
-// thr = |q| 2^-20 + 2^-20; when the clamped floors of both ends agree that is the result (floor and clamp are
-// monotonic), else (q within thr of an integer that the clamp does not absorb) the quotient is taken.
-__device__ __forceinline__ int floor_div_clamp(float x, float vs, float ivs, int lo, int hi) {
-  const float q = x * ivs;
-  const float thr = fabsf(q) * 0x1p-20f + 0x1p-20f;
-  const int a = iclamp(__float2int_rd(q - thr), lo, hi), b = iclamp(__float2int_rd(q + thr), lo, hi);
-  if (a == b) return a;
-  return iclamp(__float2int_rd(x / vs), lo, hi);
+// traceVox (voxel.ts:121-202) split into its set-up and one iteration of its loop, so that a walk can be suspended
+// between iterations and resumed by another lane.  The f32 operations and their order are the reference's.
+struct Dda {
+  f3 o, d, inv, lo, tMax, tDelta, sp;
+  i3 c, st;
+  float vs, tEnd, tskip, tIn;
+  uint32_t L, steps;
+};
+enum { DDA_WALK = 0, DDA_MISS = 1, DDA_HIT = 2, DDA_HIT_DROP = 3 };
+
+// what the walk needs besides its position: the level's voxel size and box, the step signs and the cell increments
+__device__ __forceinline__ void dda_derived(const VoxDev &v, Dda &s) {
+  s.vs = vox_size(v, s.L);
+  s.lo = mk(v.box_lo[s.L][0], v.box_lo[s.L][1], v.box_lo[s.L][2]);
+  const f3 dd = mk(fabsf(s.d.x) < 1e-9f ? 1e-9f : s.d.x, fabsf(s.d.y) < 1e-9f ? 1e-9f : s.d.y,
+                   fabsf(s.d.z) < 1e-9f ? 1e-9f : s.d.z);
+  s.st = mki(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
+  s.sp = mk(s.st.x > 0 ? 1.0f : 0.0f, s.st.y > 0 ? 1.0f : 0.0f, s.st.z > 0 ? 1.0f : 0.0f);
+  s.tDelta = vabs(s.inv * s.vs);
 }
 
-// traceVox (voxel.ts:121-202) with a configurable step cap
+// traceVox's set-up (voxel.ts:122-138): false when the interval misses the level's box (T = 1, no step taken).
+// inv_pre: the direction's 1 / d with tiny components clamped, tabulated with the directions (the same IEEE
+// quotients), or null to divide here.
+__device__ __forceinline__ bool dda_begin(const VoxDev &v, f3 o, f3 d, float t0, float t1, float tskip, uint32_t L,
+                                          const float4 *inv_pre, Dda &s) {
+  s.o = o; s.d = d; s.L = L; s.steps = 0; s.tskip = tskip;
+  if (inv_pre) {
+    const float4 q = __ldg(inv_pre);
+    s.inv = mk(q.x, q.y, q.z);
+  } else {
+    const f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
+    s.inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
+  }
+  dda_derived(v, s);
+  const f3 hi = mk(v.box_hi[L][0], v.box_hi[L][1], v.box_hi[L][2]);
+  const f3 ta = (s.lo - o) * s.inv, tb = (hi - o) * s.inv;
+  const f3 tn = vmin(ta, tb), tf = vmax(ta, tb);
+  const float t = mx(mx(mx(tn.x, tn.y), tn.z), t0);
+  s.tEnd = mn(mn(mn(tf.x, tf.y), tf.z), t1);
+  if (t >= s.tEnd) return false;
+  const int nVox = (int)v.G * 8;
+  s.c = iclamp3(vfloori(((o + d * t) - s.lo) / s.vs), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
+  s.tMax = (((vi2f(s.c) + s.sp) * s.vs + s.lo) - o) * s.inv;
+  s.tIn = t;
+  return true;
+}
+
+// One iteration of traceVox's loop (voxel.ts:142-200) under a step cap: DDA_WALK to go on, DDA_MISS when the walk
+// ends empty, DDA_HIT (h = brick, bit, level L) or DDA_HIT_DROP (h = voxAt's brick, bit and coarser level) on the
+// first occupied voxel entered at tIn >= tSkip.  `steps` counts the iterations taken (rc.ts:232-235).
+__device__ __forceinline__ int dda_step(const VoxDev &v, Dda &s, uint32_t cap, uint3 &h) {
+  if (s.steps >= cap) return DDA_MISS;
+  s.steps++;
+  const int G = (int)v.G, nVox = G * 8;
+  const i3 b = mki(s.c.x >> 3, s.c.y >> 3, s.c.z >> 3);
+  const uint32_t ptr = __ldg(&v.ptr[s.L * (uint32_t)(G * G * G) + ((uint32_t)b.z * (uint32_t)G + (uint32_t)b.y) * (uint32_t)G
+                                    + (uint32_t)b.x]);
+  if (ptr == GI_DROP) {
+    // dropped brick: voxel by voxel, each read at the coarser level that holds it
+    const uint3 r = vox_at(v, s.L, s.c);
+    if (r.x != GI_EMPTY && s.tIn >= s.tskip) { h = r; return DDA_HIT_DROP; }
+    const float tx = mn(mn(s.tMax.x, s.tMax.y), s.tMax.z);
+    if (tx >= s.tEnd) return DDA_MISS;
+    s.tIn = tx;
+  } else if (ptr >= GI_MARK) {
+    // empty brick: jump to its exit
+    const f3 bt = (((vi2f(mki(b.x * 8, b.y * 8, b.z * 8)) + s.sp * 8.0f) * s.vs + s.lo) - s.o) * s.inv;
+    const float te = mn(mn(bt.x, bt.y), bt.z);
+    if (te >= s.tEnd) return DDA_MISS;
+    i3 nb = b;
+    if (bt.x <= bt.y && bt.x <= bt.z) nb.x += s.st.x; else if (bt.y <= bt.z) nb.y += s.st.y; else nb.z += s.st.z;
+    if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) return DDA_MISS;
+    s.tIn = te;
+    s.c = iclamp3(vfloori(((s.o + s.d * te) - s.lo) / s.vs), mki(nb.x * 8, nb.y * 8, nb.z * 8),
+                  mki(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
+    s.tMax = (((vi2f(s.c) + s.sp) * s.vs + s.lo) - s.o) * s.inv;
+    return DDA_WALK;
+  } else {
+    const uint32_t bit = (uint32_t)((s.c.x & 7) + 8 * (s.c.y & 7) + 64 * (s.c.z & 7));
+    const uint32_t occ = __ldg(&v.occ[ptr * 16u + (bit >> 5)]);
+    const float tExit = mn(mn(s.tMax.x, s.tMax.y), s.tMax.z);
+    if ((occ & (1u << (bit & 31u))) != 0u && s.tIn >= s.tskip) { h = make_uint3(ptr, bit, s.L); return DDA_HIT; }
+    if (tExit >= s.tEnd) return DDA_MISS;
+    s.tIn = tExit;
+  }
+  if (s.tMax.x <= s.tMax.y && s.tMax.x <= s.tMax.z) { s.c.x += s.st.x; s.tMax.x += s.tDelta.x; }
+  else if (s.tMax.y <= s.tMax.z) { s.c.y += s.st.y; s.tMax.y += s.tDelta.y; }
+  else { s.c.z += s.st.z; s.tMax.z += s.tDelta.z; }
+  if (s.c.x < 0 || s.c.y < 0 || s.c.z < 0 || s.c.x >= nVox || s.c.y >= nVox || s.c.z >= nVox) return DDA_MISS;
+  return DDA_WALK;
+}
+
+// The shading point of a hit: the voxel's centre and size (for a dropped brick, the coarser voxel that holds the cell)
+__device__ __forceinline__ void dda_hit_voxel(const VoxDev &v, const Dda &s, int kind, uint32_t hl, f3 &pc, float &vsz) {
+  if (kind == DDA_HIT) {
+    pc = s.lo + adds(vi2f(s.c), 0.5f) * s.vs;
+    vsz = s.vs;
+  } else {
+    vsz = vox_size(v, hl);
+    const f3 pcl = s.lo + adds(vi2f(s.c), 0.5f) * s.vs;
+    pc = adds(vfloor(pcl / vsz), 0.5f) * vsz;
+  }
+}
+
+// traceVox (voxel.ts:121-202) with a configurable step cap: the walk, then the hit's voxShade
 template <class BS>
 __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restrict__ F, const float *__restrict__ unorm8,
                                           f3 o, f3 d, float t0, float t1,
@@ -235,106 +308,18 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
                                           const float4 *inv_pre = nullptr) {
   out.rad = mk(0.0f, 0.0f, 0.0f); out.T = 1.0f; out.lvl = GI_EMPTY; out.ptr = GI_EMPTY; out.bit = 0; out.tin = 0;
   out.steps = 0;
-  float vs = vox_size(v, L);
-  int G = (int)v.G;
-#if GI_X1
-  const f3 lo = mk(v.box_lo[L][0], v.box_lo[L][1], v.box_lo[L][2]), hi = mk(v.box_hi[L][0], v.box_hi[L][1], v.box_hi[L][2]);
-#else
-  f3 lo = (vi2f(org(v, L)) * vs) * 8.0f;
-  f3 hi = adds(lo, (float)G * vs * 8.0f);
-#endif
-  f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
-  f3 inv;
-  if (inv_pre) {   // the direction's 1 / dd, tabulated with the directions (the same IEEE quotients)
-    const float4 q = __ldg(inv_pre);
-    inv = mk(q.x, q.y, q.z);
-  } else {
-    inv = mk(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z);
-  }
-  f3 ta = (lo - o) * inv, tb = (hi - o) * inv;
-  f3 tn = vmin(ta, tb), tf = vmax(ta, tb);
-  float t = mx(mx(mx(tn.x, tn.y), tn.z), t0);
-  float tEnd = mn(mn(mn(tf.x, tf.y), tf.z), t1);
-  if (t >= tEnd) return;
-  i3 st = mki(dd.x > 0.0f ? 1 : -1, dd.y > 0.0f ? 1 : -1, dd.z > 0.0f ? 1 : -1);
-  f3 sp = mk(st.x > 0 ? 1.0f : 0.0f, st.y > 0 ? 1.0f : 0.0f, st.z > 0 ? 1.0f : 0.0f);
-  int nVox = G * 8;
-#if GI_X2
-  const float ivs = v.inv_vs[L];
-  i3 c;
-  {
-    const f3 x = (o + d * t) - lo;
-    c = mki(floor_div_clamp(x.x, vs, ivs, 0, nVox - 1), floor_div_clamp(x.y, vs, ivs, 0, nVox - 1),
-            floor_div_clamp(x.z, vs, ivs, 0, nVox - 1));
-  }
-#else
-  i3 c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(0, 0, 0), mki(nVox - 1, nVox - 1, nVox - 1));
-#endif
-  f3 tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
-  f3 tDelta = vabs(inv * vs);
-  float tIn = t;
-  const uint32_t Lbase = L * (uint32_t)(G * G * G);
-  for (uint32_t it = 0; it < cap; it++) {
-    out.steps++;
-    i3 b = mki(c.x >> 3, c.y >> 3, c.z >> 3);
-    uint32_t ptr = __ldg(&v.ptr[Lbase + ((uint32_t)b.z * (uint32_t)G + (uint32_t)b.y) * (uint32_t)G + (uint32_t)b.x]);
-    if (ptr == GI_DROP) {
-      uint3 r = vox_at(v, L, c);
-      if (r.x != GI_EMPTY && tIn >= tskip) {
-        // the coarser voxel that holds the cell: its size and centre
-        const float vl = vox_size(v, r.z);
-        const f3 pcl = lo + adds(vi2f(c), 0.5f) * vs;
-        const f3 pc = adds(vfloor(pcl / vl), 0.5f) * vl;
-        out.rad = shade_voxel(v, F, unorm8, r.x, r.y, d, o + d * tIn, pc, vl, bs); out.T = 0.0f;
-        out.lvl = r.z; out.ptr = r.x; out.bit = r.y; out.tin = __float_as_uint(tIn);
-        return;
-      }
-      float tx = mn(mn(tMax.x, tMax.y), tMax.z);
-      if (tx >= tEnd) break;
-      tIn = tx;
-      if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
-      else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
-      else { c.z += st.z; tMax.z += tDelta.z; }
-      if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
-      continue;
-    }
-    if (ptr >= GI_MARK) {
-      // empty brick: jump to its exit
-      f3 bt = (((vi2f(mki(b.x * 8, b.y * 8, b.z * 8)) + sp * 8.0f) * vs + lo) - o) * inv;
-      float te = mn(mn(bt.x, bt.y), bt.z);
-      if (te >= tEnd) break;
-      i3 nb = b;
-      if (bt.x <= bt.y && bt.x <= bt.z) nb.x += st.x; else if (bt.y <= bt.z) nb.y += st.y; else nb.z += st.z;
-      if (nb.x < 0 || nb.y < 0 || nb.z < 0 || nb.x >= G || nb.y >= G || nb.z >= G) break;
-      t = te; tIn = te;
-#if GI_X2
-      {
-        const f3 x = (o + d * t) - lo;
-        c = mki(floor_div_clamp(x.x, vs, ivs, nb.x * 8, nb.x * 8 + 7), floor_div_clamp(x.y, vs, ivs, nb.y * 8, nb.y * 8 + 7),
-                floor_div_clamp(x.z, vs, ivs, nb.z * 8, nb.z * 8 + 7));
-      }
-#else
-      c = iclamp3(vfloori(((o + d * t) - lo) / vs), mki(nb.x * 8, nb.y * 8, nb.z * 8),
-                  mki(nb.x * 8 + 7, nb.y * 8 + 7, nb.z * 8 + 7));
-#endif
-      tMax = (((vi2f(c) + sp) * vs + lo) - o) * inv;
-      continue;
-    }
-    uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
-    uint32_t occ = __ldg(&v.occ[ptr * 16u + (bit >> 5)]);
-    float tExit = mn(mn(tMax.x, tMax.y), tMax.z);
-    if ((occ & (1u << (bit & 31u))) != 0u && tIn >= tskip) {
-      out.rad = shade_voxel(v, F, unorm8, ptr, bit, d, o + d * tIn, lo + adds(vi2f(c), 0.5f) * vs, vs, bs); out.T = 0.0f;
-      out.lvl = L; out.ptr = ptr; out.bit = bit; out.tin = __float_as_uint(tIn);
-      return;
-    }
-    if (tExit >= tEnd) break;
-    tIn = tExit;
-    if (tMax.x <= tMax.y && tMax.x <= tMax.z) { c.x += st.x; tMax.x += tDelta.x; }
-    else if (tMax.y <= tMax.z) { c.y += st.y; tMax.y += tDelta.y; }
-    else { c.z += st.z; tMax.z += tDelta.z; }
-    if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= nVox || c.y >= nVox || c.z >= nVox) break;
-  }
+  Dda s;
+  if (!dda_begin(v, o, d, t0, t1, tskip, L, inv_pre, s)) return;
+  uint3 h = make_uint3(0u, 0u, 0u);
+  int k;
+  while ((k = dda_step(v, s, cap, h)) == DDA_WALK) {}
+  out.steps = s.steps;
+  if (k == DDA_MISS) return;
+  f3 pc;
+  float vsz;
+  dda_hit_voxel(v, s, k, h.z, pc, vsz);
+  out.rad = shade_voxel(v, F, unorm8, h.x, h.y, s.d, s.o + s.d * s.tIn, pc, vsz, bs); out.T = 0.0f;
+  out.lvl = h.z; out.ptr = h.x; out.bit = h.y; out.tin = __float_as_uint(s.tIn);
 }
 
 // voxLevel (rc.ts:210-213), round(log2) taken exactly
@@ -472,6 +457,219 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
       atomicAdd(&r.counts[24 + cur_c], tr); atomicAdd(&r.counts[32 + cur_c], sp); atomicAdd(&r.counts[64 + cur_c], cp);
     }
   }
+}
+
+// ---- giTrace as a wavefront inside each warp ------------------------------------------------------------------------
+// k_trace_wave: persistent warps.  A warp sets up 32 rays at a time with all its lanes (the probe, the voxel level, the
+// entry into the level's box: traceVox's set-up), queues their walks in a ring in shared memory and steps them: at
+// every iteration each lane whose walk has ended takes the next queued walk, so the lanes stay busy while walks of
+// very different lengths end, and a new batch is set up whenever fewer than 32 walks are queued.  A walk's outcome
+// (a miss, or the voxel hit and where the ray entered it) goes to trec; k_trace_shade then shades the hits with every
+// lane of a warp busy and writes the atlas.  Each ray takes traceVox's f32 operations in their order: only the
+// interleaving of rays over the lanes differs from one thread per ray.
+constexpr uint32_t WAVE_RING = 64;    // queued walks per warp (at most 31 + 32 are queued at once)
+constexpr uint32_t WAVE_WORDS = 13;   // words of a queued walk
+constexpr uint32_t WAVE_WARPS = 8;    // warps per block (256 threads)
+
+// The walk record of a ray (uint4): brick; kind (0 probe not valid, DDA_MISS, DDA_HIT, DDA_HIT_DROP) | trace level << 2
+// | hit level << 5 | bit << 8 | (cell z >> 10) << 17; the cell (x | y << 11 | (z & 1023) << 22); tIn bits
+__device__ __forceinline__ uint32_t cell_pack(i3 c) {
+  return (uint32_t)c.x | ((uint32_t)c.y << 11) | (((uint32_t)c.z & 1023u) << 22);
+}
+__device__ __forceinline__ i3 cell_unpack(uint32_t w, uint32_t zhi) {
+  return mki((int)(w & 2047u), (int)((w >> 11) & 2047u), (int)((w >> 22) | (zhi << 10)));
+}
+
+// trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) up to the walk: the atlas element of the ray at position j of
+// the trace order (cascade c), whether its probe is valid, and whether its interval enters the level's box (s set up)
+template <int A>
+__device__ __forceinline__ uint32_t wave_setup(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, bool &valid,
+                                               bool &walk, Dda &s) {
+  const CascDev &L = r.c[c];
+  uint32_t t = j - L.ray_off, pi, di;
+  if (r.trace_order == 0) {           // probe-major: the atlas order
+    pi = t >> L.dirs_log2;
+    di = t & ((1u << L.dirs_log2) - 1u);
+  } else {                            // direction-major: one direction over consecutive probes
+    di = t / L.np;
+    pi = t - di * L.np;
+  }
+  const float4 pos = r.probes[L.probe_off + pi].pos;
+  valid = pos.w > 0.0f;
+  walk = false;
+  if (valid) {
+    const float4 nrm = r.probes[L.probe_off + pi].nrm, dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
+    const f3 dir = mk(dv.x, dv.y, dv.z), po = ld3(pos), pn = ld3(nrm);
+    const float s0 = pos.w, t0 = L.b0 * s0, t1 = L.b1 * s0;
+    const uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
+    const float vs = vox_size(v, Lv);
+    walk = dda_begin(v, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.idirs + L.dir_off + di, s);
+  }
+  return L.ray_off + (pi << L.dirs_log2) + di;
+}
+
+// per-lane DDA counters (rc.ts:232-235), flushed when the lane's cascade changes
+struct WaveStats {
+  uint32_t steps = 0, traces = 0, cap = 0, c = 0xffffffffu;
+  __device__ __forceinline__ void add(const RcDev &r, uint32_t cc, uint32_t n) {
+    if (cc != c && c != 0xffffffffu) {
+      atomicAdd(&r.counts[24 + c], traces); atomicAdd(&r.counts[32 + c], steps); atomicAdd(&r.counts[64 + c], cap);
+      traces = steps = cap = 0;
+    }
+    c = cc;
+    traces++; steps += n; cap += n >= r.dda_cap ? 1u : 0u;
+  }
+  __device__ __forceinline__ void flush(const RcDev &r) {   // the whole warp, converged
+    const uint32_t lane = threadIdx.x & 31u;
+    const unsigned grp = __match_any_sync(0xffffffffu, c);
+    const uint32_t tr = __reduce_add_sync(grp, traces), sp = __reduce_add_sync(grp, steps), cp = __reduce_add_sync(grp, cap);
+    if (c != 0xffffffffu && (uint32_t)(__ffs(grp) - 1) == lane) {
+      atomicAdd(&r.counts[24 + c], tr); atomicAdd(&r.counts[32 + c], sp); atomicAdd(&r.counts[64 + c], cp);
+    }
+  }
+};
+
+template <int A>
+#ifndef GI_WAVE_MINB
+#define GI_WAVE_MINB 1
+#endif
+__global__ void __launch_bounds__(256, GI_WAVE_MINB) k_trace_wave(RcDev r, VoxDev v, uint32_t *ray_counter) {
+  __shared__ uint32_t ring[WAVE_WARPS][WAVE_WORDS][WAVE_RING];
+  grid_dep_wait();
+  const unsigned FULL = 0xffffffffu;
+  const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
+  uint32_t (*q)[WAVE_RING] = ring[threadIdx.x >> 5];
+  uint32_t head = 0, pending = 0;   // the warp's queue (the same in every lane)
+  bool more = true, act = false;
+  Dda s;                            // the lane's walk, its atlas element and cascade
+  uint32_t i = 0, c = 0;
+  WaveStats stats;
+  for (;;) {
+    if (more && pending < 32u) {
+      // set up the next 32 rays of the trace order; queue those whose interval enters the box
+      __syncwarp();
+      uint32_t base = 0;
+      if (lane == 0) base = atomicAdd(ray_counter, 32u);
+      base = __shfl_sync(FULL, base, 0);
+      if (base >= r.rays_total) {
+        more = false;
+      } else {
+        const uint32_t j = base + lane;
+        bool walk = false;
+        Dda t;
+        uint32_t ij = 0, cj = 0;
+        if (j < r.rays_total) {
+          cj = casc_of_ray(r, j);
+          bool valid;
+          ij = wave_setup<A>(r, v, j, cj, valid, walk, t);
+          if (!valid) r.trec[ij] = make_uint4(0u, 0u, 0u, 0u);
+          else if (!walk) {
+            r.trec[ij] = make_uint4(0u, (uint32_t)DDA_MISS, 0u, 0u);
+            if (r.stats) stats.add(r, cj, 0u);
+          }
+        }
+        const unsigned m = __ballot_sync(FULL, walk);
+        if (walk) {
+          const uint32_t k = (head + pending + (uint32_t)__popc(m & lt)) & (WAVE_RING - 1u);
+          q[0][k] = ij; q[1][k] = cj | (t.L << 3) | (((uint32_t)t.c.z >> 10) << 6); q[2][k] = t.steps;
+          q[3][k] = __float_as_uint(t.o.x); q[4][k] = __float_as_uint(t.o.y); q[5][k] = __float_as_uint(t.o.z);
+          q[6][k] = __float_as_uint(t.tEnd); q[7][k] = __float_as_uint(t.tskip); q[8][k] = __float_as_uint(t.tIn);
+          q[9][k] = cell_pack(t.c);
+          q[10][k] = __float_as_uint(t.tMax.x); q[11][k] = __float_as_uint(t.tMax.y); q[12][k] = __float_as_uint(t.tMax.z);
+        }
+        pending += (uint32_t)__popc(m);
+        __syncwarp();
+      }
+    }
+    // the lanes whose walk has ended take the next queued walks
+    const unsigned idle = __ballot_sync(FULL, !act);
+#ifndef GI_WAVE_R
+#define GI_WAVE_R 1
+#endif
+    if (pending != 0u && ((uint32_t)__popc(idle) >= GI_WAVE_R || idle == FULL)) {
+      const uint32_t take = min((uint32_t)__popc(idle), pending);
+      if (!act) {
+        const uint32_t rk = (uint32_t)__popc(idle & lt);
+        if (rk < take) {
+          const uint32_t k = (head + rk) & (WAVE_RING - 1u);
+          i = q[0][k];
+          const uint32_t meta = q[1][k];
+          c = meta & 7u;
+          s.L = (meta >> 3) & 7u;
+          s.steps = q[2][k];
+          s.o = mk(__uint_as_float(q[3][k]), __uint_as_float(q[4][k]), __uint_as_float(q[5][k]));
+          s.tEnd = __uint_as_float(q[6][k]); s.tskip = __uint_as_float(q[7][k]); s.tIn = __uint_as_float(q[8][k]);
+          s.c = cell_unpack(q[9][k], (meta >> 6) & 1u);
+          s.tMax = mk(__uint_as_float(q[10][k]), __uint_as_float(q[11][k]), __uint_as_float(q[12][k]));
+          const CascDev &L = r.c[c];
+          const uint32_t di = (i - L.ray_off) & ((1u << L.dirs_log2) - 1u);
+          const float4 dv = __ldg(&r.dirs[L.dir_off + di]), iv = __ldg(&r.idirs[L.dir_off + di]);
+          s.d = mk(dv.x, dv.y, dv.z);
+          s.inv = mk(iv.x, iv.y, iv.z);
+          dda_derived(v, s);
+          act = true;
+        }
+      }
+      head = (head + take) & (WAVE_RING - 1u);
+      pending -= take;
+    }
+    if (__ballot_sync(FULL, act) == 0u) {
+      if (!more && pending == 0u) break;
+      continue;
+    }
+    if (act) {
+      uint3 h = make_uint3(0u, 0u, 0u);
+      const int k = dda_step(v, s, r.dda_cap, h);
+      if (k != DDA_WALK) {
+        act = false;
+        if (r.stats) stats.add(r, c, s.steps);
+        r.trec[i] = k == DDA_MISS ? make_uint4(0u, (uint32_t)DDA_MISS | (s.L << 2), 0u, 0u)
+                                  : make_uint4(h.x, (uint32_t)k | (s.L << 2) | (h.z << 5) | (h.y << 8)
+                                                    | (((uint32_t)s.c.z >> 10) << 17), cell_pack(s.c), __float_as_uint(s.tIn));
+      }
+    }
+  }
+  if (r.stats) stats.flush(r);
+}
+
+// The hits of k_trace_wave shaded (voxShade, rc.ts:136-140) and every atlas element written, one thread per ray in
+// atlas order: the entry point and the shading voxel rebuilt from the walk record with traceWorld's operations.
+template <int A>
+__global__ void __launch_bounds__(256) k_trace_shade(RcDev r, VoxDev v) {
+  typedef typename Atlas<A>::T T;
+  grid_dep_wait();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= r.rays_total) return;
+  const uint4 w = r.trec[i];
+  const int kind = (int)(w.y & 3u);
+  f3 rad = mk(0.0f, 0.0f, 0.0f);
+  float tr = 1.0f;
+  uint4 hit = make_uint4(GI_EMPTY, GI_EMPTY, 0u, 0u);
+  if (kind >= DDA_HIT) {
+    const uint32_t c = casc_of_ray(r, i);
+    const CascDev &L = r.c[c];
+    const uint32_t t = i - L.ray_off, pi = t >> L.dirs_log2, di = t & ((1u << L.dirs_log2) - 1u);
+    const float4 pos = r.probes[L.probe_off + pi].pos, nrm = r.probes[L.probe_off + pi].nrm;
+    const float4 dv = __ldg(&r.dirs[L.dir_off + di]);
+    Dda s;
+    s.L = (w.y >> 2) & 7u;
+    s.vs = vox_size(v, s.L);
+    s.lo = mk(v.box_lo[s.L][0], v.box_lo[s.L][1], v.box_lo[s.L][2]);
+    s.c = cell_unpack(w.z, (w.y >> 17) & 1u);
+    s.tIn = __uint_as_float(w.w);
+    s.d = mk(dv.x, dv.y, dv.z);
+    s.o = ld3(pos) + ld3(nrm) * (r.vox_offset * s.vs);
+    const uint32_t hl = (w.y >> 5) & 7u, bit = (w.y >> 8) & 511u;
+    f3 pc;
+    float vsz;
+    dda_hit_voxel(v, s, kind, hl, pc, vsz);
+    rad = shade_voxel(v, r.frame, r.unorm8, w.x, bit, s.d, s.o + s.d * s.tIn, pc, vsz, InjectedBounce{r.bn_inj});
+    tr = 0.0f;
+    hit = make_uint4(hl, w.x, bit, w.w);
+  }
+  Atlas<A>::store(reinterpret_cast<T *>(r.rad), i, make_float4(rad.x, rad.y, rad.z, tr));
+  if (r.hits) r.hits[i] = hit;
+  if (r.rad_traced) Atlas<A>::store(reinterpret_cast<T *>(r.rad_traced), i, make_float4(rad.x, rad.y, rad.z, tr));
 }
 
 __device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
@@ -1081,7 +1279,12 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
+#if GI_WAVE
+  GI_TRY(gi_launch(k_trace_wave<A>, tb, 256, st, r, v, counter));
+  GI_TRY(gi_launch(k_trace_shade<A>, (r.rays_total + 255u) / 256u, 256, st, r, v));
+#else
   GI_TRY(gi_launch(k_trace<A>, tb, 256, st, r, v, counter));
+#endif
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];

@@ -300,7 +300,7 @@ __global__ void __launch_bounds__(256) k_alloc_bricks(VoxDev v, uint32_t kpt, ui
   uint32_t ex = block_scan_256(c, &tot);
   __shared__ uint32_t s_pre;
   if (threadIdx.x == 0) {
-    uint32_t pre = chain_prefix(v.look, blk, tot, v.hdr);
+    uint32_t pre = chain_prefix(v.look, blk, tot, v.hdr, v.scan_hold);
     s_pre = pre;
     if (blk == nblocks - 1u) { v.hdr[0] = pre + tot; v.hdr[5] = pre + tot; }
   }
@@ -679,6 +679,7 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
         if (bit == 0u) r -= pc;
       }
     }
+    if (bit == 0u) continue;   // rank past the brick's voxels: only after a scan that gave up (header word 6)
     bit -= 1u;
     uint32_t code = v.code[ptr];
     uint32_t L = code >> 27;

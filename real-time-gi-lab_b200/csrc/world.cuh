@@ -208,7 +208,7 @@ __global__ void k_w_clear(RcDev r, WorldDev w) {
 // history parity flips here (Rc.encode, rc.ts:1180), after k_w_clear has read it.
 __global__ void __launch_bounds__(256) k_w_register_pixels(RcDev r, WorldDev w) {
   grid_dep_wait();
-  if (blockIdx.x == 0 && threadIdx.x == 0) { w.state[0] ^= 1u; w.state[16] = 0u; }
+  if (blockIdx.x == 0 && threadIdx.x == 0) { w.state[0] ^= 1u; w.state[16] = 0u; w.state[7] = 0u; }
   const float *F = r.frame;
   const uint32_t st = max(reinterpret_cast<const uint32_t *>(F)[F_RU + 2], 1u);
   const uint32_t sx = (r.width + st - 1u) / st, sy = (r.height + st - 1u) / st;

@@ -30,6 +30,7 @@ SIGNATURES = {
     "gi_vox_update": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "gi_vox_build": (C.c_int, [_P, _P]),
     "gi_vox_read_counters": (C.c_int, [_P, _P, _P]),
+    "gi_vox_debug_hold_scan": (C.c_int, [_P, C.c_int32]),
     "gi_vox_used_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
     "gi_vox_read_state": (C.c_int, [_P, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     "gi_vox_destroy": (C.c_int, [_P]),

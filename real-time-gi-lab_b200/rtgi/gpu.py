@@ -156,6 +156,11 @@ class VoxWorld:
                 "bigOverflow": int(hdr[3]), "voxelOverflow": int(hdr[4]), "bricksPerLevel": [int(x) for x in hdr[8:8 + NL]],
                 "bigPerLevel": [int(x) for x in hdr[16:16 + NL]], "hdr": hdr}
 
+    def debug_hold_scan(self, part: int) -> None:
+        """Test hook (gi_vox_debug_hold_scan): part `part` of the next rebuilds' brick scan publishes nothing, so the
+        bounded wait after it gives up and read_counters raises GiError(GI_ERR_TIMEOUT); part < 0 turns it off."""
+        _lib.call("gi_vox_debug_hold_scan", self.handle, int(part))
+
     def used_bytes(self) -> dict:
         a, b = C.c_uint64(), C.c_uint64()
         _lib.call("gi_vox_used_bytes", self.handle, C.byref(a), C.byref(b))
