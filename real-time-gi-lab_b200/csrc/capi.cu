@@ -192,7 +192,6 @@ static void free_rc(gi_rc *r) {
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
-  cudaFree(r->dev.trec);
   cudaFree((void *)r->dev.unorm8);
   cudaFree(r->shadow); cudaFree(r->sm_rec); cudaFree(r->sm_pre); cudaFree(r->sm_sums); cudaFree(r->sm_counter);
   cudaFree((void *)r->bn.dirs); cudaFree(r->bn.vol[0]); cudaFree(r->bn.vol[1]); cudaFree(r->bn.list); cudaFree(r->bn.inj);
@@ -756,7 +755,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
       (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->sh_elem_bytes)) ||
       (e = cudaMalloc(&irr, npx * r->irr_elem_bytes)) || (e = dalloc(&counts, 96)) ||
-      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, 2u * dir_total)) || (e = dalloc(&d.trec, ray_total))) {
+      (e = dalloc(&plevel, probe_total)) || (e = dalloc(&dirs, 2u * dir_total))) {
     d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
     free_rc(r);
     delete r;
@@ -803,7 +802,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
     delete r;
     return cuda_fail(e, "gi_rc_create: direction table");
   }
-  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 32 + ray_total * (r->rad_elem_bytes + 16u) +
+  r->bytes = r->mavg_bytes + 160 * 4 + npx * (4 + 8 + 16) + (uint64_t)r->ntiles * 8u + 4u + probe_total * 52 + dir_total * 32 + ray_total * r->rad_elem_bytes +
              r->sh_elems * r->sh_elem_bytes + npx * r->irr_elem_bytes + 96 * 4;
   if (wp) {
     WorldDev &w = r->w;

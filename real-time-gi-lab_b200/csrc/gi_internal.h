@@ -44,7 +44,6 @@ struct RcDev {
   uint32_t *counts;        // 80 words
   uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
   void *rad_traced;        // optional: copy of the atlas after the trace
-  uint4 *trec;             // per ray (atlas order) the outcome of its walk, read by the shading pass (k_trace_shade)
   float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
   const float *unorm8;     // [k] = k / 255.0f, [256 + k] = (k / 255.0f) / pi for k = 0..255 (IEEE quotients, host)
   const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)

@@ -195,8 +195,9 @@ __device__ __forceinline__ f3 shade_voxel(const VoxDev &v, const float *__restri
 
 struct TraceOut { f3 rad; float T; uint32_t lvl, ptr, bit, tin, steps; };
 
-// traceVox (voxel.ts:121-202) split into its set-up and one iteration of its loop, so that a walk can be suspended
-// between iterations and resumed by another lane.  The f32 operations and their order are the reference's.
+// traceVox (voxel.ts:121-202) as its set-up and one iteration of its loop; the f32 operations and their order are the
+// reference's.  The box of each level and 1 / d come from tables (VoxDev.box_lo/box_hi, RcDev.idirs) holding the
+// same numbers.
 struct Dda {
   f3 o, d, inv, lo, tMax, tDelta, sp;
   i3 c, st;
@@ -457,219 +458,6 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
       atomicAdd(&r.counts[24 + cur_c], tr); atomicAdd(&r.counts[32 + cur_c], sp); atomicAdd(&r.counts[64 + cur_c], cp);
     }
   }
-}
-
-// ---- giTrace as a wavefront inside each warp ------------------------------------------------------------------------
-// k_trace_wave: persistent warps.  A warp sets up 32 rays at a time with all its lanes (the probe, the voxel level, the
-// entry into the level's box: traceVox's set-up), queues their walks in a ring in shared memory and steps them: at
-// every iteration each lane whose walk has ended takes the next queued walk, so the lanes stay busy while walks of
-// very different lengths end, and a new batch is set up whenever fewer than 32 walks are queued.  A walk's outcome
-// (a miss, or the voxel hit and where the ray entered it) goes to trec; k_trace_shade then shades the hits with every
-// lane of a warp busy and writes the atlas.  Each ray takes traceVox's f32 operations in their order: only the
-// interleaving of rays over the lanes differs from one thread per ray.
-constexpr uint32_t WAVE_RING = 64;    // queued walks per warp (at most 31 + 32 are queued at once)
-constexpr uint32_t WAVE_WORDS = 13;   // words of a queued walk
-constexpr uint32_t WAVE_WARPS = 8;    // warps per block (256 threads)
-
-// The walk record of a ray (uint4): brick; kind (0 probe not valid, DDA_MISS, DDA_HIT, DDA_HIT_DROP) | trace level << 2
-// | hit level << 5 | bit << 8 | (cell z >> 10) << 17; the cell (x | y << 11 | (z & 1023) << 22); tIn bits
-__device__ __forceinline__ uint32_t cell_pack(i3 c) {
-  return (uint32_t)c.x | ((uint32_t)c.y << 11) | (((uint32_t)c.z & 1023u) << 22);
-}
-__device__ __forceinline__ i3 cell_unpack(uint32_t w, uint32_t zhi) {
-  return mki((int)(w & 2047u), (int)((w >> 11) & 2047u), (int)((w >> 22) | (zhi << 10)));
-}
-
-// trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) up to the walk: the atlas element of the ray at position j of
-// the trace order (cascade c), whether its probe is valid, and whether its interval enters the level's box (s set up)
-template <int A>
-__device__ __forceinline__ uint32_t wave_setup(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, bool &valid,
-                                               bool &walk, Dda &s) {
-  const CascDev &L = r.c[c];
-  uint32_t t = j - L.ray_off, pi, di;
-  if (r.trace_order == 0) {           // probe-major: the atlas order
-    pi = t >> L.dirs_log2;
-    di = t & ((1u << L.dirs_log2) - 1u);
-  } else {                            // direction-major: one direction over consecutive probes
-    di = t / L.np;
-    pi = t - di * L.np;
-  }
-  const float4 pos = r.probes[L.probe_off + pi].pos;
-  valid = pos.w > 0.0f;
-  walk = false;
-  if (valid) {
-    const float4 nrm = r.probes[L.probe_off + pi].nrm, dv = r.dirs[L.dir_off + di];   // dirOf(di, res), tabulated
-    const f3 dir = mk(dv.x, dv.y, dv.z), po = ld3(pos), pn = ld3(nrm);
-    const float s0 = pos.w, t0 = L.b0 * s0, t1 = L.b1 * s0;
-    const uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
-    const float vs = vox_size(v, Lv);
-    walk = dda_begin(v, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.idirs + L.dir_off + di, s);
-  }
-  return L.ray_off + (pi << L.dirs_log2) + di;
-}
-
-// per-lane DDA counters (rc.ts:232-235), flushed when the lane's cascade changes
-struct WaveStats {
-  uint32_t steps = 0, traces = 0, cap = 0, c = 0xffffffffu;
-  __device__ __forceinline__ void add(const RcDev &r, uint32_t cc, uint32_t n) {
-    if (cc != c && c != 0xffffffffu) {
-      atomicAdd(&r.counts[24 + c], traces); atomicAdd(&r.counts[32 + c], steps); atomicAdd(&r.counts[64 + c], cap);
-      traces = steps = cap = 0;
-    }
-    c = cc;
-    traces++; steps += n; cap += n >= r.dda_cap ? 1u : 0u;
-  }
-  __device__ __forceinline__ void flush(const RcDev &r) {   // the whole warp, converged
-    const uint32_t lane = threadIdx.x & 31u;
-    const unsigned grp = __match_any_sync(0xffffffffu, c);
-    const uint32_t tr = __reduce_add_sync(grp, traces), sp = __reduce_add_sync(grp, steps), cp = __reduce_add_sync(grp, cap);
-    if (c != 0xffffffffu && (uint32_t)(__ffs(grp) - 1) == lane) {
-      atomicAdd(&r.counts[24 + c], tr); atomicAdd(&r.counts[32 + c], sp); atomicAdd(&r.counts[64 + c], cp);
-    }
-  }
-};
-
-template <int A>
-#ifndef GI_WAVE_MINB
-#define GI_WAVE_MINB 1
-#endif
-__global__ void __launch_bounds__(256, GI_WAVE_MINB) k_trace_wave(RcDev r, VoxDev v, uint32_t *ray_counter) {
-  __shared__ uint32_t ring[WAVE_WARPS][WAVE_WORDS][WAVE_RING];
-  grid_dep_wait();
-  const unsigned FULL = 0xffffffffu;
-  const uint32_t lane = threadIdx.x & 31u, lt = (1u << lane) - 1u;
-  uint32_t (*q)[WAVE_RING] = ring[threadIdx.x >> 5];
-  uint32_t head = 0, pending = 0;   // the warp's queue (the same in every lane)
-  bool more = true, act = false;
-  Dda s;                            // the lane's walk, its atlas element and cascade
-  uint32_t i = 0, c = 0;
-  WaveStats stats;
-  for (;;) {
-    if (more && pending < 32u) {
-      // set up the next 32 rays of the trace order; queue those whose interval enters the box
-      __syncwarp();
-      uint32_t base = 0;
-      if (lane == 0) base = atomicAdd(ray_counter, 32u);
-      base = __shfl_sync(FULL, base, 0);
-      if (base >= r.rays_total) {
-        more = false;
-      } else {
-        const uint32_t j = base + lane;
-        bool walk = false;
-        Dda t;
-        uint32_t ij = 0, cj = 0;
-        if (j < r.rays_total) {
-          cj = casc_of_ray(r, j);
-          bool valid;
-          ij = wave_setup<A>(r, v, j, cj, valid, walk, t);
-          if (!valid) r.trec[ij] = make_uint4(0u, 0u, 0u, 0u);
-          else if (!walk) {
-            r.trec[ij] = make_uint4(0u, (uint32_t)DDA_MISS, 0u, 0u);
-            if (r.stats) stats.add(r, cj, 0u);
-          }
-        }
-        const unsigned m = __ballot_sync(FULL, walk);
-        if (walk) {
-          const uint32_t k = (head + pending + (uint32_t)__popc(m & lt)) & (WAVE_RING - 1u);
-          q[0][k] = ij; q[1][k] = cj | (t.L << 3) | (((uint32_t)t.c.z >> 10) << 6); q[2][k] = t.steps;
-          q[3][k] = __float_as_uint(t.o.x); q[4][k] = __float_as_uint(t.o.y); q[5][k] = __float_as_uint(t.o.z);
-          q[6][k] = __float_as_uint(t.tEnd); q[7][k] = __float_as_uint(t.tskip); q[8][k] = __float_as_uint(t.tIn);
-          q[9][k] = cell_pack(t.c);
-          q[10][k] = __float_as_uint(t.tMax.x); q[11][k] = __float_as_uint(t.tMax.y); q[12][k] = __float_as_uint(t.tMax.z);
-        }
-        pending += (uint32_t)__popc(m);
-        __syncwarp();
-      }
-    }
-    // the lanes whose walk has ended take the next queued walks
-    const unsigned idle = __ballot_sync(FULL, !act);
-#ifndef GI_WAVE_R
-#define GI_WAVE_R 1
-#endif
-    if (pending != 0u && ((uint32_t)__popc(idle) >= GI_WAVE_R || idle == FULL)) {
-      const uint32_t take = min((uint32_t)__popc(idle), pending);
-      if (!act) {
-        const uint32_t rk = (uint32_t)__popc(idle & lt);
-        if (rk < take) {
-          const uint32_t k = (head + rk) & (WAVE_RING - 1u);
-          i = q[0][k];
-          const uint32_t meta = q[1][k];
-          c = meta & 7u;
-          s.L = (meta >> 3) & 7u;
-          s.steps = q[2][k];
-          s.o = mk(__uint_as_float(q[3][k]), __uint_as_float(q[4][k]), __uint_as_float(q[5][k]));
-          s.tEnd = __uint_as_float(q[6][k]); s.tskip = __uint_as_float(q[7][k]); s.tIn = __uint_as_float(q[8][k]);
-          s.c = cell_unpack(q[9][k], (meta >> 6) & 1u);
-          s.tMax = mk(__uint_as_float(q[10][k]), __uint_as_float(q[11][k]), __uint_as_float(q[12][k]));
-          const CascDev &L = r.c[c];
-          const uint32_t di = (i - L.ray_off) & ((1u << L.dirs_log2) - 1u);
-          const float4 dv = __ldg(&r.dirs[L.dir_off + di]), iv = __ldg(&r.idirs[L.dir_off + di]);
-          s.d = mk(dv.x, dv.y, dv.z);
-          s.inv = mk(iv.x, iv.y, iv.z);
-          dda_derived(v, s);
-          act = true;
-        }
-      }
-      head = (head + take) & (WAVE_RING - 1u);
-      pending -= take;
-    }
-    if (__ballot_sync(FULL, act) == 0u) {
-      if (!more && pending == 0u) break;
-      continue;
-    }
-    if (act) {
-      uint3 h = make_uint3(0u, 0u, 0u);
-      const int k = dda_step(v, s, r.dda_cap, h);
-      if (k != DDA_WALK) {
-        act = false;
-        if (r.stats) stats.add(r, c, s.steps);
-        r.trec[i] = k == DDA_MISS ? make_uint4(0u, (uint32_t)DDA_MISS | (s.L << 2), 0u, 0u)
-                                  : make_uint4(h.x, (uint32_t)k | (s.L << 2) | (h.z << 5) | (h.y << 8)
-                                                    | (((uint32_t)s.c.z >> 10) << 17), cell_pack(s.c), __float_as_uint(s.tIn));
-      }
-    }
-  }
-  if (r.stats) stats.flush(r);
-}
-
-// The hits of k_trace_wave shaded (voxShade, rc.ts:136-140) and every atlas element written, one thread per ray in
-// atlas order: the entry point and the shading voxel rebuilt from the walk record with traceWorld's operations.
-template <int A>
-__global__ void __launch_bounds__(256) k_trace_shade(RcDev r, VoxDev v) {
-  typedef typename Atlas<A>::T T;
-  grid_dep_wait();
-  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= r.rays_total) return;
-  const uint4 w = r.trec[i];
-  const int kind = (int)(w.y & 3u);
-  f3 rad = mk(0.0f, 0.0f, 0.0f);
-  float tr = 1.0f;
-  uint4 hit = make_uint4(GI_EMPTY, GI_EMPTY, 0u, 0u);
-  if (kind >= DDA_HIT) {
-    const uint32_t c = casc_of_ray(r, i);
-    const CascDev &L = r.c[c];
-    const uint32_t t = i - L.ray_off, pi = t >> L.dirs_log2, di = t & ((1u << L.dirs_log2) - 1u);
-    const float4 pos = r.probes[L.probe_off + pi].pos, nrm = r.probes[L.probe_off + pi].nrm;
-    const float4 dv = __ldg(&r.dirs[L.dir_off + di]);
-    Dda s;
-    s.L = (w.y >> 2) & 7u;
-    s.vs = vox_size(v, s.L);
-    s.lo = mk(v.box_lo[s.L][0], v.box_lo[s.L][1], v.box_lo[s.L][2]);
-    s.c = cell_unpack(w.z, (w.y >> 17) & 1u);
-    s.tIn = __uint_as_float(w.w);
-    s.d = mk(dv.x, dv.y, dv.z);
-    s.o = ld3(pos) + ld3(nrm) * (r.vox_offset * s.vs);
-    const uint32_t hl = (w.y >> 5) & 7u, bit = (w.y >> 8) & 511u;
-    f3 pc;
-    float vsz;
-    dda_hit_voxel(v, s, kind, hl, pc, vsz);
-    rad = shade_voxel(v, r.frame, r.unorm8, w.x, bit, s.d, s.o + s.d * s.tIn, pc, vsz, InjectedBounce{r.bn_inj});
-    tr = 0.0f;
-    hit = make_uint4(hl, w.x, bit, w.w);
-  }
-  Atlas<A>::store(reinterpret_cast<T *>(r.rad), i, make_float4(rad.x, rad.y, rad.z, tr));
-  if (r.hits) r.hits[i] = hit;
-  if (r.rad_traced) Atlas<A>::store(reinterpret_cast<T *>(r.rad_traced), i, make_float4(rad.x, rad.y, rad.z, tr));
 }
 
 __device__ __forceinline__ void sh_basis(f3 n, float y[9]) {
@@ -1279,12 +1067,7 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
-#if GI_WAVE
-  GI_TRY(gi_launch(k_trace_wave<A>, tb, 256, st, r, v, counter));
-  GI_TRY(gi_launch(k_trace_shade<A>, (r.rays_total + 255u) / 256u, 256, st, r, v));
-#else
   GI_TRY(gi_launch(k_trace<A>, tb, 256, st, r, v, counter));
-#endif
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
