@@ -19,6 +19,7 @@ class Case:
     rc: configs.RcParams
     frame: np.ndarray = field(default=None)
     shadow: int = 0          # sun shadow map size (0: none, every voxel's sun visibility 1)
+    movers: tuple = None     # (rtgi.movers.MovingObjects, t): objects posed on the device before the G-buffer
 
 
 def _frame(scene, W, H, p: configs.RcParams, sun_e=None, sky=None, shadow=False):
@@ -121,4 +122,83 @@ def overflow(atlas: str = "f32") -> Case:
     c = room_lit(atlas)
     c.name = "overflow"
     c.vox = configs.vox_params({"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 300, "maxVoxels": 20000})
+    return c
+
+
+def batch_shape(name: str, seed: int, tris: int, G: int, levels: int, v0: float, W: int, H: int, cascades: int,
+                atlas: str) -> Case:
+    """A solve of the batching / serving distribution (rtgi.batch.solve_params): the procedural box/column mix, its
+    clipmap shape, resolution and cascade count."""
+    s = scenes.mixed_scene(seed, tris)
+    p = configs.parse_config(f"screen-8-voxel-{atlas}-dda256", {"cascades": cascades})
+    v = configs.vox_params({"v0": v0, "levels": levels, "G": G, "maxBricks": min(levels * G ** 3, 32768),
+                            "maxVoxels": 1 << 21})
+    c = Case(name, s, W, H, v, p)
+    c.frame = _frame(s, W, H, p)
+    return c
+
+
+def batch_g4_l1() -> Case:
+    return batch_shape("batch-g4-l1", 7, 20_000, 4, 1, 0.2, 320, 180, 2, "f32")
+
+
+def batch_g4_l4() -> Case:
+    return batch_shape("batch-g4-l4", 8, 30_000, 4, 4, 0.15, 320, 180, 4, "f16")
+
+
+def batch_g32_l1() -> Case:
+    return batch_shape("batch-g32-l1", 9, 40_000, 32, 1, 0.1, 480, 270, 3, "f32")
+
+
+def batch_g32_l4() -> Case:
+    """4 levels of 256^3 voxels (131,072 brick pointers per rebuild), f16 atlas, 5 cascades."""
+    return batch_shape("batch-g32-l4", 10, 60_000, 32, 4, 0.1, 480, 270, 5, "f16")
+
+
+def posed(scene: scenes.Scene, objs, t: float) -> scenes.Scene:
+    """The scene with its moving objects posed at t as gi_scene_rigid_apply poses them on the device: each vertex
+    through its object's 3x4 transform, ((m0 x + m1 y) + m2 z) + m3 in f32 per row."""
+    import dataclasses
+    m = objs.transforms(t)
+    per, n = objs.per, objs.centres.shape[0]
+    P = scene.positions.astype(np.float32).copy()
+    N = scene.normals.astype(np.float32).copy()
+    rest_p = P[objs.first:objs.first + per * n].reshape(n, per, 3)
+    rest_n = N[objs.first:objs.first + per * n].reshape(n, per, 3)
+    M = m.reshape(n, 1, 12)
+    out_p = np.empty_like(rest_p)
+    out_n = np.empty_like(rest_n)
+    for r in range(3):
+        out_p[..., r] = ((M[..., 4 * r] * rest_p[..., 0] + M[..., 4 * r + 1] * rest_p[..., 1])
+                         + M[..., 4 * r + 2] * rest_p[..., 2]) + M[..., 4 * r + 3]
+        out_n[..., r] = (M[..., 4 * r] * rest_n[..., 0] + M[..., 4 * r + 1] * rest_n[..., 1]) + M[..., 4 * r + 2] * rest_n[..., 2]
+    P[objs.first:objs.first + per * n] = out_p.reshape(-1, 3)
+    N[objs.first:objs.first + per * n] = out_n.reshape(-1, 3)
+    return dataclasses.replace(scene, positions=P, normals=N)
+
+
+def movers_f16() -> Case:
+    """A serving request: the box/column mix with 80 moving boxes posed on the device (gi_scene_rigid_apply) at
+    t = 0.6 s, f16 atlas, 2 levels of 128^3, 320 x 180, 3 cascades.  The oracle gets the same poses from `posed`."""
+    from rtgi import movers
+    base = scenes.mixed_scene(5, 25_000)
+    s, objs = movers.with_moving_boxes(base, 80, scenes.PCG32(17, stream=3))
+    c = batch_shape("movers-f16", 5, 25_000, 16, 2, 0.1, 320, 180, 3, "f16")
+    c.scene, c.movers = s, (objs, 0.6)
+    c.frame = _frame(s, c.width, c.height, c.rc)
+    return c
+
+
+def toon(style: bool = True, atlas: str = "f32") -> Case:
+    """room_lit with every other box material toon (flag 4): their hits inject style.ts's emission-side operator
+    (toonSun, rc.ts:114) while the frame's style word is on, Lambert when it is off."""
+    import dataclasses
+    c = room_lit(atlas)
+    mats = [dataclasses.replace(m, flags=m.flags | scenes.FLAG_TOON) if m.name.startswith("box") and i % 2 else m
+            for i, m in enumerate(c.scene.materials)]
+    c.scene = dataclasses.replace(c.scene, materials=mats)
+    c.name = "toon" if style else "toon-style-off"
+    c.frame = _frame(c.scene, c.width, c.height, c.rc, sun_e=fr.SUN_E, sky=fr.SKY)
+    if not style:
+        c.frame[136] = 0.0
     return c

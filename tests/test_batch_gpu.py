@@ -68,6 +68,18 @@ def test_batch_equals_solves_alone():
         for i, x in enumerate(solves):
             got = x.rc.read_irradiance(stream)
             assert np.array_equal(got.view(np.uint32), alone[i].view(np.uint32)), f"solve {i} differs pass by pass (launch {rep})"
+    # and every solve of the batch against the oracle, on the oracle's own G-buffer (the batched pass kernels:
+    # k_setup_batch, k_trace_batch, k_merge_batch, k_gather_batch)
+    from oracle import bind
+    from rtgi import configs
+    for i, x in enumerate(solves):
+        W, H = x.spec["width"], x.spec["height"]
+        p, v = batch.solve_params(x.spec)
+        depth, normal, _ = bind.raster_gbuffer(x.scene, x.frame, W, H)
+        st = bind.vox_build(x.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, x.scene.camera.eye)
+        o = bind.rc_solve(st, configs.cascade_layout(p, W, H), x.frame, depth, normal)
+        got = x.rc.read_irradiance(stream)
+        assert np.array_equal(got.view(np.uint32), o["irr"].view(np.uint32)), f"solve {i} differs from the oracle"
     b.destroy()
     for x in solves:
         x.destroy()

@@ -39,6 +39,11 @@ def _close(a, b, rel, what):
 
 def run_gpu(ctx, case, debug=True):
     sg = gpu.SceneGpu(ctx, case.scene)
+    if case.movers:   # pose the moving objects on the device, as the serving loop does
+        objs, t = case.movers
+        sg.rigid_define(objs.first, objs.per, objs.centres.shape[0])
+        sg.rigid_upload(objs.transforms(t))
+        sg.rigid_apply()
     vw = gpu.VoxWorld(sg, case.vox)
     rc = gpu.Rc(ctx, case.rc, case.width, case.height)
     rc.set_frame(case.frame)
@@ -63,9 +68,13 @@ def run_gpu(ctx, case, debug=True):
     return res
 
 
+def oracle_scene(case):
+    return gi_cases.posed(case.scene, *case.movers) if case.movers else case.scene
+
+
 def run_oracle(case, depth, normal, shadow=None):
     v = case.vox
-    st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+    st = bind.vox_build(oracle_scene(case), v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
     if shadow is not None:
         bind.vox_sun(st, case.frame, shadow)
     lay = dict(gi_cases.configs.cascade_layout(case.rc, case.width, case.height))
@@ -77,7 +86,10 @@ CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_
          "leak_sun": gi_cases.leak_sun, "empty": gi_cases.empty, "single_triangle": gi_cases.single_triangle,
          "tiny": gi_cases.tiny,
          "room_lit_f32out": lambda: gi_cases.room_lit("f16-f32out"),
-         "overflow": gi_cases.overflow, "config1": gi_cases.config1}
+         "overflow": gi_cases.overflow, "config1": gi_cases.config1,
+         "batch_g4_l1": gi_cases.batch_g4_l1, "batch_g4_l4": gi_cases.batch_g4_l4,
+         "batch_g32_l1": gi_cases.batch_g32_l1, "batch_g32_l4": gi_cases.batch_g32_l4,
+         "movers_f16": gi_cases.movers_f16, "toon": gi_cases.toon, "toon_style_off": lambda: gi_cases.toon(False)}
 
 
 @pytest.mark.parametrize("name", list(CASES))
@@ -85,12 +97,12 @@ def test_parity(ctx, name):
     case = CASES[name]()
     g = run_gpu(ctx, case)
     # G-buffer: the GPU raster against the oracle's, bit for bit
-    depth, normal, _ = bind.raster_gbuffer(case.scene, case.frame, case.width, case.height)
+    depth, normal, _ = bind.raster_gbuffer(oracle_scene(case), case.frame, case.width, case.height)
     assert np.array_equal(g["depth"].view(np.uint32), depth.view(np.uint32)), "G-buffer depth differs"
     assert np.array_equal(g["normal"].astype(np.float32), normal), "G-buffer normal differs"
     shadow = None
     if case.shadow:   # the sun shadow map, bit for bit
-        shadow = bind.shadow_render(case.scene, case.frame, case.shadow)
+        shadow = bind.shadow_render(oracle_scene(case), case.frame, case.shadow)
         assert np.array_equal(g["shadow"].view(np.uint32), shadow.view(np.uint32)), \
             f"shadow map differs at {(g['shadow'] != shadow).sum()} texels"
         assert (shadow < 1.0).any() or case.scene.triangle_count == 0
@@ -110,6 +122,14 @@ def test_parity(ctx, name):
         sv = st["sunvis"][:nv]
         if case.name.startswith("leak") or case.name == "config1":
             assert (sv == 0.0).any() and (sv == 1.0).any(), "the case should hold shadowed and lit voxels"
+    if case.name.startswith("toon"):   # the toon branch is reached: toon voxels (albedo alpha 255) are hit
+        toon_vox = (gv["attr"][0:nv * 4:4] >> 24) == 255
+        assert toon_vox.any() and not toon_vox.all()
+        toon_hits = (g["hits"][:, 1] != 0xffffffff) & (g["hits"][:, 0] != 0xffffffff)
+        assert toon_hits.any()
+    if case.movers:
+        objs, t = case.movers
+        assert not np.array_equal(oracle_scene(case).positions, case.scene.positions)
     # probes and DDA hits
     assert np.array_equal(g["probes"].view(np.uint32), o["probes"].view(np.uint32)), "probes differ"
     assert np.array_equal(g["hits"], o["hit"]), f"DDA hits differ at {np.argwhere((g['hits'] != o['hit']).any(1))[:5].ravel()}"
