@@ -9,6 +9,7 @@
 #include <stdlib.h>
 #include "gi_oracle.h"
 #include "orc_math.h"
+#include "orc_par.h"
 
 #define BIG 8u
 
@@ -144,7 +145,42 @@ static surf_t surface_at(const orc_scene *s, const tri_t *T, v3 p, int want_attr
   return r;
 }
 
-static void mark_brick(orc_vox *vx, uint32_t i) { if (vx->ptr[i] == ORC_EMPTY) vx->ptr[i] = ORC_MARK; }
+/* The triangle passes run on every host thread (orc_parallel).  Their writes commute: a mark sets EMPTY to MARK, an
+ * occupancy word takes an OR, a representative the larger key, so atomics give the sequential result whatever the
+ * order; the big-triangle lists are collected per chunk of threads and appended in chunk order, the sequential
+ * loop's order. */
+static void mark_brick(orc_vox *vx, uint32_t i) {
+  uint32_t e = ORC_EMPTY;
+  __atomic_compare_exchange_n(&vx->ptr[i], &e, ORC_MARK, 0, __ATOMIC_RELAXED, __ATOMIC_RELAXED);
+}
+static void atomic_max_u32(uint32_t *p, uint32_t v) {
+  uint32_t cur = __atomic_load_n(p, __ATOMIC_RELAXED);
+  while (cur < v && !__atomic_compare_exchange_n(p, &cur, v, 1, __ATOMIC_RELAXED, __ATOMIC_RELAXED)) {}
+}
+
+/* (triangle, level) pairs of one chunk of a triangle pass bound for the big lists */
+typedef struct { uint32_t *t, n, cap; } biglist_t;
+static void big_push(biglist_t *b, uint32_t t, uint32_t L) {
+  if (b->n + 2u > b->cap) {
+    b->cap = b->cap ? 2u * b->cap : 256u;
+    b->t = (uint32_t *)realloc(b->t, (size_t)b->cap * 4u);
+  }
+  b->t[b->n++] = t; b->t[b->n++] = L;
+}
+/* appends the chunks' pairs in chunk order to the lists at big + (list0 + L) * cap, counting into hdr[cnt0 + L] */
+static void big_merge(orc_vox *vx, biglist_t *ch, uint64_t nch, uint32_t list0, uint32_t cnt0) {
+  const uint32_t cap = vx->big_cap;
+  for (uint64_t c = 0; c < nch; c++) {
+    for (uint32_t j = 0; j < ch[c].n; j += 2u) {
+      uint32_t t = ch[c].t[j], L = ch[c].t[j + 1u];
+      uint32_t k = vx->hdr[cnt0 + L]++;
+      if (k < cap) vx->big[(list0 + L) * cap + k] = t; else vx->hdr[3]++;
+    }
+    free(ch[c].t);
+  }
+  free(ch);
+}
+#define TRI_GRAIN 512u
 
 /* markRange (voxel.ts:348-358), all of the range's bricks */
 static void mark_range(orc_vox *vx, const tri_t *T, uint32_t L, range_t r) {
@@ -174,168 +210,151 @@ static void voxelize_one(const orc_scene *s, orc_vox *vx, const tri_t *T, uint32
   i3 l = I(c.x & 7, c.y & 7, c.z & 7);
   uint32_t bit = (uint32_t)(l.x + 8 * l.y + 64 * l.z);
   if (!surface_at(s, T, p, 0).ok) return;
-  vx->occ[ptr * 16u + (bit >> 5)] |= 1u << (bit & 31u);
-  uint32_t *rp = &vx->rep[ptr * 512u + bit];
-  if (*rp < t + 1u) *rp = t + 1u;
+  __atomic_fetch_or(&vx->occ[ptr * 16u + (bit >> 5)], 1u << (bit & 31u), __ATOMIC_RELAXED);
+  atomic_max_u32(&vx->rep[ptr * 512u + bit], t + 1u);
 }
 
-void orc_vox_origins(float v0, uint32_t levels, uint32_t G, const double eye[3], int32_t origin_out[8][4]) {
-  for (uint32_t L = 0; L < 8; L++) for (int a = 0; a < 4; a++) origin_out[L][a] = 0;
-  for (uint32_t L = 0; L < levels; L++) {
-    double bs = (double)v0 * ldexp(1.0, (int)L) * 8.0;   /* v0 * 2 ** L * 8 in the host's f64 */
-    for (int a = 0; a < 3; a++) origin_out[L][a] = (int32_t)floor(eye[a] / bs) - (int32_t)(G / 2);
-  }
-}
+typedef struct { const orc_scene *s; orc_vox *vx; biglist_t *ch; } tri_pass_t;
 
-int orc_vox_build(const orc_scene *s, orc_vox *vx) {
-  const uint32_t NL = vx->levels, G = vx->G, per = G * G * G, cap = vx->big_cap;
-  /* clear (voxel.ts:338) */
-  memset(vx->hdr, 0, ORC_HDR * 4);
-  for (uint32_t i = 0; i < NL * per; i++) vx->ptr[i] = ORC_EMPTY;
-
-  /* markBricks + markBricksBig (voxel.ts:359-387) */
-  for (uint32_t i = 0; i < threads_of(s); i++) {
-    uint32_t L0, t = work_at(s, i, &L0);
-    tri_t T = load_tri(s, t);
-    for (uint32_t L = L0; L < NL; L++) {
+/* markBricks (voxel.ts:359-372) over threads [b, e) */
+static void mark_pass(void *p, uint64_t b, uint64_t e) {
+  tri_pass_t *j = (tri_pass_t *)p;
+  orc_vox *vx = j->vx;
+  biglist_t *bl = &j->ch[b / TRI_GRAIN];
+  for (uint32_t i = (uint32_t)b; i < (uint32_t)e; i++) {
+    uint32_t L0, t = work_at(j->s, i, &L0);
+    tri_t T = load_tri(j->s, t);
+    for (uint32_t L = L0; L < vx->levels; L++) {
       range_t r = vox_range(vx, &T, L, vox_size(vx, L) * 8.0f);
       int32_t n = r.n.x * r.n.y * r.n.z;
       if (n == 0 || (!vx->coarse_from_triangles && finer_holds_range(vx, L, r, 8))) continue;
-      if (n > 8) {
-        uint32_t k = vx->hdr[24 + L]++;
-        if (k < cap) vx->big[(8u + L) * cap + k] = t; else vx->hdr[3]++;
-        continue;
-      }
+      if (n > 8) { big_push(bl, t, L); continue; }
       mark_range(vx, &T, L, r);
     }
   }
-  for (uint32_t L = 0; L < NL; L++) {
-    uint32_t n = vx->hdr[24 + L] < cap ? vx->hdr[24 + L] : cap;
-    for (uint32_t k = 0; k < n; k++) {
-      tri_t T = load_tri(s, vx->big[(8u + L) * cap + k]);
-      mark_range(vx, &T, L, vox_range(vx, &T, L, vox_size(vx, L) * 8.0f));
+}
+/* markBricksBig (voxel.ts:374-387): item k of the concatenated lists of every level */
+typedef struct { const orc_scene *s; orc_vox *vx; uint32_t list0, cnt0, off[9]; } big_pass_t;
+static void big_item(const big_pass_t *j, uint32_t k, uint32_t *L, uint32_t *t) {
+  uint32_t l = 0;
+  while (k >= j->off[l + 1u]) l++;
+  *L = l;
+  *t = j->vx->big[(j->list0 + l) * j->vx->big_cap + (k - j->off[l])];
+}
+static void big_pass_init(big_pass_t *j, const orc_scene *s, orc_vox *vx, uint32_t list0, uint32_t cnt0) {
+  j->s = s; j->vx = vx; j->list0 = list0; j->cnt0 = cnt0; j->off[0] = 0;
+  for (uint32_t L = 0; L < 8; L++) {
+    uint32_t n = L < vx->levels ? (vx->hdr[cnt0 + L] < vx->big_cap ? vx->hdr[cnt0 + L] : vx->big_cap) : 0u;
+    j->off[L + 1u] = j->off[L] + n;
+  }
+}
+static void mark_big_pass(void *p, uint64_t b, uint64_t e) {
+  big_pass_t *j = (big_pass_t *)p;
+  for (uint32_t k = (uint32_t)b; k < (uint32_t)e; k++) {
+    uint32_t L, t;
+    big_item(j, k, &L, &t);
+    tri_t T = load_tri(j->s, t);
+    mark_range(j->vx, &T, L, vox_range(j->vx, &T, L, vox_size(j->vx, L) * 8.0f));
+  }
+}
+/* voxBits (voxel.ts:492-512) over threads [b, e) */
+static void bits_pass(void *p, uint64_t b, uint64_t e) {
+  tri_pass_t *j = (tri_pass_t *)p;
+  orc_vox *vx = j->vx;
+  biglist_t *bl = &j->ch[b / TRI_GRAIN];
+  for (uint32_t i = (uint32_t)b; i < (uint32_t)e; i++) {
+    uint32_t L0, t = work_at(j->s, i, &L0);
+    tri_t T = load_tri(j->s, t);
+    for (uint32_t L = L0; L < vx->levels; L++) {
+      range_t r = vox_range(vx, &T, L, vox_size(vx, L));
+      int32_t n = r.n.x * r.n.y * r.n.z;
+      if (n == 0 || (!vx->coarse_from_triangles && finer_built_range(vx, L, r))) continue;
+      if ((uint32_t)n > BIG) { big_push(bl, t, L); continue; }
+      for (int32_t k = 0; k < n; k++)
+        voxelize_one(j->s, vx, &T, t, L, I(r.lo.x + k % r.n.x, r.lo.y + (k / r.n.x) % r.n.y, r.lo.z + k / (r.n.x * r.n.y)), n == 1);
     }
   }
-  /* markParents (voxel.ts:390-403) */
-  for (uint32_t i = 0; i < (NL - 1) * per; i++) {
-    if (vx->ptr[i] != ORC_MARK) continue;
+}
+/* voxBitsBig (voxel.ts:514-534) */
+static void bits_big_pass(void *p, uint64_t b, uint64_t e) {
+  big_pass_t *j = (big_pass_t *)p;
+  for (uint32_t k = (uint32_t)b; k < (uint32_t)e; k++) {
+    uint32_t L, t;
+    big_item(j, k, &L, &t);
+    tri_t T = load_tri(j->s, t);
+    range_t r = vox_range(j->vx, &T, L, vox_size(j->vx, L));
+    int32_t n = r.n.x * r.n.y * r.n.z;
+    for (int32_t q = 0; q < n; q++)
+      voxelize_one(j->s, j->vx, &T, t, L, I(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y)), 0);
+  }
+}
+/* markParents (voxel.ts:390-403) over pointers [b, e) */
+static void parents_pass(void *p, uint64_t b, uint64_t e) {
+  orc_vox *vx = (orc_vox *)p;
+  const uint32_t NL = vx->levels, G = vx->G, per = G * G * G;
+  for (uint32_t i = (uint32_t)b; i < (uint32_t)e; i++) {
+    if (__atomic_load_n(&vx->ptr[i], __ATOMIC_RELAXED) != ORC_MARK) continue;
     uint32_t L = i / per, r = i % per;
     i3 o = org(vx, L);
     i3 w = I(o.x + (int32_t)(r % G), o.y + (int32_t)((r / G) % G), o.z + (int32_t)(r / (G * G)));
     for (L++; L < NL; L++) {
       w = ishr(w, 1);
       i3 ol = org(vx, L);
-      i3 b = I(w.x - ol.x, w.y - ol.y, w.z - ol.z);
-      if (b.x < 0 || b.y < 0 || b.z < 0 || b.x >= (int32_t)G || b.y >= (int32_t)G || b.z >= (int32_t)G) break;
-      mark_brick(vx, ptr_index(vx, L, b));
+      i3 bb = I(w.x - ol.x, w.y - ol.y, w.z - ol.z);
+      if (bb.x < 0 || bb.y < 0 || bb.z < 0 || bb.x >= (int32_t)G || bb.y >= (int32_t)G || bb.z >= (int32_t)G) break;
+      mark_brick(vx, ptr_index(vx, L, bb));
     }
   }
-  /* countMarks / scanMarks / allocBricks (voxel.ts:411-470), in the ordered form: coarse levels first, then pointer
-   * index; a brick past the pool is dropped. */
-  uint32_t marked = 0;
-  for (uint32_t i = 0; i < NL * per; i++) marked += vx->ptr[i] == ORC_MARK;
-  vx->hdr[5] = marked;
-  vx->hdr[0] = marked;
-  uint32_t idx = 0;
-  for (uint32_t o = 0; o < NL * per; o++) {
-    uint32_t L = NL - 1u - o / per, i = L * per + o % per;
-    if (vx->ptr[i] != ORC_MARK) continue;
-    uint32_t k = idx++;
-    if (k >= vx->max_bricks) { vx->ptr[i] = ORC_DROP; vx->hdr[2]++; continue; }
-    vx->hdr[8 + L]++;
-    vx->ptr[i] = k;
-    for (uint32_t w = 0; w < 16; w++) vx->occ[k * 16u + w] = 0;
-    vx->base[k] = 0;
-    uint32_t r = i % per;
-    vx->code[k] = (L << 27) | ((r % G) << 18) | (((r / G) % G) << 9) | (r / (G * G));
-  }
-  uint32_t nb = marked < vx->max_bricks ? marked : vx->max_bricks;
-  /* clearKeys */
-  memset(vx->rep, 0, (size_t)nb * 512u * 4u);
+}
 
-  /* voxBits + voxBitsBig (voxel.ts:492-534) */
-  for (uint32_t i = 0; i < threads_of(s); i++) {
-    uint32_t L0, t = work_at(s, i, &L0);
-    tri_t T = load_tri(s, t);
-    for (uint32_t L = L0; L < NL; L++) {
-      range_t r = vox_range(vx, &T, L, vox_size(vx, L));
-      int32_t n = r.n.x * r.n.y * r.n.z;
-      if (n == 0 || (!vx->coarse_from_triangles && finer_built_range(vx, L, r))) continue;
-      if ((uint32_t)n > BIG) {
-        uint32_t k = vx->hdr[16 + L]++;
-        if (k < cap) vx->big[L * cap + k] = t; else vx->hdr[3]++;
-        continue;
+/* reduce of level L (voxel.ts:540-577) for the level L-1 bricks [b, e): their words ORed into the parents, the
+ * representatives' maxima taken (atomics: OR and max commute) */
+typedef struct { orc_vox *vx; uint32_t L; } reduce_job_t;
+static void reduce_pass(void *p, uint64_t b0, uint64_t e0) {
+  reduce_job_t *j = (reduce_job_t *)p;
+  orc_vox *vx = j->vx;
+  const uint32_t L = j->L;
+  for (uint32_t ptr = (uint32_t)b0; ptr < (uint32_t)e0; ptr++) {
+    uint32_t code = vx->code[ptr];
+    uint32_t Lc = code >> 27;
+    if (Lc + 1u != L) continue;
+    for (uint32_t w = 0; w < 16; w++) {
+      uint32_t word = __atomic_load_n(&vx->occ[ptr * 16u + w], __ATOMIC_RELAXED);
+      if (word == 0u) continue;
+      i3 b = I((int32_t)((code >> 18) & 511u), (int32_t)((code >> 9) & 511u), (int32_t)(code & 511u));
+      i3 c0 = I(b.x * 8, b.y * 8 + (int32_t)((w & 1u) * 4u), b.z * 8 + (int32_t)(w >> 1));
+      i3 oc = org(vx, Lc), ol = org(vx, L);
+      i3 pc0 = I(((oc.x * 8 + c0.x) >> 1) - ol.x * 8, ((oc.y * 8 + c0.y) >> 1) - ol.y * 8, ((oc.z * 8 + c0.z) >> 1) - ol.z * 8);
+      uint32_t pptr = vx->ptr[ptr_index(vx, L, ishr(pc0, 3))];
+      if (pptr >= ORC_MARK) continue;
+      i3 l0 = I(pc0.x & 7, pc0.y & 7, pc0.z & 7);
+      uint32_t pbit0 = (uint32_t)(l0.x + 8 * l0.y + 64 * l0.z);
+      uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
+      while (word != 0u) {
+        uint32_t k = (uint32_t)__builtin_ctz(word);
+        word &= word - 1u;
+        uint32_t px = (k & 7u) >> 1, py = k >> 4;
+        mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
+        uint32_t rv = __atomic_load_n(&vx->rep[ptr * 512u + w * 32u + k], __ATOMIC_RELAXED);
+        if (py == 0u) { if (rv > lo[px]) lo[px] = rv; } else { if (rv > hi[px]) hi[px] = rv; }
       }
-      for (int32_t k = 0; k < n; k++)
-        voxelize_one(s, vx, &T, t, L, I(r.lo.x + k % r.n.x, r.lo.y + (k / r.n.x) % r.n.y, r.lo.z + k / (r.n.x * r.n.y)), n == 1);
-    }
-  }
-  for (uint32_t L = 0; L < NL; L++) {
-    uint32_t nbig = vx->hdr[16 + L] < cap ? vx->hdr[16 + L] : cap;
-    for (uint32_t k = 0; k < nbig; k++) {
-      uint32_t t = vx->big[L * cap + k];
-      tri_t T = load_tri(s, t);
-      range_t r = vox_range(vx, &T, L, vox_size(vx, L));
-      int32_t n = r.n.x * r.n.y * r.n.z;
-      for (int32_t q = 0; q < n; q++)
-        voxelize_one(s, vx, &T, t, L, I(r.lo.x + q % r.n.x, r.lo.y + (q / r.n.x) % r.n.y, r.lo.z + q / (r.n.x * r.n.y)), 0);
-    }
-  }
-
-  /* reduce, levels 1 .. NL-1 (voxel.ts:540-577) */
-  if (!vx->coarse_from_triangles) {
-    for (uint32_t L = 1; L < NL; L++) {
-      for (uint32_t ptr = 0; ptr < nb; ptr++) {
-        uint32_t code = vx->code[ptr];
-        uint32_t Lc = code >> 27;
-        if (Lc + 1u != L) continue;
-        for (uint32_t w = 0; w < 16; w++) {
-          uint32_t word = vx->occ[ptr * 16u + w];
-          if (word == 0u) continue;
-          i3 b = I((int32_t)((code >> 18) & 511u), (int32_t)((code >> 9) & 511u), (int32_t)(code & 511u));
-          i3 c0 = I(b.x * 8, b.y * 8 + (int32_t)((w & 1u) * 4u), b.z * 8 + (int32_t)(w >> 1));
-          i3 oc = org(vx, Lc), ol = org(vx, L);
-          i3 pc0 = I(((oc.x * 8 + c0.x) >> 1) - ol.x * 8, ((oc.y * 8 + c0.y) >> 1) - ol.y * 8, ((oc.z * 8 + c0.z) >> 1) - ol.z * 8);
-          uint32_t pptr = vx->ptr[ptr_index(vx, L, ishr(pc0, 3))];
-          if (pptr >= ORC_MARK) continue;
-          i3 l0 = I(pc0.x & 7, pc0.y & 7, pc0.z & 7);
-          uint32_t pbit0 = (uint32_t)(l0.x + 8 * l0.y + 64 * l0.z);
-          uint32_t mask = 0, lo[4] = {0, 0, 0, 0}, hi[4] = {0, 0, 0, 0};
-          while (word != 0u) {
-            uint32_t k = (uint32_t)__builtin_ctz(word);
-            word &= word - 1u;
-            uint32_t px = (k & 7u) >> 1, py = k >> 4;
-            mask |= 1u << ((pbit0 + px + 8u * py) & 31u);
-            uint32_t rv = vx->rep[ptr * 512u + w * 32u + k];
-            if (py == 0u) { if (rv > lo[px]) lo[px] = rv; } else { if (rv > hi[px]) hi[px] = rv; }
-          }
-          vx->occ[pptr * 16u + (pbit0 >> 5)] |= mask;
-          for (uint32_t px = 0; px < 4; px++)
-            for (uint32_t py = 0; py < 2; py++) {
-              uint32_t rv = py == 0 ? lo[px] : hi[px];
-              if (rv == 0u) continue;
-              uint32_t *rp = &vx->rep[pptr * 512u + pbit0 + px + 8u * py];
-              if (*rp < rv) *rp = rv;
-            }
+      __atomic_fetch_or(&vx->occ[pptr * 16u + (pbit0 >> 5)], mask, __ATOMIC_RELAXED);
+      for (uint32_t px = 0; px < 4; px++)
+        for (uint32_t py = 0; py < 2; py++) {
+          uint32_t rv = py == 0 ? lo[px] : hi[px];
+          if (rv != 0u) atomic_max_u32(&vx->rep[pptr * 512u + pbit0 + px + 8u * py], rv);
         }
-      }
     }
   }
+}
 
-  /* allocVoxels (voxel.ts:579-588), bases in brick order */
-  uint32_t total = 0;
-  for (uint32_t b = 0; b < nb; b++) {
-    uint32_t n = 0;
-    for (uint32_t w = 0; w < 16; w++) n += popc(vx->occ[b * 16u + w]);
-    uint32_t first = total;
-    total += n;
-    if (first + n > vx->max_voxels) { vx->base[b] = ORC_EMPTY; vx->hdr[4]++; continue; }
-    vx->base[b] = first;
-  }
-  vx->hdr[1] = total;
-
-  /* resolveAttr (voxel.ts:596-620) */
-  for (uint32_t ptr = 0; ptr < nb; ptr++) {
+/* resolveAttr (voxel.ts:596-620) of the bricks [b0, e0) */
+typedef struct { const orc_scene *s; orc_vox *vx; } resolve_job_t;
+static void resolve_pass(void *p, uint64_t b0, uint64_t e0) {
+  resolve_job_t *j = (resolve_job_t *)p;
+  const orc_scene *s = j->s;
+  orc_vox *vx = j->vx;
+  for (uint32_t ptr = (uint32_t)b0; ptr < (uint32_t)e0; ptr++) {
     uint32_t first = vx->base[ptr];
     if (first == ORC_EMPTY) continue;
     uint32_t code = vx->code[ptr];
@@ -374,6 +393,95 @@ int orc_vox_build(const orc_scene *s, orc_vox *vx) {
       vx->plane[ai] = dot(sf.n, sub(sf.q, p));
       vx->sunvis[ai] = 1.0f;
     }
+  }
+}
+
+void orc_vox_origins(float v0, uint32_t levels, uint32_t G, const double eye[3], int32_t origin_out[8][4]) {
+  for (uint32_t L = 0; L < 8; L++) for (int a = 0; a < 4; a++) origin_out[L][a] = 0;
+  for (uint32_t L = 0; L < levels; L++) {
+    double bs = (double)v0 * ldexp(1.0, (int)L) * 8.0;   /* v0 * 2 ** L * 8 in the host's f64 */
+    for (int a = 0; a < 3; a++) origin_out[L][a] = (int32_t)floor(eye[a] / bs) - (int32_t)(G / 2);
+  }
+}
+
+int orc_vox_build(const orc_scene *s, orc_vox *vx) {
+  const uint32_t NL = vx->levels, G = vx->G, per = G * G * G;
+  /* clear (voxel.ts:338) */
+  memset(vx->hdr, 0, ORC_HDR * 4);
+  for (uint32_t i = 0; i < NL * per; i++) vx->ptr[i] = ORC_EMPTY;
+
+  /* markBricks + markBricksBig (voxel.ts:359-387) */
+  {
+    uint32_t nt = threads_of(s);
+    uint64_t nch = ((uint64_t)nt + TRI_GRAIN - 1u) / TRI_GRAIN;
+    tri_pass_t j = {s, vx, (biglist_t *)calloc(nch ? nch : 1u, sizeof(biglist_t))};
+    orc_parallel(nt, TRI_GRAIN, mark_pass, &j);
+    big_merge(vx, j.ch, nch, 8u, 24u);
+    big_pass_t bj;
+    big_pass_init(&bj, s, vx, 8u, 24u);
+    orc_parallel(bj.off[8], 64u, mark_big_pass, &bj);
+  }
+  /* markParents (voxel.ts:390-403) */
+  orc_parallel((uint64_t)(NL - 1) * per, 4096u, parents_pass, vx);
+  /* countMarks / scanMarks / allocBricks (voxel.ts:411-470), in the ordered form: coarse levels first, then pointer
+   * index; a brick past the pool is dropped. */
+  uint32_t marked = 0;
+  for (uint32_t i = 0; i < NL * per; i++) marked += vx->ptr[i] == ORC_MARK;
+  vx->hdr[5] = marked;
+  vx->hdr[0] = marked;
+  uint32_t idx = 0;
+  for (uint32_t o = 0; o < NL * per; o++) {
+    uint32_t L = NL - 1u - o / per, i = L * per + o % per;
+    if (vx->ptr[i] != ORC_MARK) continue;
+    uint32_t k = idx++;
+    if (k >= vx->max_bricks) { vx->ptr[i] = ORC_DROP; vx->hdr[2]++; continue; }
+    vx->hdr[8 + L]++;
+    vx->ptr[i] = k;
+    for (uint32_t w = 0; w < 16; w++) vx->occ[k * 16u + w] = 0;
+    vx->base[k] = 0;
+    uint32_t r = i % per;
+    vx->code[k] = (L << 27) | ((r % G) << 18) | (((r / G) % G) << 9) | (r / (G * G));
+  }
+  uint32_t nb = marked < vx->max_bricks ? marked : vx->max_bricks;
+  /* clearKeys */
+  memset(vx->rep, 0, (size_t)nb * 512u * 4u);
+
+  /* voxBits + voxBitsBig (voxel.ts:492-534) */
+  {
+    uint32_t nt = threads_of(s);
+    uint64_t nch = ((uint64_t)nt + TRI_GRAIN - 1u) / TRI_GRAIN;
+    tri_pass_t j = {s, vx, (biglist_t *)calloc(nch ? nch : 1u, sizeof(biglist_t))};
+    orc_parallel(nt, TRI_GRAIN, bits_pass, &j);
+    big_merge(vx, j.ch, nch, 0u, 16u);
+    big_pass_t bj;
+    big_pass_init(&bj, s, vx, 0u, 16u);
+    orc_parallel(bj.off[8], 16u, bits_big_pass, &bj);
+  }
+
+  /* reduce, levels 1 .. NL-1 (voxel.ts:540-577), each level's bricks in parallel */
+  if (!vx->coarse_from_triangles) {
+    for (uint32_t L = 1; L < NL; L++) {
+      reduce_job_t j = {vx, L};
+      orc_parallel(nb, 64u, reduce_pass, &j);
+    }
+  }
+
+  /* allocVoxels (voxel.ts:579-588), bases in brick order */
+  uint32_t total = 0;
+  for (uint32_t b = 0; b < nb; b++) {
+    uint32_t n = 0;
+    for (uint32_t w = 0; w < 16; w++) n += popc(vx->occ[b * 16u + w]);
+    uint32_t first = total;
+    total += n;
+    if (first + n > vx->max_voxels) { vx->base[b] = ORC_EMPTY; vx->hdr[4]++; continue; }
+    vx->base[b] = first;
+  }
+  vx->hdr[1] = total;
+
+  /* resolveAttr (voxel.ts:596-620), bricks in parallel */
+  {
+    resolve_job_t j = {s, vx};
+    orc_parallel(nb, 16u, resolve_pass, &j);
   }
   return 0;
 }
