@@ -181,11 +181,13 @@ int gi_scene_rigid_apply(gi_scene *scene, void *stream);
  * takes the scene and every output in the caller's device memory and allocates nothing: its scratch (representatives,
  * big-triangle lists, scan sums) is a static device array of 14.2 MiB that the library holds on every GPU it is loaded
  * on.  Limits: max_bricks <= 4096, levels * G^3 <= 2^25, 65,536 big triangles per list (more count as bigOverflow,
- * header word 3).  Inputs: pos4/nrm4 4 floats per vertex (w ignored), tri4 (i0, i1, i2, material) with indices below
+ * header word 3; gi_vox_build keeps up to 262,144, so past 65,536 the two give different voxels and only this one
+ * reports the overflow).  Inputs: pos4/nrm4 4 floats per vertex (w ignored), tri4 (i0, i1, i2, material) with indices below
  * nverts / nmats (not checked: they are device memory), mats device gi_material[nmats]; pos4, nrm4, tri4, occ, attr
  * 16-byte aligned.  Outputs as gi_vox_read_state lays them out (hdr 64 words, ptr levels*G^3, occ max_bricks*16,
  * base/code max_bricks, attr max_voxels*4, plane/sunvis max_voxels).  Runs on the current device and `stream`; the
- * first call on a device looks up the scratch's address there.  All calls share the scratch: two calls that overlap
+ * first call on a device looks up the scratch's address there, in the device's primary context (the one the CUDA
+ * runtime uses); the address stays valid until that context is reset.  All calls share the scratch: two calls that overlap
  * on the GPU race and corrupt each other, so serialise them. */
 int gi_vox_build_noalloc(const gi_vox_params *params, const double eye[3], const float *pos4, const float *nrm4,
                          uint32_t nverts, const uint32_t *tri4, uint32_t ntris, const gi_material *mats, uint32_t nmats,

@@ -4,8 +4,10 @@ A renderer that hands out every buffer from its own device pool, a thread in the
 serving loop that must not stall the GPU with an allocation cannot let the library call cudaMalloc.  This entry point
 takes the scene and the outputs in the caller's memory and uses a static device array for its scratch.  The GPU test
 checks it against the allocating entry point (gi_vox_create + gi_vox_build) on two calls in a row: the outputs must
-be bit-identical, the second call showing that the scratch left by the first does not leak into the result.  This
-file is collected last so that a run stopping at the first failure has run every other test already.
+be bit-identical, the second call showing that the scratch left by the first does not leak into the result.  Before
+them a call on a larger scene (the colonnade, which fills the brick pool) leaves the scratch full of another build's
+representatives and lists.  This file is collected last so that a run stopping at the first failure has run every
+other test already.
 """
 import ctypes as C
 
@@ -68,6 +70,23 @@ def test_noalloc_matches_allocating_build_twice():
     nb = int(min(ref["hdr"][0], v.maxBricks))
     nv = int(min(ref["hdr"][1], v.maxVoxels))
     assert nb > 100 and nv > 1000
+    # a larger build first: the colonnade's 261k triangles fill the brick pool and the scratch
+    from rtgi import scenes
+    big = scenes.colonnade_scene(0)
+    bpos = torch.zeros((big.positions.shape[0], 4), dtype=torch.float32, device=dev)
+    bnrm = torch.zeros_like(bpos)
+    bpos[:, :3] = torch.from_numpy(big.positions).to(dev)
+    bnrm[:, :3] = torch.from_numpy(big.normals).to(dev)
+    btri = torch.from_numpy(big.tri.astype(np.uint32).view(np.int32)).to(dev).contiguous()
+    bmats = torch.from_numpy(big.material_array().view(np.uint8)).to(dev)
+    be = (C.c_double * 3)(*[float(x) for x in big.camera.eye])
+    st = lib.gi_vox_build_noalloc(C.byref(_params(v)), be, bpos.data_ptr(), bnrm.data_ptr(), bpos.shape[0],
+                                  btri.data_ptr(), btri.shape[0], bmats.data_ptr(), len(big.materials),
+                                  *[out[k].data_ptr() for k in ("hdr", "ptr", "occ", "base", "code", "attr", "plane", "sunvis")],
+                                  None)
+    assert st == 0, lib.gi_last_error()
+    torch.cuda.synchronize()
+    assert out["hdr"][0].item() > nb   # more bricks wanted than the room uses
     for call in range(2):
         for t in out.values():
             t.fill_(-1)   # garbage: every word the build owns must be rewritten
