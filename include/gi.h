@@ -46,6 +46,7 @@ typedef struct gi_ctx gi_ctx;
 typedef struct gi_scene gi_scene;
 typedef struct gi_vox gi_vox;
 typedef struct gi_rc gi_rc;
+typedef struct gi_dyn gi_dyn;
 
 /* Material (scene_gpu.ts:95-106 `struct Material`): base colour factor, flags (1 alpha mask, 2 double-sided,
  * 4 toon, 8 object), alpha cutoff.  emissive: radiance added at a voxel hit (no counterpart in the reference,
@@ -119,6 +120,10 @@ int gi_scene_update_vertices(gi_scene *scene, uint32_t first, uint32_t count, co
 /* The rasters (G-buffer, shadow map) draw rows [0, count); rows past it are voxelised only (a world's clustered
  * copies, world.ts:20-24).  All rows by default. */
 int gi_scene_set_draw_count(gi_scene *scene, uint32_t count);
+/* The rows the voxel rebuild reads: [0, count) (createVoxWorld's firstDynamicTri, voxel.ts:746); the rows after it are
+ * the dynamic triangles, which go to a dynamic layer (gi_dyn_create) instead.  count = the scene's rows: all (the
+ * default).  The rasters still draw every row. */
+int gi_scene_set_static_count(gi_scene *scene, uint32_t count);
 /* The rasters draw those rows at n instance offsets (3 floats each, instance 0 at the origin; n <= 1: once), drawn
  * triangle i * count + row for instance i (the instanced draws of a world, world.ts:4-6). */
 int gi_scene_set_draw_instances(gi_scene *scene, const float *offsets, uint32_t n);
@@ -340,6 +345,32 @@ typedef struct gi_vox_tuning {
 int gi_vox_set_tuning(gi_vox *vox, const gi_vox_tuning *t);
 int gi_vox_get_tuning(gi_vox *vox, gi_vox_tuning *t);
 int gi_rc_destroy(gi_rc *rc);
+
+/* ---- the dynamic layer (src/core/dynlayer.ts) ---------------------------------------------------------------------
+ * Moving triangles (the scene's rows from first_dynamic on; gi_scene_set_static_count keeps them out of the voxel
+ * rebuild) splatted every frame into a layer of coverage and mean radiance per voxel of the clipmap's levels (fixed
+ * point at level 0, prefiltered to the coarser levels), which the cascades' traces read at the width of a direction
+ * bin's cone (traceDyn, rc.ts:223-231).  createDynLayer (dynlayer.ts:680): `bricks` is VoxParams.dynBricks (the
+ * reference's default 512); albedo 1 writes the area x albedo words (the reference's DYN_ALB, configs with the token
+ * obj; the received light of dynInject, phase 31, is not built).  G^3 must be a multiple of 32. */
+int gi_dyn_create(gi_vox *vox, uint32_t bricks, uint32_t first_dynamic, uint32_t albedo, gi_dyn **out);
+/* DynLayer.encode (dynlayer.ts:738-741): mark .. resolve at the voxel world's current windows, shaded with the rc's
+ * frame (sun, style) and its sun shadow map when it has one.  Stream-ordered.  gi_solve runs it after the static
+ * rebuild when the layer is bound to the rc (gi_rc_set_dyn). */
+int gi_dyn_build(gi_dyn *dyn, gi_rc *rc, void *stream);
+/* readCounters (dynlayer.ts:749-759): the 64 header words (0 wanted bricks, 1 dropped, 2-7 bounds in cm + 2^30,
+ * 8 allocated, 9 triangles outside every clipmap, 10 frame counter, 16 + L first slot and 24 + L bricks of level L).
+ * Synchronises; GI_ERR_TIMEOUT when the allocation's bounded scan wait gave up (word 12). */
+int gi_dyn_read_counters(gi_dyn *dyn, uint32_t hdr[64], void *stream);
+/* The layer's arrays (any may be NULL): ptr levels*G^3, bits 2*levels*G^3/32, meta bricks, mask bricks*16, data
+ * bricks*512*13 words.  Synchronises. */
+int gi_dyn_read_state(gi_dyn *dyn, uint32_t *ptr, uint32_t *bits, uint32_t *meta, uint32_t *mask, uint32_t *data,
+                      void *stream);
+int gi_dyn_bytes(gi_dyn *dyn, uint64_t *bytes);
+int gi_dyn_destroy(gi_dyn *dyn);
+/* The layer the rc's traces read, or NULL for none (dyn[0] = 0 in the reference: no dynamic objects).  Drops a
+ * captured graph (it was captured without the layer). */
+int gi_rc_set_dyn(gi_rc *rc, gi_dyn *dyn);
 
 #ifdef __cplusplus
 }

@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgi_oracle.so")
-SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "shadow.c", "world.c", "orc_par.c", "gi_oracle.h", "orc_math.h",
+SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "shadow.c", "world.c", "dyn.c", "orc_par.c", "gi_oracle.h", "orc_math.h",
            "orc_par.h", "orc_rc.h", "Makefile"]
 
 
@@ -65,6 +65,12 @@ def lib():
         _lib.orc_bounce_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_gi_exp.argtypes = [C.c_float]
         _lib.orc_gi_exp.restype = C.c_float
+        _lib.orc_dyn_init.argtypes = [C.c_void_p, C.c_void_p]
+        _lib.orc_dyn_build.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p,
+                                       C.c_uint32]
+        _lib.orc_trace_dyn.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_float, C.c_void_p]
+        _lib.orc_log2.argtypes = [C.c_float]
+        _lib.orc_log2.restype = C.c_float
     return _lib
 
 
@@ -87,7 +93,12 @@ class OrcVox(C.Structure):
                 ("origin", (C.c_int32 * 4) * 8),
                 ("hdr", C.c_void_p), ("ptr", C.c_void_p), ("occ", C.c_void_p), ("base", C.c_void_p),
                 ("code", C.c_void_p), ("rep", C.c_void_p), ("big", C.c_void_p), ("attr", C.c_void_p),
-                ("plane", C.c_void_p), ("sunvis", C.c_void_p), ("bn_inj", C.c_void_p)]
+                ("plane", C.c_void_p), ("sunvis", C.c_void_p), ("bn_inj", C.c_void_p), ("dyn", C.c_void_p)]
+
+
+class OrcDyn(C.Structure):
+    _fields_ = [("nb", C.c_uint32), ("albedo", C.c_uint32), ("hdr", C.c_void_p), ("ptr", C.c_void_p),
+                ("bits", C.c_void_p), ("meta", C.c_void_p), ("mask", C.c_void_p), ("data", C.c_void_p)]
 
 
 class OrcBounce(C.Structure):
@@ -204,6 +215,7 @@ def _vox_struct(st: dict) -> OrcVox:
         setattr(vx, k, _p(st[k]))
     vx.big = None
     vx.bn_inj = _p(st["bn_inj"]) if st.get("bn_inj") is not None else None
+    vx.dyn = C.addressof(st["dyn"].struct) if st.get("dyn") is not None else None
     return vx
 
 
@@ -414,3 +426,41 @@ def hash32(x: int) -> int:
 def lod_for(frame: np.ndarray, dist: float) -> int:
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     return int(lib().orc_lod_for(_p(frame), C.c_float(dist)))
+
+
+class Dyn:
+    """The dynamic layer (oracle/dyn.c, dynlayer.ts) of a voxel world built by vox_build: its arrays laid out as the
+    CUDA path's (gi_dyn_read_state).  Set vox["dyn"] = this to make the cascades' traces read it."""
+
+    def __init__(self, vox: dict, bricks: int = 512, albedo: bool = False):
+        nptr = vox["levels"] * vox["G"] ** 3
+        self.nb = bricks
+        self.arrays = {"hdr": np.zeros(64, np.uint32), "ptr": np.zeros(nptr, np.uint32),
+                       "bits": np.zeros(2 * nptr // 32, np.uint32), "meta": np.zeros(bricks, np.uint32),
+                       "mask": np.zeros(bricks * 16, np.uint32), "data": np.zeros(bricks * 512 * 13, np.uint32)}
+        a = self.arrays
+        self.struct = OrcDyn(bricks, 1 if albedo else 0, _p(a["hdr"]), _p(a["ptr"]), _p(a["bits"]), _p(a["meta"]),
+                             _p(a["mask"]), _p(a["data"]))
+        vx = _vox_struct(vox)
+        lib().orc_dyn_init(C.byref(vx), C.byref(self.struct))
+
+    def build(self, scene, vox: dict, first: int, end: int, frame: np.ndarray, shadow: np.ndarray = None) -> None:
+        """One build of the dynamic triangles [first, end) in the windows of `vox` (its origins)."""
+        s, keep = _scene_struct(scene)
+        frame = np.ascontiguousarray(frame, dtype=np.float32)
+        vx = _vox_struct({**vox, "dyn": None})
+        sm = None if shadow is None else np.ascontiguousarray(shadow, dtype=np.float32)
+        lib().orc_dyn_build(C.byref(s), C.byref(vx), C.byref(self.struct), first, end, _p(frame),
+                            _p(sm) if sm is not None else None, 0 if sm is None else sm.shape[0])
+
+    def trace(self, vox: dict, o, d, t0: float, t1: float, k: float) -> np.ndarray:
+        """traceDyn of one segment: covered radiance rgb and coverage."""
+        vx = _vox_struct({**vox, "dyn": self})
+        oo, dd = np.asarray(o, np.float32).copy(), np.asarray(d, np.float32).copy()
+        out = np.zeros(4, np.float32)
+        lib().orc_trace_dyn(C.byref(vx), _p(oo), _p(dd), t0, t1, k, _p(out))
+        return out
+
+
+def log2(x: float) -> float:
+    return float(lib().orc_log2(x))

@@ -89,7 +89,35 @@ typedef struct {
   float *sunvis;                   /* max_voxels: sun visibility of the voxel (1 when no visibility pass runs) */
   const float *bn_inj;             /* NULL, or max_voxels * 6: the bounce volume's irradiance on the voxel's two sides
                                       (front rgb, back rgb, f16 values; orc_bounce_frame writes it) */
+  const struct orc_dyn_s *dyn;     /* NULL, or the dynamic layer the cascades' traces read (traceDyn, rc.ts:227-231) */
 } orc_vox;
+
+/* The dynamic layer (src/core/dynlayer.ts), laid out as the CUDA path lays it out in device memory: the 64 header
+ * words (dynlayer.ts:53-55), a pointer per brick of every level (slot, DYN_EMPTY or DYN_DROPPED), the two brick
+ * bitsets (bit order: coarse levels first), slot -> brick, per slot 16 words of its non-zero voxels, per voxel of a
+ * slot 13 words (P+x P-x P+y P-y P+z P-z, area, area x radiance rgb, area x albedo rgb), level 0 in fixed point
+ * (x 65536), levels above as f32 after the resolve. */
+typedef struct orc_dyn_s {
+  uint32_t nb;                     /* brick pool (DYN_MAX_BRICKS) */
+  uint32_t albedo;                 /* 1: the splat writes the albedo words (configs whose objects receive light) */
+  uint32_t *hdr;                   /* 64 */
+  uint32_t *ptr;                   /* levels * G^3 */
+  uint32_t *bits;                  /* 2 * levels * G^3 / 32 */
+  uint32_t *meta;                  /* nb */
+  uint32_t *mask;                  /* nb * 16 */
+  uint32_t *data;                  /* nb * 512 * 13 */
+} orc_dyn;
+
+/* createDynLayer's initial state (dynlayer.ts:690-694) over the voxel world's levels and G. */
+void orc_dyn_init(const orc_vox *vx, orc_dyn *dl);
+/* One build (mark .. resolve, dynlayer.ts:592) of the dynamic triangles [first, end) of the scene in the voxel world's
+ * current windows, shaded with the frame's sun and style and the sun shadow map (map NULL: visibility 1). */
+int orc_dyn_build(const orc_scene *s, const orc_vox *vx, orc_dyn *dl, uint32_t first, uint32_t end, const float *frame,
+                  const float *map, uint32_t S);
+/* traceDyn (dynlayer.ts:118-162): covered radiance (rgb) and coverage of [t0, t1] along d from o, cone width k * t. */
+void orc_trace_dyn(const orc_vox *vx, float o[3], float d[3], float t0, float t1, float k, float out[4]);
+/* log2 as this library defines it (the reference's WGSL log2 is implementation-defined). */
+float orc_log2(float x);
 
 /* Host writeUniform (voxel.ts:868-876): per level origin = floor(eye / bs) - G/2, bs = v0 * 2^L * 8 (f64 host math). */
 void orc_vox_origins(float v0, uint32_t levels, uint32_t G, const double eye[3], int32_t origin_out[8][4]);

@@ -40,4 +40,6 @@ uint32_t vox_level(const orc_vox *vx, const orc_layout *ly, float s0, uint32_t c
 void trace_vox(const ctx_t *cx, v3 o, v3 d, float t0, float t1, float tskip, uint32_t L, uint32_t cap, trace_t *out);
 void sh_basis(v3 n, float y[9]);
 v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_t q, uint32_t u, uint32_t v, uint32_t lr);
+/* dyn.c */
+void dyn_compose(const orc_vox *vx, v3 o, v3 d, float t0, float t1, v3 ooff, float k, trace_t *tr);
 #endif

@@ -5,8 +5,8 @@
  * (setupScreen), :600-622 (trace), :681-743 (upperAvg, mergeScreen), :745-774 (shBasis, projectSH),
  * :819-829 (evalSH), :929-954 (gatherScreen), and voxel.ts:81-202 (voxRank, voxAt, voxLevelFor, traceVox).
  * Multi-bounce (bounce.ts) is restated too: the volume's frame (orc_bounce_frame) and the cascades' read of the
- * irradiance it injects into the voxels (when orc_vox.bn_inj is set).  The dynamic layer (dyn[0] = 0) and the triangle
- * comparator are off.  The hit radiance adds the voxel's emissive radiance (the reference has no emission). */
+ * irradiance it injects into the voxels (when orc_vox.bn_inj is set), and the cascades' read of the dynamic layer
+ * (dyn.c) when orc_vox.dyn is set.  The triangle comparator is off.  The hit radiance adds the voxel's emissive radiance (the reference has no emission). */
 #include <stdlib.h>
 #include "gi_oracle.h"
 #include "orc_math.h"
@@ -314,7 +314,9 @@ static void trace_range(void *p, uint64_t b, uint64_t e) {
       v3 pn = V(pr->nrm[0], pr->nrm[1], pr->nrm[2]);
       uint32_t Lv = vox_level_for(vx, vox_level(vx, ly, s0, j->c), add(po, muls(dir, t1)));
       float v = vox_size(vx, Lv);
-      trace_vox(j->cx, add(po, muls(pn, ly->vox_offset * v)), dir, t0, t1, ly->vox_skip * v, Lv, ly->dda_cap, &tr);
+      v3 ooff = add(po, muls(pn, ly->vox_offset * v));
+      trace_vox(j->cx, ooff, dir, t0, t1, ly->vox_skip * v, Lv, ly->dda_cap, &tr);
+      dyn_compose(vx, po, dir, t0, t1, ooff, 3.5449077f / (float)L->res, &tr);
       n_traces += 1;
       n_steps += tr.steps;
       n_cap += tr.steps >= ly->dda_cap ? 1u : 0u;

@@ -250,7 +250,9 @@ static void w_trace_range(void *p, uint64_t b, uint64_t e) {
       v3 pn = V(pr->nrm[0], pr->nrm[1], pr->nrm[2]);
       uint32_t Lv = vox_level_for(vx, vox_level(vx, ly, s0, j->c), add(po, muls(dir, t1)));
       float v = vox_size(vx, Lv);
-      trace_vox(j->cx, add(po, muls(pn, ly->vox_offset * v)), dir, t0, t1, ly->vox_skip * v, Lv, ly->dda_cap, &tr);
+      v3 ooff = add(po, muls(pn, ly->vox_offset * v));
+      trace_vox(j->cx, ooff, dir, t0, t1, ly->vox_skip * v, Lv, ly->dda_cap, &tr);
+      dyn_compose(vx, po, dir, t0, t1, ooff, 3.5449077f / (float)L->res, &tr);
       n_traces += 1;
       n_steps += tr.steps;
       n_cap += tr.steps >= ly->dda_cap ? 1u : 0u;

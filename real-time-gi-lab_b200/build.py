@@ -14,7 +14,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIB_DIR, "libgi_b200.so")
-SOURCES = ["vox_build.cu", "rc_solve.cu", "gbuffer.cu", "shadow.cu", "capi.cu", "noalloc.cu", "ref64.cu"]
+SOURCES = ["vox_build.cu", "rc_solve.cu", "gbuffer.cu", "shadow.cu", "dyn.cu", "capi.cu", "noalloc.cu", "ref64.cu"]
 HEADERS = ["gi_dev.cuh", "gi_internal.h", "gi_scan.cuh", "world.cuh"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17", "-fmad=false",

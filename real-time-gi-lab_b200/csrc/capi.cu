@@ -103,6 +103,7 @@ struct gi_scene {
   float4 *draw_inst = nullptr; // offsets of the drawn instances (gi_scene_set_draw_instances), instance 0 at the origin
   uint32_t draw_ninst = 1;
   uint32_t raster_tris = 0;    // triangles the raster scratch holds
+  uint32_t static_tris = 0;    // rows the voxel rebuild reads ([0, static_tris); gi_scene_set_static_count), 0: all
 };
 
 struct gi_vox {
@@ -123,6 +124,8 @@ struct gi_vox {
   SceneDev build_scene() const {
     SceneDev d = scene->dev();
     d.ntris = scene->ntris;
+    if (scene->static_tris) d.threads = scene->static_tris == 0xffffffffu ? 0u : scene->static_tris;   // the dynamic tail
+                                                                                                       // goes to the dynamic layer
     if (world) {
       d.items = w_items; d.lists = w_lists; d.inst = w_inst; d.nitems = w_nitems; d.threads = w_threads;
       d.key_stride = w_stride; d.key_limit = w_ninst * w_stride;
@@ -169,6 +172,14 @@ struct gi_rc {
   gi_vox *bn_vox = nullptr;
   bool world = false;                // world probes (gi_rc_create_world)
   WorldDev w = {};
+  struct gi_dyn *dyn = nullptr;      // gi_rc_set_dyn: the dynamic layer its traces read (gi_solve also builds it)
+};
+
+// The dynamic layer of a voxel world (dynlayer.ts createDynLayer): its device state and the scene's dynamic rows
+struct gi_dyn {
+  gi_vox *vox;
+  DynDev dev;
+  uint64_t bytes = 0;
 };
 
 static void free_scene(gi_scene *s) {
@@ -556,6 +567,14 @@ int gi_scene_set_draw_count(gi_scene *s, uint32_t count) {
   int st = ensure_raster_scratch(s, (uint64_t)count * s->draw_ninst, "gi_scene_set_draw_count");
   if (st) return st;
   s->ndraw = count;
+  return GI_OK;
+}
+
+int gi_scene_set_static_count(gi_scene *s, uint32_t count) {
+  if (!s) return fail(GI_ERR_INVALID, "gi_scene_set_static_count: NULL scene");
+  if (count > s->ntris) return fail(GI_ERR_INVALID, "gi_scene_set_static_count: %u of %u rows", count, s->ntris);
+  s->static_tris = count == s->ntris ? 0u : count;
+  if (count == 0 && s->ntris) s->static_tris = 0xffffffffu;   // every row dynamic: the rebuild reads none
   return GI_OK;
 }
 
@@ -1019,6 +1038,11 @@ int gi_solve(gi_rc *r, gi_vox *v, void *stream) {
   }
   int st = vox_build_sun(v, r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, stream);
   if (st != GI_OK) return st;
+  if (r->dyn) {   // the dynamic layer after the static rebuild (rcrun.ts encodeFrame: one 'vox' pass holds both)
+    if (r->dyn->vox != v) return fail(GI_ERR_INVALID, "gi_solve: the rc's dynamic layer belongs to another voxel world");
+    CK(gi_launch_dyn_build(r->dyn->dev, v->dev, v->scene->dev(), r->frame, r->shadow, r->shadow ? r->shadow_size : 0u,
+                           r->ctx->sm_count, S(stream)), "gi_solve: dynamic layer");
+  }
   st = gi_rc_solve(r, v, stream);
   r->timed_vox = st == GI_OK && r->timing;
   return st;
@@ -1515,6 +1539,108 @@ int gi_rc_read_irradiance_f64(gi_rc *r, double *rgba, void *stream) {
   CK(cudaMemcpyAsync(rgba, r->irr64, (size_t)r->W * r->H * 32u, cudaMemcpyDefault, S(stream)),
      "gi_rc_read_irradiance_f64: copy");
   CK(cudaStreamSynchronize(S(stream)), "gi_rc_read_irradiance_f64: sync");
+  return GI_OK;
+}
+
+// ---- the dynamic layer (dynlayer.ts) ----------------------------------------------------------------------------------
+int gi_dyn_create(gi_vox *v, uint32_t bricks, uint32_t first_dynamic, uint32_t albedo, gi_dyn **out) {
+  if (!v || !out) return fail(GI_ERR_INVALID, "gi_dyn_create: NULL argument");
+  *out = nullptr;
+  const uint32_t G = v->p.G, G3 = G * G * G, levels = v->p.levels;
+  if (G3 % 32u) return fail(GI_ERR_INVALID, "gi_dyn_create: G^3 must be a multiple of 32 (dynlayer.ts:687)");
+  if (bricks < 1 || bricks > (1u << 20)) return fail(GI_ERR_INVALID, "gi_dyn_create: %u bricks (1 .. 2^20)", bricks);
+  if (first_dynamic > v->scene->ntris)
+    return fail(GI_ERR_INVALID, "gi_dyn_create: first dynamic row %u of %u", first_dynamic, v->scene->ntris);
+  CK(cudaSetDevice(v->scene->ctx->device), "gi_dyn_create: cudaSetDevice");
+  gi_dyn *d = new (std::nothrow) gi_dyn;
+  if (!d) return fail(GI_ERR_OOM, "gi_dyn_create: host allocation");
+  d->vox = v;
+  DynDev &q = d->dev;
+  memset(&q, 0, sizeof q);
+  q.nb = bricks; q.albedo = albedo ? 1u : 0u; q.first = first_dynamic; q.end = v->scene->ntris;
+  const size_t np = (size_t)levels * G3, nw = np / 32u;
+  q.look_cap = (uint32_t)((nw + 255u) / 256u);
+  cudaError_t e;
+  if ((e = dalloc(&q.hdr, 64)) || (e = dalloc(&q.ptr, np)) || (e = dalloc(&q.bits, 2u * nw)) || (e = dalloc(&q.meta, bricks)) ||
+      (e = dalloc(&q.mask, (size_t)bricks * 16u)) || (e = dalloc(&q.data, (size_t)bricks * 512u * DYN_W)) ||
+      (e = dalloc(&q.look, (size_t)q.look_cap + 1u))) {
+    cudaFree(q.hdr); cudaFree(q.ptr); cudaFree(q.bits); cudaFree(q.meta); cudaFree(q.mask); cudaFree(q.data); cudaFree(q.look);
+    delete d;
+    return cuda_fail(e, "gi_dyn_create");
+  }
+  // createDynLayer's initial state (dynlayer.ts:690-694): empty pointers, bounds reset, zero bitsets
+  uint32_t h[64] = {};
+  h[32] = h[33] = h[34] = 0xffffffffu;
+  if ((e = cudaMemcpy(q.hdr, h, sizeof h, cudaMemcpyHostToDevice)) || (e = cudaMemset(q.ptr, 0xff, np * 4u)) ||
+      (e = cudaMemset(q.bits, 0, 2u * nw * 4u)) || (e = cudaMemset(q.meta, 0, (size_t)bricks * 4u)) ||
+      (e = cudaMemset(q.mask, 0, (size_t)bricks * 64u)) || (e = cudaMemset(q.data, 0, (size_t)bricks * 512u * DYN_W * 4u))) {
+    cudaFree(q.hdr); cudaFree(q.ptr); cudaFree(q.bits); cudaFree(q.meta); cudaFree(q.mask); cudaFree(q.data); cudaFree(q.look);
+    delete d;
+    return cuda_fail(e, "gi_dyn_create: init");
+  }
+  d->bytes = (64u + np + 2u * nw + (uint64_t)bricks * (1u + 16u + 512u * DYN_W) + q.look_cap + 1u) * 4u;
+  *out = d;
+  return GI_OK;
+}
+
+int gi_dyn_build(gi_dyn *d, gi_rc *r, void *stream) {
+  if (!d || !r) return fail(GI_ERR_INVALID, "gi_dyn_build: NULL argument");
+  if (!r->frame_set) return fail(GI_ERR_STATE, "gi_dyn_build: the rc has no frame");
+  if (!d->vox->updated) return fail(GI_ERR_STATE, "gi_dyn_build: gi_vox_update was not called");
+  CK(cudaSetDevice(d->vox->scene->ctx->device), "gi_dyn_build: cudaSetDevice");
+  CK(gi_launch_dyn_build(d->dev, d->vox->dev, d->vox->scene->dev(), r->frame, r->shadow, r->shadow ? r->shadow_size : 0u,
+                         d->vox->scene->ctx->sm_count, S(stream)), "gi_dyn_build: launch");
+  return GI_OK;
+}
+
+int gi_dyn_read_counters(gi_dyn *d, uint32_t hdr[64], void *stream) {
+  if (!d || !hdr) return fail(GI_ERR_INVALID, "gi_dyn_read_counters: NULL argument");
+  CK(cudaSetDevice(d->vox->scene->ctx->device), "gi_dyn_read_counters: cudaSetDevice");
+  CK(cudaMemcpyAsync(hdr, d->dev.hdr, 64 * 4, cudaMemcpyDeviceToHost, S(stream)), "gi_dyn_read_counters: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_dyn_read_counters: sync");
+  if (hdr[12] != 0u)
+    return fail(GI_ERR_TIMEOUT, "gi_dyn_read_counters: a bounded wait of the allocation scan gave up (header word 12)");
+  return GI_OK;
+}
+
+int gi_dyn_read_state(gi_dyn *d, uint32_t *ptr, uint32_t *bits, uint32_t *meta, uint32_t *mask, uint32_t *data, void *stream) {
+  if (!d) return fail(GI_ERR_INVALID, "gi_dyn_read_state: NULL dynamic layer");
+  CK(cudaSetDevice(d->vox->scene->ctx->device), "gi_dyn_read_state: cudaSetDevice");
+  const DynDev &q = d->dev;
+  const size_t np = (size_t)d->vox->p.levels * d->vox->p.G * d->vox->p.G * d->vox->p.G;
+  struct { void *dst; const void *src; size_t bytes; } c[5] = {
+      {ptr, q.ptr, np * 4u}, {bits, q.bits, np / 32u * 2u * 4u}, {meta, q.meta, (size_t)q.nb * 4u},
+      {mask, q.mask, (size_t)q.nb * 64u}, {data, q.data, (size_t)q.nb * 512u * DYN_W * 4u}};
+  for (auto &x : c)
+    if (x.dst) CK(cudaMemcpyAsync(x.dst, x.src, x.bytes, cudaMemcpyDeviceToHost, S(stream)), "gi_dyn_read_state: copy");
+  CK(cudaStreamSynchronize(S(stream)), "gi_dyn_read_state: sync");
+  return GI_OK;
+}
+
+int gi_dyn_bytes(gi_dyn *d, uint64_t *bytes) {
+  if (!d || !bytes) return fail(GI_ERR_INVALID, "gi_dyn_bytes: NULL argument");
+  *bytes = d->bytes;
+  return GI_OK;
+}
+
+int gi_dyn_destroy(gi_dyn *d) {
+  if (!d) return GI_OK;
+  cudaSetDevice(d->vox->scene->ctx->device);
+  const DynDev &q = d->dev;
+  cudaFree(q.hdr); cudaFree(q.ptr); cudaFree(q.bits); cudaFree(q.meta); cudaFree(q.mask); cudaFree(q.data); cudaFree(q.look);
+  delete d;
+  return GI_OK;
+}
+
+int gi_rc_set_dyn(gi_rc *r, gi_dyn *d) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_dyn: NULL rc");
+  if (d && d->vox->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_set_dyn: layer on another device");
+  r->dyn = d;
+  r->dev.dyn_hdr = d ? d->dev.hdr : nullptr;
+  r->dev.dyn_ptr = d ? d->dev.ptr : nullptr;
+  r->dev.dyn_data = d ? d->dev.data : nullptr;
+  r->dev.dyn_nb = d ? d->dev.nb : 0u;
+  if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; r->graph_vox = nullptr; }   // captured without it
   return GI_OK;
 }
 

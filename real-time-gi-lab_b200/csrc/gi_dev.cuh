@@ -68,6 +68,27 @@ __device__ __forceinline__ int round_log2(float x) {
   return mm >= 0.5 ? e : e - 1;
 }
 
+// log2(x) for x > 0 (the reference's WGSL log2 is implementation-defined; this library defines it): x = m 2^e with m in
+// [sqrt(1/2), sqrt(2)), log2 m = 2 atanh(s) / ln 2 with s = (m - 1) / (m + 1) by its series through s^11 (|s| <= 0.172)
+// in Horner form with fused multiply-adds.  Exact for powers of two, relative error below 1e-7 elsewhere; the oracle
+// evaluates the same f32 sequence.
+__device__ __forceinline__ float gi_log2(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? __int_as_float(0xff800000) : __int_as_float(0x7fffffff);
+  if (isinf(x)) return x;
+  int e;
+  float m = frexpf(x, &e);
+  if (m < 0.70710678f) { m = m * 2.0f; e -= 1; }
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float z = s * s;
+  float p = 0.09090909f;
+  p = __fmaf_rn(p, z, 0.11111111f);
+  p = __fmaf_rn(p, z, 0.14285715f);
+  p = __fmaf_rn(p, z, 0.2f);
+  p = __fmaf_rn(p, z, 0.33333334f);
+  p = __fmaf_rn(p, z, 1.0f);
+  return (float)e + (s * p) * 2.8853900817779268f;
+}
+
 // e^x of the merge and gather weights: Cody & Waite's two-constant reduction x = k ln2 + r (|r| <= ln2/2, the split of
 // ln2 keeps k * hi exact), e^r by its degree-7 Taylor polynomial in Horner form with fused multiply-adds,
 // e^x = 2^k e^r.  Relative error below 3e-7 on [-80, 88]; below -80 the result is 0.  The oracle evaluates the same f32

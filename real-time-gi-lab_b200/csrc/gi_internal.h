@@ -47,7 +47,23 @@ struct RcDev {
   float4 *mavg[2];         // merge: quad averages of the cascade above (ping-pong by cascade parity)
   const float *unorm8;     // [k] = k / 255.0f, [256 + k] = (k / 255.0f) / pi for k = 0..255 (IEEE quotients, host)
   const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)
+  const uint32_t *dyn_hdr; // the dynamic layer the traces read (gi_rc_set_dyn; null: none): header, pointers, data
+  const uint32_t *dyn_ptr;
+  const uint32_t *dyn_data;
+  uint32_t dyn_nb, pad_dyn;
 };
+
+// The dynamic layer (dynlayer.ts): header (64 words), a pointer per brick of every level (slot, DYN_EMPTY or
+// DYN_DROPPED), two bitsets of wanted bricks (bit order: coarse levels first), slot -> brick, per slot 16 words of its
+// non-zero voxels, per voxel of a slot 13 words (P+x P-x P+y P-y P+z P-z, area, area x radiance, area x albedo),
+// level 0 in fixed point (x 65536), the levels above as f32 after the resolve.
+struct DynDev {
+  uint32_t nb, albedo, first, end;   // brick pool; splat the albedo words; dynamic triangles [first, end)
+  uint32_t *hdr, *ptr, *bits, *meta, *mask, *data;
+  unsigned long long *look;          // the allocation's chained scan: ticket and block states
+  uint32_t look_cap, pad;
+};
+constexpr uint32_t DYN_W = 13, DYN_EMPTY = 0xffffffffu, DYN_DROPPED = 0xfffffffdu;
 
 // World probes (the method 'world', rc.ts:253-570): per cascade a hash table of probe keys, the probes compacted from
 // it in slot order, and the parents each probe merges; the c0 history of two solves.  Probes and atlas entries are laid
@@ -140,6 +156,10 @@ inline void vox_bounds(VoxDev &d) {
 }  // namespace gi
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
+// One build of the dynamic layer (mark .. resolve) in the voxel world's windows; frame: sun, style, light view; shadow:
+// the sun's S x S map or null (visibility 1)
+cudaError_t gi_launch_dyn_build(const gi::DynDev &d, const gi::VoxDev &v, const gi::SceneDev &s, const float *frame,
+                                const float *shadow, uint32_t S, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_shadow(const gi::SceneDev &s, const float *frame_dev, uint32_t S, const gi::ShadowRaster &sr,
                              uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.

@@ -323,6 +323,107 @@ __device__ __forceinline__ void trace_vox(const VoxDev &v, const float *__restri
   out.lvl = h.z; out.ptr = h.x; out.bit = h.y; out.tin = __float_as_uint(s.tIn);
 }
 
+// ---- the dynamic layer's read (dynlayer.ts:71-162) ------------------------------------------------------------------
+// dynFind: the data base of the voxel at p of level L, or of the first coarser level whose brick was not dropped;
+// 0xffffffff when empty.  lvl: the level read.
+__device__ __forceinline__ uint32_t dyn_find(const RcDev &r, const VoxDev &v, uint32_t L, f3 p, uint32_t &lvl) {
+  const int G = (int)v.G;
+  const uint32_t ug = v.G, nl = v.levels;
+  uint32_t l = L;
+  for (;;) {
+    const float vs = vox_size(v, l);
+    const i3 c = vfloori((p - mk(v.box_lo[l][0], v.box_lo[l][1], v.box_lo[l][2])) / vs);
+    lvl = l;
+    if (c.x < 0 || c.y < 0 || c.z < 0 || c.x >= G * 8 || c.y >= G * 8 || c.z >= G * 8) return 0xffffffffu;
+    const uint32_t ptr = __ldg(&r.dyn_ptr[l * ug * ug * ug + ((uint32_t)(c.z >> 3) * ug + (uint32_t)(c.y >> 3)) * ug
+                                           + (uint32_t)(c.x >> 3)]);
+    if (ptr == DYN_DROPPED && l + 1u < nl) { l++; continue; }
+    if (ptr >= r.dyn_nb) return 0xffffffffu;
+    return (ptr * 512u + (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7))) * DYN_W;
+  }
+}
+// dynWord: level 0 in fixed point, the levels above as resolved f32
+__device__ __forceinline__ float dyn_word(const RcDev &r, uint32_t base, uint32_t k, uint32_t L) {
+  const uint32_t u = __ldg(&r.dyn_data[base + k]);
+  return L == 0u ? (float)u / 65536.0f : __uint_as_float(u);
+}
+// dynRead: mean radiance and coverage per voxel length for direction d (the three faces against d)
+__device__ __forceinline__ float4 dyn_read(const RcDev &r, uint32_t base, uint32_t L, f3 d) {
+  if (base == 0xffffffffu) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float a = dyn_word(r, base, 6u, L);
+  if (a <= 0.0f) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const f3 ad = vabs(d);
+  const uint32_t sx = d.x > 0.0f ? 1u : 0u, sy = d.y > 0.0f ? 1u : 0u, sz = d.z > 0.0f ? 1u : 0u;
+  const float front = ad.x * dyn_word(r, base, sx, L) + ad.y * dyn_word(r, base, 2u + sy, L) + ad.z * dyn_word(r, base, 4u + sz, L);
+  return make_float4(dyn_word(r, base, 7u, L) / a, dyn_word(r, base, 8u, L) / a, dyn_word(r, base, 9u, L) / a, mn(front, 1.0f));
+}
+// traceDyn: covered radiance and coverage of [t0, t1] along d from o for a cone of width k t, read at the two levels
+// around the cone width and interpolated between them
+__device__ __forceinline__ float4 trace_dyn(const RcDev &r, const VoxDev &v, f3 o, f3 d, float t0, float t1, float k) {
+  const uint32_t *h = r.dyn_hdr;
+  if (h[0] == 0u || t1 <= t0) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const f3 bmin = adds(mk((float)h[2], (float)h[3], (float)h[4]), -1073741824.0f) * 0.01f;
+  const f3 bmax = adds(mk((float)h[5], (float)h[6], (float)h[7]), -1073741824.0f) * 0.01f;
+  const f3 dd = mk(fabsf(d.x) < 1e-9f ? 1e-9f : d.x, fabsf(d.y) < 1e-9f ? 1e-9f : d.y, fabsf(d.z) < 1e-9f ? 1e-9f : d.z);
+  const f3 qa = bmin - o, qb = bmax - o;
+  const f3 ta = mk(qa.x / dd.x, qa.y / dd.y, qa.z / dd.z), tb = mk(qb.x / dd.x, qb.y / dd.y, qb.z / dd.z);
+  const f3 tn = vmin(ta, tb), tf = vmax(ta, tb);
+  const float ba = mx(mx(mx(tn.x, tn.y), tn.z), t0);
+  const float bb = mn(mn(mn(tf.x, tf.y), tf.z), t1);
+  if (ba >= bb) return make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  const float v0 = v.v0;
+  const uint32_t nl = v.levels;
+  f3 rad = mk(0.0f, 0.0f, 0.0f);
+  float cov = 0.0f, t = t0;
+  for (uint32_t i = 0; i < 128u; i++) {
+    if (t >= bb || cov >= 1.0f) break;
+    const float w = mx(k * t, v0);
+    const float te = mn(t + 0.5f * w, t1);
+    if (te > ba) {
+      const float len = te - t;
+      const f3 p = o + d * (0.5f * (t + te));
+      const float lf = fclampf(gi_log2(w / v0), 0.0f, (float)(nl - 1u));
+      uint32_t L0 = (uint32_t)floorf(lf);
+      float f = lf - (float)L0;
+      const uint32_t Lw = vox_level_for(v, L0, p);
+      if (Lw != L0) { L0 = Lw; f = 0.0f; }
+      uint32_t la, lb;
+      const float4 sa = dyn_read(r, dyn_find(r, v, L0, p, la), la, d);
+      float aa = sa.w * len / vox_size(v, la);
+      f3 ra = mk(sa.x, sa.y, sa.z) * aa;
+      if (f > 0.0f && L0 + 1u < nl) {
+        const float4 sb = dyn_read(r, dyn_find(r, v, L0 + 1u, p, lb), lb, d);
+        const float ab = sb.w * len / vox_size(v, lb);
+        const f3 rb = mk(sb.x, sb.y, sb.z) * ab;
+        ra = ra * (1.0f - f) + rb * f;   // mix(ra, rb, f)
+        aa = aa * (1.0f - f) + ab * f;
+      }
+      if (aa > 0.0f) {
+        const float a = mn(aa, 1.0f - cov);
+        rad = rad + ra * (a / aa);
+        cov += a;
+      }
+    }
+    t = te;
+  }
+  return make_float4(rad.x, rad.y, rad.z, cov);
+}
+// traceWorld's read of the dynamic layer (rc.ts:223-231): in front of the static hit (or to t1 on a miss), from at
+// least one level-0 voxel out, composited over the voxel trace's result.  o: the probe; ooff: the trace's start (o moved
+// along the probe normal); k: the cone width per unit distance (3.5449077 / res).
+__device__ __forceinline__ void dyn_compose(const RcDev &r, const VoxDev &v, f3 o, f3 d, float t0, float t1, f3 ooff, float k,
+                                            TraceOut &out) {
+  if (!r.dyn_hdr || __ldg(&r.dyn_hdr[0]) == 0u) return;
+  float tS = t1;
+  if (out.T < 0.5f) tS = dot((ooff + d * __uint_as_float(out.tin)) - o, d);
+  const float4 dl = trace_dyn(r, v, o, d, mx(t0, v.v0), mn(t1, tS), k);
+  if (dl.w > 0.0f) {
+    const float s = 1.0f - dl.w;
+    out.rad = mk(dl.x + s * out.rad.x, dl.y + s * out.rad.y, dl.z + s * out.rad.z);
+    out.T = s * out.T;
+  }
+}
+
 // voxLevel (rc.ts:210-213), round(log2) taken exactly
 __device__ __forceinline__ uint32_t vox_level(const VoxDev &v, const RcDev &r, float s0, uint32_t c) {
   float vv = r.vox_scale * s0 * exp2_(r.level_map * (float)c);
@@ -406,8 +507,10 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
     f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
     uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
     float vs = vox_size(v, Lv);
-    trace_vox(v, F, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out,
-              InjectedBounce{r.bn_inj}, r.idirs + L.dir_off + di);
+    const f3 ooff = po + pn * (r.vox_offset * vs);
+    trace_vox(v, F, r.unorm8, ooff, dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out, InjectedBounce{r.bn_inj},
+              r.idirs + L.dir_off + di);
+    dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
     traced = true;
   }
   Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -965,7 +1068,7 @@ __global__ void __launch_bounds__(256) k_setup_batch(BatchDev B) {
 // Persistent over the rays of every solve: warps take 32 rays at a time; solves are padded to 32 rays, so a fetch
 // belongs to one solve
 template <int A>
-__global__ void __launch_bounds__(256) k_trace_batch(BatchDev B) {
+__global__ void __launch_bounds__(256, 4) k_trace_batch(BatchDev B) {
   grid_dep_wait();
   const uint32_t lane = threadIdx.x & 31u, total = B.ray_pre[B.n];
   for (;;) {

@@ -471,8 +471,10 @@ __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uin
     const f3 po = ld3(pr.pos), pn = ld3(pr.nrm);
     const uint32_t Lv = vox_level_for(v, r.plevel[L.probe_off + pi], po + dir * t1);
     const float vs = vox_size(v, Lv);
-    trace_vox(v, r.frame, r.unorm8, po + pn * (r.vox_offset * vs), dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out,
-              InjectedBounce{r.bn_inj}, r.idirs + L.dir_off + di);
+    const f3 ooff = po + pn * (r.vox_offset * vs);
+    trace_vox(v, r.frame, r.unorm8, ooff, dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out, InjectedBounce{r.bn_inj},
+              r.idirs + L.dir_off + di);
+    dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
     traced = true;
   }
   Atlas<A>::store(reinterpret_cast<T *>(r.rad), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -483,7 +485,7 @@ __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uin
 
 // Persistent trace over the rays of every cascade's live probes (first rays in state[16 ..]), probe-major
 template <int A>
-__global__ void __launch_bounds__(256) k_w_trace(RcDev r, VoxDev v, WorldDev w, uint32_t *ray_counter) {
+__global__ void __launch_bounds__(256, 4) k_w_trace(RcDev r, VoxDev v, WorldDev w, uint32_t *ray_counter) {
   grid_dep_wait();
   __shared__ uint32_t s_first[9];
   if (threadIdx.x <= r.cascades) s_first[threadIdx.x] = w.state[16 + threadIdx.x];

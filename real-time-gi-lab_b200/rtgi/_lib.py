@@ -83,6 +83,14 @@ SIGNATURES = {
     "gi_rc_set_timing": (C.c_int, [_P, C.c_int]),
     "gi_rc_pass_times": (C.c_int, [_P, _P]),
     "gi_rc_destroy": (C.c_int, [_P]),
+    "gi_scene_set_static_count": (C.c_int, [_P, C.c_uint32]),
+    "gi_dyn_create": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, C.POINTER(_P)]),
+    "gi_dyn_build": (C.c_int, [_P, _P, _P]),
+    "gi_dyn_read_counters": (C.c_int, [_P, _P, _P]),
+    "gi_dyn_read_state": (C.c_int, [_P, _P, _P, _P, _P, _P, _P]),
+    "gi_dyn_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
+    "gi_dyn_destroy": (C.c_int, [_P]),
+    "gi_rc_set_dyn": (C.c_int, [_P, _P]),
 }
 
 

@@ -63,6 +63,10 @@ class SceneGpu:
         """The rasters draw rows [0, count) (a world's clustered copies are voxelised only)."""
         _lib.call("gi_scene_set_draw_count", self.handle, int(count))
 
+    def set_static_count(self, count: int) -> None:
+        """The voxel rebuild reads rows [0, count) (createVoxWorld's firstDynamicTri); the rest are dynamic."""
+        _lib.call("gi_scene_set_static_count", self.handle, int(count))
+
     def set_draw_instances(self, offsets) -> None:
         """The rasters draw the drawn rows at every offset (instance 0 at the origin; None: once)."""
         if offsets is None or len(offsets) <= 1:
@@ -292,6 +296,10 @@ class Rc:
         _lib.call("gi_rc_set_stats", self.handle, level)
         self.params.stats = level
 
+    def set_dyn(self, dyn: Optional["DynLayer"]):
+        """The dynamic layer the traces read (gi_rc_set_dyn); gi_solve builds it after the static rebuild."""
+        _lib.call("gi_rc_set_dyn", self.handle, dyn.handle if dyn is not None else None)
+
     def set_debug_hits(self, on: bool):
         _lib.call("gi_rc_set_debug_hits", self.handle, 1 if on else 0)
 
@@ -393,6 +401,40 @@ class Rc:
     def destroy(self):
         if self.handle:
             _lib.call("gi_rc_destroy", self.handle)
+            self.handle = None
+
+
+class DynLayer:
+    """The dynamic layer (dynlayer.ts createDynLayer / DynLayer) of a voxel world: its scene's rows from first_dynamic
+    on, splatted every build; bind it to an Rc (Rc.set_dyn) for its traces to read it."""
+
+    def __init__(self, vox: VoxWorld, first_dynamic: int, bricks: int = 512, albedo: bool = False):
+        h = C.c_void_p()
+        _lib.call("gi_dyn_create", vox.handle, bricks, first_dynamic, 1 if albedo else 0, C.byref(h))
+        self.handle, self.vox, self.bricks = h, vox, bricks
+
+    def build(self, rc: "Rc", stream=None) -> None:
+        _lib.call("gi_dyn_build", self.handle, rc.handle, _stream(stream))
+
+    def read_counters(self, stream=None) -> dict:
+        hdr = np.zeros(64, np.uint32)
+        _lib.call("gi_dyn_read_counters", self.handle, _ptr(hdr), _stream(stream))
+        return {"bricks": int(hdr[8]), "brickOverflow": int(hdr[1]), "outside": int(hdr[9]), "hdr": hdr}
+
+    def read_state(self, stream=None) -> dict:
+        p = self.vox.params
+        nptr = p.levels * p.G ** 3
+        st = {"ptr": np.zeros(nptr, np.uint32), "bits": np.zeros(2 * nptr // 32, np.uint32),
+              "meta": np.zeros(self.bricks, np.uint32), "mask": np.zeros(self.bricks * 16, np.uint32),
+              "data": np.zeros(self.bricks * 512 * 13, np.uint32)}
+        _lib.call("gi_dyn_read_state", self.handle, *[_ptr(st[k]) for k in ("ptr", "bits", "meta", "mask", "data")],
+                  _stream(stream))
+        st["hdr"] = self.read_counters(stream)["hdr"]
+        return st
+
+    def destroy(self):
+        if self.handle:
+            _lib.call("gi_dyn_destroy", self.handle)
             self.handle = None
 
 
