@@ -1220,6 +1220,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
       return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has another atlas format or probe spacing than solve 0", i);
     if (r->bounce) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has multi-bounce on (capture its chain with gi_batch_capture)", i);
     if (r->world) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u has world probes (capture its chain with gi_batch_capture)", i);
+    if (r->dyn) return fail(GI_ERR_INVALID, "gi_batch_capture_passes: solve %u reads a dynamic layer (capture its chain with gi_batch_capture)", i);
   }
   const uint32_t P0 = r0.c[0].tile_size;
   if (P0 != 8u && P0 != 16u && P0 != 32u)

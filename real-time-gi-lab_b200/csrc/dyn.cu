@@ -5,7 +5,7 @@
 // Passes (dynlayer.ts:592): mark (thread per dynamic triangle: splat level, wanted bricks, bounds), parents (thread per
 // bitset word: every wanted brick wants its ancestors), alloc (the reference's count + alloc as one chained scan over
 // the bitset words: slots by rank in bit order, bricks only wanted last frame emptied), finalize (one thread), clear
-// (thread per voxel of the allocated bricks), splat (thread per dynamic triangle, its m^2 samples added in fixed point
+// (thread per voxel of the allocated bricks), splat (a warp per dynamic triangle, its m^2 samples added in fixed point
 // with atomics: exact sums, so the result is the reference's whatever the order), resolve (per level from fine to
 // coarse, thread per voxel).  The reference gathers a workgroup's samples in a window of workgroup memory before adding
 // them; here every sample is added to the layer, and a voxel is marked non-zero when a sample's weight on it is
@@ -227,11 +227,13 @@ __device__ __forceinline__ void splat_sample(const DynDev &d, const VoxDev &v, u
   }
 }
 
-// splat (dynlayer.ts:458-526): thread per dynamic triangle, its m^2 sub-triangles' centroids as samples
+// splat (dynlayer.ts:458-526): a warp per dynamic triangle, its m^2 sub-triangles' centroids dealt over the lanes (a
+// sample's sums are fixed point, so which lane adds it and when changes nothing).  Sample q of row u: the row's m - u
+// upright sub-triangles first, then its m - u - 1 flipped ones.
 __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev s, const float *__restrict__ F,
                                                    const float *__restrict__ map, uint32_t S) {
   grid_dep_wait();
-  const uint32_t t = d.first + blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t t = d.first + (blockIdx.x * blockDim.x + threadIdx.x) / 32u, lane = threadIdx.x & 31u;
   if (t >= d.end) return;
   const uint4 ti = s.tri[t];
   const f3 a = dyn_pos(s, ti.x), b = dyn_pos(s, ti.y), c = dyn_pos(s, ti.z);
@@ -244,19 +246,19 @@ __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev 
   const float fm = (float)m, sa = area / (fm * fm);
   const gi_material mat = s.mats[ti.w];
   const f3 n0 = dyn_nrm(s, ti.x), n1 = dyn_nrm(s, ti.y), n2 = dyn_nrm(s, ti.z);
-  for (uint32_t u = 0; u < m; u++)
-    for (uint32_t vv = 0; vv + u < m; vv++)
-      for (uint32_t flip = 0; flip < 2u; flip++) {
-        if (flip == 1u && u + vv + 1u >= m) continue;
-        const float off = flip == 1u ? 2.0f / 3.0f : 1.0f / 3.0f;
-        const float wb = ((float)u + off) / fm, wc = ((float)vv + off) / fm, wa = (1.0f - wb) - wc;
-        const f3 p = (a * wa + b * wb) + c * wc;
-        f3 nr = (n0 * wa + n1 * wb) + n2 * wc;
-        nr = normalize3(dot(nr, nr) > 1e-12f ? nr : cross(b - a, c - a));
-        f3 rad, alb;
-        if (!shade_sample(mat, F, map, S, p, nr, rad, alb)) continue;
-        splat_sample(d, v, L, p, nr, sa, rad, alb);
-      }
+  for (uint32_t q = lane; q < m * m; q += 32u) {
+    uint32_t u = 0, r = q;
+    while (r >= 2u * (m - u) - 1u) { r -= 2u * (m - u) - 1u; u++; }
+    const uint32_t flip = r >= m - u ? 1u : 0u, vv = flip ? r - (m - u) : r;
+    const float off = flip == 1u ? 2.0f / 3.0f : 1.0f / 3.0f;
+    const float wb = ((float)u + off) / fm, wc = ((float)vv + off) / fm, wa = (1.0f - wb) - wc;
+    const f3 p = (a * wa + b * wb) + c * wc;
+    f3 nr = (n0 * wa + n1 * wb) + n2 * wc;
+    nr = normalize3(dot(nr, nr) > 1e-12f ? nr : cross(b - a, c - a));
+    f3 rad, alb;
+    if (!shade_sample(mat, F, map, S, p, nr, rad, alb)) continue;
+    splat_sample(d, v, L, p, nr, sa, rad, alb);
+  }
 }
 
 // resolve (dynlayer.ts:527-587) of level L >= 1: own splats (fixed point) + a quarter of each non-zero child (fixed
@@ -320,7 +322,7 @@ cudaError_t gi_launch_dyn_build(const DynDev &d, const VoxDev &v, const SceneDev
   GI_TRY(gi_launch(k_dyn_alloc, (nw + 255u) / 256u, 256, st, d, v));
   GI_TRY(gi_launch(k_dyn_finalize, 1, 1, st, d, v));
   GI_TRY(gi_launch(k_dyn_clear, persist, 256, st, d));
-  GI_TRY(gi_launch(k_dyn_splat, (nt + 255u) / 256u, 256, st, d, v, s, frame, shadow, S));
+  GI_TRY(gi_launch(k_dyn_splat, (nt * 32u + 255u) / 256u, 256, st, d, v, s, frame, shadow, S));
   for (uint32_t L = 1; L < v.levels; L++) GI_TRY(gi_launch(k_dyn_resolve, persist, 256, st, d, v, L));
   return cudaGetLastError();
 }

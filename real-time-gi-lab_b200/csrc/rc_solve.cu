@@ -480,7 +480,7 @@ __global__ void k_setup_screen(RcDev r, VoxDev v) {
 
 // trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) of the ray at position j of the trace order (cascade c): writes
 // its atlas element (and the debug copies); true when its probe is valid and the ray was marched.
-template <int A>
+template <int A, bool DYN = false>
 __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, TraceOut &out) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
@@ -510,7 +510,7 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
     const f3 ooff = po + pn * (r.vox_offset * vs);
     trace_vox(v, F, r.unorm8, ooff, dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out, InjectedBounce{r.bn_inj},
               r.idirs + L.dir_off + di);
-    dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
+    if (DYN) dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
     traced = true;
   }
   Atlas<A>::store(rad, i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -520,7 +520,7 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
 }
 
 // Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time.
-template <int A>
+template <int A, bool DYN>
 __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
   grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
@@ -538,7 +538,7 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
     uint32_t c = live ? casc_of_ray(r, j) : 0u;
     TraceOut out;
     out.steps = 0;
-    bool traced = live && trace_ray<A>(r, v, j, c, out);
+    bool traced = live && trace_ray<A, DYN>(r, v, j, c, out);
     if (r.stats) {
       // per-cascade counters (rc.ts:232-235); flush when the lane's cascade changes
       if (live && traced) {
@@ -1068,7 +1068,7 @@ __global__ void __launch_bounds__(256) k_setup_batch(BatchDev B) {
 // Persistent over the rays of every solve: warps take 32 rays at a time; solves are padded to 32 rays, so a fetch
 // belongs to one solve
 template <int A>
-__global__ void __launch_bounds__(256, 4) k_trace_batch(BatchDev B) {
+__global__ void __launch_bounds__(256) k_trace_batch(BatchDev B) {
   grid_dep_wait();
   const uint32_t lane = threadIdx.x & 31u, total = B.ray_pre[B.n];
   for (;;) {
@@ -1170,7 +1170,9 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
-  GI_TRY(gi_launch(k_trace<A>, tb, 256, st, r, v, counter));
+  // the dynamic layer's read is compiled into a kernel of its own: without a layer the trace keeps its registers
+  if (r.dyn_hdr) GI_TRY(gi_launch(k_trace<A, true>, tb, 256, st, r, v, counter));
+  else GI_TRY(gi_launch(k_trace<A, false>, tb, 256, st, r, v, counter));
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];

@@ -455,7 +455,7 @@ __global__ void __launch_bounds__(256) k_w_build(RcDev r, VoxDev v, WorldDev w, 
 }
 
 // trace (rc.ts:600-622) of ray (pi, di) of a world probe of cascade c into atlas element i
-template <int A>
+template <int A, bool DYN>
 __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uint32_t c, uint32_t pi, uint32_t di,
                                             size_t i, TraceOut &out) {
   typedef typename Atlas<A>::T T;
@@ -474,7 +474,7 @@ __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uin
     const f3 ooff = po + pn * (r.vox_offset * vs);
     trace_vox(v, r.frame, r.unorm8, ooff, dir, t0, t1, r.vox_skip * vs, Lv, r.dda_cap, out, InjectedBounce{r.bn_inj},
               r.idirs + L.dir_off + di);
-    dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
+    if (DYN) dyn_compose(r, v, po, dir, t0, t1, ooff, 3.5449077f / (float)L.res, out);
     traced = true;
   }
   Atlas<A>::store(reinterpret_cast<T *>(r.rad), i, make_float4(out.rad.x, out.rad.y, out.rad.z, out.T));
@@ -484,8 +484,8 @@ __device__ __forceinline__ bool w_trace_ray(const RcDev &r, const VoxDev &v, uin
 }
 
 // Persistent trace over the rays of every cascade's live probes (first rays in state[16 ..]), probe-major
-template <int A>
-__global__ void __launch_bounds__(256, 4) k_w_trace(RcDev r, VoxDev v, WorldDev w, uint32_t *ray_counter) {
+template <int A, bool DYN>
+__global__ void __launch_bounds__(256) k_w_trace(RcDev r, VoxDev v, WorldDev w, uint32_t *ray_counter) {
   grid_dep_wait();
   __shared__ uint32_t s_first[9];
   if (threadIdx.x <= r.cascades) s_first[threadIdx.x] = w.state[16 + threadIdx.x];
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(256, 4) k_w_trace(RcDev r, VoxDev v, WorldDev 
       if (live) {
         const CascDev &L = r.c[c];
         const uint32_t t = j - s_first[c];
-        traced = w_trace_ray<A>(r, v, c, t >> L.dirs_log2, t & ((1u << L.dirs_log2) - 1u), (size_t)L.rad_off + t, out);
+        traced = w_trace_ray<A, DYN>(r, v, c, t >> L.dirs_log2, t & ((1u << L.dirs_log2) - 1u), (size_t)L.rad_off + t, out);
       }
       if (r.stats && live && traced) {   // per-cascade counters (rc.ts:232-235)
         if (c != cur_c && cur_c != 0xffffffffu) {
@@ -783,7 +783,8 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
   if (ev) cudaEventRecord(ev[1], st);
   if (bn) GI_TRY(launch_bounce(*bn, v, r.frame, r.unorm8, sm_count, st));
   const uint32_t tb = sm_count * (ls ? ls->trace_blocks : 8u);
-  GI_TRY(gi_launch(k_w_trace<A>, tb, 256, st, r, v, w, counter));
+  if (r.dyn_hdr) GI_TRY(gi_launch(k_w_trace<A, true>, tb, 256, st, r, v, w, counter));
+  else GI_TRY(gi_launch(k_w_trace<A, false>, tb, 256, st, r, v, w, counter));
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)N - 1; c >= 0; c--)
     GI_TRY(gi_launch(k_w_merge<A>, blocks((uint64_t)w.cap[c] << r.c[c].dirs_log2), 256, st, r, w, (uint32_t)c));
