@@ -14,6 +14,7 @@ value is all ranks' solves over the slowest rank's device time.  Rank 0 prints o
 WGSL through Dawn) cannot run here, so its CPU restatement (oracle/) runs with every host thread.
 """
 import argparse
+import dataclasses
 import json
 import math
 import os
@@ -36,14 +37,14 @@ def workload(name):
     if name == "colonnade":
         s = scenes.colonnade_scene(0)
         W, H = 1920, 1080
-        p = configs.parse_config("screen-8-voxel-f32-dda256", {"cascades": 5})
+        p = configs.parse_config("screen-8-voxel-f32-dda256-irr16", {"cascades": 5})
         v = configs.vox_params({"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22})
         sun_e, sky = s.sun_e, s.sky
         shadow = fr.SHADOW_SIZE   # the sun's shadow map over the scene (voxSun in every rebuild)
     else:
         s = scenes.room_scene(0)
         W, H = 256, 256
-        p = configs.parse_config("screen-8-voxel-f32-dda64", {"cascades": 2})
+        p = configs.parse_config("screen-8-voxel-f32-dda64-irr16", {"cascades": 2})
         v = configs.vox_params({"v0": 0.16, "levels": 1, "G": 8, "maxBricks": 512, "maxVoxels": 1 << 18})
         sun_e, sky = (0.0, 0.0, 0.0), (0.0, 0.0, 0.0)
         shadow = 0                # sun off
@@ -54,9 +55,12 @@ def workload(name):
     F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=sun_e, sky=sky,
                                      cascades=p.cascades, P=p.P, light_view_proj=lvp, shadow_bias=bias))
     desc = {"workload": f"{name}: {s.triangle_count} triangles, clipmap {v.levels} x {v.G * 8}^3 voxels from "
-                        f"{v.v0} m, {p.cascades} cascades at {W}x{H}, DDA cap {p.ddaCap}, atlas {p.atlas}",
+                        f"{v.v0} m, {p.cascades} cascades at {W}x{H}, DDA cap {p.ddaCap}, atlas {p.atlas}, "
+                        f"irradiance {'rgba16float' if p.irr16 else 'rgba32float'}",
             "triangles": s.triangle_count, "resolution": [W, H], "cascades": p.cascades, "levels": v.levels,
             "G": v.G, "v0": v.v0, "dda_cap": p.ddaCap, "atlas": p.atlas, "method": "screen-8-voxel",
+            "irradiance": "rgba16float, the reference's rc.irr format (rc.ts:1073); every pass before the store in f32"
+                          if p.irr16 else "rgba32float",
             "shadow_map": shadow}
     if shadow:
         desc["workload"] += f", sun shadow map {shadow}^2"
@@ -288,25 +292,30 @@ def run_precision(args, ctx):
     return r
 
 
-def run_served(args, ctx):
+def run_served(args, ctx, rank=0, world=1):
     """The serving loop (continuous batching, 8 slots, HBM budget 150 GB, f16 atlases) against the plain one-at-a-time
     loop, on Poisson request streams at several rates over 12 resident scenes of the batch distribution, each with
-    1-200 moving objects.  Latency = arrival to irradiance in host memory (host wall clock)."""
-    from rtgi import autotune, scenes, serve
+    1-200 moving objects.  Latency = arrival to irradiance in host memory (host wall clock).  On N GPUs the stream's
+    rate is the whole job's: requests are routed to the ranks owning their scenes (rtgi.route), each rank serves its
+    share, and the statistics pool every rank's requests."""
+    from rtgi import autotune, route, scenes, serve
     specs = [scenes.batch_spec(1000 + s) for s in range(12)]
     ex = serve.GpuExecutor(ctx, slots=8, atlas="f16", tuner=autotune.Autotuner(reps=3))
     srv = serve.Server(ex, specs, slots=8, hbm_budget=150e9)
-    for i, sp in enumerate(specs):   # scenes resident before the streams start
+    rs = route.RoutedServer(lambda mine: srv, specs, rank, world)
+    for i in rs.mine:   # this rank's scenes resident before the streams start
         srv._ensure_resident(i, 0.0)
     plain = serve.PlainExecutor(ex)
+    served = lambda reqs: rs.run(reqs)
+    plained = lambda reqs: rs.run_with(lambda mine, clock: serve.plain_loop(plain, mine, clock), reqs)
     # warm-up of both paths (every slot's stream)
-    serve.plain_loop(plain, serve.poisson_arrivals(1000.0, 24, len(specs), seed=7))
-    srv.run(serve.poisson_arrivals(4000.0, 64, len(specs), seed=7))
+    plained(serve.poisson_arrivals(1000.0 * world, 24 * world, len(specs), seed=7))
+    served(serve.poisson_arrivals(4000.0 * world, 64 * world, len(specs), seed=7))
     rates = []
     for rate in args.serve_rates:
         n = int(min(args.serve_max, max(50, rate * args.serve_seconds)))
-        st = srv.run(serve.poisson_arrivals(rate, n, len(specs)))
-        pl = serve.plain_loop(plain, serve.poisson_arrivals(rate, n, len(specs)))
+        st = served(serve.poisson_arrivals(rate, n, len(specs)))
+        pl = plained(serve.poisson_arrivals(rate, n, len(specs)))
         rates.append({"rate": rate, "requests": n, "served": st, "plain": pl,
                       "throughput_ratio": st["solves_per_s"] / pl["solves_per_s"]})
     # the criterion as worded: per path the highest sustained rate whose p99 stays within a budget, on a rate grid
@@ -315,8 +324,8 @@ def run_served(args, ctx):
     sweep = {"served": [], "plain": []}
     for rate in grid:
         n = int(min(args.serve_max, max(200, rate * 0.5)))
-        sweep["served"].append((rate, srv.run(serve.poisson_arrivals(rate, n, len(specs), seed=11))))
-        sweep["plain"].append((rate, serve.plain_loop(plain, serve.poisson_arrivals(rate, n, len(specs), seed=11))))
+        sweep["served"].append((rate, served(serve.poisson_arrivals(rate, n, len(specs), seed=11))))
+        sweep["plain"].append((rate, plained(serve.poisson_arrivals(rate, n, len(specs), seed=11))))
     budgets = {}
     for b in (2.0, 5.0):
         best = {}
@@ -333,6 +342,7 @@ def run_served(args, ctx):
     res_bytes = srv.resident_bytes()
     ex.destroy()
     return {"scenes": len(specs), "slots": 8, "atlas": "f16", "hbm_budget_bytes": 150e9, "resident_bytes": res_bytes,
+            "ranks": world, "owners": rs.owners,
             "objects_per_scene": [ex.n_objects(sp) for sp in specs], "rates": rates,
             "ratio_at_p99_budget": budgets,
             "sweep": {path: [{"rate": rate, "solves_per_s": r["solves_per_s"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"]}
@@ -600,6 +610,39 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
     return out
 
 
+def run_e2e(ctx, vw, p, W, H, F, host, shadow, tuned, n, dist, world, slots=2):
+    """Solves/s through rtgi.pipeline with host buffers: every step uploads its frame and G-buffer from pinned memory
+    and downloads its irradiance into pinned memory, the copies of neighbouring frames overlapping the solve."""
+    import torch
+    from rtgi import pipeline
+    frame_h, depth_h, normal_h = host
+    pipe = pipeline.FramePipeline(ctx, vw, p, W, H, F, depth_h.data_ptr(), normal_h.data_ptr(), slots=slots,
+                                  shadow=shadow, tuning=tuned["rc"])
+    irr_h = [torch.empty(pipe.irr_bytes, dtype=torch.uint8).pin_memory() for _ in range(slots)]
+    for k in range(2 * slots):
+        pipe.submit(frame_h.data_ptr(), depth_h.data_ptr(), normal_h.data_ptr(), irr_h[k % slots].data_ptr())
+    pipe.wait()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for k in range(n):
+        pipe.submit(frame_h.data_ptr(), depth_h.data_ptr(), normal_h.data_ptr(), irr_h[k % slots].data_ptr())
+    pipe.wait()
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - e0
+    pipe.destroy()
+    value = whole_job_rate(n, max_over_ranks(e2e_s, dist, "cuda"), world)
+    if dist:
+        dist.barrier()
+    return {"value": value, "unit": "solves/s",
+            "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
+            "d2h_bytes_per_step": int(irr_h[0].numel()), "steps": n,
+            "irradiance": "rgba16float" if p.irr16 else "rgba32float",
+            "mode": f"rtgi.pipeline: copies of neighbouring frames overlap the solve ({slots} cascade sets); wall "
+                    "clock around the steps, max over ranks"}
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     torch.cuda.set_device(local_rank)
@@ -687,30 +730,17 @@ def run_ours(args, rank, world, local_rank):
     # end to end through the public API with host buffers: every step copies its frame + G-buffer from pinned host
     # memory and reads its irradiance back into pinned host memory; rtgi.pipeline overlaps those copies of
     # neighbouring frames with the solve (two cascade sets, upload / compute / download streams)
-    from rtgi import pipeline
     depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
     normal_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_NORMAL).view(np.uint16).copy()).pin_memory()
     frame_h = torch.from_numpy(F.copy()).pin_memory()
-    pipe = pipeline.FramePipeline(ctx, vw, p, W, H, F, depth_h.data_ptr(), normal_h.data_ptr(), slots=2,
-                                  shadow=(sg, desc["shadow_map"]) if desc["shadow_map"] else None)
-    irr_h = [torch.empty(pipe.irr_bytes, dtype=torch.uint8).pin_memory() for _ in range(2)]
-    n_e2e = max(3, min(n_ev, 400))
-    for k in range(4):
-        pipe.submit(frame_h.data_ptr(), depth_h.data_ptr(), normal_h.data_ptr(), irr_h[k % 2].data_ptr())
-    pipe.wait()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    e0 = time.perf_counter()
-    for k in range(n_e2e):
-        pipe.submit(frame_h.data_ptr(), depth_h.data_ptr(), normal_h.data_ptr(), irr_h[k % 2].data_ptr())
-    pipe.wait()
-    torch.cuda.synchronize()
-    e2e_s = time.perf_counter() - e0
-    pipe.destroy()
-    e2e_value = whole_job_rate(n_e2e, max_over_ranks(e2e_s, dist, "cuda"), world)
-    if dist:
-        dist.barrier()
+    host = (frame_h, depth_h, normal_h)
+    shadow_in = (sg, desc["shadow_map"]) if desc["shadow_map"] else None
+    e2e_out = run_e2e(ctx, vw, p, W, H, F, host, shadow_in, tuned, max(3, min(n_ev, 400)), dist, world)
+    # the same with the irradiance stored and read back as f32 (twice the download)
+    e2e_f32 = None
+    if p.irr16:
+        e2e_f32 = run_e2e(ctx, vw, dataclasses.replace(p, irr16=False), W, H, F, host, shadow_in, tuned,
+                          max(3, min(n_ev, 400)), dist, world)
 
     # two frames in flight: a second voxel world and cascade set solve the same workload on a second stream, the two
     # captured solves launched side by side (what a renderer does with consecutive frames); device time of the job
@@ -825,10 +855,8 @@ def run_ours(args, rank, world, local_rank):
                "roofline": {"kernel": "k_trace (giTrace)", "bound": "hbm", "achieved": achieved, "peak": peak,
                             "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                             "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": trace_ms},
-               "e2e": {"value": e2e_value, "unit": "solves/s",
-                       "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
-                       "d2h_bytes_per_step": int(irr_h[0].numel()),
-                       "mode": "rtgi.pipeline: copies of neighbouring frames overlap the solve (2 cascade sets)"},
+               "e2e": e2e_out,
+               "e2e_irr_f32": e2e_f32,
                "gpu_launches": n_ev * (11 + (1 if v.levels > 1 else 0) + 3 + p.cascades),
                "clocks": clk, "wall_s": wall}
     if args.batch > 0:
@@ -836,7 +864,7 @@ def run_ours(args, rank, world, local_rank):
         if out is not None:
             out["batched"] = bt
     if args.serve_rates:
-        sv = run_served(args, ctx)
+        sv = run_served(args, ctx, rank, world)
         if out is not None:
             out["served"] = sv
     if args.precision_frames > 0:

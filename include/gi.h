@@ -87,7 +87,10 @@ typedef struct {
   uint32_t atlas;        /* gi_atlas */
   uint32_t f32_out;      /* 1: SH and irradiance stored as f32 whatever the atlas (the reference stores both f16,
                             rc.ts:768-773, :1073); 0: stored like the atlas, f16 for F16/BF16 */
-  uint32_t reserved[4];
+  uint32_t irr_f16;      /* 1: the irradiance stored as rgba16float whatever the atlas and f32_out (the format of the
+                            reference's rc.irr texture, rc.ts:1073): every pass before the store keeps its precision,
+                            the store rounds to nearest even; half the bytes of an f32 readback */
+  uint32_t reserved[3];
 } gi_rc_params;
 
 /* World probes (RcParams.method 'world', rc.ts:253-570): probes on a world-space grid registered from the G-buffer's

@@ -116,7 +116,7 @@ class OrcCasc(C.Structure):
 class OrcLayout(C.Structure):
     _fields_ = [("cascades", C.c_uint32), ("c", OrcCasc * 8), ("vox_scale", C.c_float), ("vox_offset", C.c_float),
                 ("level_map", C.c_float), ("vox_skip", C.c_float), ("dda_cap", C.c_uint32), ("stats", C.c_uint32),
-                ("atlas", C.c_uint32), ("f32_out", C.c_uint32)]
+                ("atlas", C.c_uint32), ("f32_out", C.c_uint32), ("irr_f16", C.c_uint32)]
 
 
 class OrcGbuf(C.Structure):
@@ -229,6 +229,7 @@ def layout_struct(lay: dict) -> OrcLayout:
     ly.vox_scale, ly.vox_offset, ly.level_map, ly.vox_skip = lay["vox_scale"], lay["vox_offset"], lay["level_map"], lay["vox_skip"]
     ly.dda_cap, ly.stats, ly.atlas = lay["dda_cap"], lay["stats"], lay["atlas"]
     ly.f32_out = lay.get("f32_out", 0)
+    ly.irr_f16 = lay.get("irr_f16", 0)
     return ly
 
 

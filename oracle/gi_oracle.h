@@ -139,6 +139,7 @@ typedef struct {
   uint32_t stats;         /* 0 off, 1 DDA step counters (rc.ts:232-235) */
   uint32_t atlas;         /* 0: f32 storage, 1: f16 (the reference's rgba16 packing), 2: bf16 */
   uint32_t f32_out;       /* 1: SH and irradiance stored as f32 whatever the atlas */
+  uint32_t irr_f16;       /* 1: irradiance stored as rgba16float whatever the atlas and f32_out */
 } orc_layout;
 
 /* One probe (rc.ts:157): pos.xyz + s0, nrm.xyz + view depth, grid. 48 bytes. */

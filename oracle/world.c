@@ -376,7 +376,7 @@ static void w_gather_range(void *p, uint64_t b, uint64_t e) {
   const orc_vox *vx = j->cx->vx;
   const float *F = g->frame;
   int32_t W = (int32_t)g->width;
-  uint32_t out_fmt = (ly->atlas == 0 || ly->f32_out) ? 0u : 1u;
+  uint32_t out_fmt = ((ly->atlas == 0 || ly->f32_out) && !ly->irr_f16) ? 0u : 1u;
   for (int32_t py = (int32_t)b; py < (int32_t)e; py++)
     for (int32_t px = 0; px < W; px++) {
       size_t q = (size_t)py * (size_t)W + (size_t)px;

@@ -725,6 +725,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   d.dda_cap = p->dda_cap; d.stats = p->stats;
   d.trace_order = 0; d.trace_rays = 1;
   d.f32_out = p->f32_out ? 1u : 0u;
+  d.irr_f16 = p->irr_f16 ? 1u : 0u;
   // cascade layout (rc.ts:1027-1035)
   uint64_t probe_total = 0, ray_total = 0, dir_total = 0;
   for (uint32_t i = 0; i < p->cascades; i++) {
@@ -760,7 +761,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   d.rays_total = (uint32_t)ray_total;
   r->rad_elem_bytes = atlas_elem_bytes(p->atlas);
   r->sh_elem_bytes = p->f32_out ? 16u : r->rad_elem_bytes;
-  r->irr_elem_bytes = p->f32_out ? 16u : atlas_elem_bytes(p->atlas);
+  r->irr_elem_bytes = p->irr_f16 ? 8u : p->f32_out ? 16u : atlas_elem_bytes(p->atlas);
   r->sh_elems = (size_t)d.c[0].tiles_x * d.c[0].tiles_y * 8u;
   size_t npx = (size_t)W * H;
   r->ntiles = gi_raster_tiles(W, H);

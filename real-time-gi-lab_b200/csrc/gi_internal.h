@@ -30,7 +30,8 @@ struct RcDev {
   float vox_scale, vox_offset, level_map, vox_skip;
   uint32_t dda_cap, stats, probes_total, rays_total;
   uint32_t trace_order, trace_rays;   // tuning of k_trace (gi_rc_tuning)
-  uint32_t f32_out, pad_t;            // SH and irradiance stored as f32 whatever the atlas
+  uint32_t f32_out;                   // SH and irradiance stored as f32 whatever the atlas
+  uint32_t irr_f16;                   // irradiance stored as rgba16f whatever the atlas and f32_out
   const float *frame;      // 160 words (packFrame)
   const float *depth;      // W*H
   const uint2 *normal;     // W*H rgba16f
@@ -40,7 +41,7 @@ struct RcDev {
   const float4 *idirs;     // the same directions' 1 / d (tiny components clamped as traceVox does), after dirs
   void *rad;               // rays_total atlas elements
   void *sh;                // probes of cascade 0 x 8 atlas elements
-  void *irr;               // W*H: float4 (atlas F32) or rgba16f (uint2)
+  void *irr;               // W*H: float4 (atlas F32 or f32_out, without irr_f16) or rgba16f (uint2)
   uint32_t *counts;        // 80 words
   uint4 *hits;             // optional: per ray (level, brick, bit, tIn bits)
   void *rad_traced;        // optional: copy of the atlas after the trace

@@ -763,7 +763,7 @@ __device__ __forceinline__ void gather_pixel(const RcDev &r, uint32_t px, uint32
     }
     if (ws > 0.0f) res = e / ws;
   }
-  if (A == GI_ATLAS_F32 || r.f32_out) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
+  if ((A == GI_ATLAS_F32 || r.f32_out) && !r.irr_f16) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
   else reinterpret_cast<uint2 *>(r.irr)[q] = make_uint2((uint32_t)f2h(res.x) | ((uint32_t)f2h(res.y) << 16),
                                                        (uint32_t)f2h(res.z) | ((uint32_t)f2h(alpha) << 16));
 }
@@ -1129,7 +1129,7 @@ __global__ void k_irr_to_f32(RcDev r, float4 *dst) {
   grid_dep_wait();
   size_t n = (size_t)r.width * r.height;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    if (r.atlas == GI_ATLAS_F32 || r.f32_out) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
+    if ((r.atlas == GI_ATLAS_F32 || r.f32_out) && !r.irr_f16) dst[i] = reinterpret_cast<const float4 *>(r.irr)[i];
     else {
       uint2 u = reinterpret_cast<const uint2 *>(r.irr)[i];
       dst[i] = make_float4(h2f(u.x & 0xffffu), h2f(u.x >> 16), h2f(u.y & 0xffffu), h2f(u.y >> 16));

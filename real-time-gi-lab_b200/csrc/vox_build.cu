@@ -353,9 +353,14 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
   if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return;
   uint32_t wi = ptr * 16u + (bit >> 5);
   uint32_t msk = 1u << (bit & 31u);
-  if ((v.occ[wi] & msk) == 0u) atomicOr(&v.occ[wi], msk);
   uint32_t ri = ptr * 512u + bit;
+#if GI_VB_NOREAD
+  atomicOr(&v.occ[wi], msk);
+  atomicMax(&v.rep[ri], t + 1u);
+#else
+  if ((v.occ[wi] & msk) == 0u) atomicOr(&v.occ[wi], msk);
   if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
+#endif
 }
 
 // voxBits (voxel.ts:492-513)
@@ -500,8 +505,13 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
       uint32_t grp = __match_any_sync(0xffffffffu, ok ? wi : 0xffffffffu);
       uint32_t m = __reduce_or_sync(grp, msk);
       if (ok) {
+#if GI_VB_NOREAD
+        if ((uint32_t)(__ffs(grp) - 1) == lane) atomicOr(&v.occ[wi], m);
+        atomicMax(&v.rep[ri], t + 1u);
+#else
         if ((uint32_t)(__ffs(grp) - 1) == lane && (v.occ[wi] & m) != m) atomicOr(&v.occ[wi], m);
         if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
+#endif
       }
     }
   }
@@ -655,11 +665,23 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t nv = nb ? min(v.vpre[nb], v.max_voxels) : 0u;
   for (uint32_t ai = blockIdx.x * blockDim.x + threadIdx.x; ai < nv; ai += gridDim.x * blockDim.x) {
+#if GI_RA_WARPSEARCH
+    // the last brick b with vpre[b] <= ai: searched once per warp for its first voxel, then walked forward per lane
+    // (a warp's 32 consecutive voxels span a few bricks)
+    const uint32_t a0 = __shfl_sync(__activemask(), ai, __ffs(__activemask()) - 1);
+    uint32_t lo = 0, hi = nb;
+    while (hi - lo > 1u) {
+      uint32_t m = (lo + hi) >> 1;
+      if (v.vpre[m] <= a0) lo = m; else hi = m;
+    }
+    while (lo + 1u < nb && v.vpre[lo + 1u] <= ai) lo++;
+#else
     uint32_t lo = 0, hi = nb;   // the last brick b with vpre[b] <= ai
     while (hi - lo > 1u) {
       uint32_t m = (lo + hi) >> 1;
       if (v.vpre[m] <= ai) lo = m; else hi = m;
     }
+#endif
     uint32_t ptr = lo;
     if (v.base[ptr] == GI_EMPTY) continue;   // past the voxel pool: no attributes (voxel.ts:586)
     uint32_t r = ai - v.vpre[ptr];

@@ -738,7 +738,7 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
   const unsigned act = __activemask();
   const unsigned grp = __match_any_sync(act, black ? (px & 7u) : 8u);
   if (black && (uint32_t)(__ffs(grp) - 1) == (threadIdx.x & 31u)) atomicAdd(&r.counts[72 + (px & 7u)], (uint32_t)__popc(grp));
-  if (A == GI_ATLAS_F32 || r.f32_out) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
+  if ((A == GI_ATLAS_F32 || r.f32_out) && !r.irr_f16) reinterpret_cast<float4 *>(r.irr)[q] = make_float4(res.x, res.y, res.z, alpha);
   else reinterpret_cast<uint2 *>(r.irr)[q] = make_uint2((uint32_t)f2h(res.x) | ((uint32_t)f2h(res.y) << 16),
                                                        (uint32_t)f2h(res.z) | ((uint32_t)f2h(alpha) << 16));
 }

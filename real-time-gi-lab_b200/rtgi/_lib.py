@@ -111,7 +111,7 @@ class GiRcParams(C.Structure):
     _fields_ = [("cascades", C.c_uint32), ("P", C.c_uint32), ("k_interval", C.c_float), ("vox_scale", C.c_float),
                 ("vox_offset", C.c_float), ("vox_skip", C.c_float), ("level_map", C.c_float), ("res_cap", C.c_uint32),
                 ("dda_cap", C.c_uint32), ("stats", C.c_uint32), ("atlas", C.c_uint32), ("f32_out", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("irr_f16", C.c_uint32), ("reserved", C.c_uint32 * 3)]
 
 
 class GiRcTuning(C.Structure):

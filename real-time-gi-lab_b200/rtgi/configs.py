@@ -2,9 +2,10 @@
 VoxParams / DEFAULT_VOX / voxParams, src/runner/configs.ts:47-73 parseConfig).
 
 Same names, defaults and error behaviour: unknown config tokens and unknown voxel parameters raise.  This build adds
-four RcParams fields and their tokens: ``ddaCap`` (token ``dda<N>``; the reference hard-codes 1024 steps,
+five RcParams fields and their tokens: ``ddaCap`` (token ``dda<N>``; the reference hard-codes 1024 steps,
 voxel.ts:142), ``atlas`` (tokens ``f32``/``f16``/``bf16``; the reference stores f16), ``f32Out`` (token ``f32out``:
-SH and irradiance kept in f32 whatever the atlas) and ``stats``.
+SH and irradiance kept in f32 whatever the atlas), ``irr16`` (token ``irr16``: the irradiance stored as rgba16float,
+the reference's rc.irr format, whatever the atlas; the passes before the store keep their precision) and ``stats``.
 """
 from __future__ import annotations
 
@@ -49,6 +50,7 @@ class RcParams:
     ddaCap: int = 1024
     atlas: str = "f16"
     f32Out: bool = False
+    irr16: bool = False
 
 
 DEFAULT_PARAMS = RcParams()
@@ -83,6 +85,7 @@ def parse_config(name: str, overrides: Optional[dict] = None) -> RcParams:
         elif re.fullmatch(r"dda\d+", t): p.ddaCap = int(t[3:])
         elif t in ("f32", "f16", "bf16"): p.atlas = t
         elif t == "f32out": p.f32Out = True
+        elif t == "irr16": p.irr16 = True
         else: raise ValueError(f"unknown config token {t} in {name}")
     return p
 
@@ -127,7 +130,7 @@ def cascade_layout(p: RcParams, width: int, height: int) -> dict:
     atlas = {"f32": 0, "f16": 1, "bf16": 2}[p.atlas]
     return {"cascades": p.cascades, "casc": casc, "vox_scale": p.voxScale, "vox_offset": p.voxOffset,
             "level_map": p.levelMap, "vox_skip": p.voxSkip, "dda_cap": p.ddaCap, "stats": p.stats, "atlas": atlas,
-            "f32_out": 1 if p.f32Out else 0,
+            "f32_out": 1 if p.f32Out else 0, "irr_f16": 1 if p.irr16 else 0,
             "probes_total": probe_off, "rays_total": rad_off}
 
 
@@ -154,5 +157,6 @@ def world_layout(p: RcParams) -> dict:
     relocate = {"gbuffer": 0, "none": 1, "voxel": 2}[p.relocate]
     return {"cascades": p.cascades, "casc": casc, "vox_scale": p.voxScale, "vox_offset": p.voxOffset,
             "level_map": p.levelMap, "vox_skip": p.voxSkip, "dda_cap": p.ddaCap, "stats": p.stats, "atlas": atlas,
-            "f32_out": 1 if p.f32Out else 0, "probes_total": probe_off, "rays_total": rad_off,
+            "f32_out": 1 if p.f32Out else 0, "irr_f16": 1 if p.irr16 else 0, "probes_total": probe_off,
+            "rays_total": rad_off,
             "hash_total": hash_off, "relocate": relocate, "world": True}

@@ -228,6 +228,7 @@ class Rc:
         p.vox_scale, p.vox_offset, p.vox_skip, p.level_map = params.voxScale, params.voxOffset, params.voxSkip, params.levelMap
         p.res_cap, p.dda_cap, p.stats, p.atlas = params.resCap, params.ddaCap, params.stats, ATLAS_CODES[params.atlas]
         p.f32_out = 1 if params.f32Out else 0
+        p.irr_f16 = 1 if params.irr16 else 0
         h = _P()
         if self.world:
             wp = _lib.GiWorldParams()
@@ -336,7 +337,8 @@ class Rc:
         _lib.call("gi_rc_read_irradiance_async", self.handle, ptr, self.irr_bytes(), _stream(stream))
 
     def irr_bytes(self) -> int:
-        return self.width * self.height * (16 if self.params.atlas == "f32" or self.params.f32Out else 8)
+        wide = (self.params.atlas == "f32" or self.params.f32Out) and not self.params.irr16
+        return self.width * self.height * (16 if wide else 8)
 
     def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None):
         """G-buffer from host pointers (pinned memory makes the copies asynchronous)."""

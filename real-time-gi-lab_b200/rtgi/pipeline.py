@@ -16,10 +16,11 @@ from . import gpu
 
 class FramePipeline:
     def __init__(self, ctx: gpu.Context, vox: gpu.VoxWorld, params, width: int, height: int, frame, depth_ptr: int,
-                 normal_f16_ptr: int, slots: int = 2, shadow=None):
+                 normal_f16_ptr: int, slots: int = 2, shadow=None, tuning=None):
         """frame/depth/normal: a first frame's inputs (frame as an array, the G-buffer as pinned host pointers), used
         to capture each slot's graph.  shadow: (SceneGpu, size) to give every slot the sun's shadow map drawn from
-        that frame (a static sun and scene; draw it again with Rc.render_shadow when they move)."""
+        that frame (a static sun and scene; draw it again with Rc.render_shadow when they move).  tuning: launch
+        shapes for every slot (Rc.set_tuning's keywords; results do not depend on them)."""
         import torch
         self.torch = torch
         self.vox = vox
@@ -29,6 +30,8 @@ class FramePipeline:
             rc = gpu.Rc(ctx, params, width, height)
             rc.set_frame(frame, self.comp)
             rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.comp)
+            if tuning:
+                rc.set_tuning(**tuning)
             if shadow is not None:
                 rc.render_shadow(shadow[0], shadow[1], self.comp)
             rc.graph_capture(vox, self.comp)

@@ -195,6 +195,29 @@ def test_f32out_token_and_layout():
     assert configs.cascade_layout(configs.parse_config("screen-8-voxel-f16"), 64, 32)["f32_out"] == 0
 
 
+def test_irr16_token_and_the_oracle_store():
+    """irr16: the irradiance rounded to rgba16float at the store (round to nearest even), nothing before it changed."""
+    p = configs.parse_config("screen-8-voxel-f32-irr16", {"cascades": 3})
+    assert p.atlas == "f32" and p.irr16 and not p.f32Out
+    assert configs.cascade_layout(p, 64, 32)["irr_f16"] == 1
+    assert configs.cascade_layout(configs.parse_config("screen-8-voxel-f32"), 64, 32)["irr_f16"] == 0
+    s = scenes.room_scene(0)
+    W, H = 96, 64
+    v = configs.vox_params({"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 8192, "maxVoxels": 1 << 20})
+    st = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, s.camera.eye)
+    outs = []
+    for name in ("screen-8-voxel-f32", "screen-8-voxel-f32-irr16"):
+        q = configs.parse_config(name, {"cascades": 3})
+        F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=fr.SUN_E,
+                                         sky=fr.SKY, cascades=q.cascades, P=q.P))
+        depth, normal, _ = bind.raster_gbuffer(s, F, W, H)
+        outs.append(bind.rc_solve(st, configs.cascade_layout(q, W, H), F, depth, normal.astype(np.float16).astype(np.float32)))
+    wide, narrow = outs
+    assert np.array_equal(wide["rad"].view(np.uint32), narrow["rad"].view(np.uint32))
+    assert (wide["irr"] > 0).any()
+    assert np.array_equal(wide["irr"].astype(np.float16).astype(np.float32).view(np.uint32), narrow["irr"].view(np.uint32))
+
+
 def test_quotient_shortcuts_of_the_shading_are_exact():
     """The hit shading replaces two f32 divisions by f64 products rounded to f32: k / 32767 for every 16-bit k (the
     snorm normal) and a / pi for the 256 albedo bytes a = k / 255.  Both equal the IEEE f32 quotients everywhere."""

@@ -86,6 +86,7 @@ CASES = {"config0": gi_cases.config0, "room_lit": gi_cases.room_lit, "leak": gi_
          "leak_sun": gi_cases.leak_sun, "empty": gi_cases.empty, "single_triangle": gi_cases.single_triangle,
          "tiny": gi_cases.tiny,
          "room_lit_f32out": lambda: gi_cases.room_lit("f16-f32out"),
+         "room_lit_irr16": lambda: gi_cases.room_lit("f32-irr16"),
          "overflow": gi_cases.overflow, "config1": gi_cases.config1,
          "batch_g4_l1": gi_cases.batch_g4_l1, "batch_g4_l4": gi_cases.batch_g4_l4,
          "batch_g32_l1": gi_cases.batch_g32_l1, "batch_g32_l4": gi_cases.batch_g32_l4,
@@ -185,3 +186,29 @@ def test_bounce_parity(ctx):
     finally:
         for h in (rc, vw, sg):
             h.destroy()
+
+
+def test_irr16_is_the_rounded_f32_solve(ctx):
+    """irr16 stores the irradiance as rgba16float (the reference's rc.irr format): the same solve as the f32 one up
+    to the store, which rounds to nearest even; the readback is half the bytes."""
+    wide, narrow = gi_cases.room_lit("f32"), gi_cases.room_lit("f32-irr16")
+    out = []
+    for case in (wide, narrow):
+        sg = gpu.SceneGpu(ctx, case.scene)
+        vw = gpu.VoxWorld(sg, case.vox)
+        rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+        rc.set_frame(case.frame)
+        rc.render_gbuffer(sg)
+        vw.update(case.scene.camera.eye)
+        rc.solve(vw)
+        raw = np.zeros(rc.irr_bytes(), np.uint8)
+        rc.read_irradiance_raw(raw)
+        out.append((raw, rc.read_atlas(_lib.GI_RC_RAD), rc.read_atlas(_lib.GI_RC_SH)))
+        for h in (rc, vw, sg):
+            h.destroy()
+    (w_raw, w_rad, w_sh), (n_raw, n_rad, n_sh) = out
+    assert n_raw.size * 2 == w_raw.size == wide.width * wide.height * 16
+    assert np.array_equal(w_rad.view(np.uint32), n_rad.view(np.uint32)) and np.array_equal(w_sh.view(np.uint32), n_sh.view(np.uint32))
+    w = w_raw.view(np.float32)
+    assert (w > 0.0).any()
+    assert np.array_equal(w.astype(np.float16).view(np.uint16), n_raw.view(np.uint16))

@@ -63,6 +63,8 @@ def cases():
     return [
         _case("room-vrel-f32", room, 256, 192, "world-48-voxel-rc2-vrel-f32", ROOM_VOX, [8192, 4096, 2048, 1024, 512]),
         _case("room-gbuffer-f16", room, 256, 192, "world-24-voxel-rc2-f16", ROOM_VOX, [8192, 4096, 2048, 1024, 512]),
+        _case("room-gbuffer-f32-irr16", room, 160, 120, "world-24-voxel-rc2-f32-irr16", ROOM_VOX,
+              [8192, 4096, 2048, 1024, 512]),
         _case("room-none-overflow", room, 200, 150, "world-16-voxel-norel-f32", ROOM_VOX, [1100, 400, 160, 70, 40]),
         _case("colonnade-vrel-sun", scenes.colonnade_scene(0), 480, 270, "world-48-voxel-rc2-vrel-f32",
               {"v0": 0.1, "levels": 4, "G": 16, "maxBricks": 16384, "maxVoxels": 1 << 22}, [16384, 8192, 4096, 2048, 1024],
