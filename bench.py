@@ -611,13 +611,15 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
 
 
 def run_e2e(ctx, vw, p, W, H, F, host, shadow, tuned, n, dist, world, slots=2):
+    """host: (frame, depth, normal) pinned tensors; a normal tensor of 3 halves per pixel is uploaded as rgb16f."""
     """Solves/s through rtgi.pipeline with host buffers: every step uploads its frame and G-buffer from pinned memory
     and downloads its irradiance into pinned memory, the copies of neighbouring frames overlapping the solve."""
     import torch
     from rtgi import pipeline
     frame_h, depth_h, normal_h = host
+    rgb = normal_h.numel() == 3 * W * H
     pipe = pipeline.FramePipeline(ctx, vw, p, W, H, F, depth_h.data_ptr(), normal_h.data_ptr(), slots=slots,
-                                  shadow=shadow, tuning=tuned["rc"])
+                                  shadow=shadow, tuning=tuned["rc"], normal_rgb=rgb)
     irr_h = [torch.empty(pipe.irr_bytes, dtype=torch.uint8).pin_memory() for _ in range(slots)]
     for k in range(2 * slots):
         pipe.submit(frame_h.data_ptr(), depth_h.data_ptr(), normal_h.data_ptr(), irr_h[k % slots].data_ptr())
@@ -639,6 +641,7 @@ def run_e2e(ctx, vw, p, W, H, F, host, shadow, tuned, n, dist, world, slots=2):
             "h2d_bytes_per_step": int(depth_h.numel() * 4 + normal_h.numel() * 2 + frame_h.numel() * 4),
             "d2h_bytes_per_step": int(irr_h[0].numel()), "steps": n,
             "irradiance": "rgba16float" if p.irr16 else "rgba32float",
+            "normal_upload": "rgb16f (3 halves per pixel)" if rgb else "rgba16f",
             "mode": f"rtgi.pipeline: copies of neighbouring frames overlap the solve ({slots} cascade sets); wall "
                     "clock around the steps, max over ranks"}
 
@@ -733,14 +736,18 @@ def run_ours(args, rank, world, local_rank):
     depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
     normal_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_NORMAL).view(np.uint16).copy()).pin_memory()
     frame_h = torch.from_numpy(F.copy()).pin_memory()
-    host = (frame_h, depth_h, normal_h)
+    # the host's normals as three halves per pixel (the path reads no alpha): 6 bytes a pixel over the bus
+    normal_rgb_h = torch.from_numpy(np.ascontiguousarray(normal_h.numpy().reshape(-1, 4)[:, :3]).reshape(-1)).pin_memory()
     shadow_in = (sg, desc["shadow_map"]) if desc["shadow_map"] else None
-    e2e_out = run_e2e(ctx, vw, p, W, H, F, host, shadow_in, tuned, max(3, min(n_ev, 400)), dist, world)
-    # the same with the irradiance stored and read back as f32 (twice the download)
-    e2e_f32 = None
+    n_e2e = max(3, min(n_ev, 400))
+    e2e_out = run_e2e(ctx, vw, p, W, H, F, (frame_h, depth_h, normal_rgb_h), shadow_in, tuned, n_e2e, dist, world)
+    # the same with four halves per normal, and with the irradiance stored and read back as f32 as well
+    e2e_more = {"rgba16f_normals": run_e2e(ctx, vw, p, W, H, F, (frame_h, depth_h, normal_h), shadow_in, tuned, n_e2e,
+                                           dist, world)}
     if p.irr16:
-        e2e_f32 = run_e2e(ctx, vw, dataclasses.replace(p, irr16=False), W, H, F, host, shadow_in, tuned,
-                          max(3, min(n_ev, 400)), dist, world)
+        e2e_more["rgba16f_normals_f32_irradiance"] = run_e2e(ctx, vw, dataclasses.replace(p, irr16=False), W, H, F,
+                                                              (frame_h, depth_h, normal_h), shadow_in, tuned, n_e2e,
+                                                              dist, world)
 
     # two frames in flight: a second voxel world and cascade set solve the same workload on a second stream, the two
     # captured solves launched side by side (what a renderer does with consecutive frames); device time of the job
@@ -856,7 +863,7 @@ def run_ours(args, rank, world, local_rank):
                             "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_kind,
                             "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": trace_ms},
                "e2e": e2e_out,
-               "e2e_irr_f32": e2e_f32,
+               "e2e_variants": e2e_more,
                "gpu_launches": n_ev * (11 + (1 if v.levels > 1 else 0) + 3 + p.cascades),
                "clocks": clk, "wall_s": wall}
     if args.batch > 0:

@@ -216,6 +216,9 @@ int gi_rc_set_frame(gi_rc *rc, const void *frame640, void *stream);
  * rgba f32 (normal4) or in the reference's rgba16float texture format (normal_rgba16f, 4 halves per pixel). */
 int gi_rc_set_gbuffer(gi_rc *rc, const float *depth, const float *normal4, void *stream);
 int gi_rc_set_gbuffer_f16(gi_rc *rc, const float *depth, const uint16_t *normal_rgba16f, void *stream);
+/* The same with the normal as three halves per pixel (the rgba16float texture's r, g, b; the path reads no alpha):
+ * 6 bytes a pixel over the bus instead of 8, expanded on the device (stream-ordered, alpha 0 as the raster writes). */
+int gi_rc_set_gbuffer_rgb16f(gi_rc *rc, const float *depth, const uint16_t *normal_rgb16f, void *stream);
 /* G-buffer drawn on the device from the scene and the frame (one primary-ray sample per pixel centre). */
 int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
 /* The sun shadow map (encodeShadow, lighting.ts:175-189; depth32float, compare less, depth bias 2 + slope 2, cull

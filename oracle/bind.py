@@ -61,6 +61,8 @@ def lib():
         _lib.orc_shadow_render.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.orc_sun_tap.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.orc_sun_tap.restype = C.c_float
+        _lib.orc_shadow_layers.argtypes = [C.c_void_p]
+        _lib.orc_shadow_layers.restype = C.c_uint32
         _lib.orc_vox_sun.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
         _lib.orc_bounce_frame.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_gi_exp.argtypes = [C.c_float]
@@ -301,11 +303,13 @@ def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int, ndraw: int = 0, dra
 
 
 def shadow_render(scene, frame: np.ndarray, S: int, ndraw: int = 0, draw_instances=None) -> np.ndarray:
-    """The sun shadow map (S x S depths, 1 = nothing drawn) from the frame's lightViewProj."""
+    """The sun shadow map (S x S depths, 1 = nothing drawn) from the frame's lightViewProj; (2, S, S) for a frame with
+    the two camera-following layers (shadow.x = 2), layer 1 from lightViewProjFar."""
     s, keep = _scene_struct(scene)
     keep = _drawn(s, keep, ndraw, draw_instances)
     frame = np.ascontiguousarray(frame, dtype=np.float32)
-    out = np.zeros((S, S), np.float32)
+    layers = int(lib().orc_shadow_layers(_p(frame)))
+    out = np.zeros((layers, S, S) if layers > 1 else (S, S), np.float32)
     lib().orc_shadow_render(C.byref(s), _p(frame), S, _p(out))
     return out
 
@@ -314,7 +318,7 @@ def sun_tap(frame: np.ndarray, shadow: np.ndarray, x) -> float:
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     shadow = np.ascontiguousarray(shadow, dtype=np.float32)
     p = np.ascontiguousarray(x, dtype=np.float32)
-    return float(lib().orc_sun_tap(_p(frame), _p(shadow), shadow.shape[0], _p(p)))
+    return float(lib().orc_sun_tap(_p(frame), _p(shadow), shadow.shape[-1], _p(p)))
 
 
 def vox_sun(vox: dict, frame: np.ndarray, shadow: np.ndarray) -> None:
@@ -322,7 +326,7 @@ def vox_sun(vox: dict, frame: np.ndarray, shadow: np.ndarray) -> None:
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     shadow = np.ascontiguousarray(shadow, dtype=np.float32)
     vx = _vox_struct(vox)
-    lib().orc_vox_sun(C.byref(vx), _p(frame), _p(shadow), shadow.shape[0])
+    lib().orc_vox_sun(C.byref(vx), _p(frame), _p(shadow), shadow.shape[-1])
 
 
 def bounce_dirs(rays: int) -> np.ndarray:
@@ -452,7 +456,7 @@ class Dyn:
         vx = _vox_struct({**vox, "dyn": None})
         sm = None if shadow is None else np.ascontiguousarray(shadow, dtype=np.float32)
         lib().orc_dyn_build(C.byref(s), C.byref(vx), C.byref(self.struct), first, end, _p(frame),
-                            _p(sm) if sm is not None else None, 0 if sm is None else sm.shape[0])
+                            _p(sm) if sm is not None else None, 0 if sm is None else sm.shape[-1])
 
     def trace(self, vox: dict, o, d, t0: float, t1: float, k: float) -> np.ndarray:
         """traceDyn of one segment: covered radiance rgb and coverage."""

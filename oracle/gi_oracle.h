@@ -178,12 +178,15 @@ int orc_raster_gbuffer(const orc_scene *s, const float *frame, uint32_t width, u
                        float *normal_out, uint32_t *tri_out);
 
 /* Sun shadow map (lighting.ts:133-140, 175-189, restated as a per-texel-centre raster of the light's orthographic
- * clip space; the rules are stated in shadow.c): S*S depths, 1 where nothing is drawn, from the frame's
- * lightViewProj (frame words 64-79). */
+ * clip space; the rules are stated in shadow.c): per layer S*S depths, 1 where nothing is drawn; layer 0 from the
+ * frame's lightViewProj (frame words 64-79), layer 1 (frames with shadow.x = 2, word 156) from lightViewProjFar
+ * (words 140-155) at map + S*S. */
 int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float *map);
-/* shadowTap (frame.ts:47-52): the 'less-equal' comparison of x's biased light depth (frame word 157) with the map,
- * bilinear over the four texels around it; 1 outside the map. */
+/* shadowTap (frame.ts:35-52): the 'less-equal' comparison of x's biased light depth (bias: frame word 157, layer 1:
+ * 158) with the layer x projects into, bilinear over the four texels around it; 1 outside every layer. */
 float orc_sun_tap(const float *frame, const float *map, uint32_t S, const float x[3]);
+/* The frame's layer count: 2 when shadow.x (word 156) >= 1.5, else 1. */
+uint32_t orc_shadow_layers(const float *frame);
 /* voxSun (voxel.ts:633-671): the sun visibility of every occupied voxel of a built world (after orc_vox_build). */
 int orc_vox_sun(orc_vox *vx, const float *frame, const float *map, uint32_t S);
 

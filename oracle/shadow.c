@@ -9,8 +9,11 @@
  *     r = 2^(e - 23) of the largest |z| and the larger window-space slope) are this build's definition, shared with
  *     the CUDA kernels.  The stored depth is the smallest biased depth, so the result does not depend on the order in
  *     which triangles are drawn.
- *   - shadowCoord / shadowTap (src/core/frame.ts:35-52) for one layer: textureSampleCompareLevel with a 'less-equal'
- *     comparison sampler, linear filtering and clamp-to-edge, its four comparisons weighted bilinearly in f32.
+ *   - shadowCoord / shadowTap (src/core/frame.ts:35-52): layer 0 (lightViewProj, bias shadow.y) where x projects inside
+ *     it, else layer 1 (lightViewProjFar, bias shadow.z) when the frame has two layers (shadow.x >= 1.5; the
+ *     camera-following layers of instanced worlds, lighting.ts:93-125), else lit; textureSampleCompareLevel with a
+ *     'less-equal' comparison sampler, linear filtering and clamp-to-edge within the layer, its four comparisons
+ *     weighted bilinearly in f32.
  *   - voxSun (src/core/voxel.ts:633-671): the mean of four taps on the representative's plane.
  */
 #include <math.h>
@@ -21,7 +24,7 @@
 #include "gi_oracle.h"
 #include "orc_math.h"
 
-enum { F_LVP = 64, F_SUN_DIR = 88, F_SHADOW = 156 };
+enum { F_LVP = 64, F_SUN_DIR = 88, F_LVPF = 140, F_SHADOW = 156 };
 
 static v3 light_clip(const float *m, v3 p) {
   return V(m[0] * p.x + m[4] * p.y + m[8] * p.z + m[12] * 1.0f, m[1] * p.x + m[5] * p.y + m[9] * p.z + m[13] * 1.0f,
@@ -36,8 +39,19 @@ static float bias_unit(float zmax) {
   return ldexpf(1.0f, eb - 127 - 23);
 }
 
+/* Number of shadow-map layers the frame asks for (shadow.x: 1, or 2 for the camera-following layers of a world). */
+uint32_t orc_shadow_layers(const float *frame) { return frame[F_SHADOW] >= 1.5f ? 2u : 1u; }
+
+static void render_layer(const orc_scene *s, const float *m, uint32_t S, float *map);
+
+/* Every layer the frame asks for: layer l at map + l S^2, drawn with lightViewProj (l = 0) or lightViewProjFar. */
 int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float *map) {
-  const float *m = frame + F_LVP;
+  for (uint32_t l = 0; l < orc_shadow_layers(frame); l++)
+    render_layer(s, frame + (l ? F_LVPF : F_LVP), S, map + (size_t)l * S * S);
+  return 0;
+}
+
+static void render_layer(const orc_scene *s, const float *m, uint32_t S, float *map) {
   for (size_t i = 0; i < (size_t)S * S; i++) map[i] = 1.0f;
   const float inv = 1.0f / (float)S, fS = (float)S;
   const uint32_t nd = s->ndraw ? s->ndraw : s->ntris, ni = s->draw_inst ? s->draw_ninst : 1u;
@@ -87,14 +101,24 @@ int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float 
       }
     }
   }
-  return 0;
 }
+
+static float compare4(const float *map, uint32_t S, float u, float v, float ref);
 
 float orc_sun_tap(const float *frame, const float *map, uint32_t S, const float x3[3]) {
   v3 c = light_clip(frame + F_LVP, fromf(x3));
   float u = c.x * 0.5f + 0.5f, v = c.y * -0.5f + 0.5f;
-  if (!(u >= 0.0f && v >= 0.0f && u <= 1.0f && v <= 1.0f)) return 1.0f;   /* outside the layer: lit */
-  float ref = c.z - frame[F_SHADOW + 1];
+  if (u >= 0.0f && v >= 0.0f && u <= 1.0f && v <= 1.0f) return compare4(map, S, u, v, c.z - frame[F_SHADOW + 1]);
+  if (frame[F_SHADOW] < 1.5f) return 1.0f;   /* one layer, x outside it: lit */
+  v3 c1 = light_clip(frame + F_LVPF, fromf(x3));
+  float u1 = c1.x * 0.5f + 0.5f, v1 = c1.y * -0.5f + 0.5f;
+  if (u1 >= 0.0f && v1 >= 0.0f && u1 <= 1.0f && v1 <= 1.0f)
+    return compare4(map + (size_t)S * S, S, u1, v1, c1.z - frame[F_SHADOW + 2]);
+  return 1.0f;                                /* outside both layers: lit */
+}
+
+/* textureSampleCompareLevel of one layer: 'less-equal', linear, clamp-to-edge */
+static float compare4(const float *map, uint32_t S, float u, float v, float ref) {
   float tx = u * (float)S - 0.5f, ty = v * (float)S - 0.5f;
   float fx = floorf(tx), fy = floorf(ty);
   float ax = tx - fx, ay = ty - fy;

@@ -162,8 +162,11 @@ struct gi_rc {
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
   uint64_t graph_items_gen = 0;      // the voxel world's work items the graph was captured with
-  float *shadow = nullptr;           // gi_rc_render_shadow: shadow_size^2 depths
-  uint32_t shadow_size = 0;
+  float *shadow = nullptr;           // gi_rc_render_shadow: shadow_layers x shadow_size^2 depths
+  uint32_t shadow_size = 0, shadow_layers = 0;
+  uint32_t frame_layers = 1;         // the last frame's shadow.x (1, or 2 for a world's camera-following layers)
+  uint64_t gen = 0;                  // bumped when a buffer a captured graph reads is freed or moved (shadow map,
+  uint64_t graph_gen = 0;            // bounce volume, dynamic layer); graph_gen: gen at the rc graph's capture
   float4 *sm_rec = nullptr;          // its raster scratch, for up to sm_tris triangles
   uint32_t *sm_pre = nullptr, *sm_sums = nullptr, *sm_counter = nullptr;
   uint32_t sm_tris = 0;
@@ -460,17 +463,22 @@ int gi_vox_update(gi_vox *v, const double eye[3]) {
 }
 
 // The rebuild, with voxSun from a shadow map when one is given (gi_solve passes the rc's)
-static int vox_build_sun(gi_vox *v, const float *frame, const float *shadow, uint32_t size, void *stream) {
+static int vox_build_sun(gi_vox *v, const float *frame, const float *shadow, uint32_t size, void *stream,
+                         uint32_t layers = 1u) {
   if (!v) return fail(GI_ERR_INVALID, "gi_vox_build: NULL vox");
   if (!v->updated) return fail(GI_ERR_STATE, "gi_vox_build: gi_vox_update was not called");
   CK(cudaSetDevice(v->scene->ctx->device), "gi_vox_build: cudaSetDevice");
   VoxDev d = v->dev;
-  d.sun_frame = frame; d.shadow = shadow; d.shadow_size = shadow ? size : 0u;
+  d.sun_frame = frame; d.shadow = shadow; d.shadow_size = shadow ? size : 0u; d.shadow_layers = shadow ? layers : 0u;
   CK(gi_launch_vox_build(d, v->build_scene(), v->scene->ctx->sm_count, S(stream)), "gi_vox_build: launch");
   return GI_OK;
 }
 
 int gi_vox_build(gi_vox *v, void *stream) { return vox_build_sun(v, nullptr, nullptr, 0u, stream); }
+
+// The rebuild with the rc's shadow map (voxSun) when it holds one; refused when the frame asks for more layers than
+// the map was drawn with
+static int rc_vox_build(gi_vox *v, gi_rc *r, void *stream);
 
 int gi_vox_set_world(gi_vox *v, const float *instances, uint32_t ninst, const uint32_t *lists, uint32_t nlists,
                      uint32_t key_stride) {
@@ -607,10 +615,18 @@ int gi_scene_set_draw_instances(gi_scene *s, const float *offsets, uint32_t n) {
   return GI_OK;
 }
 
+static int rc_vox_build(gi_vox *v, gi_rc *r, void *stream) {
+  if (!r->shadow) return vox_build_sun(v, nullptr, nullptr, 0u, stream);
+  if (r->frame_layers > r->shadow_layers)
+    return fail(GI_ERR_STATE, "the frame asks for %u shadow-map layers, the map was drawn with %u; draw it again "
+                              "(gi_rc_render_shadow)", r->frame_layers, r->shadow_layers);
+  return vox_build_sun(v, r->frame, r->shadow, r->shadow_size, stream, r->shadow_layers);
+}
+
 int gi_vox_build_sun(gi_vox *v, gi_rc *r, void *stream) {
   if (!r) return fail(GI_ERR_INVALID, "gi_vox_build_sun: NULL rc");
   if (v && v->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_vox_build_sun: rc on another device");
-  return vox_build_sun(v, r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, stream);
+  return rc_vox_build(v, r, stream);
 }
 
 int gi_vox_read_counters(gi_vox *v, uint32_t hdr[64], void *stream) {
@@ -875,6 +891,7 @@ int gi_rc_set_frame(gi_rc *r, const void *frame640, void *stream) {
   CK(cudaSetDevice(r->ctx->device), "gi_rc_set_frame: cudaSetDevice");
   CK(cudaMemcpyAsync(r->frame, frame640, 640, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_frame: copy");
   r->frame_set = true;
+  r->frame_layers = f[156] >= 1.5f ? 2u : 1u;   // shadow.x: the shadow map's layers (frame.ts:20)
   return GI_OK;
 }
 
@@ -895,6 +912,18 @@ int gi_rc_set_gbuffer_f16(gi_rc *r, const float *depth, const uint16_t *normal, 
   size_t npx = (size_t)r->W * r->H;
   CK(cudaMemcpyAsync(r->depth, depth, npx * 4u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_f16: depth");
   CK(cudaMemcpyAsync(r->normal, normal, npx * 8u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_f16: normal");
+  r->gbuf_set = true;
+  return GI_OK;
+}
+
+int gi_rc_set_gbuffer_rgb16f(gi_rc *r, const float *depth, const uint16_t *normal, void *stream) {
+  if (!r || !depth || !normal) return fail(GI_ERR_INVALID, "gi_rc_set_gbuffer_rgb16f: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_gbuffer_rgb16f: cudaSetDevice");
+  size_t npx = (size_t)r->W * r->H;
+  CK(cudaMemcpyAsync(r->depth, depth, npx * 4u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_rgb16f: depth");
+  CK(cudaMemcpyAsync(r->stage, normal, npx * 6u, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_rgb16f: normal");
+  CK(gi_launch_normal_rgb_to_rgba(reinterpret_cast<const uint16_t *>(r->stage), r->normal, (uint32_t)npx, S(stream)),
+     "gi_rc_set_gbuffer_rgb16f: expand");
   r->gbuf_set = true;
   return GI_OK;
 }
@@ -922,17 +951,21 @@ int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
   if (size == 0) {
     cudaFree(r->shadow);
     r->shadow = nullptr;
-    r->shadow_size = 0;
+    r->shadow_size = r->shadow_layers = 0;
+    r->gen++;
     return GI_OK;
   }
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_render_shadow: no frame set");
   cudaError_t e;
-  if (size != r->shadow_size) {
+  const uint32_t layers = r->frame_layers;
+  if (size != r->shadow_size || layers != r->shadow_layers) {
     cudaFree(r->shadow);
     r->shadow = nullptr;
-    r->shadow_size = 0;
-    if ((e = dalloc(&r->shadow, (size_t)size * size))) return cuda_fail(e, "gi_rc_render_shadow");
+    r->shadow_size = r->shadow_layers = 0;
+    r->gen++;
+    if ((e = dalloc(&r->shadow, (size_t)size * size * layers))) return cuda_fail(e, "gi_rc_render_shadow");
     r->shadow_size = size;
+    r->shadow_layers = layers;
   }
   uint32_t nt = s->ndraw * s->draw_ninst;   // the drawn triangles (ensure_raster_scratch bounds the product)
   if (nt > r->sm_tris || !r->sm_counter) {
@@ -946,7 +979,11 @@ int gi_rc_render_shadow(gi_rc *r, gi_scene *s, uint32_t size, void *stream) {
   }
   ShadowRaster sr;
   sr.map = r->shadow; sr.rec = r->sm_rec; sr.pre = r->sm_pre; sr.sums = r->sm_sums; sr.counter = r->sm_counter;
-  CK(gi_launch_shadow(s->raster_dev(), r->frame, size, sr, r->ctx->sm_count, S(stream)), "gi_rc_render_shadow: launch");
+  for (uint32_t l = 0; l < layers; l++) {   // layer 0: lightViewProj (frame word 64), layer 1: lightViewProjFar (140)
+    sr.map = r->shadow + (size_t)l * size * size;
+    CK(gi_launch_shadow(s->raster_dev(), r->frame + (l ? 140 : 64), size, sr, r->ctx->sm_count, S(stream)),
+       "gi_rc_render_shadow: launch");
+  }
   return GI_OK;
 }
 
@@ -975,6 +1012,7 @@ int gi_rc_set_bounce(gi_rc *r, gi_vox *v, const gi_bounce_params *p) {
   cudaFree(r->bn.ray_out);
   r->bn = BounceDev{};
   r->bounce = false;
+  r->gen++;
   r->bn_vox = nullptr;
   r->dev.bn_inj = nullptr;
   if (!p) return GI_OK;
@@ -1037,11 +1075,12 @@ int gi_solve(gi_rc *r, gi_vox *v, void *stream) {
     CK(cudaSetDevice(r->ctx->device), "gi_solve: cudaSetDevice");
     CK(cudaEventRecord(r->ev[0], S(stream)), "gi_solve: event");
   }
-  int st = vox_build_sun(v, r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, stream);
+  int st = rc_vox_build(v, r, stream);
   if (st != GI_OK) return st;
   if (r->dyn) {   // the dynamic layer after the static rebuild (rcrun.ts encodeFrame: one 'vox' pass holds both)
     if (r->dyn->vox != v) return fail(GI_ERR_INVALID, "gi_solve: the rc's dynamic layer belongs to another voxel world");
-    CK(gi_launch_dyn_build(r->dyn->dev, v->dev, v->scene->dev(), r->frame, r->shadow, r->shadow ? r->shadow_size : 0u,
+    CK(gi_launch_dyn_build(r->dyn->dev, v->dev, v->scene->dev(), r->frame, r->shadow,
+                           r->shadow ? r->shadow_size : 0u, r->shadow_layers,
                            r->ctx->sm_count, S(stream)), "gi_solve: dynamic layer");
   }
   st = gi_rc_solve(r, v, stream);
@@ -1065,6 +1104,7 @@ int gi_rc_graph_capture(gi_rc *r, gi_vox *v, void *stream) {
   if (st != GI_OK) { if (g) cudaGraphDestroy(g); return st; }
   if (e != cudaSuccess) return cuda_fail(e, "gi_rc_graph_capture: end");
   e = cudaGraphInstantiate(&r->graph, g, 0);
+  r->graph_gen = r->gen;
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture: instantiate"); }
   r->graph_vox = v;
@@ -1096,6 +1136,7 @@ int gi_rc_graph_capture_frame(gi_rc *r, gi_vox *v, gi_scene *sc, void *irr_out, 
   if (st != GI_OK) { if (g) cudaGraphDestroy(g); return st; }
   if (e != cudaSuccess) return cuda_fail(e, "gi_rc_graph_capture_frame: end");
   e = cudaGraphInstantiate(&r->graph, g, 0);
+  r->graph_gen = r->gen;
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture_frame: instantiate"); }
   r->graph_vox = v;
@@ -1108,6 +1149,12 @@ int gi_rc_graph_launch(gi_rc *r, void *stream) {
   if (!r->graph) return fail(GI_ERR_STATE, "gi_rc_graph_launch: no graph captured");
   if (r->graph_vox && r->graph_vox->items_gen != r->graph_items_gen)
     return fail(GI_ERR_STATE, "gi_rc_graph_launch: the voxel world's work items changed since the capture; capture again");
+  if (r->gen != r->graph_gen)
+    return fail(GI_ERR_STATE, "gi_rc_graph_launch: the shadow map, bounce volume or dynamic layer changed since the "
+                              "capture; capture again");
+  if (r->shadow && r->frame_layers > r->shadow_layers)
+    return fail(GI_ERR_STATE, "gi_rc_graph_launch: the frame asks for %u shadow layers, the map has %u; draw it again",
+                r->frame_layers, r->shadow_layers);
   CK(cudaSetDevice(r->ctx->device), "gi_rc_graph_launch: cudaSetDevice");
   CK(cudaGraphLaunch(r->graph, S(stream)), "gi_rc_graph_launch");
   r->timed = false;
@@ -1128,6 +1175,7 @@ struct gi_batch {
   RcDev *d_rc = nullptr;
   VoxDev *d_vox = nullptr;
   uint32_t *d_pre = nullptr;
+  uint64_t *gens = nullptr;   // each rc's gen at the capture
 };
 
 static void free_batch(gi_batch *b) {
@@ -1138,7 +1186,7 @@ static void free_batch(gi_batch *b) {
   }
   if (b->start) cudaEventDestroy(b->start);
   cudaFree(b->d_rc); cudaFree(b->d_vox); cudaFree(b->d_pre);
-  delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done;
+  delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done; delete[] b->gens;
 }
 
 int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32_t n, gi_batch **out) {
@@ -1161,7 +1209,8 @@ int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32
   b->voxes = new (std::nothrow) gi_vox *[n];
   b->streams = new (std::nothrow) cudaStream_t[n]();
   b->done = new (std::nothrow) cudaEvent_t[n]();
-  if (!b->rcs || !b->voxes || !b->streams || !b->done) { free_batch(b); delete b; return fail(GI_ERR_OOM, "gi_batch_create: host allocation"); }
+  b->gens = new (std::nothrow) uint64_t[n]();
+  if (!b->rcs || !b->voxes || !b->streams || !b->done || !b->gens) { free_batch(b); delete b; return fail(GI_ERR_OOM, "gi_batch_create: host allocation"); }
   b->n = n;
   cudaError_t e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming);
   for (uint32_t i = 0; i < n && e == cudaSuccess; i++) {
@@ -1203,6 +1252,7 @@ int gi_batch_capture(gi_batch *b, void *stream) {
   if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture"); }
   if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture: end");
   e = cudaGraphInstantiate(&b->graph, g, 0);
+  for (uint32_t i = 0; i < b->n; i++) b->gens[i] = b->rcs[i]->gen;
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture: instantiate"); }
   return GI_OK;
@@ -1283,7 +1333,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
     gi_rc *r = b->rcs[i];
     e = cudaStreamWaitEvent(b->streams[i], b->start, 0);
     if (e != cudaSuccess) break;
-    status = vox_build_sun(b->voxes[i], r->shadow ? r->frame : nullptr, r->shadow, r->shadow_size, b->streams[i]);
+    status = rc_vox_build(b->voxes[i], r, b->streams[i]);
     if (status == GI_OK) e = cudaEventRecord(b->done[i], b->streams[i]);
     if (e == cudaSuccess && status == GI_OK) e = cudaStreamWaitEvent(st, b->done[i], 0);
   }
@@ -1295,6 +1345,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
   if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture_passes"); }
   if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture_passes: end");
   e = cudaGraphInstantiate(&b->graph, g, 0);
+  for (uint32_t i = 0; i < b->n; i++) b->gens[i] = b->rcs[i]->gen;
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture_passes: instantiate"); }
   return GI_OK;
@@ -1303,6 +1354,13 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
 int gi_batch_launch(gi_batch *b, void *stream) {
   if (!b) return fail(GI_ERR_INVALID, "gi_batch_launch: NULL batch");
   if (!b->graph) return fail(GI_ERR_STATE, "gi_batch_launch: no graph captured");
+  for (uint32_t i = 0; i < b->n; i++) {
+    if (b->rcs[i]->gen != b->gens[i])
+      return fail(GI_ERR_STATE, "gi_batch_launch: solve %u's shadow map, bounce volume or dynamic layer changed since "
+                                "the capture; capture again", i);
+    if (b->rcs[i]->shadow && b->rcs[i]->frame_layers > b->rcs[i]->shadow_layers)
+      return fail(GI_ERR_STATE, "gi_batch_launch: solve %u's frame asks for more shadow layers than its map has", i);
+  }
   CK(cudaSetDevice(b->ctx->device), "gi_batch_launch: cudaSetDevice");
   CK(cudaGraphLaunch(b->graph, S(stream)), "gi_batch_launch");
   return GI_OK;
@@ -1459,7 +1517,7 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
     case GI_RC_DEPTH: *bytes = npx * 4u; break;
     case GI_RC_NORMAL: *bytes = npx * 8u; break;
     case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;
-    case GI_RC_SHADOW: *bytes = (size_t)r->shadow_size * r->shadow_size * 4u; break;
+    case GI_RC_SHADOW: *bytes = (size_t)r->shadow_size * r->shadow_size * 4u * r->shadow_layers; break;
     case GI_RC_BOUNCE_VOL: *bytes = r->bounce ? 2u * (size_t)r->bn.dx * r->bn.dy * (6u * r->bn.dz + 1u) * 8u : 0u; break;
     case GI_RC_BOUNCE_INJ: *bytes = r->bounce ? (size_t)r->bn_vox->p.max_voxels * 16u : 0u; break;
     case GI_RC_BOUNCE_LIST: *bytes = r->bounce ? (4u + (size_t)r->bn.n) * 4u : 0u; break;
@@ -1589,8 +1647,11 @@ int gi_dyn_build(gi_dyn *d, gi_rc *r, void *stream) {
   if (!d || !r) return fail(GI_ERR_INVALID, "gi_dyn_build: NULL argument");
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_dyn_build: the rc has no frame");
   if (!d->vox->updated) return fail(GI_ERR_STATE, "gi_dyn_build: gi_vox_update was not called");
+  if (r->shadow && r->frame_layers > r->shadow_layers)
+    return fail(GI_ERR_STATE, "gi_dyn_build: the frame asks for more shadow-map layers than the map was drawn with");
   CK(cudaSetDevice(d->vox->scene->ctx->device), "gi_dyn_build: cudaSetDevice");
-  CK(gi_launch_dyn_build(d->dev, d->vox->dev, d->vox->scene->dev(), r->frame, r->shadow, r->shadow ? r->shadow_size : 0u,
+  CK(gi_launch_dyn_build(d->dev, d->vox->dev, d->vox->scene->dev(), r->frame, r->shadow,
+                         r->shadow ? r->shadow_size : 0u, r->shadow_layers,
                          d->vox->scene->ctx->sm_count, S(stream)), "gi_dyn_build: launch");
   return GI_OK;
 }
@@ -1638,6 +1699,7 @@ int gi_rc_set_dyn(gi_rc *r, gi_dyn *d) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_dyn: NULL rc");
   if (d && d->vox->scene->ctx->device != r->ctx->device) return fail(GI_ERR_INVALID, "gi_rc_set_dyn: layer on another device");
   r->dyn = d;
+  r->gen++;
   r->dev.dyn_hdr = d ? d->dev.hdr : nullptr;
   r->dev.dyn_ptr = d ? d->dev.ptr : nullptr;
   r->dev.dyn_data = d ? d->dev.data : nullptr;

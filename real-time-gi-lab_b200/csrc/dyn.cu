@@ -172,13 +172,13 @@ __device__ __forceinline__ uint32_t fix_of(float x) { return __float2uint_rz(rin
 
 // shadeSample (dynlayer.ts:445-455), untextured: false when the alpha test discards the sample
 __device__ __forceinline__ bool shade_sample(const gi_material &m, const float *__restrict__ F, const float *__restrict__ map,
-                                             uint32_t S, f3 p, f3 n, f3 &rad, f3 &alb) {
+                                             uint32_t S, uint32_t layers, f3 p, f3 n, f3 &rad, f3 &alb) {
   const f3 tex = mk(m.base_color[0], m.base_color[1], m.base_color[2]);
   if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;
   alb = tex;
   const float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
   if (ndl <= 0.0f) { rad = mk(0.0f, 0.0f, 0.0f); return true; }
-  const float vis = (map && S) ? sun_tap(F, map, S, p + n * 0.03f) : 1.0f;
+  const float vis = (map && S) ? sun_tap(F, map, S, layers, p + n * 0.03f) : 1.0f;
   const f3 sunE = mk(F[F_SUNE], F[F_SUNE + 1], F[F_SUNE + 2]);
   if ((m.flags & 4u) != 0u && F[F_STYLE] > 0.5f) {   // toonSun (style.ts:18-25)
     const float l = dot(tex, mk(0.2126f, 0.7152f, 0.0722f));
@@ -231,7 +231,7 @@ __device__ __forceinline__ void splat_sample(const DynDev &d, const VoxDev &v, u
 // sample's sums are fixed point, so which lane adds it and when changes nothing).  Sample q of row u: the row's m - u
 // upright sub-triangles first, then its m - u - 1 flipped ones.
 __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev s, const float *__restrict__ F,
-                                                   const float *__restrict__ map, uint32_t S) {
+                                                   const float *__restrict__ map, uint32_t S, uint32_t layers) {
   grid_dep_wait();
   const uint32_t t = d.first + (blockIdx.x * blockDim.x + threadIdx.x) / 32u, lane = threadIdx.x & 31u;
   if (t >= d.end) return;
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev 
     f3 nr = (n0 * wa + n1 * wb) + n2 * wc;
     nr = normalize3(dot(nr, nr) > 1e-12f ? nr : cross(b - a, c - a));
     f3 rad, alb;
-    if (!shade_sample(mat, F, map, S, p, nr, rad, alb)) continue;
+    if (!shade_sample(mat, F, map, S, layers, p, nr, rad, alb)) continue;
     splat_sample(d, v, L, p, nr, sa, rad, alb);
   }
 }
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256) k_dyn_resolve(DynDev d, VoxDev v, uint32_
 using namespace gi;
 
 cudaError_t gi_launch_dyn_build(const DynDev &d, const VoxDev &v, const SceneDev &s, const float *frame,
-                                const float *shadow, uint32_t S, uint32_t sm_count, cudaStream_t st) {
+                                const float *shadow, uint32_t S, uint32_t layers, uint32_t sm_count, cudaStream_t st) {
   if (d.end <= d.first) return cudaSuccess;   // no dynamic triangles: the layer keeps its state (DynLayer.encode)
   const uint32_t nt = d.end - d.first, G3 = v.G * v.G * v.G, nw = v.levels * G3 / 32u;
   const uint32_t persist = sm_count * 8u;
@@ -322,7 +322,7 @@ cudaError_t gi_launch_dyn_build(const DynDev &d, const VoxDev &v, const SceneDev
   GI_TRY(gi_launch(k_dyn_alloc, (nw + 255u) / 256u, 256, st, d, v));
   GI_TRY(gi_launch(k_dyn_finalize, 1, 1, st, d, v));
   GI_TRY(gi_launch(k_dyn_clear, persist, 256, st, d));
-  GI_TRY(gi_launch(k_dyn_splat, (nt * 32u + 255u) / 256u, 256, st, d, v, s, frame, shadow, S));
+  GI_TRY(gi_launch(k_dyn_splat, (nt * 32u + 255u) / 256u, 256, st, d, v, s, frame, shadow, S, layers));
   for (uint32_t L = 1; L < v.levels; L++) GI_TRY(gi_launch(k_dyn_resolve, persist, 256, st, d, v, L));
   return cudaGetLastError();
 }

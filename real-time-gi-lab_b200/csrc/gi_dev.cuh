@@ -245,8 +245,9 @@ struct VoxDev {
   // voxSun (voxel.ts:633-671): with a shadow map, resolveAttr also writes each voxel's sun visibility from it and
   // the frame block (lightViewProj, sun direction, shadow bias); without one the visibility is 1
   const float *sun_frame;
-  const float *shadow;        // shadow_size^2 depths
+  const float *shadow;        // shadow_layers x shadow_size^2 depths
   uint32_t shadow_size;
+  uint32_t shadow_layers;     // 1, or 2 (a world's camera-following pair); layer 1 is read only when the frame asks
   uint32_t scan_hold;          // test hook (gi_vox_debug_hold_scan): part + 1 of the brick scan that never publishes; 0 off
 };
 
@@ -296,23 +297,37 @@ __device__ __forceinline__ bool tri_box(f3 c, f3 h, f3 a, f3 b, f3 cc) {
 enum { F_VP = 0, F_IVP = 16, F_EYE = 80, F_FWD = 84, F_SUN = 88, F_SUNE = 92, F_SKY = 96, F_SIZE = 100, F_RC = 104,
        F_RC2 = 108, F_RU = 112, F_RU2 = 116, F_OMEGA = 120, F_STYLE = 136 };
 
-enum { F_LVP = 64, F_SHADOW = 156 };   // lightViewProj; shadow layers, layer-0 bias, layer-1 bias
+// lightViewProj; lightViewProjFar (the second layer of a world's camera-following pair); shadow layers, layer-0 bias,
+// layer-1 bias
+enum { F_LVP = 64, F_LVPF = 140, F_SHADOW = 156 };
 
-// x's light clip coordinates, mat4 * vec4 summed in column order
-__device__ __forceinline__ f3 light_clip(const float *__restrict__ F, f3 x) {
-  const float *m = F + F_LVP;
+// x's light clip coordinates under the 16-word matrix m (mat4 * vec4 summed in column order)
+__device__ __forceinline__ f3 light_clip(const float *__restrict__ m, f3 x) {
   return mk(m[0] * x.x + m[4] * x.y + m[8] * x.z + m[12] * 1.0f, m[1] * x.x + m[5] * x.y + m[9] * x.z + m[13] * 1.0f,
             m[2] * x.x + m[6] * x.y + m[10] * x.z + m[14] * 1.0f);
 }
 
-// shadowCoord (frame.ts:35-46, one layer) + textureSampleCompareLevel with the 'less-equal' comparison sampler
-// (linear, clamp-to-edge; lighting.ts:162): the four texels around x's map position compared with its biased light
-// depth and weighted bilinearly in f32; 1 (lit) outside the map.
-__device__ __forceinline__ float sun_tap(const float *__restrict__ F, const float *__restrict__ map, uint32_t S, f3 x) {
-  f3 c = light_clip(F, x);
-  float u = c.x * 0.5f + 0.5f, v = c.y * -0.5f + 0.5f;
-  if (!(u >= 0.0f && v >= 0.0f && u <= 1.0f && v <= 1.0f)) return 1.0f;
-  float ref = c.z - F[F_SHADOW + 1];
+__device__ __forceinline__ float sun_compare(const float *__restrict__ map, uint32_t S, float u, float v, float ref);
+
+// shadowCoord (frame.ts:35-46) + textureSampleCompareLevel with the 'less-equal' comparison sampler (linear,
+// clamp-to-edge within the layer; lighting.ts:162): layer 0 where x projects inside it, else layer 1 (at map + S^2)
+// when the frame has two (shadow.x >= 1.5), the four texels around x's map position compared with its biased light
+// depth and weighted bilinearly in f32; 1 (lit) outside every layer.
+// `layers`: the map's layer count (the host refuses a frame asking for more; a second layer is never read past it).
+__device__ __forceinline__ float sun_tap(const float *__restrict__ F, const float *__restrict__ map, uint32_t S,
+                                         uint32_t layers, f3 x) {
+  const f3 c = light_clip(F + F_LVP, x);
+  const float u = c.x * 0.5f + 0.5f, v = c.y * -0.5f + 0.5f;
+  if (u >= 0.0f && v >= 0.0f && u <= 1.0f && v <= 1.0f) return sun_compare(map, S, u, v, c.z - F[F_SHADOW + 1]);
+  if (F[F_SHADOW] < 1.5f || layers < 2u) return 1.0f;
+  const f3 c1 = light_clip(F + F_LVPF, x);
+  const float u1 = c1.x * 0.5f + 0.5f, v1 = c1.y * -0.5f + 0.5f;
+  if (u1 >= 0.0f && v1 >= 0.0f && u1 <= 1.0f && v1 <= 1.0f)
+    return sun_compare(map + (size_t)S * S, S, u1, v1, c1.z - F[F_SHADOW + 2]);
+  return 1.0f;
+}
+
+__device__ __forceinline__ float sun_compare(const float *__restrict__ map, uint32_t S, float u, float v, float ref) {
   float tx = u * (float)S - 0.5f, ty = v * (float)S - 0.5f;
   float fx = floorf(tx), fy = floorf(ty);
   float ax = tx - fx, ay = ty - fy;
@@ -326,8 +341,8 @@ __device__ __forceinline__ float sun_tap(const float *__restrict__ F, const floa
 // voxSun (voxel.ts:643-671) of one voxel: centre pc, size vs, packed oct normal and plane offset as resolveAttr stored
 // them.  The mean of four taps a quarter voxel from the centre's projection on the plane, along two tangents, lifted
 // (0.25 voxel + 3 cm) to the sunward side.
-__device__ __forceinline__ float voxel_sun(const float *__restrict__ F, const float *__restrict__ map, uint32_t S, f3 pc,
-                                           float vs, uint32_t npack, float plane) {
+__device__ __forceinline__ float voxel_sun(const float *__restrict__ F, const float *__restrict__ map, uint32_t S,
+                                           uint32_t layers, f3 pc, float vs, uint32_t npack, float plane) {
   // unpack2x16snorm: k / 32767 as the f64 product rounded to f32 (the f32 quotient for every 16-bit k)
   const double inv32767 = 1.0 / 32767.0;
   float ex = mx(__double2float_rn((double)(int16_t)(npack & 0xffffu) * inv32767), -1.0f);
@@ -345,8 +360,8 @@ __device__ __forceinline__ float voxel_sun(const float *__restrict__ F, const fl
   float h = 0.25f * vs;
   f3 o = q + ns * (0.25f * vs + 0.03f);
   f3 sp = t1 + t2, sm = t1 - t2;
-  return 0.25f * (((sun_tap(F, map, S, o + sp * h) + sun_tap(F, map, S, o + sm * h)) + sun_tap(F, map, S, o - sp * h))
-                  + sun_tap(F, map, S, o - sm * h));
+  return 0.25f * (((sun_tap(F, map, S, layers, o + sp * h) + sun_tap(F, map, S, layers, o + sm * h))
+                   + sun_tap(F, map, S, layers, o - sp * h)) + sun_tap(F, map, S, layers, o - sm * h));
 }
 
 // worldAt (frame.ts:22-26), mat4 * vec4 summed in column order

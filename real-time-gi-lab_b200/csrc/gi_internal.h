@@ -158,10 +158,10 @@ inline void vox_bounds(VoxDev &d) {
 
 cudaError_t gi_launch_vox_build(const gi::VoxDev &v, const gi::SceneDev &s, uint32_t sm_count, cudaStream_t st);
 // One build of the dynamic layer (mark .. resolve) in the voxel world's windows; frame: sun, style, light view; shadow:
-// the sun's S x S map or null (visibility 1)
+// the sun's map of `layers` S x S layers, or null (visibility 1)
 cudaError_t gi_launch_dyn_build(const gi::DynDev &d, const gi::VoxDev &v, const gi::SceneDev &s, const float *frame,
-                                const float *shadow, uint32_t S, uint32_t sm_count, cudaStream_t st);
-cudaError_t gi_launch_shadow(const gi::SceneDev &s, const float *frame_dev, uint32_t S, const gi::ShadowRaster &sr,
+                                const float *shadow, uint32_t S, uint32_t layers, uint32_t sm_count, cudaStream_t st);
+cudaError_t gi_launch_shadow(const gi::SceneDev &s, const float *matrix_dev, uint32_t S, const gi::ShadowRaster &sr,
                              uint32_t sm_count, cudaStream_t st);
 // ev (optional, 5 events): recorded after giBuild (setupScreen), giTrace, giMerge (merge + projectSH), giGather.
 // Kernel launch with programmatic dependent launch allowed: the next kernel in the stream (or graph) may be scheduled
@@ -218,6 +218,7 @@ uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
                               uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
+cudaError_t gi_launch_normal_rgb_to_rgba(const uint16_t *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);
 // FP64 reference of merge + SH + gather from the f32 traced atlas: rad64 rays_total x 4 doubles, sh64 27 doubles per

@@ -1151,6 +1151,15 @@ __global__ void k_init_dirs(RcDev r, float4 *dirs, uint32_t ndirs) {
   dirs[ndirs + i] = make_float4(1.0f / dd.x, 1.0f / dd.y, 1.0f / dd.z, 0.0f);
 }
 
+// rgb16f normals (three halves per pixel) to the rgba16f layout the kernels read, alpha 0
+__global__ void k_normal_rgb_to_rgba(const uint16_t *__restrict__ src, uint2 *__restrict__ dst, uint32_t n) {
+  grid_dep_wait();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint16_t *s = src + 3u * (size_t)i;
+    dst[i] = make_uint2((uint32_t)s[0] | ((uint32_t)s[1] << 16), (uint32_t)s[2]);
+  }
+}
+
 __global__ void k_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n) {
   grid_dep_wait();
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -1249,6 +1258,11 @@ cudaError_t gi_launch_init_dirs(const RcDev &r, float4 *dirs, uint32_t ndirs, cu
 
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st) {
   k_normal_f32_to_f16<<<256, 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+cudaError_t gi_launch_normal_rgb_to_rgba(const uint16_t *src, uint2 *dst, uint32_t n, cudaStream_t st) {
+  k_normal_rgb_to_rgba<<<1184, 256, 0, st>>>(src, dst, n);
   return cudaGetLastError();
 }
 

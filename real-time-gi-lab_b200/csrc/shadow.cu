@@ -1,7 +1,9 @@
 // Sun shadow map on sm_100a (the reference's shadow pass, src/core/lighting.ts:133-140, 175-189: depth32float cleared
 // to 1, compare 'less', depthBias 2, depthBiasSlopeScale 2, cull none, alpha-masked fragments discarded), defined for
 // a compute-only device as a raster of the light's orthographic clip space at texel centres:
-//   clip     c_k = lightViewProj * (p_k, 1) (frame words 64-79), summed in column order; w = 1 (orthographic)
+//   clip     c_k = M * (p_k, 1), summed in column order; w = 1 (orthographic).  M is the layer's matrix: layer 0
+//            lightViewProj (frame words 64-79), layer 1 of a world's camera-following pair lightViewProjFar (140-155);
+//            each layer is one launch sequence into its own S x S slice
 //   cover    texel (i, j) centre x = (i + 0.5) / S * 2 - 1, y = 1 - (j + 0.5) / S * 2 is inside when its three edge
 //            functions w_k = (b - a) x (centre - a) are all >= 0 or all <= 0 (either winding, edges included)
 //   depth    z = (w0 z0 + w1 z1 + w2 z2) / (w0 + w1 + w2), kept when 0 <= z <= 1
@@ -56,7 +58,7 @@ __device__ __forceinline__ float sm_bias_unit(float zmax) {
 
 // Per triangle: rec[4t] = (c0, bias), [4t+1] = (c1, i0 | j0 << 16), [4t+2] = (c2, bw | bh << 16), the chunk count,
 // its exclusive prefix within the block and the block's sum.  Also clears the map (grid-stride).
-__global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__restrict__ F, uint32_t S, ShadowRaster sr) {
+__global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__restrict__ M, uint32_t S, ShadowRaster sr) {
   grid_dep_wait();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < (size_t)S * S; i += (size_t)gridDim.x * blockDim.x)
     sr.map[i] = 1.0f;
@@ -68,7 +70,7 @@ __global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__res
     if (!((mt.flags & 1u) != 0u && mt.base_color[3] < mt.alpha_cutoff)) {
       f3 a = ld3(s.pos[idx.x]), b = ld3(s.pos[idx.y]), c = ld3(s.pos[idx.z]);
       if (s.inst) { a = a + off; b = b + off; c = c + off; }
-      f3 c0 = light_clip(F, a), c1 = light_clip(F, b), c2 = light_clip(F, c);
+      f3 c0 = light_clip(M, a), c1 = light_clip(M, b), c2 = light_clip(M, c);
       float det = (c1.x - c0.x) * (c2.y - c0.y) - (c2.x - c0.x) * (c1.y - c0.y);
       if (det != 0.0f) {
         const float inv = 1.0f / (float)S, fS = (float)S;
@@ -180,10 +182,10 @@ __global__ void __launch_bounds__(256) k_sm_raster(uint32_t ntris, uint32_t S, S
 
 using namespace gi;
 
-cudaError_t gi_launch_shadow(const SceneDev &s, const float *frame_dev, uint32_t S, const ShadowRaster &sr,
+cudaError_t gi_launch_shadow(const SceneDev &s, const float *matrix_dev, uint32_t S, const ShadowRaster &sr,
                              uint32_t sm_count, cudaStream_t st) {
   uint32_t nblk = s.ntris ? (s.ntris + 255u) / 256u : 1u;
-  GI_TRY(gi_launch(k_sm_setup, nblk, 256, st, s, frame_dev, S, sr));
+  GI_TRY(gi_launch(k_sm_setup, nblk, 256, st, s, matrix_dev, S, sr));
   GI_TRY(gi_launch(k_sm_scan, 1, 256, st, nblk, sr));
   if (s.ntris) GI_TRY(gi_launch(k_sm_raster, sm_count * 8u, 256, st, s.ntris, S, sr));
   return cudaGetLastError();

@@ -341,11 +341,16 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
 __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t t, uint32_t L,
                                              i3 c, bool single, uint32_t brick_overflow) {
   if (finer_built(v, L, c, brick_overflow)) return;
+#if GI_VB_EARLYPTR
+  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the test
+#endif
   float vs = vox_size(v, L);
   f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
   float hh = 0.5f * vs * 1.0001f;
   if (!single && !tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return;
+#if !GI_VB_EARLYPTR
   uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
+#endif
   if (ptr >= GI_MARK) return;
   uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
   // surfaceAt's alpha test (voxel.ts:325-332): untextured, so the sampled alpha is the factor's
@@ -354,13 +359,9 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
   uint32_t wi = ptr * 16u + (bit >> 5);
   uint32_t msk = 1u << (bit & 31u);
   uint32_t ri = ptr * 512u + bit;
-#if GI_VB_NOREAD
+  // unconditional reductions (their results unused): the warp does not wait for a read of the word first
   atomicOr(&v.occ[wi], msk);
   atomicMax(&v.rep[ri], t + 1u);
-#else
-  if ((v.occ[wi] & msk) == 0u) atomicOr(&v.occ[wi], msk);
-  if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
-#endif
 }
 
 // voxBits (voxel.ts:492-513)
@@ -443,11 +444,16 @@ __global__ void __launch_bounds__(256) k_chunks(VoxDev v, SceneDev s) {
 __device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t L, i3 c,
                                             uint32_t brick_overflow, uint32_t &wi, uint32_t &msk, uint32_t &ri) {
   if (finer_built(v, L, c, brick_overflow)) return false;
+#if GI_VB_EARLYPTR
+  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the test
+#endif
   float vs = vox_size(v, L);
   f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
   float hh = 0.5f * vs * 1.0001f;
   if (!tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return false;
+#if !GI_VB_EARLYPTR
   uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
+#endif
   if (ptr >= GI_MARK) return false;
   const gi_material &m = s.mats[T.idx.w];
   if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;
@@ -505,13 +511,8 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
       uint32_t grp = __match_any_sync(0xffffffffu, ok ? wi : 0xffffffffu);
       uint32_t m = __reduce_or_sync(grp, msk);
       if (ok) {
-#if GI_VB_NOREAD
         if ((uint32_t)(__ffs(grp) - 1) == lane) atomicOr(&v.occ[wi], m);
         atomicMax(&v.rep[ri], t + 1u);
-#else
-        if ((uint32_t)(__ffs(grp) - 1) == lane && (v.occ[wi] & m) != m) atomicOr(&v.occ[wi], m);
-        if (v.rep[ri] < t + 1u) atomicMax(&v.rep[ri], t + 1u);
-#endif
       }
     }
   }
@@ -665,23 +666,11 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
   uint32_t nb = min(v.hdr[0], v.max_bricks);
   uint32_t nv = nb ? min(v.vpre[nb], v.max_voxels) : 0u;
   for (uint32_t ai = blockIdx.x * blockDim.x + threadIdx.x; ai < nv; ai += gridDim.x * blockDim.x) {
-#if GI_RA_WARPSEARCH
-    // the last brick b with vpre[b] <= ai: searched once per warp for its first voxel, then walked forward per lane
-    // (a warp's 32 consecutive voxels span a few bricks)
-    const uint32_t a0 = __shfl_sync(__activemask(), ai, __ffs(__activemask()) - 1);
-    uint32_t lo = 0, hi = nb;
-    while (hi - lo > 1u) {
-      uint32_t m = (lo + hi) >> 1;
-      if (v.vpre[m] <= a0) lo = m; else hi = m;
-    }
-    while (lo + 1u < nb && v.vpre[lo + 1u] <= ai) lo++;
-#else
     uint32_t lo = 0, hi = nb;   // the last brick b with vpre[b] <= ai
     while (hi - lo > 1u) {
       uint32_t m = (lo + hi) >> 1;
       if (v.vpre[m] <= ai) lo = m; else hi = m;
     }
-#endif
     uint32_t ptr = lo;
     if (v.base[ptr] == GI_EMPTY) continue;   // past the voxel pool: no attributes (voxel.ts:586)
     uint32_t r = ai - v.vpre[ptr];
@@ -711,7 +700,8 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
     uint32_t rv = v.rep[ptr * 512u + bit];
     if (rv == 0u || rv > s.key_limit) {   // no representative (cannot happen for a set bit): no attributes
       v.attr[ai] = make_uint4(0u, 0u, 0u, 0u); v.plane[ai] = 0.0f;
-      v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, p, vox_size(v, L), 0u, 0.0f) : 1.0f;
+      v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, v.shadow_layers, p, vox_size(v, L), 0u,
+                                          0.0f) : 1.0f;
       continue;
     }
     Tri T = load_tri(s, rv - 1u);
@@ -741,7 +731,8 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
     float pl = dot(n, q - p);
     v.plane[ai] = pl;
     // voxSun (voxel.ts:633-671) from the values just stored
-    v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, p, vox_size(v, L), rec.y, pl) : 1.0f;
+    v.sunvis[ai] = v.shadow ? voxel_sun(v.sun_frame, v.shadow, v.shadow_size, v.shadow_layers, p, vox_size(v, L), rec.y,
+                                        pl) : 1.0f;
   }
 }
 

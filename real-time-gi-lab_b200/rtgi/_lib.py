@@ -47,6 +47,7 @@ SIGNATURES = {
     "gi_rc_set_frame": (C.c_int, [_P, _P, _P]),
     "gi_rc_set_gbuffer": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_set_gbuffer_f16": (C.c_int, [_P, _P, _P, _P]),
+    "gi_rc_set_gbuffer_rgb16f": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_render_gbuffer": (C.c_int, [_P, _P, _P]),
     "gi_rc_render_shadow": (C.c_int, [_P, _P, C.c_uint32, _P]),
     "gi_rc_set_bounce": (C.c_int, [_P, _P, _P]),

@@ -37,6 +37,37 @@ def scene_sun_view_proj(bounds_min, bounds_max, sun_dir) -> list:
                          mathx.look_at(mathx.add3(center, mathx.scale3(d, radius)), center, up))
 
 
+# The camera-following shadow layers of an instanced world (lighting.ts:93-96): layer 0 of half width NEAR_R m, layer 1
+# of FAR_R m, depth DEPTH_R m on either side of the camera along the sun; biases in metres over the 2 DEPTH_R range
+SHADOW_NEAR_R, SHADOW_FAR_R, SHADOW_DEPTH_R = 32, 410, 300
+SHADOW_WORLD_BIAS = (0.012 / (2 * SHADOW_DEPTH_R), 0.15 / (2 * SHADOW_DEPTH_R))
+
+
+def _js_round(x: float) -> float:
+    """Math.round: the nearest integer, halves toward +infinity (exact, unlike floor(x + 0.5) near 0.5)."""
+    r = math.floor(x)
+    return float(r + 1 if x - r >= 0.5 else r)
+
+
+def world_sun_view_projs(sun_dir, eye, size: int = SHADOW_SIZE) -> tuple:
+    """cameraMatrix (lighting.ts:115-123) for layer 0 (NEAR_R) and layer 1 (FAR_R): an orthographic light view of
+    half width r centred on the camera, the centre snapped to the layer's texels across the sun (so the map does not
+    shimmer as the camera moves), depth 0 DEPTH_R m sunward of the camera and 1 DEPTH_R m past it."""
+    sun = mathx.scale3(sun_dir, 1 / mathx.hypot(*sun_dir))
+    up0 = [0, 0, 1] if abs(sun[1]) > 0.99 else [0, 1, 0]
+    right = mathx.normalize(mathx.cross(up0, sun))
+    up = mathx.cross(sun, right)
+
+    def layer(r):
+        texel = 2 * r / size
+        snap = lambda x: _js_round(x / texel) * texel
+        c = mathx.add3(mathx.add3(mathx.scale3(right, snap(mathx.dot(eye, right))), mathx.scale3(up, snap(mathx.dot(eye, up)))),
+                       mathx.scale3(sun, mathx.dot(eye, sun)))
+        return mathx.mat_mul(mathx.ortho_zo(r, r, 0, 2 * SHADOW_DEPTH_R),
+                             mathx.look_at(mathx.add3(c, mathx.scale3(sun, SHADOW_DEPTH_R)), c, up0))
+    return layer(SHADOW_NEAR_R), layer(SHADOW_FAR_R)
+
+
 def scene_bounds(positions) -> tuple:
     """boundsMin / boundsMax (gltf.ts:147) of f32 vertex positions, as f64 values."""
     p = np.asarray(positions, dtype=np.float32)

@@ -273,8 +273,10 @@ class Rc:
         _lib.call("gi_rc_set_bounce", self.handle, vox.handle, C.byref(p))
 
     def read_shadow(self, stream=None) -> np.ndarray:
+        """The shadow map: (S, S), or (2, S, S) when drawn for a frame with two layers."""
         S = getattr(self, "shadow_size", 0)
-        return self.read_buffer(_lib.GI_RC_SHADOW, stream).view(np.float32).reshape(S, S)
+        m = self.read_buffer(_lib.GI_RC_SHADOW, stream).view(np.float32).reshape(-1, S, S)
+        return m[0] if m.shape[0] == 1 else m
 
     def encode(self, vox: VoxWorld, stream=None):
         _lib.call("gi_rc_solve", self.handle, vox.handle, _stream(stream))
@@ -340,9 +342,11 @@ class Rc:
         wide = (self.params.atlas == "f32" or self.params.f32Out) and not self.params.irr16
         return self.width * self.height * (16 if wide else 8)
 
-    def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None):
-        """G-buffer from host pointers (pinned memory makes the copies asynchronous)."""
-        _lib.call("gi_rc_set_gbuffer_f16", self.handle, depth_ptr, normal_f16_ptr, _stream(stream))
+    def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None, rgb: bool = False):
+        """G-buffer from host pointers (pinned memory makes the copies asynchronous); rgb: the normals as three
+        halves per pixel (gi_rc_set_gbuffer_rgb16f) instead of four."""
+        _lib.call("gi_rc_set_gbuffer_rgb16f" if rgb else "gi_rc_set_gbuffer_f16", self.handle, depth_ptr,
+                  normal_f16_ptr, _stream(stream))
 
     def set_frame_ptr(self, frame_ptr: int, stream=None):
         _lib.call("gi_rc_set_frame", self.handle, frame_ptr, _stream(stream))

@@ -1,7 +1,7 @@
 """Frames streamed through the drop-in path with the host copies overlapped (no counterpart in the reference, which
 submits one frame per queue and maps its readback buffer when the frame is done, rcrun.ts:322-335).
 
-Each frame's inputs (the 640-byte frame block, depth f32, normal rgba16f) are copied from pinned host memory on an
+Each frame's inputs (the 640-byte frame block, depth f32, normal rgba16f or its rgb halves) are copied from pinned host memory on an
 upload stream, the frame is solved (voxel rebuild + cascades, one captured graph) on the compute stream, and its
 irradiance is copied back on a download stream.  `slots` cascade sets take turns, so frame k+1's upload and frame
 k-1's download run while frame k is solved: the step time approaches the slower of the PCIe copies and the solve
@@ -16,20 +16,22 @@ from . import gpu
 
 class FramePipeline:
     def __init__(self, ctx: gpu.Context, vox: gpu.VoxWorld, params, width: int, height: int, frame, depth_ptr: int,
-                 normal_f16_ptr: int, slots: int = 2, shadow=None, tuning=None):
+                 normal_f16_ptr: int, slots: int = 2, shadow=None, tuning=None, normal_rgb: bool = False):
         """frame/depth/normal: a first frame's inputs (frame as an array, the G-buffer as pinned host pointers), used
         to capture each slot's graph.  shadow: (SceneGpu, size) to give every slot the sun's shadow map drawn from
         that frame (a static sun and scene; draw it again with Rc.render_shadow when they move).  tuning: launch
-        shapes for every slot (Rc.set_tuning's keywords; results do not depend on them)."""
+        shapes for every slot (Rc.set_tuning's keywords; results do not depend on them).  normal_rgb: the host
+        normals are three halves per pixel (6 bytes over the bus instead of 8; the path reads no alpha)."""
         import torch
         self.torch = torch
         self.vox = vox
+        self.rgb = normal_rgb
         self.up, self.comp, self.down = torch.cuda.Stream(), torch.cuda.Stream(), torch.cuda.Stream()
         self.rcs: List[gpu.Rc] = []
         for _ in range(slots):
             rc = gpu.Rc(ctx, params, width, height)
             rc.set_frame(frame, self.comp)
-            rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.comp)
+            rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.comp, rgb=normal_rgb)
             if tuning:
                 rc.set_tuning(**tuning)
             if shadow is not None:
@@ -57,7 +59,7 @@ class FramePipeline:
         rc = self.rcs[s]
         self.up.wait_event(self.solved[s])          # the slot's previous solve has read its inputs
         rc.set_frame_ptr(frame_ptr, self.up)
-        rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.up)
+        rc.set_gbuffer_ptrs(depth_ptr, normal_f16_ptr, self.up, rgb=self.rgb)
         self.uploaded[s].record(self.up)
         self.comp.wait_event(self.uploaded[s])
         self.comp.wait_event(self.downloaded[s])   # the slot's previous irradiance has been read back

@@ -1,4 +1,5 @@
-"""rtgi.pipeline: frames streamed with overlapped host copies give each frame the irradiance of a plain solve."""
+"""rtgi.pipeline: frames streamed with overlapped host copies give each frame the irradiance of a plain solve, with
+the normals uploaded as rgba16f or as their three rgb halves (gi_rc_set_gbuffer_rgb16f)."""
 import numpy as np
 import pytest
 import torch
@@ -9,7 +10,8 @@ from rtgi import _lib, frame as fr, gpu, pipeline, scenes
 pytestmark = pytest.mark.gpu
 
 
-def test_pipeline_matches_plain_solves():
+@pytest.mark.parametrize("rgb", [False, True], ids=["rgba16f", "rgb16f"])
+def test_pipeline_matches_plain_solves(rgb):
     case = gi_cases.room_lit()
     ctx = gpu.Context(0)
     sg = gpu.SceneGpu(ctx, case.scene)
@@ -29,6 +31,8 @@ def test_pipeline_matches_plain_solves():
         out = np.zeros(rc.irr_bytes(), np.uint8)
         rc.read_irradiance_raw(out)
         expect.append(out)
+        if rgb:
+            n = np.ascontiguousarray(n.reshape(-1, 4)[:, :3]).reshape(-1)
         inputs.append((torch.from_numpy(F.copy()).pin_memory(), torch.from_numpy(d).pin_memory(),
                        torch.from_numpy(n).pin_memory()))
     rc.destroy()
@@ -36,7 +40,7 @@ def test_pipeline_matches_plain_solves():
     order = [0, 1, 1, 0, 1, 0, 0, 1]
     outs = [torch.empty(expect[0].size, dtype=torch.uint8).pin_memory() for _ in order]
     pipe = pipeline.FramePipeline(ctx, vw, case.rc, case.width, case.height, frames[0], inputs[0][1].data_ptr(),
-                                  inputs[0][2].data_ptr(), slots=2)
+                                  inputs[0][2].data_ptr(), slots=2, normal_rgb=rgb)
     for k, i in enumerate(order):
         f, d, n = inputs[i]
         pipe.submit(f.data_ptr(), d.data_ptr(), n.data_ptr(), outs[k].data_ptr())

@@ -113,3 +113,74 @@ def test_voxel_sun_visibility_known_answer():
     assert (vis[under] == 0.0).all()
     assert (vis[open_] == 1.0).all()
     assert (vis[top] == 1.0).all()
+
+
+def test_js_round_is_math_round():
+    """Math.round: halves toward +infinity, and no double rounding below one half."""
+    assert fr._js_round(0.49999999999999994) == 0.0 and fr._js_round(0.5) == 1.0
+    assert fr._js_round(-2.5) == -2.0 and fr._js_round(2.5) == 3.0 and fr._js_round(-0.6) == -1.0
+
+
+def test_camera_following_layers():
+    """cameraMatrix (lighting.ts:115-123): layer 0 of half width 32 m and layer 1 of 410 m centred on the camera's
+    position across the sun, snapped to the layer's texels, depth 0.5 at the camera; moving the camera less than a
+    texel across the sun leaves the lateral placement where it was."""
+    sun = (0.3, 1.0, 0.2)
+    eye = (13.37, 1.6, -7.21)
+    S = 4096
+    near, far = fr.world_sun_view_projs(sun, eye, S)
+    for m, r in ((near, fr.SHADOW_NEAR_R), (far, fr.SHADOW_FAR_R)):
+        M = np.array(m, np.float64).reshape(4, 4).T
+        q = M @ np.array([*eye, 1.0])
+        texel_ndc = 2.0 / S
+        assert abs(q[0]) <= 0.5 * texel_ndc + 1e-6 and abs(q[1]) <= 0.5 * texel_ndc + 1e-6   # centred within a texel
+        assert abs(q[2] - 0.5) < 1e-5
+        d = np.array(sun) / np.linalg.norm(sun)
+        assert abs((M @ np.array([*(np.array(eye) + d * fr.SHADOW_DEPTH_R), 1.0]))[2]) < 1e-4
+        x = np.array(eye) + np.cross(d, [0, 1.0, 0]) / np.linalg.norm(np.cross(d, [0, 1.0, 0])) * (r * 0.999)
+        assert abs(abs((M @ np.array([*x, 1.0]))[0]) - 0.999) < 1e-3 or abs(abs((M @ np.array([*x, 1.0]))[1]) - 0.999) < 1e-3
+    # the snapped placement: a step of a tenth of a layer-0 texel across the sun keeps x/y translation
+    t0 = 2 * fr.SHADOW_NEAR_R / S
+    up0 = np.array([0, 1.0, 0])
+    right = np.cross(up0, np.array(sun) / np.linalg.norm(sun))
+    right /= np.linalg.norm(right)
+    e2 = tuple(np.array(eye) + right * (0.1 * t0))
+    n2, _ = fr.world_sun_view_projs(sun, e2, S)
+    snap = lambda e: fr._js_round(float(np.dot(e, right)) / t0)
+    if snap(eye) == snap(e2):
+        assert n2[12] == near[12] and n2[13] == near[13]
+
+
+def _world_frame(s, S, eye):
+    near, far = fr.world_sun_view_projs(s.sun_dir, eye, S)
+    return fr.pack_frame(fr.FrameParams(cam=s.camera, width=64, height=64, sun_dir=s.sun_dir, light_view_proj=near,
+                                        shadow_far=far, shadow_bias=fr.SHADOW_WORLD_BIAS, cascades=2))
+
+
+def test_two_layer_tap_picks_the_layer():
+    """shadowCoord with two layers: a point inside layer 0 reads layer 0; a point outside it reads layer 1 as a
+    one-layer frame made of layer 1 would; outside both it is lit.  The layers are drawn from their own matrices."""
+    b = scenes.Builder([scenes.Material("grey", (0.5, 0.5, 0.5, 1.0))])
+    b.quad([-300, 0, 300], [300, 0, 300], [300, 0, -300], [-300, 0, -300])
+    b.box((0.0, 1.5, 0.0), (1.0, 0.5, 1.0))     # a box near the camera
+    b.box((100.0, 1.5, 0.0), (8.0, 0.5, 8.0))   # a wide one 100 m away (layer 1 only: 1.6 m texels at 512^2)
+    s = b.scene("layers", scenes.Camera((0, 3, 6), (0, 0, 0), 60, 0.05), sun_dir=(0.0, 1.0, 0.0))
+    S = 512
+    F = _world_frame(s, S, (0.0, 1.6, 0.0))
+    assert int(F[156]) == 2
+    m = bind.shadow_render(s, F, S)
+    assert m.shape == (2, S, S) and (m[0] < 1).any() and (m[1] < 1).any()
+    # layer 1 alone, as a one-layer frame: the same map and the same taps outside layer 0
+    F1 = F.copy()
+    F1[64:80] = F[140:156]
+    F1[156:159] = [1, F[158], 0]
+    m1 = bind.shadow_render(s, F1, S)
+    assert np.array_equal(m1.view(np.uint32), m[1].view(np.uint32))
+    assert bind.sun_tap(F, m, [0.0, 0.03, 0.0]) == 0.0          # under the near box: layer 0
+    far_pt = [100.0, 0.03, 0.0]                                 # under the far box: outside layer 0, inside layer 1
+    assert bind.sun_tap(F, m, far_pt) == bind.sun_tap(F1, m1, far_pt) == 0.0
+    assert bind.sun_tap(F, m, [100.0, 0.03, 30.0]) == 1.0
+    assert bind.sun_tap(F, m, [0.0, 0.03, 900.0]) == 1.0        # outside both layers
+    F_one = F.copy()
+    F_one[156] = 1                                              # one layer: the far box's shadow is not seen
+    assert bind.sun_tap(F_one, m, far_pt) == 1.0
