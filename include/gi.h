@@ -219,6 +219,12 @@ int gi_rc_set_gbuffer_f16(gi_rc *rc, const float *depth, const uint16_t *normal_
 /* The same with the normal as three halves per pixel (the rgba16float texture's r, g, b; the path reads no alpha):
  * 6 bytes a pixel over the bus instead of 8, expanded on the device (stream-ordered, alpha 0 as the raster writes). */
 int gi_rc_set_gbuffer_rgb16f(gi_rc *rc, const float *depth, const uint16_t *normal_rgb16f, void *stream);
+/* The G-buffer's style tag (gbuffer.ts:2: the alpha byte of its rgba8 albedo: 1 toon, 0.5 another measured object,
+ * 0 photoreal), W*H bytes from host memory.  gatherWorld applies the receiving operator to toon pixels
+ * (rc.ts:877-926: the interpolated L0/L1 SH through toonReceive, style.ts:30-42, output alpha 2 + band + 2 contrast)
+ * and counts only photoreal pixels as black.  All zero at creation; gi_rc_render_gbuffer writes it from the
+ * materials' flags (4 toon, 8 object).  The screen method does not read it. */
+int gi_rc_set_gbuffer_tag(gi_rc *rc, const uint8_t *tag, void *stream);
 /* G-buffer drawn on the device from the scene and the frame (one primary-ray sample per pixel centre). */
 int gi_rc_render_gbuffer(gi_rc *rc, gi_scene *scene, void *stream);
 /* The sun shadow map (encodeShadow, lighting.ts:175-189; depth32float, compare less, depth bias 2 + slope 2, cull
@@ -305,15 +311,16 @@ enum {
   GI_RC_NORMAL = 4,     /* W*H*4 halves */
   GI_RC_HITS = 5,       /* per ray: level, brick, bit, tIn bits (only after gi_rc_set_debug_hits(rc, 1)) */
   GI_RC_RAD_TRACED = 6, /* the atlas right after the trace, before the merge (only with debug hits on) */
-  GI_RC_SHADOW = 7,     /* size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
+  GI_RC_SHADOW = 7,     /* layers*size*size f32, the sun shadow map (only after gi_rc_render_shadow) */
   GI_RC_BOUNCE_VOL = 8, /* the two bounce volumes, dx*dy*(6dz+1) rgba16f texels each (only with multi-bounce on) */
   GI_RC_BOUNCE_INJ = 9, /* per voxel the injected irradiance: 8 halves (front rgb, 0, back rgb, 0) (multi-bounce on) */
   GI_RC_BOUNCE_LIST = 10, /* 4 + dx*dy*dz words: listed probes, frame counter, current volume, then the list */
   GI_RC_WORLD_KEYS = 11,  /* world probes: every cascade's hash table of probe keys (0 = empty) */
   GI_RC_WORLD_SLOTS = 12, /* world probes: per hash slot the key's probe (0xffffffff: none, or past the capacity) */
   GI_RC_WORLD_PARENTS = 13, /* world probes: per probe the 8 probes of the cascade above it merges (0xffffffff: none) */
-  GI_RC_WORLD_STATE = 14  /* world probes: 64 words: [0] history parity, [7] nonzero if a compaction's scan stopped
+  GI_RC_WORLD_STATE = 14, /* world probes: 64 words: [0] history parity, [7] nonzero if a compaction's scan stopped
                              waiting (never expected), [8 + c] probes of cascade c, [16 + c] first ray of cascade c */
+  GI_RC_TAG = 15          /* W*H bytes: the G-buffer's style tag (its albedo's alpha byte: 255 toon, 128 object, 0) */
 };
 int gi_rc_read_buffer(gi_rc *rc, int what, void *out, size_t bytes, void *stream);
 int gi_rc_buffer_bytes(gi_rc *rc, int what, size_t *bytes);
@@ -332,7 +339,9 @@ int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);
 typedef struct gi_rc_tuning {
   uint32_t trace_order;    /* 0: probe-major (a warp's lanes take consecutive directions of a probe, coalesced atlas
                               writes), 1: direction-major (a warp's lanes take one direction of 32 neighbouring probes,
-                              coherent voxel paths) */
+                              coherent voxel paths), 2: walk-length order (screen probes; the rays by the previous
+                              solve's DDA step count and hit, longest first, so a warp's lanes walk alike; the first
+                              solve after choosing it keeps the atlas order; 13 bytes per ray more) */
   uint32_t trace_rays;     /* rays per lane per queue fetch: 1, 2 or 4 */
   uint32_t trace_blocks;   /* resident 256-thread blocks per SM of the persistent trace: 1..16 (default 8) */
   uint32_t gather_shape;   /* gather: 0, 1, 2 blocks of 16x16, 32x8, 8x32 pixels; 3 (default) warps on pixel tiles

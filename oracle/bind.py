@@ -123,7 +123,7 @@ class OrcLayout(C.Structure):
 
 class OrcGbuf(C.Structure):
     _fields_ = [("frame", C.c_void_p), ("width", C.c_uint32), ("height", C.c_uint32), ("depth", C.c_void_p),
-                ("normal", C.c_void_p)]
+                ("normal", C.c_void_p), ("tag", C.c_void_p)]
 
 
 class OrcRcOut(C.Structure):
@@ -251,7 +251,7 @@ def rc_solve(vox: dict, lay: dict, frame: np.ndarray, depth: np.ndarray, normal:
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     depth = np.ascontiguousarray(depth, dtype=np.float32)
     normal = np.ascontiguousarray(normal, dtype=np.float32)
-    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal), None)
     o = OrcRcOut(_p(out["probes"]), _p(out["rad"]), _p(out["sh"]), _p(out["irr"]), _p(out["counts"]),
                  _p(out["hit"]) if want_hit else None)
     vx = _vox_struct(vox)
@@ -272,7 +272,7 @@ def merge_gather_f64(lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np
     probes = np.ascontiguousarray(probes)
     rad = np.ascontiguousarray(rad_traced, dtype=np.float32)
     irr = np.zeros((H, W, 4), np.float64)
-    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal), None)
     lib().orc_rc_merge_gather_f64(C.byref(ly), C.byref(g), _p(probes), _p(rad), _p(irr))
     return irr
 
@@ -300,6 +300,27 @@ def raster_gbuffer(scene, frame: np.ndarray, W: int, H: int, ndraw: int = 0, dra
     if r != 0:
         raise MemoryError("oracle raster: out of memory")
     return depth, normal, tri
+
+
+def toon_receive(c, n, soft: float) -> np.ndarray:
+    """toonReceive of (c0, c1y, c1z, c1x) (12 floats) for normal n: (E rgb, band, contrast)."""
+    c = np.ascontiguousarray(c, np.float32)
+    n = np.ascontiguousarray(n, np.float32)
+    out = np.zeros(5, np.float32)
+    lib().orc_toon_receive(_p(c), _p(n), C.c_float(soft), _p(out))
+    return out
+
+
+def gbuffer_tags(scene, tri: np.ndarray, ndraw: int = 0) -> np.ndarray:
+    """The G-buffer's style tags (gbuffer.ts:2, the albedo's alpha byte) from the raster's triangle per pixel
+    (instance * ndraw + row; 0xffffffff: background): 255 for a toon material (flag 4), 128 for another measured
+    object (flag 8), 0 for photoreal materials and the background."""
+    flags = np.array([int(m.flags) for m in scene.materials], np.uint32)
+    t = np.asarray(tri, np.int64)
+    bg = t == 0xffffffff
+    row = np.where(bg, 0, t % (ndraw or scene.triangle_count))
+    f = np.where(bg, 0, flags[np.asarray(scene.tri, np.int64)[row, 3]])
+    return np.where(f & 4, 255, np.where(f & 8, 128, 0)).astype(np.uint8)
 
 
 def shadow_render(scene, frame: np.ndarray, S: int, ndraw: int = 0, draw_instances=None) -> np.ndarray:
@@ -397,8 +418,9 @@ def wlayout_struct(lay: dict) -> OrcWLayout:
 
 
 def world_solve(vox: dict, lay: dict, state: WorldState, frame: np.ndarray, depth: np.ndarray, normal: np.ndarray,
-                want_hit: bool = False) -> dict:
-    """One world-probe solve (orc_world_solve) over a built voxel world; `state` carries over between solves."""
+                want_hit: bool = False, tag: np.ndarray = None) -> dict:
+    """One world-probe solve (orc_world_solve) over a built voxel world; `state` carries over between solves.
+    tag: the G-buffer's style tags (H x W bytes: 255 toon, 128 object, 0), or None (all photoreal)."""
     H, W = depth.shape
     wl = wlayout_struct(lay)
     cap0 = lay["casc"][0]["cap"]
@@ -410,7 +432,8 @@ def world_solve(vox: dict, lay: dict, state: WorldState, frame: np.ndarray, dept
     frame = np.ascontiguousarray(frame, dtype=np.float32)
     depth = np.ascontiguousarray(depth, dtype=np.float32)
     normal = np.ascontiguousarray(normal, dtype=np.float32)
-    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal))
+    tag = None if tag is None else np.ascontiguousarray(tag, dtype=np.uint8)
+    g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal), None if tag is None else _p(tag))
     o = OrcRcOut(_p(out["probes"]), _p(out["rad"]), _p(out["sh"]), _p(out["irr"]), _p(out["counts"]),
                  _p(out["hit"]) if want_hit else None)
     ws = OrcWState(_p(state.keys), _p(state.slot_probe), _p(state.parents), _p(state.hist_tab), _p(state.hist_grid),

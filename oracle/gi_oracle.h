@@ -150,6 +150,7 @@ typedef struct {
   uint32_t width, height;
   const float *depth;       /* W*H reversed-Z depth (0 = background) */
   const float *normal;      /* W*H*4, the G-buffer normal as read from its rgba16float texture */
+  const uint8_t *tag;       /* W*H style tags (the albedo's alpha byte: 255 toon, 128 object, 0), or NULL (all 0) */
 } orc_gbuf;
 
 typedef struct {
@@ -185,6 +186,8 @@ int orc_shadow_render(const orc_scene *s, const float *frame, uint32_t S, float 
 /* shadowTap (frame.ts:35-52): the 'less-equal' comparison of x's biased light depth (bias: frame word 157, layer 1:
  * 158) with the layer x projects into, bilinear over the four texels around it; 1 outside every layer. */
 float orc_sun_tap(const float *frame, const float *map, uint32_t S, const float x[3]);
+/* toonReceive (style.ts:30-42) on c = (c0, c1y, c1z, c1x) as 12 floats: out = (E rgb, band, contrast). */
+void orc_toon_receive(const float c[12], const float n[3], float soft, float out[5]);
 /* The frame's layer count: 2 when shadow.x (word 156) >= 1.5, else 1. */
 uint32_t orc_shadow_layers(const float *frame);
 /* voxSun (voxel.ts:633-671): the sun visibility of every occupied voxel of a built world (after orc_vox_build). */

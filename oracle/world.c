@@ -367,6 +367,51 @@ static v3 eval_sh(const float *sh, const float y[9]) {
 }
 
 /* gatherWorld (rc.ts:880-927), rows [b, e) */
+/* toonReceive (style.ts:30-42): ambient from L0, the dominant direction d from the luminance gradient of L1 and its
+ * directional colour, the direction through a two-band ramp (smoothstep of half width soft, or a step) */
+typedef struct { v3 e; float band, contrast; } toon_recv;
+static toon_recv toon_receive(v3 c0, v3 c1y, v3 c1z, v3 c1x, v3 n, float soft) {
+  const v3 lw = V(0.2126f, 0.7152f, 0.0722f);
+  v3 amb = muls(c0, 0.282095f);
+  v3 g = V(dot(c1x, lw), dot(c1y, lw), dot(c1z, lw));
+  float gl = length3(g);
+  toon_recv out;
+  if (gl < 1e-6f) {
+    out.e = V(fmaxf_(amb.x, 0.0f), fmaxf_(amb.y, 0.0f), fmaxf_(amb.z, 0.0f));
+    out.band = 0.0f; out.contrast = 0.0f;
+    return out;
+  }
+  v3 d = divs(g, gl);
+  v3 s = add(add(muls(c1x, d.x), muls(c1y, d.y)), muls(c1z, d.z));
+  v3 dir = muls(s, 0.488603f);
+  dir = V(fmaxf_(dir.x, 0.0f), fmaxf_(dir.y, 0.0f), fmaxf_(dir.z, 0.0f));
+  float x = dot(n, d), ramp;
+  if (soft > 0.0f) {
+    float t = fminf_(fmaxf_((x - -soft) / (soft - -soft), 0.0f), 1.0f);
+    ramp = t * t * (3.0f - 2.0f * t);
+  } else {
+    ramp = x > 0.0f ? 1.0f : 0.0f;
+  }
+  v3 e = add(sub(amb, dir), muls(muls(dir, 2.0f), ramp));
+  out.e = V(fmaxf_(e.x, 0.0f), fmaxf_(e.y, 0.0f), fmaxf_(e.z, 0.0f));
+  out.band = x > 0.0f ? 1.0f : 0.0f;
+  out.contrast = dot(dir, lw) / fmaxf_(dot(amb, lw), 1e-6f);
+  return out;
+}
+
+/* toonReceive on c = (c0, c1y, c1z, c1x) as 12 floats: out = (E rgb, band, contrast) */
+void orc_toon_receive(const float c[12], const float n[3], float soft, float out[5]) {
+  toon_recv r = toon_receive(V(c[0], c[1], c[2]), V(c[3], c[4], c[5]), V(c[6], c[7], c[8]), V(c[9], c[10], c[11]),
+                             V(n[0], n[1], n[2]), soft);
+  out[0] = r.e.x; out[1] = r.e.y; out[2] = r.e.z; out[3] = r.band; out[4] = r.contrast;
+}
+
+/* shL1 + shAdd (rc.ts:831-840): the L0 and L1 coefficients (basis order 0, y, z, x) of a stored SH, added with
+ * weight w */
+static void sh_l1_add(const float *sh, float w, v3 acc[4]) {
+  for (int k = 0; k < 4; k++) acc[k] = fmas(V(sh[3 * k], sh[3 * k + 1], sh[3 * k + 2]), w, acc[k]);
+}
+
 static void w_gather_range(void *p, uint64_t b, uint64_t e) {
   wjob *j = (wjob *)p;
   const orc_wlayout *wl = j->wl;
@@ -397,6 +442,10 @@ static void w_gather_range(void *p, uint64_t b, uint64_t e) {
       v3 acc = V(0.0f, 0.0f, 0.0f);
       float ws = 0.0f, ww[8];
       uint32_t hidden = 0, qq[8];
+      /* the G-buffer's style tag (rc.ts:881-883): toon pixels also interpolate L0 / L1 */
+      float tagA = g->tag ? (float)g->tag[q] / 255.0f : 0.0f;
+      int toon = tagA > 0.75f;
+      v3 l1[4] = {V(0.0f, 0.0f, 0.0f), V(0.0f, 0.0f, 0.0f), V(0.0f, 0.0f, 0.0f), V(0.0f, 0.0f, 0.0f)};
       for (uint32_t k = 0; k < 8u; k++) {
         i3 oo = corner(k);
         uint32_t qi = lookup(wl, j->ws->keys, j->ws->slot_probe, 0u, key_for(F, I(bb.x + oo.x, bb.y + oo.y, bb.z + oo.z), lod, 0u));
@@ -410,6 +459,7 @@ static void w_gather_range(void *p, uint64_t b, uint64_t e) {
         if (wl->relocate == 2u && seg_occluded(vx, xo1, pp, Lo)) { hidden |= 1u << k; ww[k] = w; qq[k] = qi; continue; }
         acc = fmas(eval_sh(o->sh + 32u * qi, y), w, acc);
         ws += w;
+        if (toon) sh_l1_add(o->sh + 32u * qi, w, l1);
       }
       if (ws <= 0.0f && hidden != 0u) {
         v3 xo2 = add(x, muls(n, 2.0f * vox_size(vx, Lo)));
@@ -419,14 +469,27 @@ static void w_gather_range(void *p, uint64_t b, uint64_t e) {
           if (seg_occluded(vx, xo2, fromf(pr->pos), Lo)) continue;
           acc = fmas(eval_sh(o->sh + 32u * qq[k], y), ww[k], acc);
           ws += ww[k];
+          if (toon) sh_l1_add(o->sh + 32u * qq[k], ww[k], l1);
         }
       }
-      if (ws <= 0.0f && hidden != 0u) __atomic_fetch_add(&o->counts[72 + (px & 7)], 1u, __ATOMIC_RELAXED);
+      if (ws <= 0.0f && hidden != 0u && tagA <= 0.25f) __atomic_fetch_add(&o->counts[72 + (px & 7)], 1u, __ATOMIC_RELAXED);
       v3 r = ws > 0.0f ? divs(acc, ws) : V(0.0f, 0.0f, 0.0f);
+      /* alpha (rc.ts:916-925): 1 photoreal; toon 2 + band + 2 when the directional part is at least a tenth of the
+       * ambient (the receiving operator's irradiance replacing the physical one when style.y > 0.5); other tagged
+       * pixels 2 */
+      float alpha = 1.0f;
+      if (toon && ws > 0.0f) {
+        float iw = 1.0f / ws;
+        toon_recv tr = toon_receive(muls(l1[0], iw), muls(l1[1], iw), muls(l1[2], iw), muls(l1[3], iw), n, F[F_STYLE + 2]);
+        if (F[F_STYLE + 1] > 0.5f) r = tr.e;
+        alpha = 2.0f + tr.band + (tr.contrast >= 0.1f ? 2.0f : 0.0f);
+      } else if (toon || tagA > 0.25f) {
+        alpha = 2.0f;
+      }
       out[0] = out_fmt ? round_store(r.x, 1) : r.x;
       out[1] = out_fmt ? round_store(r.y, 1) : r.y;
       out[2] = out_fmt ? round_store(r.z, 1) : r.z;
-      out[3] = 1.0f;
+      out[3] = out_fmt ? round_store(alpha, 1) : alpha;
     }
 }
 

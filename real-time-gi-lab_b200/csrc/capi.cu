@@ -75,6 +75,7 @@ struct gi_scene {
   uint4 *tri = nullptr;
   gi_material *mats = nullptr;
   uint32_t nverts = 0, ntris = 0, nmats = 0;
+  uint32_t mat_flags = 0;    // OR of the materials' flags (4 toon, 8 object: the G-buffer raster writes style tags)
   // G-buffer raster scratch (gbuffer.cu): two renders of one scene must not overlap on the GPU
   float4 *raster_rec = nullptr;
   uint32_t *raster_ntile = nullptr, *raster_pre = nullptr, *raster_sums = nullptr, *raster_counter = nullptr;
@@ -142,6 +143,7 @@ struct gi_rc {
   float *frame = nullptr;
   float *depth = nullptr;
   uint2 *normal = nullptr;
+  uint8_t *tag = nullptr;            // W*H style tags (zero at creation)
   uint32_t *tile_cnt = nullptr, *tile_fill = nullptr;   // G-buffer raster: per 16 x 16 tile (+1)
   uint32_t ntiles = 0;
   uint64_t mavg_bytes = 0;
@@ -203,6 +205,7 @@ static void free_rc(gi_rc *r) {
   for (cudaEvent_t &e : r->ev)
     if (e) { cudaEventDestroy(e); e = nullptr; }
   cudaFree(r->frame); cudaFree(r->depth); cudaFree(r->normal); cudaFree(r->tile_cnt); cudaFree(r->tile_fill); cudaFree(r->stage);
+  cudaFree(r->tag); cudaFree(r->dev.rsteps); cudaFree(r->dev.rperm); cudaFree(r->dev.rhist);
   cudaFree(r->hits); cudaFree(r->rad_traced); cudaFree(r->rad64); cudaFree(r->sh64); cudaFree(r->irr64);
   cudaFree(r->dev.probes); cudaFree(r->dev.rad); cudaFree(r->dev.sh); cudaFree(r->dev.irr); cudaFree(r->dev.counts);
   cudaFree(r->dev.plevel); cudaFree((void *)r->dev.dirs); cudaFree(r->dev.mavg[0]); cudaFree(r->dev.mavg[1]);
@@ -278,6 +281,7 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
   gi_scene *s = new (std::nothrow) gi_scene;
   if (!s) return fail(GI_ERR_OOM, "gi_scene_upload: host allocation");
   s->ctx = ctx; s->nverts = nverts; s->ntris = ntris; s->nmats = nmats; s->ndraw = ntris; s->raster_tris = ntris;
+  for (uint32_t m = 0; m < nmats; m++) s->mat_flags |= mats[m].flags;
   s->raster_cap = raster_list_cap(ntris);
   cudaError_t e = cudaSuccess;
   float4 *h4 = nullptr;
@@ -787,6 +791,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   uint32_t *counts = nullptr, *plevel = nullptr;
   float4 *dirs = nullptr;
   if ((e = dalloc(&r->frame, 160)) || (e = dalloc(&r->depth, npx)) || (e = dalloc(&r->normal, npx)) ||
+      (e = cudaMalloc(&r->tag, npx)) || (e = cudaMemset(r->tag, 0, npx)) ||
       (e = dalloc(&r->tile_cnt, (size_t)r->ntiles + 1u)) || (e = dalloc(&r->tile_fill, r->ntiles)) ||
       (e = dalloc(&r->stage, npx)) || (e = dalloc(&probes, probe_total)) ||
       (e = cudaMalloc(&rad, ray_total * r->rad_elem_bytes)) || (e = cudaMalloc(&sh, r->sh_elems * r->sh_elem_bytes)) ||
@@ -799,7 +804,7 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   }
   d.probes = probes; d.rad = rad; d.sh = sh; d.irr = irr; d.counts = counts; d.plevel = plevel; d.dirs = dirs;
   d.idirs = dirs + dir_total;
-  d.frame = r->frame; d.depth = r->depth; d.normal = r->normal;
+  d.frame = r->frame; d.depth = r->depth; d.normal = r->normal; d.tag = r->tag;
   // the merge's quad averages of a cascade whose resolution is twice the one below
   size_t avg_elems = 1;
   for (uint32_t i = 1; i < p->cascades && !wp; i++)
@@ -928,6 +933,22 @@ int gi_rc_set_gbuffer_rgb16f(gi_rc *r, const float *depth, const uint16_t *norma
   return GI_OK;
 }
 
+// From the first tagged G-buffer on, the world gather reads the tags (a kernel variant; graphs captured before are
+// refused, as their launches hold the variant without)
+static void use_tags(gi_rc *r) {
+  if (r->dev.tag_any) return;
+  r->dev.tag_any = 1u;
+  r->gen++;
+}
+
+int gi_rc_set_gbuffer_tag(gi_rc *r, const uint8_t *tag, void *stream) {
+  if (!r || !tag) return fail(GI_ERR_INVALID, "gi_rc_set_gbuffer_tag: NULL argument");
+  CK(cudaSetDevice(r->ctx->device), "gi_rc_set_gbuffer_tag: cudaSetDevice");
+  CK(cudaMemcpyAsync(r->tag, tag, (size_t)r->W * r->H, cudaMemcpyHostToDevice, S(stream)), "gi_rc_set_gbuffer_tag: copy");
+  use_tags(r);
+  return GI_OK;
+}
+
 int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   if (!r || !s) return fail(GI_ERR_INVALID, "gi_rc_render_gbuffer: NULL argument");
   if (!r->frame_set) return fail(GI_ERR_STATE, "gi_rc_render_gbuffer: no frame set");
@@ -937,8 +958,9 @@ int gi_rc_render_gbuffer(gi_rc *r, gi_scene *s, void *stream) {
   rd.rec = s->raster_rec; rd.ntile = s->raster_ntile; rd.pre = s->raster_pre; rd.sums = s->raster_sums;
   rd.counter = s->raster_counter; rd.list = s->raster_list; rd.over = s->raster_over;
   rd.tile_cnt = r->tile_cnt; rd.tile_fill = r->tile_fill; rd.list_cap = s->raster_cap; rd.ntiles = r->ntiles;
-  CK(gi_launch_gbuffer(s->raster_dev(), r->frame, r->W, r->H, r->depth, r->normal, rd, r->ctx->sm_count, S(stream)),
+  CK(gi_launch_gbuffer(s->raster_dev(), r->frame, r->W, r->H, r->depth, r->normal, r->tag, rd, r->ctx->sm_count, S(stream)),
      "gi_rc_render_gbuffer: launch");
+  if (s->mat_flags & 12u) use_tags(r);   // toon or object materials: the tags matter
   r->gbuf_set = true;
   return GI_OK;
 }
@@ -1446,13 +1468,31 @@ int gi_rc_set_stats(gi_rc *r, uint32_t level) {
 
 int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
   if (!r || !t) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: NULL argument");
-  if (t->trace_order > 1) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_order %u", t->trace_order);
+  if (t->trace_order > 2) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_order %u", t->trace_order);
+  if (t->trace_order == 2 && r->world)
+    return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_order 2 (walk-length order) is for screen probes");
   if (t->trace_rays != 1 && t->trace_rays != 2 && t->trace_rays != 4)
     return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_rays %u (1, 2 or 4)", t->trace_rays);
   if (t->trace_blocks < 1 || t->trace_blocks > 16) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_blocks %u", t->trace_blocks);
   if (t->gather_shape > 3) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: gather_shape %u", t->gather_shape);
   if (t->merge_threads != 64 && t->merge_threads != 128 && t->merge_threads != 256 && t->merge_threads != 512)
     return fail(GI_ERR_INVALID, "gi_rc_set_tuning: merge_threads %u", t->merge_threads);
+  if (t->trace_order == 2 && !r->dev.rperm) {   // the walk-length order's buffers, on first use
+    CK(cudaSetDevice(r->ctx->device), "gi_rc_set_tuning: cudaSetDevice");
+    const size_t n = r->dev.rays_total;
+    uint8_t *steps = nullptr;
+    uint32_t *perm = nullptr, *hist = nullptr;
+    cudaError_t e;
+    if ((e = cudaMalloc(&steps, n)) || (e = cudaMemset(steps, 0, n)) || (e = cudaMalloc(&perm, n * 4u)) ||
+        (e = cudaMalloc(&hist, 256u * 4u)) || (e = cudaMemset(hist, 0, 256u * 4u)) ||
+        (e = gi_launch_iota(perm, (uint32_t)n, nullptr)) || (e = cudaDeviceSynchronize())) {
+      cudaFree(steps); cudaFree(perm); cudaFree(hist);
+      return cuda_fail(e, "gi_rc_set_tuning: walk-length order buffers");
+    }
+    r->dev.rsteps = steps; r->dev.rperm = perm; r->dev.rhist = hist;
+    r->gen++;   // graphs captured before launch the other trace
+  }
+  if ((t->trace_order == 2) != (r->dev.trace_order == 2)) r->gen++;
   r->dev.trace_order = t->trace_order;
   r->dev.trace_rays = t->trace_rays;
   r->launch.trace_blocks = t->trace_blocks;
@@ -1516,6 +1556,7 @@ int gi_rc_buffer_bytes(gi_rc *r, int what, size_t *bytes) {
     case GI_RC_SH: *bytes = r->sh_elems * r->sh_elem_bytes; break;
     case GI_RC_DEPTH: *bytes = npx * 4u; break;
     case GI_RC_NORMAL: *bytes = npx * 8u; break;
+    case GI_RC_TAG: *bytes = npx; break;
     case GI_RC_HITS: *bytes = (size_t)r->dev.rays_total * 16u; break;
     case GI_RC_SHADOW: *bytes = (size_t)r->shadow_size * r->shadow_size * 4u * r->shadow_layers; break;
     case GI_RC_BOUNCE_VOL: *bytes = r->bounce ? 2u * (size_t)r->bn.dx * r->bn.dy * (6u * r->bn.dz + 1u) * 8u : 0u; break;
@@ -1542,6 +1583,7 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
     case GI_RC_SH: src = r->dev.sh; break;
     case GI_RC_DEPTH: src = r->depth; break;
     case GI_RC_NORMAL: src = r->normal; break;
+    case GI_RC_TAG: src = r->tag; break;
     case GI_RC_HITS: src = r->hits; break;
     case GI_RC_RAD_TRACED: src = r->rad_traced; break;
     case GI_RC_SHADOW: src = r->shadow; break;

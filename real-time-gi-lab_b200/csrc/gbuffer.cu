@@ -254,7 +254,8 @@ __device__ __forceinline__ uint32_t block_min_256(uint32_t x, uint32_t *ws) {
 // One block per tile: the tile's list, then the overflow list, in chunks of 256 sorted by depth bound (largest
 // first); then the winner's depth and normal
 __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
-                                                  uint32_t tiles_x, RasterDev rd, float *depth, uint2 *normal) {
+                                                  uint32_t tiles_x, RasterDev rd, float *depth, uint2 *normal,
+                                                  uint8_t *tag) {
   grid_dep_wait();
   __shared__ float4 sa[256], se1[256], se2[256];
   __shared__ uint32_t skey[256], sval[256];
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__res
   }
   if (!inside) return;
   size_t q = (size_t)y * W + x;
-  if (best == 0ull) { depth[q] = 0.0f; normal[q] = make_uint2(0u, 0u); return; }
+  if (best == 0ull) { depth[q] = 0.0f; normal[q] = make_uint2(0u, 0u); tag[q] = 0u; return; }
   uint32_t t = 0xffffffffu - (uint32_t)(best & 0xffffffffull);
   depth[q] = __uint_as_float((uint32_t)(best >> 32));
   float4 a4 = rd.rec[3u * t], e14 = rd.rec[3u * t + 1u], e24 = rd.rec[3u * t + 2u];
@@ -333,6 +334,9 @@ __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__res
   float flip = dot(cross(e1, e2), eye - a) > 0.0f ? 1.0f : -1.0f;
   nn = normalize3(nn) * flip;
   normal[q] = make_uint2((uint32_t)f2h(nn.x) | ((uint32_t)f2h(nn.y) << 16), (uint32_t)f2h(nn.z));
+  // the albedo's alpha (gbuffer.ts:2): 1 toon, 0.5 another measured object, 0 photoreal, as an 8-bit unorm
+  const uint32_t fl = s.mats[idx.w].flags;
+  tag[q] = (fl & 4u) ? 255u : ((fl & 8u) ? 128u : 0u);
 }
 
 }  // namespace gi
@@ -342,7 +346,7 @@ using namespace gi;
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H) { return ((W + RT - 1u) / RT) * ((H + RT - 1u) / RT); }
 
 cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
-                              uint2 *normal, const RasterDev &rd, uint32_t sm_count, cudaStream_t st) {
+                              uint2 *normal, uint8_t *tag, const RasterDev &rd, uint32_t sm_count, cudaStream_t st) {
   uint32_t tiles_x = (W + RT - 1u) / RT;
   uint32_t nblk = s.ntris ? (s.ntris + 255u) / 256u : 1u;
   GI_TRY(gi_launch(k_rs_setup, nblk, 256, st, s, frame_dev, W, H, rd));
@@ -350,6 +354,6 @@ cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_
   if (s.ntris) GI_TRY(gi_launch(k_rs_bin<false>, sm_count * 8u, 256, st, s.ntris, tiles_x, rd));
   GI_TRY(gi_launch(k_rs_tile_scan, 1, 1024, st, rd));
   if (s.ntris) GI_TRY(gi_launch(k_rs_bin<true>, sm_count * 8u, 256, st, s.ntris, tiles_x, rd));
-  GI_TRY(gi_launch(k_rs_tiles, rd.ntiles, 256, st, s, frame_dev, W, H, tiles_x, rd, depth, normal));
+  GI_TRY(gi_launch(k_rs_tiles, rd.ntiles, 256, st, s, frame_dev, W, H, tiles_x, rd, depth, normal, tag));
   return cudaGetLastError();
 }

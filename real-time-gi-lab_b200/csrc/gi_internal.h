@@ -29,12 +29,17 @@ struct RcDev {
   CascDev c[8];
   float vox_scale, vox_offset, level_map, vox_skip;
   uint32_t dda_cap, stats, probes_total, rays_total;
-  uint32_t trace_order, trace_rays;   // tuning of k_trace (gi_rc_tuning)
+  uint32_t trace_order, trace_rays;   // tuning of k_trace (gi_rc_tuning; trace_order 2: walk-length order)
   uint32_t f32_out;                   // SH and irradiance stored as f32 whatever the atlas
   uint32_t irr_f16;                   // irradiance stored as rgba16f whatever the atlas and f32_out
+  uint32_t tag_any, pad_tag;          // nonzero once a G-buffer with style tags was set or drawn (world gather)
   const float *frame;      // 160 words (packFrame)
   const float *depth;      // W*H
   const uint2 *normal;     // W*H rgba16f
+  const uint8_t *tag;      // W*H: the G-buffer albedo's alpha byte (style tag: 255 toon, 128 object, 0 photoreal)
+  uint8_t *rsteps;         // trace_order 2: per atlas element the key of its last walk (steps, hit); null otherwise
+  uint32_t *rperm;         // trace_order 2: the trace order (atlas indices by descending key)
+  uint32_t *rhist;         // trace_order 2: 128 key counts, then 128 scatter cursors
   ProbeDev *probes;
   uint32_t *plevel;        // per probe: voxLevel(s0, c) (rc.ts:210-213), computed once by setupScreen
   const float4 *dirs;      // per cascade, res^2 texel directions dirOf(di, res) (rc.ts:308), computed at creation
@@ -216,9 +221,10 @@ cudaError_t gi_launch_rc_solve(const gi::RcDev &r, const gi::VoxDev &v, uint32_t
                                const gi::WorldDev *w = nullptr);
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H);
 cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,
-                              uint2 *normal, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);
+                              uint2 *normal, uint8_t *tag, const gi::RasterDev &rd, uint32_t sm_count, cudaStream_t st);
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_normal_rgb_to_rgba(const uint16_t *src, uint2 *dst, uint32_t n, cudaStream_t st);
+cudaError_t gi_launch_iota(uint32_t *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);
 // FP64 reference of merge + SH + gather from the f32 traced atlas: rad64 rays_total x 4 doubles, sh64 27 doubles per

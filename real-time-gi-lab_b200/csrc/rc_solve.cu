@@ -469,11 +469,15 @@ __device__ __forceinline__ void setup_probe(const RcDev &r, const VoxDev &v, uin
   r.plevel[i] = pr.pos.w > 0.0f ? vox_level(v, r, pr.pos.w, c) : 0u;
 }
 
+constexpr uint32_t RS_KEYS = 128, RS_PER_BLOCK = 1024;   // walk-length order: keys, rays per scatter block
+
 // every cascade in one launch
 __global__ void k_setup_screen(RcDev r, VoxDev v) {
   grid_dep_wait();
-  // the 80 counter words and the trace's ray counter start at zero (words below `cascades` are set by the probes)
+  // the 80 counter words and the trace's ray counter start at zero (words below `cascades` are set by the probes);
+  // the walk-length order's key counts and cursors too
   if (blockIdx.x == 0 && threadIdx.x < 81u && threadIdx.x >= r.cascades) r.counts[threadIdx.x] = 0u;
+  if (blockIdx.x == 0 && r.rhist && threadIdx.x < 2u * RS_KEYS) r.rhist[threadIdx.x] = 0u;
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < r.probes_total) setup_probe(r, v, i);
 }
@@ -481,7 +485,8 @@ __global__ void k_setup_screen(RcDev r, VoxDev v) {
 // trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) of the ray at position j of the trace order (cascade c): writes
 // its atlas element (and the debug copies); true when its probe is valid and the ray was marched.
 template <int A, bool DYN = false>
-__device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, TraceOut &out) {
+__device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint32_t j, uint32_t c, TraceOut &out,
+                                          bool probe_major) {
   typedef typename Atlas<A>::T T;
   T *rad = reinterpret_cast<T *>(r.rad);
   const float *F = r.frame;
@@ -490,7 +495,7 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
   bool traced = false;
   const CascDev &L = r.c[c];
   uint32_t t = j - L.ray_off, pi, di;
-  if (r.trace_order == 0) {           // probe-major: the atlas order
+  if (probe_major) {                  // probe-major: the atlas order
     pi = t >> L.dirs_log2;
     di = t & ((1u << L.dirs_log2) - 1u);
   } else {                            // direction-major: one direction over consecutive probes
@@ -519,8 +524,64 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
   return traced;
 }
 
-// Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time.
-template <int A, bool DYN>
+// Walk-length order (trace_order 2, screen probes): the rays are handed out by the previous solve's DDA step count and
+// hit, longest walks first, so a warp's lanes walk about as long as each other and the persistent queue ends on short
+// rays.  Each ray's result does not depend on which lane traces it or when.  A ray's key: its step count (exact below
+// 48, then in 16-step groups up to 63) x 2 + hit; k_trace stores it per atlas element, the next solve counts the keys
+// (k_rsort_hist) and scatters the atlas indices by key (k_rsort_scatter) before its trace.
+__device__ __forceinline__ uint32_t rsort_key(uint32_t steps, bool hit) {
+  const uint32_t s = steps < 48u ? steps : min(48u + ((steps - 48u) >> 4), 63u);
+  return s * 2u + (hit ? 1u : 0u);
+}
+
+// per-key ray counts of the stored keys (rhist[0 .. 127], zeroed by the setup with the cursors after them)
+__global__ void __launch_bounds__(256) k_rsort_hist(RcDev r) {
+  grid_dep_wait();
+  __shared__ uint32_t h[RS_KEYS];
+  if (threadIdx.x < RS_KEYS) h[threadIdx.x] = 0u;
+  __syncthreads();
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < r.rays_total; i += gridDim.x * blockDim.x)
+    atomicAdd(&h[r.rsteps[i]], 1u);
+  __syncthreads();
+  if (threadIdx.x < RS_KEYS && h[threadIdx.x]) atomicAdd(&r.rhist[threadIdx.x], h[threadIdx.x]);
+}
+
+// the trace order: atlas indices by descending key; a block ranks its 1024 rays per key in shared memory and reserves
+// each key's range with one atomic (the order inside a key is whatever the blocks' reservations give)
+__global__ void __launch_bounds__(256) k_rsort_scatter(RcDev r) {
+  grid_dep_wait();
+  __shared__ uint32_t cnt[RS_KEYS], start[RS_KEYS], base[RS_KEYS];
+  if (threadIdx.x < RS_KEYS) { cnt[threadIdx.x] = 0u; start[threadIdx.x] = r.rhist[threadIdx.x]; }
+  __syncthreads();
+  if (threadIdx.x == 0) {   // rays with larger keys come first
+    uint32_t a = 0;
+    for (int k = (int)RS_KEYS - 1; k >= 0; k--) { const uint32_t n = start[k]; start[k] = a; a += n; }
+  }
+  const uint32_t b0 = blockIdx.x * RS_PER_BLOCK;
+  uint32_t key[4], rank[4];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t i = b0 + (uint32_t)k * 256u + threadIdx.x;
+    key[k] = i < r.rays_total ? (uint32_t)r.rsteps[i] : RS_KEYS;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; k++) rank[k] = key[k] < RS_KEYS ? atomicAdd(&cnt[key[k]], 1u) : 0u;
+  __syncthreads();
+  if (threadIdx.x < RS_KEYS && cnt[threadIdx.x])
+    base[threadIdx.x] = start[threadIdx.x] + atomicAdd(&r.rhist[RS_KEYS + threadIdx.x], cnt[threadIdx.x]);
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (key[k] >= RS_KEYS) continue;
+    const uint32_t pos = base[key[k]] + rank[k];
+    if (pos < r.rays_total) r.rperm[pos] = b0 + (uint32_t)k * 256u + threadIdx.x;
+  }
+}
+
+// Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time.  SORT: positions go through the
+// walk-length order (rperm) and each ray's key is stored for the next solve.
+template <int A, bool DYN, bool SORT>
 __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
   grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
@@ -535,10 +596,12 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
    for (uint32_t k = 0; k < r.trace_rays; k++) {
     uint32_t j = base + k * 32u + lane;   // position in the trace order
     bool live = j < r.rays_total;
+    if (SORT && live) j = r.rperm[j];     // the atlas element at that position
     uint32_t c = live ? casc_of_ray(r, j) : 0u;
     TraceOut out;
     out.steps = 0;
-    bool traced = live && trace_ray<A, DYN>(r, v, j, c, out);
+    bool traced = live && trace_ray<A, DYN>(r, v, j, c, out, SORT || r.trace_order == 0u);
+    if (SORT && live) r.rsteps[j] = (uint8_t)rsort_key(traced ? out.steps : 0u, traced && out.T < 0.5f);
     if (r.stats) {
       // per-cascade counters (rc.ts:232-235); flush when the lane's cascade changes
       if (live && traced) {
@@ -1081,7 +1144,7 @@ __global__ void __launch_bounds__(256) k_trace_batch(BatchDev B) {
     const uint32_t j = base - B.ray_pre[s] + lane;
     if (j < r.rays_total) {
       TraceOut out;
-      trace_ray<A>(r, B.vox[s], j, casc_of_ray(r, j), out);
+      trace_ray<A>(r, B.vox[s], j, casc_of_ray(r, j), out, r.trace_order != 1u);
     }
   }
 }
@@ -1180,8 +1243,16 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);
   // the dynamic layer's read is compiled into a kernel of its own: without a layer the trace keeps its registers
-  if (r.dyn_hdr) GI_TRY(gi_launch(k_trace<A, true>, tb, 256, st, r, v, counter));
-  else GI_TRY(gi_launch(k_trace<A, false>, tb, 256, st, r, v, counter));
+  if (r.trace_order == 2u && r.rperm) {   // walk-length order from the previous solve's keys
+    GI_TRY(gi_launch(k_rsort_hist, min((r.rays_total + 1023u) / 1024u, sm_count * 8u), 256, st, r));
+    GI_TRY(gi_launch(k_rsort_scatter, (r.rays_total + RS_PER_BLOCK - 1u) / RS_PER_BLOCK, 256, st, r));
+    if (r.dyn_hdr) GI_TRY(gi_launch(k_trace<A, true, true>, tb, 256, st, r, v, counter));
+    else GI_TRY(gi_launch(k_trace<A, false, true>, tb, 256, st, r, v, counter));
+  } else if (r.dyn_hdr) {
+    GI_TRY(gi_launch(k_trace<A, true, false>, tb, 256, st, r, v, counter));
+  } else {
+    GI_TRY(gi_launch(k_trace<A, false, false>, tb, 256, st, r, v, counter));
+  }
   if (ev) cudaEventRecord(ev[2], st);
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
@@ -1258,6 +1329,15 @@ cudaError_t gi_launch_init_dirs(const RcDev &r, float4 *dirs, uint32_t ndirs, cu
 
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st) {
   k_normal_f32_to_f16<<<256, 256, 0, st>>>(src, dst, n);
+  return cudaGetLastError();
+}
+
+__global__ void k_iota(uint32_t *dst, uint32_t n) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) dst[i] = i;
+}
+
+cudaError_t gi_launch_iota(uint32_t *dst, uint32_t n, cudaStream_t st) {
+  k_iota<<<1184, 256, 0, st>>>(dst, n);
   return cudaGetLastError();
 }
 

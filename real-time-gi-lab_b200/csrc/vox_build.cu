@@ -341,16 +341,11 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
 __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t t, uint32_t L,
                                              i3 c, bool single, uint32_t brick_overflow) {
   if (finer_built(v, L, c, brick_overflow)) return;
-#if GI_VB_EARLYPTR
-  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the test
-#endif
+  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the box test
   float vs = vox_size(v, L);
   f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
   float hh = 0.5f * vs * 1.0001f;
   if (!single && !tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return;
-#if !GI_VB_EARLYPTR
-  uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
-#endif
   if (ptr >= GI_MARK) return;
   uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
   // surfaceAt's alpha test (voxel.ts:325-332): untextured, so the sampled alpha is the factor's
@@ -444,16 +439,11 @@ __global__ void __launch_bounds__(256) k_chunks(VoxDev v, SceneDev s) {
 __device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t L, i3 c,
                                             uint32_t brick_overflow, uint32_t &wi, uint32_t &msk, uint32_t &ri) {
   if (finer_built(v, L, c, brick_overflow)) return false;
-#if GI_VB_EARLYPTR
-  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the test
-#endif
+  const uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];   // in flight during the box test
   float vs = vox_size(v, L);
   f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
   float hh = 0.5f * vs * 1.0001f;
   if (!tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return false;
-#if !GI_VB_EARLYPTR
-  uint32_t ptr = v.ptr[ptr_index(v, L, mki(c.x >> 3, c.y >> 3, c.z >> 3))];
-#endif
   if (ptr >= GI_MARK) return false;
   const gi_material &m = s.mats[T.idx.w];
   if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;

@@ -674,10 +674,52 @@ __device__ __forceinline__ f3 w_eval_sh(const RcDev &r, uint32_t qi, const float
   return vmax(es, mk(0.0f, 0.0f, 0.0f));
 }
 
+// The L0 and L1 coefficients (basis order 0, y, z, x) of a probe's stored SH, added with weight wt (shL1 + shAdd,
+// rc.ts:831-840)
+template <int A>
+__device__ __forceinline__ void w_sh_l1_add(const RcDev &r, uint32_t qi, float wt, f3 &c0, f3 &cy, f3 &cz, f3 &cx) {
+  const float4 a = sh_load<A>(r, (size_t)qi * 8u), b = sh_load<A>(r, (size_t)qi * 8u + 1u),
+               c = sh_load<A>(r, (size_t)qi * 8u + 2u);
+  c0 = fma3(mk(a.x, a.y, a.z), wt, c0);
+  cy = fma3(mk(a.w, b.x, b.y), wt, cy);
+  cz = fma3(mk(b.z, b.w, c.x), wt, cz);
+  cx = fma3(mk(c.y, c.z, c.w), wt, cx);
+}
+
+// toonReceive (style.ts:30-42): from L0 an ambient colour, from the luminance gradient of L1 a dominant direction d
+// and its directional colour, the direction put through a two-band ramp (smoothstep of half width soft, or a step):
+// E = max(amb - dir + 2 dir ramp(n . d), 0); band = n . d > 0; contrast = lum(dir) / max(lum(amb), 1e-6)
+struct ToonRecv { f3 e; float band, contrast; };
+__device__ __forceinline__ ToonRecv toon_receive(f3 c0, f3 c1y, f3 c1z, f3 c1x, f3 n, float soft) {
+  const f3 lw = mk(0.2126f, 0.7152f, 0.0722f);
+  const f3 amb = c0 * 0.282095f;
+  const f3 g = mk(dot(c1x, lw), dot(c1y, lw), dot(c1z, lw));
+  const float gl = length3(g);
+  ToonRecv out;
+  if (gl < 1e-6f) { out.e = vmax(amb, mk(0.0f, 0.0f, 0.0f)); out.band = 0.0f; out.contrast = 0.0f; return out; }
+  const f3 d = g / gl;
+  const f3 dir = vmax(((c1x * d.x + c1y * d.y) + c1z * d.z) * 0.488603f, mk(0.0f, 0.0f, 0.0f));
+  const float x = dot(n, d);
+  float ramp;
+  if (soft > 0.0f) {
+    const float t = fclampf((x - -soft) / (soft - -soft), 0.0f, 1.0f);
+    ramp = t * t * (3.0f - 2.0f * t);
+  } else {
+    ramp = x > 0.0f ? 1.0f : 0.0f;
+  }
+  out.e = vmax((amb - dir) + (dir * 2.0f) * ramp, mk(0.0f, 0.0f, 0.0f));
+  out.band = x > 0.0f ? 1.0f : 0.0f;
+  out.contrast = dot(dir, lw) / mx(dot(amb, lw), 1e-6f);
+  return out;
+}
+
 // gatherWorld (rc.ts:880-927), one thread per pixel: the eight c0 probes of the pixel's grid cell, weighted
 // trilinearly and by the side of the surface they are on; with relocate 'voxel' the probes voxels hide are skipped
-// (retested from two voxels out when every probe is hidden).  Pixels left black count in words 72-79.
-template <int A>
+// (retested from two voxels out when every probe is hidden).  Photoreal pixels left black count in words 72-79.
+// TAG (once the G-buffer carries style tags): toon pixels (tag > 0.75) also interpolate the L0/L1 coefficients and
+// go through the receiving operator (the irradiance replaced when the frame's style.y > 0.5), alpha 2 + band + 2 when
+// the directional part is at least a tenth of the ambient; other tagged pixels (tag > 0.25) get alpha 2.
+template <int A, bool TAG>
 __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w) {
   grid_dep_wait();
   // a warp takes a 4 x 8 tile of the block's 16 x 16 pixels (neighbouring pixels share probes and segment lengths;
@@ -709,6 +751,9 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
     float ws = 0.0f, ww[8];
     uint32_t hidden = 0, qq[8];
     const bool vrel = w.relocate == 2u;
+    const float tagA = TAG ? r.unorm8[r.tag[q]] : 0.0f;
+    const bool toon = TAG && tagA > 0.75f;
+    f3 l0 = mk(0.0f, 0.0f, 0.0f), ly = l0, lz = l0, lx = l0;   // toon pixels: the L0 / L1 sums
     for (uint32_t k = 0; k < 8u; k++) {
       const i3 o = w_corner(k);
       const uint32_t qi = w_lookup(w, 0u, w_key_at(mki(bb.x + o.x, bb.y + o.y, bb.z + o.z), org0, lod));
@@ -721,6 +766,7 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
       if (vrel && w_seg_occluded(v, xo1, pp, Lo)) { hidden |= 1u << k; ww[k] = wt; qq[k] = qi; continue; }
       e = fma3(w_eval_sh<A>(r, qi, y), wt, e);
       ws += wt;
+      if (toon) w_sh_l1_add<A>(r, qi, wt, l0, ly, lz, lx);
     }
     if (ws <= 0.0f && hidden != 0u) {
       const f3 xo2 = x + n * (2.0f * vox_size(v, Lo));
@@ -729,10 +775,21 @@ __global__ void __launch_bounds__(256) k_w_gather(RcDev r, VoxDev v, WorldDev w)
         if (w_seg_occluded(v, xo2, ld3(r.probes[r.c[0].probe_off + qq[k]].pos), Lo)) continue;
         e = fma3(w_eval_sh<A>(r, qq[k], y), ww[k], e);
         ws += ww[k];
+        if (toon) w_sh_l1_add<A>(r, qq[k], ww[k], l0, ly, lz, lx);
       }
     }
-    black = ws <= 0.0f && hidden != 0u;
+    black = ws <= 0.0f && hidden != 0u && tagA <= 0.25f;
     if (ws > 0.0f) res = e / ws;
+    if (TAG) {
+      if (toon && ws > 0.0f) {
+        const float iw = 1.0f / ws;
+        const ToonRecv tr = toon_receive(l0 * iw, ly * iw, lz * iw, lx * iw, n, F[F_STYLE + 2]);
+        if (F[F_STYLE + 1] > 0.5f) res = tr.e;
+        alpha = 2.0f + tr.band + (tr.contrast >= 0.1f ? 2.0f : 0.0f);
+      } else if (toon || tagA > 0.25f) {
+        alpha = 2.0f;
+      }
+    }
   }
   // black pixels: one atomic per counter word among the warp's lanes
   const unsigned act = __activemask();
@@ -790,7 +847,8 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
     GI_TRY(gi_launch(k_w_merge<A>, blocks((uint64_t)w.cap[c] << r.c[c].dirs_log2), 256, st, r, w, (uint32_t)c));
   GI_TRY(gi_launch(k_w_project_sh<A>, blocks(w.cap[0]), 256, st, r, w));
   if (ev) cudaEventRecord(ev[3], st);
-  GI_TRY(gi_launch(k_w_gather<A>, dim3((r.width + 15u) / 16u, (r.height + 15u) / 16u), 256, st, r, v, w));
+  if (r.tag_any) GI_TRY(gi_launch(k_w_gather<A, true>, dim3((r.width + 15u) / 16u, (r.height + 15u) / 16u), 256, st, r, v, w));
+  else GI_TRY(gi_launch(k_w_gather<A, false>, dim3((r.width + 15u) / 16u, (r.height + 15u) / 16u), 256, st, r, v, w));
   if (ev) cudaEventRecord(ev[4], st);
   return cudaGetLastError();
 }

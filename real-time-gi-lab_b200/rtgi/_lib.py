@@ -12,7 +12,8 @@ LIB_PATH = os.path.join(PKG, "lib", "libgi_b200.so")
 GI_OK, GI_ERR_INVALID, GI_ERR_OOM, GI_ERR_CUDA, GI_ERR_TIMEOUT, GI_ERR_OVERFLOW, GI_ERR_STATE = 0, -1, -2, -3, -4, -5, -6
 GI_ATLAS_F32, GI_ATLAS_F16, GI_ATLAS_BF16 = 0, 1, 2
 (GI_RC_PROBES, GI_RC_RAD, GI_RC_SH, GI_RC_DEPTH, GI_RC_NORMAL, GI_RC_HITS, GI_RC_RAD_TRACED, GI_RC_SHADOW, GI_RC_BOUNCE_VOL,
- GI_RC_BOUNCE_INJ, GI_RC_BOUNCE_LIST, GI_RC_WORLD_KEYS, GI_RC_WORLD_SLOTS, GI_RC_WORLD_PARENTS, GI_RC_WORLD_STATE) = range(15)
+ GI_RC_BOUNCE_INJ, GI_RC_BOUNCE_LIST, GI_RC_WORLD_KEYS, GI_RC_WORLD_SLOTS, GI_RC_WORLD_PARENTS, GI_RC_WORLD_STATE,
+ GI_RC_TAG) = range(16)
 GI_RELOCATE_GBUFFER, GI_RELOCATE_NONE, GI_RELOCATE_VOXEL = 0, 1, 2
 
 # Every symbol include/gi.h declares, with its ctypes signature (restype, argtypes).
@@ -48,6 +49,7 @@ SIGNATURES = {
     "gi_rc_set_gbuffer": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_set_gbuffer_f16": (C.c_int, [_P, _P, _P, _P]),
     "gi_rc_set_gbuffer_rgb16f": (C.c_int, [_P, _P, _P, _P]),
+    "gi_rc_set_gbuffer_tag": (C.c_int, [_P, _P, _P]),
     "gi_rc_render_gbuffer": (C.c_int, [_P, _P, _P]),
     "gi_rc_render_shadow": (C.c_int, [_P, _P, C.c_uint32, _P]),
     "gi_rc_set_bounce": (C.c_int, [_P, _P, _P]),

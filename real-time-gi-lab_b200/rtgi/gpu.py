@@ -342,6 +342,13 @@ class Rc:
         wide = (self.params.atlas == "f32" or self.params.f32Out) and not self.params.irr16
         return self.width * self.height * (16 if wide else 8)
 
+    def set_gbuffer_tag(self, tag: np.ndarray, stream=None):
+        """The G-buffer's style tags (H x W bytes, the albedo's alpha: 255 toon, 128 object, 0 photoreal)."""
+        tag = np.ascontiguousarray(tag, dtype=np.uint8)
+        if tag.size != self.width * self.height:
+            raise _lib.GiError(_lib.GI_ERR_INVALID, f"tag of {tag.size} bytes for {self.width}x{self.height}")
+        _lib.call("gi_rc_set_gbuffer_tag", self.handle, _ptr(tag), _stream(stream))
+
     def set_gbuffer_ptrs(self, depth_ptr: int, normal_f16_ptr: int, stream=None, rgb: bool = False):
         """G-buffer from host pointers (pinned memory makes the copies asynchronous); rgb: the normals as three
         halves per pixel (gi_rc_set_gbuffer_rgb16f) instead of four."""

@@ -178,3 +178,48 @@ def test_world_with_bounce(ctx):
     finally:
         for h in (rc, vw, sg):
             h.destroy()
+
+
+@pytest.mark.parametrize("soft", [0.0, 0.25])
+def test_world_toon_receiving_operator(ctx, soft):
+    """The room with every other box toon (flag 4) and one box flagged as a measured object (flag 8), world probes:
+    the G-buffer raster's style tags equal the oracle's (from the materials of the pixels' triangles), and the gather
+    applies the receiving operator to toon pixels (rc.ts:877-926) bit for bit with the oracle, for a hard and a soft
+    ramp; the tags reach the output alpha (2 + band + 2 contrast for toon, 2 for objects)."""
+    base = gi_cases.toon()
+    mats = list(base.scene.materials)
+    k = next(i for i, m in enumerate(mats) if m.name.startswith("box") and not (m.flags & scenes.FLAG_TOON))
+    mats[k] = dataclasses.replace(mats[k], flags=mats[k].flags | 8)
+    scene = dataclasses.replace(base.scene, materials=mats)
+    case = _case("room-toon", scene, 200, 150, "world-24-voxel-rc2-f32", ROOM_VOX, [8192, 4096, 2048, 1024, 512])
+    case.frame = case.frame.copy()
+    case.frame[136:139] = [1.0, 1.0, soft]
+    sg = gpu.SceneGpu(ctx, case.scene)
+    vw = gpu.VoxWorld(sg, case.vox)
+    rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    try:
+        rc.set_frame(case.frame)
+        rc.render_gbuffer(sg)
+        vw.update(case.scene.camera.eye)
+        rc.solve(vw)
+        g_irr, g_tag = rc.read_irradiance(), rc.read_buffer(_lib.GI_RC_TAG).reshape(case.height, case.width)
+        g_counts = rc.read_counts()
+        depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width)
+        normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4).astype(np.float32)
+    finally:
+        for h in (rc, vw, sg):
+            h.destroy()
+    _, _, tri = bind.raster_gbuffer(case.scene, case.frame, case.width, case.height)
+    tag = bind.gbuffer_tags(case.scene, tri)
+    _eq(g_tag, tag, "style tags")
+    assert (tag == 255).any() and (tag == 128).any() and (tag == 0).any()
+    v = case.vox
+    st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, case.scene.camera.eye)
+    lay = configs.world_layout(case.rc)
+    o = bind.world_solve(st, lay, bind.WorldState(lay), case.frame, depth, normal, tag=tag)
+    _eq(g_counts, o["counts"], "counts")
+    _eq(g_irr, o["irr"], "irradiance")
+    alpha = g_irr[..., 3]
+    assert (alpha[tag == 128] == 2.0).all()
+    assert np.isin(alpha[(tag == 255) & (depth > 0)], [2.0, 3.0, 4.0, 5.0]).all()
+    assert (alpha[(tag == 255) & (depth > 0)] >= 3.0).any()
