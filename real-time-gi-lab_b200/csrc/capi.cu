@@ -877,8 +877,23 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   return GI_OK;
 }
 
+static cudaError_t alloc_walk_order(gi_rc *r);
+
+// Screen probes trace in walk-length order by default (trace_order 2, two rays per lane per fetch)
 int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_rc **out) {
-  return rc_create(ctx, p, nullptr, W, H, out);
+  const int st = rc_create(ctx, p, nullptr, W, H, out);
+  if (st != GI_OK) return st;
+  gi_rc *r = *out;
+  const cudaError_t e = alloc_walk_order(r);
+  if (e != cudaSuccess) {
+    gi_rc_destroy(r);
+    *out = nullptr;
+    return cuda_fail(e, "gi_rc_create: walk-length order buffers");
+  }
+  r->dev.trace_order = 2u;
+  r->dev.trace_rays = 2u;
+  r->bytes += 5u * (uint64_t)r->dev.rays_total + 1024u;
+  return GI_OK;
 }
 
 int gi_rc_create_world(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *world, uint32_t W, uint32_t H,
@@ -1466,6 +1481,24 @@ int gi_rc_set_stats(gi_rc *r, uint32_t level) {
   return GI_OK;
 }
 
+// The walk-length order's buffers (trace_order 2): a key per ray (zero: the first solve's order is the keys' initial
+// one), the order (the identity until the first scatter), the key counts and cursors
+static cudaError_t alloc_walk_order(gi_rc *r) {
+  const size_t n = r->dev.rays_total;
+  uint8_t *steps = nullptr;
+  uint32_t *perm = nullptr, *hist = nullptr;
+  cudaError_t e;
+  if ((e = cudaMalloc(&steps, n ? n : 1u)) || (e = cudaMemset(steps, 0, n ? n : 1u)) ||
+      (e = cudaMalloc(&perm, (n ? n : 1u) * 4u)) || (e = cudaMalloc(&hist, 256u * 4u)) ||
+      (e = cudaMemset(hist, 0, 256u * 4u)) || (e = gi_launch_iota(perm, (uint32_t)n, nullptr)) ||
+      (e = cudaDeviceSynchronize())) {
+    cudaFree(steps); cudaFree(perm); cudaFree(hist);
+    return e;
+  }
+  r->dev.rsteps = steps; r->dev.rperm = perm; r->dev.rhist = hist;
+  return cudaSuccess;
+}
+
 int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
   if (!r || !t) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: NULL argument");
   if (t->trace_order > 2) return fail(GI_ERR_INVALID, "gi_rc_set_tuning: trace_order %u", t->trace_order);
@@ -1479,17 +1512,7 @@ int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
     return fail(GI_ERR_INVALID, "gi_rc_set_tuning: merge_threads %u", t->merge_threads);
   if (t->trace_order == 2 && !r->dev.rperm) {   // the walk-length order's buffers, on first use
     CK(cudaSetDevice(r->ctx->device), "gi_rc_set_tuning: cudaSetDevice");
-    const size_t n = r->dev.rays_total;
-    uint8_t *steps = nullptr;
-    uint32_t *perm = nullptr, *hist = nullptr;
-    cudaError_t e;
-    if ((e = cudaMalloc(&steps, n)) || (e = cudaMemset(steps, 0, n)) || (e = cudaMalloc(&perm, n * 4u)) ||
-        (e = cudaMalloc(&hist, 256u * 4u)) || (e = cudaMemset(hist, 0, 256u * 4u)) ||
-        (e = gi_launch_iota(perm, (uint32_t)n, nullptr)) || (e = cudaDeviceSynchronize())) {
-      cudaFree(steps); cudaFree(perm); cudaFree(hist);
-      return cuda_fail(e, "gi_rc_set_tuning: walk-length order buffers");
-    }
-    r->dev.rsteps = steps; r->dev.rperm = perm; r->dev.rhist = hist;
+    CK(alloc_walk_order(r), "gi_rc_set_tuning: walk-length order buffers");
     r->gen++;   // graphs captured before launch the other trace
   }
   if ((t->trace_order == 2) != (r->dev.trace_order == 2)) r->gen++;

@@ -212,3 +212,43 @@ def test_irr16_is_the_rounded_f32_solve(ctx):
     w = w_raw.view(np.float32)
     assert (w > 0.0).any()
     assert np.array_equal(w.astype(np.float16).view(np.uint16), n_raw.view(np.uint16))
+
+
+def test_walk_length_order_parity(ctx):
+    """The config-1 solve traced in walk-length order (trace_order 2, the screen default): three solves, the first in
+    the order of the initial keys, the next two in the order of the previous walks; the last one's hits, traced and
+    merged atlas and irradiance bit for bit with the oracle, and every ray traced once (the DDA counters equal the
+    atlas order's)."""
+    case = gi_cases.config1()
+    sg = gpu.SceneGpu(ctx, case.scene)
+    vw = gpu.VoxWorld(sg, case.vox)
+    rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    try:
+        rc.set_frame(case.frame)
+        rc.render_gbuffer(sg)
+        rc.render_shadow(sg, case.shadow)
+        vw.update(case.scene.camera.eye)
+        rc.set_stats(1)
+        rc.set_tuning(trace_order=0, trace_rays=1)
+        rc.solve(vw)
+        ref_counts = rc.read_counts()
+        rc.set_tuning(trace_order=2, trace_rays=2)
+        rc.set_debug_hits(True)
+        for _ in range(3):
+            rc.solve(vw)
+        counts = rc.read_counts()
+        g = {"hits": rc.read_buffer(_lib.GI_RC_HITS).view(np.uint32).reshape(-1, 4),
+             "rad_traced": rc.read_atlas(_lib.GI_RC_RAD_TRACED), "rad": rc.read_atlas(_lib.GI_RC_RAD),
+             "irr": rc.read_irradiance()}
+        depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width)
+        normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4)
+        shadow = rc.read_shadow()
+    finally:
+        for h in (rc, vw, sg):
+            h.destroy()
+    assert np.array_equal(counts, ref_counts), "DDA counters differ from the atlas order's"
+    st, o = run_oracle(case, depth, normal.astype(np.float32), shadow)
+    assert np.array_equal(g["hits"], o["hit"]), "DDA hits differ"
+    _close(g["rad_traced"], o["rad_traced"], 1e-4, "traced radiance")
+    _close(g["rad"], o["rad"], 1e-4, "merged atlas")
+    _close(g["irr"], o["irr"], 1e-4, "irradiance")

@@ -29,6 +29,7 @@ def _solve(ctx, case, rc_tuning=None, vox_tuning=None):
         vw.update(case.scene.camera.eye)
         rc.set_debug_hits(True)
         rc.solve(vw)
+        rc.solve(vw)   # the walk-length order (trace_order 2) uses the first solve's walks in the second
         st = vw.read_state()
         out = {"irr": rc.read_buffer(_lib.GI_RC_RAD), "sh": rc.read_buffer(_lib.GI_RC_SH),
                "hits": rc.read_buffer(_lib.GI_RC_HITS), "traced": rc.read_buffer(_lib.GI_RC_RAD_TRACED)}
@@ -44,7 +45,9 @@ def _solve(ctx, case, rc_tuning=None, vox_tuning=None):
 
 
 VARIANTS = [
+    ({"trace_order": 0, "trace_rays": 1}, None),
     ({"trace_order": 1}, None),
+    ({"trace_order": 2, "trace_rays": 1, "trace_blocks": 4}, None),
     ({"trace_rays": 4, "trace_blocks": 2}, None),
     ({"trace_order": 1, "trace_rays": 2, "trace_blocks": 16}, None),
     ({"gather_shape": 0}, None),
@@ -70,11 +73,11 @@ def test_tuning_rejects_bad_values(ctx):
     case = gi_cases.config0()
     rc = gpu.Rc(ctx, case.rc, case.width, case.height)
     try:
-        for bad in ({"trace_rays": 3}, {"trace_order": 2}, {"trace_blocks": 0}, {"gather_shape": 4},
+        for bad in ({"trace_rays": 3}, {"trace_order": 3}, {"trace_blocks": 0}, {"gather_shape": 4},
                     {"merge_threads": 100}):
             with pytest.raises(_lib.GiError):
                 rc.set_tuning(**bad)
-        assert rc.get_tuning() == {"trace_order": 0, "trace_rays": 1, "trace_blocks": 8, "gather_shape": 3,
+        assert rc.get_tuning() == {"trace_order": 2, "trace_rays": 2, "trace_blocks": 8, "gather_shape": 3,
                                    "merge_threads": 256}
     finally:
         rc.destroy()
