@@ -339,10 +339,11 @@ int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);
 typedef struct gi_rc_tuning {
   uint32_t trace_order;    /* 0: probe-major (a warp's lanes take consecutive directions of a probe, coalesced atlas
                               writes), 1: direction-major (a warp's lanes take one direction of 32 neighbouring probes,
-                              coherent voxel paths), 2: walk-length order (screen probes, their default; the rays by
-                              the previous solve's DDA step count and hit, longest first, so a warp's lanes walk
-                              alike; 5 bytes per ray; world probes take 0 or 1, default 0) */
-  uint32_t trace_rays;     /* rays per lane per queue fetch: 1, 2 or 4 (default 2 for screen probes, 1 for world) */
+                              coherent voxel paths), 2: walk-length order (screen probes; the rays by the previous
+                              solve's DDA step count and hit, longest first, so a warp's lanes walk alike: for a camera
+                              that holds still, as the keys come from the previous solve's rays and screen probes move
+                              with the camera; 5 bytes per ray, allocated when chosen).  Default 0 */
+  uint32_t trace_rays;     /* rays per lane per queue fetch: 1, 2 or 4 (default 1) */
   uint32_t trace_blocks;   /* resident 256-thread blocks per SM of the persistent trace: 1..16 (default 8) */
   uint32_t gather_shape;   /* gather: 0, 1, 2 blocks of 16x16, 32x8, 8x32 pixels; 3 (default) warps on pixel tiles
                               aligned to the probe cells, the shared probes staged in shared memory (cascade-0 tile

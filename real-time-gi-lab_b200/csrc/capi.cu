@@ -877,23 +877,8 @@ static int rc_create(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *
   return GI_OK;
 }
 
-static cudaError_t alloc_walk_order(gi_rc *r);
-
-// Screen probes trace in walk-length order by default (trace_order 2, two rays per lane per fetch)
 int gi_rc_create(gi_ctx *ctx, const gi_rc_params *p, uint32_t W, uint32_t H, gi_rc **out) {
-  const int st = rc_create(ctx, p, nullptr, W, H, out);
-  if (st != GI_OK) return st;
-  gi_rc *r = *out;
-  const cudaError_t e = alloc_walk_order(r);
-  if (e != cudaSuccess) {
-    gi_rc_destroy(r);
-    *out = nullptr;
-    return cuda_fail(e, "gi_rc_create: walk-length order buffers");
-  }
-  r->dev.trace_order = 2u;
-  r->dev.trace_rays = 2u;
-  r->bytes += 5u * (uint64_t)r->dev.rays_total + 1024u;
-  return GI_OK;
+  return rc_create(ctx, p, nullptr, W, H, out);
 }
 
 int gi_rc_create_world(gi_ctx *ctx, const gi_rc_params *p, const gi_world_params *world, uint32_t W, uint32_t H,
@@ -1513,6 +1498,7 @@ int gi_rc_set_tuning(gi_rc *r, const gi_rc_tuning *t) {
   if (t->trace_order == 2 && !r->dev.rperm) {   // the walk-length order's buffers, on first use
     CK(cudaSetDevice(r->ctx->device), "gi_rc_set_tuning: cudaSetDevice");
     CK(alloc_walk_order(r), "gi_rc_set_tuning: walk-length order buffers");
+    r->bytes += 5u * (uint64_t)r->dev.rays_total + 1024u;
     r->gen++;   // graphs captured before launch the other trace
   }
   if ((t->trace_order == 2) != (r->dev.trace_order == 2)) r->gen++;

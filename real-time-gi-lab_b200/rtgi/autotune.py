@@ -2,9 +2,10 @@
 WGSL).  The tunables change how work is laid onto the GPU, never the result (tested bit-exact):
 
   giTrace   trace_order (probe-major: a warp's lanes take a probe's consecutive directions, coalesced atlas writes;
-            direction-major: one direction over 32 neighbouring probes, coherent voxel paths; walk-length order,
-            screen probes only: the rays by the previous solve's step count and hit, longest first), trace_rays
-            (rays per lane per queue fetch), trace_blocks (resident blocks per SM of the persistent trace)
+            direction-major: one direction over 32 neighbouring probes, coherent voxel paths), trace_rays (rays per
+            lane per queue fetch), trace_blocks (resident blocks per SM of the persistent trace).  The walk-length
+            order (trace_order 2) is left out: it pays only while the camera holds still, and the tuner's repeated
+            solves of one frame would favour it for any workload.
   giMerge   merge_threads (block size)
   giGather  gather_shape (16x16, 32x8 or 8x32 pixels per block, or warps on probe-aligned tiles)
   vox       chunk_cells (cells per big-triangle work item of voxBits), blocks (resident blocks per SM)
@@ -22,7 +23,7 @@ import statistics
 from typing import Dict, Optional
 
 RC_GROUPS = {
-    "giTrace": {"trace_order": [0, 1, 2], "trace_rays": [1, 2, 4], "trace_blocks": [4, 8, 16]},
+    "giTrace": {"trace_order": [0, 1], "trace_rays": [1, 2, 4], "trace_blocks": [4, 8, 16]},
     "giMerge": {"merge_threads": [128, 256, 512]},
     "giGather": {"gather_shape": [0, 1, 2, 3]},
 }
@@ -68,8 +69,6 @@ class Autotuner:
             best_ms = {}
             for pass_name, space in list(RC_GROUPS.items()) + list(VOX_GROUPS.items()):
                 target = vox if pass_name == "vox" else rc
-                if pass_name == "giTrace" and getattr(rc, "world", False):   # the walk-length order is screen-only
-                    space = {**space, "trace_order": [0, 1]}
                 names = list(space)
                 best = None
                 for combo in itertools.product(*[space[n] for n in names]):

@@ -215,8 +215,8 @@ def test_irr16_is_the_rounded_f32_solve(ctx):
 
 
 def test_walk_length_order_parity(ctx):
-    """The config-1 solve traced in walk-length order (trace_order 2, the screen default): three solves, the first in
-    the order of the initial keys, the next two in the order of the previous walks; the last one's hits, traced and
+    """The config-1 solve traced in walk-length order (trace_order 2): three solves, the first in the order of the
+    initial keys, the next two in the order of the previous walks; the last one's hits, traced and
     merged atlas and irradiance bit for bit with the oracle, and every ray traced once (the DDA counters equal the
     atlas order's)."""
     case = gi_cases.config1()

@@ -45,9 +45,9 @@ def _solve(ctx, case, rc_tuning=None, vox_tuning=None):
 
 
 VARIANTS = [
-    ({"trace_order": 0, "trace_rays": 1}, None),
     ({"trace_order": 1}, None),
-    ({"trace_order": 2, "trace_rays": 1, "trace_blocks": 4}, None),
+    ({"trace_order": 2}, None),
+    ({"trace_order": 2, "trace_rays": 2, "trace_blocks": 4}, None),
     ({"trace_rays": 4, "trace_blocks": 2}, None),
     ({"trace_order": 1, "trace_rays": 2, "trace_blocks": 16}, None),
     ({"gather_shape": 0}, None),
@@ -77,7 +77,7 @@ def test_tuning_rejects_bad_values(ctx):
                     {"merge_threads": 100}):
             with pytest.raises(_lib.GiError):
                 rc.set_tuning(**bad)
-        assert rc.get_tuning() == {"trace_order": 2, "trace_rays": 2, "trace_blocks": 8, "gather_shape": 3,
+        assert rc.get_tuning() == {"trace_order": 0, "trace_rays": 1, "trace_blocks": 8, "gather_shape": 3,
                                    "merge_threads": 256}
     finally:
         rc.destroy()
