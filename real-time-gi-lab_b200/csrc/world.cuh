@@ -115,25 +115,11 @@ __device__ __forceinline__ uint32_t w_seg_samples(const VoxDev &v, f3 d, uint32_
 // (i + 0.5) / k for k = 1..16, i < k: the IEEE quotients, tabulated on the host (gi_world_tables)
 __device__ float g_seg_t[16 * 16];
 __device__ __forceinline__ float w_seg_t(uint32_t i, uint32_t k) { return g_seg_t[(k - 1u) * 16u + i]; }
-#ifndef GI_SEG_GROUP
-#define GI_SEG_GROUP 1
-#endif
 __device__ __forceinline__ bool w_seg_occluded(const VoxDev &v, f3 a, f3 b, uint32_t L) {
   const f3 d = b - a;
   const uint32_t k = w_seg_samples(v, d, L);
-#if GI_SEG_GROUP > 1
-  // any sample occupied: the samples are looked up GI_SEG_GROUP at a time, their loads in flight together
-  for (uint32_t i = 0; i < k; i += GI_SEG_GROUP) {
-    bool any = false;
-#pragma unroll
-    for (uint32_t u = 0; u < GI_SEG_GROUP; u++)
-      if (i + u < k) any |= w_vox_occ(v, L, a + d * w_seg_t(i + u, k));
-    if (any) return true;
-  }
-#else
   for (uint32_t i = 0; i < k; i++)
     if (w_vox_occ(v, L, a + d * w_seg_t(i, k))) return true;
-#endif
   return false;
 }
 
