@@ -50,14 +50,16 @@ typedef struct gi_dyn gi_dyn;
 
 /* Material (scene_gpu.ts:95-106 `struct Material`): base colour factor, flags (1 alpha mask, 2 double-sided,
  * 4 toon, 8 object), alpha cutoff.  emissive: radiance added at a voxel hit (no counterpart in the reference,
- * whose materials do not emit).  Textures are not supported: the base colour is the factor (the reference's
- * untextured materials sample a white default layer).  48 bytes. */
+ * whose materials do not emit).  base_color_tex: 1 + the base colour texture layer (gi_scene_set_textures) the
+ * colour is sampled from and multiplied by the factor; 0: untextured, the factor alone (the reference's white
+ * default layer, layers.x = 0).  48 bytes. */
 typedef struct {
   float base_color[4];
   uint32_t flags;
   float alpha_cutoff;
   float emissive[3];
-  uint32_t reserved[3];
+  uint32_t base_color_tex;
+  uint32_t reserved[2];
 } gi_material;
 
 /* VoxParams (voxel.ts:31-38).  levels <= 8; G a multiple of 4, <= 256 (brick coordinates are packed in 9 bits). */
@@ -117,6 +119,16 @@ int gi_ctx_destroy(gi_ctx *ctx);
 /* pos, nrm: nverts x 3 floats.  tri4: ntris x (i0, i1, i2, material), absolute vertex indices. */
 int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nverts, const uint32_t *tri4,
                     uint32_t ntris, const gi_material *mats, uint32_t nmats, gi_scene **out);
+/* Base colour textures (scene_gpu.ts:60-89; voxel.ts:325-336 surfaceAt; gbuffer.ts:90-94 and the shadow pass's
+ * alpha test; dynlayer.ts:451-454 shadeSample).  rgba8: layers x size x size texels, rgb sRGB-encoded and alpha
+ * linear (the reference's rgba8unorm-srgb), row-major; uv: nverts x 2 floats per vertex.  The library decodes the
+ * texels to linear f32 and builds each layer's mip chain on the device (level k + 1: the mean of 2 x 2 texels of level
+ * k, sums in a fixed order); a sample is bilinear within one level, repeat addressing, texel centres at (i + 0.5) /
+ * size.  The voxel passes sample at level 3 + L (the reference's textureSampleLevel), the rasters' alpha test and the
+ * dynamic layer likewise at their levels (G-buffer and shadow map: level 0, where the reference's hardware picks a
+ * level from derivatives).  size a power of two, 1 .. 4096; layers >= 1; the data is copied (stream-ordered on the
+ * null stream, synchronised before return).  Calling it again replaces the textures. */
+int gi_scene_set_textures(gi_scene *scene, const uint8_t *rgba8, uint32_t size, uint32_t layers, const float *uv);
 /* Replaces vertices [first, first + count) (the per-frame pose of moving objects, rcrun.ts:206-214). */
 int gi_scene_update_vertices(gi_scene *scene, uint32_t first, uint32_t count, const float *pos, const float *nrm,
                              void *stream);

@@ -15,7 +15,7 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libgi_oracle.so")
-SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "shadow.c", "world.c", "dyn.c", "orc_par.c", "gi_oracle.h", "orc_math.h",
+SOURCES = ["builtins.c", "vox.c", "rc.c", "rc64.c", "raster.c", "shadow.c", "world.c", "dyn.c", "tex.c", "orc_par.c", "gi_oracle.h", "orc_math.h",
            "orc_par.h", "orc_rc.h", "Makefile"]
 
 
@@ -61,6 +61,10 @@ def lib():
         _lib.orc_shadow_render.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.orc_sun_tap.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p]
         _lib.orc_sun_tap.restype = C.c_float
+        _lib.orc_tex_levels.argtypes = [C.c_uint32, C.c_void_p]
+        _lib.orc_tex_levels.restype = C.c_uint32
+        _lib.orc_tex_build.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p]
+        _lib.orc_tex_sample.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_float, C.c_uint32, C.c_void_p]
         _lib.orc_shadow_layers.argtypes = [C.c_void_p]
         _lib.orc_shadow_layers.restype = C.c_uint32
         _lib.orc_vox_sun.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32]
@@ -86,7 +90,9 @@ class OrcScene(C.Structure):
                 ("ntris", C.c_uint32), ("mats", C.c_void_p), ("nmats", C.c_uint32),
                 ("items", C.c_void_p), ("nitems", C.c_uint32), ("threads", C.c_uint32), ("key_stride", C.c_uint32),
                 ("ninst", C.c_uint32), ("lists", C.c_void_p), ("inst", C.c_void_p),
-                ("ndraw", C.c_uint32), ("draw_ninst", C.c_uint32), ("draw_inst", C.c_void_p)]
+                ("ndraw", C.c_uint32), ("draw_ninst", C.c_uint32), ("draw_inst", C.c_void_p),
+                ("uv", C.c_void_p), ("tex", C.c_void_p), ("tex_size", C.c_uint32), ("tex_levels", C.c_uint32),
+                ("tex_layers", C.c_uint32), ("tex_layer_texels", C.c_uint32)]
 
 
 class OrcVox(C.Structure):
@@ -150,7 +156,51 @@ def _scene_struct(scene):
     tri = np.ascontiguousarray(scene.tri, dtype=np.uint32)
     mats = scene.material_array()
     s = OrcScene(_p(pos), _p(nrm), pos.shape[0], _p(tri), tri.shape[0], _p(mats), len(mats))
-    return s, (pos, nrm, tri, mats)
+    keep = [pos, nrm, tri, mats]
+    if getattr(scene, "textures", None) is not None:
+        img = np.ascontiguousarray(scene.textures, dtype=np.uint8)
+        uv = np.ascontiguousarray(scene.uvs, dtype=np.float32)
+        tex = texture_chain(img)
+        size, layers = img.shape[1], img.shape[0]
+        per = C.c_uint32(0)
+        levels = lib().orc_tex_levels(size, C.byref(per))
+        s.uv, s.tex, s.tex_size, s.tex_levels, s.tex_layers, s.tex_layer_texels = \
+            _p(uv), _p(tex), size, levels, layers, per.value
+        keep += [uv, tex]
+    return s, tuple(keep)
+
+
+def tex_sample(img: np.ndarray, u: float, v: float, lod: int, layer: int = 1) -> np.ndarray:
+    """One sample of the oracle's texture definition (orc_tex_sample) from images (layers, size, size, 4) u8."""
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    tex = texture_chain(img)
+    per = C.c_uint32(0)
+    levels = lib().orc_tex_levels(img.shape[1], C.byref(per))
+    s = OrcScene()
+    uv = np.zeros(2, np.float32)
+    s.uv, s.tex, s.tex_size, s.tex_levels, s.tex_layers, s.tex_layer_texels = \
+        _p(uv), _p(tex), img.shape[1], levels, img.shape[0], per.value
+    out = np.zeros(4, np.float32)
+    lib().orc_tex_sample(C.byref(s), layer, C.c_float(u), C.c_float(v), lod, _p(out))
+    return out
+
+
+_TEX_CACHE = {}
+
+
+def texture_chain(img: np.ndarray) -> np.ndarray:
+    """The decoded layers and their mip chains (orc_tex_build), cached per image content."""
+    key = (img.shape, hash(img.tobytes()))
+    hit = _TEX_CACHE.get(key)
+    if hit is not None:
+        return hit
+    per = C.c_uint32(0)
+    lib().orc_tex_levels(img.shape[1], C.byref(per))
+    out = np.zeros((img.shape[0], per.value, 4), np.float32)
+    lib().orc_tex_build(_p(img), img.shape[1], img.shape[0], _p(out))
+    _TEX_CACHE.clear()
+    _TEX_CACHE[key] = out
+    return out
 
 
 def vox_origins(v0: float, levels: int, G: int, eye) -> np.ndarray:

@@ -70,10 +70,12 @@ static inline uint32_t fix_of(float x) {
   return (uint32_t)q;
 }
 
-/* shadeSample (dynlayer.ts:445-455), untextured: rgb and the albedo; 0 when the alpha test discards the sample */
-static int shade_sample(const orc_material *m, const float *F, const float *map, uint32_t S, v3 p, v3 n, v3 *rad, v3 *alb) {
-  v3 tex = V(m->base_color[0], m->base_color[1], m->base_color[2]);
-  if ((m->flags & 1u) != 0u && m->base_color[3] < m->alpha_cutoff) return 0;
+/* shadeSample (dynlayer.ts:445-455): tc the sampled base colour (texture times factor, or the factor untextured); rgb
+ * and the albedo; 0 when the alpha test discards the sample */
+static int shade_sample(const orc_material *m, const float tc[4], const float *F, const float *map, uint32_t S, v3 p,
+                        v3 n, v3 *rad, v3 *alb) {
+  v3 tex = V(tc[0], tc[1], tc[2]);
+  if ((m->flags & 1u) != 0u && tc[3] < m->alpha_cutoff) return 0;
   *alb = tex;
   float ndl = fmaxf_(dot(n, fromf(F + F_SUN)), 0.0f);
   if (ndl <= 0.0f) { *rad = V(0.0f, 0.0f, 0.0f); return 1; }
@@ -221,6 +223,7 @@ int orc_dyn_build(const orc_scene *s, const orc_vox *vx, orc_dyn *dl, uint32_t f
     uint32_t m = (uint32_t)fclampf(ceilf(e / vox_size(vx, L)), 1.0f, 16.0f);
     float fm = (float)m, sa = area / (fm * fm);
     const orc_material *mat = &s->mats[ti[3]];
+    const uint32_t tex_layer = orc_tex_layer_of(s, mat);
     for (uint32_t u = 0; u < m; u++)
       for (uint32_t vv = 0; vv + u < m; vv++)
         for (uint32_t flip = 0; flip < 2u; flip++) {
@@ -231,7 +234,14 @@ int orc_dyn_build(const orc_scene *s, const orc_vox *vx, orc_dyn *dl, uint32_t f
           v3 nr = add(add(muls(N3(s, ti[0]), wa), muls(N3(s, ti[1]), wb)), muls(N3(s, ti[2]), wc));
           nr = normalize3(dot(nr, nr) > 1e-12f ? nr : cross(sub(b, a), sub(c, a)));
           v3 rad, alb;
-          if (!shade_sample(mat, F, map, S, p, nr, &rad, &alb)) continue;
+          float tc[4] = {mat->base_color[0], mat->base_color[1], mat->base_color[2], mat->base_color[3]};
+          if (tex_layer) {   /* the texture at level 3 + L at the sample's uv, times the factor */
+            float uv[2], t[4];
+            orc_tri_uv(s, ti, wa, wb, wc, uv);
+            orc_tex_sample(s, tex_layer, uv[0], uv[1], 3u + L, t);
+            for (int k = 0; k < 4; k++) tc[k] = t[k] * mat->base_color[k];
+          }
+          if (!shade_sample(mat, tc, F, map, S, p, nr, &rad, &alb)) continue;
           splat_sample(vx, dl, L, p, nr, sa, rad, alb);
         }
   }

@@ -44,7 +44,8 @@ typedef struct {
   uint32_t flags;
   float alpha_cutoff;
   float emissive[3];
-  uint32_t reserved[3];
+  uint32_t base_color_tex;   /* 1 + texture layer; 0 untextured */
+  uint32_t reserved[2];
 } orc_material;
 
 typedef struct {
@@ -66,7 +67,21 @@ typedef struct {
    * one instance at the origin), drawn triangle i * ndraw + row; ndraw 0: every row */
   uint32_t ndraw, draw_ninst;
   const float *draw_inst;
+  /* Base colour textures (tex.c): a uv per vertex (2 floats), every layer's mip chain of linear rgba f32 texels
+   * (orc_tex_build); uv or tex NULL: every material untextured */
+  const float *uv;
+  const float *tex;
+  uint32_t tex_size, tex_levels, tex_layers, tex_layer_texels;
 } orc_scene;
+
+/* Textures (tex.c): levels of a size (and texels a layer); decode + mip chain of `layers` rgba8 images into out
+ * (layers x per-layer texels x 4 floats); 1 + layer of a material's texture or 0; a bilinear sample at a level; the uv
+ * at barycentric weights. */
+uint32_t orc_tex_levels(uint32_t size, uint32_t *per_layer);
+void orc_tex_build(const uint8_t *rgba8, uint32_t size, uint32_t layers, float *out);
+uint32_t orc_tex_layer_of(const orc_scene *s, const orc_material *m);
+void orc_tex_sample(const orc_scene *s, uint32_t layer1, float u, float v, uint32_t lod, float out[4]);
+void orc_tri_uv(const orc_scene *s, const uint32_t idx[3], float wx, float wy, float wz, float uv[2]);
 
 /* Voxel world state, laid out exactly as the CUDA path lays it out in device memory (struct of arrays). */
 typedef struct {

@@ -123,9 +123,9 @@ static v3 closest_bary(v3 p, v3 a, v3 b, v3 c) {
 }
 
 typedef struct { int ok; float albedo[3]; v3 n; float toon; v3 q; } surf_t;
-/* surfaceAt (voxel.ts:325-336) for untextured materials: the base colour texture's default layer is white, so the
- * sampled colour is the material's baseColorFactor exactly. */
-static surf_t surface_at(const orc_scene *s, const tri_t *T, v3 p, int want_attr) {
+/* surfaceAt (voxel.ts:325-336): the base colour texture at level 3 + L at p's closest point, times the factor
+ * (untextured: the factor alone, the reference's white default layer); the alpha test when masked and not wantAttr. */
+static surf_t surface_at(const orc_scene *s, const tri_t *T, v3 p, uint32_t L, int want_attr) {
   surf_t r;
   memset(&r, 0, sizeof r);
   const orc_material *m = &s->mats[T->idx[3]];
@@ -133,12 +133,20 @@ static surf_t surface_at(const orc_scene *s, const tri_t *T, v3 p, int want_attr
   r.q = p;
   if (!masked && !want_attr) { r.ok = 1; return r; }
   v3 w = closest_bary(p, T->a, T->b, T->c);
-  if (masked && m->base_color[3] < m->alpha_cutoff) { r.ok = 0; return r; }
+  float tex[4] = {m->base_color[0], m->base_color[1], m->base_color[2], m->base_color[3]};
+  uint32_t layer = orc_tex_layer_of(s, m);
+  if (layer) {
+    float uv[2], t[4];
+    orc_tri_uv(s, T->idx, w.x, w.y, w.z, uv);
+    orc_tex_sample(s, layer, uv[0], uv[1], 3u + L, t);
+    for (int k = 0; k < 4; k++) tex[k] = t[k] * m->base_color[k];
+  }
+  if (masked && tex[3] < m->alpha_cutoff) { r.ok = 0; return r; }
   v3 n0 = fromf(s->nrm + 3u * T->idx[0]), n1 = fromf(s->nrm + 3u * T->idx[1]), n2 = fromf(s->nrm + 3u * T->idx[2]);
   v3 n = add(add(muls(n0, w.x), muls(n1, w.y)), muls(n2, w.z));
   if (!(dot(n, n) > 1e-12f)) n = cross(sub(T->b, T->a), sub(T->c, T->a));
   r.ok = 1;
-  r.albedo[0] = m->base_color[0]; r.albedo[1] = m->base_color[1]; r.albedo[2] = m->base_color[2];
+  r.albedo[0] = tex[0]; r.albedo[1] = tex[1]; r.albedo[2] = tex[2];
   r.n = normalize3(n);
   r.toon = (m->flags & 4u) ? 1.0f : 0.0f;
   r.q = add(add(muls(T->a, w.x), muls(T->b, w.y)), muls(T->c, w.z));
@@ -209,7 +217,7 @@ static void voxelize_one(const orc_scene *s, orc_vox *vx, const tri_t *T, uint32
   if (ptr >= ORC_MARK) return;
   i3 l = I(c.x & 7, c.y & 7, c.z & 7);
   uint32_t bit = (uint32_t)(l.x + 8 * l.y + 64 * l.z);
-  if (!surface_at(s, T, p, 0).ok) return;
+  if (!surface_at(s, T, p, L, 0).ok) return;
   __atomic_fetch_or(&vx->occ[ptr * 16u + (bit >> 5)], 1u << (bit & 31u), __ATOMIC_RELAXED);
   atomic_max_u32(&vx->rep[ptr * 512u + bit], t + 1u);
 }
@@ -374,7 +382,7 @@ static void resolve_pass(void *p, uint64_t b0, uint64_t e0) {
         continue;
       }
       tri_t T = load_tri(s, rv - 1u);
-      surf_t sf = surface_at(s, &T, p, 1);
+      surf_t sf = surface_at(s, &T, p, L, 1);
       float alb[4] = {sf.albedo[0], sf.albedo[1], sf.albedo[2], sf.toon};
       /* octEnc (voxel.ts:590-594) */
       v3 n = sf.n;

@@ -76,6 +76,9 @@ struct gi_scene {
   gi_material *mats = nullptr;
   uint32_t nverts = 0, ntris = 0, nmats = 0;
   uint32_t mat_flags = 0;    // OR of the materials' flags (4 toon, 8 object: the G-buffer raster writes style tags)
+  float2 *uv = nullptr;      // base colour textures (gi_scene_set_textures): a uv per vertex, every layer's mip chain
+  float4 *tex = nullptr;
+  uint32_t tex_size = 0, tex_levels = 0, tex_layers = 0, tex_layer_texels = 0;
   // G-buffer raster scratch (gbuffer.cu): two renders of one scene must not overlap on the GPU
   float4 *raster_rec = nullptr;
   uint32_t *raster_ntile = nullptr, *raster_pre = nullptr, *raster_sums = nullptr, *raster_counter = nullptr;
@@ -91,6 +94,8 @@ struct gi_scene {
     s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
     s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
     s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
+    s.uv = uv; s.tex = tex;
+    s.tex_size = tex_size; s.tex_levels = tex_levels; s.tex_layers = tex_layers; s.tex_layer_texels = tex_layer_texels;
     return s;
   }
   // the scene as the rasters draw it: rows [0, ndraw) at every draw instance, triangle i * ndraw + row of instance i
@@ -191,6 +196,7 @@ static void free_scene(gi_scene *s) {
   cudaFree(s->pos); cudaFree(s->nrm); cudaFree(s->tri); cudaFree(s->mats);
   cudaFree(s->raster_rec); cudaFree(s->raster_ntile); cudaFree(s->raster_pre); cudaFree(s->raster_sums);
   cudaFree(s->raster_counter); cudaFree(s->raster_list); cudaFree(s->raster_over); cudaFree(s->stage);
+  cudaFree(s->uv); cudaFree(s->tex);
   cudaFree(s->rigid_rest); cudaFree(s->rigid_m); cudaFree(s->draw_inst);
 }
 static void free_vox(gi_vox *v) {
@@ -311,6 +317,48 @@ int gi_scene_upload(gi_ctx *ctx, const float *pos, const float *nrm, uint32_t nv
 __global__ void k_pack_vertices(const float *src, float4 *dst, uint32_t n) {
   uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) dst[i] = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], 0.0f);
+}
+
+// sRGB decode of an 8-bit channel (the rgba8unorm-srgb read): c / 12.92 up to 0.04045, ((c + 0.055) / 1.055)^2.4
+// above, c = k / 255, evaluated in double and rounded to f32
+static void srgb_table(float lut[256]) {
+  for (int k = 0; k < 256; k++) {
+    const double c = (double)k / 255.0;
+    lut[k] = (float)(c <= 0.04045 ? c / 12.92 : pow((c + 0.055) / 1.055, 2.4));
+  }
+}
+
+int gi_scene_set_textures(gi_scene *s, const uint8_t *rgba8, uint32_t size, uint32_t layers, const float *uv) {
+  if (!s || !rgba8 || !uv) return fail(GI_ERR_INVALID, "gi_scene_set_textures: NULL argument");
+  if (size < 1 || size > 4096 || (size & (size - 1u)) != 0u)
+    return fail(GI_ERR_INVALID, "gi_scene_set_textures: size %u (a power of two, 1 .. 4096)", size);
+  if (layers < 1 || (uint64_t)layers * size * size > (1ull << 28))
+    return fail(GI_ERR_INVALID, "gi_scene_set_textures: %u layers of %u^2 texels (at most 2^28 texels)", layers, size);
+  CK(cudaSetDevice(s->ctx->device), "gi_scene_set_textures: cudaSetDevice");
+  uint32_t levels = 0, per = 0;
+  for (uint32_t n = size; n >= 1u; n >>= 1) { levels++; per += n * n; if (n == 1u) break; }
+  cudaFree(s->uv); cudaFree(s->tex);
+  s->uv = nullptr; s->tex = nullptr; s->tex_size = s->tex_levels = s->tex_layers = s->tex_layer_texels = 0;
+  float lut[256];
+  srgb_table(lut);
+  uint8_t *raw = nullptr;
+  float *dlut = nullptr;
+  const size_t nraw = (size_t)layers * size * size * 4u;
+  cudaError_t e;
+  if ((e = cudaMalloc(&s->uv, (size_t)(s->nverts ? s->nverts : 1u) * sizeof(float2))) ||
+      (e = cudaMalloc(&s->tex, (size_t)layers * per * sizeof(float4))) || (e = cudaMalloc(&raw, nraw)) ||
+      (e = cudaMalloc(&dlut, sizeof lut)) ||
+      (e = cudaMemcpy(s->uv, uv, (size_t)s->nverts * sizeof(float2), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(raw, rgba8, nraw, cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(dlut, lut, sizeof lut, cudaMemcpyHostToDevice)) ||
+      (e = gi_launch_tex_build(raw, dlut, s->tex, size, levels, layers, per)) || (e = cudaDeviceSynchronize())) {
+    cudaFree(raw); cudaFree(dlut); cudaFree(s->uv); cudaFree(s->tex);
+    s->uv = nullptr; s->tex = nullptr;
+    return cuda_fail(e, "gi_scene_set_textures");
+  }
+  cudaFree(raw); cudaFree(dlut);
+  s->tex_size = size; s->tex_levels = levels; s->tex_layers = layers; s->tex_layer_texels = per;
+  return GI_OK;
 }
 
 int gi_scene_update_vertices(gi_scene *s, uint32_t first, uint32_t count, const float *pos, const float *nrm, void *stream) {

@@ -170,11 +170,13 @@ __global__ void __launch_bounds__(256) k_dyn_clear(DynDev d) {
 // WGSL u32(round(x)) of a non-negative x: round half to even, saturating
 __device__ __forceinline__ uint32_t fix_of(float x) { return __float2uint_rz(rintf(x * DYN_FIX)); }
 
-// shadeSample (dynlayer.ts:445-455), untextured: false when the alpha test discards the sample
-__device__ __forceinline__ bool shade_sample(const gi_material &m, const float *__restrict__ F, const float *__restrict__ map,
-                                             uint32_t S, uint32_t layers, f3 p, f3 n, f3 &rad, f3 &alb) {
-  const f3 tex = mk(m.base_color[0], m.base_color[1], m.base_color[2]);
-  if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;
+// shadeSample (dynlayer.ts:445-455): tc the sampled base colour (texture times factor, or the factor untextured); false
+// when the alpha test discards the sample
+__device__ __forceinline__ bool shade_sample(const gi_material &m, float4 tc, const float *__restrict__ F,
+                                             const float *__restrict__ map, uint32_t S, uint32_t layers, f3 p, f3 n,
+                                             f3 &rad, f3 &alb) {
+  const f3 tex = mk(tc.x, tc.y, tc.z);
+  if ((m.flags & 1u) != 0u && tc.w < m.alpha_cutoff) return false;
   alb = tex;
   const float ndl = mx(dot(n, mk(F[F_SUN], F[F_SUN + 1], F[F_SUN + 2])), 0.0f);
   if (ndl <= 0.0f) { rad = mk(0.0f, 0.0f, 0.0f); return true; }
@@ -245,6 +247,7 @@ __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev 
   const uint32_t m = (uint32_t)fclampf(ceilf(e / vox_size(v, L)), 1.0f, 16.0f);
   const float fm = (float)m, sa = area / (fm * fm);
   const gi_material mat = s.mats[ti.w];
+  const uint32_t tex_layer = tex_layer_of(s, mat);
   const f3 n0 = dyn_nrm(s, ti.x), n1 = dyn_nrm(s, ti.y), n2 = dyn_nrm(s, ti.z);
   for (uint32_t q = lane; q < m * m; q += 32u) {
     uint32_t u = 0, r = q;
@@ -256,7 +259,13 @@ __global__ void __launch_bounds__(256) k_dyn_splat(DynDev d, VoxDev v, SceneDev 
     f3 nr = (n0 * wa + n1 * wb) + n2 * wc;
     nr = normalize3(dot(nr, nr) > 1e-12f ? nr : cross(b - a, c - a));
     f3 rad, alb;
-    if (!shade_sample(mat, F, map, S, layers, p, nr, rad, alb)) continue;
+    float4 tc = make_float4(mat.base_color[0], mat.base_color[1], mat.base_color[2], mat.base_color[3]);
+    if (tex_layer) {   // the texture at level 3 + L at the sample's uv, times the factor
+      const float2 uv = tri_uv(s, ti, wa, wb, wc);
+      const float4 t = tex_sample(s, tex_layer, uv.x, uv.y, 3u + L);
+      tc = make_float4(t.x * mat.base_color[0], t.y * mat.base_color[1], t.z * mat.base_color[2], t.w * mat.base_color[3]);
+    }
+    if (!shade_sample(mat, tc, F, map, S, layers, p, nr, rad, alb)) continue;
     splat_sample(d, v, L, p, nr, sa, rad, alb);
   }
 }

@@ -343,6 +343,44 @@ __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__res
 
 using namespace gi;
 
+namespace gi {
+// Level 0 of every layer: the texels decoded (rgb through the sRGB table, alpha k / 255)
+__global__ void k_tex_decode(const uint8_t *__restrict__ rgba8, const float *__restrict__ lut, float4 *tex, uint32_t size,
+                             uint32_t layers, uint32_t per) {
+  const uint64_t n = (uint64_t)size * size;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n * layers; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t l = i / n, t = i - l * n;
+    const uchar4 c = reinterpret_cast<const uchar4 *>(rgba8)[i];
+    tex[l * per + t] = make_float4(lut[c.x], lut[c.y], lut[c.z], (float)c.w / 255.0f);
+  }
+}
+// Level k + 1 of every layer (size m) from level k (size 2m): the mean of its 2 x 2 texels, ((a + b) + (c + d)) / 4
+__global__ void k_tex_mip(float4 *tex, uint32_t m, uint32_t src_off, uint32_t dst_off, uint32_t layers, uint32_t per) {
+  const uint64_t n = (uint64_t)m * m;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n * layers; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t l = i / n, t = i - l * n;
+    const uint32_t x = (uint32_t)(t % m), y = (uint32_t)(t / m), w = 2u * m;
+    const float4 *s = tex + l * per + src_off;
+    const float4 a = s[(2u * y) * w + 2u * x], b = s[(2u * y) * w + 2u * x + 1u];
+    const float4 c = s[(2u * y + 1u) * w + 2u * x], d = s[(2u * y + 1u) * w + 2u * x + 1u];
+    tex[l * per + dst_off + t] = make_float4(((a.x + b.x) + (c.x + d.x)) * 0.25f, ((a.y + b.y) + (c.y + d.y)) * 0.25f,
+                                             ((a.z + b.z) + (c.z + d.z)) * 0.25f, ((a.w + b.w) + (c.w + d.w)) * 0.25f);
+  }
+}
+}  // namespace gi
+
+cudaError_t gi_launch_tex_build(const uint8_t *rgba8, const float *lut, float4 *tex, uint32_t size, uint32_t levels,
+                                uint32_t layers, uint32_t per) {
+  k_tex_decode<<<1184, 256>>>(rgba8, lut, tex, size, layers, per);
+  uint32_t off = 0;
+  for (uint32_t k = 0; k + 1u < levels; k++) {
+    const uint32_t n = size >> k;
+    k_tex_mip<<<1184, 256>>>(tex, n / 2u, off, off + n * n, layers, per);
+    off += n * n;
+  }
+  return cudaGetLastError();
+}
+
 uint32_t gi_raster_tiles(uint32_t W, uint32_t H) { return ((W + RT - 1u) / RT) * ((H + RT - 1u) / RT); }
 
 cudaError_t gi_launch_gbuffer(const SceneDev &s, const float *frame_dev, uint32_t W, uint32_t H, float *depth,

@@ -201,7 +201,42 @@ struct SceneDev {
   const uint32_t *lists;
   const float4 *inst;
   uint32_t nitems, threads, key_stride, key_limit;   // threads of the triangle passes; keys below key_limit
+  // Base colour textures (gi_scene_set_textures): a uv per vertex; per layer the mip chain of linear float4 texels
+  const float2 *uv;          // null: no texture coordinates (every material untextured)
+  const float4 *tex;
+  uint32_t tex_size, tex_levels, tex_layers, tex_layer_texels;
 };
+
+// 1 + layer of a textured material this scene can sample, else 0
+__device__ __forceinline__ uint32_t tex_layer_of(const SceneDev &s, const gi_material &m) {
+  return (s.uv && s.tex && m.base_color_tex != 0u && m.base_color_tex <= s.tex_layers) ? m.base_color_tex : 0u;
+}
+// Bilinear sample of layer (1-based) at level lod (clamped to the chain), repeat addressing: texel (i, j) of a level of
+// size n has its centre at ((i + 0.5) / n, (j + 0.5) / n); the four texels around (u, v) weighted in f32 as
+// (t00 (1 - ax) + t10 ax) (1 - ay) + (t01 (1 - ax) + t11 ax) ay
+__device__ __forceinline__ float4 tex_sample(const SceneDev &s, uint32_t layer1, float u, float v, uint32_t lod) {
+  const uint32_t L = lod < s.tex_levels ? lod : s.tex_levels - 1u;
+  uint32_t off = 0;
+  for (uint32_t k = 0; k < L; k++) off += (s.tex_size >> k) * (s.tex_size >> k);
+  const uint32_t n = s.tex_size >> L;
+  const float4 *t = s.tex + (size_t)(layer1 - 1u) * s.tex_layer_texels + off;
+  const float x = u * (float)n - 0.5f, y = v * (float)n - 0.5f;
+  const float fx = floorf(x), fy = floorf(y);
+  const float ax = x - fx, ay = y - fy;
+  const int m = (int)n - 1;
+  const int i0 = f2i(fx) & m, i1 = (int)((uint32_t)f2i(fx) + 1u) & m;
+  const int j0 = f2i(fy) & m, j1 = (int)((uint32_t)f2i(fy) + 1u) & m;
+  const float4 a = __ldg(&t[j0 * (int)n + i0]), b = __ldg(&t[j0 * (int)n + i1]);
+  const float4 c = __ldg(&t[j1 * (int)n + i0]), d = __ldg(&t[j1 * (int)n + i1]);
+  const float bx = 1.0f - ax, by = 1.0f - ay;
+  return make_float4((a.x * bx + b.x * ax) * by + (c.x * bx + d.x * ax) * ay, (a.y * bx + b.y * ax) * by + (c.y * bx + d.y * ax) * ay,
+                     (a.z * bx + b.z * ax) * by + (c.z * bx + d.z * ax) * ay, (a.w * bx + b.w * ax) * by + (c.w * bx + d.w * ax) * ay);
+}
+// The uv at barycentric weights w of the triangle's vertices (UV(a) w.x + UV(b) w.y + UV(c) w.z, voxel.ts:330)
+__device__ __forceinline__ float2 tri_uv(const SceneDev &s, uint4 idx, float wx, float wy, float wz) {
+  const float2 a = s.uv[idx.x], b = s.uv[idx.y], c = s.uv[idx.z];
+  return make_float2((a.x * wx + b.x * wy) + c.x * wz, (a.y * wx + b.y * wy) + c.y * wz);
+}
 
 // Drawn triangle t of a raster: row t of the table, or with drawn instances (inst set) row t mod key_stride of
 // instance t / key_stride, moved by its offset

@@ -225,6 +225,10 @@ cudaError_t gi_launch_gbuffer(const gi::SceneDev &s, const float *frame_dev, uin
 cudaError_t gi_launch_normal_f32_to_f16(const float4 *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_normal_rgb_to_rgba(const uint16_t *src, uint2 *dst, uint32_t n, cudaStream_t st);
 cudaError_t gi_launch_iota(uint32_t *dst, uint32_t n, cudaStream_t st);
+// Base colour textures: rgba8 (sRGB rgb, linear alpha) decoded to linear float4 through lut, then every layer's mip
+// chain (levels of size >> k, per texels a layer), on the null stream
+cudaError_t gi_launch_tex_build(const uint8_t *rgba8, const float *lut, float4 *tex, uint32_t size, uint32_t levels,
+                                uint32_t layers, uint32_t per);
 cudaError_t gi_launch_irr_to_f32(const gi::RcDev &r, float4 *dst, cudaStream_t st);
 cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs, cudaStream_t st);
 // FP64 reference of merge + SH + gather from the f32 traced atlas: rad64 rays_total x 4 doubles, sh64 27 doubles per

@@ -146,6 +146,8 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
   s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
   s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
+  s.uv = nullptr; s.tex = nullptr;   // no textures here: the base colour is the factor
+  s.tex_size = s.tex_levels = s.tex_layers = s.tex_layer_texels = 0;
   e = gi_launch_vox_build(v, s, sms, (cudaStream_t)stream);
   if (e != cudaSuccess) return fail(GI_ERR_CUDA, "gi_vox_build_noalloc: launch: %s", cudaGetErrorString(e));
   return GI_OK;

@@ -336,6 +336,47 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= v.scan_cap; q += gridDim.x * blockDim.x) v.look[q] = 0ull;
 }
 
+// closestBary (voxel.ts:250-267)
+__device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
+  f3 ab = b - a, ac = c - a, ap = p - a;
+  float d1 = dot(ab, ap), d2 = dot(ac, ap);
+  if (d1 <= 0.0f && d2 <= 0.0f) return mk(1.0f, 0.0f, 0.0f);
+  f3 bp = p - b;
+  float d3 = dot(ab, bp), d4 = dot(ac, bp);
+  if (d3 >= 0.0f && d4 <= d3) return mk(0.0f, 1.0f, 0.0f);
+  float vc = d1 * d4 - d3 * d2;
+  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) { float w = d1 / (d1 - d3); return mk(1.0f - w, w, 0.0f); }
+  f3 cp = p - c;
+  float d5 = dot(ab, cp), d6 = dot(ac, cp);
+  if (d6 >= 0.0f && d5 <= d6) return mk(0.0f, 0.0f, 1.0f);
+  float vb = d5 * d2 - d1 * d6;
+  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) { float w = d2 / (d2 - d6); return mk(1.0f - w, 0.0f, w); }
+  float va = d3 * d6 - d5 * d4;
+  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
+    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+    return mk(0.0f, 1.0f - w, w);
+  }
+  float dn = 1.0f / (va + vb + vc);
+  float vv = vb * dn, ww = vc * dn;
+  return mk(1.0f - vv - ww, vv, ww);
+}
+
+// surfaceAt's alpha test (voxel.ts:325-332): a masked material keeps the cell when its alpha — the base colour texture
+// at level 3 + L at the voxel centre's closest point on the triangle, times the factor; the factor alone untextured —
+// reaches the cutoff
+__device__ __forceinline__ bool alpha_passes(const SceneDev &s, const Tri &T, f3 p, uint32_t L) {
+  const gi_material &m = s.mats[T.idx.w];
+  if ((m.flags & 1u) == 0u) return true;
+  float a = m.base_color[3];
+  const uint32_t layer = tex_layer_of(s, m);
+  if (layer) {
+    const f3 w = closest_bary(p, T.a, T.b, T.c);
+    const float2 uv = tri_uv(s, T.idx, w.x, w.y, w.z);
+    a = tex_sample(s, layer, uv.x, uv.y, 3u + L).w * m.base_color[3];
+  }
+  return !(a < m.alpha_cutoff);
+}
+
 // voxelizeOne (voxel.ts:476-490)
 
 __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s, const Tri &T, uint32_t t, uint32_t L,
@@ -348,9 +389,7 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
   if (!single && !tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return;
   if (ptr >= GI_MARK) return;
   uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
-  // surfaceAt's alpha test (voxel.ts:325-332): untextured, so the sampled alpha is the factor's
-  const gi_material &m = s.mats[T.idx.w];
-  if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return;
+  if (!alpha_passes(s, T, p, L)) return;
   uint32_t wi = ptr * 16u + (bit >> 5);
   uint32_t msk = 1u << (bit & 31u);
   uint32_t ri = ptr * 512u + bit;
@@ -445,8 +484,7 @@ __device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, 
   float hh = 0.5f * vs * 1.0001f;
   if (!tri_box(p, mk(hh, hh, hh), T.a, T.b, T.c)) return false;
   if (ptr >= GI_MARK) return false;
-  const gi_material &m = s.mats[T.idx.w];
-  if ((m.flags & 1u) != 0u && m.base_color[3] < m.alpha_cutoff) return false;
+  if (!alpha_passes(s, T, p, L)) return false;
   uint32_t bit = (uint32_t)((c.x & 7) + 8 * (c.y & 7) + 64 * (c.z & 7));
   wi = ptr * 16u + (bit >> 5);
   msk = 1u << (bit & 31u);
@@ -623,30 +661,6 @@ __global__ void __launch_bounds__(256) k_alloc_voxels(VoxDev v, uint32_t nblocks
   if (blk == nblocks - 1u && threadIdx.x == 255u) v.hdr[1] = first + c;
 }
 
-// closestBary (voxel.ts:250-267)
-__device__ __forceinline__ f3 closest_bary(f3 p, f3 a, f3 b, f3 c) {
-  f3 ab = b - a, ac = c - a, ap = p - a;
-  float d1 = dot(ab, ap), d2 = dot(ac, ap);
-  if (d1 <= 0.0f && d2 <= 0.0f) return mk(1.0f, 0.0f, 0.0f);
-  f3 bp = p - b;
-  float d3 = dot(ab, bp), d4 = dot(ac, bp);
-  if (d3 >= 0.0f && d4 <= d3) return mk(0.0f, 1.0f, 0.0f);
-  float vc = d1 * d4 - d3 * d2;
-  if (vc <= 0.0f && d1 >= 0.0f && d3 <= 0.0f) { float w = d1 / (d1 - d3); return mk(1.0f - w, w, 0.0f); }
-  f3 cp = p - c;
-  float d5 = dot(ab, cp), d6 = dot(ac, cp);
-  if (d6 >= 0.0f && d5 <= d6) return mk(0.0f, 0.0f, 1.0f);
-  float vb = d5 * d2 - d1 * d6;
-  if (vb <= 0.0f && d2 >= 0.0f && d6 <= 0.0f) { float w = d2 / (d2 - d6); return mk(1.0f - w, 0.0f, w); }
-  float va = d3 * d6 - d5 * d4;
-  if (va <= 0.0f && (d4 - d3) >= 0.0f && (d5 - d6) >= 0.0f) {
-    float w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
-    return mk(0.0f, 1.0f - w, w);
-  }
-  float dn = 1.0f / (va + vb + vc);
-  float vv = vb * dn, ww = vc * dn;
-  return mk(1.0f - vv - ww, vv, ww);
-}
 
 // resolveAttr (voxel.ts:596-620): one thread per voxel of the attribute pool (voxel ai of brick b is rank
 // ai - vpre[b] of b's occupancy), so every occupied voxel is resolved in parallel and the attribute writes are
@@ -713,7 +727,15 @@ __global__ void __launch_bounds__(256) k_resolve_attr(VoxDev v, SceneDev s) {
       oy = (1.0f - fabsf(tx)) * (ty >= 0.0f ? 1.0f : -1.0f);
     }
     uint4 rec;
-    rec.x = pack4x8unorm(m.base_color[0], m.base_color[1], m.base_color[2], toon);
+    // the albedo: the base colour texture at level 3 + L at the closest point, times the factor (surfaceAt)
+    float ar = m.base_color[0], ag = m.base_color[1], ab = m.base_color[2];
+    const uint32_t layer = tex_layer_of(s, m);
+    if (layer) {
+      const float2 uv = tri_uv(s, T.idx, wb.x, wb.y, wb.z);
+      const float4 t = tex_sample(s, layer, uv.x, uv.y, 3u + L);
+      ar = t.x * m.base_color[0]; ag = t.y * m.base_color[1]; ab = t.z * m.base_color[2];
+    }
+    rec.x = pack4x8unorm(ar, ag, ab, toon);
     rec.y = pack2x16snorm(ox, oy);
     rec.z = (uint32_t)f2h(m.emissive[0]) | ((uint32_t)f2h(m.emissive[1]) << 16);
     rec.w = (uint32_t)f2h(m.emissive[2]);

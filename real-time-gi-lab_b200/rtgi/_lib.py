@@ -26,6 +26,7 @@ SIGNATURES = {
     "gi_ctx_destroy": (C.c_int, [_P]),
     "gi_scene_upload": (C.c_int, [_P, _P, _P, C.c_uint32, _P, C.c_uint32, _P, C.c_uint32, C.POINTER(_P)]),
     "gi_scene_update_vertices": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P, _P, _P]),
+    "gi_scene_set_textures": (C.c_int, [_P, _P, C.c_uint32, C.c_uint32, _P]),
     "gi_scene_destroy": (C.c_int, [_P]),
     "gi_vox_create": (C.c_int, [_P, _P, C.POINTER(_P)]),
     "gi_vox_update": (C.c_int, [_P, C.POINTER(C.c_double)]),

@@ -58,6 +58,18 @@ class SceneGpu:
         _lib.call("gi_scene_upload", ctx.handle, _ptr(pos), _ptr(nrm), pos.shape[0], _ptr(tri), tri.shape[0],
                   _ptr(mats), len(mats), C.byref(h))
         self.handle = h
+        if scene.textures is not None:
+            self.set_textures(scene.textures, scene.uvs)
+
+    def set_textures(self, images: np.ndarray, uvs: np.ndarray) -> None:
+        """Base colour textures (gi_scene_set_textures): images (layers, size, size, 4) u8, uvs (V, 2) f32."""
+        img = np.ascontiguousarray(images, dtype=np.uint8)
+        uv = np.ascontiguousarray(uvs, dtype=np.float32)
+        if img.ndim != 4 or img.shape[1] != img.shape[2] or img.shape[3] != 4:
+            raise _lib.GiError(_lib.GI_ERR_INVALID, f"textures of shape {img.shape}: (layers, size, size, 4) expected")
+        if uv.shape != (self.scene.positions.shape[0], 2):
+            raise _lib.GiError(_lib.GI_ERR_INVALID, f"uvs of shape {uv.shape} for {self.scene.positions.shape[0]} vertices")
+        _lib.call("gi_scene_set_textures", self.handle, _ptr(img), img.shape[1], img.shape[0], _ptr(uv))
 
     def set_draw_count(self, count: int) -> None:
         """The rasters draw rows [0, count) (a world's clustered copies are voxelised only)."""

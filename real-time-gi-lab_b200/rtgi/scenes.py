@@ -18,7 +18,7 @@ from . import mathx
 from .frame import Camera
 
 MATERIAL_DTYPE = np.dtype([("base_color", "<f4", (4,)), ("flags", "<u4"), ("alpha_cutoff", "<f4"),
-                           ("emissive", "<f4", (3,)), ("reserved", "<u4", (3,))])
+                           ("emissive", "<f4", (3,)), ("base_color_tex", "<u4"), ("reserved", "<u4", (2,))])
 assert MATERIAL_DTYPE.itemsize == 48
 
 FLAG_ALPHA_MASK, FLAG_DOUBLE_SIDED, FLAG_TOON, FLAG_OBJECT = 1, 2, 4, 8
@@ -31,6 +31,7 @@ class Material:
     flags: int = 0
     alpha_cutoff: float = 0.5
     emissive: tuple = (0.0, 0.0, 0.0)
+    base_color_tex: int = 0        # 1 + the scene's texture layer (layers.x of the reference); 0: untextured
 
 
 GREY = Material("grey", (0.7, 0.7, 0.7, 1.0))   # scenes.ts:173
@@ -47,6 +48,8 @@ class Scene:
     sun_dir: tuple = (0.0, 1.0, 0.0)
     sun_e: tuple = (0.0, 0.0, 0.0)
     sky: tuple = (0.0, 0.0, 0.0)
+    uvs: Optional[np.ndarray] = None        # (V, 2) f32 texture coordinates, or None
+    textures: Optional[np.ndarray] = None   # (layers, size, size, 4) u8 base colour images (sRGB rgb, linear alpha)
 
     @property
     def triangle_count(self) -> int:
@@ -59,6 +62,7 @@ class Scene:
             a[i]["flags"] = m.flags
             a[i]["alpha_cutoff"] = m.alpha_cutoff
             a[i]["emissive"] = m.emissive
+            a[i]["base_color_tex"] = m.base_color_tex
         return a
 
 
@@ -325,3 +329,42 @@ def batch_spec(seed: int) -> dict:
     cascades = 2 + int(rng.uniform(0, 4 - 1e-9))
     v0 = [0.1, 0.15, 0.2][int(rng.uniform(0, 3 - 1e-9))]
     return {"seed": seed, "tris": tris, "G": G, "levels": levels, "width": W, "height": H, "cascades": cascades, "v0": v0}
+
+
+def textured_scene(size: int = 64) -> Scene:
+    """The room of 60 boxes with base colour textures: every box face mapped to a coloured stripe image (layer 1),
+    and four alpha-masked panels in the room (a cut-out lattice, layer 2: alpha 0 in the holes, cutoff 0.5), so the
+    voxel passes' alpha test, the albedo sampling and the rasters' alpha test all see texels.  uvs: each quad's corners
+    (0,0) (2,0) (2,2) (0,2) — repeat addressing tiles the image twice."""
+    import dataclasses
+    s = room_scene(0, n_boxes=60)
+    nv = s.positions.shape[0]
+    corners = np.array([[0.0, 0.0], [2.0, 0.0], [2.0, 2.0], [0.0, 2.0]], np.float32)
+    uvs = np.tile(corners, (nv // 4 + 1, 1))[:nv]
+    # layer 1: stripes of four colours; layer 2: a lattice, opaque bars of size/8 texels every size/2, alpha 0 between
+    # (holes wider than a level-3 texel, so the voxel passes' sampling at level 3 + L still sees them)
+    img = np.zeros((2, size, size, 4), np.uint8)
+    x = np.arange(size)
+    pal = np.array([[230, 60, 40], [40, 200, 80], [50, 90, 230], [240, 220, 60]], np.uint8)
+    img[0, :, :, :3] = pal[(x[None, :] * 4 // size) % 4]
+    img[0, :, :, 3] = 255
+    bars = ((x[:, None] % (size // 2)) < size // 8) | ((x[None, :] % (size // 2)) < size // 8)
+    img[1, :, :, :3] = 200
+    img[1, :, :, 3] = np.where(bars, 255, 0)
+    mats = [dataclasses.replace(m, base_color_tex=1) if m.name.startswith("box") else m for m in s.materials]
+    # the panels: 1.5 m squares standing in the room
+    b = Builder([Material("panel", (0.9, 0.9, 0.9, 1.0), flags=FLAG_ALPHA_MASK, alpha_cutoff=0.5,
+                          base_color_tex=2)])
+    for k, (cx, cz) in enumerate(((1.0, 1.0), (-2.0, 0.5), (0.5, -2.5), (2.5, -1.0))):
+        b.quad([cx - 0.75, 0.2, cz], [cx + 0.75, 0.2, cz], [cx + 0.75, 1.7, cz], [cx - 0.75, 1.7, cz])
+    panel = b.scene("panels", s.camera)
+    pos = np.concatenate([s.positions, panel.positions]).astype(np.float32)
+    nrm = np.concatenate([s.normals, panel.normals]).astype(np.float32)
+    ptri = panel.tri.astype(np.int64).copy()
+    ptri[:, :3] += nv
+    ptri[:, 3] = len(mats)
+    tri = np.concatenate([s.tri.astype(np.int64), ptri]).astype(np.uint32)
+    puv = np.tile(corners, (panel.positions.shape[0] // 4, 1))
+    return dataclasses.replace(s, name="room-textured", positions=pos, normals=nrm, tri=tri,
+                               materials=mats + list(panel.materials), uvs=np.concatenate([uvs, puv]).astype(np.float32),
+                               textures=img)
