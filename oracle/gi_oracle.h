@@ -82,6 +82,9 @@ void orc_tex_build(const uint8_t *rgba8, uint32_t size, uint32_t layers, float *
 uint32_t orc_tex_layer_of(const orc_scene *s, const orc_material *m);
 void orc_tex_sample(const orc_scene *s, uint32_t layer1, float u, float v, uint32_t lod, float out[4]);
 void orc_tri_uv(const orc_scene *s, const uint32_t idx[3], float wx, float wy, float wz, float uv[2]);
+/* The rasters' alpha test (gbuffer.ts:94, the shadow pass's discard): a masked material's alpha at barycentric weights
+ * (the texture at level 0 times the factor; the factor alone untextured) against the cutoff; 1 when kept. */
+int orc_raster_alpha_ok(const orc_scene *s, const uint32_t idx[4], float wa, float wb, float wc);
 
 /* Voxel world state, laid out exactly as the CUDA path lays it out in device memory (struct of arrays). */
 typedef struct {

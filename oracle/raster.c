@@ -104,7 +104,7 @@ int orc_raster_gbuffer(const orc_scene *s, const float *F, uint32_t W, uint32_t 
         if (!(w >= near)) continue;
         float depth = near / w;
         uint64_t k = ((uint64_t)ubits(depth) << 32) | (uint64_t)(0xffffffffu - t);
-        if (k > key[q]) key[q] = k;
+        if (k > key[q] && orc_raster_alpha_ok(s, i, (1.0f - uu) - vv, uu, vv)) key[q] = k;   /* masked: discard */
       }
   }
   for (size_t q = 0; q < npx; q++) {

@@ -8,7 +8,8 @@
  *     (inclusive edge functions at texel centres, depth interpolated with the edge weights, the Vulkan depth-bias terms
  *     r = 2^(e - 23) of the largest |z| and the larger window-space slope) are this build's definition, shared with
  *     the CUDA kernels.  The stored depth is the smallest biased depth, so the result does not depend on the order in
- *     which triangles are drawn.
+ *     which triangles are drawn.  Alpha-masked materials: untextured, every fragment kept or none (the factor's alpha
+ *     against the cutoff); textured, each texel by the texture at level 0 at its barycentric weights times the factor.
  *   - shadowCoord / shadowTap (src/core/frame.ts:35-52): layer 0 (lightViewProj, bias shadow.y) where x projects inside
  *     it, else layer 1 (lightViewProjFar, bias shadow.z) when the frame has two layers (shadow.x >= 1.5; the
  *     camera-following layers of instanced worlds, lighting.ts:93-125), else lit; textureSampleCompareLevel with a
@@ -58,7 +59,9 @@ static void render_layer(const orc_scene *s, const float *m, uint32_t S, float *
   for (uint32_t t = 0; t < nd * ni; t++) {
     const uint32_t *idx = &s->tri[4u * (t % nd)];
     const orc_material *mt = &s->mats[idx[3]];
-    if ((mt->flags & 1u) != 0u && mt->base_color[3] < mt->alpha_cutoff) continue;   /* every fragment discarded */
+    /* alpha-masked: untextured, every fragment discarded or none; textured, each texel tested */
+    int per_texel = (mt->flags & 1u) != 0u && orc_tex_layer_of(s, mt) != 0u;
+    if (!per_texel && (mt->flags & 1u) != 0u && mt->base_color[3] < mt->alpha_cutoff) continue;
     v3 o = s->draw_inst ? fromf(s->draw_inst + 4u * (t / nd)) : V(0.0f, 0.0f, 0.0f);
     v3 pa = fromf(&s->pos[3u * idx[0]]), pb = fromf(&s->pos[3u * idx[1]]), pc = fromf(&s->pos[3u * idx[2]]);
     if (s->draw_inst) { pa = add(pa, o); pb = add(pb, o); pc = add(pc, o); }
@@ -95,6 +98,7 @@ static void render_layer(const orc_scene *s, const float *m, uint32_t S, float *
         if (!(sum != 0.0f)) continue;
         float z = ((w0 * c0.z + w1 * c1.z) + w2 * c2.z) / sum;
         if (!(z >= 0.0f && z <= 1.0f)) continue;   /* depth clipping */
+        if (per_texel && !orc_raster_alpha_ok(s, idx, w0 / sum, w1 / sum, w2 / sum)) continue;
         float zb = z + bias;
         float *d = &map[(size_t)j * S + (size_t)i];
         if (zb < *d) *d = zb;

@@ -87,3 +87,17 @@ void orc_tri_uv(const orc_scene *s, const uint32_t idx[3], float wx, float wy, f
   uv[0] = (a[0] * wx + b[0] * wy) + c[0] * wz;
   uv[1] = (a[1] * wx + b[1] * wy) + c[1] * wz;
 }
+
+int orc_raster_alpha_ok(const orc_scene *s, const uint32_t idx[4], float wa, float wb, float wc) {
+  const orc_material *m = &s->mats[idx[3]];
+  if ((m->flags & 1u) == 0u) return 1;
+  float a = m->base_color[3];
+  uint32_t layer = orc_tex_layer_of(s, m);
+  if (layer) {
+    float uv[2], t[4];
+    orc_tri_uv(s, idx, wa, wb, wc, uv);
+    orc_tex_sample(s, layer, uv[0], uv[1], 0u, t);
+    a = t[3] * m->base_color[3];
+  }
+  return !(a < m->alpha_cutoff);
+}

@@ -91,7 +91,8 @@ struct gi_scene {
   uint32_t rigid_first = 0, rigid_per = 0, rigid_n = 0;
   SceneDev dev() const {
     SceneDev s;
-    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+    s.pos = pos; s.nrm = nrm; s.tri = tri; s.mats = mats; s.ntris = ntris; s.nverts = nverts; s.nmats = nmats;
+    s.masked = (mat_flags & 1u) ? 1u : 0u;
     s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
     s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
     s.uv = uv; s.tex = tex;

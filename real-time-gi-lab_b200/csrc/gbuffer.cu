@@ -87,8 +87,8 @@ __device__ __forceinline__ bool screen_box(const float *__restrict__ F, uint32_t
 
 // The key of (pixel ray, triangle): depth bits << 32 | ~t, or 0 when the ray misses or the hit is nearer than near
 __device__ __forceinline__ unsigned long long pixel_key(const float *__restrict__ F, f3 eye, f3 dir, f3 a, f3 e1, f3 e2,
-                                                        uint32_t t) {
-  float tt, uu, vv;
+                                                        uint32_t t, float &uu, float &vv) {
+  float tt;
   if (!ray_tri(eye, dir, a, e1, e2, tt, uu, vv)) return 0ull;
   float w = tt * dot(dir, mk(F[F_FWD], F[F_FWD + 1], F[F_FWD + 2]));
   float near = F[F_EYE + 3];
@@ -252,7 +252,8 @@ __device__ __forceinline__ uint32_t block_min_256(uint32_t x, uint32_t *ws) {
 }
 
 // One block per tile: the tile's list, then the overflow list, in chunks of 256 sorted by depth bound (largest
-// first); then the winner's depth and normal
+// first), fragments of alpha-masked materials whose alpha falls below the cutoff left out; then the winner's depth,
+// normal and style tag
 __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__restrict__ F, uint32_t W, uint32_t H,
                                                   uint32_t tiles_x, RasterDev rd, float *depth, uint2 *normal,
                                                   uint8_t *tag) {
@@ -311,9 +312,16 @@ __global__ void __launch_bounds__(256) k_rs_tiles(SceneDev s, const float *__res
         float4 e1 = se1[j], e2 = se2[j];
         uint32_t bx = __float_as_uint(e1.w), by = __float_as_uint(e2.w);
         if (x < (bx & 0xffffu) || x > (bx >> 16) || y < (by & 0xffffu) || y > (by >> 16)) continue;
+        float uu = 0.0f, vv = 0.0f;
         unsigned long long k = pixel_key(F, eye, dir, mk(a.x, a.y, a.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z),
-                                         sval[j]);
-        if (k > best) { best = k; my_depth = (uint32_t)(k >> 32); }
+                                         sval[j], uu, vv);
+        if (k > best) {
+          if (s.masked) {   // an alpha-masked fragment is discarded (gbuffer.ts:94)
+            f3 off;
+            if (!raster_alpha_ok(s, drawn_tri(s, sval[j], off), (1.0f - uu) - vv, uu, vv)) continue;
+          }
+          best = k; my_depth = (uint32_t)(k >> 32);
+        }
       }
       __syncthreads();
     }

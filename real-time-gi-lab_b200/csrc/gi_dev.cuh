@@ -193,7 +193,7 @@ struct SceneDev {
   const float4 *nrm;       // xyz, w = 0
   const uint4 *tri;        // i0, i1, i2, material
   const gi_material *mats;
-  uint32_t ntris, nverts, nmats, pad;
+  uint32_t ntris, nverts, nmats, masked;   // masked: some material has the alpha-mask flag
   // World work items of the voxel build (world.ts, voxel.ts:270-288); items NULL: every row once, instance 0.
   // items: (first thread, source, instance, first level), the source an offset into lists or 0x80000000 | first row;
   // a triangle's key is instance * key_stride + row, moved by inst[instance]
@@ -236,6 +236,19 @@ __device__ __forceinline__ float4 tex_sample(const SceneDev &s, uint32_t layer1,
 __device__ __forceinline__ float2 tri_uv(const SceneDev &s, uint4 idx, float wx, float wy, float wz) {
   const float2 a = s.uv[idx.x], b = s.uv[idx.y], c = s.uv[idx.z];
   return make_float2((a.x * wx + b.x * wy) + c.x * wz, (a.y * wx + b.y * wy) + c.y * wz);
+}
+// The rasters' alpha test (gbuffer.ts:94 and the shadow pass's discard): a masked material's alpha at barycentric
+// weights (wa, wb, wc) — the texture at level 0 times the factor, or the factor alone untextured — against the cutoff
+__device__ __forceinline__ bool raster_alpha_ok(const SceneDev &s, uint4 idx, float wa, float wb, float wc) {
+  const gi_material &m = s.mats[idx.w];
+  if ((m.flags & 1u) == 0u) return true;
+  float a = m.base_color[3];
+  const uint32_t layer = tex_layer_of(s, m);
+  if (layer) {
+    const float2 uv = tri_uv(s, idx, wa, wb, wc);
+    a = tex_sample(s, layer, uv.x, uv.y, 0u).w * m.base_color[3];
+  }
+  return !(a < m.alpha_cutoff);
 }
 
 // Drawn triangle t of a raster: row t of the table, or with drawn instances (inst set) row t mod key_stride of

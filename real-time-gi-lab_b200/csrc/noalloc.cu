@@ -143,7 +143,7 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   SceneDev s;
   s.pos = reinterpret_cast<const float4 *>(pos4); s.nrm = reinterpret_cast<const float4 *>(nrm4);
   s.tri = reinterpret_cast<const uint4 *>(tri4); s.mats = mats;
-  s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.pad = 0;
+  s.ntris = ntris; s.nverts = nverts; s.nmats = nmats; s.masked = 0;
   s.items = nullptr; s.lists = nullptr; s.inst = nullptr;
   s.nitems = 0; s.threads = ntris; s.key_stride = ntris; s.key_limit = ntris;
   s.uv = nullptr; s.tex = nullptr;   // no textures here: the base colour is the factor

@@ -11,6 +11,9 @@
 //            texel (Vulkan's depth-bias terms for a float depth buffer)
 //   stored   the smallest z + bias over the covering triangles, 1 where none; so the result does not depend on the
 //            order in which the triangles are drawn
+//   alpha    an alpha-masked material whose factor's alpha is below the cutoff draws nothing untextured; textured, a
+//            texel is left out where the texture at level 0 at its barycentric weights w_k / (w0 + w1 + w2), times
+//            the factor, falls below the cutoff
 //
 // Work: k_sm_setup gives every triangle its clip record, texel box and the number of 128-texel chunks of that box
 // (prefix within blocks of 256 triangles); k_sm_scan turns the block sums into offsets and the chunk total; warps of
@@ -67,7 +70,9 @@ __global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__res
     f3 off;
     uint4 idx = drawn_tri(s, t, off);
     const gi_material &mt = s.mats[idx.w];
-    if (!((mt.flags & 1u) != 0u && mt.base_color[3] < mt.alpha_cutoff)) {
+    // an alpha-masked material: untextured, every fragment or none; textured, each texel tested (record word 12)
+    const bool per_texel = (mt.flags & 1u) != 0u && tex_layer_of(s, mt) != 0u;
+    if (per_texel || !((mt.flags & 1u) != 0u && mt.base_color[3] < mt.alpha_cutoff)) {
       f3 a = ld3(s.pos[idx.x]), b = ld3(s.pos[idx.y]), c = ld3(s.pos[idx.z]);
       if (s.inst) { a = a + off; b = b + off; c = c + off; }
       f3 c0 = light_clip(M, a), c1 = light_clip(M, b), c2 = light_clip(M, c);
@@ -92,6 +97,7 @@ __global__ void __launch_bounds__(256) k_sm_setup(SceneDev s, const float *__res
           sr.rec[4u * t] = make_float4(c0.x, c0.y, c0.z, bias);
           sr.rec[4u * t + 1u] = make_float4(c1.x, c1.y, c1.z, __uint_as_float((uint32_t)i0 | ((uint32_t)j0 << 16)));
           sr.rec[4u * t + 2u] = make_float4(c2.x, c2.y, c2.z, __uint_as_float(bw | (bh << 16)));
+          sr.rec[4u * t + 3u] = make_float4(per_texel ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
         }
       }
     }
@@ -121,7 +127,7 @@ __global__ void __launch_bounds__(256) k_sm_scan(uint32_t nblk, ShadowRaster sr)
 
 __device__ __forceinline__ uint32_t sm_first(const ShadowRaster &sr, uint32_t t) { return sr.pre[t] + sr.sums[t >> 8]; }
 
-__global__ void __launch_bounds__(256) k_sm_raster(uint32_t ntris, uint32_t S, ShadowRaster sr) {
+__global__ void __launch_bounds__(256) k_sm_raster(SceneDev s, uint32_t ntris, uint32_t S, ShadowRaster sr) {
   grid_dep_wait();
   const uint32_t lane = threadIdx.x & 31u;
   const uint32_t nwarps = gridDim.x * (blockDim.x >> 5), w0 = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -143,6 +149,9 @@ __global__ void __launch_bounds__(256) k_sm_raster(uint32_t ntris, uint32_t S, S
     const float4 ra = sr.rec[4u * t], rb = sr.rec[4u * t + 1u], rc = sr.rec[4u * t + 2u];
     const f3 c0 = mk(ra.x, ra.y, ra.z), c1 = mk(rb.x, rb.y, rb.z), c2 = mk(rc.x, rc.y, rc.z);
     const float bias = ra.w;
+    const bool per_texel = sr.rec[4u * t + 3u].x != 0.0f;
+    f3 toff;
+    const uint4 tidx = per_texel ? drawn_tri(s, t, toff) : make_uint4(0u, 0u, 0u, 0u);
     const uint32_t ij = __float_as_uint(rb.w), wh = __float_as_uint(rc.w);
     const int i0 = (int)(ij & 0xffffu), j0 = (int)(ij >> 16), bw = (int)(wh & 0xffffu), bh = (int)(wh >> 16);
     const int area = bw * bh;
@@ -164,7 +173,7 @@ __global__ void __launch_bounds__(256) k_sm_raster(uint32_t ntris, uint32_t S, S
           float sum = (e0 + e1) + e2;
           if (sum != 0.0f) {
             float z = ((e0 * c0.z + e1 * c1.z) + e2 * c2.z) / sum;
-            if (z >= 0.0f && z <= 1.0f) {
+            if (z >= 0.0f && z <= 1.0f && (!per_texel || raster_alpha_ok(s, tidx, e0 / sum, e1 / sum, e2 / sum))) {
               uint32_t zb = __float_as_uint(z + bias);
               uint32_t *d = reinterpret_cast<uint32_t *>(sr.map) + (size_t)j * S + (size_t)i;
               if (zb < *d) atomicMin(d, zb);
@@ -187,6 +196,6 @@ cudaError_t gi_launch_shadow(const SceneDev &s, const float *matrix_dev, uint32_
   uint32_t nblk = s.ntris ? (s.ntris + 255u) / 256u : 1u;
   GI_TRY(gi_launch(k_sm_setup, nblk, 256, st, s, matrix_dev, S, sr));
   GI_TRY(gi_launch(k_sm_scan, 1, 256, st, nblk, sr));
-  if (s.ntris) GI_TRY(gi_launch(k_sm_raster, sm_count * 8u, 256, st, s.ntris, S, sr));
+  if (s.ntris) GI_TRY(gi_launch(k_sm_raster, sm_count * 8u, 256, st, s, s.ntris, S, sr));
   return cudaGetLastError();
 }

@@ -67,3 +67,27 @@ def test_masked_panels_and_textured_albedo_in_the_rebuild():
     alb = tex["attr"][0: nv * 4: 4]
     albp = plain["attr"][0: int(plain["hdr"][1]) * 4: 4]
     assert len(np.unique(alb & 0xffffff)) > len(np.unique(albp & 0xffffff))
+
+
+def test_rasters_cut_the_holes():
+    """The G-buffer and the shadow map leave out masked fragments: the lattice panels' holes show what is behind
+    them; an untextured masked material whose factor's alpha is below the cutoff draws nothing at all."""
+    from rtgi import frame as fr
+    s = scenes.textured_scene()
+    W, H = 160, 120
+    bmin, bmax = fr.scene_bounds(s.positions)
+    F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, cascades=2,
+                                     light_view_proj=fr.scene_sun_view_proj(bmin, bmax, s.sun_dir),
+                                     shadow_bias=fr.SHADOW_BIAS))
+    solid = dataclasses.replace(s, textures=None, uvs=None)
+    d_tex, _, tri_tex = bind.raster_gbuffer(s, F, W, H)
+    d_solid, _, tri_solid = bind.raster_gbuffer(solid, F, W, H)
+    panel = len(s.materials) - 1
+    on_panel = lambda tri: (tri != 0xffffffff) & (s.tri[np.where(tri == 0xffffffff, 0, tri), 3] == panel)
+    assert on_panel(tri_solid).sum() > on_panel(tri_tex).sum() > 0
+    m_tex, m_solid = bind.shadow_render(s, F, 256), bind.shadow_render(solid, F, 256)
+    assert (m_tex != m_solid).any() and (m_tex >= m_solid).all()   # holes let the depth fall back further
+    clear = [dataclasses.replace(m, base_color=(0.9, 0.9, 0.9, 0.2)) if m.name == "panel" else m for m in s.materials]
+    gone = dataclasses.replace(solid, materials=clear)
+    _, _, tri_gone = bind.raster_gbuffer(gone, F, W, H)
+    assert on_panel(tri_gone).sum() == 0
