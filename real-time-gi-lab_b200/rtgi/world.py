@@ -94,6 +94,7 @@ def with_world(scene, instances: Sequence[Sequence[float]], v0: float, levels: i
     keys = sorted(by_chunk)
     lod_pos: List[float] = []
     lod_nrm: List[float] = []
+    lod_uv: List[int] = []        # per cluster vertex the source vertex of its uv
     lod_rows: List[int] = []
     first_row = T
     pending: List[list] = [[] for _ in range(levels)]
@@ -148,6 +149,7 @@ def with_world(scene, instances: Sequence[Sequence[float]], v0: float, levels: i
                         bd, best = dd, v
                 lod_pos.extend(p)
                 lod_nrm.extend([x / l for x in cl["nrm"]] if l > 1e-12 else [N[best * 3], N[best * 3 + 1], N[best * 3 + 2]])
+                lod_uv.append(best)   # the cluster's uv: the vertex nearest the mean's (world.ts:124, 137)
             seen = set()
             mine = []
             for i, t in enumerate(tris):
@@ -182,7 +184,11 @@ def with_world(scene, instances: Sequence[Sequence[float]], v0: float, levels: i
                           np.asarray(lod_nrm, np.float64).reshape(-1, 3).astype(np.float32)])
     lod_table = np.asarray(lod_rows, np.uint32).reshape(-1, 4)
     tri = np.concatenate([np.asarray(scene.tri, np.uint32).reshape(-1, 4), lod_table])
-    out = dataclasses.replace(scene, positions=pos, normals=nrm, tri=tri)
+    extra = {}
+    if getattr(scene, "uvs", None) is not None:
+        uv0 = np.asarray(scene.uvs, np.float32).reshape(-1, 2)
+        extra["uvs"] = np.concatenate([uv0, uv0[np.asarray(lod_uv, np.int64)].reshape(-1, 2)]).astype(np.float32)
+    out = dataclasses.replace(scene, positions=pos, normals=nrm, tri=tri, **extra)
     world = World(inst, T, V0, v0, levels, chunks, V0, nv, lod_table, rows=int(tri.shape[0]))
     off = 0
     for ch in chunks:

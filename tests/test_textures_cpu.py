@@ -91,3 +91,14 @@ def test_rasters_cut_the_holes():
     gone = dataclasses.replace(solid, materials=clear)
     _, _, tri_gone = bind.raster_gbuffer(gone, F, W, H)
     assert on_panel(tri_gone).sum() == 0
+
+
+def test_world_clusters_carry_uvs():
+    """with_world's clustered vertices take the uv of the member vertex nearest their mean (world.ts:124, 137)."""
+    from rtgi import world as W
+    s = scenes.textured_scene()
+    s2, w = W.with_world(s, [(0, 0, 0), (12, 0, 0)], 0.08, 3)
+    assert s2.uvs.shape == (s2.positions.shape[0], 2)
+    assert np.array_equal(s2.uvs[: s.positions.shape[0]], s.uvs)
+    extra = s2.uvs[s.positions.shape[0]:]
+    assert len(extra) > 0 and set(map(tuple, extra)) <= set(map(tuple, s.uvs))
