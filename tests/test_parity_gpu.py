@@ -215,14 +215,30 @@ def test_irr16_is_the_rounded_f32_solve(ctx):
 
 
 def test_walk_length_order_parity(ctx):
-    """The config-1 solve traced in walk-length order (trace_order 2): three solves, the first in the order of the
-    initial keys, the next two in the order of the previous walks; the last one's hits, traced and
-    merged atlas and irradiance bit for bit with the oracle, and every ray traced once (the DDA counters equal the
-    atlas order's)."""
+    """The config-1 solve traced in walk-length order (trace_order 2): three solves of one frame (the first in the
+    order of the initial keys, the next in the order of the previous walks), then a frame with the camera moved (the
+    keys of the previous frame's rays, which now walk elsewhere); the last solve of each frame checked bit for bit
+    against the oracle — hits, traced and merged atlas, irradiance — and every ray traced once (the DDA counters of
+    the atlas order)."""
+    import dataclasses
+    from rtgi import frame as fr, scenes as sc
     case = gi_cases.config1()
+    cam = case.scene.camera
+    cam2 = sc.Camera(tuple(a + b for a, b in zip(cam.eye, (0.12, 0.0, -0.08))),
+                     tuple(a + b for a, b in zip(cam.target, (0.3, 0.0, 0.0))), cam.fov_y_deg, cam.near)
+    F2 = gi_cases._frame(dataclasses.replace(case.scene, camera=cam2), case.width, case.height, case.rc,
+                         sun_e=case.scene.sun_e, sky=case.scene.sky, shadow=True)
+    # the same frame naming the first camera as the previous view
+    F2p = fr.pack_frame(fr.FrameParams(cam=cam2, width=case.width, height=case.height, sun_dir=case.scene.sun_dir,
+                                       sun_e=case.scene.sun_e, sky=case.scene.sky, cascades=case.rc.cascades,
+                                       P=case.rc.P, s_min=case.rc.sMin, lift=case.rc.lift,
+                                       light_view_proj=F2[64:80].tolist(), shadow_bias=(float(F2[157]), float(F2[158])),
+                                       prev_cam=cam, prev_valid=True))
+    assert np.array_equal(F2p[:32], F2[:32]) and int(F2p.view(np.uint32)[118]) == 1
     sg = gpu.SceneGpu(ctx, case.scene)
     vw = gpu.VoxWorld(sg, case.vox)
     rc = gpu.Rc(ctx, case.rc, case.width, case.height)
+    got = []
     try:
         rc.set_frame(case.frame)
         rc.render_gbuffer(sg)
@@ -234,21 +250,31 @@ def test_walk_length_order_parity(ctx):
         ref_counts = rc.read_counts()
         rc.set_tuning(trace_order=2, trace_rays=2)
         rc.set_debug_hits(True)
-        for _ in range(3):
+        for f, F in enumerate((case.frame, case.frame, case.frame, F2p)):
+            if f == 3:
+                rc.set_frame(F)
+                rc.render_gbuffer(sg)
+                vw.update(cam2.eye)
             rc.solve(vw)
-        counts = rc.read_counts()
-        g = {"hits": rc.read_buffer(_lib.GI_RC_HITS).view(np.uint32).reshape(-1, 4),
-             "rad_traced": rc.read_atlas(_lib.GI_RC_RAD_TRACED), "rad": rc.read_atlas(_lib.GI_RC_RAD),
-             "irr": rc.read_irradiance()}
-        depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width)
-        normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4)
+            if f in (2, 3):
+                got.append({"counts": rc.read_counts(),
+                            "hits": rc.read_buffer(_lib.GI_RC_HITS).view(np.uint32).reshape(-1, 4),
+                            "rad_traced": rc.read_atlas(_lib.GI_RC_RAD_TRACED), "rad": rc.read_atlas(_lib.GI_RC_RAD),
+                            "irr": rc.read_irradiance(), "F": F, "eye": cam.eye if f == 2 else cam2.eye,
+                            "depth": rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(case.height, case.width),
+                            "normal": rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4)})
         shadow = rc.read_shadow()
     finally:
         for h in (rc, vw, sg):
             h.destroy()
-    assert np.array_equal(counts, ref_counts), "DDA counters differ from the atlas order's"
-    st, o = run_oracle(case, depth, normal.astype(np.float32), shadow)
-    assert np.array_equal(g["hits"], o["hit"]), "DDA hits differ"
-    _close(g["rad_traced"], o["rad_traced"], 1e-4, "traced radiance")
-    _close(g["rad"], o["rad"], 1e-4, "merged atlas")
-    _close(g["irr"], o["irr"], 1e-4, "irradiance")
+    assert np.array_equal(got[0]["counts"], ref_counts), "DDA counters differ from the atlas order's"
+    v = case.vox
+    for g in got:
+        st = bind.vox_build(case.scene, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, g["eye"])
+        bind.vox_sun(st, g["F"], shadow)
+        lay = dict(gi_cases.configs.cascade_layout(case.rc, case.width, case.height))
+        o = bind.rc_solve(st, lay, g["F"], g["depth"], g["normal"].astype(np.float32), want_hit=True)
+        assert np.array_equal(g["hits"], o["hit"]), "DDA hits differ"
+        _close(g["rad_traced"], o["rad_traced"], 1e-4, "traced radiance")
+        _close(g["rad"], o["rad"], 1e-4, "merged atlas")
+        _close(g["irr"], o["irr"], 1e-4, "irradiance")
