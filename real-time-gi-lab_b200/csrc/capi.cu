@@ -76,6 +76,7 @@ struct gi_scene {
   gi_material *mats = nullptr;
   uint32_t nverts = 0, ntris = 0, nmats = 0;
   uint32_t mat_flags = 0;    // OR of the materials' flags (4 toon, 8 object: the G-buffer raster writes style tags)
+  uint64_t gen = 0;          // bumped when a buffer or a count a captured graph holds is replaced
   float2 *uv = nullptr;      // base colour textures (gi_scene_set_textures): a uv per vertex, every layer's mip chain
   float4 *tex = nullptr;
   uint32_t tex_size = 0, tex_levels = 0, tex_layers = 0, tex_layer_texels = 0;
@@ -170,6 +171,7 @@ struct gi_rc {
   cudaGraphExec_t graph = nullptr;   // one captured gi_solve (gi_rc_graph_capture)
   gi_vox *graph_vox = nullptr;
   uint64_t graph_items_gen = 0;      // the voxel world's work items the graph was captured with
+  uint64_t graph_scene_gen = 0;      // its scene's gen at the capture
   float *shadow = nullptr;           // gi_rc_render_shadow: shadow_layers x shadow_size^2 depths
   uint32_t shadow_size = 0, shadow_layers = 0;
   uint32_t frame_layers = 1;         // the last frame's shadow.x (1, or 2 for a world's camera-following layers)
@@ -340,6 +342,7 @@ int gi_scene_set_textures(gi_scene *s, const uint8_t *rgba8, uint32_t size, uint
   for (uint32_t n = size; n >= 1u; n >>= 1) { levels++; per += n * n; if (n == 1u) break; }
   cudaFree(s->uv); cudaFree(s->tex);
   s->uv = nullptr; s->tex = nullptr; s->tex_size = s->tex_levels = s->tex_layers = s->tex_layer_texels = 0;
+  s->gen++;
   float lut[256];
   srgb_table(lut);
   uint8_t *raw = nullptr;
@@ -359,6 +362,7 @@ int gi_scene_set_textures(gi_scene *s, const uint8_t *rgba8, uint32_t size, uint
   }
   cudaFree(raw); cudaFree(dlut);
   s->tex_size = size; s->tex_levels = levels; s->tex_layers = layers; s->tex_layer_texels = per;
+  s->gen++;
   return GI_OK;
 }
 
@@ -414,6 +418,7 @@ int gi_scene_rigid_define(gi_scene *s, uint32_t first, uint32_t verts_per_object
   cudaFree(s->rigid_rest); cudaFree(s->rigid_m);
   s->rigid_rest = rest; s->rigid_m = m;
   s->rigid_first = first; s->rigid_per = verts_per_object; s->rigid_n = n_objects;
+  s->gen++;
   return GI_OK;
 }
 
@@ -618,6 +623,7 @@ static int ensure_raster_scratch(gi_scene *s, uint64_t n, const char *what) {
   cudaFree(s->raster_over);
   s->raster_rec = rec; s->raster_ntile = ntile; s->raster_pre = pre; s->raster_sums = sums; s->raster_over = over;
   if (list) { cudaFree(s->raster_list); s->raster_list = list; s->raster_cap = cap; }
+  s->gen++;
   s->raster_tris = (uint32_t)n;
   return GI_OK;
 }
@@ -628,6 +634,7 @@ int gi_scene_set_draw_count(gi_scene *s, uint32_t count) {
   int st = ensure_raster_scratch(s, (uint64_t)count * s->draw_ninst, "gi_scene_set_draw_count");
   if (st) return st;
   s->ndraw = count;
+  s->gen++;
   return GI_OK;
 }
 
@@ -636,6 +643,7 @@ int gi_scene_set_static_count(gi_scene *s, uint32_t count) {
   if (count > s->ntris) return fail(GI_ERR_INVALID, "gi_scene_set_static_count: %u of %u rows", count, s->ntris);
   s->static_tris = count == s->ntris ? 0u : count;
   if (count == 0 && s->ntris) s->static_tris = 0xffffffffu;   // every row dynamic: the rebuild reads none
+  s->gen++;
   return GI_OK;
 }
 
@@ -650,6 +658,7 @@ int gi_scene_set_draw_instances(gi_scene *s, const float *offsets, uint32_t n) {
     cudaFree(s->draw_inst);
     s->draw_inst = nullptr;
     s->draw_ninst = 1;
+    s->gen++;
     return GI_OK;
   }
   int st = ensure_raster_scratch(s, (uint64_t)s->ndraw * n, "gi_scene_set_draw_instances");
@@ -665,6 +674,7 @@ int gi_scene_set_draw_instances(gi_scene *s, const float *offsets, uint32_t n) {
   cudaFree(s->draw_inst);
   s->draw_inst = d;
   s->draw_ninst = n;
+  s->gen++;
   return GI_OK;
 }
 
@@ -746,6 +756,7 @@ int gi_scene_set_raster_capacity(gi_scene *s, uint32_t entries) {
   cudaFree(s->raster_list);   // synchronises with work still using the old list
   s->raster_list = list;
   s->raster_cap = entries;
+  s->gen++;
   return GI_OK;
 }
 
@@ -1180,6 +1191,7 @@ int gi_rc_graph_capture(gi_rc *r, gi_vox *v, void *stream) {
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture: instantiate"); }
   r->graph_vox = v;
   r->graph_items_gen = v->items_gen;
+  r->graph_scene_gen = v->scene->gen;
   return GI_OK;
 }
 
@@ -1212,6 +1224,7 @@ int gi_rc_graph_capture_frame(gi_rc *r, gi_vox *v, gi_scene *sc, void *irr_out, 
   if (e != cudaSuccess) { r->graph = nullptr; return cuda_fail(e, "gi_rc_graph_capture_frame: instantiate"); }
   r->graph_vox = v;
   r->graph_items_gen = v->items_gen;
+  r->graph_scene_gen = v->scene->gen;
   return GI_OK;
 }
 
@@ -1220,6 +1233,9 @@ int gi_rc_graph_launch(gi_rc *r, void *stream) {
   if (!r->graph) return fail(GI_ERR_STATE, "gi_rc_graph_launch: no graph captured");
   if (r->graph_vox && r->graph_vox->items_gen != r->graph_items_gen)
     return fail(GI_ERR_STATE, "gi_rc_graph_launch: the voxel world's work items changed since the capture; capture again");
+  if (r->graph_vox && r->graph_vox->scene->gen != r->graph_scene_gen)
+    return fail(GI_ERR_STATE, "gi_rc_graph_launch: the scene's textures, rigid objects, draw counts or raster buffers "
+                              "changed since the capture; capture again");
   if (r->gen != r->graph_gen)
     return fail(GI_ERR_STATE, "gi_rc_graph_launch: the shadow map, bounce volume or dynamic layer changed since the "
                               "capture; capture again");
@@ -1247,6 +1263,7 @@ struct gi_batch {
   VoxDev *d_vox = nullptr;
   uint32_t *d_pre = nullptr;
   uint64_t *gens = nullptr;   // each rc's gen at the capture
+  uint64_t *sgens = nullptr;  // each voxel world's scene gen at the capture
 };
 
 static void free_batch(gi_batch *b) {
@@ -1257,7 +1274,7 @@ static void free_batch(gi_batch *b) {
   }
   if (b->start) cudaEventDestroy(b->start);
   cudaFree(b->d_rc); cudaFree(b->d_vox); cudaFree(b->d_pre);
-  delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done; delete[] b->gens;
+  delete[] b->rcs; delete[] b->voxes; delete[] b->streams; delete[] b->done; delete[] b->gens; delete[] b->sgens;
 }
 
 int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32_t n, gi_batch **out) {
@@ -1281,7 +1298,8 @@ int gi_batch_create(gi_ctx *ctx, gi_rc *const *rcs, gi_vox *const *voxes, uint32
   b->streams = new (std::nothrow) cudaStream_t[n]();
   b->done = new (std::nothrow) cudaEvent_t[n]();
   b->gens = new (std::nothrow) uint64_t[n]();
-  if (!b->rcs || !b->voxes || !b->streams || !b->done || !b->gens) { free_batch(b); delete b; return fail(GI_ERR_OOM, "gi_batch_create: host allocation"); }
+  b->sgens = new (std::nothrow) uint64_t[n]();
+  if (!b->rcs || !b->voxes || !b->streams || !b->done || !b->gens || !b->sgens) { free_batch(b); delete b; return fail(GI_ERR_OOM, "gi_batch_create: host allocation"); }
   b->n = n;
   cudaError_t e = cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming);
   for (uint32_t i = 0; i < n && e == cudaSuccess; i++) {
@@ -1323,7 +1341,7 @@ int gi_batch_capture(gi_batch *b, void *stream) {
   if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture"); }
   if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture: end");
   e = cudaGraphInstantiate(&b->graph, g, 0);
-  for (uint32_t i = 0; i < b->n; i++) b->gens[i] = b->rcs[i]->gen;
+  for (uint32_t i = 0; i < b->n; i++) { b->gens[i] = b->rcs[i]->gen; b->sgens[i] = b->voxes[i]->scene->gen; }
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture: instantiate"); }
   return GI_OK;
@@ -1416,7 +1434,7 @@ int gi_batch_capture_passes(gi_batch *b, void *stream) {
   if (e != cudaSuccess) { if (g) cudaGraphDestroy(g); return cuda_fail(e, "gi_batch_capture_passes"); }
   if (e2 != cudaSuccess) return cuda_fail(e2, "gi_batch_capture_passes: end");
   e = cudaGraphInstantiate(&b->graph, g, 0);
-  for (uint32_t i = 0; i < b->n; i++) b->gens[i] = b->rcs[i]->gen;
+  for (uint32_t i = 0; i < b->n; i++) { b->gens[i] = b->rcs[i]->gen; b->sgens[i] = b->voxes[i]->scene->gen; }
   cudaGraphDestroy(g);
   if (e != cudaSuccess) { b->graph = nullptr; return cuda_fail(e, "gi_batch_capture_passes: instantiate"); }
   return GI_OK;
@@ -1426,6 +1444,8 @@ int gi_batch_launch(gi_batch *b, void *stream) {
   if (!b) return fail(GI_ERR_INVALID, "gi_batch_launch: NULL batch");
   if (!b->graph) return fail(GI_ERR_STATE, "gi_batch_launch: no graph captured");
   for (uint32_t i = 0; i < b->n; i++) {
+    if (b->voxes[i]->scene->gen != b->sgens[i])
+      return fail(GI_ERR_STATE, "gi_batch_launch: solve %u's scene changed its buffers since the capture; capture again", i);
     if (b->rcs[i]->gen != b->gens[i])
       return fail(GI_ERR_STATE, "gi_batch_launch: solve %u's shadow map, bounce volume or dynamic layer changed since "
                                 "the capture; capture again", i);

@@ -62,3 +62,37 @@ def test_textured_scene_parity():
     g0, *_ = _run(dataclasses.replace(s, textures=None, uvs=None))
     assert int(g0["vox"]["hdr"][1]) > nv
     assert not np.array_equal(g0["irr"], g["irr"])
+
+
+def test_graph_refused_after_the_textures_change():
+    """A captured solve holds the scene's buffers: replacing the textures (or a draw count) afterwards makes the replay
+    refuse until the solve is captured again."""
+    s = scenes.textured_scene(16)
+    p = configs.parse_config("screen-8-voxel-f32", {"cascades": 2})
+    v = configs.vox_params(VOX)
+    F = gi_cases._frame(s, 64, 48, p, sun_e=fr.SUN_E, sky=fr.SKY)
+    ctx = gpu.Context(0)
+    sg = gpu.SceneGpu(ctx, s)
+    vw = gpu.VoxWorld(sg, v)
+    rc = gpu.Rc(ctx, p, 64, 48)
+    import torch
+    st = torch.cuda.Stream()
+    try:
+        rc.set_frame(F, st)
+        rc.render_gbuffer(sg, st)
+        vw.update(s.camera.eye)
+        rc.graph_capture(vw, st)
+        rc.graph_launch(st)
+        sg.set_textures(s.textures[::-1].copy(), s.uvs)
+        with pytest.raises(_lib.GiError) as e:
+            rc.graph_launch(st)
+        assert e.value.status == _lib.GI_ERR_STATE
+        rc.graph_capture(vw, st)
+        rc.graph_launch(st)
+        sg.set_draw_count(s.triangle_count - 2)
+        with pytest.raises(_lib.GiError):
+            rc.graph_launch(st)
+        st.synchronize()
+    finally:
+        for h in (rc, vw, sg, ctx):
+            h.destroy()
