@@ -411,6 +411,12 @@ def max_over_ranks(x: float, dist, device) -> float:
     return float(t.item())
 
 
+def rebuild_launches(levels: int) -> int:
+    """Kernels of one voxel rebuild (gi_launch_vox_build): clear, markBricks and its big items, allocBricks, the brick
+    init, voxBits and its big items, reduce (more than one level), allocVoxels, resolveAttr."""
+    return 9 + (1 if levels > 1 else 0)
+
+
 def whole_job_rate(units_per_rank: float, max_seconds: float, world: int) -> float:
     """Units all ranks processed over the slowest rank's time (replicas: weak scaling)."""
     return world * units_per_rank / max_seconds
@@ -605,7 +611,7 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
                       "passes_ms": {k: statistics.median(x) for k, x in b_pass.items()}},
            # voxel rebuild, then clear, registerPixels, the paired compact / relocateVox / registerUp / linkParents
            # launches (2N + 1 with voxel relocation), the trace, a merge per cascade, projectSH, the gather
-           "gpu_launches_per_solve": (11 + (1 if v.levels > 1 else 0)) + 2 + 2 * p.cascades + 1 + 1 + p.cascades + 2}
+           "gpu_launches_per_solve": rebuild_launches(v.levels) + 2 + 2 * p.cascades + 1 + 1 + p.cascades + 2}
     rc.destroy()
     return out
 
@@ -864,7 +870,7 @@ def run_ours(args, rank, world, local_rank):
                             "traffic": traffic, "algorithmic_bytes": alg, "launch_ms": trace_ms},
                "e2e": e2e_out,
                "e2e_variants": e2e_more,
-               "gpu_launches": n_ev * (11 + (1 if v.levels > 1 else 0) + 3 + p.cascades),
+               "gpu_launches": n_ev * (rebuild_launches(v.levels) + 3 + p.cascades),
                "clocks": clk, "wall_s": wall}
     if args.batch > 0:
         bt = run_batched(args, ctx, stream, flush)

@@ -343,6 +343,11 @@ int gi_rc_set_debug_hits(gi_rc *rc, int on);
  * the stages.  The yardstick of the f32/f16/bf16 atlas error.  Needs an F32 atlas with debug hits on (GI_ERR_STATE
  * otherwise); allocates its f64 buffers (32 bytes per ray and per pixel) on the first call.  Stream-ordered. */
 int gi_rc_merge_gather_f64(gi_rc *rc, void *stream);
+/* The same with the atlas storage of the cascades in bit mask f16_cascades rounded to f16 (round to nearest even) and
+ * every stage still in double: their traced intervals as they are read, and (cascades above 0) their merged radiances
+ * as they are stored for the cascade below.  The storage error of a per-cascade f16/f32 atlas apart from the f32
+ * arithmetic; mask 0 is gi_rc_merge_gather_f64.  No counterpart in the reference. */
+int gi_rc_merge_gather_f64_rounded(gi_rc *rc, uint32_t f16_cascades, void *stream);
 /* W*H*4 doubles (rgb, a = 1 valid / 0 background) of the last gi_rc_merge_gather_f64, into host or device memory.
  * Synchronises. */
 int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);

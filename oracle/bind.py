@@ -43,6 +43,8 @@ def lib():
         _lib.orc_lod_for.restype = C.c_int32
         _lib.orc_rc_merge_gather.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_rc_merge_gather_f64.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+        _lib.orc_rc_merge_gather_f64_rounded.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                                                         C.c_void_p]
         _lib.orc_raster_gbuffer.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p]
         _lib.orc_pack4x8unorm.argtypes = [C.c_void_p]
         _lib.orc_pack4x8unorm.restype = C.c_uint32
@@ -313,7 +315,8 @@ def rc_solve(vox: dict, lay: dict, frame: np.ndarray, depth: np.ndarray, normal:
 
 
 def merge_gather_f64(lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np.ndarray, probes: np.ndarray,
-                     rad_traced: np.ndarray) -> np.ndarray:
+                     rad_traced: np.ndarray, f16_cascades: int = 0) -> np.ndarray:
+    """FP64 merge + SH + gather of the traced intervals; f16_cascades: cascades whose atlas storage is rounded to f16."""
     H, W = depth.shape
     ly = layout_struct(lay)
     frame = np.ascontiguousarray(frame, dtype=np.float32)
@@ -323,7 +326,7 @@ def merge_gather_f64(lay: dict, frame: np.ndarray, depth: np.ndarray, normal: np
     rad = np.ascontiguousarray(rad_traced, dtype=np.float32)
     irr = np.zeros((H, W, 4), np.float64)
     g = OrcGbuf(_p(frame), W, H, _p(depth), _p(normal), None)
-    lib().orc_rc_merge_gather_f64(C.byref(ly), C.byref(g), _p(probes), _p(rad), _p(irr))
+    lib().orc_rc_merge_gather_f64_rounded(C.byref(ly), C.byref(g), _p(probes), _p(rad), int(f16_cascades), _p(irr))
     return irr
 
 

@@ -189,6 +189,10 @@ int orc_rc_merge_gather(const orc_layout *ly, const orc_gbuf *g, orc_rc_out *o);
  * rad_in: traced intervals (f32, unmerged).  irr_out: W*H*4 doubles. */
 int orc_rc_merge_gather_f64(const orc_layout *ly, const orc_gbuf *g, const orc_probe *probes, const float *rad_in,
                             double *irr_out);
+/* The same with the atlas storage of the cascades in bit mask f16_cascades rounded to f16 (ties to even): their traced
+ * intervals, and above cascade 0 their merged radiances as the cascade below reads them; every stage in double. */
+int orc_rc_merge_gather_f64_rounded(const orc_layout *ly, const orc_gbuf *g, const orc_probe *probes,
+                                    const float *rad_in, unsigned f16_cascades, double *irr_out);
 
 /* Headless G-buffer: depth (reversed Z, infinite far) and the shading normal (interpolated vertex normal,
  * flipped to the viewer for back faces), one sample at each pixel centre.  normal_out is rgba, w = 0.

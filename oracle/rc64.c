@@ -39,7 +39,21 @@ static void sh_basis(d3 n, double y[9]) {
 
 typedef struct {
   const orc_layout *ly; const orc_gbuf *g; const orc_probe *probes; double *rad; double *sh; double *irr; unsigned c;
+  unsigned f16;   /* cascades whose atlas storage is rounded to f16 */
 } job64;
+
+/* x rounded to the nearest f16 value, ties to even, as a double: 11 significant bits, a quantum of 2^-24 below 2^-14
+ * (subnormals), infinity past 65504.  The scalings by powers of two are exact; nearbyint rounds half to even. */
+static double as_f16(double x) {
+  if (x != x || x == 0.0 || isinf(x)) return x;
+  double a = fabs(x);
+  int e;
+  frexp(a, &e);                     /* a = m 2^e, m in [0.5, 1): the 11-bit significand's quantum is 2^(e - 11) */
+  int q = e - 11 < -24 ? -24 : e - 11;
+  double r = ldexp(nearbyint(ldexp(a, -q)), q);
+  if (r > 65504.0) r = INFINITY;
+  return x < 0.0 ? -r : r;
+}
 
 static void merge64(void *p, uint64_t b, uint64_t e) {
   job64 *j = (job64 *)p;
@@ -92,6 +106,7 @@ static void merge64(void *p, uint64_t b, uint64_t e) {
       }
     }
     rv[0] = rv[0] + rv[3] * up.x; rv[1] = rv[1] + rv[3] * up.y; rv[2] = rv[2] + rv[3] * up.z; rv[3] = 1.0;
+    if (c > 0u && ((j->f16 >> c) & 1u)) { rv[0] = as_f16(rv[0]); rv[1] = as_f16(rv[1]); rv[2] = as_f16(rv[2]); }
   }
 }
 
@@ -167,6 +182,11 @@ static void gather64(void *p, uint64_t b, uint64_t e) {
 
 int orc_rc_merge_gather_f64(const orc_layout *ly, const orc_gbuf *g, const orc_probe *probes, const float *rad_in,
                             double *irr_out) {
+  return orc_rc_merge_gather_f64_rounded(ly, g, probes, rad_in, 0u, irr_out);
+}
+
+int orc_rc_merge_gather_f64_rounded(const orc_layout *ly, const orc_gbuf *g, const orc_probe *probes,
+                                    const float *rad_in, unsigned f16_cascades, double *irr_out) {
   size_t nrad = 0;
   for (unsigned c = 0; c < ly->cascades; c++) {
     size_t end = (size_t)ly->c[c].rad_off + (size_t)ly->c[c].tiles_x * ly->c[c].tiles_y * ly->c[c].res * ly->c[c].res;
@@ -177,7 +197,13 @@ int orc_rc_merge_gather_f64(const orc_layout *ly, const orc_gbuf *g, const orc_p
   double *sh = (double *)malloc((size_t)np0 * 27 * sizeof(double));
   if (!rad || !sh) { free(rad); free(sh); return -1; }
   for (size_t i = 0; i < nrad * 4; i++) rad[i] = rad_in[i];
-  job64 j = {ly, g, probes, rad, sh, irr_out, 0};
+  for (unsigned c = 0; c < ly->cascades; c++) {
+    if (!((f16_cascades >> c) & 1u)) continue;
+    size_t a = 4u * (size_t)ly->c[c].rad_off;
+    size_t n = 4u * (size_t)ly->c[c].tiles_x * ly->c[c].tiles_y * ly->c[c].res * ly->c[c].res;
+    for (size_t i = a; i < a + n; i++) rad[i] = as_f16(rad[i]);
+  }
+  job64 j = {ly, g, probes, rad, sh, irr_out, 0, f16_cascades};
   for (int ci = (int)ly->cascades - 1; ci >= 0; ci--) {
     j.c = (unsigned)ci;
     const orc_casc *L = &ly->c[j.c];

@@ -205,7 +205,7 @@ static void free_scene(gi_scene *s) {
 static void free_vox(gi_vox *v) {
   VoxDev &d = v->dev;
   cudaFree(d.hdr); cudaFree(d.ptr); cudaFree(d.occ); cudaFree(d.base); cudaFree(d.code); cudaFree(d.rep);
-  cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis); cudaFree(d.scan);
+  cudaFree(d.big); cudaFree(d.attr); cudaFree(d.plane); cudaFree(d.sunvis);
   cudaFree(d.vpre); cudaFree(d.work); cudaFree(d.cpre); cudaFree(d.citem); cudaFree(d.look);
   cudaFree(v->w_inst); cudaFree(v->w_lists); cudaFree(v->w_items);
 }
@@ -475,18 +475,16 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
   vox_derived(d);
   d.citem_cap = VOX_CITEM_CAP;
   uint64_t nptr = (uint64_t)p->levels * p->G * p->G * p->G;
-  uint32_t scan_words = (uint32_t)((nptr + 255u) / 256u);   // block sums of the brick allocation, 256 entries each
-  uint32_t vscan = (p->max_bricks + 255u) / 256u;
+  uint32_t scan_words = (uint32_t)((nptr + 255u) / 256u);   // blocks of the brick allocation, 256 entries each
+  uint32_t vscan = (p->max_bricks + 255u) / 256u;             // and of the voxel allocation
   if (vscan > scan_words) scan_words = vscan;
-  uint32_t cscan = 8u * d.big_cap / 256u;   // chunk-prefix block sums of the voxBits big lists
-  if (cscan > scan_words) scan_words = cscan;
   d.scan_cap = scan_words;
   cudaError_t e;
   if ((e = dalloc(&d.hdr, GI_HDR)) || (e = dalloc(&d.ptr, nptr)) || (e = dalloc(&d.occ, (size_t)p->max_bricks * 16u)) ||
       (e = dalloc(&d.base, p->max_bricks)) || (e = dalloc(&d.code, p->max_bricks)) ||
       (e = dalloc(&d.rep, (size_t)p->max_bricks * 512u)) || (e = dalloc(&d.big, (size_t)16u * d.big_cap)) ||
       (e = dalloc(&d.attr, p->max_voxels)) || (e = dalloc(&d.plane, p->max_voxels)) ||
-      (e = dalloc(&d.sunvis, p->max_voxels)) || (e = dalloc(&d.scan, scan_words)) ||
+      (e = dalloc(&d.sunvis, p->max_voxels)) ||
       (e = dalloc(&d.vpre, (size_t)p->max_bricks + 1u)) || (e = dalloc(&d.work, 4)) ||
       (e = dalloc(&d.cpre, (size_t)8u * d.big_cap)) || (e = dalloc(&d.citem, (size_t)VOX_CITEM_CAP)) ||
       (e = dalloc(&d.look, (size_t)scan_words + 1u))) {
@@ -495,7 +493,7 @@ int gi_vox_create(gi_scene *scene, const gi_vox_params *p, gi_vox **out) {
     return cuda_fail(e, "gi_vox_create");
   }
   v->bytes = (GI_HDR + nptr + (uint64_t)p->max_bricks * (16u + 2u + 512u) + (uint64_t)16u * d.big_cap +
-              (uint64_t)p->max_voxels * 6u + scan_words + p->max_bricks + 5u + (uint64_t)8u * d.big_cap +
+              (uint64_t)p->max_voxels * 6u + p->max_bricks + 5u + (uint64_t)8u * d.big_cap +
               VOX_CITEM_CAP + 2u * ((uint64_t)scan_words + 1u)) * 4u;
   memset(v->hdr, 0, sizeof v->hdr);
   *out = v;
@@ -1689,7 +1687,9 @@ int gi_rc_read_buffer(gi_rc *r, int what, void *out, size_t bytes, void *stream)
   return GI_OK;
 }
 
-int gi_rc_merge_gather_f64(gi_rc *r, void *stream) {
+int gi_rc_merge_gather_f64(gi_rc *r, void *stream) { return gi_rc_merge_gather_f64_rounded(r, 0u, stream); }
+
+int gi_rc_merge_gather_f64_rounded(gi_rc *r, uint32_t f16_cascades, void *stream) {
   if (!r) return fail(GI_ERR_INVALID, "gi_rc_merge_gather_f64: NULL rc");
   if (r->world) return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: screen probes only");
   if (r->p.atlas != GI_ATLAS_F32) return fail(GI_ERR_STATE, "gi_rc_merge_gather_f64: needs an F32 atlas");
@@ -1707,7 +1707,7 @@ int gi_rc_merge_gather_f64(gi_rc *r, void *stream) {
     }
   }
   CK(gi_launch_merge_gather_f64(r->dev, reinterpret_cast<const float4 *>(r->rad_traced), r->rad64, r->sh64, r->irr64,
-                                S(stream)), "gi_rc_merge_gather_f64: launch");
+                                f16_cascades, S(stream)), "gi_rc_merge_gather_f64: launch");
   r->have64 = true;
   return GI_OK;
 }

@@ -268,7 +268,7 @@ struct VoxDev {
   float v0;
   uint32_t levels, G, max_bricks, max_voxels, big_cap;
   uint32_t chunk_log2, blocks;   // tuning: cells per big-triangle work item (log2), resident blocks per SM
-  uint32_t citem_cap, scan_cap;  // entries of citem (0: no table); words of scan
+  uint32_t citem_cap, scan_cap;  // entries of citem (0: no table); blocks the chained scans may take
   float vs[8];         // voxel size per level, ldexpf(v0, L) (vox_derived)
   int32_t lim_vox[8], lim_brick[8];   // voxRange's limit f2i(G * size * 8 / cell), voxel and brick cells (vox_derived)
   int32_t origin[8][4];
@@ -284,11 +284,10 @@ struct VoxDev {
   uint4 *attr;         // max_voxels: albedo, normal, emissive rg, emissive b (one 16-byte load per hit)
   float *plane;        // max_voxels
   float *sunvis;       // max_voxels
-  uint32_t *scan;      // build temporary: block sums of the ordered allocations
   uint32_t *vpre;      // build temporary: max_bricks + 1 exclusive prefix of the bricks' voxel counts
-  uint32_t *work;      // build temporary: 4 words, queue counters and the chunk total of the big-triangle passes
-  uint32_t *cpre;      // build temporary: 8 * big_cap, chunk prefix of the voxBits big items
-  uint32_t *citem;     // build temporary (optional): the item of each chunk, citem_cap entries
+  uint32_t *work;      // build temporary: 4 words, the big-triangle queues, the chunk total, the items listed whole
+  uint32_t *cpre;      // build temporary: 8 * big_cap, per voxBits big-list slot its item's first chunk
+  uint32_t *citem;     // build temporary (optional): the big-list slot of each chunk, citem_cap entries
   unsigned long long *look;   // build temporary: scan_cap + 1 words, the chained scans' ticket and block states
   // voxSun (voxel.ts:633-671): with a shadow map, resolveAttr also writes each voxel's sun visibility from it and
   // the frame block (lightViewProj, sun direction, shadow bias); without one the visibility is 1

@@ -234,4 +234,4 @@ cudaError_t gi_launch_init_dirs(const gi::RcDev &r, float4 *dirs, uint32_t ndirs
 // FP64 reference of merge + SH + gather from the f32 traced atlas: rad64 rays_total x 4 doubles, sh64 27 doubles per
 // cascade-0 probe, irr64 W*H x 4 doubles.
 cudaError_t gi_launch_merge_gather_f64(const gi::RcDev &r, const float4 *traced, void *rad64, double *sh64, void *irr64,
-                                       cudaStream_t st);
+                                       uint32_t f16_cascades, cudaStream_t st);

@@ -29,10 +29,10 @@ namespace {
 
 constexpr uint32_t NOALLOC_MAX_BRICKS = 4096;          // representative table: 4096 x 512 words = 8 MiB
 constexpr uint32_t NOALLOC_BIG_CAP = 1u << 16;         // per big-triangle list: 16 x 65536 words = 4 MiB
-constexpr uint32_t NOALLOC_SCAN_WORDS = 1u << 14;      // block sums: levels * G^3 <= 2^25 pointers
+constexpr uint32_t NOALLOC_SCAN_WORDS = 1u << 14;      // chained-scan blocks: levels * G^3 <= 2^25 pointers
 // the chained scans' states (64-bit words) start on an even word
-constexpr uint32_t NOALLOC_LOOK_AT = (NOALLOC_MAX_BRICKS * 512u + 16u * NOALLOC_BIG_CAP + NOALLOC_SCAN_WORDS +
-                                      NOALLOC_MAX_BRICKS + 1u + 4u + 8u * NOALLOC_BIG_CAP + 1u) & ~1u;
+constexpr uint32_t NOALLOC_LOOK_AT = (NOALLOC_MAX_BRICKS * 512u + 16u * NOALLOC_BIG_CAP + NOALLOC_MAX_BRICKS + 1u + 4u +
+                                      8u * NOALLOC_BIG_CAP + 1u) & ~1u;
 constexpr uint32_t NOALLOC_WORDS = NOALLOC_LOOK_AT + 2u * (NOALLOC_SCAN_WORDS + 1u);
 
 // The scratch.  In host code `g_noalloc_scratch` only names the symbol; its device address comes from
@@ -134,8 +134,7 @@ extern "C" int gi_vox_build_noalloc(const gi_vox_params *p, const double eye[3],
   v.attr = reinterpret_cast<uint4 *>(attr); v.plane = plane; v.sunvis = sunvis;
   v.rep = scratch;
   v.big = scratch + NOALLOC_MAX_BRICKS * 512u;
-  v.scan = v.big + 16u * NOALLOC_BIG_CAP;
-  v.vpre = v.scan + NOALLOC_SCAN_WORDS;
+  v.vpre = v.big + 16u * NOALLOC_BIG_CAP;
   v.work = v.vpre + NOALLOC_MAX_BRICKS + 1u;
   v.cpre = v.work + 4u;
   v.look = reinterpret_cast<unsigned long long *>(scratch + NOALLOC_LOOK_AT);

@@ -31,16 +31,22 @@ __device__ __forceinline__ void sh_basis64(d3 n, double y[9]) {
   y[7] = 1.092548 * n.x * n.z; y[8] = 0.546274 * (n.x * n.x - n.y * n.y);
 }
 
-__global__ void k_widen64(const float4 *__restrict__ src, dbl4 *__restrict__ dst, uint32_t n) {
+// a value as an f16 atlas stores it (round to nearest even), back in double
+__device__ __forceinline__ double as_f16(double x) { return (double)__half2float(__double2half(x)); }
+
+// the traced intervals [first, first + n) widened to double; f16: rounded to f16 first (the storage-rounding study)
+__global__ void k_widen64(const float4 *__restrict__ src, dbl4 *__restrict__ dst, uint32_t first, uint32_t n, bool f16) {
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    float4 s = src[i];
+    float4 s = src[first + i];
     dbl4 d = {s.x, s.y, s.z, s.w};
-    dst[i] = d;
+    if (f16) { d.x = as_f16(d.x); d.y = as_f16(d.y); d.z = as_f16(d.z); d.w = as_f16(d.w); }
+    dst[first + i] = d;
   }
 }
 
 // mergeScreen for cascade c, in place on the f64 atlas: radiance + T * (weighted average of the upper cascade)
-__global__ void __launch_bounds__(256) k_merge64(RcDev r, dbl4 *rad, uint32_t c) {
+// f16: the merged radiance is rounded to f16 as it is stored (cascades above 0; cascade 0's feeds projectSH unstored)
+__global__ void __launch_bounds__(256) k_merge64(RcDev r, dbl4 *rad, uint32_t c, bool f16) {
   const CascDev &L = r.c[c];
   uint32_t dirs = L.res * L.res;
   uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -86,6 +92,7 @@ __global__ void __launch_bounds__(256) k_merge64(RcDev r, dbl4 *rad, uint32_t c)
     }
   }
   dbl4 o = {rv.x + rv.w * up.x, rv.y + rv.w * up.y, rv.z + rv.w * up.z, 1.0};
+  if (f16) { o.x = as_f16(o.x); o.y = as_f16(o.y); o.z = as_f16(o.z); }
   rad[(size_t)L.rad_off + t] = o;
 }
 
@@ -173,13 +180,17 @@ __global__ void __launch_bounds__(256) k_gather64(RcDev r, const double *__restr
 using namespace gi;
 
 cudaError_t gi_launch_merge_gather_f64(const RcDev &r, const float4 *traced, void *rad64, double *sh64, void *irr64,
-                                       cudaStream_t st) {
+                                       uint32_t f16_cascades, cudaStream_t st) {
   dbl4 *rad = reinterpret_cast<dbl4 *>(rad64);
-  k_widen64<<<1024, 256, 0, st>>>(traced, rad, r.rays_total);
+  for (uint32_t c = 0; c < r.cascades; c++) {
+    const CascDev &L = r.c[c];
+    const uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
+    k_widen64<<<min((n + 255u) / 256u, 1024u), 256, 0, st>>>(traced, rad, L.rad_off, n, ((f16_cascades >> c) & 1u) != 0u);
+  }
   for (int c = (int)r.cascades - 1; c >= 0; c--) {
     const CascDev &L = r.c[c];
     uint32_t n = L.tiles_x * L.tiles_y * L.res * L.res;
-    k_merge64<<<(n + 255u) / 256u, 256, 0, st>>>(r, rad, (uint32_t)c);
+    k_merge64<<<(n + 255u) / 256u, 256, 0, st>>>(r, rad, (uint32_t)c, c > 0 && ((f16_cascades >> c) & 1u) != 0u);
   }
   k_project_sh64<<<(r.c[0].tiles_x * r.c[0].tiles_y + 255u) / 256u, 256, 0, st>>>(r, rad, sh64);
   dim3 gg((r.width + 15u) / 16u, (r.height + 15u) / 16u);

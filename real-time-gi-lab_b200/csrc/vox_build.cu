@@ -7,8 +7,9 @@
 //    can produce; they make the whole state deterministic, so the GPU state equals the oracle's word for word.
 //  * the representative-table clear (clearKeys) zeroes every allocated brick in one full-grid pass;
 //  * indirect dispatches (writeArgs) become grid-stride loops that read the device-side counts;
-//  * the big-triangle passes run one warp per (triangle, level), taken from a queue, instead of one 64-wide
-//    workgroup; resolveAttr runs one thread per voxel;
+//  * the big-triangle passes run one warp per (triangle, level) (markBricksBig) or per chunk of one (voxBitsBig), taken
+//    from a queue, instead of one 64-wide workgroup; resolveAttr runs one thread per voxel;
+//  * markParents is folded into markBrick: the thread that marks a brick marks its ancestors;
 //  * list appends are warp-aggregated atomics.
 #include <cuda_runtime.h>
 
@@ -158,9 +159,24 @@ __device__ __forceinline__ void warp_deal(const SmallItem &it, uint32_t mine, F 
   }
 }
 
-// markBrick (voxel.ts:347): read before the atomic
-__device__ __forceinline__ void mark_brick(const VoxDev &v, uint32_t i) {
-  if (v.ptr[i] == GI_EMPTY) atomicMin(&v.ptr[i], GI_MARK);
+// markBrick (voxel.ts:347), read before the atomic, with markParents (voxel.ts:390-403) folded in: the thread whose
+// atomic turned brick b of level L from empty to marked walks its parents up the levels, marking each, and stops at
+// the first parent outside its level's window or already marked.  An already marked parent was turned by another
+// thread, which walks the same chain above it, so the marked set is the closure markParents gives.
+__device__ __forceinline__ void mark_brick(const VoxDev &v, uint32_t L, i3 b) {
+  uint32_t i = ptr_index(v, L, b);
+  if (v.ptr[i] != GI_EMPTY || atomicMin(&v.ptr[i], GI_MARK) != GI_EMPTY) return;
+  const int G = (int)v.G;
+  const i3 o = org(v, L);
+  i3 w = mki(o.x + b.x, o.y + b.y, o.z + b.z);
+  for (L++; L < v.levels; L++) {
+    w = mki(w.x >> 1, w.y >> 1, w.z >> 1);
+    const i3 ol = org(v, L);
+    const i3 p = mki(w.x - ol.x, w.y - ol.y, w.z - ol.z);
+    if (p.x < 0 || p.y < 0 || p.z < 0 || p.x >= G || p.y >= G || p.z >= G) return;
+    i = ptr_index(v, L, p);
+    if (v.ptr[i] != GI_EMPTY || atomicMin(&v.ptr[i], GI_MARK) != GI_EMPTY) return;
+  }
 }
 
 // markRange body for one brick j of the range (voxel.ts:348-358)
@@ -170,7 +186,7 @@ __device__ __forceinline__ void mark_one(const VoxDev &v, const Tri &T, uint32_t
   float bs = vox_size(v, L) * 8.0f;
   f3 c = region_lo(v, L) + adds(vi2f(b), 0.5f) * bs;
   float hh = 0.5f * bs * 1.0001f;
-  if (n == 1u || tri_box(c, mk(hh, hh, hh), T.a, T.b, T.c)) mark_brick(v, ptr_index(v, L, b));
+  if (n == 1u || tri_box(c, mk(hh, hh, hh), T.a, T.b, T.c)) mark_brick(v, L, b);
 }
 
 // clear (voxel.ts:338-344)
@@ -231,12 +247,6 @@ __device__ __forceinline__ bool big_item(const VoxDev &v, uint32_t seg0, uint32_
   return false;
 }
 
-__device__ __forceinline__ uint32_t big_total(const VoxDev &v, uint32_t hdr0) {
-  uint32_t n = 0;
-  for (uint32_t L = 0; L < v.levels; L++) n += min(v.hdr[hdr0 + L], v.big_cap);
-  return n;
-}
-
 // markBricksBig (voxel.ts:377-387): one warp per big (triangle, level), lanes over the range's bricks.
 __global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s) {
   grid_dep_wait();
@@ -251,25 +261,6 @@ __global__ void __launch_bounds__(256, 4) k_mark_bricks_big(VoxDev v, SceneDev s
     Range r = vox_range(v, T, L, true);
     uint32_t n = (uint32_t)(r.n.x * r.n.y * r.n.z);
     for (uint32_t j = lane; j < n; j += 32u) mark_one(v, T, L, r, n, j);
-  }
-}
-
-// markParents (voxel.ts:390-403)
-__global__ void k_mark_parents(VoxDev v) {
-  grid_dep_wait();
-  uint32_t G = v.G, per = G * G * G, NL = v.levels;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (NL - 1u) * per; i += gridDim.x * blockDim.x) {
-    if (v.ptr[i] != GI_MARK) continue;
-    uint32_t L = i / per, r = i % per;
-    i3 o = org(v, L);
-    i3 w = mki(o.x + (int)(r % G), o.y + (int)((r / G) % G), o.z + (int)(r / (G * G)));
-    for (L++; L < NL; L++) {
-      w = mki(w.x >> 1, w.y >> 1, w.z >> 1);
-      i3 ol = org(v, L);
-      i3 b = mki(w.x - ol.x, w.y - ol.y, w.z - ol.z);
-      if (b.x < 0 || b.y < 0 || b.z < 0 || b.x >= (int)G || b.y >= (int)G || b.z >= (int)G) break;
-      mark_brick(v, ptr_index(v, L, b));
-    }
   }
 }
 
@@ -332,8 +323,6 @@ __global__ void __launch_bounds__(256) k_init_bricks(VoxDev v) {
     if (q < nb * 4u) occ[q] = z;
     else rep[q - nb * 4u] = z;
   }
-  // the big items' chunk scan
-  for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= v.scan_cap; q += gridDim.x * blockDim.x) v.look[q] = 0ull;
 }
 
 // closestBary (voxel.ts:250-267)
@@ -398,6 +387,39 @@ __device__ __forceinline__ void voxelize_one(const VoxDev &v, const SceneDev &s,
   atomicMax(&v.rep[ri], t + 1u);
 }
 
+// The big items' work for k_vox_bits_big: every big (triangle, level) of voxBits is cut into chunks of
+// 2^chunk_log2 cells (a wall triangle clipped to a window covers ~10^4 cells; one warp per triangle left one warp working
+// long after the rest).  The warp reserves its items' chunks with one atomic, item after item; the item's first chunk
+// goes to cpre[slot] and, below citem_cap, the slot of every chunk to citem (written by the whole warp).  An item with
+// chunks at or past citem_cap is listed for k_vox_bits_big to walk from there to its end with one warp.  All lanes call
+// it (nch = 0: no item).  Which chunk numbers an item gets does not change the voxels: the occupancy and
+// representative updates are ORs and maxima.
+__device__ __forceinline__ void big_chunks(const VoxDev &v, uint32_t slot, uint32_t nch) {
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t incl = nch;
+#pragma unroll
+  for (int d = 1; d < 32; d <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+    if (lane >= (uint32_t)d) incl += y;
+  }
+  const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+  if (total == 0u) return;
+  uint32_t base = 0;
+  if (lane == 31u) base = atomicAdd(&v.work[2], total);
+  base = __shfl_sync(0xffffffffu, base, 31);
+  const uint32_t first = base + incl - nch;
+  if (nch != 0u) {
+    v.cpre[slot] = first;
+    if (first + nch > v.citem_cap) v.big[8u * v.big_cap + atomicAdd(&v.work[3], 1u)] = slot;
+  }
+  for (uint32_t m = __ballot_sync(0xffffffffu, nch != 0u); m != 0u; m &= m - 1u) {
+    const int src = __ffs(m) - 1;
+    const uint32_t f = __shfl_sync(0xffffffffu, first, src), c = __shfl_sync(0xffffffffu, nch, src);
+    const uint32_t sl = __shfl_sync(0xffffffffu, slot, src);
+    for (uint32_t j = lane; j < c && f + j < v.citem_cap; j += 32u) v.citem[f + j] = sl;
+  }
+}
+
 // voxBits (voxel.ts:492-513)
 __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
   grid_dep_wait();
@@ -422,54 +444,22 @@ __global__ void __launch_bounds__(256, 4) k_vox_bits(VoxDev v, SceneDev s) {
       else big = (uint32_t)n > GI_BIG_SMALL;
     }
     uint32_t k = warp_append(&v.hdr[16 + L], big);
+    uint32_t slot = 0, nch = 0;
     if (big) {
-      if (k < v.big_cap) v.big[L * v.big_cap + k] = t; else atomicAdd(&v.hdr[3], 1u);
+      if (k < v.big_cap) {
+        slot = L * v.big_cap + k;
+        v.big[slot] = t;
+        nch = ((uint32_t)n + (1u << v.chunk_log2) - 1u) >> v.chunk_log2;
+      } else {
+        atomicAdd(&v.hdr[3], 1u);
+      }
     }
+    big_chunks(v, slot, nch);
     SmallItem it;
     it.T = T; it.t = t; it.r = r; it.n = n;
     warp_deal(it, (!big && n > 0) ? (uint32_t)n : 0u, [&](const SmallItem &w, int q) {
       voxelize_one(v, s, w.T, w.t, L, range_cell_small(w.r, q), w.n == 1, bo);
     });
-  }
-}
-
-// voxBitsBig (voxel.ts:515-534), balanced: every big (triangle, level) is cut into chunks of VB_CHUNK cells (a wall
-// triangle clipped to a window covers ~10^4 cells; one warp per triangle left one warp working long after the rest).
-// k_chunks, one chained scan over the items in blocks of 256: per item its chunk count, its prefix within the block
-// (cpre), the blocks' offsets (scan), the chunk total (work[2]) and, below citem_cap, the item of every chunk (a table
-// lookup for k_vox_bits_big instead of ~16 dependent loads of a binary search).  Warps of k_vox_bits_big take chunks
-// from a queue.
-// VB_CHUNK = 1 << v.chunk_log2 cells per work item (gi_vox_tuning; default 128)
-
-__global__ void __launch_bounds__(256) k_chunks(VoxDev v, SceneDev s) {
-  grid_dep_wait();
-  uint32_t items = big_total(v, 16u);
-  uint32_t nblk = (items + 255u) / 256u;
-  __shared__ uint32_t s_pre;
-  for (;;) {
-    uint32_t b = chain_ticket(v.look);
-    if (b >= nblk) break;
-    uint32_t w = b * 256u + threadIdx.x, L, t, c = 0;
-    if (w < items && big_item(v, 0u, 16u, w, L, t)) {
-      Tri T = load_tri(s, t);
-      Range r = vox_range(v, T, L, false);
-      c = ((uint32_t)(r.n.x * r.n.y * r.n.z) + (1u << v.chunk_log2) - 1u) >> v.chunk_log2;
-    }
-    uint32_t tot;
-    uint32_t ex = block_scan_256(c, &tot);
-    if (threadIdx.x == 0) {
-      uint32_t pre = chain_prefix(v.look, b, tot, v.hdr);
-      s_pre = pre;
-      v.scan[b] = pre;
-      if (b == nblk - 1u) v.work[2] = pre + tot;
-    }
-    __syncthreads();
-    uint32_t first = s_pre + ex;
-    if (w < items) {
-      v.cpre[w] = ex;
-      for (uint32_t ch = first; ch < first + c && ch < v.citem_cap; ch++) v.citem[ch] = w;
-    }
-    __syncthreads();   // s_pre is rewritten by the next part
   }
 }
 
@@ -492,38 +482,31 @@ __device__ __forceinline__ bool voxel_takes(const VoxDev &v, const SceneDev &s, 
   return true;
 }
 
-// One warp per chunk.  The lanes' occupancy bits are ORed per word inside the warp (neighbouring cells share a
-// word), one atomic per word.
+// voxBitsBig (voxel.ts:515-534), balanced: one warp per chunk of a big item, taken from a queue (big_chunks cut the
+// items); then one warp per item listed with chunks past the table, from its first untabulated chunk to its end.  The
+// lanes' occupancy bits are ORed per word inside the warp (neighbouring cells share a word), one atomic per word.
 __global__ void __launch_bounds__(256, 4) k_vox_bits_big(VoxDev v, SceneDev s) {
   grid_dep_wait();
   uint32_t lane = threadIdx.x & 31u;
   uint32_t bo = v.hdr[2];
-  uint32_t items = big_total(v, 16u);
-  uint32_t chunks = v.work[2];
-  // the attribute allocation's chained scan (the chunk scan is done: its offsets are in scan)
+  const uint32_t tab = min(v.work[2], v.citem_cap);   // chunks found through the table
+  const uint32_t work = tab + v.work[3];               // + the listed items
+  // the attribute allocation's chained scan (the brick allocation's is done)
   for (uint32_t q = blockIdx.x * blockDim.x + threadIdx.x; q <= v.scan_cap; q += gridDim.x * blockDim.x) v.look[q] = 0ull;
   for (;;) {
     uint32_t ch = 0;
     if (lane == 0) ch = atomicAdd(&v.work[1], 1u);
     ch = __shfl_sync(0xffffffffu, ch, 0);
-    if (ch >= chunks) break;
-    uint32_t lo = 0;
-    if (ch < v.citem_cap) {
-      lo = v.citem[ch];              // the chunk's item, tabulated by k_chunks
-    } else {
-      uint32_t hi = items;           // the last item whose first chunk is <= ch
-      while (hi - lo > 1u) {
-        uint32_t m = (lo + hi) >> 1;
-        if (v.cpre[m] + v.scan[m >> 8] <= ch) lo = m; else hi = m;
-      }
-    }
-    uint32_t L, t;
-    big_item(v, 0u, 16u, lo, L, t);
-    uint32_t part = ch - (v.cpre[lo] + v.scan[lo >> 8]);
+    if (ch >= work) break;
+    const bool whole = ch >= tab;
+    const uint32_t slot = whole ? v.big[8u * v.big_cap + (ch - tab)] : v.citem[ch];
+    const uint32_t first = v.cpre[slot];
+    const uint32_t part = whole ? max(first, v.citem_cap) - first : ch - first;
+    const uint32_t L = slot / v.big_cap, t = v.big[slot];
     Tri T = load_tri(s, t);
     Range r = vox_range(v, T, L, false);
     int n = r.n.x * r.n.y * r.n.z;
-    int q_end = min(n, (int)((part + 1u) << v.chunk_log2));
+    int q_end = whole ? n : min(n, (int)((part + 1u) << v.chunk_log2));
     // the lane's cell, then 32 cells further in range order per step: 32 = dz * nx * ny + dy * nx + dx
     int q = (int)(part << v.chunk_log2) + (int)lane;
     i3 cell = range_cell(r, q);
@@ -760,14 +743,12 @@ cudaError_t gi_launch_vox_build(const VoxDev &v, const SceneDev &s, uint32_t sm_
   uint32_t tb = (s.threads + 255u) / 256u;   // threads of the triangle passes (the work items' triangles)
   if (tb) GI_TRY(gi_launch(k_mark_bricks, tb, 256, st, v, s));
   GI_TRY(gi_launch(k_mark_bricks_big, persist, 256, st, v, s));
-  if (v.levels > 1) GI_TRY(gi_launch(k_mark_parents, min(((v.levels - 1u) * per + 255u) / 256u, persist), 256, st, v));
   uint32_t kpt = 1;
   while ((nptr + 256u * kpt - 1u) / (256u * kpt) > v.scan_cap && kpt < 32u) kpt *= 2u;
   uint32_t ab = (nptr + 256u * kpt - 1u) / (256u * kpt);
   GI_TRY(gi_launch(k_alloc_bricks, ab, 256, st, v, kpt, ab));
   GI_TRY(gi_launch(k_init_bricks, persist, 256, st, v));
   if (tb) GI_TRY(gi_launch(k_vox_bits, tb, 256, st, v, s));
-  GI_TRY(gi_launch(k_chunks, persist, 256, st, v, s));
   GI_TRY(gi_launch(k_vox_bits_big, persist, 256, st, v, s));
   if (v.levels > 1) GI_TRY(gi_launch(k_reduce, persist, 256, st, v));
   uint32_t vb = (v.max_bricks + VOX_CHUNK - 1u) / VOX_CHUNK;

@@ -67,6 +67,7 @@ SIGNATURES = {
     "gi_rc_buffer_bytes": (C.c_int, [_P, C.c_int, C.POINTER(C.c_size_t)]),
     "gi_rc_set_debug_hits": (C.c_int, [_P, C.c_int]),
     "gi_rc_merge_gather_f64": (C.c_int, [_P, _P]),
+    "gi_rc_merge_gather_f64_rounded": (C.c_int, [_P, C.c_uint32, _P]),
     "gi_scene_set_raster_capacity": (C.c_int, [_P, C.c_uint32]),
     "gi_scene_rigid_define": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32]),
     "gi_scene_rigid_upload": (C.c_int, [_P, _P, _P]),

@@ -333,9 +333,14 @@ class Rc:
         _lib.call("gi_rc_read_irradiance_raw", self.handle, out.ctypes.data if isinstance(out, np.ndarray) else out,
                   out.nbytes if isinstance(out, np.ndarray) else self.irr_bytes(), _stream(stream))
 
-    def merge_gather_f64(self, stream=None):
-        """FP64 reference of merge + SH + gather from the last trace (f32 atlas, debug hits on)."""
-        _lib.call("gi_rc_merge_gather_f64", self.handle, _stream(stream))
+    def merge_gather_f64(self, stream=None, f16_cascades: int = 0):
+        """FP64 reference of merge + SH + gather from the last trace (f32 atlas, debug hits on).  f16_cascades: bit
+        mask of cascades whose atlas storage is rounded to f16 (traced intervals and, above cascade 0, merged
+        radiances), every stage still in double."""
+        if f16_cascades:
+            _lib.call("gi_rc_merge_gather_f64_rounded", self.handle, int(f16_cascades), _stream(stream))
+        else:
+            _lib.call("gi_rc_merge_gather_f64", self.handle, _stream(stream))
 
     def read_irradiance_f64(self, ptr: Optional[int] = None, stream=None) -> Optional[np.ndarray]:
         """The FP64 irradiance, (H, W, 4) doubles; into the host or device memory at ptr when given."""

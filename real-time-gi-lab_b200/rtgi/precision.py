@@ -88,14 +88,23 @@ class ErrorStats:
                 "values": self.n, "frames": self.frames, "alpha_mismatch": self.alpha_mismatch}
 
 
+# storage-rounding study: cascades whose atlas storage is rounded to f16 with every stage in double
+# (gi_rc_merge_gather_f64_rounded), named by the cascades rounded
+ROUNDED = {"c0": 0b00001, "c4": 0b10000, "c3-c4": 0b11000, "c2-c4": 0b11100, "c1-c4": 0b11110, "c0-c4": 0b11111}
+
+
 def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
         atlases: Sequence[str] = ("f32", "f16", "bf16", "f16-f32out", "bf16-f32out"),
         seed: int = 0, n_boxes: int = 64, width: int = 1920, height: int = 1080, device: int = 0,
-        shadow_size: int = fr.SHADOW_SIZE) -> dict:
+        shadow_size: int = fr.SHADOW_SIZE, rounded: Dict[str, int] = ROUNDED) -> dict:
     """The study: per frame, pose the boxes, draw the sun's shadow map (the boxes move; shadow_size 0: no sun
     visibility), rebuild the clipmap with voxSun, solve the cascades in every atlas mode, run the FP64 merge and
     gather from the f32 mode's trace, and accumulate each mode's irradiance error.  Also times each mode's cascade
-    solve (CUDA events on the solve stream; median over frames)."""
+    solve (CUDA events on the solve stream; median over frames).
+
+    rounded: the storage-rounding study, per entry a bit mask of cascades whose atlas storage (traced intervals and,
+    above cascade 0, merged radiances) is rounded to f16 while every stage stays in double; its error against the
+    exact FP64 result is the storage's alone, without the f32 arithmetic, and its atlas bytes are stated beside it."""
     import torch
     dev = torch.device("cuda", device)
     stream = torch.cuda.current_stream(dev)
@@ -127,6 +136,8 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
                                dtype=torch.float32 if rc.irr_bytes() == 16 * width * height else torch.float16)
                 for a, rc in rcs.items()}
         stats = {a: ErrorStats(torch, dev) for a in rcs}
+        rstats = {k: ErrorStats(torch, dev) for k in rounded}
+        tmp = torch.empty((height, width, 4), dtype=torch.float64, device=dev) if rounded else None
         times = {a: [] for a in rcs}
         counters = []
         for f in range(frames):
@@ -148,14 +159,26 @@ def run(ctx: gpu.Context, frames: int = 100, dt: float = 1.0 / 30.0,
             rcs["f32"].read_irradiance_f64(ref.data_ptr(), stream)
             for a in rcs:
                 stats[a].add(outs[a], ref)
+            for k, mask in rounded.items():
+                rcs["f32"].merge_gather_f64(stream, f16_cascades=mask)
+                rcs["f32"].read_irradiance_f64(tmp.data_ptr(), stream)
+                rstats[k].add(tmp, ref)
             stream.synchronize()
             for a, (e0, e1) in ev.items():
                 times[a].append(e0.elapsed_time(e1))
             if f == 0 or f == frames - 1:
                 counters.append(vox.read_counters(stream))
         out = {a: dict(stats[a].summary(), solve_ms=float(np.median(times[a]))) for a in rcs}
+        lay = configs.cascade_layout(rcs["f32"].params, width, height)
+        rays = [c["tiles_x"] * c["tiles_y"] * c["res"] ** 2 for c in lay["casc"]]
+        r_out = {k: dict(rstats[k].summary(), f16_cascades=[c for c in range(len(rays)) if (m >> c) & 1],
+                         atlas_bytes=sum(n * (8 if (m >> c) & 1 else 16) for c, n in enumerate(rays)))
+                 for k, m in rounded.items()}
         return {"scene": f"colonnade + {n_boxes} moving boxes: {s.triangle_count} triangles", "frames": frames,
                 "dt_s": dt, "resolution": [width, height], "atlases": out, "shadow_map": shadow_size,
+                "storage_rounding": {"modes": r_out, "rays_per_cascade": rays, "atlas_bytes_f32": 16 * sum(rays),
+                                     "reference": "exact FP64 merge + SH + gather of the f32 trace; each mode rounds "
+                                                  "the storage of its cascades to f16 with every stage in double"},
                 "bricks_first_last": [c["bricks"] for c in counters],
                 "error": "per valid pixel and rgb channel |x - x64| / max(|x64|, 1e-3 x frame mean |x64|); "
                          "quantiles are upper edges of 0.1-decade histogram bins"}

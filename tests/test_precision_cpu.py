@@ -74,3 +74,35 @@ def test_rigid_transforms_reproduce_pose():
         pp, nn = objs.pose(t)
         np.testing.assert_allclose(p.reshape(-1, 3), pp, atol=2e-5)
         np.testing.assert_allclose(n.reshape(-1, 3), nn, atol=1e-6)
+
+
+def test_f64_storage_rounding_in_the_oracle():
+    """The oracle's FP64 merge with the atlas storage of some cascades rounded to f16.  Cascade 0 alone rounds only its
+    traced intervals (its merged radiances feed projectSH unstored), so it equals rounding them beforehand with numpy's
+    float16 (round to nearest even).  Every cascade rounded moves the irradiance by about f16's relative step."""
+    from oracle import bind
+    from rtgi import configs, frame as fr
+    s = scenes.room_scene(0)
+    W, H = 96, 64
+    v = configs.vox_params({"v0": 0.08, "levels": 3, "G": 16, "maxBricks": 8192, "maxVoxels": 1 << 20})
+    st = bind.vox_build(s, v.v0, v.levels, v.G, v.maxBricks, v.maxVoxels, s.camera.eye)
+    q = configs.parse_config("screen-8-voxel-f32", {"cascades": 3})
+    F = fr.pack_frame(fr.FrameParams(cam=s.camera, width=W, height=H, sun_dir=s.sun_dir, sun_e=fr.SUN_E, sky=fr.SKY,
+                                     cascades=q.cascades, P=q.P))
+    depth, normal, _ = bind.raster_gbuffer(s, F, W, H)
+    nrm = normal.astype(np.float16).astype(np.float32)
+    lay = configs.cascade_layout(q, W, H)
+    o = bind.rc_solve(st, lay, F, depth, nrm, merge=False)
+    args = (lay, F, depth, nrm, o["probes"])
+    exact = bind.merge_gather_f64(*args, o["rad_traced"])
+    c0 = lay["casc"][0]
+    a, n = c0["rad_off"], c0["tiles_x"] * c0["tiles_y"] * c0["res"] ** 2
+    pre = o["rad_traced"].copy()
+    pre[a:a + n] = pre[a:a + n].astype(np.float16).astype(np.float32)
+    assert np.array_equal(bind.merge_gather_f64(*args, o["rad_traced"], f16_cascades=1), bind.merge_gather_f64(*args, pre))
+    every = bind.merge_gather_f64(*args, o["rad_traced"], f16_cascades=0b111)
+    valid = exact[..., 3] > 0
+    assert valid.any() and np.array_equal(every[..., 3], exact[..., 3])
+    d, r = (every - exact)[..., :3][valid], exact[..., :3][valid]
+    rel_l2 = np.sqrt((d * d).sum() / (r * r).sum())
+    assert 1e-6 < rel_l2 < 2.0 ** -10

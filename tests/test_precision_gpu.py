@@ -37,6 +37,10 @@ def test_f64_reference_matches_oracle(ctx):
         normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(case.height, case.width, 4)
         probes = rc.read_buffer(_lib.GI_RC_PROBES).view(bind.PROBE_DTYPE)
         traced = rc.read_atlas(_lib.GI_RC_RAD_TRACED)
+        rounded = {}
+        for mask in (0b00001, 0b10110, 0b11111):
+            rc.merge_gather_f64(f16_cascades=mask)
+            rounded[mask] = rc.read_irradiance_f64()
     finally:
         for h in (rc, vw, sg):
             h.destroy()
@@ -47,6 +51,13 @@ def test_f64_reference_matches_oracle(ctx):
     assert scale > 0.0, "the lit room must carry irradiance"
     # same double operations in the same order; only exp() may differ in the last bit
     np.testing.assert_allclose(irr64, ref, rtol=1e-12, atol=1e-12 * scale)
+    # the storage of some cascades rounded to f16 (round to nearest even, in the traced intervals and the merged
+    # radiances above cascade 0), every stage still in double
+    for mask, got in rounded.items():
+        want = bind.merge_gather_f64(lay, case.frame, depth, normal.astype(np.float32), probes, traced, f16_cascades=mask)
+        assert np.array_equal(got[..., 3], want[..., 3])
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * scale, err_msg=f"f16 cascades {mask:05b}")
+        assert not np.array_equal(got, irr64)
     # the f32 path's irradiance against its own FP64 merge + gather
     valid = ref[..., 3] > 0
     d = irr32[..., :3][valid].astype(np.float64) - ref[..., :3][valid]
@@ -77,3 +88,9 @@ def test_precision_study_small(ctx):
     assert a["bf16"]["rel_l2"] < 2e-2
     # SH and irradiance in f32: only the atlas and the merge round to 16 bits
     assert a["f16-f32out"]["rel_l2"] < a["f16"]["rel_l2"] and a["bf16-f32out"]["rel_l2"] < a["bf16"]["rel_l2"]
+    # storage rounding with every stage in double: more cascades rounded, fewer atlas bytes and a larger error
+    m = r["storage_rounding"]["modes"]
+    assert m["c0-c4"]["atlas_bytes"] * 2 == r["storage_rounding"]["atlas_bytes_f32"]
+    assert m["c4"]["atlas_bytes"] > m["c3-c4"]["atlas_bytes"] > m["c2-c4"]["atlas_bytes"] > m["c1-c4"]["atlas_bytes"]
+    assert 0.0 < m["c4"]["rel_l2"] <= m["c1-c4"]["rel_l2"] <= m["c0-c4"]["rel_l2"] < 2.0 ** -10
+    assert all(x["alpha_mismatch"] == 0 for x in m.values())
