@@ -477,8 +477,9 @@ def run_world_items(args, ctx, stream):
 def run_dynamic(args, ctx, stream, flush, dist, world):
     """The dynamic layer (dynlayer.ts) on the colonnade with 64 moving boxes as the scene's dynamic tail: the static rows
     rebuilt into the clipmap, the boxes splatted into the layer, the cascades reading it (traceDyn), solves replayed from
-    one graph; against the same solve with the layer unbound (the boxes then absent).  Device time, L2 flushed between
-    steps outside the step events."""
+    one graph; against the same solve with the layer unbound (the boxes then absent).  With multi-bounce on, the layer
+    (with its albedo words) without and with the token obj (the boxes receive the bounce volume's light and block and
+    reflect its rays: dynInject, bnTraceDyn).  Device time, L2 flushed between steps outside the step events."""
     import torch
     from rtgi import frame as fr, gpu, movers, scenes
     s0, W, H, p, v, F0, desc = workload(args.workload)
@@ -493,14 +494,19 @@ def run_dynamic(args, ctx, stream, flush, dist, world):
     vw = gpu.VoxWorld(sg, v)
     rc = gpu.Rc(ctx, p, W, H)
     dyn = gpu.DynLayer(vw, first, bricks=2048)
+    dyn_alb = gpu.DynLayer(vw, first, bricks=2048, albedo=True)
     out = {"objects": 64, "dynamic_triangles": s.triangle_count - first, "bricks_pool": 2048}
     with torch.cuda.stream(stream):
         rc.set_frame(F, stream)
         rc.render_gbuffer(sg, stream)
         rc.render_shadow(sg, desc["shadow_map"] or 4096, stream)
         vw.update(s.camera.eye)
-        for name, layer in (("with_layer", dyn), ("without", None)):
+        for name, layer, bounce, objects in (("with_layer", dyn, False, False), ("without", None, False, False),
+                                             ("bounce_with_layer", dyn_alb, True, False),
+                                             ("bounce_objects", dyn_alb, True, True)):
             rc.set_dyn(layer)
+            rc.set_bounce(vw if bounce else None)
+            rc.set_objects(objects)
             rc.set_timing(True)
             pm = {k: [] for k in rc.PASSES}
             for _ in range(max(5, args.warmup)):
@@ -523,7 +529,8 @@ def run_dynamic(args, ctx, stream, flush, dist, world):
                          "passes_ms": {k: statistics.median(x) for k, x in pm.items()}}
         out["layer"] = {k: val for k, val in dyn.read_counters(stream).items() if k != "hdr"}
     rc.set_dyn(None)
-    for h in (rc, dyn, vw, sg):
+    rc.set_bounce(None)
+    for h in (rc, dyn, dyn_alb, vw, sg):
         h.destroy()
     return out
 

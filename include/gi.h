@@ -385,7 +385,7 @@ int gi_rc_destroy(gi_rc *rc);
  * point at level 0, prefiltered to the coarser levels), which the cascades' traces read at the width of a direction
  * bin's cone (traceDyn, rc.ts:223-231).  createDynLayer (dynlayer.ts:680): `bricks` is VoxParams.dynBricks (the
  * reference's default 512); albedo 1 writes the area x albedo words (the reference's DYN_ALB, configs with the token
- * obj; the received light of dynInject, phase 31, is not built).  G^3 must be a multiple of 32. */
+ * obj, whose objects receive light: gi_rc_set_objects).  G^3 must be a multiple of 32. */
 int gi_dyn_create(gi_vox *vox, uint32_t bricks, uint32_t first_dynamic, uint32_t albedo, gi_dyn **out);
 /* DynLayer.encode (dynlayer.ts:738-741): mark .. resolve at the voxel world's current windows, shaded with the rc's
  * frame (sun, style) and its sun shadow map when it has one.  Stream-ordered.  gi_solve runs it after the static
@@ -404,6 +404,13 @@ int gi_dyn_destroy(gi_dyn *dyn);
 /* The layer the rc's traces read, or NULL for none (dyn[0] = 0 in the reference: no dynamic objects).  Drops a
  * captured graph (it was captured without the layer). */
 int gi_rc_set_dyn(gi_rc *rc, gi_dyn *dyn);
+/* The token obj (RcParams.objects, rc.ts:79-80; phase 31, off by default): with multi-bounce on (gi_rc_set_bounce) and a
+ * layer bound, every solve's trace pass first adds to the layer's voxels the light they receive from the previous
+ * frame's bounce volume (dynInject, dynlayer.ts:165-191, with bounce.ts:265-296's dynE), and the volume's irradiance
+ * rays read the layer in front of their static hits (bnTraceDyn, bounce.ts:169-174).  The layer should be created
+ * with albedo 1 (DynLayer.setAlbedo): without its albedo words the received light is 0.  Captured graphs made before
+ * the change are refused (GI_ERR_STATE). */
+int gi_rc_set_objects(gi_rc *rc, int on);
 
 #ifdef __cplusplus
 }

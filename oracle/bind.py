@@ -114,7 +114,7 @@ class OrcDyn(C.Structure):
 class OrcBounce(C.Structure):
     _fields_ = [("cell", C.c_float), ("v0", C.c_float), ("dx", C.c_uint32), ("dy", C.c_uint32), ("dz", C.c_uint32),
                 ("rays", C.c_uint32), ("div", C.c_uint32), ("dirs", C.c_void_p), ("vol", C.c_void_p * 2),
-                ("list", C.c_void_p)]
+                ("list", C.c_void_p), ("objects", C.c_uint32)]
 
 
 class OrcCasc(C.Structure):
@@ -426,14 +426,17 @@ def bounce_dirs(rays: int) -> np.ndarray:
 class Bounce:
     """The oracle's multi-bounce volume state (orc_bounce) across frames."""
 
-    def __init__(self, vox: dict, cell: float = 1.2, dims=(32, 16, 32), rays: int = 16, div: int = 2):
+    def __init__(self, vox: dict, cell: float = 1.2, dims=(32, 16, 32), rays: int = 16, div: int = 2,
+                 objects: bool = False):
+        """objects: the token obj (phase 31); the dynamic layer in vox['dyn'] at each frame receives the previous
+        volume and is read by the volume's irradiance rays."""
         dx, dy, dz = dims
         self.dirs = bounce_dirs(rays)
         texels = dx * dy * (6 * dz + 1)
         self.vol = [np.zeros(texels * 4, np.float32), np.zeros(texels * 4, np.float32)]
         self.list = np.zeros(4 + dx * dy * dz, np.uint32)
         self.b = OrcBounce(np.float32(cell), np.float32(vox["v0"]), dx, dy, dz, rays, div, _p(self.dirs),
-                           (C.c_void_p * 2)(_p(self.vol[0]), _p(self.vol[1])), _p(self.list))
+                           (C.c_void_p * 2)(_p(self.vol[0]), _p(self.vol[1])), _p(self.list), 1 if objects else 0)
 
     def frame(self, vox: dict, frame: np.ndarray) -> np.ndarray:
         """One frame over a built world; returns (and stores in vox['bn_inj']) the injected irradiance."""

@@ -310,6 +310,14 @@ static inline float dyn_word(const orc_dyn *dl, uint32_t base, uint32_t k, uint3
   uint32_t u = dl->data[base + k];
   return L == 0u ? (float)u / DYN_FIX : fbits(u);
 }
+float dyn_word_at(const orc_dyn *dl, uint32_t base, uint32_t k, uint32_t L) { return dyn_word(dl, base, k, L); }
+void dyn_add_radiance(orc_dyn *dl, uint32_t base, uint32_t L, const float add[3]) {
+  for (uint32_t k = 0; k < 3u; k++) {
+    uint32_t *w = &dl->data[base + 7u + k];
+    if (L == 0u) *w += fix_of(add[k]);
+    else *w = ubits(fbits(*w) + add[k]);
+  }
+}
 /* dynRead: mean radiance and coverage per voxel length for direction d (the three faces against d) */
 static void dyn_read(const orc_dyn *dl, uint32_t base, uint32_t L, v3 d, float out[4]) {
   out[0] = out[1] = out[2] = out[3] = 0.0f;

@@ -223,9 +223,12 @@ typedef struct {
   const float *dirs;              /* rays * 4: sfDir(r, rays) (the same table the GPU path uses) */
   float *vol[2];                  /* dx * dy * (6 dz + 1) * 4 each, texel (x, y, z) at ((z dy + y) dx + x) * 4 */
   uint32_t *list;                 /* 4 + dx dy dz words: [0] listed, [1] frame counter, [2] this frame's volume */
+  uint32_t objects;               /* token obj (phase 31): with a dynamic layer in the voxel world (vx->dyn), its
+                                     voxels receive the previous volume first (dynInject) and the volume's irradiance
+                                     rays read it (bnTraceDyn) */
 } orc_bounce;
-/* One frame of the volume (Bounce.encode, bounce.ts:356-368) over a built voxel world: clear, classify, update,
- * inject (into inj_out, max_voxels * 6).  The list order is the probe order (the GPU's atomics order it otherwise;
+/* One frame of the volume (Bounce.encode, bounce.ts:356-368) over a built voxel world: (objects: dynInject into
+ * vx->dyn,) clear, classify, update, inject (into inj_out, max_voxels * 6).  The list order is the probe order (the GPU's atomics order it otherwise;
  * the result does not depend on it). */
 int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *frame, float *inj_out);
 

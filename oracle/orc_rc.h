@@ -42,4 +42,9 @@ void sh_basis(v3 n, float y[9]);
 v3 upper_avg(const orc_layout *ly, const float *rad, uint32_t cu, uint32_t q, uint32_t u, uint32_t v, uint32_t lr);
 /* dyn.c */
 void dyn_compose(const orc_vox *vx, v3 o, v3 d, float t0, float t1, v3 ooff, float k, trace_t *tr);
+/* word k of the voxel at data base `base` of level L: level 0 fixed point (/ 65536), the levels above f32 */
+float dyn_word_at(const orc_dyn *dl, uint32_t base, uint32_t k, uint32_t L);
+/* dynInject's store (dynlayer.ts:186-189): add[0..2] added to the voxel's radiance words 7..9, level 0 in fixed point
+ * (u32(round(x * 65536)), the sum wrapping as u32), the levels above in f32 */
+void dyn_add_radiance(orc_dyn *dl, uint32_t base, uint32_t L, const float add[3]);
 #endif

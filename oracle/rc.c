@@ -578,7 +578,75 @@ static v3 bn_axis_vec(uint32_t a) {
   return a / 2u == 0u ? V(s, 0.0f, 0.0f) : (a / 2u == 1u ? V(0.0f, s, 0.0f) : V(0.0f, 0.0f, s));
 }
 
+/* dynE of the bounce volume (bounce.ts:267-296): the irradiance at p of a dynamic voxel with projected areas P over
+ * its six axis faces, E = sum_a P_a E_a / sum_a P_a, E_a trilinear over the 8 probes around p with bnRead's rules
+ * (active, reach, side of the face) */
+static v3 dyn_e(const orc_bounce *b, const float *vol, v3 p, const float P[6]) {
+  i3 org0 = bn_origin(b, vol);
+  v3 g = sub(V(p.x / b->cell, p.y / b->cell, p.z / b->cell), vi2f(org0));
+  i3 bb = vf2i(vfloor(g));
+  v3 fr = sub(g, vi2f(bb));
+  float tol = 0.5f * b->v0;
+  v3 e[6];
+  float ws[6];
+  for (int a = 0; a < 6; a++) { e[a] = V(0.0f, 0.0f, 0.0f); ws[a] = 0.0f; }
+  for (int k = 0; k < 8; k++) {
+    i3 off = I(k & 1, (k >> 1) & 1, (k >> 2) & 1);
+    i3 cc = I(bb.x + off.x, bb.y + off.y, bb.z + off.z);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= (int32_t)b->dx || cc.y >= (int32_t)b->dy || cc.z >= (int32_t)b->dz) continue;
+    v3 pp = muls(vi2f(I(org0.x + cc.x, org0.y + cc.y, org0.z + cc.z)), b->cell);
+    v3 u = sub(p, pp);
+    if (bn_axis_a(b, vol, cc, 0) <= 0.0f) continue;
+    if (fabsf(u.x) > bn_axis_a(b, vol, cc, u.x >= 0.0f ? 0 : 1) + tol || fabsf(u.y) > bn_axis_a(b, vol, cc, u.y >= 0.0f ? 2 : 3) + tol
+        || fabsf(u.z) > bn_axis_a(b, vol, cc, u.z >= 0.0f ? 4 : 5) + tol) continue;
+    v3 t3 = V(off.x == 1 ? fr.x : 1.0f - fr.x, off.y == 1 ? fr.y : 1.0f - fr.y, off.z == 1 ? fr.z : 1.0f - fr.z);
+    float wt = t3.x * t3.y * t3.z;
+    for (int a = 0; a < 6; a++) {
+      if (P[a] <= 0.0f) continue;
+      float w = wt * smoothstep_(-0.05f, 0.25f, dot(sub(pp, p), bn_axis_vec((uint32_t)a)) / b->cell);
+      if (w <= 0.0f) continue;
+      e[a] = add(e[a], muls(bn_axis_rgb(b, vol, cc, a), w));
+      ws[a] += w;
+    }
+  }
+  v3 sum = V(0.0f, 0.0f, 0.0f);
+  float ps = 0.0f;
+  for (int a = 0; a < 6; a++) {
+    if (ws[a] > 1e-6f) sum = add(sum, divs(muls(e[a], P[a]), ws[a]));
+    ps += P[a];
+  }
+  return divs(sum, fmaxf_(ps, 1e-9f));
+}
+
+/* dynInject (dynlayer.ts:173-191), phase 31: every voxel of the layer's allocated bricks with area adds albedo / pi
+ * times dynE of the previous frame's volume to its radiance (the layer as this frame's build left it) */
+static void dyn_inject_bounce(const orc_bounce *b, const orc_vox *vx, orc_dyn *dl, const float *prev) {
+  const uint32_t G = vx->G, G3 = G * G * G;
+  const uint32_t slots = dl->hdr[8] < dl->nb ? dl->hdr[8] : dl->nb;
+  for (uint32_t slot = 0; slot < slots; slot++) {
+    const uint32_t pi = dl->meta[slot], L = pi / G3, r = pi % G3;
+    for (uint32_t bit = 0; bit < 512u; bit++) {
+      const uint32_t base = (slot * 512u + bit) * 13u;
+      if (dyn_word_at(dl, base, 6u, L) <= 0.0f) continue;
+      float P[6];
+      for (uint32_t k = 0; k < 6u; k++) P[k] = dyn_word_at(dl, base, k, L);
+      i3 c = I((int32_t)(r % G) * 8 + (int32_t)(bit & 7u), (int32_t)((r / G) % G) * 8 + (int32_t)((bit >> 3) & 7u),
+               (int32_t)(r / (G * G)) * 8 + (int32_t)(bit >> 6));
+      float v = vox_size(vx, L);
+      v3 p = add(muls(muls(vi2f(org(vx, L)), v), 8.0f), muls(adds(vi2f(c), 0.5f), v));
+      v3 E = dyn_e(b, prev, p, P);
+      v3 alb = V(dyn_word_at(dl, base, 10u, L), dyn_word_at(dl, base, 11u, L), dyn_word_at(dl, base, 12u, L));
+      v3 a = mul(divs(alb, PI_F), E);
+      float add3[3] = {a.x, a.y, a.z};
+      dyn_add_radiance(dl, base, L, add3);
+    }
+  }
+}
+
 int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *F, float *inj_out) {
+  /* phase 31: the layer receives the previous frame's volume (the last one written) before it is swapped */
+  const int objects = b->objects && vx->dyn;
+  if (objects) dyn_inject_bounce(b, vx, (orc_dyn *)vx->dyn, b->vol[b->list[2]]);
   /* bnClear */
   b->list[0] = 0u; b->list[1] += 1u; b->list[2] ^= 1u;
   float *cur = b->vol[b->list[2]];
@@ -623,7 +691,14 @@ int orc_bounce_frame(orc_bounce *b, const orc_vox *vx, const float *F, float *in
     uint32_t i = b->list[4u + slot];
     i3 c = I((int32_t)(i % b->dx), (int32_t)((i / b->dx) % b->dy), (int32_t)(i / (b->dx * b->dy)));
     v3 p = muls(vi2f(I(o.x + c.x, o.y + c.y, o.z + c.z)), b->cell);
-    for (uint32_t r = 0; r < b->rays; r++) bn_trace(&cx, b, p, fromf(b->dirs + 4u * r), 1e9f, rad[r]);
+    for (uint32_t r = 0; r < b->rays; r++) {
+      bn_trace(&cx, b, p, fromf(b->dirs + 4u * r), 1e9f, rad[r]);
+      if (objects) {   /* bnTraceDyn (bounce.ts:169-174): the layer in front of the static result, one ray's cone */
+        float oo[3] = {p.x, p.y, p.z}, dd[3] = {b->dirs[4u * r], b->dirs[4u * r + 1u], b->dirs[4u * r + 2u]}, dl[4];
+        orc_trace_dyn(vx, oo, dd, 0.0f, fminf_(rad[r][3], 1e4f), sqrtf((4.0f * PI_F) / (float)b->rays), dl);
+        for (int k = 0; k < 3; k++) rad[r][k] = dl[k] + (1.0f - dl[3]) * rad[r][k];
+      }
+    }
     for (uint32_t a = 0; a < 6u; a++) {
       float t[4];
       bn_trace(&cx, b, p, bn_axis_vec(a), 1.5f * b->cell, t);

@@ -1823,8 +1823,16 @@ int gi_rc_set_dyn(gi_rc *r, gi_dyn *d) {
   r->dev.dyn_hdr = d ? d->dev.hdr : nullptr;
   r->dev.dyn_ptr = d ? d->dev.ptr : nullptr;
   r->dev.dyn_data = d ? d->dev.data : nullptr;
+  r->dev.dyn_meta = d ? d->dev.meta : nullptr;
   r->dev.dyn_nb = d ? d->dev.nb : 0u;
   if (r->graph) { cudaGraphExecDestroy(r->graph); r->graph = nullptr; r->graph_vox = nullptr; }   // captured without it
+  return GI_OK;
+}
+
+int gi_rc_set_objects(gi_rc *r, int on) {
+  if (!r) return fail(GI_ERR_INVALID, "gi_rc_set_objects: NULL rc");
+  r->dev.objects = on ? 1u : 0u;
+  r->gen++;
   return GI_OK;
 }
 

@@ -18,7 +18,6 @@
 
 namespace gi {
 
-constexpr float DYN_FIX = 65536.0f;
 constexpr uint32_t DYN_NONE = 0xffffffffu;
 
 __device__ __forceinline__ f3 dyn_lo(const VoxDev &v, uint32_t L) { return mk(v.box_lo[L][0], v.box_lo[L][1], v.box_lo[L][2]); }

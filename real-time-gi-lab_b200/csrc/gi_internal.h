@@ -55,8 +55,10 @@ struct RcDev {
   const uint4 *bn_inj;     // multi-bounce on: per voxel the bounce volume's irradiance on its two sides (bnInject)
   const uint32_t *dyn_hdr; // the dynamic layer the traces read (gi_rc_set_dyn; null: none): header, pointers, data
   const uint32_t *dyn_ptr;
-  const uint32_t *dyn_data;
-  uint32_t dyn_nb, pad_dyn;
+  uint32_t *dyn_data;      // (written only by dynInject, objects on)
+  const uint32_t *dyn_meta;  // slot -> brick pointer index (dynInject)
+  uint32_t dyn_nb;
+  uint32_t objects;        // token obj (phase 31): the layer receives the bounce volume and the volume's rays read it
 };
 
 // The dynamic layer (dynlayer.ts): header (64 words), a pointer per brick of every level (slot, DYN_EMPTY or
@@ -70,6 +72,7 @@ struct DynDev {
   uint32_t look_cap, pad;
 };
 constexpr uint32_t DYN_W = 13, DYN_EMPTY = 0xffffffffu, DYN_DROPPED = 0xfffffffdu;
+constexpr float DYN_FIX = 65536.0f;   // level-0 words: fixed point x 65536
 
 // World probes (the method 'world', rc.ts:253-570): per cascade a hash table of probe keys, the probes compacted from
 // it in slot order, and the parents each probe merges; the c0 history of two solves.  Probes and atlas entries are laid

@@ -998,9 +998,13 @@ __device__ __forceinline__ f3 bn_axis_vec(uint32_t a) {
   const float sg = (a & 1u) == 1u ? -1.0f : 1.0f;
   return a / 2u == 0u ? mk(sg, 0.0f, 0.0f) : (a / 2u == 1u ? mk(0.0f, sg, 0.0f) : mk(0.0f, 0.0f, sg));
 }
-__global__ void __launch_bounds__(256) k_bn_rays(BounceDev b, VoxDev v, const float *__restrict__ F,
-                                                 const float *__restrict__ unorm8) {
+// DYN (objects on, a layer bound): the irradiance rays read the dynamic layer in front of the static result at the
+// width of one ray's cone (bnTraceDyn, bounce.ts:169-174)
+template <bool DYN>
+__global__ void __launch_bounds__(256) k_bn_rays(BounceDev b, VoxDev v, RcDev r) {
   grid_dep_wait();
+  const float *__restrict__ F = r.frame;
+  const float *__restrict__ unorm8 = r.unorm8;
   const uint32_t per = b.rays + 6u, total = b.list[0] * per;
   const uint2 *prev = b.vol[b.list[2] ^ 1u];
   const i3 o = bn_origin_now(b, F);
@@ -1013,6 +1017,12 @@ __global__ void __launch_bounds__(256) k_bn_rays(BounceDev b, VoxDev v, const fl
     if (k < b.rays) {
       const float4 dv = b.dirs[k];
       res = bn_trace(v, F, unorm8, b, prev, p, mk(dv.x, dv.y, dv.z), 1e9f);
+      if (DYN) {
+        const float4 dl = trace_dyn(r, v, p, mk(dv.x, dv.y, dv.z), 0.0f, mn(res.w, 1e4f),
+                                    sqrtf((4.0f * GI_PI) / (float)b.rays));
+        const float s = 1.0f - dl.w;
+        res = make_float4(dl.x + s * res.x, dl.y + s * res.y, dl.z + s * res.z, res.w);
+      }
     } else {
       res = make_float4(0.0f, 0.0f, 0.0f,
                         mx(mn(bn_trace(v, F, unorm8, b, prev, p, bn_axis_vec(k - b.rays), 1.5f * b.cell).w, 1.5f * b.cell), 1e-3f));
@@ -1095,12 +1105,93 @@ __global__ void __launch_bounds__(256) k_bn_inject(BounceDev b, VoxDev v) {
   }
 }
 
-// One frame of the bounce volume (Bounce.encode, bounce.ts:356-368), at the start of the trace pass
-static cudaError_t launch_bounce(const BounceDev &b, const VoxDev &v, const float *frame, const float *unorm8,
-                                 uint32_t sm_count, cudaStream_t st) {
+// dynE of the bounce volume (bounce.ts:267-296): the irradiance at p of a dynamic voxel with projected areas P over its
+// six axis faces, E = sum_a P_a E_a / sum_a P_a, E_a trilinear over the 8 probes around p with bnRead's rules (active,
+// reach, side of the face)
+__device__ f3 dyn_e(const BounceDev &b, const uint2 *vol, f3 p, const float P[6]) {
+  const i3 org0 = bn_origin(b, vol);
+  const f3 g = mk(p.x / b.cell, p.y / b.cell, p.z / b.cell) - vi2f(org0);
+  const i3 bb = vfloori(g);
+  const f3 fr = g - vi2f(bb);
+  const float tol = 0.5f * b.v0;
+  f3 e[6];
+  float ws[6];
+#pragma unroll
+  for (int a = 0; a < 6; a++) { e[a] = mk(0.0f, 0.0f, 0.0f); ws[a] = 0.0f; }
+  for (int k = 0; k < 8; k++) {
+    const i3 off = mki(k & 1, (k >> 1) & 1, (k >> 2) & 1);
+    const i3 cc = mki(bb.x + off.x, bb.y + off.y, bb.z + off.z);
+    if (cc.x < 0 || cc.y < 0 || cc.z < 0 || cc.x >= (int)b.dx || cc.y >= (int)b.dy || cc.z >= (int)b.dz) continue;
+    const f3 pp = vi2f(mki(org0.x + cc.x, org0.y + cc.y, org0.z + cc.z)) * b.cell;
+    const f3 u = p - pp;
+    if (bn_axis(b, vol, cc, 0).w <= 0.0f) continue;
+    if (fabsf(u.x) > bn_axis(b, vol, cc, u.x >= 0.0f ? 0 : 1).w + tol || fabsf(u.y) > bn_axis(b, vol, cc, u.y >= 0.0f ? 2 : 3).w + tol
+        || fabsf(u.z) > bn_axis(b, vol, cc, u.z >= 0.0f ? 4 : 5).w + tol) continue;
+    const f3 t3 = mk(off.x == 1 ? fr.x : 1.0f - fr.x, off.y == 1 ? fr.y : 1.0f - fr.y, off.z == 1 ? fr.z : 1.0f - fr.z);
+    const float wt = t3.x * t3.y * t3.z;
+#pragma unroll
+    for (int a = 0; a < 6; a++) {
+      if (P[a] <= 0.0f) continue;
+      const float w = wt * smoothstep_(-0.05f, 0.25f, dot(pp - p, bn_axis_vec((uint32_t)a)) / b.cell);
+      if (w <= 0.0f) continue;
+      const float4 ax = bn_axis(b, vol, cc, a);
+      e[a] = e[a] + mk(ax.x, ax.y, ax.z) * w;
+      ws[a] += w;
+    }
+  }
+  f3 sum = mk(0.0f, 0.0f, 0.0f);
+  float ps = 0.0f;
+#pragma unroll
+  for (int a = 0; a < 6; a++) {
+    if (ws[a] > 1e-6f) sum = sum + (e[a] * P[a]) / ws[a];
+    ps += P[a];
+  }
+  return sum / mx(ps, 1e-9f);
+}
+
+// dynInject (dynlayer.ts:173-191), phase 31: before this frame's volume, every voxel of the layer's allocated bricks
+// with area adds albedo / pi times dynE of the previous frame's volume to its radiance words (level 0 in fixed point,
+// the levels above in f32).  One thread per voxel slot; each thread owns its voxel's words.
+__global__ void __launch_bounds__(256) k_dyn_inject(RcDev r, BounceDev b, VoxDev v) {
+  grid_dep_wait();
+  const uint2 *prev = b.vol[b.list[2]];   // the volume written last (k_bn_clear swaps after this)
+  const uint32_t G = v.G, G3 = G * G * G;
+  const uint32_t n = min(r.dyn_hdr[8], r.dyn_nb) * 512u;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const uint32_t slot = i >> 9, bit = i & 511u;
+    const uint32_t pi = r.dyn_meta[slot], L = pi / G3, rr = pi % G3;
+    const uint32_t base = i * DYN_W;
+    if (dyn_word(r, base, 6u, L) <= 0.0f) continue;
+    float P[6];
+#pragma unroll
+    for (uint32_t k = 0; k < 6u; k++) P[k] = dyn_word(r, base, k, L);
+    const i3 c = mki((int)(rr % G) * 8 + (int)(bit & 7u), (int)((rr / G) % G) * 8 + (int)((bit >> 3) & 7u),
+                     (int)(rr / (G * G)) * 8 + (int)(bit >> 6));
+    const float vs = vox_size(v, L);
+    const f3 p = region_lo(v, L) + adds(vi2f(c), 0.5f) * vs;
+    const f3 E = dyn_e(b, prev, p, P);
+    const f3 alb = mk(dyn_word(r, base, 10u, L), dyn_word(r, base, 11u, L), dyn_word(r, base, 12u, L));
+    const f3 add = (alb / GI_PI) * E;
+    const float a3[3] = {add.x, add.y, add.z};
+#pragma unroll
+    for (uint32_t k = 0; k < 3u; k++) {
+      uint32_t *w = &r.dyn_data[base + 7u + k];
+      if (L == 0u) *w += __float2uint_rz(rintf(a3[k] * DYN_FIX));
+      else *w = __float_as_uint(__uint_as_float(*w) + a3[k]);
+    }
+  }
+}
+
+// One frame of the bounce volume (Bounce.encode, bounce.ts:356-368), at the start of the trace pass; with objects on
+// and a layer bound, dynInject first and the irradiance rays reading the layer
+static cudaError_t launch_bounce(const BounceDev &b, const VoxDev &v, const RcDev &r, uint32_t sm_count, cudaStream_t st) {
+  const float *frame = r.frame;
+  const bool dyn = r.objects && r.dyn_hdr;
+  if (dyn) GI_TRY(gi_launch(k_dyn_inject, sm_count * 8u, 256, st, r, b, v));
   GI_TRY(gi_launch(k_bn_clear, 1, 32, st, b));
   GI_TRY(gi_launch(k_bn_classify, (b.n + 1u + 255u) / 256u, 256, st, b, v, frame));
-  GI_TRY(gi_launch(k_bn_rays, sm_count * 4u, 256, st, b, v, frame, unorm8));
+  if (dyn) GI_TRY(gi_launch(k_bn_rays<true>, sm_count * 4u, 256, st, b, v, r));
+  else GI_TRY(gi_launch(k_bn_rays<false>, sm_count * 4u, 256, st, b, v, r));
   GI_TRY(gi_launch(k_bn_sum, sm_count, 256, st, b));
   GI_TRY(gi_launch(k_bn_inject, sm_count * 8u, 256, st, b, v));
   return cudaSuccess;
@@ -1238,7 +1329,7 @@ static cudaError_t launch_solve(const RcDev &r, const VoxDev &v, uint32_t sm_cou
   if (ev) cudaEventRecord(ev[0], st);
   GI_TRY(gi_launch(k_setup_screen, (r.probes_total + 255u) / 256u, 256, st, r, v));
   if (ev) cudaEventRecord(ev[1], st);
-  if (bn) GI_TRY(launch_bounce(*bn, v, r.frame, r.unorm8, sm_count, st));   // counted in giTrace, as the reference
+  if (bn) GI_TRY(launch_bounce(*bn, v, r, sm_count, st));   // counted in giTrace, as the reference
   RcLaunch d = {8u, 3u, 256u};
   if (ls) d = *ls;
   uint32_t tb = min((r.rays_total + 255u) / 256u, sm_count * d.trace_blocks);

@@ -838,7 +838,7 @@ static cudaError_t launch_world(const RcDev &r, const VoxDev &v, const WorldDev 
   }
   if (N >= 2) GI_TRY(pair(W_LINK, N - 2u, nb_warps(N - 2u), W_NONE_TASK, 0, 0));
   if (ev) cudaEventRecord(ev[1], st);
-  if (bn) GI_TRY(launch_bounce(*bn, v, r.frame, r.unorm8, sm_count, st));
+  if (bn) GI_TRY(launch_bounce(*bn, v, r, sm_count, st));
   const uint32_t tb = sm_count * (ls ? ls->trace_blocks : 8u);
   if (r.dyn_hdr) GI_TRY(gi_launch(k_w_trace<A, true>, tb, 256, st, r, v, w, counter));
   else GI_TRY(gi_launch(k_w_trace<A, false>, tb, 256, st, r, v, w, counter));

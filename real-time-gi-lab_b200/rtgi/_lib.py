@@ -96,6 +96,7 @@ SIGNATURES = {
     "gi_dyn_bytes": (C.c_int, [_P, C.POINTER(C.c_uint64)]),
     "gi_dyn_destroy": (C.c_int, [_P]),
     "gi_rc_set_dyn": (C.c_int, [_P, _P]),
+    "gi_rc_set_objects": (C.c_int, [_P, C.c_int]),
 }
 
 

@@ -252,6 +252,8 @@ class Rc:
         else:
             _lib.call("gi_rc_create", ctx.handle, C.byref(p), width, height, C.byref(h))
         self.handle = h
+        if params.objects:
+            self.set_objects(True)
 
     def set_frame(self, frame: np.ndarray, stream=None):
         frame = np.ascontiguousarray(frame, dtype=np.float32)
@@ -314,6 +316,11 @@ class Rc:
     def set_dyn(self, dyn: Optional["DynLayer"]):
         """The dynamic layer the traces read (gi_rc_set_dyn); gi_solve builds it after the static rebuild."""
         _lib.call("gi_rc_set_dyn", self.handle, dyn.handle if dyn is not None else None)
+
+    def set_objects(self, on: bool):
+        """The token obj (phase 31): the bound layer's objects receive the bounce volume's light and block and
+        reflect the volume's rays (gi_rc_set_objects); set from RcParams.objects at creation."""
+        _lib.call("gi_rc_set_objects", self.handle, 1 if on else 0)
 
     def set_debug_hits(self, on: bool):
         _lib.call("gi_rc_set_debug_hits", self.handle, 1 if on else 0)

@@ -152,3 +152,36 @@ def test_log2_definition():
     for x in 2.0 ** xs[:2000]:
         x = float(np.float32(x))
         assert abs(bind.log2(x) - math.log2(x)) <= 2e-7 * max(1.0, abs(math.log2(x)))
+
+
+def test_objects_receive_the_bounce_volume(world):
+    """The token obj (phase 31) in the oracle: from the second frame on, dynInject adds albedo / pi times the previous
+    volume's irradiance to the layer's radiance words (level 0 in fixed point: never less than before); a layer without
+    albedo words receives nothing; the volume's rays, which read the layer, then differ from a volume without it."""
+    s, objs, first, v, st0, F = world
+    bn = {"cell": 0.8, "dims": (16, 8, 16), "rays": 16, "div": 1}
+    runs = {}
+    for name, albedo, objects in (("obj", True, True), ("plain", True, False), ("no-albedo", False, True)):
+        st = dict(st0)
+        dl = bind.Dyn(st, 512, albedo=albedo)
+        ob = bind.Bounce(st, objects=objects, **bn)
+        grew = 0
+        for f in range(2):
+            dl.build(s, st, first, s.triangle_count, F)
+            st["dyn"] = dl
+            before = dl.arrays["data"].copy()
+            ob.frame(st, F)
+            after = dl.arrays["data"]
+            if f == 0 or not objects or not albedo:
+                assert np.array_equal(after, before), f"{name}, frame {f}: the layer changed"
+            else:
+                h = dl.arrays["hdr"]
+                s0, n0 = int(h[16]), int(h[24])
+                a = after.reshape(-1, 512, 13)[s0:s0 + n0, :, 7:10]
+                b = before.reshape(-1, 512, 13)[s0:s0 + n0, :, 7:10]
+                assert (a >= b).all(), "level 0 receives non-negative light (fixed point)"
+                grew = int((a > b).sum())
+        runs[name] = (grew, [x.copy() for x in ob.vol])
+    assert runs["obj"][0] > 100
+    # the volume's rays see the objects: its second volume differs from the one traced without the layer
+    assert not np.array_equal(runs["obj"][1][1], runs["plain"][1][1])

@@ -118,3 +118,73 @@ def test_dyn_layer_and_traces(cfg):
     finally:
         for h in (rc, dyn, vw, sg, ctx):
             h.destroy()
+
+
+BOUNCE = {"cell": 0.8, "dims": (16, 8, 16), "rays": 16, "div": 2}
+
+
+def test_objects_receive_and_block_the_bounce():
+    """The token obj (phase 31) over three frames with the boxes moving: before each frame's bounce volume the layer's
+    voxels receive the previous volume (dynInject), and the volume's irradiance rays read the layer (bnTraceDyn).
+    Compared with the oracle's frames: the layer's words after the injection (bit for bit), both bounce volumes, the
+    probe list and the static voxels' injected irradiance (bit for bit), and the irradiance."""
+    s, objs, first = _scene()
+    p = configs.parse_config("screen-8-voxel-f32-dda256-obj", {"cascades": 4})
+    assert p.objects
+    v = configs.vox_params(VOX)
+    lay = configs.cascade_layout(p, W, H)
+    F = gi_cases._frame(s, W, H, p, sun_e=fr.SUN_E, sky=fr.SKY, shadow=True)
+    ctx = gpu.Context(0)
+    sg = gpu.SceneGpu(ctx, s)
+    sg.set_static_count(first)
+    vw = gpu.VoxWorld(sg, v)
+    rc = gpu.Rc(ctx, p, W, H)
+    dyn = gpu.DynLayer(vw, first, bricks=512, albedo=True)
+    rc.set_dyn(dyn)
+    rc.set_bounce(vw, **BOUNCE)
+    dl = ob = None
+    received = 0
+    try:
+        for f, t in enumerate((0.0, 0.3, 0.6)):
+            sc = _posed(s, objs, t)
+            if f:
+                sg.update_vertices(objs.first, sc.positions[objs.first:], sc.normals[objs.first:])
+            rc.set_frame(F)
+            rc.render_gbuffer(sg)
+            rc.render_shadow(sg, SHADOW)
+            vw.update(s.camera.eye)
+            rc.solve(vw)
+            g = dyn.read_state()
+            g_vol = rc.read_buffer(_lib.GI_RC_BOUNCE_VOL).view(np.float16).astype(np.float32).reshape(2, -1)
+            g_list = rc.read_buffer(_lib.GI_RC_BOUNCE_LIST).view(np.uint32)
+            depth = rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).reshape(H, W)
+            normal = rc.read_buffer(_lib.GI_RC_NORMAL).view(np.float16).reshape(H, W, 4).astype(np.float32)
+            shadow = rc.read_shadow()
+            irr = rc.read_irradiance()
+            st = bind.vox_build(dataclasses.replace(sc, tri=sc.tri[:first]), v.v0, v.levels, v.G, v.maxBricks,
+                                v.maxVoxels, s.camera.eye)
+            bind.vox_sun(st, F, shadow)
+            if dl is None:
+                dl = bind.Dyn(st, 512, albedo=True)
+                ob = bind.Bounce(st, objects=True, **BOUNCE)
+            dl.build(sc, st, first, sc.triangle_count, F, shadow)
+            st["dyn"] = dl
+            before = dl.arrays["data"].copy()
+            inj = ob.frame(st, F)
+            received += int((dl.arrays["data"] != before).sum())
+            _check_layer(g, dl, f"frame {f} (after dynInject)")
+            for k in range(2):
+                _eq(g_vol[k].view(np.uint32), ob.vol[k].view(np.uint32), f"frame {f} bounce volume {k}")
+            _eq(g_list[:3], ob.list[:3], f"frame {f} probe list header")
+            nv = int(min(st["hdr"][1], v.maxVoxels))
+            g_inj = rc.read_buffer(_lib.GI_RC_BOUNCE_INJ).view(np.float16).reshape(-1, 8)[:nv]
+            g6 = np.concatenate([g_inj[:, 0:3], g_inj[:, 4:7]], axis=1).astype(np.float32)
+            _eq(g6.view(np.uint32), inj[: nv * 6].reshape(nv, 6).view(np.uint32), f"frame {f} injected irradiance")
+            o = bind.rc_solve(st, lay, F, depth, normal)
+            valid = o["irr"][..., 3] > 0
+            np.testing.assert_allclose(irr[valid], o["irr"][valid], rtol=1e-4, atol=1e-4 * np.abs(o["irr"]).max(),
+                                       err_msg=f"frame {f} irradiance")
+        assert received > 100, "the moving boxes received the volume's light"
+    finally:
+        for h in (rc, dyn, vw, sg, ctx):
+            h.destroy()

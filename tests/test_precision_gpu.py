@@ -52,12 +52,19 @@ def test_f64_reference_matches_oracle(ctx):
     # same double operations in the same order; only exp() may differ in the last bit
     np.testing.assert_allclose(irr64, ref, rtol=1e-12, atol=1e-12 * scale)
     # the storage of some cascades rounded to f16 (round to nearest even, in the traced intervals and the merged
-    # radiances above cascade 0), every stage still in double
+    # radiances above cascade 0), every stage still in double.  Rounding a merged radiance to f16 is discontinuous: where
+    # exp()'s last bit moves it across a rounding boundary, GPU and oracle store neighbouring f16 values, so those
+    # masks agree to 1e-12 except at a few pixels, which stay within a fraction of one f16 step.
     for mask, got in rounded.items():
         want = bind.merge_gather_f64(lay, case.frame, depth, normal.astype(np.float32), probes, traced, f16_cascades=mask)
         assert np.array_equal(got[..., 3], want[..., 3])
-        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * scale, err_msg=f"f16 cascades {mask:05b}")
         assert not np.array_equal(got, irr64)
+        if mask == 0b00001:   # cascade 0: only the traced intervals (identical inputs) are rounded
+            np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * scale, err_msg=f"f16 cascades {mask:05b}")
+            continue
+        off = np.abs(got - want) > 1e-12 * scale + 1e-12 * np.abs(want)
+        assert off.mean() < 0.01, f"f16 cascades {mask:05b}: {off.mean():.4f} of the values differ"
+        np.testing.assert_allclose(got, want, rtol=2.0 ** -14, atol=2.0 ** -14 * scale, err_msg=f"f16 cascades {mask:05b}")
     # the f32 path's irradiance against its own FP64 merge + gather
     valid = ref[..., 3] > 0
     d = irr32[..., :3][valid].astype(np.float64) - ref[..., :3][valid]
