@@ -354,8 +354,8 @@ int gi_rc_read_irradiance_f64(gi_rc *rc, double *rgba, void *stream);
 /* Launch tuning (no counterpart in the reference; results do not depend on it, tested bit-exact).  Picked per solve
  * shape by the autotuner (rtgi/autotune.py); takes effect at the next solve or graph capture. */
 typedef struct gi_rc_tuning {
-  uint32_t trace_order;    /* 0: probe-major (a warp's lanes take consecutive directions of a probe, coalesced atlas
-                              writes), 1: direction-major (a warp's lanes take one direction of 32 neighbouring probes,
+  uint32_t trace_order;    /* 0: probe-major (a warp's lanes take an 8 x 4 tile of a probe's direction map, or all
+                              of a small map: neighbouring directions walk alike; atlas writes in 128-byte runs), 1: direction-major (a warp's lanes take one direction of 32 neighbouring probes,
                               coherent voxel paths), 2: walk-length order (screen probes; the rays by the previous
                               solve's DDA step count and hit, longest first, so a warp's lanes walk alike: for a camera
                               that holds still, as the keys come from the previous solve's rays and screen probes move

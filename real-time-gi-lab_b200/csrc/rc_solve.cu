@@ -482,6 +482,15 @@ __global__ void k_setup_screen(RcDev r, VoxDev v) {
   if (i < r.probes_total) setup_probe(r, v, i);
 }
 
+// The direction a probe's k-th ray takes in the probe-major orders: 32 consecutive rays (a warp) take an 8 x 4 tile of
+// the probe's direction map, tiles row by row (res >= 16; a smaller map is one or two warps as it is).  Neighbouring
+// directions walk alike, so a warp's lanes idle less than on 32 directions of a row.  A bijection of [0, res^2).
+__device__ __forceinline__ uint32_t dir_tile(const CascDev &L, uint32_t k) {
+  if (L.res < 16u) return k;
+  const uint32_t w = k & 31u, tt = k >> 5, tl = L.dirs_log2 / 2u - 3u;   // res / 8 = 2^tl tiles per row
+  return (((tt >> tl) << 2) + (w >> 3)) * L.res + ((tt & ((1u << tl) - 1u)) << 3) + (w & 7u);
+}
+
 // trace (rc.ts:600-622) -> traceWorld (rc.ts:216-245) of the ray at position j of the trace order (cascade c): writes
 // its atlas element (and the debug copies); true when its probe is valid and the ray was marched.
 template <int A, bool DYN = false>
@@ -495,9 +504,10 @@ __device__ __forceinline__ bool trace_ray(const RcDev &r, const VoxDev &v, uint3
   bool traced = false;
   const CascDev &L = r.c[c];
   uint32_t t = j - L.ray_off, pi, di;
-  if (probe_major) {                  // probe-major: the atlas order
+  if (probe_major) {                  // probe-major: a probe's rays together; a warp's on neighbouring directions
     pi = t >> L.dirs_log2;
     di = t & ((1u << L.dirs_log2) - 1u);
+    di = dir_tile(L, di);
   } else {                            // direction-major: one direction over consecutive probes
     di = t / L.np;
     pi = t - di * L.np;

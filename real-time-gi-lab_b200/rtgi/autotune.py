@@ -1,7 +1,7 @@
 """Autotuner of the launch shapes of one solve (no counterpart in the reference, whose workgroup sizes are fixed in its
 WGSL).  The tunables change how work is laid onto the GPU, never the result (tested bit-exact):
 
-  giTrace   trace_order (probe-major: a warp's lanes take a probe's consecutive directions, coalesced atlas writes;
+  giTrace   trace_order (probe-major: a warp's lanes take an 8 x 4 tile of a probe's directions, alike walks;
             direction-major: one direction over 32 neighbouring probes, coherent voxel paths), trace_rays (rays per
             lane per queue fetch), trace_blocks (resident blocks per SM of the persistent trace).  The walk-length
             order (trace_order 2) is left out: it pays only while the camera holds still, and the tuner's repeated

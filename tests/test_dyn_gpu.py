@@ -185,6 +185,16 @@ def test_objects_receive_and_block_the_bounce():
             np.testing.assert_allclose(irr[valid], o["irr"][valid], rtol=1e-4, atol=1e-4 * np.abs(o["irr"]).max(),
                                        err_msg=f"frame {f} irradiance")
         assert received > 100, "the moving boxes received the volume's light"
+        # a graph captured with the objects on is refused once they are turned off
+        import torch
+        st = torch.cuda.Stream()
+        torch.cuda.synchronize()
+        rc.graph_capture(vw, st)
+        rc.graph_launch(st)
+        rc.set_objects(False)
+        with pytest.raises(_lib.GiError):
+            rc.graph_launch(st)
+        st.synchronize()
     finally:
         for h in (rc, dyn, vw, sg, ctx):
             h.destroy()
