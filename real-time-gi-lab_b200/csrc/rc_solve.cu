@@ -589,8 +589,10 @@ __global__ void __launch_bounds__(256) k_rsort_scatter(RcDev r) {
   }
 }
 
-// Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time.  SORT: positions go through the
-// walk-length order (rperm) and each ray's key is stored for the next solve.
+// Persistent: every warp takes rays from a global counter, 32 x trace_rays at a time, the top cascade's first (its
+// walks are the longest; a queue that ended on them left SMs idle behind its last warps: 0.197 -> 0.170 ms on the
+// colonnade).  SORT: positions go through the walk-length order (rperm) and each ray's key is stored for the next
+// solve.
 template <int A, bool DYN, bool SORT>
 __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_counter) {
   grid_dep_wait();
@@ -607,6 +609,7 @@ __global__ void __launch_bounds__(256) k_trace(RcDev r, VoxDev v, uint32_t *ray_
     uint32_t j = base + k * 32u + lane;   // position in the trace order
     bool live = j < r.rays_total;
     if (SORT && live) j = r.rperm[j];     // the atlas element at that position
+    else if (live) j = r.rays_total - 1u - j;   // the top cascade first: the queue ends on the shortest walks
     uint32_t c = live ? casc_of_ray(r, j) : 0u;
     TraceOut out;
     out.steps = 0;

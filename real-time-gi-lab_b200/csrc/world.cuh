@@ -498,8 +498,9 @@ __global__ void __launch_bounds__(256) k_w_trace(RcDev r, VoxDev v, WorldDev w, 
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
     for (uint32_t k = 0; k < r.trace_rays; k++) {
-      const uint32_t j = base + k * 32u + lane;
-      const bool live = j < total;
+      const uint32_t j0 = base + k * 32u + lane;
+      const bool live = j0 < total;
+      const uint32_t j = live ? total - 1u - j0 : 0u;   // the top cascade first: the queue ends on the shortest walks
       uint32_t c = 0;
       for (uint32_t q = 1; q < r.cascades; q++)
         if (j >= s_first[q]) c = q;
