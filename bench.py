@@ -623,7 +623,7 @@ def run_world(args, ctx, stream, sg, vw, s, W, H, v, desc, flush, dist, world):
     return out
 
 
-def run_e2e(ctx, vw, p, W, H, F, host, shadow, tuned, n, dist, world, slots=3):
+def run_e2e(ctx, vw, p, W, H, F, host, shadow, tuned, n, dist, world, slots=2):
     """host: (frame, depth, normal) pinned tensors; a normal tensor of 3 halves per pixel is uploaded as rgb16f."""
     """Solves/s through rtgi.pipeline with host buffers: every step uploads its frame and G-buffer from pinned memory
     and downloads its irradiance into pinned memory, the copies of neighbouring frames overlapping the solve."""
@@ -745,7 +745,7 @@ def run_ours(args, rank, world, local_rank):
 
     # end to end through the public API with host buffers: every step copies its frame + G-buffer from pinned host
     # memory and reads its irradiance back into pinned host memory; rtgi.pipeline overlaps those copies of
-    # neighbouring frames with the solve (three cascade sets, upload / compute / download streams)
+    # neighbouring frames with the solve (two cascade sets, upload / compute / download streams)
     depth_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_DEPTH).view(np.float32).copy()).pin_memory()
     normal_h = torch.from_numpy(rc.read_buffer(_lib.GI_RC_NORMAL).view(np.uint16).copy()).pin_memory()
     frame_h = torch.from_numpy(F.copy()).pin_memory()
@@ -757,8 +757,8 @@ def run_ours(args, rank, world, local_rank):
     # the same with four halves per normal, and with the irradiance stored and read back as f32 as well
     e2e_more = {"rgba16f_normals": run_e2e(ctx, vw, p, W, H, F, (frame_h, depth_h, normal_h), shadow_in, tuned, n_e2e,
                                            dist, world),
-                "two_slots": run_e2e(ctx, vw, p, W, H, F, (frame_h, depth_h, normal_rgb_h), shadow_in, tuned, n_e2e,
-                                     dist, world, slots=2)}
+                "three_slots": run_e2e(ctx, vw, p, W, H, F, (frame_h, depth_h, normal_rgb_h), shadow_in, tuned, n_e2e,
+                                       dist, world, slots=3)}
     if p.irr16:
         e2e_more["rgba16f_normals_f32_irradiance"] = run_e2e(ctx, vw, dataclasses.replace(p, irr16=False), W, H, F,
                                                               (frame_h, depth_h, normal_h), shadow_in, tuned, n_e2e,

@@ -3,9 +3,8 @@ submits one frame per queue and maps its readback buffer when the frame is done,
 
 Each frame's inputs (the 640-byte frame block, depth f32, normal rgba16f or its rgb halves) are copied from pinned host memory on an
 upload stream, the frame is solved (voxel rebuild + cascades, one captured graph) on the compute stream, and its
-irradiance is copied back on a download stream.  `slots` cascade sets take turns (three by default: on the colonnade
-1989 frames/s against 1857 with two), so the uploads of the next frames and the download of the last run while frame k
-is solved: the step time approaches the slower of the PCIe copies and the solve
+irradiance is copied back on a download stream.  `slots` cascade sets take turns (two by default; three measured the
+same on the colonnade), so the upload of the next frame and the download of the last run while frame k is solved: the step time approaches the slower of the PCIe copies and the solve
 instead of their sum.  The voxel world is shared and only the compute stream touches it, so solves stay in order.
 """
 from __future__ import annotations
@@ -17,7 +16,7 @@ from . import gpu
 
 class FramePipeline:
     def __init__(self, ctx: gpu.Context, vox: gpu.VoxWorld, params, width: int, height: int, frame, depth_ptr: int,
-                 normal_f16_ptr: int, slots: int = 3, shadow=None, tuning=None, normal_rgb: bool = False):
+                 normal_f16_ptr: int, slots: int = 2, shadow=None, tuning=None, normal_rgb: bool = False):
         """frame/depth/normal: a first frame's inputs (frame as an array, the G-buffer as pinned host pointers), used
         to capture each slot's graph.  shadow: (SceneGpu, size) to give every slot the sun's shadow map drawn from
         that frame (a static sun and scene; draw it again with Rc.render_shadow when they move).  tuning: launch
